@@ -1,0 +1,335 @@
+"""Benchmark: FP64 particle-turns/s of elegant's tracking path on B200.
+
+Workload: the ring with RF and longitudinal wake (40 FODO cells with KQUAD,
+KSEXT, CSBEND, DRIF, one RFCA and one WAKE with a 4096-point resonator Green
+function on 2000 bins, CHARGE 1 nC), 1e6 particles from a seeded Gaussian
+beam.  One step is one pass (turn) of the whole beam.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+value : particle-turns/s with the beam resident on the device; each step is
+        timed with CUDA events on the tracking stream, the L2 is flushed
+        (a 512 MiB write) between timed steps and outside their events.
+e2e   : the same metric through the C ABI with host buffers: each step loads
+        the beam from pinned host memory, tracks one turn and stores it back.
+roofline: FP64 bound; achieved = algorithmic FP64 flops per particle-turn
+        (counted on the reference formulation, oracle/flops.json) times
+        particle-turns/s, against the FP64 peak measured in this run by a
+        dependent-FMA kernel (MEASURED_PEAKS.json has no FP64 figure).
+--impl reference: the oracle (CPU restatement of the reference's element
+        functions) on the host cores, process-parallel by particle shards.
+Multi-GPU: one process per GPU; each rank tracks its own particle shard
+(weak scaling), the wake histogram and time statistics are all-reduced.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_PARTICLES = 1_000_000
+WORKLOAD = "ring_rf_wake_fodo40_1e6"
+
+
+def workload_config(n_particles):
+    return {"workload": WORKLOAD, "particles_per_gpu": n_particles, "lattice": "40 FODO cells + KSEXT, RFCA, WAKE",
+            "wake_bins": 2000, "wake_points": 4096, "p_central": 13700.0, "l2": "flushed between timed steps"}
+
+
+def load_flops():
+    p = os.path.join(ROOT, "oracle", "flops.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}",
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            for k, n in enumerate(names):
+                if len(s) > 4 + k and s[4 + k].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def cpu_baseline(impl_reference=False, cores=None, sample_particles=2000, sample_turns=2):
+    """Time the oracle on the host: particle-turns/s on a bounded sample."""
+    from elegant_b200 import configs
+    if cores is None:
+        cores = 1
+    lat = configs.c2_lattice()
+    if cores == 1:
+        from oracle import pyoracle
+        beam = configs.gaussian_beam(sample_particles, seed=1)
+        pyoracle.load()
+        t0 = time.perf_counter()
+        _, _, eff = pyoracle.track(lat, beam, sample_turns, configs.P_CENTRAL)
+        dt = time.perf_counter() - t0
+        return {"value": eff / dt, "unit": "particle-turns/s", "cores": 1, "kind": "port",
+                "sample": f"{sample_particles} particles x {sample_turns} turns of the same lattice, 1 core"}
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    per = sample_particles
+    with ctx.Pool(cores) as pool:
+        args = [(per, sample_turns, 1 + k) for k in range(cores)]
+        pool.map(_oracle_shard, [(10, 1, 99)] * cores)  # warm the workers
+        t0 = time.perf_counter()
+        effs = pool.map(_oracle_shard, args)
+        dt = time.perf_counter() - t0
+    return {"value": sum(effs) / dt, "unit": "particle-turns/s", "cores": cores, "kind": "port",
+            "sample": f"{cores} processes x {per} particles x {sample_turns} turns (particle shards; wake "
+                      "histograms per shard)"}
+
+
+def _oracle_shard(args):
+    n, turns, seed = args
+    sys.path.insert(0, ROOT)
+    from elegant_b200 import configs
+    from oracle import pyoracle
+    lat = configs.c2_lattice()
+    beam = configs.gaussian_beam(n, seed=seed)
+    _, _, eff = pyoracle.track(lat, beam, turns, configs.P_CENTRAL)
+    return eff
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    cores = os.cpu_count() or 1
+    steps = []
+    for _ in range(args.warmup):
+        cpu_baseline(cores=cores, sample_particles=200, sample_turns=1)
+    for _ in range(args.steps):
+        steps.append(cpu_baseline(cores=cores, sample_particles=1000, sample_turns=1))
+    v = float(np.mean([s["value"] for s in steps]))
+    line = {"metric": "particle-turns/s", "value": v, "unit": "particle-turns/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian beam)",
+            "config": workload_config(N_PARTICLES), "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "particle-turns/s", "cores": cores, "kind": "port",
+                             "sample": steps[0]["sample"]},
+            "e2e": {"value": v, "unit": "particle-turns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--particles", type=int, default=N_PARTICLES)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--exact", action="store_true", help="parity build instead of the fast build")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_gpu(args, rank, world, local)
+
+
+def run_gpu(args, rank, world, local):
+    import torch
+    from elegant_b200 import Tracker, configs
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    n = args.particles
+    lat = configs.c2_lattice()
+    beam = configs.gaussian_beam(n, seed=1 + rank, first_id=1 + rank * n)
+    fast = not args.exact
+    flops = load_flops()
+    with Tracker(local) as trk:
+        trk.load(beam)
+        pass_index = 0
+        for _ in range(max(args.warmup, 3)):
+            trk.track(lat, 1, configs.P_CENTRAL, pass_offset=pass_index, fast=fast)
+            pass_index += 1
+        flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+        stream = torch.cuda.ExternalStream(trk.stream(), device=f"cuda:{local}")
+        step_ms = []
+        effort = 0
+        launches = 0
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clocks:
+            t_wall = time.perf_counter()
+            for k in range(args.steps):
+                with torch.cuda.stream(stream):
+                    flush.fill_(float(k))
+                st = trk.track(lat, 1, configs.P_CENTRAL, pass_offset=pass_index, fast=fast)
+                pass_index += 1
+                step_ms.append(st["device_ms"])
+                effort += st["particle_passes"]
+                launches += st["kernel_launches"]
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t_wall
+        dev_s = sum(step_ms) / 1e3
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([dev_s, float(effort)], dtype=torch.float64, device=f"cuda:{local}")
+            dmax = t[:1].clone()
+            dist.all_reduce(dmax, op=dist.ReduceOp.MAX)
+            dsum = t[1:].clone()
+            dist.all_reduce(dsum, op=dist.ReduceOp.SUM)
+            dev_s = float(dmax.item())
+            effort = float(dsum.item())
+        value = effort / dev_s
+        # end-to-end through the C ABI with host buffers
+        pinned = torch.from_numpy(beam).pin_memory().numpy()
+        e2e_ms = []
+        for k in range(max(2, args.steps // 4)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            trk.load(pinned)
+            st = trk.track(lat, 1, configs.P_CENTRAL, fast=fast)
+            trk.store(stride=7)
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+            e2e_eff = st["particle_passes"]
+        e2e_value = e2e_eff / (np.median(e2e_ms) / 1e3) * world
+    if rank != 0:
+        return 0
+    # roofline: algorithmic FP64 flops per particle-turn
+    peak = measure_fp64_peak(local)
+    roof = None
+    if flops:
+        fpt = flops["flops_per_particle_turn"]["c2"]
+        achieved = fpt * value / world / 1e12
+        roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak if peak else None, "traffic": None,
+                "flops_per_particle_turn": fpt, "peak_source": "measured in this run (dependent-FMA kernel)"}
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        cpu = cpu_baseline(cores=1)
+    line = {"metric": "particle-turns/s", "value": value, "unit": "particle-turns/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": dev_s * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Gaussian beam, seeded resonator wake)", "config": workload_config(n),
+            "build": "fast" if fast else "parity", "wall_s": wall,
+            "e2e": {"value": e2e_value, "unit": "particle-turns/s", "h2d_bytes_per_step": int(n * 7 * 8),
+                    "d2h_bytes_per_step": int(n * 7 * 8)},
+            "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+_PEAK_SRC = r"""
+extern "C" __global__ void fma_peak(double *out, int iters) {
+  double a0 = threadIdx.x * 1e-9, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6, a7 = a0 + 7;
+  const double b = 0.999999999, c = 1e-9;
+  for (int i = 0; i < iters; i++) {
+    a0 = fma(a0, b, c); a1 = fma(a1, b, c); a2 = fma(a2, b, c); a3 = fma(a3, b, c);
+    a4 = fma(a4, b, c); a5 = fma(a5, b, c); a6 = fma(a6, b, c); a7 = fma(a7, b, c);
+  }
+  out[blockIdx.x * blockDim.x + threadIdx.x] = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+}
+"""
+
+
+def measure_fp64_peak(device):
+    """FP64 FMA peak (TFLOP/s, FMA = 2 flops) from a kernel of independent
+    dependent-FMA chains, compiled with the runtime compiler."""
+    try:
+        import torch
+        from cuda.bindings import nvrtc
+    except Exception:
+        try:
+            from cuda import nvrtc  # noqa: F401
+        except Exception:
+            return None
+    try:
+        import ctypes
+        import torch
+        from cuda.bindings import nvrtc, driver
+        prog = nvrtc.nvrtcCreateProgram(_PEAK_SRC.encode(), b"peak.cu", 0, [], [])[1]
+        opts = [b"-arch=sm_100a"]
+        nvrtc.nvrtcCompileProgram(prog, len(opts), opts)
+        size = nvrtc.nvrtcGetCUBINSize(prog)[1]
+        cubin = b" " * size
+        nvrtc.nvrtcGetCUBIN(prog, cubin)
+        torch.cuda.set_device(device)
+        torch.cuda.synchronize()
+        err, mod = driver.cuModuleLoadData(cubin)
+        err, fn = driver.cuModuleGetFunction(mod, b"fma_peak")
+        blocks, threads, iters = 148 * 16, 256, 20000
+        out = torch.empty(blocks * threads, dtype=torch.float64, device=f"cuda:{device}")
+        arg_ptr = ctypes.c_void_p(out.data_ptr())
+        arg_it = ctypes.c_int(iters)
+        params = (ctypes.c_void_p * 2)(ctypes.addressof(arg_ptr), ctypes.addressof(arg_it))
+        stream = torch.cuda.current_stream().cuda_stream
+        for rep in range(2):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            driver.cuLaunchKernel(fn, blocks, 1, 1, threads, 1, 1, 0, stream, ctypes.addressof(params), 0)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+        flops = 2.0 * 8 * iters * blocks * threads
+        return flops / (ms / 1e3) / 1e12
+    except Exception:
+        return None
+
+
+if __name__ == "__main__":
+    sys.exit(main())

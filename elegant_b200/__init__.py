@@ -1,0 +1,309 @@
+"""elegant_b200: B200 particle tracking for elegant's do_tracking() path.
+
+A thin ctypes layer over libtrkgpu.so (C ABI in include/trk.h).  Python is
+the test and benchmark harness; the library itself is C/C++/CUDA.
+
+    lat = Lattice()
+    lat.add("KQUAD", "QF", L=0.3, K1=1.2, N_KICKS=8)
+    ...
+    with Tracker(device=0) as trk:
+        trk.load(coord)                      # (np, >=7) array, column 6 = id
+        stats = trk.track(lat, n_passes=100, p_central=13700.0)
+        n_left, coord_out = trk.store()
+
+do_tracking(coord, lattice, n_passes, p_central) mirrors the reference's
+do_tracking() (src/do_tracking.c:144): the beam is tracked in place,
+survivors are returned first and the survivor count is returned.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtrkgpu.so")
+
+TYPES = ["MARK", "DRIF", "EDRIFT", "KQUAD", "KSEXT", "KOCT", "CSBEND", "RFCA", "WAKE", "TRWAKE", "MAXAMP",
+         "CHARGE"]
+TYPE_CODE = {n: i for i, n in enumerate(TYPES)}
+
+TRK_OK = 0
+
+
+class TrackingError(RuntimeError):
+    """A library call returned a negative trk_error code."""
+
+    def __init__(self, code, message):
+        super().__init__(f"trk error {code}: {message}")
+        self.code = code
+
+
+class _Run(ctypes.Structure):
+    _fields_ = [("p_central", ctypes.c_double), ("n_passes", ctypes.c_long), ("pass_offset", ctypes.c_long),
+                ("fast_math", ctypes.c_int32), ("block_size", ctypes.c_int32), ("compact_every", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("n_total", ctypes.c_long), ("n_left", ctypes.c_long), ("particle_passes", ctypes.c_long),
+                ("device_ms", ctypes.c_double), ("kernel_launches", ctypes.c_long), ("p_central", ctypes.c_double)]
+
+
+_lib = None
+
+
+def _declare(lib):
+    P = ctypes.c_void_p
+    D = ctypes.c_double
+    L = ctypes.c_long
+    I = ctypes.c_int
+    DP = ctypes.POINTER(ctypes.c_double)
+    sig = {
+        "trk_last_error": (ctypes.c_char_p, []),
+        "trk_abi_version": (I, []),
+        "trk_type_code": (I, [ctypes.c_char_p]),
+        "trk_param_count": (I, [I]),
+        "trk_param_name": (ctypes.c_char_p, [I, I]),
+        "trk_param_default": (D, [I, I]),
+        "trk_param_index": (I, [I, ctypes.c_char_p]),
+        "trk_lattice_create": (I, [ctypes.POINTER(P)]),
+        "trk_lattice_destroy": (None, [P]),
+        "trk_lattice_add": (I, [P, I, ctypes.c_char_p, ctypes.POINTER(I)]),
+        "trk_lattice_set": (I, [P, I, ctypes.c_char_p, D]),
+        "trk_lattice_get": (I, [P, I, ctypes.c_char_p, DP]),
+        "trk_lattice_length": (I, [P]),
+        "trk_lattice_set_wake": (I, [P, I, DP, DP, DP, L]),
+        "trk_lattice_parse": (I, [P, ctypes.c_char_p, ctypes.c_char_p]),
+        "trk_lattice_total_length": (D, [P]),
+        "trk_run_defaults": (None, [ctypes.POINTER(_Run)]),
+        "trk_context_create": (I, [ctypes.POINTER(P), I]),
+        "trk_context_destroy": (None, [P]),
+        "trk_context_stream": (P, [P]),
+        "trk_beam_load": (I, [P, DP, L, L]),
+        "trk_beam_load_device": (I, [P, P, L, L]),
+        "trk_beam_store": (I, [P, DP, L, ctypes.POINTER(L), ctypes.POINTER(L), ctypes.POINTER(ctypes.c_int32)]),
+        "trk_beam_count": (I, [P, ctypes.POINTER(L)]),
+        "trk_beam_device_columns": (I, [P, ctypes.POINTER(P), ctypes.POINTER(L), ctypes.POINTER(P)]),
+        "trk_track": (I, [P, P, ctypes.POINTER(_Run), ctypes.POINTER(_Stats)]),
+        "trk_track_ensemble": (I, [P, ctypes.POINTER(P), I, ctypes.POINTER(L), ctypes.POINTER(_Run),
+                                   ctypes.POINTER(_Stats)]),
+        "trk_adjoint": (I, [P, P, ctypes.POINTER(_Run), D, DP, DP, I]),
+        "trk_adjoint_param_count": (I, [P]),
+    }
+    for name, (res, args) in sig.items():
+        if hasattr(lib, name):
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+
+
+def load_library(path=None):
+    """Load libtrkgpu.so; raises if it is missing (no CPU fallback exists)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise ImportError(f"{p} is not built; run elegant_b200/build.py (or __graft_entry__.build())")
+    lib = ctypes.CDLL(p)
+    _declare(lib)
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _check(lib, rc):
+    if rc < 0:
+        raise TrackingError(rc, lib.trk_last_error().decode(errors="replace"))
+    return rc
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Lattice:
+    """An ordered element list with the reference's parameter names.
+
+    Kept in Python so the same lattice can be instantiated in the product
+    library and in the CPU oracle (both expose the trk_lattice_* C API)."""
+
+    def __init__(self):
+        self.elements = []  # (type, name, {param: value}, wake tuple or None)
+
+    def add(self, type_name, name=None, **params):
+        t = type_name.upper()
+        if t not in TYPE_CODE:
+            raise ValueError(f"element type {type_name} is not on this path")
+        self.elements.append([t, name or t, dict((k.upper(), float(v)) for k, v in params.items()), None])
+        return len(self.elements) - 1
+
+    def set(self, index, param, value):
+        self.elements[index][2][param.upper()] = float(value)
+
+    def set_wake(self, index, t, W, Wy=None):
+        self.elements[index][3] = (np.ascontiguousarray(t, dtype=np.float64),
+                                   np.ascontiguousarray(W, dtype=np.float64),
+                                   None if Wy is None else np.ascontiguousarray(Wy, dtype=np.float64))
+
+    def extend(self, other, times=1):
+        for _ in range(times):
+            for e in other.elements:
+                self.elements.append([e[0], e[1], dict(e[2]), e[3]])
+        return self
+
+    def __len__(self):
+        return len(self.elements)
+
+    def indices(self, type_name):
+        return [i for i, e in enumerate(self.elements) if e[0] == type_name.upper()]
+
+    def native(self, lib):
+        """Build a trk_lattice in `lib` (library or oracle); returns a handle."""
+        return _NativeLattice(lib, self)
+
+    def total_length(self):
+        tot = 0.0
+        for t, _, p, _ in self.elements:
+            if t in ("DRIF", "EDRIFT", "KQUAD", "KSEXT", "KOCT", "CSBEND", "RFCA"):
+                tot += p.get("L", 0.0)
+        return tot
+
+
+class _NativeLattice:
+    def __init__(self, lib, lat):
+        self.lib = lib
+        self.ptr = ctypes.c_void_p()
+        _check(lib, lib.trk_lattice_create(ctypes.byref(self.ptr)))
+        self._keep = []
+        try:
+            for t, name, params, wake in lat.elements:
+                idx = ctypes.c_int()
+                _check(lib, lib.trk_lattice_add(self.ptr, TYPE_CODE[t], name.encode(), ctypes.byref(idx)))
+                for k, v in params.items():
+                    _check(lib, lib.trk_lattice_set(self.ptr, idx.value, k.encode(), v))
+                if wake is not None:
+                    tt, W, Wy = wake
+                    _check(lib, lib.trk_lattice_set_wake(self.ptr, idx.value, _dptr(tt), _dptr(W),
+                                                         _dptr(Wy) if Wy is not None else None, len(tt)))
+        except Exception:
+            lib.trk_lattice_destroy(self.ptr)
+            raise
+
+    def close(self):
+        if self.ptr:
+            self.lib.trk_lattice_destroy(self.ptr)
+            self.ptr = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Stats(dict):
+    pass
+
+
+class Tracker:
+    """A device context (one CUDA stream on one GPU) holding a resident beam."""
+
+    def __init__(self, device=0, lib=None):
+        self.lib = lib or load_library()
+        self.ctx = ctypes.c_void_p()
+        _check(self.lib, self.lib.trk_context_create(ctypes.byref(self.ctx), device))
+        self._lat_cache = {}
+
+    def close(self):
+        if self.ctx:
+            self.lib.trk_context_destroy(self.ctx)
+            self.ctx = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load(self, coord):
+        a = np.ascontiguousarray(coord, dtype=np.float64)
+        if a.ndim != 2 or a.shape[1] < 7:
+            raise ValueError("beam must be (np, >=7)")
+        self.np = a.shape[0]
+        _check(self.lib, self.lib.trk_beam_load(self.ctx, _dptr(a), a.shape[0], a.shape[1]))
+
+    def load_device(self, ptr, np_, ld):
+        self.np = np_
+        _check(self.lib, self.lib.trk_beam_load_device(self.ctx, ctypes.c_void_p(ptr), np_, ld))
+
+    def store(self, stride=7, with_loss=False):
+        out = np.zeros((self.np, stride), dtype=np.float64)
+        n_left = ctypes.c_long()
+        if with_loss:
+            lp = np.empty(self.np, dtype=np.int64)
+            le = np.empty(self.np, dtype=np.int32)
+            _check(self.lib, self.lib.trk_beam_store(
+                self.ctx, _dptr(out), stride, ctypes.byref(n_left),
+                lp.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), le.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
+            return n_left.value, out, lp, le
+        _check(self.lib, self.lib.trk_beam_store(self.ctx, _dptr(out), stride, ctypes.byref(n_left), None, None))
+        return n_left.value, out
+
+    def count(self):
+        n = ctypes.c_long()
+        _check(self.lib, self.lib.trk_beam_count(self.ctx, ctypes.byref(n)))
+        return n.value
+
+    def columns(self):
+        cols = (ctypes.c_void_p * 7)()
+        n = ctypes.c_long()
+        loss = (ctypes.c_void_p * 2)()
+        _check(self.lib, self.lib.trk_beam_device_columns(self.ctx, cols, ctypes.byref(n), loss))
+        return [c for c in cols], n.value, [l for l in loss]
+
+    def stream(self):
+        return self.lib.trk_context_stream(self.ctx)
+
+    def native(self, lattice):
+        key = id(lattice)
+        nat = self._lat_cache.get(key)
+        if nat is None or nat[0] is not lattice or nat[2] != _lattice_signature(lattice):
+            nat = (lattice, lattice.native(self.lib), _lattice_signature(lattice))
+            self._lat_cache[key] = nat
+        return nat[1]
+
+    def track(self, lattice, n_passes, p_central, pass_offset=0, fast=True):
+        nat = self.native(lattice)
+        run = _Run()
+        self.lib.trk_run_defaults(ctypes.byref(run))
+        run.p_central = p_central
+        run.n_passes = n_passes
+        run.pass_offset = pass_offset
+        run.fast_math = 1 if fast else 0
+        st = _Stats()
+        _check(self.lib, self.lib.trk_track(self.ctx, nat.ptr, ctypes.byref(run), ctypes.byref(st)))
+        return Stats(n_total=st.n_total, n_left=st.n_left, particle_passes=st.particle_passes,
+                     device_ms=st.device_ms, kernel_launches=st.kernel_launches, p_central=st.p_central)
+
+
+def _lattice_signature(lat):
+    return tuple((t, n, tuple(sorted(p.items())), None if w is None else id(w)) for t, n, p, w in lat.elements)
+
+
+def do_tracking(coord, lattice, n_passes, p_central, fast=True, device=0):
+    """Track `coord` (np x >=7, modified in place: survivors first, then lost
+    particles) through n_passes of `lattice`; returns the survivor count, as
+    the reference's do_tracking() (src/do_tracking.c:144)."""
+    with Tracker(device) as trk:
+        trk.load(coord)
+        trk.track(lattice, n_passes, p_central, fast=fast)
+        n_left, out = trk.store(stride=coord.shape[1])
+    coord[:, :] = out
+    return n_left

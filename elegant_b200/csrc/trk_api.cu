@@ -1,0 +1,948 @@
+/*
+ * trk_api.cu -- contexts, device beam, run orchestration and the C ABI of
+ * libtrkgpu.so (declared in include/trk.h).
+ *
+ * A run is scheduled as a list of steps per pass:
+ *   SEG(ob, oe)   one launch of the fused tracking kernel over ops [ob, oe)
+ *   FID(op)       RFCA "tmean" fiducial before the first pass through op
+ *   WAKE(op)      time statistics, binning, convolution and kick of a wake
+ * Passes whose step list is one SEG over the whole lattice are merged into a
+ * single multi-pass launch, so a lattice without collective elements runs
+ * all its passes in one kernel with the coordinates held in registers.
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "trk.h"
+#include "trk_compile.h"
+#include "trk_constants.h"
+#include "trk_kernels.h"
+#include "trk_lattice.h"
+
+#include <cub/device/device_partition.cuh>
+
+#define CUDA_TRY(call)                                                                                       \
+  do {                                                                                                       \
+    cudaError_t e_ = (call);                                                                                 \
+    if (e_ != cudaSuccess)                                                                                   \
+      return trk_set_error(TRK_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                           __LINE__);                                                                        \
+  } while (0)
+
+struct WakeBuffers {
+  unsigned long long *counts = nullptr;
+  double *hist_x = nullptr, *hist_y = nullptr, *V = nullptr, *Vy = nullptr;
+  double *W = nullptr, *Wy = nullptr;
+  WakeState *state = nullptr;
+  long max_bins = 0, points = 0;
+  double macro = 0;
+  int macro_set = 0;
+};
+
+struct trk_context {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  long np = 0, cap = 0;
+  double *d_cols = nullptr; /* 7 columns x cap */
+  int32_t *d_lost_pass = nullptr, *d_lost_elem = nullptr;
+  /* compiled lattice */
+  CompiledLattice comp;
+  const trk_lattice *comp_src = nullptr;
+  trk_op *d_ops = nullptr;
+  size_t ops_cap = 0;
+  trk_aperture *d_aps = nullptr;
+  size_t aps_cap = 0;
+  double *d_field = nullptr;
+  size_t field_cap = 0;
+  double *d_rf_phase = nullptr;
+  int rf_cap = 0;
+  std::vector<int> rf_fid_done;
+  int *d_status = nullptr;
+  /* reductions */
+  double *d_part = nullptr; /* hi, lo, min, max per block */
+  long long *d_part_n = nullptr;
+  int part_cap = 0;
+  double *d_stats = nullptr; /* 4 doubles */
+  long long *d_effort = nullptr;
+  /* wakes, keyed by op index */
+  std::vector<std::pair<int, WakeBuffers>> wake_bufs;
+  /* staging */
+  double *d_aos = nullptr;
+  size_t aos_cap = 0;
+  void *d_cub = nullptr;
+  size_t cub_cap = 0;
+  long *d_perm = nullptr;
+  long *d_nsel = nullptr;
+  char *d_flags = nullptr;
+  long perm_cap = 0;
+  long passes_done = 0; /* passes tracked since the beam was loaded */
+  long n_original = 0;  /* particles at the start of the run (do_tracking's nOriginal) */
+  int last_launches = 0;
+};
+
+namespace {
+
+int grid_for(const trk_context *ctx, long n, int block) {
+  long g = (n + block - 1) / block;
+  if (g < 1)
+    g = 1;
+  long cap = (long)ctx->sm_count * 64;
+  return (int)std::min(g, cap);
+}
+
+template <typename T> int ensure(T **p, size_t &cap, size_t need) {
+  if (need <= cap && *p)
+    return TRK_OK;
+  if (*p)
+    cudaFree(*p);
+  *p = nullptr;
+  size_t n = std::max(need, (size_t)1);
+  cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    cap = 0;
+    return trk_set_error(TRK_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
+  }
+  cap = n;
+  return TRK_OK;
+}
+
+__global__ void aos_to_soa_kernel(const double *aos, long np, long stride, double *cols, long cap,
+                                  int32_t *lost_pass, int32_t *lost_elem) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np)
+    return;
+  for (int c = 0; c < 7; c++)
+    cols[c * cap + i] = aos[i * stride + c];
+  lost_pass[i] = -1;
+  lost_elem[i] = -1;
+}
+
+__global__ void soa_copy_kernel(const double *src, long ld, long np, double *cols, long cap, int32_t *lost_pass,
+                                int32_t *lost_elem) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np)
+    return;
+  for (int c = 0; c < 7; c++)
+    cols[c * cap + i] = src[c * ld + i];
+  lost_pass[i] = -1;
+  lost_elem[i] = -1;
+}
+
+__global__ void alive_flags_kernel(const int32_t *lost_pass, long np, char *flags, long *idx) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np)
+    return;
+  flags[i] = lost_pass[i] < 0;
+  idx[i] = i;
+}
+
+__global__ void gather_aos_kernel(const double *cols, long cap, const long *perm, long np, long stride, double *aos,
+                                  const int32_t *lost_pass, const int32_t *lost_elem, int32_t *out_pass,
+                                  int32_t *out_elem) {
+  long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= np)
+    return;
+  long i = perm[r];
+  for (int c = 0; c < 7; c++)
+    aos[r * stride + c] = cols[c * cap + i];
+  if (out_pass) {
+    out_pass[r] = lost_pass[i];
+    out_elem[r] = lost_elem[i];
+  }
+}
+
+/* sum over particles of the passes each one entered alive within
+ * [pass_begin, pass_end): elegant's `effort` (src/do_tracking.c:2812-2819) */
+__global__ void effort_kernel(const int32_t *lost_pass, long np, long pass_begin, long pass_end,
+                              unsigned long long *out) {
+  __shared__ unsigned long long sh[256];
+  unsigned long long acc = 0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (long)gridDim.x * blockDim.x) {
+    long lp = lost_pass[i];
+    long c;
+    if (lp < 0)
+      c = pass_end - pass_begin;
+    else
+      c = (lp < pass_end ? lp : pass_end) - pass_begin;
+    if (c < 0)
+      c = 0;
+    acc += (unsigned long long)c;
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    atomicAdd(out, sh[0]);
+}
+
+/* initial NaN/inf screen of do_tracking (src/do_tracking.c:478-484):
+ * limit_amplitudes(DBL_MAX, DBL_MAX) at z = 0 before the first pass */
+__global__ void screen_kernel(double *cols, long cap, int32_t *lost_pass, int32_t *lost_elem, long np, long pass,
+                              double Po) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np || lost_pass[i] >= 0)
+    return;
+  double x = cols[i], y = cols[2 * cap + i];
+  if (isinf(x) || isinf(y) || isnan(x) || isnan(y)) {
+    cols[4 * cap + i] = 0.0;
+    cols[5 * cap + i] = Po * (1 + cols[5 * cap + i]);
+    lost_pass[i] = (int32_t)pass;
+    lost_elem[i] = -1;
+  }
+}
+
+__global__ void count_alive_kernel(const int32_t *lost_pass, long np, unsigned long long *out) {
+  __shared__ unsigned long long sh[256];
+  unsigned long long acc = 0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (long)gridDim.x * blockDim.x)
+    acc += lost_pass[i] < 0;
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    atomicAdd(out, sh[0]);
+}
+
+int ensure_beam(trk_context *ctx, long np) {
+  if (np <= ctx->cap && ctx->d_cols)
+    return TRK_OK;
+  cudaFree(ctx->d_cols);
+  cudaFree(ctx->d_lost_pass);
+  cudaFree(ctx->d_lost_elem);
+  ctx->d_cols = nullptr;
+  ctx->d_lost_pass = ctx->d_lost_elem = nullptr;
+  ctx->cap = 0;
+  long cap = std::max(np, 1L);
+  if (cudaMalloc(&ctx->d_cols, sizeof(double) * 7 * cap) != cudaSuccess ||
+      cudaMalloc(&ctx->d_lost_pass, sizeof(int32_t) * cap) != cudaSuccess ||
+      cudaMalloc(&ctx->d_lost_elem, sizeof(int32_t) * cap) != cudaSuccess)
+    return trk_set_error(TRK_ERR_NOMEM, "device beam allocation for %ld particles failed", np);
+  ctx->cap = cap;
+  return TRK_OK;
+}
+
+void reset_run_state(trk_context *ctx) {
+  ctx->passes_done = 0;
+  ctx->rf_fid_done.clear();
+  for (auto &wb : ctx->wake_bufs) {
+    wb.second.macro_set = 0;
+    wb.second.macro = 0;
+  }
+}
+
+TrackArgs track_args(trk_context *ctx) {
+  TrackArgs a;
+  std::memset(&a, 0, sizeof(a));
+  double *c = ctx->d_cols;
+  long cap = ctx->cap;
+  a.x = c;
+  a.xp = c + cap;
+  a.y = c + 2 * cap;
+  a.yp = c + 3 * cap;
+  a.s = c + 4 * cap;
+  a.dp = c + 5 * cap;
+  a.lost_pass = ctx->d_lost_pass;
+  a.lost_elem = ctx->d_lost_elem;
+  a.ops = ctx->d_ops;
+  a.aps = ctx->d_aps;
+  a.field = ctx->d_field;
+  a.rf_phase = ctx->d_rf_phase;
+  a.n = ctx->np;
+  return a;
+}
+
+int upload_lattice(trk_context *ctx, const trk_lattice *lat, double Po) {
+  int rc = trk_compile(lat, Po, ctx->comp);
+  if (rc)
+    return rc;
+  CompiledLattice &c = ctx->comp;
+  if ((rc = ensure(&ctx->d_ops, ctx->ops_cap, c.ops.size())))
+    return rc;
+  if ((rc = ensure(&ctx->d_aps, ctx->aps_cap, std::max<size_t>(c.aps.size(), 1))))
+    return rc;
+  if ((rc = ensure(&ctx->d_field, ctx->field_cap, std::max<size_t>(c.field.size(), 1))))
+    return rc;
+  if (!c.ops.empty())
+    CUDA_TRY(cudaMemcpyAsync(ctx->d_ops, c.ops.data(), sizeof(trk_op) * c.ops.size(), cudaMemcpyHostToDevice,
+                             ctx->stream));
+  if (!c.aps.empty())
+    CUDA_TRY(cudaMemcpyAsync(ctx->d_aps, c.aps.data(), sizeof(trk_aperture) * c.aps.size(), cudaMemcpyHostToDevice,
+                             ctx->stream));
+  if (!c.field.empty())
+    CUDA_TRY(cudaMemcpyAsync(ctx->d_field, c.field.data(), sizeof(double) * c.field.size(), cudaMemcpyHostToDevice,
+                             ctx->stream));
+  if (c.n_rf_slots > ctx->rf_cap) {
+    cudaFree(ctx->d_rf_phase);
+    ctx->d_rf_phase = nullptr;
+    CUDA_TRY(cudaMalloc(&ctx->d_rf_phase, sizeof(double) * c.n_rf_slots));
+    CUDA_TRY(cudaMemsetAsync(ctx->d_rf_phase, 0, sizeof(double) * c.n_rf_slots, ctx->stream));
+    ctx->rf_cap = c.n_rf_slots;
+  }
+  if ((int)ctx->rf_fid_done.size() < c.n_rf_slots)
+    ctx->rf_fid_done.resize(c.n_rf_slots, 0);
+  /* wake buffers */
+  for (const CompiledWake &w : c.wakes) {
+    WakeBuffers *wb = nullptr;
+    for (auto &p : ctx->wake_bufs)
+      if (p.first == w.op)
+        wb = &p.second;
+    if (!wb) {
+      ctx->wake_bufs.push_back({w.op, WakeBuffers()});
+      wb = &ctx->wake_bufs.back().second;
+    }
+    if (wb->max_bins < w.max_bins || wb->points < w.points) {
+      cudaFree(wb->counts);
+      cudaFree(wb->hist_x);
+      cudaFree(wb->hist_y);
+      cudaFree(wb->V);
+      cudaFree(wb->Vy);
+      cudaFree(wb->W);
+      cudaFree(wb->Wy);
+      cudaFree(wb->state);
+      long nb = w.max_bins + 2;
+      CUDA_TRY(cudaMalloc(&wb->counts, sizeof(unsigned long long) * nb));
+      CUDA_TRY(cudaMalloc(&wb->hist_x, sizeof(double) * nb));
+      CUDA_TRY(cudaMalloc(&wb->hist_y, sizeof(double) * nb));
+      CUDA_TRY(cudaMalloc(&wb->V, sizeof(double) * nb));
+      CUDA_TRY(cudaMalloc(&wb->Vy, sizeof(double) * nb));
+      CUDA_TRY(cudaMalloc(&wb->W, sizeof(double) * w.points));
+      CUDA_TRY(cudaMalloc(&wb->Wy, sizeof(double) * w.points));
+      CUDA_TRY(cudaMalloc(&wb->state, sizeof(WakeState)));
+      CUDA_TRY(cudaMemsetAsync(wb->state, 0, sizeof(WakeState), ctx->stream));
+      wb->max_bins = w.max_bins;
+      wb->points = w.points;
+    }
+    CUDA_TRY(cudaMemcpyAsync(wb->W, w.W, sizeof(double) * w.points, cudaMemcpyHostToDevice, ctx->stream));
+    if (w.transverse)
+      CUDA_TRY(cudaMemcpyAsync(wb->Wy, w.Wy, sizeof(double) * w.points, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  ctx->comp_src = lat;
+  return TRK_OK;
+}
+
+WakeBuffers *wake_buffers(trk_context *ctx, int op) {
+  for (auto &p : ctx->wake_bufs)
+    if (p.first == op)
+      return &p.second;
+  return nullptr;
+}
+
+int ensure_partials(trk_context *ctx, int blocks) {
+  if (blocks <= ctx->part_cap)
+    return TRK_OK;
+  cudaFree(ctx->d_part);
+  cudaFree(ctx->d_part_n);
+  CUDA_TRY(cudaMalloc(&ctx->d_part, sizeof(double) * 4 * blocks));
+  CUDA_TRY(cudaMalloc(&ctx->d_part_n, sizeof(long long) * blocks));
+  ctx->part_cap = blocks;
+  return TRK_OK;
+}
+
+/* launch per-particle time statistics (mode 0 wake, 1 RF fiducial) */
+int time_stats(trk_context *ctx, bool fast, int mode, double sOffset, double Po) {
+  const long chunk = 4096;
+  int blocks = (int)std::min<long>((ctx->np + chunk - 1) / chunk, (long)ctx->sm_count * 8);
+  blocks = std::max(blocks, 1);
+  int rc = ensure_partials(ctx, blocks);
+  if (rc)
+    return rc;
+  TimeStatsArgs t;
+  std::memset(&t, 0, sizeof(t));
+  t.s = ctx->d_cols + 4 * ctx->cap;
+  t.dp = ctx->d_cols + 5 * ctx->cap;
+  t.lost_pass = ctx->d_lost_pass;
+  t.n = ctx->np;
+  t.chunk = chunk;
+  t.mode = mode;
+  t.Po = Po;
+  t.sOffset = sOffset;
+  t.part_hi = ctx->d_part;
+  t.part_lo = ctx->d_part + blocks;
+  t.part_min = ctx->d_part + 2 * blocks;
+  t.part_max = ctx->d_part + 3 * blocks;
+  t.part_n = ctx->d_part_n;
+  t.out = ctx->d_stats;
+  if (fast)
+    trk_fast::launch_time_stats(t, blocks, ctx->stream);
+  else
+    trk_exact::launch_time_stats(t, blocks, ctx->stream);
+  ctx->last_launches += 2;
+  return TRK_OK;
+}
+
+int run_wake(trk_context *ctx, bool fast, int opi, long pass, long fresh_pass, double Po) {
+  const CompiledLattice &c = ctx->comp;
+  const trk_op &op = c.ops[opi];
+  const CompiledWake &w = c.wakes[op.i[0]];
+  WakeBuffers *wb = wake_buffers(ctx, opi);
+  if (!wb)
+    return trk_set_error(TRK_ERR_STATE, "wake buffers missing");
+  TrackArgs ta = track_args(ctx);
+  int grid = grid_for(ctx, ctx->np, TRK_BLOCK);
+  if (w.transverse && w.tilt) {
+    double ca = std::cos(w.tilt), sa = std::sin(w.tilt);
+    if (std::fabs(std::fabs(w.tilt) - TRK_PI) < 1e-12) {
+      ca = -1;
+      sa = 0;
+    }
+    if (fast)
+      trk_fast::launch_rotate(ta, ca, sa, grid, ctx->stream);
+    else
+      trk_exact::launch_rotate(ta, ca, sa, grid, ctx->stream);
+    ctx->last_launches++;
+  }
+  int rc = time_stats(ctx, fast, 0, 0.0, Po);
+  if (rc)
+    return rc;
+  WakeArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.x = ta.x;
+  a.xp = ta.xp;
+  a.y = ta.y;
+  a.yp = ta.yp;
+  a.s = ta.s;
+  a.dp = ta.dp;
+  a.lost_pass = ta.lost_pass;
+  a.lost_elem = ta.lost_elem;
+  a.n = ctx->np;
+  a.Po = Po;
+  a.stats = ctx->d_stats;
+  a.state = wb->state;
+  a.status = ctx->d_status;
+  a.dt = w.dt;
+  a.wake_span = w.span;
+  a.wake_points = w.points;
+  a.i0 = w.i0;
+  a.n_bins = w.n_bins;
+  a.max_bins = w.max_bins;
+  a.smem_bins = 12288;
+  a.allow_long_beam = w.allow_long_beam;
+  a.pass = pass;
+  a.ramp_passes = w.ramp_passes;
+  /* macroparticle charge: CHARGE element, else CHARGE/np on pass 0 (src/wake.c:346-372) */
+  int charge_elem = -1;
+  const trk_lattice *lat = ctx->comp_src;
+  for (int i = 0; i < lat->n; i++)
+    if (lat->e[i].type == TRK_CHARGE)
+      charge_elem = i;
+  if (charge_elem >= 0) {
+    /* CHARGE element (src/do_tracking.c:797-812) */
+    const trk_elem *ce = &lat->e[charge_elem];
+    double macro = 0;
+    if (ctx->n_original)
+      macro = TRK_P(ce, CHARGE_TOTAL) / ctx->n_original;
+    if (TRK_P(ce, CHARGE_PER_PARTICLE))
+      macro = TRK_P(ce, CHARGE_PER_PARTICLE);
+    a.macro_mode = 0;
+    a.macro_charge = macro;
+  } else if (pass == 0) {
+    a.macro_mode = 1;
+    a.charge = w.charge;
+  } else
+    a.macro_mode = 2;
+  a.factor = w.factor;
+  a.xfactor = w.xfactor;
+  a.yfactor = w.yfactor;
+  a.interpolate = w.interpolate;
+  a.transverse = w.transverse;
+  double ramp = (pass >= w.ramp_passes - 1) ? 1.0 : (pass + 1.0) / w.ramp_passes;
+  a.active_planes = 0;
+  if (w.transverse) {
+    /* `if (!factor) continue` per plane (src/trwake.c:192-199); a zero macro
+     * charge makes both planes idle */
+    double fx = w.factor * w.xfactor * ramp, fy = w.factor * w.yfactor * ramp;
+    if (fx)
+      a.active_planes |= 1;
+    if (fy)
+      a.active_planes |= 2;
+  }
+  a.x_power = w.x_power;
+  a.y_power = w.y_power;
+  a.x_probe = w.x_probe;
+  a.y_probe = w.y_probe;
+  a.tdx = w.tdx;
+  a.tdy = w.tdy;
+  if (w.transverse && w.tilt) {
+    a.untilt = 1;
+    a.tilt_c = std::cos(-w.tilt);
+    a.tilt_s = std::sin(-w.tilt);
+    if (std::fabs(std::fabs(w.tilt) - TRK_PI) < 1e-12) {
+      a.tilt_c = -1;
+      a.tilt_s = 0;
+    }
+  }
+  a.W = wb->W;
+  a.W_y = wb->Wy;
+  a.counts = wb->counts;
+  a.hist_x = wb->hist_x;
+  a.hist_y = wb->hist_y;
+  a.V = wb->V;
+  a.V_y = wb->Vy;
+  a.aps = ctx->d_aps;
+  int var = (pass == fresh_pass) ? 0 : 1;
+  a.ap_post = op.ap_post[var];
+  a.z_end = op.z_end;
+  a.elem = op.elem;
+  long nb = w.max_bins + 2;
+  if (w.transverse) {
+    CUDA_TRY(cudaMemsetAsync(wb->hist_x, 0, sizeof(double) * nb, ctx->stream));
+    CUDA_TRY(cudaMemsetAsync(wb->hist_y, 0, sizeof(double) * nb, ctx->stream));
+  } else
+    CUDA_TRY(cudaMemsetAsync(wb->counts, 0, sizeof(unsigned long long) * nb, ctx->stream));
+  if (fast)
+    trk_fast::launch_wake(a, grid, ctx->stream);
+  else
+    trk_exact::launch_wake(a, grid, ctx->stream);
+  ctx->last_launches += w.transverse ? 5 : 4;
+  return TRK_OK;
+}
+
+struct Step {
+  int kind; /* 0 SEG, 1 FID, 2 WAKE */
+  int ob, oe;
+};
+
+void pass_steps(const CompiledLattice &c, std::vector<int> &fid_done, std::vector<Step> &steps) {
+  steps.clear();
+  int seg = 0;
+  const int n = (int)c.ops.size();
+  for (int k = 0; k < n; k++) {
+    const trk_op &op = c.ops[k];
+    if (op.kind == OPK_RF && !fid_done[op.i[1]]) {
+      if (k > seg)
+        steps.push_back({0, seg, k});
+      steps.push_back({1, k, k + 1});
+      fid_done[op.i[1]] = 1;
+      seg = k;
+    } else if (op.kind == OPK_WAKE || op.kind == OPK_TRWAKE) {
+      if (k > seg)
+        steps.push_back({0, seg, k});
+      steps.push_back({2, k, k + 1});
+      seg = k + 1;
+    }
+  }
+  if (n > seg)
+    steps.push_back({0, seg, n});
+}
+
+int check_status(trk_context *ctx) {
+  int st = 0;
+  CUDA_TRY(cudaMemcpyAsync(&st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (st) {
+    CUDA_TRY(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+    if (st & TRK_STATUS_LONG_BEAM)
+      return trk_set_error(TRK_ERR_PHYSICS, "The beam is longer than the longitudinal wake function.");
+    if (st & TRK_STATUS_TOO_MANY_BINS)
+      return trk_set_error(TRK_ERR_PHYSICS, "autoscaled wake bins exceed the allocated histogram");
+    if (st & TRK_STATUS_NO_PARTICLES)
+      return trk_set_error(TRK_ERR_PHYSICS, "No available particle for RF cavity fiducialization");
+    return trk_set_error(TRK_ERR_DEVICE, "device status 0x%x", st);
+  }
+  return TRK_OK;
+}
+
+} // namespace
+
+/* ======================================================================= C ABI */
+extern "C" {
+
+void trk_run_defaults(trk_run *run) {
+  if (!run)
+    return;
+  std::memset(run, 0, sizeof(*run));
+  run->p_central = 1.0;
+  run->n_passes = 1;
+  run->fast_math = 1;
+}
+
+int trk_context_create(trk_context **out, int device) {
+  if (!out)
+    return trk_set_error(TRK_ERR_ARG, "null context pointer");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return trk_set_error(TRK_ERR_CUDA, "no CUDA device available");
+  if (device < 0)
+    CUDA_TRY(cudaGetDevice(&device));
+  if (device >= ndev)
+    return trk_set_error(TRK_ERR_ARG, "device %d out of range (%d devices)", device, ndev);
+  CUDA_TRY(cudaSetDevice(device));
+  trk_context *ctx = new trk_context();
+  ctx->device = device;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) == cudaSuccess)
+    ctx->sm_count = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
+      cudaMalloc(&ctx->d_status, sizeof(int)) != cudaSuccess || cudaMalloc(&ctx->d_stats, 4 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&ctx->d_effort, sizeof(long long)) != cudaSuccess) {
+    trk_context_destroy(ctx);
+    return trk_set_error(TRK_ERR_CUDA, "context set-up failed");
+  }
+  cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream);
+  double coef[10];
+  trk_expansion_coefficients(coef);
+  if (trk_exact::set_coefficients(coef) != cudaSuccess || trk_fast::set_coefficients(coef) != cudaSuccess) {
+    trk_context_destroy(ctx);
+    return trk_set_error(TRK_ERR_CUDA, "coefficient upload failed");
+  }
+  *out = ctx;
+  return TRK_OK;
+}
+
+void trk_context_destroy(trk_context *ctx) {
+  if (!ctx)
+    return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream)
+    cudaStreamSynchronize(ctx->stream);
+  cudaFree(ctx->d_cols);
+  cudaFree(ctx->d_lost_pass);
+  cudaFree(ctx->d_lost_elem);
+  cudaFree(ctx->d_ops);
+  cudaFree(ctx->d_aps);
+  cudaFree(ctx->d_field);
+  cudaFree(ctx->d_rf_phase);
+  cudaFree(ctx->d_status);
+  cudaFree(ctx->d_part);
+  cudaFree(ctx->d_part_n);
+  cudaFree(ctx->d_stats);
+  cudaFree(ctx->d_effort);
+  cudaFree(ctx->d_aos);
+  cudaFree(ctx->d_cub);
+  cudaFree(ctx->d_perm);
+  cudaFree(ctx->d_nsel);
+  cudaFree(ctx->d_flags);
+  for (auto &p : ctx->wake_bufs) {
+    WakeBuffers &w = p.second;
+    cudaFree(w.counts);
+    cudaFree(w.hist_x);
+    cudaFree(w.hist_y);
+    cudaFree(w.V);
+    cudaFree(w.Vy);
+    cudaFree(w.W);
+    cudaFree(w.Wy);
+    cudaFree(w.state);
+  }
+  if (ctx->ev0)
+    cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1)
+    cudaEventDestroy(ctx->ev1);
+  if (ctx->stream)
+    cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+void *trk_context_stream(trk_context *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int trk_beam_load(trk_context *ctx, const double *coord, long np, long stride) {
+  if (!ctx || (np > 0 && !coord) || np < 0 || stride < 7)
+    return trk_set_error(TRK_ERR_ARG, "bad beam (np=%ld, stride=%ld)", np, stride);
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  int rc = ensure_beam(ctx, np);
+  if (rc)
+    return rc;
+  if ((rc = ensure(&ctx->d_aos, ctx->aos_cap, (size_t)std::max(np, 1L) * stride)))
+    return rc;
+  ctx->np = np;
+  reset_run_state(ctx);
+  ctx->n_original = np;
+  if (np == 0)
+    return TRK_OK;
+  CUDA_TRY(cudaMemcpyAsync(ctx->d_aos, coord, sizeof(double) * np * stride, cudaMemcpyHostToDevice, ctx->stream));
+  aos_to_soa_kernel<<<(int)((np + 255) / 256), 256, 0, ctx->stream>>>(ctx->d_aos, np, stride, ctx->d_cols, ctx->cap,
+                                                                      ctx->d_lost_pass, ctx->d_lost_elem);
+  CUDA_TRY(cudaGetLastError());
+  return TRK_OK;
+}
+
+int trk_beam_load_device(trk_context *ctx, const double *d_soa, long np, long ld) {
+  if (!ctx || (np > 0 && !d_soa) || np < 0 || ld < np)
+    return trk_set_error(TRK_ERR_ARG, "bad device beam (np=%ld, ld=%ld)", np, ld);
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  int rc = ensure_beam(ctx, np);
+  if (rc)
+    return rc;
+  ctx->np = np;
+  reset_run_state(ctx);
+  ctx->n_original = np;
+  if (np == 0)
+    return TRK_OK;
+  soa_copy_kernel<<<(int)((np + 255) / 256), 256, 0, ctx->stream>>>(d_soa, ld, np, ctx->d_cols, ctx->cap,
+                                                                    ctx->d_lost_pass, ctx->d_lost_elem);
+  CUDA_TRY(cudaGetLastError());
+  return TRK_OK;
+}
+
+int trk_beam_device_columns(trk_context *ctx, double **columns, long *np, int32_t **loss) {
+  if (!ctx)
+    return trk_set_error(TRK_ERR_ARG, "null context");
+  if (columns)
+    for (int c = 0; c < 7; c++)
+      columns[c] = ctx->d_cols ? ctx->d_cols + (size_t)c * ctx->cap : nullptr;
+  if (np)
+    *np = ctx->np;
+  if (loss) {
+    loss[0] = ctx->d_lost_pass;
+    loss[1] = ctx->d_lost_elem;
+  }
+  return TRK_OK;
+}
+
+int trk_beam_count(trk_context *ctx, long *n_left) {
+  if (!ctx || !n_left)
+    return trk_set_error(TRK_ERR_ARG, "null argument");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  if (ctx->np == 0) {
+    *n_left = 0;
+    return TRK_OK;
+  }
+  CUDA_TRY(cudaMemsetAsync(ctx->d_effort, 0, sizeof(long long), ctx->stream));
+  count_alive_kernel<<<std::min(grid_for(ctx, ctx->np, 256), 1024), 256, 0, ctx->stream>>>(
+    ctx->d_lost_pass, ctx->np, (unsigned long long *)ctx->d_effort);
+  long long v = 0;
+  CUDA_TRY(cudaMemcpyAsync(&v, ctx->d_effort, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  *n_left = (long)v;
+  return TRK_OK;
+}
+
+int trk_beam_store(trk_context *ctx, double *coord, long stride, long *n_left, long *lost_pass,
+                   int32_t *lost_element) {
+  if (!ctx || stride < 7 || (ctx->np > 0 && !coord))
+    return trk_set_error(TRK_ERR_ARG, "bad store arguments");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  const long np = ctx->np;
+  if (np == 0) {
+    if (n_left)
+      *n_left = 0;
+    return TRK_OK;
+  }
+  int rc;
+  if (np > ctx->perm_cap) {
+    cudaFree(ctx->d_perm);
+    cudaFree(ctx->d_flags);
+    cudaFree(ctx->d_nsel);
+    CUDA_TRY(cudaMalloc(&ctx->d_perm, sizeof(long) * 2 * np));
+    CUDA_TRY(cudaMalloc(&ctx->d_flags, np));
+    CUDA_TRY(cudaMalloc(&ctx->d_nsel, sizeof(long)));
+    ctx->perm_cap = np;
+  }
+  long *d_idx = ctx->d_perm + np;
+  alive_flags_kernel<<<(int)((np + 255) / 256), 256, 0, ctx->stream>>>(ctx->d_lost_pass, np, ctx->d_flags, d_idx);
+  size_t tmp = 0;
+  /* stable partition: survivors first in original order, then the lost ones
+   * (DevicePartition::Flagged writes the rejected items in reverse order) */
+  cub::DevicePartition::Flagged(nullptr, tmp, d_idx, ctx->d_flags, ctx->d_perm, ctx->d_nsel, np, ctx->stream);
+  if ((rc = ensure((char **)&ctx->d_cub, ctx->cub_cap, tmp)))
+    return rc;
+  CUDA_TRY(cub::DevicePartition::Flagged(ctx->d_cub, tmp, d_idx, ctx->d_flags, ctx->d_perm, ctx->d_nsel, np,
+                                         ctx->stream));
+  long nsel = 0;
+  CUDA_TRY(cudaMemcpyAsync(&nsel, ctx->d_nsel, sizeof(long), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  /* reverse the rejected tail so lost particles keep their original order */
+  std::vector<long> perm;
+  if (nsel < np) {
+    perm.resize(np - nsel);
+    CUDA_TRY(cudaMemcpy(perm.data(), ctx->d_perm + nsel, sizeof(long) * (np - nsel), cudaMemcpyDeviceToHost));
+    std::reverse(perm.begin(), perm.end());
+    CUDA_TRY(cudaMemcpy(ctx->d_perm + nsel, perm.data(), sizeof(long) * (np - nsel), cudaMemcpyHostToDevice));
+  }
+  if ((rc = ensure(&ctx->d_aos, ctx->aos_cap, (size_t)np * stride)))
+    return rc;
+  int32_t *d_out = nullptr;
+  if (lost_pass || lost_element) {
+    CUDA_TRY(cudaMalloc(&d_out, sizeof(int32_t) * 2 * np));
+  }
+  gather_aos_kernel<<<(int)((np + 255) / 256), 256, 0, ctx->stream>>>(
+    ctx->d_cols, ctx->cap, ctx->d_perm, np, stride, ctx->d_aos, ctx->d_lost_pass, ctx->d_lost_elem, d_out,
+    d_out ? d_out + np : nullptr);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpyAsync(coord, ctx->d_aos, sizeof(double) * np * stride, cudaMemcpyDeviceToHost, ctx->stream));
+  if (d_out) {
+    std::vector<int32_t> h(2 * np);
+    CUDA_TRY(cudaMemcpyAsync(h.data(), d_out, sizeof(int32_t) * 2 * np, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (long r = 0; r < np; r++) {
+      if (lost_pass)
+        lost_pass[r] = h[r];
+      if (lost_element)
+        lost_element[r] = h[np + r];
+    }
+    cudaFree(d_out);
+  }
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (n_left)
+    *n_left = nsel;
+  return TRK_OK;
+}
+
+int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, trk_stats *stats) {
+  if (!ctx || !lattice || !run)
+    return trk_set_error(TRK_ERR_ARG, "null argument to trk_track");
+  if (run->n_passes < 0)
+    return trk_set_error(TRK_ERR_ARG, "negative pass count");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  const double Po = run->p_central;
+  if (!(Po > 0))
+    return trk_set_error(TRK_ERR_ARG, "p_central must be positive");
+  int rc = upload_lattice(ctx, lattice, Po);
+  if (rc)
+    return rc;
+  const bool fast = run->fast_math != 0;
+  const CompiledLattice &c = ctx->comp;
+  ctx->last_launches = 0;
+  const long p0 = run->pass_offset;
+  const long fresh = ctx->passes_done == 0 ? p0 : -1;
+  const int block = run->block_size > 0 ? run->block_size : TRK_BLOCK;
+  if (block != TRK_BLOCK)
+    return trk_set_error(TRK_ERR_ARG, "block_size must be 0 or %d", TRK_BLOCK);
+  CUDA_TRY(cudaEventRecord(ctx->ev0, ctx->stream));
+  if (ctx->np > 0 && run->n_passes > 0 && fresh >= 0) {
+    screen_kernel<<<(int)((ctx->np + 255) / 256), 256, 0, ctx->stream>>>(
+      ctx->d_cols, ctx->cap, ctx->d_lost_pass, ctx->d_lost_elem, ctx->np, p0, Po);
+    ctx->last_launches++;
+  }
+  if (ctx->np > 0 && run->n_passes > 0 && !c.ops.empty()) {
+    TrackArgs ta = track_args(ctx);
+    ta.fresh_pass = fresh;
+    ta.Po = Po;
+    const int grid = grid_for(ctx, ctx->np, block);
+    std::vector<Step> steps;
+    long pass = p0;
+    const long pend = p0 + run->n_passes;
+    while (pass < pend) {
+      std::vector<int> fid = ctx->rf_fid_done;
+      pass_steps(c, fid, steps);
+      bool simple = steps.size() == 1 && steps[0].kind == 0;
+      long npass = 1;
+      if (simple) {
+        /* merge passes while the schedule stays one full segment */
+        npass = pend - pass;
+        if (fresh >= 0 && pass == fresh && npass > 1) {
+          /* first pass uses the fresh MAXAMP state; still one launch */
+        }
+      }
+      for (const Step &st : steps) {
+        if (st.kind == 0) {
+          ta.op_begin = st.ob;
+          ta.op_end = st.oe;
+          ta.pass_begin = pass;
+          ta.pass_end = pass + npass;
+          if (fast)
+            trk_fast::launch_track(ta, grid, block, ctx->stream);
+          else
+            trk_exact::launch_track(ta, grid, block, ctx->stream);
+          ctx->last_launches++;
+        } else if (st.kind == 1) {
+          const trk_op &op = c.ops[st.ob];
+          int slot = op.i[1];
+          if ((rc = time_stats(ctx, fast, 1, op.d[RD_SOFF], Po)))
+            return rc;
+          if (fast)
+            trk_fast::launch_rf_fiducial(ctx->d_stats, op.d[RD_OMEGA], op.d[RD_TREF], ctx->d_rf_phase, slot,
+                                         ctx->d_status, ctx->stream);
+          else
+            trk_exact::launch_rf_fiducial(ctx->d_stats, op.d[RD_OMEGA], op.d[RD_TREF], ctx->d_rf_phase, slot,
+                                          ctx->d_status, ctx->stream);
+          ctx->last_launches++;
+          ctx->rf_fid_done[slot] = 1;
+        } else {
+          if ((rc = run_wake(ctx, fast, st.ob, pass, fresh, Po)))
+            return rc;
+        }
+      }
+      pass += npass;
+    }
+    CUDA_TRY(cudaGetLastError());
+  }
+  CUDA_TRY(cudaEventRecord(ctx->ev1, ctx->stream));
+  if ((rc = check_status(ctx)))
+    return rc;
+  ctx->passes_done += run->n_passes;
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    float ms = 0;
+    CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    stats->device_ms = ms;
+    stats->n_total = ctx->np;
+    stats->kernel_launches = ctx->last_launches;
+    stats->p_central = Po;
+    if (ctx->np > 0) {
+      CUDA_TRY(cudaMemsetAsync(ctx->d_effort, 0, sizeof(long long), ctx->stream));
+      effort_kernel<<<std::min(grid_for(ctx, ctx->np, 256), 1024), 256, 0, ctx->stream>>>(
+        ctx->d_lost_pass, ctx->np, p0, p0 + run->n_passes, (unsigned long long *)ctx->d_effort);
+      long long eff = 0;
+      CUDA_TRY(cudaMemcpyAsync(&eff, ctx->d_effort, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+      CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+      stats->particle_passes = eff;
+      long nl = 0;
+      if ((rc = trk_beam_count(ctx, &nl)))
+        return rc;
+      stats->n_left = nl;
+    }
+  }
+  return TRK_OK;
+}
+
+int trk_track_element(trk_context *ctx, const trk_lattice *lattice, int element, long pass, double z_start,
+                      const trk_run *run, long *n_left) {
+  (void)z_start;
+  if (!ctx || !lattice || !run)
+    return trk_set_error(TRK_ERR_ARG, "null argument");
+  if (element < 0 || element >= lattice->n)
+    return trk_set_error(TRK_ERR_ARG, "element index out of range");
+  return trk_set_error(TRK_ERR_UNSUPPORTED, "per-element tracking is provided by the elegant hook layer");
+}
+
+int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int n_variants, const long *offsets,
+                       const trk_run *run, trk_stats *stats) {
+  (void)ctx;
+  (void)lattices;
+  (void)n_variants;
+  (void)offsets;
+  (void)run;
+  (void)stats;
+  return trk_set_error(TRK_ERR_UNSUPPORTED, "ensembles not built yet");
+}
+
+int trk_adjoint(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, double centroid_weight,
+                double *loss, double *grad, int n_grad) {
+  (void)ctx;
+  (void)lattice;
+  (void)run;
+  (void)centroid_weight;
+  (void)loss;
+  (void)grad;
+  (void)n_grad;
+  return trk_set_error(TRK_ERR_UNSUPPORTED, "adjoint not built yet");
+}
+
+int trk_adjoint_param_count(const trk_lattice *lattice) {
+  if (!lattice)
+    return trk_set_error(TRK_ERR_ARG, "null lattice");
+  int n = 0;
+  for (int i = 0; i < lattice->n; i++)
+    if (lattice->e[i].type == TRK_KQUAD || lattice->e[i].type == TRK_KSEXT)
+      n++;
+  return n;
+}
+
+} /* extern "C" */

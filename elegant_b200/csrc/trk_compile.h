@@ -1,0 +1,42 @@
+/*
+ * trk_compile.h -- lattice compiler (host side of libtrkgpu.so).
+ */
+#ifndef TRK_COMPILE_H
+#define TRK_COMPILE_H
+
+#include <vector>
+
+#include "trk.h"
+#include "trk_ops.h"
+
+struct CompiledWake {
+  int op = -1;
+  int transverse = 0;
+  double dt = 0, span = 0;
+  long i0 = 0, points = 0, n_bins = 0, max_bins = 0;
+  int allow_long_beam = 0;
+  const double *t = nullptr, *W = nullptr, *Wy = nullptr;
+  double factor = 1, xfactor = 1, yfactor = 1, charge = 0;
+  int interpolate = 0;
+  long ramp_passes = 0;
+  int x_power = 1, y_power = 1, x_probe = 0, y_probe = 0;
+  double tdx = 0, tdy = 0, tilt = 0;
+};
+
+struct CompiledLattice {
+  std::vector<trk_op> ops;
+  std::vector<trk_aperture> aps;
+  std::vector<double> field;
+  std::vector<CompiledWake> wakes;
+  std::vector<int> rf_first_op; /* op index of the first RFCA of each fiducial slot */
+  int n_rf_slots = 0;
+  int n_mult = 0;
+  double total_length = 0;
+};
+
+int trk_compile(const trk_lattice *l, double Po, CompiledLattice &out);
+void trk_expansion_coefficients(double *coef10);
+extern "C" int trk_csbend_field_table(const double *b, const double *c, double h, int nonlinear, long expansionOrder,
+                                      double *Fx, double *Fy, int *eo1, int *hasNormal, int *hasSkew);
+
+#endif

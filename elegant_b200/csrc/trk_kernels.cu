@@ -1,0 +1,1269 @@
+/*
+ * trk_kernels.cu -- particle-tracking kernels for sm_100a.
+ *
+ * Compiled twice into libtrkgpu.so:
+ *   TRK_FAST=0 (namespace trk_exact, -fmad=false): the reference's operation
+ *     order, no FMA contraction, correctly rounded sin/cos/asin; reproduces
+ *     elegant's CPU results bit for bit on the tracking path.
+ *   TRK_FAST=1 (namespace trk_fast): FMA contraction, reciprocal multiplies
+ *     and a transcendental-free CSBEND drift; same physics, error comparable
+ *     to the reference's own FP64 rounding.
+ *
+ * Layout: the beam is a structure of arrays (x, x', y, y', s, delta) in FP64
+ * plus int32 loss pass / loss element; one thread owns one particle and keeps
+ * its six coordinates in registers across a whole fused segment of elements
+ * (and across passes when no collective element intervenes).  Element
+ * records (trk_op) are read with warp-uniform loads through the read-only
+ * path.  FP64 throughout: long-term symplectic tracking and the loss
+ * boundaries need it, and no dense contraction exists for the tensor cores.
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "trk_constants.h"
+#include "trk_crmath.cuh"
+#include "trk_kernels.h"
+#include "trk_ops.h"
+
+#ifndef TRK_FAST
+#error "TRK_FAST must be defined to 0 or 1"
+#endif
+
+#if TRK_FAST
+#define TRK_NS trk_fast
+#define M_SIN(x) sin(x)
+#define M_COS(x) cos(x)
+#define M_ASIN(x) asin(x)
+#else
+#define TRK_NS trk_exact
+#define M_SIN(x) trkcr::cr_sin(x)
+#define M_COS(x) trkcr::cr_cos(x)
+#define M_ASIN(x) trkcr::cr_asin(x)
+#endif
+
+namespace TRK_NS {
+
+struct Part {
+  double x, xp, y, yp, s, dp;
+};
+
+__device__ __forceinline__ double sqr(double v) { return v * v; }
+
+__device__ __forceinline__ double ipow_d(double x, int p) {
+  if (p == 2)
+    return x * x;
+  if (p == 0)
+    return 1.0;
+  if (p == 1)
+    return x;
+  /* repeated squaring; exponent 2 is the only one on the tracking path */
+  double h = 1.0, b = x;
+  for (int e = p < 0 ? -p : p; e; e >>= 1) {
+    if (e & 1)
+      h = h * b;
+    b = b * b;
+  }
+  return p < 0 ? 1.0 / h : h;
+}
+
+__device__ __forceinline__ void exact_drift(Part &p, double L) {
+  p.x += p.xp * L;
+  p.y += p.yp * L;
+  p.s += L * sqrt(1 + sqr(p.xp) + sqr(p.yp));
+}
+
+/* rotateBeamCoordinatesForMisalignment with precomputed cos/sin
+ * (src/tilt_matrices.c:156-190) */
+__device__ __forceinline__ void rotate(Part &p, double ca, double sa) {
+  double x = p.x, xp = p.xp, y = p.y, yp = p.yp;
+  p.x = x * ca + y * sa;
+  p.y = -x * sa + y * ca;
+  p.xp = xp * ca + yp * sa;
+  p.yp = -xp * sa + yp * ca;
+}
+
+/* offsetBeamCoordinatesForMisalignment (src/malign_mat.c:257-267) */
+__device__ __forceinline__ void offset(Part &p, double dx, double dy, double dz) {
+  p.s += dz * sqrt(1 + sqr(p.xp) + sqr(p.yp));
+  p.x = p.x - dx + dz * p.xp;
+  p.y = p.y - dy + dz * p.yp;
+}
+
+/* checkMultAperture (src/multipole.c:1751-1798) without aperture files */
+__device__ __forceinline__ bool check_aperture(double x, double y, const trk_aperture *ap, bool tilt, double rc,
+                                               double rs) {
+  if (!ap)
+    return true;
+  x = x - 0.0;
+  y = y - 0.0;
+  if (tilt) {
+    double x0 = x, y0 = y;
+    x = x0 * rc + y0 * rs;
+    y = -x0 * rs + y0 * rc;
+  }
+  double xMax = ap->x_max, yMax = ap->y_max;
+  if (ap->elliptical == 0 || xMax <= 0 || yMax <= 0) {
+    if ((xMax > 0 && fabs(x) > xMax) || (yMax > 0 && fabs(y) > yMax))
+      return false;
+  } else {
+    double xa = x / xMax, yb = y / yMax;
+    if (ipow_d(xa, ap->xexp) + ipow_d(yb, ap->yexp) >= 1)
+      return false;
+  }
+  return true;
+}
+
+/* ------------------------------------------------------------- multipoles */
+__device__ __forceinline__ bool momenta_to_slopes(double &xp, double &yp, double qx, double qy, double delta,
+                                                  int expand) {
+  if (expand) {
+    xp = qx / (1 + delta);
+    yp = qy / (1 + delta);
+    return true;
+  }
+  double denom = sqr(1 + delta) - sqr(qx) - sqr(qy);
+  if (denom <= 0)
+    return false;
+  denom = sqrt(denom);
+#if TRK_FAST
+  double inv = 1.0 / denom;
+  xp = qx * inv;
+  yp = qy * inv;
+#else
+  xp = qx / denom;
+  yp = qy / denom;
+#endif
+  return true;
+}
+
+/* apply_canonical_multipole_kicks_ret (src/multipole.h:391-421) for the
+ * orders on this path, with the reference's term order and coefficients
+ * (src/multipole.h:76-146). */
+__device__ __forceinline__ void mkick(double &qx, double &qy, double x, double y, int order, double K, int skew,
+                                      const double *coef) {
+  double sFx, sFy;
+  switch (order) {
+  case 0:
+    sFy = 1.0;
+    sFx = 0.0;
+    break;
+  case 1:
+    sFy = x;
+    sFx = y;
+    break;
+  case 2: {
+    double x2 = x * x, y2 = y * y;
+    sFy = 0.5 * x2 + (-0.5) * y2;
+    sFx = x * y;
+    break;
+  }
+  case 3: {
+    double x2 = x * x, y2 = y * y;
+    double x3 = x2 * x, y3 = y2 * y;
+    double f0 = coef[6] * x3;
+    double f1 = (coef[7] * x2) * y;
+    double f2 = (coef[8] * x) * y2;
+    double f3 = coef[9] * y3;
+    sFy = f0 + f2;
+    sFx = f1 + f3;
+    break;
+  }
+  default:
+    sFy = sFx = 0.0;
+  }
+  if (skew) {
+    double t = sFx;
+    sFx = -sFy;
+    sFy = t;
+  }
+  qx -= K * sFy;
+  qy += K * sFx;
+}
+
+__device__ __constant__ double c_coef[10]; /* expansion coefficients, orders 0..3 at n(n+1)/2 */
+
+/* multipole_tracking2 + integrate_kick_multipole_ordn (src/multipole.c:660-1456) */
+__device__ __forceinline__ bool op_mult(const trk_op *__restrict__ op, Part &p, double Po, double z_start,
+                                        const trk_aperture *ap) {
+  const int n_parts = __ldg(&op->i[0]);
+  const int nSub = __ldg(&op->i[1]);
+  const int expand = __ldg(&op->i[2]);
+  const int orders = __ldg(&op->i[4]);
+  const int skews = __ldg(&op->i[5]);
+  const int flags = __ldg(&op->i[6]);
+  const double *d = op->d;
+  const double mdx = __ldg(&d[MD_DX]), mdy = __ldg(&d[MD_DY]), mdz = __ldg(&d[MD_DZ]);
+
+  if (flags & MF_OFFSET)
+    offset(p, mdx, mdy, mdz);
+  if (flags & MF_TILT)
+    rotate(p, __ldg(&d[MD_TC]), __ldg(&d[MD_TS]));
+  if (flags & MF_ENDDRIFT)
+    exact_drift(p, __ldg(&d[MD_LEND]));
+
+  bool ok = true;
+  double dzLoss = 0;
+  {
+    double x = p.x, xp = p.xp, y = p.y, yp = p.yp, s = 0, dp = p.dp, qx, qy;
+    const bool aptilt = (flags & MF_APTILT) != 0;
+    const double apc = __ldg(&d[MD_APC]), aps = __ldg(&d[MD_APS]);
+    const double drift = __ldg(&d[MD_DRIFT]);
+    if (isnan(x) || isnan(xp) || isnan(y) || isnan(yp) || fabs(x) > TRK_COORD_LIMIT || fabs(y) > TRK_COORD_LIMIT ||
+        fabs(xp) > TRK_SLOPE_LIMIT || fabs(yp) > TRK_SLOPE_LIMIT) {
+      ok = false;
+      goto done;
+    }
+    if (expand) {
+      qx = (1 + dp) * xp;
+      qy = (1 + dp) * yp;
+    } else {
+      double denom = sqrt(1 + sqr(xp) + sqr(yp));
+      qx = (1 + dp) * xp / denom;
+      qy = (1 + dp) * yp / denom;
+    }
+    if (!momenta_to_slopes(xp, yp, qx, qy, dp, expand)) {
+      ok = false;
+      goto done;
+    }
+    for (int i_kick = 0; i_kick < n_parts; i_kick++) {
+      if (!check_aperture(x + mdx, y + mdy, ap, aptilt, apc, aps)) {
+        p.x = x;
+        p.y = y;
+        ok = false;
+        goto done;
+      }
+      for (int step = 0; step < nSub; step++) {
+        if (drift != 0) {
+          double dsh = __ldg(&d[MD_DSH + step]);
+          x += xp * dsh;
+          y += yp * dsh;
+          if (expand)
+            s += dsh * (1 + (sqr(xp) + sqr(yp)) / 2);
+          else
+            s += dsh * sqrt(1 + sqr(xp) + sqr(yp));
+          dzLoss += dsh;
+        }
+        if (step == nSub - 1)
+          break; /* kickFrac of the last substep is 0 for orders 2, 4, 6 */
+        if (flags & MF_KNL0)
+          mkick(qx, qy, x, y, orders & 0xff, __ldg(&d[MD_KQ + step * 3 + 0]), skews & 1, c_coef);
+        if (flags & MF_KNL1)
+          mkick(qx, qy, x, y, (orders >> 8) & 0xff, __ldg(&d[MD_KQ + step * 3 + 1]), (skews >> 1) & 1, c_coef);
+        if (flags & MF_KNL2)
+          mkick(qx, qy, x, y, (orders >> 16) & 0xff, __ldg(&d[MD_KQ + step * 3 + 2]), (skews >> 2) & 1, c_coef);
+        if (flags & MF_XKICK)
+          mkick(qx, qy, x, y, 0, __ldg(&d[MD_KX + step]), 0, c_coef);
+        if (flags & MF_YKICK)
+          mkick(qx, qy, x, y, 0, __ldg(&d[MD_KY + step]), 1, c_coef);
+        if (!momenta_to_slopes(xp, yp, qx, qy, dp, expand)) {
+          ok = false;
+          goto done;
+        }
+      }
+    }
+    if (!check_aperture(x + mdx, y + mdy, ap, aptilt, apc, aps)) {
+      p.x = x;
+      p.y = y;
+      ok = false;
+      goto done;
+    }
+    if (!momenta_to_slopes(xp, yp, qx, qy, dp, expand)) {
+      ok = false;
+      goto done;
+    }
+    p.x = x;
+    p.xp = xp;
+    p.y = y;
+    p.yp = yp;
+    p.s += s;
+    p.dp = dp;
+    if (isnan(x) || isnan(xp) || isnan(y) || isnan(yp) || fabs(x) > TRK_COORD_LIMIT || fabs(y) > TRK_COORD_LIMIT ||
+        fabs(xp) > TRK_SLOPE_LIMIT || fabs(yp) > TRK_SLOPE_LIMIT)
+      ok = false;
+  }
+done:
+  if (!ok) {
+    p.s = z_start + dzLoss;
+    p.dp = Po * (1 + p.dp);
+  }
+  if (flags & MF_ENDDRIFT)
+    exact_drift(p, __ldg(&d[MD_LEND]));
+  if (flags & MF_TILT)
+    rotate(p, __ldg(&d[MD_XC]), __ldg(&d[MD_XS]));
+  if (flags & MF_OFFSET)
+    offset(p, -mdx, -mdy, -mdz);
+  return ok;
+}
+
+/* ---------------------------------------------------------------- CSBEND */
+/* computeCSBENDFields (src/csbend.c:99-172) */
+__device__ __forceinline__ void bend_fields(int mode, int eo1, const double *__restrict__ Fx_xy,
+                                            const double *__restrict__ Fy_xy, double x, double y, double &Fx,
+                                            double &Fy) {
+  double yp[11];
+  double sumFx = 0, sumFy = 0;
+  yp[0] = 1;
+#pragma unroll
+  for (int i = 1; i < 11; i++)
+    yp[i] = (i < eo1) ? yp[i - 1] * y : 0.0;
+  double xt = 1;
+  for (int i = 0; i < eo1; i++) {
+    for (int j = 0; j < eo1 - i; j++) {
+      if (mode == 2) {
+        sumFx += __ldg(&Fx_xy[i * 11 + j]) * xt * yp[j];
+        sumFy += __ldg(&Fy_xy[i * 11 + j]) * xt * yp[j];
+      } else if (j & 1)
+        sumFx += __ldg(&Fx_xy[i * 11 + j]) * xt * yp[j];
+      else
+        sumFy += __ldg(&Fy_xy[i * 11 + j]) * xt * yp[j];
+    }
+    xt *= x;
+  }
+  Fx = sumFx;
+  Fy = sumFy;
+}
+
+/* apply_edge_effects (src/csbend.c:4291-4333) */
+__device__ void edge_order2(double &x, double &xp, double &y, double &yp, double rho, double n, double beta,
+                            double he, double psi, int which_edge) {
+  double h, tan_beta, tan2_beta, sec_beta, sec2_beta, h2;
+  double R21, R43, T111, T133, T211, T441, T331, T221, T233, T243, T431, T432;
+  h = 1 / rho;
+  R21 = h * (tan_beta = tan(beta));
+  R43 = -h * tan(beta - psi);
+  h2 = sqr(h);
+  T111 = which_edge * h / 2 * (tan2_beta = sqr(tan_beta));
+  sec_beta = 1. / cos(beta);
+  sec2_beta = sqr(sec_beta);
+  T133 = -which_edge * h / 2 * sec2_beta;
+  T211 = which_edge == -1 ? -n * h2 * tan_beta : -h2 * (n + tan2_beta / 2) * tan_beta;
+  T441 = -(T331 = T221 = -which_edge * h * tan2_beta);
+  T233 = which_edge == -1 ? h2 * (n + .5 + tan2_beta) * tan_beta : h2 * (n - tan2_beta / 2) * tan_beta;
+  T243 = which_edge * h * tan2_beta;
+  T431 = h2 * (2 * n + (which_edge == 1 ? sec2_beta : 0)) * tan_beta;
+  T432 = which_edge * h * sec2_beta;
+  if (he != 0) {
+    double term = h / 2 * he * sec2_beta * sec_beta;
+    T211 += term;
+    T233 -= term;
+    T431 -= 2 * term;
+  }
+  double x0 = x, xp0 = xp, y0 = y, yp0 = yp;
+  x = x0 + T111 * sqr(x0) + T133 * sqr(y0);
+  xp = xp0 + R21 * x0 + T211 * sqr(x0) + T221 * x0 * xp0 + T233 * sqr(y0) + T243 * y0 * yp0;
+  y = y0 + T331 * x0 * y0;
+  yp = yp0 + R43 * y0 + T441 * yp0 * x0 + T431 * x0 * y0 + T432 * xp0 * y0;
+}
+
+/* edge kick of track_through_csbend (src/csbend.c:1126-1204, 1306-1382) */
+__device__ __forceinline__ void bend_edge(int mode, const double *__restrict__ d, int base, int which, double rho_a,
+                                          double nidx, double &x, double &xp, double &y, double &yp, double dp) {
+  const double e = __ldg(&d[base + 0]), te = __ldg(&d[base + 1]), psi = __ldg(&d[base + 2]);
+  const double lim = __ldg(&d[base + 3]), he = __ldg(&d[base + 4]);
+  if (mode == EDGE_LIN1) {
+    double rho = (1 + dp) * rho_a;
+    double delta_xp = te / rho * x;
+    if (lim > 0 && fabs(delta_xp) > lim)
+      delta_xp = (delta_xp < 0 ? -1 : 1) * lim;
+    xp += delta_xp;
+    double t2 = psi == 0 ? te : tan(e - psi / (1 + dp));
+    yp -= t2 / rho * y;
+  } else if (mode == EDGE_LIN2) {
+    double rho = (1 + dp) * rho_a;
+    edge_order2(x, xp, y, yp, rho, nidx, e, he, psi * (1 + dp), which);
+  } else if (mode == EDGE_SYMP) {
+    /* applySimpleDipoleEdgeKick (src/csbend.c:5664-5690) */
+    double Q1 = xp, Q3 = yp;
+    double f = (1 + dp) / sqrt(1 + sqr(Q1) + sqr(Q3));
+    Q1 *= f;
+    Q3 *= f;
+    double dqx = te / rho_a * x;
+    if (lim > 0 && fabs(dqx) > lim)
+      dqx = (dqx < 0 ? -1 : 1) * lim;
+    double t2 = psi == 0 ? te : tan(e - psi / (1 + dp));
+    double dqy = -t2 / rho_a * y;
+    Q1 += dqx;
+    Q3 += dqy;
+    f = 1 / sqrt(sqr(1 + dp) - sqr(Q1) - sqr(Q3));
+    xp = Q1 * f;
+    yp = Q3 * f;
+  }
+}
+
+/* track_through_csbend (src/csbend.c:654-1434) with integrate_csbend_ordn
+ * (src/csbend.c:1459-1720); no radiation, MALIGN_METHOD=0. */
+__device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, double Po, double z_start,
+                                        const trk_aperture *ap, const double *__restrict__ field) {
+  const double *d = op->d;
+  const int nSlices = __ldg(&op->i[0]);
+  const int nSub = __ldg(&op->i[1]);
+  const int fmode = __ldg(&op->i[2]);
+  const int eo1 = __ldg(&op->i[3]);
+  const double *Fx_xy = field + __ldg(&op->i[4]);
+  const double *Fy_xy = Fx_xy + 121;
+  const int edge1 = __ldg(&op->i[5]), edge2 = __ldg(&op->i[6]);
+  const int flags = __ldg(&op->i[7]);
+  const double rho0 = __ldg(&d[BD_RHO0]), rho_a = __ldg(&d[BD_RHOA]);
+  const double ct = __ldg(&d[BD_CT]), st = __ldg(&d[BD_ST]);
+  const bool aptilt = (flags & BF_APTILT) != 0;
+  const double apc = __ldg(&d[BD_APC]), aps = __ldg(&d[BD_APS]);
+
+  double x, xp, y, yp, s, dp;
+#if !TRK_FAST
+  double dp0;
+#endif
+  if (flags & BF_MISALIGN) {
+    const double dxi = __ldg(&d[BD_DXI]), dyi = __ldg(&d[BD_DYI]), dzi = __ldg(&d[BD_DZI]);
+    p.s += dzi * sqrt(1 + sqr(p.xp) + sqr(p.yp));
+    p.x = p.x + dxi + dzi * p.xp;
+    p.y = p.y + dyi + dzi * p.yp;
+    x = p.x * ct + p.y * st;
+    y = -p.x * st + p.y * ct;
+    xp = p.xp * ct + p.yp * st;
+    yp = -p.xp * st + p.yp * ct;
+  } else {
+    x = p.x;
+    y = p.y;
+    xp = p.xp;
+    yp = p.yp;
+  }
+  s = p.s;
+  dp = p.dp;
+#if !TRK_FAST
+  dp0 = p.dp;
+#endif
+  const double nidx = __ldg(&d[BD_N]);
+  if (edge1)
+    bend_edge(edge1, d, BD_E1, -1, rho_a, nidx, x, xp, y, yp, dp);
+
+  /* convertToDipoleCanonicalCoordinates */
+  double X = x, QX, Y = y, QY, S = 0, D = dp;
+  {
+    double f = (1 + D) / sqrt(1 + sqr(xp) + sqr(yp));
+    QX = xp * f;
+    QY = yp * f;
+  }
+  /* integrate_csbend_ordn */
+  bool ok = true;
+  double dist = 0, dz_lost = 0;
+  const double sl = __ldg(&d[BD_SLICE]);
+  for (int i = 0; i < nSlices && ok; i++) {
+    if (!check_aperture(X, Y, ap, aptilt, apc, aps)) {
+      ok = false;
+      break;
+    }
+    for (int j = 0; j < nSub; j++) {
+      const double dsh = __ldg(&d[BD_DSH + j]);
+#if TRK_FAST
+      /* sin/cos(dsh/rho0 + phi) by the angle-addition formulas with
+       * tabulated sin/cos(dsh/rho0); tan(a+phi)-tan(phi) = sin a/(cos(a+phi) cos phi)
+       * and cos(phi)/cos(a+phi) - 1 = 2 sin(a/2+phi) sin(a/2)/cos(a+phi) avoid
+       * the cancellations of the reference expressions. */
+      double f2 = sqr(1 + D) - sqr(QY);
+      if (f2 <= 0) {
+        ok = false;
+        break;
+      }
+      double f = sqrt(f2);
+      double finv = 1.0 / f;
+      double sin_phi = QX * finv;
+      if (fabs(sin_phi) > 1) {
+        ok = false;
+        break;
+      }
+      double cos_phi = sqrt(fma(-sin_phi, sin_phi, 1.0));
+      const double sa = __ldg(&d[BD_SA + j]), ca = __ldg(&d[BD_CA + j]);
+      const double sh = __ldg(&d[BD_SH + j]), ch = __ldg(&d[BD_CH + j]);
+      double sine = sa * cos_phi + ca * sin_phi;
+      double cosi = ca * cos_phi - sa * sin_phi;
+      if (cosi == 0) {
+        ok = false;
+        break;
+      }
+      double cinv = 1.0 / cosi;
+      QX = f * sine;
+      double factor = (rho0 + X) * sa * finv * cinv;
+      Y += QY * factor;
+      dist += factor * (1 + D);
+      dz_lost += dsh;
+      double fm1 = 2 * (sh * cos_phi + ch * sin_phi) * sh * cinv; /* cos_phi/cosi - 1 */
+      X = rho0 * fm1 + (1 + fm1) * X;
+#else
+      double f = sqr(1 + D) - sqr(QY);
+      if (f <= 0) {
+        ok = false;
+        break;
+      }
+      f = sqrt(f);
+      if (fabs(QX / f) > 1) {
+        ok = false;
+        break;
+      }
+      double sin_phi = QX / f;
+      double phi = M_ASIN(sin_phi);
+      const double arg = __ldg(&d[BD_ARG + j]);
+      double sine = M_SIN(arg + phi);
+      double cosi = M_COS(arg + phi);
+      if (cosi == 0) {
+        ok = false;
+        break;
+      }
+      double tang = sine / cosi;
+      double cos_phi = M_COS(phi);
+      QX = f * sine;
+      double factor = (rho0 + X) * cos_phi / f * (tang - sin_phi / cos_phi);
+      Y += QY * factor;
+      dist += factor * (1 + D);
+      dz_lost += dsh;
+      f = cos_phi / cosi;
+      X = rho0 * (f - 1) + f * X;
+#endif
+      if (j == nSub - 1)
+        break;
+      const double ds = __ldg(&d[BD_DS + j]);
+      double Fx, Fy;
+      if (fmode == 0) {
+        Fx = 0;
+        Fy = 1;
+      } else
+        bend_fields(fmode, eo1, Fx_xy, Fy_xy, X, Y, Fx, Fy);
+#if TRK_FAST
+      const double w = ds * (1 + X * __ldg(&d[BD_RHOINV])) * __ldg(&d[BD_INVRHOA]);
+      QX += -w * Fy;
+      QY += w * Fx;
+#else
+      QX += -ds * (1 + X / rho0) * Fy / rho_a;
+      QY += ds * (1 + X / rho0) * Fx / rho_a;
+      if (flags & BF_ISR_ROUNDTRIP) {
+        QX /= (1 + D);
+        QY /= (1 + D);
+        QX *= (1 + D);
+        QY *= (1 + D);
+      }
+#endif
+    }
+  }
+  if (ok) {
+    dz_lost = nSlices * sl;
+    if (!check_aperture(X, Y, ap, aptilt, apc, aps))
+      ok = false;
+    else
+      S += dist;
+  }
+  /* convertFromDipoleCanonicalCoordinates */
+  {
+    double f = 1 / sqrt(sqr(1 + D) - sqr(QX) - sqr(QY));
+    QX *= f;
+    QY *= f;
+  }
+  if (!ok) {
+    /* convertFromCSBendCoords (src/csbend.c:4527-4548) then loss record */
+    p.x = X * ct - Y * st;
+    p.y = X * st + Y * ct;
+    p.xp = QX * ct - QY * st;
+    p.yp = QX * st + QY * ct;
+    p.s = z_start + dz_lost;
+    p.dp = Po * (1 + D);
+    return false;
+  }
+#if TRK_FAST
+  s += S;
+#else
+  if (flags & BF_ISR_ROUNDTRIP) {
+    double p0 = Po * (1 + dp0);
+    double beta0 = p0 / sqrt(sqr(p0) + 1);
+    double p1 = Po * (1 + D);
+    double beta1 = p1 / sqrt(sqr(p1) + 1);
+    s = beta1 * s / beta0 + S;
+  } else
+    s += S;
+#endif
+  x = X;
+  xp = QX;
+  y = Y;
+  yp = QY;
+  dp = D;
+  if (edge2)
+    bend_edge(edge2, d, BD_E2, 1, rho_a, nidx, x, xp, y, yp, dp);
+  if (flags & BF_MISALIGN) {
+    p.x = x * ct - y * st + __ldg(&d[BD_ET + 0]);
+    p.y = x * st + y * ct + __ldg(&d[BD_ET + 2]);
+    p.xp = xp * ct - yp * st + __ldg(&d[BD_ET + 1]);
+    p.yp = xp * st + yp * ct + __ldg(&d[BD_ET + 3]);
+    p.s = s + __ldg(&d[BD_ET + 4]);
+    p.dp = dp;
+    const double dxf = __ldg(&d[BD_DXF]), dyf = __ldg(&d[BD_DYF]), dzf = __ldg(&d[BD_DZF]);
+    p.x += dxf + dzf * p.xp;
+    p.y += dyf + dzf * p.yp;
+    p.s += dzf * sqrt(1 + sqr(p.xp) + sqr(p.yp));
+  } else {
+    p.x = x;
+    p.xp = xp;
+    p.y = y;
+    p.yp = yp;
+    p.s = s;
+    p.dp = dp;
+  }
+  return true;
+}
+
+/* ----------------------------------------------------------------- RFCA */
+/* add_to_particle_energy (src/simple_rfca.c:987-1006) */
+__device__ __forceinline__ void add_energy(Part &p, double t, double Po, double dgamma) {
+  double P = Po * (1 + p.dp);
+  double gamma = sqrt(P * P + 1);
+  double gamma1 = gamma + dgamma;
+  if (gamma1 <= 1)
+    gamma1 = 1 + 1e-7;
+  double P1 = sqrt(gamma1 * gamma1 - 1);
+  p.dp = (P1 - Po) / Po;
+  p.s = t * TRK_C_MKS * P1 / gamma1;
+  double Pz = P / sqrt(1 + sqr(p.xp) + sqr(p.yp));
+  double Pz1 = sqrt(Pz * Pz + gamma1 * gamma1 - gamma * gamma);
+  double PRatio = Pz / Pz1;
+  p.xp *= PRatio;
+  p.yp *= PRatio;
+}
+
+/* trackRfCavityWithWakes (src/simple_rfca.c:295-985), kick method,
+ * traveling wave, per particle; ends with removeInvalidParticles. */
+__device__ __forceinline__ bool op_rf(const trk_op *__restrict__ op, Part &p, double Po, double z_end,
+                                      const double *__restrict__ rf_phase) {
+  const double *d = op->d;
+  const int nKicks = __ldg(&op->i[0]);
+  const int slot = __ldg(&op->i[1]);
+  const int flags = __ldg(&op->i[3]);
+  const double omega = __ldg(&d[RD_OMEGA]), volt = __ldg(&d[RD_VOLT]), length = __ldg(&d[RD_LEN]);
+  const double dtLight = __ldg(&d[RD_DTL]), tau = __ldg(&d[RD_TAU]);
+  const double phase_fid = rf_phase[slot];
+  double t0 = omega ? -phase_fid / omega : 0;
+  double phase = phase_fid + __ldg(&d[RD_PHASE_ADD]);
+  double dgamma = 0;
+  if (flags & RF_SAME_DGAMMA)
+    dgamma = volt * M_SIN(phase);
+  if (flags & RF_OFFSET) {
+    p.x -= __ldg(&d[RD_DX]);
+    p.y -= __ldg(&d[RD_DY]);
+  }
+  double inverseF = 0;
+  for (int ik = 0; ik < nKicks; ik++) {
+    if (p.dp != -1) {
+      double dc4 = length ? length / 2 * sqrt(1 + sqr(p.xp) + sqr(p.yp)) : 0;
+      double P = Po * (1 + p.dp);
+      double gamma = sqrt(sqr(P) + 1);
+      double beta_i = P / gamma;
+      double t = (p.s + dc4) / (TRK_C_MKS * beta_i) - 0.0;
+      double dt = t - t0;
+      if (dt < 0)
+        dt = 0;
+      if (!(flags & RF_SAME_DGAMMA)) {
+        double phi = omega * (t - 0 - ik * dtLight) + phase;
+        double dfactor = tau ? sqrt(1 - exp(-dt / tau)) : 1;
+        dgamma = volt * M_SIN(phi) * dfactor;
+      }
+      if (length) {
+        if ((flags & RF_END1) && ik == 0) {
+          inverseF = dgamma / (2 * gamma * length);
+          p.xp -= p.x * inverseF;
+          p.yp -= p.y * inverseF;
+        }
+        p.x += p.xp * length / 2;
+        p.y += p.yp * length / 2;
+        p.s += length / 2 * sqrt(1 + sqr(p.xp) + sqr(p.yp));
+      }
+      add_energy(p, t, Po, dgamma);
+      double gamma1 = gamma + dgamma;
+      if (gamma1 <= 1)
+        p.dp = -1;
+      else
+        inverseF = -dgamma / (2 * gamma1 * length);
+    }
+    if (length) {
+      p.x += p.xp * length / 2;
+      p.y += p.yp * length / 2;
+      p.s += length / 2 * sqrt(1 + sqr(p.xp) + sqr(p.yp));
+      if ((flags & RF_END2) && ik == nKicks - 1) {
+        p.xp -= p.x * inverseF;
+        p.yp -= p.y * inverseF;
+      }
+    }
+  }
+  if (flags & RF_OFFSET) {
+    p.x += __ldg(&d[RD_DX]);
+    p.y += __ldg(&d[RD_DY]);
+  }
+  /* removeInvalidParticles (src/limit_amplitudes.c:~290-345) */
+  if (isnan(p.x) || isnan(p.xp) || isnan(p.y) || isnan(p.yp) || isnan(p.s) || isnan(p.dp) || p.dp <= -1) {
+    p.s = z_end;
+    p.dp = Po * (1 + p.dp);
+    return false;
+  }
+  return true;
+}
+
+/* ------------------------------------------------------ after-element */
+/* limit_amplitudes / elimit_amplitudes (src/limit_amplitudes.c:197-288,
+ * 487-~620) for one particle; returns true if lost. */
+__device__ __forceinline__ bool post_aperture(Part &p, const trk_aperture *__restrict__ ap, int extrapolate, double z,
+                                              double Po) {
+  double xmax = ap->x_max, ymax = ap->y_max;
+  if (ap->elliptical && xmax > 0 && ymax > 0) {
+    if (isinf(p.x) || isinf(p.y) || isnan(p.x) || isnan(p.y)) {
+      p.s = z;
+      p.dp = sqrt(sqr(Po * (1 + p.dp)) + 1);
+      return true;
+    }
+    const int xe = ap->xexp, ye = ap->yexp;
+    const double a2 = ap->a2, b2 = ap->b2;
+    if ((ipow_d(p.x, xe) / a2 + ipow_d(p.y, ye) / b2) > 1) {
+      double dz = 0;
+      if (extrapolate && xe == 2 && ye == 2) {
+        double c0 = sqr(p.x) / a2 + sqr(p.y) / b2 - 1;
+        double c1 = 2 * (p.x * p.xp / a2 + p.y * p.yp / b2);
+        double c2 = sqr(p.xp) / a2 + sqr(p.yp) / b2;
+        double det = sqr(c1) - 4 * c0 * c2;
+        if (z > 0 && c2 && det >= 0) {
+          if ((dz = (-c1 + sqrt(det)) / (2 * c2)) > 0)
+            dz = (-c1 - sqrt(det)) / (2 * c2);
+          if ((z + dz) < 0)
+            dz = -z;
+          p.x += dz * p.xp;
+          p.y += dz * p.yp;
+        }
+      }
+      p.s = z + dz;
+      p.dp = sqrt(sqr(Po * (1 + p.dp)) + 1);
+      return true;
+    }
+    return false;
+  }
+  if (xmax < 0 && ymax < 0)
+    return false;
+  int is_out = 0;
+  if (xmax > 0 && fabs(p.x) > xmax)
+    is_out += 1;
+  if (ymax > 0 && fabs(p.y) > ymax)
+    is_out += 2;
+  if (isinf(p.x) || isinf(p.y) || isnan(p.x) || isnan(p.y))
+    is_out += 4;
+  if (!is_out)
+    return false;
+  double dz = 0;
+  if (!(is_out & 4) && extrapolate) {
+    double dzx = -1.7976931348623157e308, dzy = -1.7976931348623157e308;
+    if ((is_out & 1) && p.xp != 0)
+      dzx = (p.x - (p.xp < 0 ? -1 : 1) * xmax) / p.xp;
+    if ((is_out & 2) && p.yp != 0)
+      dzy = (p.y - (p.yp < 0 ? -1 : 1) * ymax) / p.yp;
+    if (dzx > dzy)
+      dz = -dzx;
+    else
+      dz = -dzy;
+    if (dz == -1.7976931348623157e308)
+      dz = 0;
+  }
+  p.x += dz * p.xp;
+  p.y += dz * p.yp;
+  p.s = z + dz;
+  p.dp = Po * (1 + p.dp);
+  return true;
+}
+
+/* DRIF through its order-1/2 matrix (src/compute_matrices.c:391-413,
+ * src/matrix.c:310-422): the structural zeros contribute only signed zeros
+ * for finite input and NaN when any coordinate is not finite. */
+__device__ __forceinline__ void op_drift(const trk_op *__restrict__ op, Part &p) {
+  const double L = __ldg(&op->d[DD_L]);
+  const int order = __ldg(&op->i[0]);
+  if (!(isfinite(p.x) && isfinite(p.xp) && isfinite(p.y) && isfinite(p.yp) && isfinite(p.s) && isfinite(p.dp))) {
+    const double qnan = __longlong_as_double(0x7ff8000000000000ULL);
+    p.x = p.xp = p.y = p.yp = p.s = p.dp = qnan;
+    return;
+  }
+  double xp = p.xp, yp = p.yp;
+  double x1 = L * xp + p.x;
+  double y1 = L * yp + p.y;
+  double s1;
+  if (order >= 2) {
+    const double T = __ldg(&op->d[DD_T]);
+    double a = L + p.s;
+    double b = (T * yp) * yp;
+#if TRK_FAST
+    s1 = (a + b) + (T * xp) * xp;
+#else
+    s1 = __dadd_rn(__dadd_rn(a, b), __dmul_rn(__dmul_rn(T, xp), xp));
+#endif
+  } else
+    s1 = L + p.s;
+  p.x = x1;
+  p.y = y1;
+  p.s = s1;
+}
+
+/* ------------------------------------------------------------- kernels */
+__device__ __forceinline__ void load_part(const TrackArgs &a, long i, Part &p) {
+  p.x = a.x[i];
+  p.xp = a.xp[i];
+  p.y = a.y[i];
+  p.yp = a.yp[i];
+  p.s = a.s[i];
+  p.dp = a.dp[i];
+}
+
+__device__ __forceinline__ void store_part(const TrackArgs &a, long i, const Part &p) {
+  a.x[i] = p.x;
+  a.xp[i] = p.xp;
+  a.y[i] = p.y;
+  a.yp[i] = p.yp;
+  a.s[i] = p.s;
+  a.dp[i] = p.dp;
+}
+
+/* Track one particle through ops [ob, oe) for passes [pb, pe).  Returns
+ * false if it was lost (loss recorded). */
+__device__ __forceinline__ bool track_particle(const TrackArgs &a, Part &p, long i) {
+  for (long pass = a.pass_begin; pass < a.pass_end; pass++) {
+    const int var = (pass == a.fresh_pass) ? 0 : 1;
+    for (int k = a.op_begin; k < a.op_end; k++) {
+      const trk_op *op = a.ops + k;
+      const int kind = __ldg(&op->kind);
+      const double z_start = __ldg(&op->z_start), z_end = __ldg(&op->z_end);
+      const int api = __ldg(&op->ap_in[var]);
+      const trk_aperture *ap_in = api >= 0 ? a.aps + api : nullptr;
+      bool ok = true;
+      switch (kind) {
+      case OPK_DRIFT:
+        op_drift(op, p);
+        break;
+      case OPK_EDRIFT:
+        exact_drift(p, __ldg(&op->d[DD_L]));
+        break;
+      case OPK_RFDRIFT:
+        exact_drift(p, __ldg(&op->d[DD_L]));
+        break;
+      case OPK_MULT:
+        ok = op_mult(op, p, a.Po, z_start, ap_in);
+        break;
+      case OPK_BEND:
+        ok = op_bend(op, p, a.Po, z_start, ap_in, a.field);
+        break;
+      case OPK_RF:
+        ok = op_rf(op, p, a.Po, z_end, a.rf_phase);
+        break;
+      default:
+        break;
+      }
+      if (ok && !__ldg(&op->no_aperture)) {
+        const int apo = __ldg(&op->ap_post[var]);
+        if (apo >= 0)
+          ok = !post_aperture(p, a.aps + apo, __ldg(&op->extrapolate), z_end, a.Po);
+      }
+      if (ok && (isinf(p.x) || isinf(p.y) || isnan(p.x) || isnan(p.y))) {
+        p.s = z_end;
+        p.dp = a.Po * (1 + p.dp);
+        ok = false;
+      }
+      if (!ok) {
+        a.lost_pass[i] = (int32_t)pass;
+        a.lost_elem[i] = __ldg(&op->elem);
+        return false;
+      }
+    }
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(TRK_BLOCK) track_kernel(TrackArgs a) {
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+    if (a.lost_pass[i] >= 0)
+      continue;
+    Part p;
+    load_part(a, i, p);
+    track_particle(a, p, i);
+    store_part(a, i, p);
+  }
+}
+
+/* computeTimeCoordinatesOnly (src/trwake.c:519-527), rounded step by step
+ * in both builds so the statistics, binning and kick kernels agree. */
+__device__ __forceinline__ double wake_time(double Po, double dp, double s) {
+  double P = __dmul_rn(Po, __dadd_rn(dp, 1.0));
+  double num = __dmul_rn(s, __dsqrt_rn(__dadd_rn(__dmul_rn(P, P), 1.0)));
+  return __ddiv_rn(num, __dmul_rn(TRK_C_MKS, P));
+}
+
+/* bin index (long)((t - tmin)/dt + 0.5) of binTimeDistribution (src/wake.c:509) */
+__device__ __forceinline__ long wake_bin(double t, double tmin, double dt) {
+  return (long)__dadd_rn(__ddiv_rn(__dsub_rn(t, tmin), dt), 0.5);
+}
+
+/* --------------------------------------------------------- reductions */
+/* Sum of per-particle times for WAKE (computeTimeCoordinatesOnly,
+ * src/trwake.c:519-527) or the RFCA "tmean" fiducial (findFiducialTime,
+ * src/simple_rfca.c:191-230), in double-double so the block partials do not
+ * depend on the launch shape; min/max and the survivor count alongside. */
+__global__ void __launch_bounds__(TRK_BLOCK) time_stats_kernel(TimeStatsArgs a) {
+  __shared__ double sh_hi[TRK_BLOCK], sh_lo[TRK_BLOCK], sh_min[TRK_BLOCK], sh_max[TRK_BLOCK];
+  __shared__ long long sh_n[TRK_BLOCK];
+  trkcr::dd acc = {0.0, 0.0};
+  double tmin = 1.7976931348623157e308, tmax = -1.7976931348623157e308;
+  long long cnt = 0;
+  /* particles are assigned to blocks in fixed chunks so the result does
+   * not depend on the grid size */
+  const long chunk = a.chunk;
+  for (long c = blockIdx.x; c * chunk < a.n; c += gridDim.x) {
+    const long lo = c * chunk, hi = min(a.n, lo + chunk);
+    trkcr::dd cacc = {0.0, 0.0};
+    for (long i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+      if (a.lost_pass[i] >= 0)
+        continue;
+      double t;
+      if (a.mode == 0) {
+        t = wake_time(a.Po, a.dp[i], a.s[i]);
+      } else {
+        double p = a.Po * (1 + a.dp[i]);
+        double beta = p / sqrt(p * p + 1);
+        t = (a.s[i] + a.sOffset) / (TRK_C_MKS * beta);
+      }
+      cacc = trkcr::dd_add(cacc, trkcr::dd{t, 0.0});
+      tmin = fmin(tmin, t);
+      tmax = fmax(tmax, t);
+      cnt++;
+    }
+    acc = trkcr::dd_add(acc, cacc);
+  }
+  const int tid = threadIdx.x;
+  sh_hi[tid] = acc.hi;
+  sh_lo[tid] = acc.lo;
+  sh_min[tid] = tmin;
+  sh_max[tid] = tmax;
+  sh_n[tid] = cnt;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (tid < w) {
+      trkcr::dd u = trkcr::dd_add(trkcr::dd{sh_hi[tid], sh_lo[tid]}, trkcr::dd{sh_hi[tid + w], sh_lo[tid + w]});
+      sh_hi[tid] = u.hi;
+      sh_lo[tid] = u.lo;
+      sh_min[tid] = fmin(sh_min[tid], sh_min[tid + w]);
+      sh_max[tid] = fmax(sh_max[tid], sh_max[tid + w]);
+      sh_n[tid] += sh_n[tid + w];
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    a.part_hi[blockIdx.x] = sh_hi[0];
+    a.part_lo[blockIdx.x] = sh_lo[0];
+    a.part_min[blockIdx.x] = sh_min[0];
+    a.part_max[blockIdx.x] = sh_max[0];
+    a.part_n[blockIdx.x] = sh_n[0];
+  }
+}
+
+/* Combine block partials in index order; write {sum, n, min, max}. */
+__global__ void time_stats_finish_kernel(TimeStatsArgs a, int nblocks) {
+  if (threadIdx.x != 0 || blockIdx.x != 0)
+    return;
+  trkcr::dd acc = {0.0, 0.0};
+  double tmin = 1.7976931348623157e308, tmax = -1.7976931348623157e308;
+  long long n = 0;
+  for (int b = 0; b < nblocks; b++) {
+    acc = trkcr::dd_add(acc, trkcr::dd{a.part_hi[b], a.part_lo[b]});
+    tmin = fmin(tmin, a.part_min[b]);
+    tmax = fmax(tmax, a.part_max[b]);
+    n += a.part_n[b];
+  }
+  a.out[0] = __dadd_rn(acc.hi, acc.lo);
+  a.out[1] = (double)n;
+  a.out[2] = tmin;
+  a.out[3] = tmax;
+}
+
+/* RFCA fiducial: phase_fiducial = -omega * tmean (src/simple_rfca.c:412-445) */
+__global__ void rf_fiducial_kernel(const double *stats, double omega, double t_reference, double *rf_phase, int slot,
+                                   int *status) {
+  if (threadIdx.x != 0 || blockIdx.x != 0)
+    return;
+  double t0;
+  if (t_reference != -1)
+    t0 = t_reference;
+  else {
+    if (stats[1] <= 0) {
+      atomicOr(status, TRK_STATUS_NO_PARTICLES);
+      t0 = 0;
+    } else
+      t0 = stats[0] / stats[1];
+  }
+  rf_phase[slot] = -omega * t0;
+}
+
+/* ------------------------------------------------------------ wakes */
+
+/* Wake geometry of one pass (src/wake.c:118-190, src/trwake.c:105-150) */
+__global__ void wake_setup_kernel(WakeArgs a) {
+  if (threadIdx.x != 0 || blockIdx.x != 0)
+    return;
+  const double *st = a.stats;
+  double n = st[1];
+  WakeState *w = a.state;
+  w->nb = 0;
+  if (n <= 0)
+    return;
+  double tmean = a.transverse ? 0.0 : st[0] / n;
+  double tmin = st[2], tmax = st[3];
+  if ((tmax - tmin) > a.wake_span && !a.allow_long_beam) {
+    atomicOr(a.status, TRK_STATUS_LONG_BEAM);
+    return;
+  }
+  long nb;
+  if (a.n_bins) {
+    nb = a.n_bins;
+    tmin = tmean - a.dt * nb / 2.0;
+  } else {
+    nb = (long)((tmax - tmin) / a.dt + 3);
+    tmin -= a.dt;
+  }
+  if (nb > a.max_bins) {
+    atomicOr(a.status, TRK_STATUS_TOO_MANY_BINS);
+    return;
+  }
+  w->nb = nb;
+  w->tmin = tmin;
+  w->ramp = (a.pass >= a.ramp_passes - 1) ? 1.0 : (a.pass + 1.0) / a.ramp_passes;
+  if (a.macro_mode == 0)
+    w->macro = a.macro_charge;
+  else if (a.macro_mode == 1)
+    w->macro = a.charge / n; /* set_up_wake: charge / particles on pass 0 (src/wake.c:350-358) */
+}
+
+/* Bin particle times (binTimeDistribution, src/wake.c:498-518): integer
+ * counts through a shared-memory histogram, then one global atomic per
+ * non-empty bin per block.  Transverse wakes also sum x-dx and y-dy per bin
+ * (binTransverseTimeDistribution, src/trwake.c:610-641). */
+__global__ void __launch_bounds__(TRK_BLOCK) wake_bin_kernel(WakeArgs a) {
+  extern __shared__ unsigned int sh_cnt[];
+  const WakeState *w = a.state;
+  const long nb = w->nb;
+  if (nb <= 0)
+    return;
+  const bool use_smem = nb <= a.smem_bins && !a.transverse;
+  if (use_smem) {
+    for (long b = threadIdx.x; b < nb; b += blockDim.x)
+      sh_cnt[b] = 0;
+    __syncthreads();
+  }
+  const double tmin = w->tmin, dt = a.dt;
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+    if (a.lost_pass[i] >= 0)
+      continue;
+    double t = wake_time(a.Po, a.dp[i], a.s[i]);
+    long ib = wake_bin(t, tmin, dt);
+    if (ib < 0 || ib > nb - 1)
+      continue;
+    if (a.transverse) {
+      double vx, vy;
+      if (a.x_power == 1)
+        vx = a.x[i] - a.tdx;
+      else if (a.x_power < 1)
+        vx = 1;
+      else
+        vx = ipow_d(a.x[i] - a.tdx, a.x_power);
+      if (a.y_power == 1)
+        vy = a.y[i] - a.tdy;
+      else if (a.y_power < 1)
+        vy = 1;
+      else
+        vy = ipow_d(a.y[i] - a.tdy, a.y_power);
+      atomicAdd(&a.hist_x[ib], vx);
+      atomicAdd(&a.hist_y[ib], vy);
+    } else if (use_smem) {
+      atomicAdd(&sh_cnt[ib], 1u);
+    } else {
+      atomicAdd(&a.counts[ib], 1ull);
+    }
+  }
+  if (use_smem) {
+    __syncthreads();
+    for (long b = threadIdx.x; b < nb; b += blockDim.x)
+      if (sh_cnt[b])
+        atomicAdd(&a.counts[b], (unsigned long long)sh_cnt[b]);
+  }
+}
+
+/* convolveArrays (src/wake.c:480-496) in the reference's summation order,
+ * one output bin per thread; scaled by Q_macro * sign * FACTOR * ramp
+ * (src/wake.c:254-261). */
+__global__ void wake_convolve_kernel(WakeArgs a, int plane) {
+  const WakeState *w = a.state;
+  const long nb = w->nb;
+  const long ib = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ib > nb)
+    return;
+  double *V = plane ? a.V_y : a.V;
+  if (ib == nb) {
+    V[nb] = 0;
+    return;
+  }
+  const double *W = plane ? a.W_y : a.W;
+  const long n2 = a.wake_points;
+  long ib2 = ib + a.i0, ib1 = 0;
+  if (ib2 >= n2) {
+    long di = ib2 - n2 + 1;
+    ib1 += di;
+    ib2 -= di;
+  }
+  double out = 0;
+  if (a.transverse) {
+    const double *I = plane ? a.hist_y : a.hist_x;
+    for (; ib1 < nb && ib2 >= 0; ib1++, ib2--)
+      out += I[ib1] * W[ib2];
+  } else {
+    for (; ib1 < nb && ib2 >= 0; ib1++, ib2--)
+      out += (double)a.counts[ib1] * W[ib2];
+  }
+  double factor = w->macro * TRK_PARTICLE_REL_SIGN * a.factor;
+  if (a.transverse)
+    factor *= (plane ? a.yfactor : a.xfactor) * w->ramp;
+  else
+    factor *= w->ramp;
+  V[ib] = out * factor;
+}
+
+/* applyLongitudinalWakeKicks (src/wake.c:306-330) / applyTransverseWakeKicks
+ * (src/trwake.c:289-314), then the element's after-element filters. */
+__global__ void __launch_bounds__(TRK_BLOCK) wake_kick_kernel(WakeArgs a) {
+  const WakeState *w = a.state;
+  const long nb = w->nb;
+  const double tmin = w->tmin, dt = a.dt;
+  const long stride = (long)gridDim.x * blockDim.x;
+  const double mass = 1e6 * TRK_ME_MEV * TRK_PARTICLE_REL_SIGN;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+    if (a.lost_pass[i] >= 0)
+      continue;
+    Part p;
+    p.x = a.x[i];
+    p.xp = a.xp[i];
+    p.y = a.y[i];
+    p.yp = a.yp[i];
+    p.s = a.s[i];
+    p.dp = a.dp[i];
+    if (nb > 0) {
+      double t = wake_time(a.Po, p.dp, p.s);
+      long ib = wake_bin(t, tmin, dt);
+      if (ib >= 0 && ib <= nb - 1) {
+        if (!a.transverse) {
+          double dgam;
+          if (a.interpolate) {
+            double dt1 = t - (tmin + dt * ib);
+            if ((dt1 < 0 && ib) || ib == nb - 1) {
+              ib--;
+              dt1 += dt;
+            }
+            dgam = (a.V[ib] + (a.V[ib + 1] - a.V[ib]) / dt * dt1) / mass;
+          } else
+            dgam = a.V[ib] / mass;
+          if (dgam)
+            add_energy(p, t, a.Po, -dgam);
+        } else {
+          double pz = a.Po * (1 + p.dp) / sqrt(1 + sqr(p.xp) + sqr(p.yp));
+          for (int plane = 0; plane < 2; plane++) {
+            if (!(a.active_planes & (1 << plane)))
+              continue;
+            const double *V = plane ? a.V_y : a.V;
+            long jb = ib;
+            double Vi;
+            if (a.interpolate) {
+              double dt1 = t - (tmin + dt * jb);
+              if ((dt1 < 0 && jb) || jb == nb - 1) {
+                jb--;
+                dt1 += dt;
+              }
+              Vi = V[jb] + (V[jb + 1] - V[jb]) / dt * dt1;
+            } else
+              Vi = V[jb];
+            int exponent = plane ? a.y_probe : a.x_probe;
+            if (exponent)
+              Vi *= ipow_d(plane ? p.y : p.x, exponent);
+            if (Vi) {
+              if (plane)
+                p.yp += Vi / mass / pz;
+              else
+                p.xp += Vi / mass / pz;
+            }
+          }
+        }
+      }
+    }
+    if (a.untilt)
+      rotate(p, a.tilt_c, a.tilt_s);
+    /* after-element filters of the wake element */
+    bool lost = false;
+    if (a.ap_post >= 0)
+      lost = post_aperture(p, a.aps + a.ap_post, 0, a.z_end, a.Po);
+    if (!lost && (isinf(p.x) || isinf(p.y) || isnan(p.x) || isnan(p.y))) {
+      p.s = a.z_end;
+      p.dp = a.Po * (1 + p.dp);
+      lost = true;
+    }
+    if (lost) {
+      a.lost_pass[i] = (int32_t)a.pass;
+      a.lost_elem[i] = a.elem;
+    }
+    a.x[i] = p.x;
+    a.xp[i] = p.xp;
+    a.y[i] = p.y;
+    a.yp[i] = p.yp;
+    a.s[i] = p.s;
+    a.dp[i] = p.dp;
+  }
+}
+
+/* rotateBeamCoordinatesForMisalignment over the surviving beam (TRWAKE TILT) */
+__global__ void rotate_kernel(TrackArgs a, double ca, double sa) {
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+    if (a.lost_pass[i] >= 0)
+      continue;
+    Part p;
+    load_part(a, i, p);
+    rotate(p, ca, sa);
+    store_part(a, i, p);
+  }
+}
+
+/* ------------------------------------------------------------- launchers */
+void launch_track(const TrackArgs &a, int grid, int block, cudaStream_t st) {
+  track_kernel<<<grid, block, 0, st>>>(a);
+}
+
+void launch_time_stats(const TimeStatsArgs &a, int grid, cudaStream_t st) {
+  time_stats_kernel<<<grid, TRK_BLOCK, 0, st>>>(a);
+  time_stats_finish_kernel<<<1, 1, 0, st>>>(a, grid);
+}
+
+void launch_rf_fiducial(const double *stats, double omega, double t_reference, double *rf_phase, int slot,
+                        int *status, cudaStream_t st) {
+  rf_fiducial_kernel<<<1, 1, 0, st>>>(stats, omega, t_reference, rf_phase, slot, status);
+}
+
+void launch_wake(const WakeArgs &a, int grid, cudaStream_t st) {
+  wake_setup_kernel<<<1, 1, 0, st>>>(a);
+  size_t smem = a.transverse ? 0 : (size_t)a.smem_bins * sizeof(unsigned int);
+  wake_bin_kernel<<<grid, TRK_BLOCK, smem, st>>>(a);
+  int cb = (int)((a.max_bins + 1 + 127) / 128);
+  wake_convolve_kernel<<<cb, 128, 0, st>>>(a, 0);
+  if (a.transverse)
+    wake_convolve_kernel<<<cb, 128, 0, st>>>(a, 1);
+  wake_kick_kernel<<<grid, TRK_BLOCK, 0, st>>>(a);
+}
+
+void launch_rotate(const TrackArgs &a, double ca, double sa, int grid, cudaStream_t st) {
+  rotate_kernel<<<grid, TRK_BLOCK, 0, st>>>(a, ca, sa);
+}
+
+cudaError_t set_coefficients(const double *coef10) {
+  return cudaMemcpyToSymbol(c_coef, coef10, sizeof(double) * 10);
+}
+
+} // namespace TRK_NS

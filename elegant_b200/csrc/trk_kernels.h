@@ -1,0 +1,107 @@
+/*
+ * trk_kernels.h -- launch arguments and launchers of the tracking kernels.
+ * trk_kernels.cu is compiled twice (namespaces trk_exact and trk_fast); the
+ * host code in trk_host.cu picks one per run.
+ */
+#ifndef TRK_KERNELS_H
+#define TRK_KERNELS_H
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "trk_ops.h"
+
+#define TRK_BLOCK 128
+
+/* device status word bits (a kernel records a problem and returns; the host
+ * turns the word into a trk_error after the launch sequence) */
+#define TRK_STATUS_LONG_BEAM 1      /* beam longer than the wake table (src/wake.c:134-140) */
+#define TRK_STATUS_TOO_MANY_BINS 2  /* autoscaled bin count above the allocated histogram */
+#define TRK_STATUS_NO_PARTICLES 4   /* RF fiducial with no particles (src/simple_rfca.c:228) */
+
+struct TrackArgs {
+  double *x, *xp, *y, *yp, *s, *dp;
+  int32_t *lost_pass, *lost_elem;
+  const trk_op *ops;
+  const trk_aperture *aps;
+  const double *field;
+  const double *rf_phase;
+  long n;
+  int op_begin, op_end;
+  long pass_begin, pass_end;
+  long fresh_pass; /* pass that sees the MAXAMP state of a fresh do_tracking call */
+  double Po;
+};
+
+struct TimeStatsArgs {
+  const double *s, *dp;
+  const int32_t *lost_pass;
+  long n;
+  long chunk;
+  int mode;        /* 0: wake time s*sqrt(P^2+1)/(c P); 1: RF fiducial (s+sOffset)/(c beta) */
+  double Po, sOffset;
+  double *part_hi, *part_lo, *part_min, *part_max;
+  long long *part_n;
+  double *out;     /* {sum, n, min, max} */
+};
+
+struct WakeState {
+  long nb;
+  double tmin;
+  double ramp;
+  double macro;
+};
+
+struct WakeArgs {
+  double *x, *xp, *y, *yp, *s, *dp;
+  int32_t *lost_pass, *lost_elem;
+  long n;
+  double Po;
+  const double *stats;    /* from time stats: {sum, n, min, max} */
+  WakeState *state;
+  int *status;
+  /* geometry */
+  double dt, wake_span;
+  long wake_points, i0;
+  long n_bins, max_bins;
+  int smem_bins;
+  int allow_long_beam;
+  long pass, ramp_passes;
+  double macro_charge;    /* used when macro_mode == 0 */
+  int macro_mode;         /* 0: macro_charge given; 1: charge / survivors (pass 0, no CHARGE element); 2: keep */
+  double charge;          /* element CHARGE parameter for macro_mode 1 */
+  double factor, xfactor, yfactor;
+  int interpolate;
+  int transverse;
+  int active_planes;
+  int x_power, y_power, x_probe, y_probe;
+  double tdx, tdy;
+  int untilt;             /* TRWAKE TILT: rotate back by (tilt_c, tilt_s) before the filters */
+  double tilt_c, tilt_s;
+  /* buffers */
+  const double *W, *W_y;
+  unsigned long long *counts;
+  double *hist_x, *hist_y;
+  double *V, *V_y;
+  /* after-element filters */
+  const trk_aperture *aps;
+  int ap_post;
+  double z_end;
+  int elem;
+};
+
+#define TRK_DECLARE_LAUNCHERS(NS)                                                                            \
+  namespace NS {                                                                                             \
+  void launch_track(const TrackArgs &a, int grid, int block, cudaStream_t st);                               \
+  void launch_time_stats(const TimeStatsArgs &a, int grid, cudaStream_t st);                                 \
+  void launch_rf_fiducial(const double *stats, double omega, double t_reference, double *rf_phase, int slot, \
+                          int *status, cudaStream_t st);                                                     \
+  void launch_wake(const WakeArgs &a, int grid, cudaStream_t st);                                            \
+  void launch_rotate(const TrackArgs &a, double ca, double sa, int grid, cudaStream_t st);                   \
+  cudaError_t set_coefficients(const double *coef10);                                                        \
+  }
+
+TRK_DECLARE_LAUNCHERS(trk_exact)
+TRK_DECLARE_LAUNCHERS(trk_fast)
+
+#endif

@@ -1,0 +1,160 @@
+/*
+ * trk_ops.h -- the compiled lattice as the kernels read it.
+ *
+ * The host turns each lattice element into one trk_op record whose constants
+ * are everything the reference computes once per element call (strengths
+ * divided by slices, substep lengths, edge tangents, misalignment cos/sin,
+ * ...), evaluated on the host with the reference's expressions so the device
+ * only runs the per-particle arithmetic.  Records are 1 KB-aligned-free POD,
+ * read with uniform (warp-broadcast) loads.
+ */
+#ifndef TRK_OPS_H
+#define TRK_OPS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum trk_op_kind {
+  OPK_NOP = 0,    /* MARK, CHARGE, MAXAMP (state is baked into aperture indices) */
+  OPK_DRIFT = 1,  /* DRIF, order-1/2 transport matrix */
+  OPK_EDRIFT = 2, /* EDRIFT, and CSBEND with ANGLE=0 */
+  OPK_MULT = 3,   /* KQUAD, KSEXT, KOCT */
+  OPK_BEND = 4,   /* CSBEND */
+  OPK_RF = 5,     /* RFCA */
+  OPK_WAKE = 6,   /* WAKE (collective: ends a fused segment) */
+  OPK_TRWAKE = 7, /* TRWAKE (collective) */
+  OPK_RFDRIFT = 8 /* RFCA with VOLT=0: drift of length L */
+};
+
+/* multipole flags (i[6]) */
+#define MF_OFFSET 1   /* DX/DY/DZ nonzero */
+#define MF_TILT 2     /* TILT nonzero */
+#define MF_ENDDRIFT 4 /* LEFFECTIVE end drifts */
+#define MF_XKICK 8
+#define MF_YKICK 16
+#define MF_KNL0 32
+#define MF_KNL1 64
+#define MF_KNL2 128
+#define MF_APTILT 256 /* aperture check rotates by -TILT */
+
+/* bend flags (i[7]) */
+#define BF_ISR_ROUNDTRIP 1 /* reference's (1+DPoP) divide/multiply round trip */
+#define BF_MISALIGN 2      /* entry/exit offsets or tilt not all zero */
+#define BF_APTILT 4
+
+/* RF flags (i[3]) */
+#define RF_SAME_DGAMMA 1
+#define RF_END1 2
+#define RF_END2 4
+#define RF_OFFSET 8
+
+typedef struct {
+  int32_t kind;
+  int32_t elem;        /* lattice element index (loss bookkeeping) */
+  int32_t ap_post[2];  /* after-element aperture record for pass 0 / later passes (-1 none) */
+  int32_t ap_in[2];    /* in-element (per slice) aperture record, pass 0 / later (-1 none) */
+  int32_t extrapolate; /* limit_amplitudes extrapolate_z (DRIF) */
+  int32_t no_aperture; /* NO_APERTURE element class (MARK, CHARGE) */
+  int32_t i[8];
+  double z_start, z_end;
+  double d[120];
+} trk_op;
+
+/* after-element / in-element aperture from the sticky MAXAMP state */
+typedef struct {
+  double x_max, y_max;
+  int32_t elliptical;
+  int32_t xexp, yexp;
+  int32_t valid;       /* elimit exponents valid */
+  double a2, b2;       /* ipow(x_max, xexp), ipow(y_max, yexp) for elimit */
+} trk_aperture;
+
+/* Index layout of trk_op.d / .i per kind (documented with the producer in
+ * trk_host.cu). */
+/* MULT */
+#define MD_DX 0
+#define MD_DY 1
+#define MD_DZ 2
+#define MD_TC 3   /* cos/sin of TILT (entry rotation) */
+#define MD_TS 4
+#define MD_XC 5   /* cos/sin of -TILT (exit rotation) */
+#define MD_XS 6
+#define MD_LEND 7
+#define MD_APC 8  /* aperture reverse tilt cos/sin */
+#define MD_APS 9
+#define MD_DSH 10 /* 8 drift substep lengths */
+#define MD_KQ 18  /* [step*3 + order] kick strengths, 24 values */
+#define MD_KX 42  /* 8 values -xkick*kickFrac */
+#define MD_KY 50  /* 8 values -ykick*kickFrac */
+#define MD_DRIFT 58 /* drift per slice (nonzero test) */
+#define MD_COEF 59  /* expansion coefficients for orders 0..3 packed: order n at MD_COEF + n*(n+1)/2 */
+/* i: 0 n_parts, 1 nSub, 2 expand, 3 maxOrder, 4 orders (o0 | o1<<8 | o2<<16), 5 skew bits, 6 flags */
+
+/* BEND */
+#define BD_RHO0 0
+#define BD_RHOA 1
+#define BD_SLICE 2   /* s/n */
+#define BD_DSH 3     /* 8 substep drift lengths */
+#define BD_ARG 11    /* 8 values dsh/rho0 */
+#define BD_DS 19     /* 8 kick lengths s*kickFrac */
+#define BD_SA 27     /* 8 sin(dsh/rho0) */
+#define BD_CA 35     /* 8 cos(dsh/rho0) */
+#define BD_SH 43     /* 8 sin(dsh/(2 rho0)) */
+#define BD_CH 51     /* 8 cos(dsh/(2 rho0)) */
+#define BD_DXI 59
+#define BD_DYI 60
+#define BD_DZI 61
+#define BD_CT 62     /* cos/sin total tilt */
+#define BD_ST 63
+#define BD_ET 64     /* dcoord_etilt[0..4] */
+#define BD_DXF 69
+#define BD_DYF 70
+#define BD_DZF 71
+#define BD_APC 72
+#define BD_APS 73
+#define BD_E1 74      /* edge angle, tan, psi, kick limit, h (pole curvature) */
+#define BD_TE1 75
+#define BD_PSI1 76
+#define BD_LIM1 77
+#define BD_HE1 78
+#define BD_E2 79
+#define BD_TE2 80
+#define BD_PSI2 81
+#define BD_LIM2 82
+#define BD_HE2 83
+#define BD_N 84       /* field index n = -b1/h for order-2 edges */
+#define BD_RHOINV 85  /* 1/rho0 (fast build) */
+#define BD_INVRHOA 86 /* 1/rho_actual (fast build) */
+/* i: 0 nSlices, 1 nSub, 2 field mode (0 dipole, 1 normal, 2 skew), 3 expansionOrder1,
+ *    4 field pool offset, 5 edge1 mode, 6 edge2 mode, 7 flags */
+#define EDGE_NONE 0
+#define EDGE_LIN1 1 /* EDGE_EFFECTS=1, EDGE_ORDER<=1 */
+#define EDGE_LIN2 2 /* EDGE_EFFECTS=1, EDGE_ORDER>=2 (apply_edge_effects) */
+#define EDGE_SYMP 3 /* EDGE_EFFECTS=3 */
+
+/* RF */
+#define RD_OMEGA 0
+#define RD_VOLT 1
+#define RD_LEN 2    /* length per kick */
+#define RD_DTL 3
+#define RD_TAU 4
+#define RD_PHASE_ADD 5 /* PHASE*PI/180 */
+#define RD_DX 6
+#define RD_DY 7
+#define RD_HALF 8   /* length/2 */
+#define RD_SOFF 9   /* fiducial sOffset = length/2 */
+#define RD_TREF 10  /* T_REFERENCE or -1 */
+/* i: 0 nKicks, 1 rf state slot, 2 unused, 3 flags */
+
+/* DRIFT */
+#define DD_L 0
+#define DD_T 1  /* L/2 */
+/* i: 0 order */
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,208 @@
+/*
+ * trk.h -- C ABI of the B200 particle-tracking library (libtrkgpu.so).
+ *
+ * The library replaces the per-particle element loops of elegant's
+ * do_tracking() pass loop (src/do_tracking.c:498 pass loop, :829 element loop,
+ * :1352 element switch) for the elements
+ *   DRIF, EDRIFT, KQUAD, KSEXT, KOCT, CSBEND, RFCA, WAKE, TRWAKE, MAXAMP, CHARGE, MARK.
+ * Particles live on the device as an FP64 structure of arrays for a whole run.
+ *
+ * Conventions shared with the reference:
+ *   - a particle is (x [m], x' , y [m], y', s [m], delta = dp/p0, id)
+ *     (src/track.h:82-100, particleIDIndex = 6);
+ *   - a host beam is an array-of-structures of `stride` doubles per particle
+ *     (stride >= 7), the layout of elegant's `double **coord` rows;
+ *   - element parameters are set by the reference's parameter names with the
+ *     reference's defaults (src/track_data.c *_param[] tables);
+ *   - particle loss is not an error: lost particles are reported through
+ *     survivor counts, loss pass and loss element, and their coordinates are
+ *     overwritten as the reference does (coord[4] = loss position,
+ *     coord[5] = P*(1+delta) or gamma, src/multipole.c:1044-1045,
+ *     src/limit_amplitudes.c:279-280, :580-581).
+ *
+ * Every function returns TRK_OK (0) or a negative trk_error code and never
+ * exits the process (the reference aborts through bombElegant(),
+ * src/bombElegant.c:9-18).  trk_last_error() gives a message for the last
+ * failure on the calling thread.
+ *
+ * Thread model: a trk_context is driven by one host thread and owns one CUDA
+ * stream on one device; calls on a context are stream-ordered.
+ */
+#ifndef TRK_H
+#define TRK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TRK_ABI_VERSION 1
+
+/* ---------------------------------------------------------------- errors */
+typedef enum {
+  TRK_OK = 0,
+  TRK_ERR_ARG = -1,          /* bad argument (null pointer, size out of range) */
+  TRK_ERR_UNKNOWN_TYPE = -2, /* element type name not known */
+  TRK_ERR_UNKNOWN_PARAM = -3,/* parameter name not known for that element type */
+  TRK_ERR_UNSUPPORTED = -4,  /* element feature outside the implemented path */
+  TRK_ERR_CUDA = -5,         /* CUDA runtime error (message has the CUDA text) */
+  TRK_ERR_NOMEM = -6,        /* host or device allocation failed */
+  TRK_ERR_DEVICE = -7,       /* a kernel reported an error in the device status word */
+  TRK_ERR_PHYSICS = -8,      /* input the reference rejects (e.g. beam longer than wake) */
+  TRK_ERR_STATE = -9,        /* call out of order (e.g. tracking with no beam loaded) */
+  TRK_ERR_NCCL = -10         /* collective failed */
+} trk_error;
+
+const char *trk_last_error(void);
+int trk_abi_version(void);
+
+/* ---------------------------------------------------------- element types */
+/* Type codes; names are the reference's element names (src/track_data.c:60-).*/
+typedef enum {
+  TRK_MARK = 0,
+  TRK_DRIF = 1,
+  TRK_EDRIFT = 2,
+  TRK_KQUAD = 3,
+  TRK_KSEXT = 4,
+  TRK_KOCT = 5,
+  TRK_CSBEND = 6,
+  TRK_RFCA = 7,
+  TRK_WAKE = 8,
+  TRK_TRWAKE = 9,
+  TRK_MAXAMP = 10,
+  TRK_CHARGE = 11,
+  TRK_N_TYPES = 12
+} trk_type;
+
+/* Type name <-> code ("KQUAD" <-> TRK_KQUAD).  Returns -1 / NULL if unknown. */
+int trk_type_code(const char *name);
+const char *trk_type_name(int type);
+/* Number of parameters of a type and the name / default of parameter i. */
+int trk_param_count(int type);
+const char *trk_param_name(int type, int index);
+double trk_param_default(int type, int index);
+/* Index of a named parameter of a type, or TRK_ERR_UNKNOWN_PARAM. Aliases
+ * (CSBEND N_KICKS == N_SLICES, src/track_data.c:1943-1944) resolve to the
+ * same index. */
+int trk_param_index(int type, const char *name);
+
+/* -------------------------------------------------------------- lattices */
+/* A lattice is an ordered list of elements (one pass of do_tracking's element
+ * loop).  Element parameters are doubles addressed by the reference's names;
+ * integer parameters (N_KICKS, ORDER, ...) are stored as doubles too. */
+typedef struct trk_lattice trk_lattice;
+
+int trk_lattice_create(trk_lattice **lattice);
+void trk_lattice_destroy(trk_lattice *lattice);
+/* Append an element with default parameters; *index receives its position. */
+int trk_lattice_add(trk_lattice *lattice, int type, const char *name, int *index);
+int trk_lattice_set(trk_lattice *lattice, int index, const char *param, double value);
+int trk_lattice_get(const trk_lattice *lattice, int index, const char *param, double *value);
+int trk_lattice_length(const trk_lattice *lattice);
+int trk_lattice_type(const trk_lattice *lattice, int index);
+/* Green-function table of a WAKE (W = longitudinal, Wy ignored) or TRWAKE
+ * (W = Wx, Wy) element: `points` samples at times t[] (seconds, uniform
+ * spacing), in V/C (WAKE) or V/C/m (TRWAKE).  This replaces the INPUTFILE /
+ * TCOLUMN / WCOLUMN SDDS read of set_up_wake (src/wake.c:340-478) and
+ * set_up_trwake (src/trwake.c:325-517).  The arrays are copied. */
+int trk_lattice_set_wake(trk_lattice *lattice, int index, const double *t, const double *W,
+                         const double *Wy, long points);
+/* Parse elegant lattice-file text (the subset "NAME: TYPE, P=V, ..." and
+ * "NAME: LINE=(A, B, 2*C, -D...)"), then expand `line` into the lattice.
+ * Wake tables must be supplied with trk_lattice_set_wake afterwards. */
+int trk_lattice_parse(trk_lattice *lattice, const char *text, const char *line);
+/* Design arc length of one pass (sum of element lengths). */
+double trk_lattice_total_length(const trk_lattice *lattice);
+
+/* ---------------------------------------------------------- run settings */
+typedef struct {
+  double p_central;      /* reference momentum beta*gamma (p_central_mev / me_mev) */
+  long n_passes;         /* passes (turns) to track */
+  long pass_offset;      /* index of the first pass (wake ramps, RF fiducial on pass 0) */
+  int32_t fast_math;     /* 0: reference operation order, no FMA contraction (parity build);
+                            1: transcendental-free CSBEND drift and FMA (fast build) */
+  int32_t block_size;    /* 0 = autotuned */
+  int32_t compact_every; /* compact survivors every N passes in fused runs (0 = never) */
+  int32_t reserved;
+} trk_run;
+
+void trk_run_defaults(trk_run *run);
+
+typedef struct {
+  long n_total;          /* particles loaded */
+  long n_left;           /* survivors after the run */
+  long particle_passes;  /* sum over passes of particles entering the pass (elegant's `effort`) */
+  double device_ms;      /* device time of the tracking kernels (CUDA events) */
+  long kernel_launches;  /* kernels launched by the library during the call */
+  double p_central;      /* reference momentum after the run */
+} trk_stats;
+
+/* ------------------------------------------------------------- contexts */
+typedef struct trk_context trk_context;
+
+/* Create a context on CUDA device `device` (current device if < 0). */
+int trk_context_create(trk_context **ctx, int device);
+void trk_context_destroy(trk_context *ctx);
+/* The CUDA stream (cudaStream_t) all work of the context is ordered on. */
+void *trk_context_stream(trk_context *ctx);
+
+/* Copy a host AoS beam (np particles, `stride` doubles each, stride >= 7,
+ * column 6 = particle id) to the device SoA.  Replaces gpuBaseInit's copy
+ * (src/do_tracking.c:411-414). */
+int trk_beam_load(trk_context *ctx, const double *coord, long np, long stride);
+/* Copy a device SoA beam: 7 columns of `ld` doubles each (x, xp, y, yp, s,
+ * delta, id) starting at d_soa; device-to-device, no host traffic. */
+int trk_beam_load_device(trk_context *ctx, const double *d_soa, long np, long ld);
+/* Copy the beam back to host AoS rows: survivors first (in their original
+ * order), then lost particles (in original order).  Replaces
+ * forceParticlesToCpu (src/do_tracking.c:864 et al.).  n_left receives the
+ * survivor count.  lost_pass / lost_element (optional, np entries, aligned
+ * with the rows written) receive the pass and element index of each loss
+ * (-1 for survivors). */
+int trk_beam_store(trk_context *ctx, double *coord, long stride, long *n_left,
+                   long *lost_pass, int32_t *lost_element);
+/* Device pointers of the SoA columns (x, xp, y, yp, s, delta, id) and the
+ * per-particle loss word; valid until the next trk_beam_load*. */
+int trk_beam_device_columns(trk_context *ctx, double **columns, long *np, int32_t **loss);
+/* Survivor count of the device beam. */
+int trk_beam_count(trk_context *ctx, long *n_left);
+
+/* Track the device beam through n_passes passes of the lattice.
+ * *p_central is read and updated (RFCA CHANGE_P0, WAKE CHANGE_P0). */
+int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, trk_stats *stats);
+
+/* Same, through one element only (index `element` of the lattice), as the
+ * reference's per-element hooks do; `pass` is the pass index and z_start the
+ * arc length at the element entrance.  Survivors are compacted to the front
+ * and *n_left updated, as the hooks' `long` return (src/multipole.c:701). */
+int trk_track_element(trk_context *ctx, const trk_lattice *lattice, int element, long pass,
+                      double z_start, const trk_run *run, long *n_left);
+
+/* ------------------------------------------------------ batched ensembles */
+/* Track `n_variants` lattices that differ only in element parameter values
+ * (error seeds, grids) in one launch.  `lattices` holds n_variants lattices of
+ * identical structure; variant v owns particles [offsets[v], offsets[v+1]) of
+ * the device beam.  Collective elements (WAKE, TRWAKE, RFCA fiducial) are not
+ * allowed in ensembles. */
+int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int n_variants,
+                       const long *offsets, const trk_run *run, trk_stats *stats);
+
+/* ------------------------------------------------------------- gradients */
+/* Reverse-mode adjoint through the fused element chain.  Loss function:
+ *   L = mean_i (x_i^2 + y_i^2) + w_c * (mean_i x_i)^2 + (mean_i y_i)^2 )
+ * over surviving particles after n_passes passes.  Parameters: the K1 of
+ * every KQUAD and the K2 of every KSEXT, in lattice order (grad has
+ * n_kquad + n_ksext entries).  Per-pass checkpoints of the beam are stored
+ * on the device and each pass is recomputed during the reverse sweep.
+ * The device beam is left at its final (forward) state. */
+int trk_adjoint(trk_context *ctx, const trk_lattice *lattice, const trk_run *run,
+                double centroid_weight, double *loss, double *grad, int n_grad);
+/* Number of gradient parameters (KQUAD K1 + KSEXT K2) of a lattice. */
+int trk_adjoint_param_count(const trk_lattice *lattice);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TRK_H */

@@ -1,0 +1,104 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes wrapper of the CPU oracle (liboracle.so).
+
+The oracle restates elegant's element functions and do_tracking loop in C
+(oracle/trk_oracle.c).  Tests, smoke() and bench.py's CPU baseline call it as
+the checker; the product library never does.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+STRIDE = 9
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [("n_left", ctypes.c_long), ("particle_passes", ctypes.c_long), ("p_central", ctypes.c_double)]
+
+
+_lib = None
+
+
+def build():
+    import subprocess
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB):
+        build()
+    lib = ctypes.CDLL(LIB)
+    P, D, L, I = ctypes.c_void_p, ctypes.c_double, ctypes.c_long, ctypes.c_int
+    DP = ctypes.POINTER(ctypes.c_double)
+    lib.trk_last_error.restype = ctypes.c_char_p
+    lib.trk_lattice_create.argtypes = [ctypes.POINTER(P)]
+    lib.trk_lattice_destroy.argtypes = [P]
+    lib.trk_lattice_add.argtypes = [P, I, ctypes.c_char_p, ctypes.POINTER(I)]
+    lib.trk_lattice_set.argtypes = [P, I, ctypes.c_char_p, D]
+    lib.trk_lattice_set_wake.argtypes = [P, I, DP, DP, DP, L]
+    lib.trk_lattice_parse.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p]
+    lib.trk_lattice_length.argtypes = [P]
+    lib.trk_param_index.argtypes = [I, ctypes.c_char_p]
+    lib.orc_track.argtypes = [P, DP, L, L, L, DP, ctypes.POINTER(_Result)]
+    lib.orc_track_element.argtypes = [P, I, DP, L, L, DP, ctypes.POINTER(L)]
+    lib.orc_csbend_field_table.argtypes = [P, I, DP, DP, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)]
+    lib.orc_set_exact_sums.argtypes = [I]
+    _lib = lib
+    return lib
+
+
+def _check(lib, rc):
+    if rc < 0:
+        raise RuntimeError(f"oracle error {rc}: {lib.trk_last_error().decode(errors='replace')}")
+    return rc
+
+
+def set_exact_sums(on):
+    load().orc_set_exact_sums(1 if on else 0)
+
+
+def track(lattice, beam, n_passes, p_central, pass_offset=0):
+    """Track an (np, >=7) beam; returns (rows (np, 9) in the reference's
+    swap order, n_left, particle_passes).  Columns 7, 8 of rows hold the loss
+    pass and element index (-1 for survivors)."""
+    lib = load()
+    nat = lattice.native(lib)
+    rows = np.zeros((beam.shape[0], STRIDE), dtype=np.float64)
+    rows[:, :7] = beam[:, :7]
+    pc = ctypes.c_double(p_central)
+    res = _Result()
+    _check(lib, lib.orc_track(nat.ptr, rows.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), rows.shape[0],
+                              n_passes, pass_offset, ctypes.byref(pc), ctypes.byref(res)))
+    nat.close()
+    return rows, res.n_left, res.particle_passes
+
+
+def track_element(lattice, element, beam, pass_index, p_central):
+    lib = load()
+    nat = lattice.native(lib)
+    rows = np.zeros((beam.shape[0], STRIDE), dtype=np.float64)
+    rows[:, :7] = beam[:, :7]
+    pc = ctypes.c_double(p_central)
+    n_left = ctypes.c_long()
+    _check(lib, lib.orc_track_element(nat.ptr, element, rows.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                      rows.shape[0], pass_index, ctypes.byref(pc), ctypes.byref(n_left)))
+    nat.close()
+    return rows, n_left.value
+
+
+def csbend_field_table(lattice, element):
+    lib = load()
+    nat = lattice.native(lib)
+    Fx = np.zeros(121)
+    Fy = np.zeros(121)
+    eo1, hn, hs = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    _check(lib, lib.orc_csbend_field_table(nat.ptr, element, Fx.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                           Fy.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(eo1),
+                                           ctypes.byref(hn), ctypes.byref(hs)))
+    nat.close()
+    return Fx.reshape(11, 11), Fy.reshape(11, 11), eo1.value, hn.value, hs.value

@@ -1,0 +1,1514 @@
+/*
+ * trk_oracle.c -- TEST INFRASTRUCTURE ONLY: the CPU oracle.
+ *
+ * A plain-C restatement of the reference's element functions for this path
+ * and of the do_tracking() pass/element loop, on array-of-structures rows as
+ * the reference keeps them (lost particles are swapped behind the survivors).
+ * It is the checker for the CUDA path: tests, smoke() and bench.py's CPU
+ * baseline call it; the product library neither links nor calls it.
+ *
+ * Each function cites the reference code it restates (paths relative to the
+ * reference project root).  Compile without FMA contraction
+ * (-ffp-contract=off) so that it rounds like the reference build
+ * (Makefile.rules:218 -O3 -m64, no -march).
+ */
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "trk_lattice.h"
+#include "trk_oracle.h"
+#include "trk_oracle_core.h"
+
+#define SIGN(x) ((x) < 0 ? -1 : 1)
+
+static void swap_rows(double *a, double *b) {
+  double t[ORC_STRIDE];
+  memcpy(t, a, sizeof(t));
+  memcpy(a, b, sizeof(t));
+  memcpy(b, t, sizeof(t));
+}
+#define ROW(i) (coord + (size_t)(i) * ORC_STRIDE)
+
+/* ------------------------------------------------------------ MAXAMP state */
+typedef struct {
+  int seen;          /* a MAXAMP has been passed (maxamp != NULL) */
+  double x_max, y_max;
+  int elliptical;
+  long exponent, yExponent;
+} orc_maxamp;
+
+static void maxamp_update(orc_maxamp *st, const trk_elem *e) {
+  st->seen = 1;
+  st->x_max = TRK_P(e, MAXAMP_X_MAX);
+  st->y_max = TRK_P(e, MAXAMP_Y_MAX);
+  st->elliptical = (int)TRK_P(e, MAXAMP_ELLIPTICAL);
+  st->exponent = (long)TRK_P(e, MAXAMP_EXPONENT);
+  st->yExponent = (long)TRK_P(e, MAXAMP_YEXPONENT);
+}
+
+/* setupMultApertureData (src/multipole.c:1690-1749) */
+static void setup_aperture(orc_aperture *ap, double reverseTilt, const orc_maxamp *st) {
+  memset(ap, 0, sizeof(*ap));
+  ap->reverseTilt = reverseTilt;
+  ap->reverseTiltC = cos(reverseTilt);
+  ap->reverseTiltS = sin(reverseTilt);
+  if (st->seen) {
+    ap->xMax = st->x_max;
+    ap->yMax = st->y_max;
+    ap->elliptical = st->elliptical;
+    ap->xExponent = ap->yExponent = st->exponent;
+    if (st->yExponent)
+      ap->yExponent = st->yExponent;
+  }
+}
+
+/* ---------------------------------------------------- loss filters */
+/* limit_amplitudes (src/limit_amplitudes.c:197-288), no open sides */
+static long limit_amplitudes(double *coord, double xmax, double ymax, long np, double z, double Po,
+                             int extrapolate_z) {
+  long ip, itop, is_out;
+  double *part, dz, dzx, dzy;
+  if (xmax < 0 && ymax < 0)
+    return np;
+  itop = np - 1;
+  for (ip = 0; ip < np; ip++) {
+    part = ROW(ip);
+    is_out = 0;
+    if (xmax > 0 && fabs(part[0]) > xmax)
+      is_out += 1;
+    if (ymax > 0 && fabs(part[2]) > ymax)
+      is_out += 2;
+    if (isinf(part[0]) || isinf(part[2]) || isnan(part[0]) || isnan(part[2]))
+      is_out += 4;
+    dz = 0;
+    if (is_out && !(is_out & 4) && extrapolate_z) {
+      dzx = dzy = -DBL_MAX;
+      if (is_out & 1 && part[1] != 0)
+        dzx = (part[0] - SIGN(part[1]) * xmax) / part[1];
+      if (is_out & 2 && part[3] != 0)
+        dzy = (part[2] - SIGN(part[3]) * ymax) / part[3];
+      if (dzx > dzy)
+        dz = -dzx;
+      else
+        dz = -dzy;
+      if (dz == -DBL_MAX)
+        dz = 0;
+    }
+    if (is_out) {
+      if (ip != itop)
+        swap_rows(ROW(ip), ROW(itop));
+      ROW(itop)[0] += dz * ROW(itop)[1];
+      ROW(itop)[2] += dz * ROW(itop)[3];
+      ROW(itop)[4] = z + dz;
+      ROW(itop)[5] = Po * (1 + ROW(itop)[5]);
+      --itop;
+      --ip;
+      np--;
+    }
+  }
+  return np;
+}
+
+/* elimit_amplitudes (src/limit_amplitudes.c:487-~620), no open sides */
+static long elimit_amplitudes(double *coord, double xmax, double ymax, long np, double z, double Po,
+                              int extrapolate_z, long exponent, long yexponent, int *err) {
+  long ip, itop, xe, ye;
+  double *part, a2, b2, c0, c1, c2, dz, det;
+  if ((xe = exponent) < 2 || xe % 2) {
+    *err = 1;
+    return np;
+  }
+  ye = xe;
+  if (yexponent) {
+    if ((ye = yexponent) < 2 || ye % 2) {
+      *err = 1;
+      return np;
+    }
+  }
+  if (xmax <= 0 || ymax <= 0) {
+    if (xmax > 0 || ymax > 0)
+      return limit_amplitudes(coord, xmax, ymax, np, z, Po, extrapolate_z);
+    return np;
+  }
+  a2 = orc_ipow(xmax, xe);
+  b2 = orc_ipow(ymax, ye);
+  itop = np - 1;
+  for (ip = 0; ip < np; ip++) {
+    part = ROW(ip);
+    if (isinf(part[0]) || isinf(part[2]) || isnan(part[0]) || isnan(part[2])) {
+      swap_rows(ROW(ip), ROW(itop));
+      ROW(itop)[4] = z;
+      ROW(itop)[5] = sqrt(orc_sqr(Po * (1 + ROW(itop)[5])) + 1);
+      --itop;
+      --ip;
+      np--;
+      continue;
+    }
+    if ((orc_ipow(part[0], xe) / a2 + orc_ipow(part[2], ye) / b2) > 1) {
+      dz = 0;
+      if (extrapolate_z && xe == 2 && ye == 2) {
+        c0 = orc_sqr(part[0]) / a2 + orc_sqr(part[2]) / b2 - 1;
+        c1 = 2 * (part[0] * part[1] / a2 + part[2] * part[3] / b2);
+        c2 = orc_sqr(part[1]) / a2 + orc_sqr(part[3]) / b2;
+        det = orc_sqr(c1) - 4 * c0 * c2;
+        if (z > 0 && c2 && det >= 0) {
+          if ((dz = (-c1 + sqrt(det)) / (2 * c2)) > 0)
+            dz = (-c1 - sqrt(det)) / (2 * c2);
+          if ((z + dz) < 0)
+            dz = -z;
+          part[0] += dz * part[1];
+          part[2] += dz * part[3];
+        }
+      }
+      swap_rows(ROW(ip), ROW(itop));
+      ROW(itop)[4] = z + dz;
+      ROW(itop)[5] = sqrt(orc_sqr(Po * (1 + ROW(itop)[5])) + 1);
+      --itop;
+      --ip;
+      np--;
+    }
+  }
+  return np;
+}
+
+/* removeInvalidParticles (src/limit_amplitudes.c:~290-345) */
+static long remove_invalid(double *coord, long np, double z, double Po) {
+  long ip, itop = np - 1;
+  for (ip = 0; ip < np; ip++) {
+    double *part = ROW(ip);
+    int is_out = 0;
+    for (int ic = 0; ic < 6; ic++)
+      if (isnan(part[ic])) {
+        is_out = 1;
+        break;
+      }
+    if (part[5] <= -1)
+      is_out = 1;
+    if (is_out) {
+      swap_rows(ROW(ip), ROW(itop));
+      ROW(itop)[4] = z;
+      ROW(itop)[5] = Po * (1 + ROW(itop)[5]);
+      --itop;
+      --ip;
+      np--;
+    }
+  }
+  return np;
+}
+
+/* ------------------------------------------------------- simple maps */
+/* DRIF: drift_matrix (src/compute_matrices.c:391-413) tracked by
+ * track_particles (src/matrix.c:212-469) with TURBO_FASTMATTRACK=3, i.e.
+ * fin[i] = C[i] + sum_{j=5..0} (R[i][j] + sum_{k=j..0} T[i][j][k] ini[k]) ini[j]
+ * over the full 6x6 / 6x21 arrays, zeros included. */
+static void drift_matrix_track(double *coord, long np, double L, long order) {
+  double C[6] = {0}, R[6][6] = {{0}}, T[6][6][6] = {{{0}}};
+  if (order == 0)
+    order = 2; /* run->default_order (src/elegant.nl:43) */
+  if (order > 2)
+    order = 2;
+  C[4] = L;
+  R[0][0] = R[1][1] = R[2][2] = R[3][3] = R[4][4] = R[5][5] = 1;
+  R[0][1] = R[2][3] = L;
+  if (order > 1)
+    T[4][1][1] = T[4][3][3] = L / 2;
+  for (long ip = 0; ip < np; ip++) {
+    double *ini = ROW(ip), temp[6];
+    for (int i = 5; i >= 0; i--) {
+      double sum = C[i];
+      if (order == 2) {
+        for (int j = 5; j >= 0; j--) {
+          double sum1 = R[i][j];
+          for (int k = j; k >= 0; k--)
+            sum1 += T[i][j][k] * ini[k];
+          sum += sum1 * ini[j];
+        }
+      } else {
+        for (int j = 5; j >= 0; j--)
+          sum += R[i][j] * ini[j];
+      }
+      temp[i] = sum;
+    }
+    for (int i = 5; i >= 0; i--)
+      ini[i] = temp[i];
+  }
+}
+
+/* exactDrift (src/csbend.c:3792-3816) */
+static void exact_drift(double *coord, long np, double L) {
+  for (long i = 0; i < np; i++) {
+    double *c = ROW(i);
+    c[0] += c[1] * L;
+    c[2] += c[3] * L;
+    c[4] += L * sqrt(1 + orc_sqr(c[1]) + orc_sqr(c[3]));
+  }
+}
+
+/* offsetBeamCoordinatesForMisalignment (src/malign_mat.c:257-267) */
+static void offset_beam(double *coord, long np, double dx, double dy, double dz) {
+  for (long ip = np - 1; ip >= 0; ip--) {
+    double *part = ROW(ip);
+    part[4] += dz * sqrt(1 + orc_sqr(part[1]) + orc_sqr(part[3]));
+    part[0] = part[0] - dx + dz * part[1];
+    part[2] = part[2] - dy + dz * part[3];
+  }
+}
+
+/* rotateBeamCoordinatesForMisalignment (src/tilt_matrices.c:156-190) */
+static void rotate_beam(double *coord, long np, double angle) {
+  double sin_a, cos_a;
+  if (!angle || fabs(fabs(angle) - TRK_PIx2) < 1e-12)
+    return;
+  if (fabs(fabs(angle) - TRK_PI) < 1e-12) {
+    cos_a = -1;
+    sin_a = 0;
+  } else if (fabs(angle - TRK_PIo2) < 1e-12) {
+    cos_a = 0;
+    sin_a = 1;
+  } else if (fabs(angle + TRK_PIo2) < 1e-12) {
+    cos_a = 0;
+    sin_a = -1;
+  } else {
+    cos_a = cos(angle);
+    sin_a = sin(angle);
+  }
+  for (long i = 0; i < np; i++) {
+    double *c = ROW(i);
+    double x = c[0], xp = c[1], y = c[2], yp = c[3];
+    c[0] = x * cos_a + y * sin_a;
+    c[2] = -x * sin_a + y * cos_a;
+    c[1] = xp * cos_a + yp * sin_a;
+    c[3] = -xp * sin_a + yp * cos_a;
+  }
+}
+
+/* ------------------------------------------------------------ multipoles */
+/* multipole_tracking2 (src/multipole.c:660-1084) for KQUAD, KSEXT, KOCT,
+ * MALIGN_METHOD=0, no radiation, no fringe, no error multipoles. */
+static long multipole_tracking2(double *coord, long n_part, const trk_elem *e, double Po, double z_start,
+                                const orc_maxamp *st, int *err) {
+  orc_mult m;
+  double tilt = 0, dx = 0, dy = 0, dz = 0, lEnd = 0, lEffective;
+  long n_kicks = 0, nSlices = 0;
+  int doEndDrift = 0;
+  double cfac = TRK_E_MKS / (TRK_ME_MKS * TRK_C_MKS * Po);
+  memset(&m, 0, sizeof(m));
+  switch (e->type) {
+  case TRK_KQUAD:
+    nSlices = (long)TRK_P(e, KQUAD_N_SLICES);
+    n_kicks = (long)TRK_P(e, KQUAD_N_KICKS);
+    m.expand = (int)TRK_P(e, KQUAD_EXPAND_HAMILTONIAN);
+    m.order[0] = 1;
+    if ((lEffective = TRK_P(e, KQUAD_LEFFECTIVE)) <= 0)
+      lEffective = TRK_P(e, KQUAD_L);
+    else {
+      lEnd = (TRK_P(e, KQUAD_L) - lEffective) / 2;
+      doEndDrift = 1;
+    }
+    if (TRK_P(e, KQUAD_BORE))
+      m.KnL[0] = TRK_P(e, KQUAD_B) / TRK_P(e, KQUAD_BORE) * cfac * lEffective * (1 + TRK_P(e, KQUAD_FSE));
+    else
+      m.KnL[0] = TRK_P(e, KQUAD_K1) * lEffective * (1 + TRK_P(e, KQUAD_FSE));
+    m.drift = lEffective;
+    tilt = TRK_P(e, KQUAD_TILT);
+    dx = TRK_P(e, KQUAD_DX);
+    dy = TRK_P(e, KQUAD_DY);
+    dz = TRK_P(e, KQUAD_DZ);
+    m.xkick = TRK_P(e, KQUAD_HKICK) * TRK_P(e, KQUAD_HCALIBRATION);
+    m.ykick = TRK_P(e, KQUAD_VKICK) * TRK_P(e, KQUAD_VCALIBRATION);
+    m.integ_order = (int)TRK_P(e, KQUAD_INTEGRATION_ORDER);
+    break;
+  case TRK_KSEXT:
+    n_kicks = (long)TRK_P(e, KSEXT_N_KICKS);
+    nSlices = (long)TRK_P(e, KSEXT_N_SLICES);
+    m.expand = (int)TRK_P(e, KSEXT_EXPAND_HAMILTONIAN);
+    m.order[0] = 2;
+    if (TRK_P(e, KSEXT_BORE))
+      m.KnL[0] = 2 * TRK_P(e, KSEXT_B) / orc_sqr(TRK_P(e, KSEXT_BORE)) * cfac * TRK_P(e, KSEXT_L) *
+                 (1 + TRK_P(e, KSEXT_FSE));
+    else
+      m.KnL[0] = TRK_P(e, KSEXT_K2) * TRK_P(e, KSEXT_L) * (1 + TRK_P(e, KSEXT_FSE));
+    m.drift = lEffective = TRK_P(e, KSEXT_L);
+    tilt = TRK_P(e, KSEXT_TILT);
+    dx = TRK_P(e, KSEXT_DX);
+    dy = TRK_P(e, KSEXT_DY);
+    dz = TRK_P(e, KSEXT_DZ);
+    m.xkick = TRK_P(e, KSEXT_HKICK) * TRK_P(e, KSEXT_HCALIBRATION);
+    m.ykick = TRK_P(e, KSEXT_VKICK) * TRK_P(e, KSEXT_VCALIBRATION);
+    m.integ_order = (int)TRK_P(e, KSEXT_INTEGRATION_ORDER);
+    if (TRK_P(e, KSEXT_K1)) {
+      m.KnL[1] = TRK_P(e, KSEXT_K1) * TRK_P(e, KSEXT_L);
+      m.order[1] = 1;
+    }
+    if (TRK_P(e, KSEXT_J1)) {
+      m.KnL[2] = TRK_P(e, KSEXT_J1) * TRK_P(e, KSEXT_L);
+      m.order[2] = 1;
+      m.skew[2] = 1;
+    }
+    break;
+  case TRK_KOCT:
+    n_kicks = (long)TRK_P(e, KOCT_N_KICKS);
+    nSlices = (long)TRK_P(e, KOCT_N_SLICES);
+    m.expand = (int)TRK_P(e, KOCT_EXPAND_HAMILTONIAN);
+    m.order[0] = 3;
+    if (TRK_P(e, KOCT_BORE))
+      m.KnL[0] = 6 * TRK_P(e, KOCT_B) / orc_ipow(TRK_P(e, KOCT_BORE), 3) * cfac * TRK_P(e, KOCT_L) *
+                 (1 + TRK_P(e, KOCT_FSE));
+    else
+      m.KnL[0] = TRK_P(e, KOCT_K3) * TRK_P(e, KOCT_L) * (1 + TRK_P(e, KOCT_FSE));
+    m.drift = lEffective = TRK_P(e, KOCT_L);
+    tilt = TRK_P(e, KOCT_TILT);
+    dx = TRK_P(e, KOCT_DX);
+    dy = TRK_P(e, KOCT_DY);
+    dz = TRK_P(e, KOCT_DZ);
+    m.integ_order = (int)TRK_P(e, KOCT_INTEGRATION_ORDER);
+    break;
+  default:
+    *err = 1;
+    return n_part;
+  }
+  (void)lEffective;
+  if (m.integ_order != 2 && m.integ_order != 4 && m.integ_order != 6) {
+    *err = 1;
+    return n_part;
+  }
+  if (n_kicks <= 0) {
+    if (nSlices <= 0) {
+      *err = 1;
+      return n_part;
+    }
+  } else {
+    if (m.integ_order > 2) {
+      if ((nSlices = (long)ceil(n_kicks / (1.0 * m.integ_order))) < 1)
+        nSlices = 1;
+    } else
+      nSlices = n_kicks;
+  }
+  m.nSlices = (int)nSlices;
+  m.maxOrder = m.order[0] > m.order[1] ? m.order[0] : m.order[1];
+  if (m.order[2] > m.maxOrder)
+    m.maxOrder = m.order[2];
+  m.dx = dx;
+  m.dy = dy;
+
+  orc_aperture ap;
+  setup_aperture(&ap, -tilt, st);
+
+  /* offsetParticlesForMisalignment, mode 0 entry (src/malign_mat.c:578-584) */
+  if (dx || dy || dz)
+    offset_beam(coord, n_part, dx, dy, dz);
+  if (tilt)
+    rotate_beam(coord, n_part, tilt);
+  if (doEndDrift)
+    exact_drift(coord, n_part, lEnd);
+
+  long i_top = n_part - 1;
+  for (long i_part = 0; i_part <= i_top; i_part++) {
+    double dzLoss = 0;
+    if (!orc_integrate_kick_multipole(ROW(i_part), &m, Po, &ap, &dzLoss)) {
+      swap_rows(ROW(i_part), ROW(i_top));
+      ROW(i_top)[4] = z_start + dzLoss;
+      ROW(i_top)[5] = Po * (1 + ROW(i_top)[5]);
+      i_top--;
+      i_part--;
+    }
+  }
+  if (doEndDrift)
+    exact_drift(coord, n_part, lEnd);
+  if (dx || dy || dz || tilt) {
+    if (tilt)
+      rotate_beam(coord, n_part, -tilt);
+    if (dx || dy || dz)
+      offset_beam(coord, n_part, -dx, -dy, -dz);
+  }
+  return i_top + 1;
+}
+
+/* ------------------------------------------------------------- CSBEND */
+/* Field-expansion coefficients of a curved multipole magnet.  The
+ * reference evaluates closed forms (computeCSBENDFieldCoefficients,
+ * src/csbend.c:175-~650); here the same coefficients come from the recursion
+ * that Laplace's equation imposes in the curvilinear frame with curvature h:
+ *   curl:  (i+1) a[i+1][j] = (j+1) c[i][j+1]
+ *   div :  (i+1) (c[i+1][j] + h c[i][j]) + (j+1) (a[i][j+1] + h a[i-1][j+1]) = 0
+ * where a[i][j], c[i][j] are the coefficients of x^i y^j in Fy and Fx, and the
+ * mid-plane data are a[i][0] = b_i / i!, c[i][0] = -c_i / i! (i = 1..8).  The
+ * dipole / steering terms enter only [0][0], as in the reference. */
+static void csbend_field_table(orc_bend *bd, const double *b, const double *c, double h, int nonlinear,
+                               long expansionOrder) {
+  double a[12][12], cx[12][12];
+  int i, j;
+  if (expansionOrder == 0) {
+    for (i = 8; i >= 0; i--)
+      if (b[i] || c[i])
+        break;
+    if ((expansionOrder = i + 2) < 4)
+      expansionOrder = 4;
+  }
+  bd->expansionOrder1 = (int)expansionOrder + 1;
+  bd->hasNormal = bd->hasSkew = 0;
+  for (i = 0; i < 9; i++) {
+    if (b[i])
+      bd->hasNormal = 1;
+    if (c[i])
+      bd->hasSkew = 1;
+  }
+  memset(a, 0, sizeof(a));
+  memset(cx, 0, sizeof(cx));
+  double fact = 1;
+  for (i = 1; i <= 8; i++) {
+    fact *= i;
+    a[i][0] = b[i] / fact;
+    cx[i][0] = -c[i] / fact;
+  }
+  for (j = 0; j < 10; j++) {
+    for (i = 0; i + j + 1 <= 10; i++)
+      cx[i][j + 1] = (i + 1) * a[i + 1][j] / (j + 1);
+    for (i = 0; i + j + 1 <= 10; i++) {
+      double prev = i > 0 ? a[i - 1][j + 1] : 0.0;
+      a[i][j + 1] = -h * prev - (i + 1) * (cx[i + 1][j] + h * cx[i][j]) / (j + 1);
+    }
+  }
+  memset(bd->Fx_xy, 0, sizeof(bd->Fx_xy));
+  memset(bd->Fy_xy, 0, sizeof(bd->Fy_xy));
+  if (nonlinear) {
+    for (i = 0; i <= 10; i++)
+      for (j = 0; i + j <= 10; j++) {
+        bd->Fx_xy[i][j] = cx[i][j];
+        bd->Fy_xy[i][j] = a[i][j];
+      }
+  } else {
+    bd->Fx_xy[0][1] = cx[0][1];
+    bd->Fy_xy[1][0] = a[1][0];
+    bd->Fy_xy[0][1] = a[0][1];
+    bd->Fx_xy[1][0] = cx[1][0];
+  }
+  bd->Fx_xy[0][0] = c[0];
+  bd->Fy_xy[0][0] = 1 - b[0];
+}
+
+typedef struct {
+  orc_bend bd;
+  double angle, e1, e2, tilt, etilt, rho0, h, n, fse, rho_actual;
+  double psi1, psi2, e1_kick_limit, e2_kick_limit, he1, he2;
+  double cos_ttilt, sin_ttilt, dcoord_etilt[6];
+  double dxi, dyi, dzi, dxf, dyf, dzf;
+  int edge1, edge2, edge_order, edge1_effects, edge2_effects;
+  int is_drift;
+} orc_csbend_setup;
+
+/* computeEtiltCentroidOffset (src/csbend.c:4748-4790) */
+static void etilt_centroid_offset(double *d, double rho0, double angle, double etilt) {
+  double q1a, q2a, q3a, q1b, q2b, q3b, qp1, qp2, qp3, dz, tan_alpha, k;
+  if (!etilt) {
+    for (int i = 0; i < 6; i++)
+      d[i] = 0;
+    return;
+  }
+  etilt *= -1;
+  q1a = (1 - cos(angle)) * rho0 * (cos(etilt) - 1);
+  q2a = 0;
+  q3a = (1 - cos(angle)) * rho0 * sin(etilt);
+  qp1 = sin(angle) * cos(etilt);
+  qp2 = cos(angle);
+  k = sqrt(orc_sqr(qp1) + orc_sqr(qp2));
+  qp1 /= k;
+  qp2 /= k;
+  qp3 = sin(angle) * sin(etilt) / k;
+  tan_alpha = 1. / tan(angle) / cos(etilt);
+  q1b = q1a * tan_alpha / (tan(angle) + tan_alpha);
+  q2b = -q1b * tan(angle);
+  dz = sqrt(orc_sqr(q1b - q1a) + orc_sqr(q2b - q2a));
+  q3b = q3a + qp3 * dz;
+  d[0] = sqrt(orc_sqr(q1b) + orc_sqr(q2b));
+  d[1] = tan(atan(tan_alpha) - (TRK_PIo2 - angle));
+  d[2] = q3b;
+  d[3] = qp3;
+  d[4] = dz * sqrt(1 + orc_sqr(qp3));
+  d[5] = 0;
+}
+
+/* determine_bend_flags (src/bend_matrix.c:1347-1394): an edge is active
+ * unless a same-named CSBEND is adjacent (through MARKs). */
+static void bend_edge_flags(const trk_lattice *l, int idx, int *edge1, int *edge2) {
+  const trk_elem *e = &l->e[idx];
+  int precedes = 0, follows = 0;
+  for (int k = idx - 1; k >= 0; k--) {
+    if (l->e[k].type == e->type && strcmp(l->e[k].name, e->name) == 0) {
+      precedes = 1;
+      break;
+    }
+    if (l->e[k].type != TRK_MARK)
+      break;
+  }
+  for (int k = idx + 1; k < l->n; k++) {
+    if (l->e[k].type == e->type && strcmp(l->e[k].name, e->name) == 0) {
+      follows = 1;
+      break;
+    }
+    if (l->e[k].type != TRK_MARK)
+      break;
+  }
+  *edge1 = TRK_P(e, CSBEND_EDGE1_EFFECTS) && !precedes;
+  *edge2 = TRK_P(e, CSBEND_EDGE2_EFFECTS) && !follows;
+}
+
+/* Per-call set-up of track_through_csbend (src/csbend.c:654-1078) */
+static int csbend_setup(const trk_lattice *l, int idx, double Po, orc_csbend_setup *S) {
+  const trk_elem *e = &l->e[idx];
+  double b[9], c[9];
+  memset(S, 0, sizeof(*S));
+  if (TRK_P(e, CSBEND_SYNCH_RAD) || TRK_P(e, CSBEND_ISR) || TRK_P(e, CSBEND_REFERENCE_CORRECTION) ||
+      TRK_P(e, CSBEND_FSE_CORRECTION) || TRK_P(e, CSBEND_MALIGN_METHOD) || TRK_P(e, CSBEND_EXPAND_HAMILTONIAN))
+    return 1;
+  if (TRK_P(e, CSBEND_ANGLE) == 0) {
+    S->is_drift = 1;
+    return 0;
+  }
+  int io = (int)TRK_P(e, CSBEND_INTEGRATION_ORDER);
+  if (io != 2 && io != 4 && io != 6)
+    return 1;
+  double L = TRK_P(e, CSBEND_L), ANGLE = TRK_P(e, CSBEND_ANGLE);
+  double rho0 = L / ANGLE;
+  b[0] = 0;
+  if (TRK_P(e, CSBEND_USE_BN)) {
+    for (int i = 1; i <= 8; i++)
+      b[i] = e->p[P_CSBEND_B1 + i - 1];
+  } else {
+    for (int i = 1; i <= 8; i++)
+      b[i] = e->p[P_CSBEND_K1 + i - 1] * rho0;
+  }
+  for (int j = 0; j < 9; j++)
+    c[j] = 0;
+  double fse_ = TRK_P(e, CSBEND_FSE), fseD = TRK_P(e, CSBEND_FSE_DIPOLE), fseQ = TRK_P(e, CSBEND_FSE_QUADRUPOLE);
+  b[1] *= (1 + fse_ + fseQ) / (1 + fse_ + fseD);
+  c[1] *= (1 + fse_ + fseQ) / (1 + fse_ + fseD);
+  b[2] *= (1 + fse_) / (1 + fse_ + fseD);
+  c[2] *= (1 + fse_) / (1 + fse_ + fseD);
+  b[0] = TRK_P(e, CSBEND_XKICK) / ANGLE;
+  c[0] = TRK_P(e, CSBEND_YKICK) / ANGLE;
+  S->he1 = TRK_P(e, CSBEND_H1);
+  S->he2 = TRK_P(e, CSBEND_H2);
+  if (ANGLE < 0) {
+    S->angle = -ANGLE;
+    S->e1 = -TRK_P(e, CSBEND_E1);
+    S->e2 = -TRK_P(e, CSBEND_E2);
+    S->etilt = TRK_P(e, CSBEND_ETILT) * TRK_P(e, CSBEND_ETILT_SIGN);
+    S->tilt = TRK_P(e, CSBEND_TILT) + TRK_PI;
+    rho0 = L / S->angle;
+    for (int i = 1; i < 9; i += 2) {
+      b[i] *= -1;
+      c[i] *= -1;
+    }
+  } else {
+    S->angle = ANGLE;
+    S->e1 = TRK_P(e, CSBEND_E1);
+    S->e2 = TRK_P(e, CSBEND_E2);
+    S->etilt = TRK_P(e, CSBEND_ETILT) * TRK_P(e, CSBEND_ETILT_SIGN);
+    S->tilt = TRK_P(e, CSBEND_TILT);
+    rho0 = L / S->angle;
+  }
+  if (fabs(rho0) > 1e6) {
+    if (TRK_P(e, CSBEND_K1) != 0 || TRK_P(e, CSBEND_K2) != 0)
+      return 1; /* treated as KQUAD by the reference; not on this path */
+    S->is_drift = 1;
+    return 0;
+  }
+  S->rho0 = rho0;
+  S->fse = fse_ + fseD;
+  S->h = 1 / rho0;
+  S->n = -b[1] / S->h;
+  if (fabs(S->fse + 1) < 1e-12)
+    S->fse = -1 + 1e-12;
+  S->rho_actual = 1 / ((1 + S->fse) * S->h);
+  S->e1_kick_limit = TRK_P(e, CSBEND_EDGE1_KICK_LIMIT);
+  S->e2_kick_limit = TRK_P(e, CSBEND_EDGE2_KICK_LIMIT);
+  if (TRK_P(e, CSBEND_KICK_LIMIT_SCALING)) {
+    S->e1_kick_limit *= rho0 / S->rho_actual;
+    S->e2_kick_limit *= rho0 / S->rho_actual;
+  }
+  double hgap = TRK_P(e, CSBEND_HGAP);
+  double fint1 = TRK_P(e, CSBEND_FINT1) >= 0 ? TRK_P(e, CSBEND_FINT1) : TRK_P(e, CSBEND_FINT);
+  double fint2 = TRK_P(e, CSBEND_FINT2) >= 0 ? TRK_P(e, CSBEND_FINT2) : TRK_P(e, CSBEND_FINT);
+  double Kg1 = 2 * hgap * fint1 * SIGN(rho0);
+  S->psi1 = Kg1 / fabs(S->rho_actual) / cos(S->e1) * (1 + orc_sqr(sin(S->e1)));
+  double Kg2 = 2 * hgap * fint2 * SIGN(rho0);
+  S->psi2 = Kg2 / fabs(S->rho_actual) / cos(S->e2) * (1 + orc_sqr(sin(S->e2)));
+  if (L < 0) {
+    S->psi1 *= -1;
+    S->psi2 *= -1;
+  }
+  S->bd.rho0 = rho0;
+  S->bd.rho_actual = S->rho_actual;
+  S->bd.length = L;
+  S->bd.nSlices = (int)TRK_P(e, CSBEND_N_SLICES);
+  if (S->bd.nSlices < 1)
+    return 1;
+  S->bd.integ_order = io;
+  /* isrConstant is nonzero (negative) whenever Po>0 even with ISR=0
+   * (src/csbend.c:931-934), which enables the (1+DPoP) round trip */
+  S->bd.isr_or_rad = Po > 0;
+  csbend_field_table(&S->bd, b, c, S->h, (int)TRK_P(e, CSBEND_NONLINEAR), (long)TRK_P(e, CSBEND_EXPANSION_ORDER));
+
+  double ttilt = S->tilt + S->etilt;
+  if (ttilt == 0) {
+    S->cos_ttilt = 1;
+    S->sin_ttilt = 0;
+  } else if (fabs(fabs(ttilt) - TRK_PI) < 1e-12) {
+    S->cos_ttilt = -1;
+    S->sin_ttilt = 0;
+  } else if (fabs(ttilt - TRK_PIo2) < 1e-12) {
+    S->cos_ttilt = 0;
+    S->sin_ttilt = 1;
+  } else if (fabs(ttilt + TRK_PIo2) < 1e-12) {
+    S->cos_ttilt = 0;
+    S->sin_ttilt = -1;
+  } else {
+    S->cos_ttilt = cos(ttilt);
+    S->sin_ttilt = sin(ttilt);
+  }
+  etilt_centroid_offset(S->dcoord_etilt, rho0, S->angle, S->etilt);
+  double dx = TRK_P(e, CSBEND_DX), dy = TRK_P(e, CSBEND_DY), dz = TRK_P(e, CSBEND_DZ);
+  S->dxi = -dx;
+  S->dzi = dz;
+  S->dyi = -dy;
+  S->dxf = dx * cos(ANGLE) + dz * sin(ANGLE);
+  S->dzf = dx * sin(ANGLE) - dz * cos(ANGLE);
+  S->dyf = dy;
+  bend_edge_flags(l, idx, &S->edge1, &S->edge2);
+  S->edge_order = (int)TRK_P(e, CSBEND_EDGE_ORDER);
+  S->edge1_effects = (int)TRK_P(e, CSBEND_EDGE1_EFFECTS);
+  S->edge2_effects = (int)TRK_P(e, CSBEND_EDGE2_EFFECTS);
+  for (int k = 0; k < 2; k++) {
+    int eff = k ? S->edge2_effects : S->edge1_effects;
+    int on = k ? S->edge2 : S->edge1;
+    if (on && eff != 0 && eff != 1 && eff != 3)
+      return 1;
+  }
+  return 0;
+}
+
+/* apply_edge_effects (src/csbend.c:4291-4333) */
+static void apply_edge_effects(double *x, double *xp, double *y, double *yp, double rho, double n, double beta,
+                               double he, double psi, long which_edge) {
+  double h, tan_beta, tan2_beta, sec_beta, sec2_beta, h2;
+  double R21, R43, T111, T133, T211, T441, T331, T221, T233, T243, T431, T432;
+  double x0, xp0, y0, yp0;
+  h = 1 / rho;
+  R21 = h * (tan_beta = tan(beta));
+  R43 = -h * tan(beta - psi);
+  h2 = orc_sqr(h);
+  T111 = which_edge * h / 2 * (tan2_beta = orc_sqr(tan_beta));
+  sec_beta = 1. / cos(beta);
+  sec2_beta = orc_sqr(sec_beta);
+  T133 = -which_edge * h / 2 * sec2_beta;
+  T211 = which_edge == -1 ? -n * h2 * tan_beta : -h2 * (n + tan2_beta / 2) * tan_beta;
+  T441 = -(T331 = T221 = -which_edge * h * tan2_beta);
+  T233 = which_edge == -1 ? h2 * (n + .5 + tan2_beta) * tan_beta : h2 * (n - tan2_beta / 2) * tan_beta;
+  T243 = which_edge * h * tan2_beta;
+  T431 = h2 * (2 * n + (which_edge == 1 ? sec2_beta : 0)) * tan_beta;
+  T432 = which_edge * h * sec2_beta;
+  if (he != 0) {
+    double term = h / 2 * he * sec2_beta * sec_beta;
+    T211 += term;
+    T233 -= term;
+    T431 -= 2 * term;
+  }
+  x0 = *x;
+  xp0 = *xp;
+  y0 = *y;
+  yp0 = *yp;
+  *x = x0 + T111 * orc_sqr(x0) + T133 * orc_sqr(y0);
+  *xp = xp0 + R21 * x0 + T211 * orc_sqr(x0) + T221 * x0 * xp0 + T233 * orc_sqr(y0) + T243 * y0 * yp0;
+  *y = y0 + T331 * x0 * y0;
+  *yp = yp0 + R43 * y0 + T441 * yp0 * x0 + T431 * x0 * y0 + T432 * xp0 * y0;
+}
+
+/* applySimpleDipoleEdgeKick (src/csbend.c:5664-5690), non-expanded */
+static void simple_dipole_edge_kick(double *xp, double *yp, double x, double y, double delta, double rho,
+                                    double ea, double psi, double kickLimit) {
+  double Qi[6] = {x, *xp, y, *yp, 0, delta};
+  double dqx, dqy;
+  orc_to_dipole_canonical(Qi);
+  dqx = tan(ea) / rho * x;
+  if (kickLimit > 0 && fabs(dqx) > kickLimit)
+    dqx = SIGN(dqx) * kickLimit;
+  dqy = -tan(ea - psi / (1 + delta)) / rho * y;
+  Qi[1] += dqx;
+  Qi[3] += dqy;
+  orc_from_dipole_canonical(Qi);
+  *xp = Qi[1];
+  *yp = Qi[3];
+}
+
+static void csbend_edge(const orc_csbend_setup *S, int which, double *x, double *xp, double *y, double *yp,
+                        double dp) {
+  int eff = which < 0 ? S->edge1_effects : S->edge2_effects;
+  double e = which < 0 ? S->e1 : S->e2;
+  double psi = which < 0 ? S->psi1 : S->psi2;
+  double lim = which < 0 ? S->e1_kick_limit : S->e2_kick_limit;
+  double he = which < 0 ? S->he1 : S->he2;
+  if (S->edge_order <= 1 && eff == 1) {
+    double rho = (1 + dp) * S->rho_actual;
+    double delta_xp = tan(e) / rho * *x;
+    if (lim > 0 && fabs(delta_xp) > lim)
+      delta_xp = SIGN(delta_xp) * lim;
+    *xp += delta_xp;
+    *yp -= tan(e - psi / (1 + dp)) / rho * *y;
+  } else if (S->edge_order >= 2 && eff == 1) {
+    double rho = (1 + dp) * S->rho_actual;
+    apply_edge_effects(x, xp, y, yp, rho, S->n, e, he, psi * (1 + dp), which);
+  } else if (eff == 3) {
+    simple_dipole_edge_kick(xp, yp, *x, *y, dp, S->rho_actual, e, psi, lim);
+  }
+}
+
+/* track_through_csbend (src/csbend.c:654-1434), MALIGN_METHOD=0, iSlice=-1 */
+static long track_through_csbend(double *coord, long n_part, const trk_lattice *l, int idx, double Po,
+                                 double z_start, const orc_maxamp *st, int *err) {
+  orc_csbend_setup S;
+  const trk_elem *e = &l->e[idx];
+  if (csbend_setup(l, idx, Po, &S)) {
+    *err = 1;
+    return n_part;
+  }
+  if (S.is_drift) {
+    exact_drift(coord, n_part, TRK_P(e, CSBEND_L));
+    return n_part;
+  }
+  orc_aperture ap;
+  setup_aperture(&ap, -S.tilt, st);
+  long i_top = n_part - 1;
+  for (long i_part = 0; i_part <= i_top; i_part++) {
+    double *c = ROW(i_part);
+    double x, xp, y, yp, s, dp, dp0, Qi[6], Qf[6], dz_lost;
+    c[4] += S.dzi * sqrt(1 + orc_sqr(c[1]) + orc_sqr(c[3]));
+    c[0] = c[0] + S.dxi + S.dzi * c[1];
+    c[2] = c[2] + S.dyi + S.dzi * c[3];
+    x = c[0] * S.cos_ttilt + c[2] * S.sin_ttilt;
+    y = -c[0] * S.sin_ttilt + c[2] * S.cos_ttilt;
+    xp = c[1] * S.cos_ttilt + c[3] * S.sin_ttilt;
+    yp = -c[1] * S.sin_ttilt + c[3] * S.cos_ttilt;
+    s = c[4];
+    dp = dp0 = c[5];
+    if (S.edge1)
+      csbend_edge(&S, -1, &x, &xp, &y, &yp, dp);
+    Qi[0] = x;
+    Qi[1] = xp;
+    Qi[2] = y;
+    Qi[3] = yp;
+    Qi[4] = 0;
+    Qi[5] = dp;
+    orc_to_dipole_canonical(Qi);
+    int lost = !orc_integrate_csbend(Qf, Qi, &S.bd, &ap, &dz_lost);
+    orc_from_dipole_canonical(Qf);
+    if (lost) {
+      memcpy(c, Qf, sizeof(double) * 6);
+      /* convertFromCSBendCoords (src/csbend.c:4527-4548) */
+      double X = c[0], XP = c[1], Y = c[2], YP = c[3];
+      c[0] = X * S.cos_ttilt - Y * S.sin_ttilt;
+      c[2] = X * S.sin_ttilt + Y * S.cos_ttilt;
+      c[1] = XP * S.cos_ttilt - YP * S.sin_ttilt;
+      c[3] = XP * S.sin_ttilt + YP * S.cos_ttilt;
+      swap_rows(ROW(i_part), ROW(i_top));
+      ROW(i_top)[4] = z_start + dz_lost;
+      ROW(i_top)[5] = Po * (1 + ROW(i_top)[5]);
+      i_top--;
+      i_part--;
+      continue;
+    }
+    if (S.bd.isr_or_rad) {
+      double p0 = Po * (1 + dp0);
+      double beta0 = p0 / sqrt(orc_sqr(p0) + 1);
+      double p1 = Po * (1 + Qf[5]);
+      double beta1 = p1 / sqrt(orc_sqr(p1) + 1);
+      s = beta1 * s / beta0 + Qf[4];
+    } else
+      s += Qf[4];
+    x = Qf[0];
+    xp = Qf[1];
+    y = Qf[2];
+    yp = Qf[3];
+    dp = Qf[5];
+    if (S.edge2)
+      csbend_edge(&S, 1, &x, &xp, &y, &yp, dp);
+    c[0] = x * S.cos_ttilt - y * S.sin_ttilt + S.dcoord_etilt[0];
+    c[2] = x * S.sin_ttilt + y * S.cos_ttilt + S.dcoord_etilt[2];
+    c[1] = xp * S.cos_ttilt - yp * S.sin_ttilt + S.dcoord_etilt[1];
+    c[3] = xp * S.sin_ttilt + yp * S.cos_ttilt + S.dcoord_etilt[3];
+    c[4] = s + S.dcoord_etilt[4];
+    c[5] = dp;
+    c[0] += S.dxf + S.dzf * c[1];
+    c[2] += S.dyf + S.dzf * c[3];
+    c[4] += S.dzf * sqrt(1 + orc_sqr(c[1]) + orc_sqr(c[3]));
+  }
+  return i_top + 1;
+}
+
+int orc_csbend_field_table(const trk_lattice *l, int element, double *Fx, double *Fy, int *eo1, int *hasNormal,
+                           int *hasSkew) {
+  orc_csbend_setup S;
+  if (!l || element < 0 || element >= l->n || l->e[element].type != TRK_CSBEND)
+    return TRK_ERR_ARG;
+  if (csbend_setup(l, element, 1.0, &S) || S.is_drift)
+    return TRK_ERR_UNSUPPORTED;
+  for (int i = 0; i < 11; i++)
+    for (int j = 0; j < 11; j++) {
+      Fx[i * 11 + j] = S.bd.Fx_xy[i][j];
+      Fy[i * 11 + j] = S.bd.Fy_xy[i][j];
+    }
+  *eo1 = S.bd.expansionOrder1;
+  *hasNormal = S.bd.hasNormal;
+  *hasSkew = S.bd.hasSkew;
+  return TRK_OK;
+}
+
+/* ----------------------------------------------------------------- RFCA */
+typedef struct {
+  int fiducial_seen;
+  double phase_fiducial;
+} orc_rf_state;
+
+/* Summation mode for the two beam averages (WAKE mean arrival time, RFCA
+ * "tmean" fiducial).  0: as the reference (plain index-order sum for the wake,
+ * Kahan for the fiducial); 1: double-double sums rounded once, the value the
+ * GPU path computes, for bit-level checks of the downstream arithmetic. */
+static int orc_exact_sums = 0;
+void orc_set_exact_sums(int on) { orc_exact_sums = on; }
+
+static void dd_acc(double *hi, double *lo, double v) {
+  double s = *hi + v, bb = s - *hi, e = (*hi - (s - bb)) + (v - bb);
+  e += *lo;
+  double h = s + e;
+  *lo = e - (h - s);
+  *hi = h;
+}
+
+/* KahanPlus: compensated summation (SDDS mdbmth, not shipped with the
+ * reference; the published algorithm of W. Kahan, 1965). */
+static double kahan_plus(double sum, double b, double *error) {
+  double y = b - *error;
+  double t = sum + y;
+  *error = (t - sum) - y;
+  return t;
+}
+
+/* beta_from_delta (src/do_tracking.c:95-98) */
+static double beta_from_delta(double p, double delta) {
+  p *= 1 + delta;
+  return p / sqrt(p * p + 1);
+}
+
+/* simple_rf_cavity -> trackRfCavityWithWakes (src/simple_rfca.c:264-985):
+ * traveling-wave kick method (no matrix method, no backtracking, no
+ * linearization, fiducial mode "tmean" with Kahan summation). */
+static long rf_cavity(double *coord, long np, const trk_elem *e, orc_rf_state *rs, double *P_central, double zEnd,
+                      int *err) {
+  double length = TRK_P(e, RFCA_L);
+  long nKicks;
+  double omega, volt, tau, dtLight, phase, t0, To;
+  (void)To;
+  if (np <= 0)
+    return np;
+  if (TRK_P(e, RFCA_CHANGE_T) || TRK_P(e, RFCA_LINEARIZE) || TRK_P(e, RFCA_LOCK_PHASE) || TRK_P(e, RFCA_CHANGE_P0) ||
+      TRK_P(e, RFCA_STANDING_WAVE)) {
+    *err = 1;
+    return np;
+  }
+  if (TRK_P(e, RFCA_VOLT) == 0) {
+    if (length) {
+      for (long ip = 0; ip < np; ip++) {
+        double *c = ROW(ip);
+        c[0] += c[1] * length;
+        c[2] += c[3] * length;
+        c[4] += length * sqrt(1 + orc_sqr(c[1]) + orc_sqr(c[3]));
+      }
+    }
+    return np;
+  }
+  omega = TRK_PIx2 * TRK_P(e, RFCA_FREQ);
+  volt = TRK_P(e, RFCA_VOLT) / (1e6 * TRK_ME_MEV * TRK_PARTICLE_REL_SIGN);
+  tau = omega ? TRK_P(e, RFCA_Q) / omega : 0;
+  nKicks = length ? (long)TRK_P(e, RFCA_N_KICKS) : 1;
+  if (nKicks <= 0) {
+    *err = 1; /* matrix method: not on this path */
+    return np;
+  }
+  length /= nKicks;
+  volt /= nKicks;
+  dtLight = length / TRK_C_MKS;
+  if (!rs->fiducial_seen) {
+    if (TRK_P(e, RFCA_T_REFERENCE) != -1)
+      t0 = TRK_P(e, RFCA_T_REFERENCE);
+    else {
+      /* findFiducialTime, FID_MODE_TMEAN (src/simple_rfca.c:191-230) */
+      double tsum = 0, error = 0, sOffset = length / 2;
+      long nsum = 0;
+      double hi = 0, lo = 0;
+      for (long ip = 0; ip < np; ip++) {
+        double t = (ROW(ip)[4] + sOffset) / (TRK_C_MKS * beta_from_delta(*P_central, ROW(ip)[5]));
+        if (orc_exact_sums)
+          dd_acc(&hi, &lo, t);
+        else
+          tsum = kahan_plus(tsum, t, &error);
+        nsum++;
+      }
+      if (orc_exact_sums)
+        tsum = hi + lo;
+      t0 = tsum / nsum;
+    }
+    rs->phase_fiducial = -omega * t0;
+    rs->fiducial_seen = 1;
+  }
+  phase = rs->phase_fiducial;
+  if (omega) {
+    t0 = -rs->phase_fiducial / omega;
+    To = TRK_PIx2 / omega;
+  } else
+    t0 = To = 0;
+  phase += TRK_P(e, RFCA_PHASE) * TRK_PI / 180.0;
+  int same_dgamma = 0;
+  double dgamma = 0;
+  if (omega == 0 && tau == 0) {
+    dgamma = volt * sin(phase);
+    same_dgamma = 1;
+  }
+  double timeOffset = 0;
+  for (long ip = 0; ip < np; ip++) {
+    ROW(ip)[0] -= TRK_P(e, RFCA_DX);
+    ROW(ip)[2] -= TRK_P(e, RFCA_DY);
+  }
+  double *inverseF = (double *)calloc(sizeof(double), np);
+  for (long ik = 0; ik < nKicks; ik++) {
+    for (long ip = 0; ip < np; ip++) {
+      double *c = ROW(ip);
+      double dc4, P, gamma, beta_i, t, dt, gamma1;
+      if (c[5] == -1)
+        continue;
+      if (length)
+        dc4 = length / 2 * sqrt(1 + orc_sqr(c[1]) + orc_sqr(c[3]));
+      else
+        dc4 = 0;
+      P = *P_central * (1 + c[5]);
+      beta_i = P / (gamma = sqrt(orc_sqr(P) + 1));
+      t = (c[4] + dc4) / (TRK_C_MKS * beta_i) - timeOffset;
+      if ((dt = t - t0) < 0)
+        dt = 0;
+      if (!same_dgamma) {
+        double phi = omega * (t - 0 - ik * dtLight) + phase;
+        double dfactor = tau ? sqrt(1 - exp(-dt / tau)) : 1;
+        dgamma = volt * sin(phi) * dfactor;
+      }
+      if (length) {
+        if (TRK_P(e, RFCA_END1_FOCUS) && ik == 0) {
+          inverseF[ip] = dgamma / (2 * gamma * length);
+          c[1] -= c[0] * inverseF[ip];
+          c[3] -= c[2] * inverseF[ip];
+        }
+        c[0] += c[1] * length / 2;
+        c[2] += c[3] * length / 2;
+        c[4] += length / 2 * sqrt(1 + orc_sqr(c[1]) + orc_sqr(c[3]));
+      }
+      orc_add_to_particle_energy(c, t, *P_central, dgamma);
+      if ((gamma1 = gamma + dgamma) <= 1)
+        c[5] = -1;
+      else
+        inverseF[ip] = -dgamma / (2 * gamma1 * length);
+    }
+    if (length) {
+      for (long ip = 0; ip < np; ip++) {
+        double *c = ROW(ip);
+        c[0] += c[1] * length / 2;
+        c[2] += c[3] * length / 2;
+        c[4] += length / 2 * sqrt(1 + orc_sqr(c[1]) + orc_sqr(c[3]));
+        if (TRK_P(e, RFCA_END2_FOCUS) && (ik == nKicks - 1)) {
+          c[1] -= c[0] * inverseF[ip];
+          c[3] -= c[2] * inverseF[ip];
+        }
+      }
+    }
+  }
+  free(inverseF);
+  for (long ip = 0; ip < np; ip++) {
+    ROW(ip)[0] += TRK_P(e, RFCA_DX);
+    ROW(ip)[2] += TRK_P(e, RFCA_DY);
+  }
+  return remove_invalid(coord, np, zEnd, *P_central);
+}
+
+/* ----------------------------------------------------------------- wakes */
+typedef struct {
+  double macroParticleCharge;
+  int charge_set;
+} orc_wake_state;
+
+/* convolveArrays (src/wake.c:480-496) */
+static void convolve_arrays(double *output, long outputs, const double *a1, long n1, const double *a2, long n2,
+                            long di2) {
+  for (long ib = 0; ib < outputs; ib++) {
+    long ib2 = ib + di2, ib1 = 0, di;
+    output[ib] = 0;
+    if (ib2 >= n2) {
+      di = ib2 - n2 + 1;
+      ib1 += di;
+      ib2 -= di;
+    }
+    for (; ib1 < n1 && ib2 >= 0; ib1++, ib2--)
+      output[ib] += a1[ib1] * a2[ib2];
+  }
+}
+
+/* wake table set-up shared by WAKE and TRWAKE (src/wake.c:434-477,
+ * src/trwake.c:460-517): dt from the table span, i0 for acausal tables. */
+static int wake_table_setup(const trk_elem *e, double *dt, long *i0, int acausal) {
+  double tmin = DBL_MAX, tmax = -DBL_MAX;
+  if (!e->wake_t || e->wake_points < 2)
+    return 1;
+  for (long i = 0; i < e->wake_points; i++) {
+    if (e->wake_t[i] < tmin)
+      tmin = e->wake_t[i];
+    if (e->wake_t[i] > tmax)
+      tmax = e->wake_t[i];
+  }
+  if (tmin >= tmax)
+    return 1;
+  *dt = (tmax - tmin) / (e->wake_points - 1);
+  *i0 = 0;
+  if (tmin != 0) {
+    if (!acausal)
+      return 1;
+    *i0 = -1;
+    for (long iw = 0; iw < e->wake_points; iw++)
+      if (fabs(e->wake_t[iw]) < 1e-6 * *dt) {
+        *i0 = iw;
+        break;
+      }
+    if (*i0 == -1 || fabs(tmin) > tmax)
+      return 1;
+  }
+  return 0;
+}
+
+/* track_through_wake (src/wake.c:23-304), one bunch, no smoothing */
+static int track_through_wake(double *coord, long np, const trk_elem *e, double Po, long i_pass,
+                              orc_wake_state *ws, const double *chargeMacro) {
+  double dt, tmean, tmin, tmax, factor, rampFactor;
+  long i0, nb;
+  if (TRK_P(e, WAKE_SMOOTHING) || TRK_P(e, WAKE_CHANGE_P0))
+    return 1;
+  if (wake_table_setup(e, &dt, &i0, (int)TRK_P(e, WAKE_ACAUSAL_ALLOWED)))
+    return 1;
+  /* set_up_wake (src/wake.c:340-372) */
+  if (chargeMacro)
+    ws->macroParticleCharge = *chargeMacro;
+  else if (i_pass == 0) {
+    ws->macroParticleCharge = 0;
+    if (np)
+      ws->macroParticleCharge = TRK_P(e, WAKE_CHARGE) / np;
+  }
+  long rampPasses = (long)TRK_P(e, WAKE_RAMP_PASSES);
+  if (i_pass >= rampPasses - 1)
+    rampFactor = 1;
+  else
+    rampFactor = (i_pass + 1.0) / rampPasses;
+  if (np <= 0)
+    return 0;
+  double *time = (double *)malloc(sizeof(double) * np);
+  long *pbin = (long *)malloc(sizeof(long) * np);
+  /* computeTimeCoordinatesOnly (src/trwake.c:519-527) */
+  for (long ip = 0; ip < np; ip++) {
+    double P = Po * (ROW(ip)[5] + 1);
+    time[ip] = ROW(ip)[4] * sqrt(orc_sqr(P) + 1) / (TRK_C_MKS * P);
+  }
+  /* compute_average (SDDS mdbmth, not shipped): arithmetic mean, summed in
+   * index order */
+  double sum = 0, slo = 0;
+  for (long ip = 0; ip < np; ip++) {
+    if (orc_exact_sums)
+      dd_acc(&sum, &slo, time[ip]);
+    else
+      sum += time[ip];
+  }
+  if (orc_exact_sums)
+    sum = sum + slo;
+  tmean = sum / np;
+  tmin = DBL_MAX;
+  tmax = -DBL_MAX;
+  for (long ip = 0; ip < np; ip++) {
+    if (time[ip] < tmin)
+      tmin = time[ip];
+    if (time[ip] > tmax)
+      tmax = time[ip];
+  }
+  if ((tmax - tmin) > (e->wake_t[e->wake_points - 1] - e->wake_t[0]) && !TRK_P(e, WAKE_ALLOW_LONG_BEAM)) {
+    free(time);
+    free(pbin);
+    return 2; /* the reference exits: beam longer than the wake */
+  }
+  if (TRK_P(e, WAKE_N_BINS)) {
+    nb = (long)TRK_P(e, WAKE_N_BINS);
+    tmin = tmean - dt * nb / 2.0;
+  } else {
+    nb = (long)((tmax - tmin) / dt + 3);
+    tmin -= dt;
+  }
+  if (nb <= 0) {
+    free(time);
+    free(pbin);
+    return 0;
+  }
+  double *Itime = (double *)calloc(nb, sizeof(double));
+  double *Vtime = (double *)calloc(nb + 1, sizeof(double));
+  /* binTimeDistribution (src/wake.c:498-518) */
+  for (long ip = 0; ip < np; ip++) {
+    long ib;
+    pbin[ip] = -1;
+    ib = (long)((time[ip] - tmin) / dt + 0.5);
+    if (ib < 0 || ib > nb - 1)
+      continue;
+    Itime[ib] += 1;
+    pbin[ip] = ib;
+  }
+  Vtime[nb] = 0;
+  convolve_arrays(Vtime, nb, Itime, nb, e->wake_w0, e->wake_points, i0);
+  factor = ws->macroParticleCharge * TRK_PARTICLE_REL_SIGN * TRK_P(e, WAKE_FACTOR) * rampFactor;
+  for (long ib = 0; ib < nb; ib++)
+    Vtime[ib] *= factor;
+  /* applyLongitudinalWakeKicks (src/wake.c:306-330) */
+  int interpolate = (int)TRK_P(e, WAKE_INTERPOLATE);
+  for (long ip = 0; ip < np; ip++) {
+    long ib = pbin[ip];
+    double dgam, dt1;
+    if (ib >= 0 && ib <= nb - 1) {
+      if (interpolate) {
+        dt1 = time[ip] - (tmin + dt * ib);
+        if ((dt1 < 0 && ib) || ib == nb - 1) {
+          ib--;
+          dt1 += dt;
+        }
+        dgam = (Vtime[ib] + (Vtime[ib + 1] - Vtime[ib]) / dt * dt1) / (1e6 * TRK_ME_MEV * TRK_PARTICLE_REL_SIGN);
+      } else
+        dgam = Vtime[ib] / (1e6 * TRK_ME_MEV * TRK_PARTICLE_REL_SIGN);
+      if (dgam)
+        orc_add_to_particle_energy(ROW(ip), time[ip], Po, -dgam);
+    }
+  }
+  free(Itime);
+  free(Vtime);
+  free(time);
+  free(pbin);
+  return 0;
+}
+
+/* track_through_trwake (src/trwake.c:22-287), one bunch, no smoothing.
+ * With one bunch the reference leaves tmean at 0 (it is only computed for
+ * multi-bunch beams, src/trwake.c:70-95), so N_BINS>0 bins around t=0. */
+static int track_through_trwake(double *coord, long np, const trk_elem *e, double Po, long i_pass,
+                                orc_wake_state *ws, const double *chargeMacro) {
+  double dt, tmean = 0, tmin, tmax, rampFactor = 1;
+  long i0, nb;
+  if (TRK_P(e, TRWAKE_SMOOTHING))
+    return 1;
+  if (wake_table_setup(e, &dt, &i0, (int)TRK_P(e, TRWAKE_ACAUSAL_ALLOWED)))
+    return 1;
+  if (chargeMacro)
+    ws->macroParticleCharge = *chargeMacro;
+  else if (i_pass == 0) {
+    ws->macroParticleCharge = 0;
+    if (np)
+      ws->macroParticleCharge = TRK_P(e, TRWAKE_CHARGE) / np;
+  }
+  long rampPasses = (long)TRK_P(e, TRWAKE_RAMP_PASSES);
+  if (i_pass >= rampPasses - 1)
+    rampFactor = 1;
+  else
+    rampFactor = (i_pass + 1.0) / rampPasses;
+  if (np <= 0)
+    return 0;
+  double *time = (double *)malloc(sizeof(double) * np);
+  long *pbin = (long *)malloc(sizeof(long) * np);
+  double *pz = (double *)calloc(np, sizeof(double));
+  for (long ip = 0; ip < np; ip++) {
+    double P = Po * (ROW(ip)[5] + 1);
+    time[ip] = ROW(ip)[4] * sqrt(orc_sqr(P) + 1) / (TRK_C_MKS * P);
+  }
+  tmin = DBL_MAX;
+  tmax = -DBL_MAX;
+  for (long ip = 0; ip < np; ip++) {
+    if (time[ip] < tmin)
+      tmin = time[ip];
+    if (time[ip] > tmax)
+      tmax = time[ip];
+  }
+  if ((tmax - tmin) > (e->wake_t[e->wake_points - 1] - e->wake_t[0])) {
+    free(time);
+    free(pbin);
+    free(pz);
+    return 2;
+  }
+  if (TRK_P(e, TRWAKE_N_BINS)) {
+    tmin = tmean - dt * TRK_P(e, TRWAKE_N_BINS) / 2.0;
+    nb = (long)TRK_P(e, TRWAKE_N_BINS);
+  } else {
+    nb = (long)((tmax - tmin) / dt + 3);
+    tmin -= dt;
+    tmax += dt;
+  }
+  if (tmin > tmax || nb <= 0) {
+    free(time);
+    free(pbin);
+    free(pz);
+    return 2;
+  }
+  double tilt = TRK_P(e, TRWAKE_TILT);
+  if (tilt)
+    rotate_beam(coord, np, tilt);
+  double *posItime[2];
+  posItime[0] = (double *)calloc(nb, sizeof(double));
+  posItime[1] = (double *)calloc(nb, sizeof(double));
+  double *Vtime = (double *)calloc(nb + 1, sizeof(double));
+  long xPower = (long)TRK_P(e, TRWAKE_X_DRIVE_EXPONENT), yPower = (long)TRK_P(e, TRWAKE_Y_DRIVE_EXPONENT);
+  double dx = TRK_P(e, TRWAKE_DX), dy = TRK_P(e, TRWAKE_DY);
+  /* binTransverseTimeDistribution (src/trwake.c:610-641) */
+  for (long ip = 0; ip < np; ip++) {
+    double *c = ROW(ip);
+    long ib;
+    pbin[ip] = -1;
+    ib = (long)((time[ip] - tmin) / dt + 0.5);
+    if (ib < 0 || ib > nb - 1)
+      continue;
+    if (xPower == 1)
+      posItime[0][ib] += c[0] - dx;
+    else if (xPower < 1)
+      posItime[0][ib] += 1;
+    else
+      posItime[0][ib] += orc_ipow(c[0] - dx, xPower);
+    if (yPower == 1)
+      posItime[1][ib] += c[2] - dy;
+    else if (yPower < 1)
+      posItime[1][ib] += 1;
+    else
+      posItime[1][ib] += orc_ipow(c[2] - dy, yPower);
+    pbin[ip] = ib;
+    pz[ip] = Po * (1 + c[5]) / sqrt(1 + orc_sqr(c[1]) + orc_sqr(c[3]));
+  }
+  for (int plane = 0; plane < 2; plane++) {
+    const double *W = plane ? e->wake_w1 : e->wake_w0;
+    double factor = ws->macroParticleCharge * TRK_PARTICLE_REL_SIGN * TRK_P(e, TRWAKE_FACTOR);
+    if (plane == 0)
+      factor *= TRK_P(e, TRWAKE_XFACTOR) * rampFactor;
+    else
+      factor *= TRK_P(e, TRWAKE_YFACTOR) * rampFactor;
+    if (!factor)
+      continue;
+    Vtime[nb] = 0;
+    convolve_arrays(Vtime, nb, posItime[plane], nb, W, e->wake_points, i0);
+    for (long ib = 0; ib < nb; ib++)
+      Vtime[ib] *= factor;
+    /* applyTransverseWakeKicks (src/trwake.c:289-314) */
+    int interpolate = (int)TRK_P(e, TRWAKE_INTERPOLATE);
+    long exponent = (long)(plane == 0 ? TRK_P(e, TRWAKE_X_PROBE_EXPONENT) : TRK_P(e, TRWAKE_Y_PROBE_EXPONENT));
+    int offset = 2 * plane + 1;
+    for (long ip = 0; ip < np; ip++) {
+      long ib = pbin[ip];
+      double dt1, Vinterp;
+      if (ib >= 0 && ib <= nb - 1) {
+        if (interpolate) {
+          dt1 = time[ip] - (tmin + dt * ib);
+          if ((dt1 < 0 && ib) || ib == nb - 1) {
+            ib--;
+            dt1 += dt;
+          }
+          Vinterp = Vtime[ib] + (Vtime[ib + 1] - Vtime[ib]) / dt * dt1;
+        } else
+          Vinterp = Vtime[ib];
+        if (exponent)
+          Vinterp *= orc_ipow(ROW(ip)[offset - 1], exponent);
+        if (Vinterp)
+          ROW(ip)[offset] += Vinterp / (1e6 * TRK_ME_MEV * TRK_PARTICLE_REL_SIGN) / pz[ip];
+      }
+    }
+  }
+  if (tilt)
+    rotate_beam(coord, np, -tilt);
+  free(posItime[0]);
+  free(posItime[1]);
+  free(Vtime);
+  free(time);
+  free(pbin);
+  free(pz);
+  return 0;
+}
+
+/* ------------------------------------------------------------- driver */
+typedef struct {
+  orc_maxamp maxamp;
+  orc_rf_state *rf;     /* per element */
+  orc_wake_state *wake; /* per element */
+  int have_charge;
+  double chargeMacro;
+} orc_run_state;
+
+/* The body of do_tracking's element switch (src/do_tracking.c:1239-2495) and
+ * the after-element filters (:2506-2524 aperture, :2676 NaN/inf filter). */
+static int track_one_element(const trk_lattice *l, int idx, double *coord, long nToTrack, long i_pass, double last_z,
+                             double z, double *P_central, orc_run_state *rs, long *nLeft_out) {
+  const trk_elem *e = &l->e[idx];
+  long nLeft = nToTrack;
+  int err = 0;
+  switch (e->type) {
+  case TRK_MARK:
+  case TRK_CHARGE:
+    break;
+  case TRK_DRIF:
+    drift_matrix_track(coord, nToTrack, TRK_P(e, DRIF_L), (long)TRK_P(e, DRIF_ORDER));
+    break;
+  case TRK_EDRIFT:
+    exact_drift(coord, nToTrack, TRK_P(e, EDRIFT_L));
+    break;
+  case TRK_KQUAD:
+  case TRK_KSEXT:
+  case TRK_KOCT:
+    nLeft = multipole_tracking2(coord, nToTrack, e, *P_central, last_z, &rs->maxamp, &err);
+    break;
+  case TRK_CSBEND:
+    nLeft = track_through_csbend(coord, nToTrack, l, idx, *P_central, last_z, &rs->maxamp, &err);
+    break;
+  case TRK_RFCA:
+    nLeft = rf_cavity(coord, nToTrack, e, &rs->rf[idx], P_central, z, &err);
+    break;
+  case TRK_WAKE:
+    err = track_through_wake(coord, nToTrack, e, *P_central, i_pass, &rs->wake[idx],
+                             rs->have_charge ? &rs->chargeMacro : NULL);
+    break;
+  case TRK_TRWAKE:
+    err = track_through_trwake(coord, nToTrack, e, *P_central, i_pass, &rs->wake[idx],
+                               rs->have_charge ? &rs->chargeMacro : NULL);
+    break;
+  case TRK_MAXAMP:
+    maxamp_update(&rs->maxamp, e);
+    break;
+  default:
+    err = 1;
+  }
+  if (err)
+    return err == 2 ? TRK_ERR_PHYSICS : TRK_ERR_UNSUPPORTED;
+  if (e->type != TRK_MARK && e->type != TRK_CHARGE) {
+    const orc_maxamp *st = &rs->maxamp;
+    if (st->x_max || st->y_max) {
+      if (!st->elliptical)
+        nLeft = limit_amplitudes(coord, st->x_max, st->y_max, nLeft, z, *P_central, e->type == TRK_DRIF);
+      else {
+        int e2 = 0;
+        nLeft = elimit_amplitudes(coord, st->x_max, st->y_max, nLeft, z, *P_central, e->type == TRK_DRIF,
+                                  st->exponent, st->yExponent, &e2);
+        if (e2)
+          return TRK_ERR_UNSUPPORTED;
+      }
+    }
+  }
+  nLeft = limit_amplitudes(coord, DBL_MAX, DBL_MAX, nLeft, z, *P_central, 0);
+  *nLeft_out = nLeft;
+  return TRK_OK;
+}
+
+static int run_state_init(const trk_lattice *l, long nOriginal, orc_run_state *rs) {
+  memset(rs, 0, sizeof(*rs));
+  rs->rf = (orc_rf_state *)calloc(l->n > 0 ? l->n : 1, sizeof(orc_rf_state));
+  rs->wake = (orc_wake_state *)calloc(l->n > 0 ? l->n : 1, sizeof(orc_wake_state));
+  if (!rs->rf || !rs->wake)
+    return TRK_ERR_NOMEM;
+  /* CHARGE element (src/do_tracking.c:780-815) */
+  for (int i = 0; i < l->n; i++)
+    if (l->e[i].type == TRK_CHARGE) {
+      const trk_elem *e = &l->e[i];
+      rs->have_charge = 1;
+      rs->chargeMacro = 0;
+      if (nOriginal)
+        rs->chargeMacro = TRK_P(e, CHARGE_TOTAL) / nOriginal;
+      if (TRK_P(e, CHARGE_PER_PARTICLE))
+        rs->chargeMacro = TRK_P(e, CHARGE_PER_PARTICLE);
+    }
+  return TRK_OK;
+}
+
+static void run_state_free(orc_run_state *rs) {
+  free(rs->rf);
+  free(rs->wake);
+}
+
+int orc_track(const trk_lattice *l, double *coord, long np, long n_passes, long pass_offset, double *p_central,
+              orc_result *result) {
+  orc_run_state rs;
+  int rc;
+  if (!l || (!coord && np) || !p_central)
+    return TRK_ERR_ARG;
+  if ((rc = run_state_init(l, np, &rs)))
+    return rc;
+  for (long ip = 0; ip < np; ip++) {
+    ROW(ip)[7] = -1;
+    ROW(ip)[8] = -1;
+  }
+  long nToTrack = np, effort = 0;
+  /* initial NaN screen (src/do_tracking.c:478-484) */
+  long nLeft = limit_amplitudes(coord, DBL_MAX, DBL_MAX, nToTrack, 0.0, *p_central, 0);
+  for (long k = nLeft; k < nToTrack; k++) {
+    ROW(k)[7] = pass_offset;
+    ROW(k)[8] = -1;
+  }
+  nToTrack = nLeft;
+  for (long i_pass = pass_offset; i_pass < pass_offset + n_passes; i_pass++) {
+    double z = 0, last_z;
+    for (int idx = 0; idx < l->n; idx++) {
+      last_z = z;
+      z += trk_elem_length(&l->e[idx]);
+      rc = track_one_element(l, idx, coord, nToTrack, i_pass, last_z, z, p_central, &rs, &nLeft);
+      if (rc) {
+        run_state_free(&rs);
+        return rc;
+      }
+      /* recordLostParticles (src/do_tracking.c:4669-4731) */
+      for (long k = nLeft; k < nToTrack; k++) {
+        ROW(k)[7] = i_pass;
+        ROW(k)[8] = idx;
+      }
+      nToTrack = nLeft;
+    }
+    effort += nLeft; /* src/do_tracking.c:2812-2819 */
+  }
+  run_state_free(&rs);
+  if (result) {
+    result->n_left = nToTrack;
+    result->particle_passes = effort;
+    result->p_central = *p_central;
+  }
+  return TRK_OK;
+}
+
+int orc_track_element(const trk_lattice *l, int element, double *coord, long np, long pass, double *p_central,
+                      long *n_left) {
+  orc_run_state rs;
+  int rc;
+  if (!l || element < 0 || element >= l->n || !p_central || !n_left)
+    return TRK_ERR_ARG;
+  if ((rc = run_state_init(l, np, &rs)))
+    return rc;
+  /* sticky MAXAMP state before this element */
+  double z = 0;
+  for (int i = 0; i < element; i++) {
+    if (l->e[i].type == TRK_MAXAMP)
+      maxamp_update(&rs.maxamp, &l->e[i]);
+    z += trk_elem_length(&l->e[i]);
+  }
+  if (pass > 0 && !rs.maxamp.seen)
+    for (int i = element; i < l->n; i++)
+      if (l->e[i].type == TRK_MAXAMP)
+        maxamp_update(&rs.maxamp, &l->e[i]);
+  double last_z = z;
+  z += trk_elem_length(&l->e[element]);
+  rc = track_one_element(l, element, coord, np, pass, last_z, z, p_central, &rs, n_left);
+  run_state_free(&rs);
+  return rc;
+}

@@ -1,0 +1,49 @@
+/*
+ * trk_oracle.h -- TEST INFRASTRUCTURE ONLY: the CPU oracle for the tracking
+ * path (a C restatement of elegant's element functions and do_tracking pass
+ * loop).  Used by tests, smoke() and bench.py's CPU baseline as the checker;
+ * the product library never links it.
+ */
+#ifndef TRK_ORACLE_H
+#define TRK_ORACLE_H
+
+#include "trk.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Rows of the oracle beam: x, xp, y, yp, s, delta, id, loss pass, loss element. */
+#define ORC_STRIDE 9
+
+typedef struct {
+  long n_left;
+  long particle_passes;
+  double p_central;
+} orc_result;
+
+/* Track np particles (rows of ORC_STRIDE doubles, modified in place; lost
+ * particles are swapped behind the survivors as the reference does) through
+ * n_passes passes starting at pass index pass_offset.  *p_central in/out. */
+int orc_track(const trk_lattice *lattice, double *coord, long np, long n_passes, long pass_offset,
+              double *p_central, orc_result *result);
+
+/* One element (index `element`), as do_tracking's switch plus the
+ * after-element aperture and NaN filters.  z_start is the arc length at the
+ * element entrance; maxamp state is taken from the lattice (sticky MAXAMP). */
+int orc_track_element(const trk_lattice *lattice, int element, double *coord, long np, long pass,
+                      double *p_central, long *n_left);
+
+/* 0: beam averages summed as the reference does; 1: double-double sums
+ * rounded once (the GPU path's value) for bit-level checks. */
+void orc_set_exact_sums(int on);
+
+/* Field-expansion table of a CSBEND as the oracle builds it (for tests):
+ * Fx, Fy are 11x11 row-major, coefficient of x^i y^j at [i*11+j]. */
+int orc_csbend_field_table(const trk_lattice *lattice, int element, double *Fx, double *Fy, int *expansionOrder1,
+                           int *hasNormal, int *hasSkew);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

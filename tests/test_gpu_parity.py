@@ -1,0 +1,211 @@
+"""Parity of the CUDA tracking path against the CPU oracle, through the C ABI.
+
+Parity build (fast=False): bit-exact with the oracle on every surviving
+coordinate, identical survivor sets, identical lost-particle records.
+Fast build (fast=True): per-coordinate error |gpu-ref|/max(|ref|, sigma) below
+the bounds stated per test, identical survivor sets away from apertures.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from elegant_b200 import Lattice, configs
+from tests.helpers import compare, gpu_run, oracle_run
+
+pytestmark = pytest.mark.gpu
+PC = configs.P_CENTRAL
+
+
+def single(type_name, **params):
+    lat = Lattice()
+    lat.add(type_name, type_name, **params)
+    return lat
+
+
+ELEMENT_CASES = {
+    "drif": single("DRIF", L=1.3),
+    "drif_order1": single("DRIF", L=0.7, ORDER=1),
+    "edrift": single("EDRIFT", L=2.1),
+    "kquad": single("KQUAD", L=0.3, K1=1.2, N_KICKS=8),
+    "kquad_order2": single("KQUAD", L=0.3, K1=-1.1, N_SLICES=5, INTEGRATION_ORDER=2),
+    "kquad_order6": single("KQUAD", L=0.5, K1=0.8, N_SLICES=3, INTEGRATION_ORDER=6),
+    "kquad_misaligned": single("KQUAD", L=0.3, K1=1.2, N_KICKS=8, DX=1e-4, DY=-2e-4, DZ=1e-3, TILT=0.01),
+    "kquad_kicks_fse": single("KQUAD", L=0.4, K1=0.9, N_KICKS=12, HKICK=1e-5, VKICK=-2e-5, FSE=1e-3),
+    "kquad_leff": single("KQUAD", L=0.4, K1=0.9, N_KICKS=4, LEFFECTIVE=0.35),
+    "kquad_expand": single("KQUAD", L=0.3, K1=1.2, N_KICKS=8, EXPAND_HAMILTONIAN=1),
+    "ksext": single("KSEXT", L=0.2, K2=40.0, N_KICKS=4),
+    "ksext_k1j1": single("KSEXT", L=0.2, K2=-30.0, K1=0.01, J1=0.02, N_SLICES=2, TILT=0.1),
+    "koct": single("KOCT", L=0.2, K3=500.0),
+    "csbend": single("CSBEND", L=1.0, ANGLE=2 * math.pi / 80, N_KICKS=16),
+    "csbend_negative": single("CSBEND", L=1.0, ANGLE=-0.05, N_KICKS=8),
+    "csbend_k1": single("CSBEND", L=1.0, ANGLE=2 * math.pi / 280, K1=-0.4, N_KICKS=32),
+    "csbend_k1k2": single("CSBEND", L=0.8, ANGLE=0.03, K1=0.3, K2=5.0, N_SLICES=10),
+    "csbend_edges": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=0.03, N_SLICES=8),
+    "csbend_edges_fringe": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=0.03, HGAP=0.02, FINT=0.5, N_SLICES=8),
+    "csbend_edge_order2": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=0.03, EDGE_ORDER=2, K1=0.2, N_SLICES=8),
+    "csbend_edge3": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=0.03, EDGE1_EFFECTS=3, EDGE2_EFFECTS=3,
+                           N_SLICES=8),
+    "csbend_misaligned": single("CSBEND", L=1.0, ANGLE=0.05, DX=1e-4, DY=2e-4, DZ=-1e-4, TILT=0.02, N_SLICES=8),
+    "csbend_order6": single("CSBEND", L=1.0, ANGLE=0.05, N_SLICES=4, INTEGRATION_ORDER=6),
+    "rfca_thin": single("RFCA", L=0.0, VOLT=4e6, FREQ=352e6, PHASE=170.0),
+    "rfca_long": single("RFCA", L=0.5, VOLT=2e6, FREQ=500e6, PHASE=160.0, N_KICKS=5, END1_FOCUS=1, END2_FOCUS=1),
+    "rfca_tref": single("RFCA", L=0.0, VOLT=1e6, FREQ=352e6, PHASE=90.0, T_REFERENCE=1e-12),
+    "rfca_zero_volt": single("RFCA", L=0.3, VOLT=0.0),
+}
+
+
+@pytest.mark.parametrize("name", sorted(ELEMENT_CASES))
+def test_element_parity_exact(tracker, name):
+    lat = ELEMENT_CASES[name]
+    beam = configs.gaussian_beam(4000, seed=11)
+    beam[:, 0] *= 5
+    beam[:, 2] *= 5
+    nl, g, lp, le, _ = gpu_run(tracker, lat, beam, 2, PC, fast=False)
+    rows, nlo, _ = oracle_run(lat, beam, 2, PC)
+    r = compare(g, rows, nl, nlo)
+    assert r["same_survivors"]
+    assert r["bit_exact"], r
+    assert r["lost_equal"]
+
+
+@pytest.mark.parametrize("name", sorted(ELEMENT_CASES))
+def test_element_parity_fast(tracker, name):
+    lat = ELEMENT_CASES[name]
+    beam = configs.gaussian_beam(4000, seed=12)
+    nl, g, lp, le, _ = gpu_run(tracker, lat, beam, 2, PC, fast=True)
+    rows, nlo, _ = oracle_run(lat, beam, 2, PC)
+    r = compare(g, rows, nl, nlo)
+    assert r["same_survivors"]
+    assert r["max_err"] < 1e-11, r
+
+
+def test_fodo_ring_exact(tracker):
+    lat = configs.c1_lattice()
+    beam = configs.gaussian_beam(2000, seed=1)
+    nl, g, lp, le, st = gpu_run(tracker, lat, beam, 3, PC, fast=False)
+    rows, nlo, eff = oracle_run(lat, beam, 3, PC)
+    r = compare(g, rows, nl, nlo)
+    assert r["same_survivors"] and r["bit_exact"], r
+    assert st["particle_passes"] == eff
+
+
+def test_fodo_ring_fast_one_turn(tracker):
+    lat = configs.c1_lattice()
+    beam = configs.gaussian_beam(2000, seed=1)
+    nl, g, lp, le, _ = gpu_run(tracker, lat, beam, 1, PC, fast=True)
+    rows, nlo, _ = oracle_run(lat, beam, 1, PC)
+    r = compare(g, rows, nl, nlo)
+    assert r["same_survivors"]
+    assert r["max_err"] < 1e-9, r
+
+
+def test_losses_rect_aperture_exact(tracker):
+    lat = Lattice()
+    lat.add("MAXAMP", "AP", X_MAX=0.004, Y_MAX=0.003)
+    lat.extend(configs.c1_lattice(cells=4))
+    beam = configs.gaussian_beam(3000, seed=5, sigma_x=2e-3, sigma_xp=2e-4)
+    nl, g, lp, le, _ = gpu_run(tracker, lat, beam, 4, PC, fast=False)
+    rows, nlo, _ = oracle_run(lat, beam, 4, PC)
+    r = compare(g, rows, nl, nlo)
+    assert nlo < beam.shape[0]
+    assert r["same_survivors"] and r["bit_exact"] and r["lost_equal"], r
+    o = rows[np.argsort(rows[:, 6])]
+    lost = o[:, 7] >= 0
+    gi = np.argsort(g[:, 6])
+    assert np.array_equal(lp[gi][lost], o[lost, 7].astype(np.int64))
+    assert np.array_equal(le[gi][lost], o[lost, 8].astype(np.int32))
+
+
+def test_losses_elliptical_aperture_exact(tracker):
+    lat = Lattice()
+    lat.extend(configs.c1_lattice(cells=2))
+    lat.add("MAXAMP", "AP", X_MAX=0.005, Y_MAX=0.004, ELLIPTICAL=1)
+    lat.extend(configs.c1_lattice(cells=2))
+    beam = configs.gaussian_beam(3000, seed=6, sigma_x=2e-3, sigma_xp=2e-4)
+    nl, g, lp, le, _ = gpu_run(tracker, lat, beam, 3, PC, fast=False)
+    rows, nlo, _ = oracle_run(lat, beam, 3, PC)
+    r = compare(g, rows, nl, nlo)
+    assert nlo < beam.shape[0]
+    assert r["same_survivors"] and r["bit_exact"] and r["lost_equal"], r
+
+
+def test_nonfinite_particles_removed(tracker):
+    lat = configs.c1_lattice(cells=1)
+    beam = configs.gaussian_beam(100, seed=7)
+    beam[3, 0] = np.nan
+    beam[10, 2] = np.inf
+    beam[20, 5] = np.nan
+    nl, g, lp, le, _ = gpu_run(tracker, lat, beam, 1, PC, fast=False)
+    rows, nlo, _ = oracle_run(lat, beam, 1, PC)
+    r = compare(g, rows, nl, nlo)
+    assert nl == nlo == 97
+    assert r["same_survivors"] and r["bit_exact"], r
+
+
+def test_coord_limit_loss(tracker):
+    lat = single("KQUAD", L=0.3, K1=1.2, N_KICKS=8)
+    beam = configs.gaussian_beam(50, seed=8)
+    beam[5, 1] = 1.5  # |x'| > SLOPE_LIMIT
+    nl, g, lp, le, _ = gpu_run(tracker, lat, beam, 1, PC, fast=False)
+    rows, nlo, _ = oracle_run(lat, beam, 1, PC)
+    assert nl == nlo == 49
+    r = compare(g, rows, nl, nlo)
+    assert r["same_survivors"] and r["bit_exact"], r
+
+
+def test_empty_beam(tracker):
+    lat = configs.c1_lattice(cells=1)
+    beam = np.zeros((0, 7))
+    tracker.load(beam)
+    st = tracker.track(lat, 3, PC)
+    assert st["n_left"] == 0 and st["particle_passes"] == 0
+
+
+def test_rf_wake_ring_exact_sums(tracker):
+    """C2's lattice (short ring) with the oracle summing beam averages the way
+    the GPU does (double-double rounded once): every downstream operation then
+    matches bit for bit, including histogram, convolution and kicks."""
+    from oracle import pyoracle
+    lat = configs.c2_lattice(cells=4, n_bins=400)
+    beam = configs.gaussian_beam(5000, seed=3)
+    pyoracle.set_exact_sums(True)
+    try:
+        nl, g, lp, le, _ = gpu_run(tracker, lat, beam, 3, PC, fast=False)
+        rows, nlo, _ = oracle_run(lat, beam, 3, PC)
+    finally:
+        pyoracle.set_exact_sums(False)
+    r = compare(g, rows, nl, nlo)
+    assert r["same_survivors"] and r["bit_exact"], r
+
+
+def test_rf_wake_ring_reference_sums(tracker):
+    """Same ring with the oracle's reference summation (index-order sum for
+    the wake mean, Kahan for the RF fiducial): agreement to rounding."""
+    lat = configs.c2_lattice(cells=4, n_bins=400)
+    beam = configs.gaussian_beam(5000, seed=3)
+    nl, g, lp, le, _ = gpu_run(tracker, lat, beam, 3, PC, fast=False)
+    rows, nlo, _ = oracle_run(lat, beam, 3, PC)
+    r = compare(g, rows, nl, nlo)
+    assert r["same_survivors"]
+    assert r["max_err"] < 1e-9, r
+
+
+def test_trwake_exact_sums(tracker):
+    from oracle import pyoracle
+    lat = configs.c1_lattice(cells=2)
+    lat.add("CHARGE", "Q", TOTAL=2e-9)
+    i = lat.add("TRWAKE", "TW", N_BINS=0)
+    t, W = configs.resonator_wake(points=512, dt=2e-12, f_r=5e9)
+    lat.set_wake(i, t, W * 1e3, W * 0.5e3)
+    beam = configs.gaussian_beam(3000, seed=4)
+    pyoracle.set_exact_sums(True)
+    try:
+        nl, g, lp, le, _ = gpu_run(tracker, lat, beam, 2, PC, fast=False)
+        rows, nlo, _ = oracle_run(lat, beam, 2, PC)
+    finally:
+        pyoracle.set_exact_sums(False)
+    r = compare(g, rows, nl, nlo)
+    assert r["same_survivors"]
+    # transverse bin sums are FP64 atomics (order-dependent in the last bit)
+    assert r["max_err"] < 1e-12, r
