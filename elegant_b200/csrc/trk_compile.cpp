@@ -561,11 +561,13 @@ int compile_bend(const trk_lattice *l, int idx, double Po, trk_op *op, std::vect
   d[BD_PSI1] = psi1;
   d[BD_LIM1] = lim1;
   d[BD_HE1] = he1;
+  d[BD_SE1] = 1. / std::cos(e1);
   d[BD_E2] = e2;
   d[BD_TE2] = std::tan(e2);
   d[BD_PSI2] = psi2;
   d[BD_LIM2] = lim2;
   d[BD_HE2] = he2;
+  d[BD_SE2] = 1. / std::cos(e2);
   d[BD_N] = n;
   d[BD_RHOINV] = 1.0 / rho0;
   d[BD_INVRHOA] = 1.0 / rho_actual;

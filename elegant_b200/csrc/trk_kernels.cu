@@ -21,7 +21,7 @@
 #include <stdint.h>
 
 #include "trk_constants.h"
-#include "trk_crmath.cuh"
+#include "trk_crmath.h"
 #include "trk_kernels.h"
 #include "trk_ops.h"
 
@@ -34,11 +34,13 @@
 #define M_SIN(x) sin(x)
 #define M_COS(x) cos(x)
 #define M_ASIN(x) asin(x)
+#define M_TAN(x) tan(x)
 #else
 #define TRK_NS trk_exact
-#define M_SIN(x) trkcr::cr_sin(x)
-#define M_COS(x) trkcr::cr_cos(x)
-#define M_ASIN(x) trkcr::cr_asin(x)
+#define M_SIN(x) trkcr_sin(x)
+#define M_COS(x) trkcr_cos(x)
+#define M_ASIN(x) trkcr_asin(x)
+#define M_TAN(x) trkcr_tan(x)
 #endif
 
 namespace TRK_NS {
@@ -325,15 +327,15 @@ __device__ __forceinline__ void bend_fields(int mode, int eo1, const double *__r
 
 /* apply_edge_effects (src/csbend.c:4291-4333) */
 __device__ void edge_order2(double &x, double &xp, double &y, double &yp, double rho, double n, double beta,
-                            double he, double psi, int which_edge) {
+                            double tanb, double secb, double he, double psi, int which_edge) {
   double h, tan_beta, tan2_beta, sec_beta, sec2_beta, h2;
   double R21, R43, T111, T133, T211, T441, T331, T221, T233, T243, T431, T432;
   h = 1 / rho;
-  R21 = h * (tan_beta = tan(beta));
-  R43 = -h * tan(beta - psi);
+  R21 = h * (tan_beta = tanb);
+  R43 = -h * M_TAN(beta - psi);
   h2 = sqr(h);
   T111 = which_edge * h / 2 * (tan2_beta = sqr(tan_beta));
-  sec_beta = 1. / cos(beta);
+  sec_beta = secb;
   sec2_beta = sqr(sec_beta);
   T133 = -which_edge * h / 2 * sec2_beta;
   T211 = which_edge == -1 ? -n * h2 * tan_beta : -h2 * (n + tan2_beta / 2) * tan_beta;
@@ -359,18 +361,18 @@ __device__ void edge_order2(double &x, double &xp, double &y, double &yp, double
 __device__ __forceinline__ void bend_edge(int mode, const double *__restrict__ d, int base, int which, double rho_a,
                                           double nidx, double &x, double &xp, double &y, double &yp, double dp) {
   const double e = __ldg(&d[base + 0]), te = __ldg(&d[base + 1]), psi = __ldg(&d[base + 2]);
-  const double lim = __ldg(&d[base + 3]), he = __ldg(&d[base + 4]);
+  const double lim = __ldg(&d[base + 3]), he = __ldg(&d[base + 4]), secb = __ldg(&d[base + 5]);
   if (mode == EDGE_LIN1) {
     double rho = (1 + dp) * rho_a;
     double delta_xp = te / rho * x;
     if (lim > 0 && fabs(delta_xp) > lim)
       delta_xp = (delta_xp < 0 ? -1 : 1) * lim;
     xp += delta_xp;
-    double t2 = psi == 0 ? te : tan(e - psi / (1 + dp));
+    double t2 = psi == 0 ? te : M_TAN(e - psi / (1 + dp));
     yp -= t2 / rho * y;
   } else if (mode == EDGE_LIN2) {
     double rho = (1 + dp) * rho_a;
-    edge_order2(x, xp, y, yp, rho, nidx, e, he, psi * (1 + dp), which);
+    edge_order2(x, xp, y, yp, rho, nidx, e, te, secb, he, psi * (1 + dp), which);
   } else if (mode == EDGE_SYMP) {
     /* applySimpleDipoleEdgeKick (src/csbend.c:5664-5690) */
     double Q1 = xp, Q3 = yp;
@@ -380,7 +382,7 @@ __device__ __forceinline__ void bend_edge(int mode, const double *__restrict__ d
     double dqx = te / rho_a * x;
     if (lim > 0 && fabs(dqx) > lim)
       dqx = (dqx < 0 ? -1 : 1) * lim;
-    double t2 = psi == 0 ? te : tan(e - psi / (1 + dp));
+    double t2 = psi == 0 ? te : M_TAN(e - psi / (1 + dp));
     double dqy = -t2 / rho_a * y;
     Q1 += dqx;
     Q3 += dqy;
@@ -906,7 +908,7 @@ __device__ __forceinline__ long wake_bin(double t, double tmin, double dt) {
 __global__ void __launch_bounds__(TRK_BLOCK) time_stats_kernel(TimeStatsArgs a) {
   __shared__ double sh_hi[TRK_BLOCK], sh_lo[TRK_BLOCK], sh_min[TRK_BLOCK], sh_max[TRK_BLOCK];
   __shared__ long long sh_n[TRK_BLOCK];
-  trkcr::dd acc = {0.0, 0.0};
+  trkcr_dd acc = trkcr_make(0.0, 0.0);
   double tmin = 1.7976931348623157e308, tmax = -1.7976931348623157e308;
   long long cnt = 0;
   /* particles are assigned to blocks in fixed chunks so the result does
@@ -914,7 +916,7 @@ __global__ void __launch_bounds__(TRK_BLOCK) time_stats_kernel(TimeStatsArgs a) 
   const long chunk = a.chunk;
   for (long c = blockIdx.x; c * chunk < a.n; c += gridDim.x) {
     const long lo = c * chunk, hi = min(a.n, lo + chunk);
-    trkcr::dd cacc = {0.0, 0.0};
+    trkcr_dd cacc = trkcr_make(0.0, 0.0);
     for (long i = lo + threadIdx.x; i < hi; i += blockDim.x) {
       if (a.lost_pass[i] >= 0)
         continue;
@@ -926,12 +928,12 @@ __global__ void __launch_bounds__(TRK_BLOCK) time_stats_kernel(TimeStatsArgs a) 
         double beta = p / sqrt(p * p + 1);
         t = (a.s[i] + a.sOffset) / (TRK_C_MKS * beta);
       }
-      cacc = trkcr::dd_add(cacc, trkcr::dd{t, 0.0});
+      cacc = trkcr_add(cacc, trkcr_make(t, 0.0));
       tmin = fmin(tmin, t);
       tmax = fmax(tmax, t);
       cnt++;
     }
-    acc = trkcr::dd_add(acc, cacc);
+    acc = trkcr_add(acc, cacc);
   }
   const int tid = threadIdx.x;
   sh_hi[tid] = acc.hi;
@@ -942,7 +944,7 @@ __global__ void __launch_bounds__(TRK_BLOCK) time_stats_kernel(TimeStatsArgs a) 
   __syncthreads();
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {
     if (tid < w) {
-      trkcr::dd u = trkcr::dd_add(trkcr::dd{sh_hi[tid], sh_lo[tid]}, trkcr::dd{sh_hi[tid + w], sh_lo[tid + w]});
+      trkcr_dd u = trkcr_add(trkcr_make(sh_hi[tid], sh_lo[tid]), trkcr_make(sh_hi[tid + w], sh_lo[tid + w]));
       sh_hi[tid] = u.hi;
       sh_lo[tid] = u.lo;
       sh_min[tid] = fmin(sh_min[tid], sh_min[tid + w]);
@@ -964,11 +966,11 @@ __global__ void __launch_bounds__(TRK_BLOCK) time_stats_kernel(TimeStatsArgs a) 
 __global__ void time_stats_finish_kernel(TimeStatsArgs a, int nblocks) {
   if (threadIdx.x != 0 || blockIdx.x != 0)
     return;
-  trkcr::dd acc = {0.0, 0.0};
+  trkcr_dd acc = trkcr_make(0.0, 0.0);
   double tmin = 1.7976931348623157e308, tmax = -1.7976931348623157e308;
   long long n = 0;
   for (int b = 0; b < nblocks; b++) {
-    acc = trkcr::dd_add(acc, trkcr::dd{a.part_hi[b], a.part_lo[b]});
+    acc = trkcr_add(acc, trkcr_make(a.part_hi[b], a.part_lo[b]));
     tmin = fmin(tmin, a.part_min[b]);
     tmax = fmax(tmax, a.part_max[b]);
     n += a.part_n[b];

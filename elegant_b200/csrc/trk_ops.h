@@ -115,19 +115,21 @@ typedef struct {
 #define BD_DZF 71
 #define BD_APC 72
 #define BD_APS 73
-#define BD_E1 74      /* edge angle, tan, psi, kick limit, h (pole curvature) */
+#define BD_E1 74      /* edge angle, tan, psi, kick limit, h (pole curvature), 1/cos */
 #define BD_TE1 75
 #define BD_PSI1 76
 #define BD_LIM1 77
 #define BD_HE1 78
-#define BD_E2 79
-#define BD_TE2 80
-#define BD_PSI2 81
-#define BD_LIM2 82
-#define BD_HE2 83
-#define BD_N 84       /* field index n = -b1/h for order-2 edges */
-#define BD_RHOINV 85  /* 1/rho0 (fast build) */
-#define BD_INVRHOA 86 /* 1/rho_actual (fast build) */
+#define BD_SE1 79
+#define BD_E2 80
+#define BD_TE2 81
+#define BD_PSI2 82
+#define BD_LIM2 83
+#define BD_HE2 84
+#define BD_SE2 85
+#define BD_N 86       /* field index n = -b1/h for order-2 edges */
+#define BD_RHOINV 87  /* 1/rho0 (fast build) */
+#define BD_INVRHOA 88 /* 1/rho_actual (fast build) */
 /* i: 0 nSlices, 1 nSub, 2 field mode (0 dipole, 1 normal, 2 skew), 3 expansionOrder1,
  *    4 field pool offset, 5 edge1 mode, 6 edge2 mode, 7 flags */
 #define EDGE_NONE 0

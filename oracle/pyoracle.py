@@ -48,6 +48,10 @@ def load():
     lib.orc_track_element.argtypes = [P, I, DP, L, L, DP, ctypes.POINTER(L)]
     lib.orc_csbend_field_table.argtypes = [P, I, DP, DP, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)]
     lib.orc_set_exact_sums.argtypes = [I]
+    lib.orc_set_cr_math.argtypes = [I]
+    for f in ('orc_cr_sin', 'orc_cr_cos', 'orc_cr_asin', 'orc_cr_tan'):
+        getattr(lib, f).argtypes = [D]
+        getattr(lib, f).restype = D
     _lib = lib
     return lib
 
@@ -60,6 +64,26 @@ def _check(lib, rc):
 
 def set_exact_sums(on):
     load().orc_set_exact_sums(1 if on else 0)
+
+
+def set_cr_math(on):
+    load().orc_set_cr_math(1 if on else 0)
+
+
+class modes:
+    """Context manager selecting the oracle's summation and libm modes."""
+
+    def __init__(self, exact_sums=False, cr_math=False):
+        self.es, self.cr = exact_sums, cr_math
+
+    def __enter__(self):
+        set_exact_sums(self.es)
+        set_cr_math(self.cr)
+        return self
+
+    def __exit__(self, *exc):
+        set_exact_sums(False)
+        set_cr_math(False)
 
 
 def track(lattice, beam, n_passes, p_central, pass_offset=0):

@@ -698,7 +698,7 @@ static void apply_edge_effects(double *x, double *xp, double *y, double *yp, dou
   double x0, xp0, y0, yp0;
   h = 1 / rho;
   R21 = h * (tan_beta = tan(beta));
-  R43 = -h * tan(beta - psi);
+  R43 = -h * orc_tan_sel(beta - psi);
   h2 = orc_sqr(h);
   T111 = which_edge * h / 2 * (tan2_beta = orc_sqr(tan_beta));
   sec_beta = 1. / cos(beta);
@@ -735,7 +735,7 @@ static void simple_dipole_edge_kick(double *xp, double *yp, double x, double y, 
   dqx = tan(ea) / rho * x;
   if (kickLimit > 0 && fabs(dqx) > kickLimit)
     dqx = SIGN(dqx) * kickLimit;
-  dqy = -tan(ea - psi / (1 + delta)) / rho * y;
+  dqy = -orc_tan_sel(ea - psi / (1 + delta)) / rho * y;
   Qi[1] += dqx;
   Qi[3] += dqy;
   orc_from_dipole_canonical(Qi);
@@ -756,7 +756,7 @@ static void csbend_edge(const orc_csbend_setup *S, int which, double *x, double 
     if (lim > 0 && fabs(delta_xp) > lim)
       delta_xp = SIGN(delta_xp) * lim;
     *xp += delta_xp;
-    *yp -= tan(e - psi / (1 + dp)) / rho * *y;
+    *yp -= orc_tan_sel(e - psi / (1 + dp)) / rho * *y;
   } else if (S->edge_order >= 2 && eff == 1) {
     double rho = (1 + dp) * S->rho_actual;
     apply_edge_effects(x, xp, y, yp, rho, S->n, e, he, psi * (1 + dp), which);
@@ -877,6 +877,11 @@ typedef struct {
  * GPU path computes, for bit-level checks of the downstream arithmetic. */
 static int orc_exact_sums = 0;
 void orc_set_exact_sums(int on) { orc_exact_sums = on; }
+void orc_set_cr_math(int on) { orc_cr_math = on; }
+double orc_cr_sin(double x) { return trkcr_sin(x); }
+double orc_cr_cos(double x) { return trkcr_cos(x); }
+double orc_cr_asin(double x) { return trkcr_asin(x); }
+double orc_cr_tan(double x) { return trkcr_tan(x); }
 
 static void dd_acc(double *hi, double *lo, double v) {
   double s = *hi + v, bb = s - *hi, e = (*hi - (s - bb)) + (v - bb);
@@ -972,7 +977,7 @@ static long rf_cavity(double *coord, long np, const trk_elem *e, orc_rf_state *r
   int same_dgamma = 0;
   double dgamma = 0;
   if (omega == 0 && tau == 0) {
-    dgamma = volt * sin(phase);
+    dgamma = volt * orc_sin_sel(phase);
     same_dgamma = 1;
   }
   double timeOffset = 0;
@@ -999,7 +1004,7 @@ static long rf_cavity(double *coord, long np, const trk_elem *e, orc_rf_state *r
       if (!same_dgamma) {
         double phi = omega * (t - 0 - ik * dtLight) + phase;
         double dfactor = tau ? sqrt(1 - exp(-dt / tau)) : 1;
-        dgamma = volt * sin(phi) * dfactor;
+        dgamma = volt * orc_sin_sel(phi) * dfactor;
       }
       if (length) {
         if (TRK_P(e, RFCA_END1_FOCUS) && ik == 0) {

@@ -38,6 +38,13 @@ int orc_track_element(const trk_lattice *lattice, int element, double *coord, lo
  * rounded once (the GPU path's value) for bit-level checks. */
 void orc_set_exact_sums(int on);
 
+/* 0: libm sin/cos/asin; 1: correctly rounded ones (what the GPU parity build computes). */
+void orc_set_cr_math(int on);
+double orc_cr_sin(double x);
+double orc_cr_cos(double x);
+double orc_cr_asin(double x);
+double orc_cr_tan(double x);
+
 /* Field-expansion table of a CSBEND as the oracle builds it (for tests):
  * Fx, Fy are 11x11 row-major, coefficient of x^i y^j at [i*11+j]. */
 int orc_csbend_field_table(const trk_lattice *lattice, int element, double *Fx, double *Fy, int *expansionOrder1,

@@ -16,14 +16,24 @@
 
 #include <math.h>
 #include "trk_constants.h"
+#include "trk_crmath.h"
+
+/* 0: the C library's sin/cos/asin (as the reference links them);
+ * 1: correctly rounded double-double evaluations (trk_crmath.h), the values a
+ *    correctly rounding libm returns and the GPU parity build computes. */
+static int orc_cr_math = 0;
+static inline double orc_sin_sel(double x) { return orc_cr_math ? trkcr_sin(x) : sin(x); }
+static inline double orc_cos_sel(double x) { return orc_cr_math ? trkcr_cos(x) : cos(x); }
+static inline double orc_asin_sel(double x) { return orc_cr_math ? trkcr_asin(x) : asin(x); }
+static inline double orc_tan_sel(double x) { return orc_cr_math ? trkcr_tan(x) : tan(x); }
 
 #ifndef ORC_R
 #define ORC_R double
 #define ORC_SQRT(x) sqrt(x)
-#define ORC_SIN(x) sin(x)
-#define ORC_COS(x) cos(x)
+#define ORC_SIN(x) orc_sin_sel(x)
+#define ORC_COS(x) orc_cos_sel(x)
 #define ORC_TAN(x) tan(x)
-#define ORC_ASIN(x) asin(x)
+#define ORC_ASIN(x) orc_asin_sel(x)
 #define ORC_FABS(x) fabs(x)
 #define ORC_ISNAN(x) isnan(x)
 #define ORC_ISINF(x) isinf(x)

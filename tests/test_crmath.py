@@ -1,0 +1,86 @@
+"""The correctly rounded sin/cos/asin used by the parity build (and by the
+oracle's CR mode) against 120-digit decimal evaluations, on the argument
+ranges tracking produces: CSBEND substep angles (|x| < 0.01), slopes for
+asin, and RF phases up to 1e6 rad."""
+import math
+from decimal import Decimal, getcontext
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle
+
+getcontext().prec = 130
+
+
+def _pi():
+    def arctan_inv(x):
+        x = Decimal(x)
+        s, t, n, sign, x2 = Decimal(0), 1 / x, 1, 1, x * x
+        while True:
+            term = t / n
+            if term < Decimal(10) ** -125:
+                return s
+            s += sign * term
+            t /= x2
+            n += 2
+            sign = -sign
+    return 4 * (4 * arctan_inv(5) - arctan_inv(239))
+
+
+PI = _pi()
+
+
+def _reduce(x):
+    x = Decimal(x)
+    k = (x / (2 * PI)).to_integral_value()
+    return x - k * 2 * PI
+
+
+def dsin(x):
+    r = _reduce(x)
+    t = s = r
+    n = 1
+    while True:
+        t = -t * r * r / ((2 * n) * (2 * n + 1))
+        n += 1
+        if abs(t) < Decimal(10) ** -120:
+            return s
+        s += t
+
+
+def dcos(x):
+    r = _reduce(x)
+    t = s = Decimal(1)
+    n = 1
+    while True:
+        t = -t * r * r / ((2 * n - 1) * (2 * n))
+        n += 1
+        if abs(t) < Decimal(10) ** -120:
+            return s
+        s += t
+
+
+def dasin(y):
+    y = Decimal(y)
+    a = Decimal(math.asin(float(y)))
+    for _ in range(8):
+        a = a - (dsin(a) - y) / dcos(a)
+    return a
+
+
+def dtan(x):
+    return dsin(x) / dcos(x)
+
+
+@pytest.mark.parametrize("kind,lo,hi", [("sin", -0.01, 0.01), ("cos", -0.01, 0.01), ("sin", -1.5, 1.5), ("tan", -0.3, 0.3),
+                                        ("cos", -3.0, 3.0), ("sin", -1e6, 1e6), ("asin", -0.01, 0.01),
+                                        ("asin", -0.6, 0.6)])
+def test_correct_rounding(kind, lo, hi):
+    lib = pyoracle.load()
+    f = {"sin": lib.orc_cr_sin, "cos": lib.orc_cr_cos, "asin": lib.orc_cr_asin, "tan": lib.orc_cr_tan}[kind]
+    ex = {"sin": dsin, "cos": dcos, "asin": dasin, "tan": dtan}[kind]
+    rng = np.random.Generator(np.random.Philox(7))
+    xs = rng.uniform(lo, hi, 150)
+    bad = [x for x in xs if f(float(x)) != float(ex(float(x)))]
+    assert not bad, f"{kind}: {len(bad)} of {len(xs)} not correctly rounded, e.g. {bad[:3]}"
