@@ -59,7 +59,7 @@ def objects():
     o = os.path.join(BUILD, "trk_lattice.o")
     out.append((src, o, ["gcc", "-std=gnu11", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math"] + INC +
                 ["-c", src, "-o", o]))
-    for extra in ("trk_hooks.cu",):
+    for extra in ("trk_noalloc.cu", "trk_hooks.cu"):
         src = os.path.join(CSRC, extra)
         if os.path.exists(src):
             o = os.path.join(BUILD, extra.replace(".cu", ".o"))

@@ -189,6 +189,38 @@ int trk_track_element(trk_context *ctx, const trk_lattice *lattice, int element,
 int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int n_variants,
                        const long *offsets, const trk_run *run, trk_stats *stats);
 
+/* ------------------------------------------------- allocation-free wake */
+/* No counterpart in the reference: elegant's WAKE (src/wake.c:23-304)
+ * allocates its histograms on every call.
+ *
+ * One WAKE element (time statistics, histogram of N bins, convolution with
+ * the Green function, energy kick; the same kernels as a WAKE in trk_track)
+ * applied to a beam the caller owns on the current device, for callers that
+ * cannot allocate device memory where they track (device memory handed out by
+ * their own pool allocator, or pipelines that cannot take the device-wide
+ * synchronization of cudaMalloc/cudaFree).  It allocates nothing: its scratch
+ * is one static device array of TRK_NOALLOC_SCRATCH_BYTES per GPU that loads
+ * the library, kept until the process exits.  The first call on each device
+ * looks up that array's address (make it before any stream capture).  All
+ * calls share the array and it keeps the last call's contents; calls that
+ * overlap on the GPU race on it.
+ *
+ *   columns[0..5]  device pointers x, x', y, y', s, delta (np each, in/out)
+ *   lost_pass, lost_element  device int32[np] (in/out; < 0 marks survivors);
+ *                  particles that become non-finite are marked with `pass`
+ *   wake_W         device pointer: W(t) at t = i*wake_dt, i < wake_points (V/C)
+ *   n_bins         2..TRK_NOALLOC_MAX_BINS (larger values are rejected)
+ *   macro_charge   charge per macroparticle (C); factor = WAKE FACTOR
+ *   fast_math      0 parity build, 1 fast build; stream = cudaStream_t
+ * Returns TRK_ERR_PHYSICS if the beam is longer than the wake (unless
+ * allow_long_beam), TRK_ERR_ARG for sizes beyond the static limits. */
+#define TRK_NOALLOC_MAX_BINS 8192
+#define TRK_NOALLOC_MAX_BLOCKS 1184
+#define TRK_NOALLOC_SCRATCH_BYTES (256 * 1024)
+int trk_wake_noalloc(double *const *columns, int32_t *lost_pass, int32_t *lost_element, long np, double p_central,
+                     const double *wake_W, long wake_points, double wake_dt, long n_bins, double macro_charge,
+                     double factor, int interpolate, int allow_long_beam, long pass, int fast_math, void *stream);
+
 /* ------------------------------------------------------------- gradients */
 /* Reverse-mode adjoint through the fused element chain.  Loss function:
  *   L = mean_i (x_i^2 + y_i^2) + w_c * (mean_i x_i)^2 + (mean_i y_i)^2 )
