@@ -172,6 +172,8 @@ def main():
     ap.add_argument("--particles", type=int, default=N_PARTICLES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--exact", action="store_true", help="parity build instead of the fast build")
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2"],
+                    help="c2: ring with RF and wake (the benchmark); c1: plain FODO ring (profiling)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -190,7 +192,7 @@ def run_gpu(args, rank, world, local):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     n = args.particles
-    lat = configs.c2_lattice()
+    lat = configs.c2_lattice() if args.workload == "c2" else configs.c1_lattice()
     beam = configs.gaussian_beam(n, seed=1 + rank, first_id=1 + rank * n)
     fast = not args.exact
     flops = load_flops()
@@ -249,7 +251,7 @@ def run_gpu(args, rank, world, local):
     peak = measure_fp64_peak(local)
     roof = None
     if flops:
-        fpt = flops["flops_per_particle_turn"]["c2"]
+        fpt = flops["flops_per_particle_turn"][args.workload]
         achieved = fpt * value / world / 1e12
         roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak if peak else None, "traffic": None,

@@ -41,7 +41,7 @@ class TrackingError(RuntimeError):
 class _Run(ctypes.Structure):
     _fields_ = [("p_central", ctypes.c_double), ("n_passes", ctypes.c_long), ("pass_offset", ctypes.c_long),
                 ("fast_math", ctypes.c_int32), ("block_size", ctypes.c_int32), ("compact_every", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("variant", ctypes.c_int32)]
 
 
 class _Stats(ctypes.Structure):
@@ -279,7 +279,7 @@ class Tracker:
             self._lat_cache[key] = nat
         return nat[1]
 
-    def track(self, lattice, n_passes, p_central, pass_offset=0, fast=True):
+    def track(self, lattice, n_passes, p_central, pass_offset=0, fast=True, variant=-1):
         nat = self.native(lattice)
         run = _Run()
         self.lib.trk_run_defaults(ctypes.byref(run))
@@ -287,6 +287,7 @@ class Tracker:
         run.n_passes = n_passes
         run.pass_offset = pass_offset
         run.fast_math = 1 if fast else 0
+        run.variant = variant
         st = _Stats()
         _check(self.lib, self.lib.trk_track(self.ctx, nat.ptr, ctypes.byref(run), ctypes.byref(st)))
         return Stats(n_total=st.n_total, n_left=st.n_left, particle_passes=st.particle_passes,

@@ -84,6 +84,7 @@ struct trk_context {
   long perm_cap = 0;
   long passes_done = 0; /* passes tracked since the beam was loaded */
   long n_original = 0;  /* particles at the start of the run (do_tracking's nOriginal) */
+  int tuned_variant = 1; /* tracking-kernel variant used when trk_run.variant < 0 */
   int last_launches = 0;
 };
 
@@ -569,6 +570,7 @@ void trk_run_defaults(trk_run *run) {
   run->p_central = 1.0;
   run->n_passes = 1;
   run->fast_math = 1;
+  run->variant = -1;
 }
 
 int trk_context_create(trk_context **out, int device) {
@@ -811,9 +813,9 @@ int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, 
   ctx->last_launches = 0;
   const long p0 = run->pass_offset;
   const long fresh = ctx->passes_done == 0 ? p0 : -1;
-  const int block = run->block_size > 0 ? run->block_size : TRK_BLOCK;
-  if (block != TRK_BLOCK)
-    return trk_set_error(TRK_ERR_ARG, "block_size must be 0 or %d", TRK_BLOCK);
+  int variant = run->variant;
+  if (variant < 0 || variant > 6)
+    variant = ctx->tuned_variant;
   CUDA_TRY(cudaEventRecord(ctx->ev0, ctx->stream));
   if (ctx->np > 0 && run->n_passes > 0 && fresh >= 0) {
     screen_kernel<<<(int)((ctx->np + 255) / 256), 256, 0, ctx->stream>>>(
@@ -824,7 +826,7 @@ int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, 
     TrackArgs ta = track_args(ctx);
     ta.fresh_pass = fresh;
     ta.Po = Po;
-    const int grid = grid_for(ctx, ctx->np, block);
+    const int max_blocks = ctx->sm_count * 256;
     std::vector<Step> steps;
     long pass = p0;
     const long pend = p0 + run->n_passes;
@@ -847,9 +849,9 @@ int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, 
           ta.pass_begin = pass;
           ta.pass_end = pass + npass;
           if (fast)
-            trk_fast::launch_track(ta, grid, block, ctx->stream);
+            trk_fast::launch_track(ta, variant, c.lean, ctx->np, max_blocks, ctx->stream);
           else
-            trk_exact::launch_track(ta, grid, block, ctx->stream);
+            trk_exact::launch_track(ta, variant, c.lean, ctx->np, max_blocks, ctx->stream);
           ctx->last_launches++;
         } else if (st.kind == 1) {
           const trk_op &op = c.ops[st.ob];

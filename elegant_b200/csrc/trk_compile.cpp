@@ -571,6 +571,11 @@ int compile_bend(const trk_lattice *l, int idx, double Po, trk_op *op, std::vect
   d[BD_N] = n;
   d[BD_RHOINV] = 1.0 / rho0;
   d[BD_INVRHOA] = 1.0 / rho_actual;
+  for (int j = 0; j < nSub; j++) {
+    d[BD_SH2 + j] = 2 * d[BD_SH + j];
+    d[BD_C1 + j] = d[BD_DS + j] * d[BD_INVRHOA];
+    d[BD_C2 + j] = d[BD_C1 + j] * d[BD_RHOINV];
+  }
   return TRK_OK;
 }
 
@@ -801,6 +806,26 @@ int trk_compile(const trk_lattice *l, double Po, CompiledLattice &out) {
     }
     if (rc != TRK_OK)
       return rc;
+    /* kinds with a specialized fast-build body (the parity build runs the
+     * general body for them) */
+    if (op.kind == OPK_MULT) {
+      const int f = op.i[6];
+      const int o = op.i[4] & 0xff;
+      if (op.i[1] == 4 && !op.i[2] && op.d[MD_DRIFT] != 0 && o >= 1 && o <= 3 && !(op.i[5] & 1) &&
+          !(f & (MF_KNL1 | MF_KNL2 | MF_XKICK | MF_YKICK | MF_OFFSET | MF_TILT | MF_ENDDRIFT)))
+        op.kind = OPK_MULT1;
+    } else if (op.kind == OPK_BEND) {
+      const bool e1_noop = op.i[5] == EDGE_NONE ||
+                           (op.i[5] == EDGE_LIN1 && op.d[BD_TE1] == 0 && op.d[BD_PSI1] == 0 && op.d[BD_LIM1] <= 0);
+      const bool e2_noop = op.i[6] == EDGE_NONE ||
+                           (op.i[6] == EDGE_LIN1 && op.d[BD_TE2] == 0 && op.d[BD_PSI2] == 0 && op.d[BD_LIM2] <= 0);
+      if (op.i[2] == 0 && op.i[1] == 4 && !(op.i[7] & BF_MISALIGN) && e1_noop && e2_noop)
+        op.kind = OPK_DIPOLE;
+    }
+    if (op.kind != OPK_NOP && op.kind != OPK_DRIFT && op.kind != OPK_EDRIFT && op.kind != OPK_RFDRIFT &&
+        op.kind != OPK_MULT1 && op.kind != OPK_DIPOLE && op.kind != OPK_RF && op.kind != OPK_WAKE &&
+        op.kind != OPK_TRWAKE)
+      out.lean = false;
     if (e->type == TRK_MAXAMP)
       cur_maxamp = i;
     /* aperture state for the first pass of a run and for later passes */
@@ -814,7 +839,7 @@ int trk_compile(const trk_lattice *l, double Po, CompiledLattice &out) {
       const trk_aperture &a = out.aps[ap_of_elem[m]];
       bool active = a.x_max > 0 || a.y_max > 0;
       /* in-element checks (checkMultAperture) only matter with a positive limit */
-      if (active && (op.kind == OPK_MULT || op.kind == OPK_BEND))
+      if (active && (op.kind == OPK_MULT || op.kind == OPK_BEND || op.kind == OPK_MULT1 || op.kind == OPK_DIPOLE))
         op.ap_in[v] = ap_of_elem[m];
       /* after-element limit if (x_max || y_max) (src/do_tracking.c:2508) */
       if (a.x_max || a.y_max)

@@ -32,6 +32,7 @@ struct CompiledLattice {
   int n_rf_slots = 0;
   int n_mult = 0;
   double total_length = 0;
+  bool lean = true; /* every op has a kind the lean kernel variant handles */
 };
 
 int trk_compile(const trk_lattice *l, double Po, CompiledLattice &out);

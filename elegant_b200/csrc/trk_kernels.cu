@@ -51,6 +51,41 @@ struct Part {
 
 __device__ __forceinline__ double sqr(double v) { return v * v; }
 
+#if TRK_FAST
+/* Reciprocal and square root for the fast build: the hardware approximation
+ * (about 20 correct bits) refined by Newton steps, y <- y(2 - xy) for 1/x
+ * and y <- y(3 - x y^2)/2 for 1/sqrt(x), then one correction
+ * s <- s + (x - s^2)/(2 sqrt x) for sqrt(x).  On B200 these agree with IEEE
+ * 1/x and sqrt(x) to within an ulp; they skip the special-value paths, so
+ * callers pass positive normal arguments. */
+__device__ __forceinline__ double rcp_fast(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+
+__device__ __forceinline__ double rsqrt_fast(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  const double h = 0.5 * x;
+  y = y * fma(-h * y, y, 1.5);
+  return y * fma(-h * y, y, 1.5);
+}
+
+__device__ __forceinline__ double sqrt_fast(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  y = y * fma(-0.5 * x * y, y, 1.5);
+  const double s = x * y;
+  const double e = fma(-s, s, x);
+  return x > 0 ? fma(e, 0.5 * y, s) : 0.0;
+}
+
+#endif
+
 __device__ __forceinline__ double ipow_d(double x, int p) {
   if (p == 2)
     return x * x;
@@ -126,12 +161,12 @@ __device__ __forceinline__ bool momenta_to_slopes(double &xp, double &yp, double
   double denom = sqr(1 + delta) - sqr(qx) - sqr(qy);
   if (denom <= 0)
     return false;
-  denom = sqrt(denom);
 #if TRK_FAST
-  double inv = 1.0 / denom;
+  const double inv = rsqrt_fast(denom);
   xp = qx * inv;
   yp = qy * inv;
 #else
+  denom = sqrt(denom);
   xp = qx / denom;
   yp = qy / denom;
 #endif
@@ -184,6 +219,58 @@ __device__ __forceinline__ void mkick(double &qx, double &qy, double x, double y
 
 __device__ __constant__ double c_coef[10]; /* expansion coefficients, orders 0..3 at n(n+1)/2 */
 
+#if TRK_FAST
+/* Fast-build body of integrate_kick_multipole_ordn for one normal multipole
+ * of order ORDER with the 4th-order integrator and no steering kicks: the
+ * four substeps are unrolled, (1+delta)^2 is hoisted and the slope
+ * conversion uses one reciprocal square root.  Returns 0 if the particle
+ * survives the body, 1 for an aperture loss (x, y at the loss point are
+ * reported), 2 for undefined slopes; `done` counts completed drift substeps. */
+template <int ORDER>
+__device__ __forceinline__ int mult_body_fast(const double *__restrict__ d, int n_parts, const trk_aperture *ap,
+                                              bool aptilt, double apc, double aps, double mdx, double mdy, double &x,
+                                              double &xp, double &y, double &yp, double &s, double &qx, double &qy,
+                                              const double dp, int &done) {
+  const double opd2 = (1 + dp) * (1 + dp);
+  done = 0;
+  for (int i_kick = 0; i_kick < n_parts; i_kick++) {
+    if (ap && !check_aperture(x + mdx, y + mdy, ap, aptilt, apc, aps))
+      return 1;
+#pragma unroll
+    for (int step = 0; step < 4; step++) {
+      const double dsh = __ldg(&d[MD_DSH + step]);
+      x = fma(xp, dsh, x);
+      y = fma(yp, dsh, y);
+      s = fma(dsh, sqrt_fast(fma(yp, yp, fma(xp, xp, 1.0))), s);
+      done++;
+      if (step == 3)
+        break;
+      const double K = __ldg(&d[MD_KQ + step * 3]);
+      if (ORDER == 1) {
+        qx = fma(-K, x, qx);
+        qy = fma(K, y, qy);
+      } else if (ORDER == 2) {
+        qx = fma(-K, 0.5 * (x * x - y * y), qx);
+        qy = fma(K, x * y, qy);
+      } else {
+        const double x2 = x * x, y2 = y * y;
+        qx = fma(-K, (x2 * x - 3 * x * y2) * (1.0 / 6), qx);
+        qy = fma(K, (3 * x2 * y - y2 * y) * (1.0 / 6), qy);
+      }
+      const double den = opd2 - qx * qx - qy * qy;
+      if (!(den > 0))
+        return 2;
+      const double r = rsqrt_fast(den);
+      xp = qx * r;
+      yp = qy * r;
+    }
+  }
+  if (ap && !check_aperture(x + mdx, y + mdy, ap, aptilt, apc, aps))
+    return 1;
+  return 0;
+}
+#endif
+
 /* multipole_tracking2 + integrate_kick_multipole_ordn (src/multipole.c:660-1456) */
 __device__ __forceinline__ bool op_mult(const trk_op *__restrict__ op, Part &p, double Po, double z_start,
                                         const trk_aperture *ap) {
@@ -219,14 +306,44 @@ __device__ __forceinline__ bool op_mult(const trk_op *__restrict__ op, Part &p, 
       qx = (1 + dp) * xp;
       qy = (1 + dp) * yp;
     } else {
+#if TRK_FAST
+      const double r = (1 + dp) * rsqrt_fast(1 + sqr(xp) + sqr(yp));
+      qx = xp * r;
+      qy = yp * r;
+#else
       double denom = sqrt(1 + sqr(xp) + sqr(yp));
       qx = (1 + dp) * xp / denom;
       qy = (1 + dp) * yp / denom;
+#endif
     }
     if (!momenta_to_slopes(xp, yp, qx, qy, dp, expand)) {
       ok = false;
       goto done;
     }
+#if TRK_FAST
+    if (nSub == 4 && !expand && drift != 0 && (orders & 0xff) >= 1 && (orders & 0xff) <= 3 && !(skews & 1) &&
+        !(flags & (MF_KNL1 | MF_KNL2 | MF_XKICK | MF_YKICK))) {
+      int done = 0, rc;
+      const int o = orders & 0xff;
+      if (o == 1)
+        rc = mult_body_fast<1>(d, n_parts, ap, aptilt, apc, aps, mdx, mdy, x, xp, y, yp, s, qx, qy, dp, done);
+      else if (o == 2)
+        rc = mult_body_fast<2>(d, n_parts, ap, aptilt, apc, aps, mdx, mdy, x, xp, y, yp, s, qx, qy, dp, done);
+      else
+        rc = mult_body_fast<3>(d, n_parts, ap, aptilt, apc, aps, mdx, mdy, x, xp, y, yp, s, qx, qy, dp, done);
+      for (int k = 0; k < done; k++)
+        dzLoss += __ldg(&d[MD_DSH + (k & 3)]);
+      if (rc) {
+        if (rc == 1) {
+          p.x = x;
+          p.y = y;
+        }
+        ok = false;
+        goto done;
+      }
+      goto body_done;
+    }
+#endif
     for (int i_kick = 0; i_kick < n_parts; i_kick++) {
       if (!check_aperture(x + mdx, y + mdy, ap, aptilt, apc, aps)) {
         p.x = x;
@@ -242,7 +359,11 @@ __device__ __forceinline__ bool op_mult(const trk_op *__restrict__ op, Part &p, 
           if (expand)
             s += dsh * (1 + (sqr(xp) + sqr(yp)) / 2);
           else
+#if TRK_FAST
+            s += dsh * sqrt_fast(1 + sqr(xp) + sqr(yp));
+#else
             s += dsh * sqrt(1 + sqr(xp) + sqr(yp));
+#endif
           dzLoss += dsh;
         }
         if (step == nSub - 1)
@@ -269,6 +390,9 @@ __device__ __forceinline__ bool op_mult(const trk_op *__restrict__ op, Part &p, 
       ok = false;
       goto done;
     }
+#if TRK_FAST
+  body_done:
+#endif
     if (!momenta_to_slopes(xp, yp, qx, qy, dp, expand)) {
       ok = false;
       goto done;
@@ -298,32 +422,125 @@ done:
 }
 
 /* ---------------------------------------------------------------- CSBEND */
-/* computeCSBENDFields (src/csbend.c:99-172) */
+/* computeCSBENDFields (src/csbend.c:99-172): y powers are formed on the fly
+ * (the same products as the reference's yp[] table) so nothing is indexed
+ * in local memory. */
 __device__ __forceinline__ void bend_fields(int mode, int eo1, const double *__restrict__ Fx_xy,
                                             const double *__restrict__ Fy_xy, double x, double y, double &Fx,
                                             double &Fy) {
-  double yp[11];
   double sumFx = 0, sumFy = 0;
-  yp[0] = 1;
-#pragma unroll
-  for (int i = 1; i < 11; i++)
-    yp[i] = (i < eo1) ? yp[i - 1] * y : 0.0;
   double xt = 1;
   for (int i = 0; i < eo1; i++) {
+    double ypj = 1;
     for (int j = 0; j < eo1 - i; j++) {
       if (mode == 2) {
-        sumFx += __ldg(&Fx_xy[i * 11 + j]) * xt * yp[j];
-        sumFy += __ldg(&Fy_xy[i * 11 + j]) * xt * yp[j];
+        sumFx += __ldg(&Fx_xy[i * 11 + j]) * xt * ypj;
+        sumFy += __ldg(&Fy_xy[i * 11 + j]) * xt * ypj;
       } else if (j & 1)
-        sumFx += __ldg(&Fx_xy[i * 11 + j]) * xt * yp[j];
+        sumFx += __ldg(&Fx_xy[i * 11 + j]) * xt * ypj;
       else
-        sumFy += __ldg(&Fy_xy[i * 11 + j]) * xt * yp[j];
+        sumFy += __ldg(&Fy_xy[i * 11 + j]) * xt * ypj;
+      ypj = ypj * y;
     }
     xt *= x;
   }
   Fx = sumFx;
   Fy = sumFy;
 }
+
+#if TRK_FAST
+/* Body of a pure-dipole CSBEND in the fast build.  With no field gradient
+ * QY and delta are constant through the body, so f = sqrt((1+delta)^2-QY^2)
+ * and 1/f are formed once per bend, and Y and the path length grow by QY and
+ * (1+delta) times the same factor each substep, so one running sum F of the
+ * factors gives both.  The drift uses the angle-addition formulas with
+ * tabulated sin/cos of the substep angle a = dsh/rho0 and two
+ * cancellation-free identities:
+ *   tan(a+phi) - tan(phi)     = sin(a) / (cos(a+phi) cos(phi))
+ *   cos(phi)/cos(a+phi) - 1   = 2 sin(a/2+phi) sin(a/2) / cos(a+phi)
+ * so with t = (rho0+X)/cos(a+phi): factor = t sin(a)/f and
+ * X' = X + t 2 sin(a/2) sin(a/2+phi).  The kick is
+ * QX -= ds (1 + X/rho0)/rho_actual.  Loss conditions are the reference's
+ * (f<=0, |QX/f|>1, cos(a+phi)=0, aperture per slice); `done` counts the
+ * completed drift substeps for the loss position. */
+/* One slice of the dipole body; `checked` evaluates the reference's loss
+ * conditions at every substep, otherwise non-finite values are left to
+ * propagate and the caller re-runs the slice checked. */
+template <int NSUB, bool CHECKED>
+__device__ __forceinline__ bool dipole_slice(const double *__restrict__ d, int nSub, double rho0, double f,
+                                             double finv, double &X, double &QX, double &F, int &done) {
+#pragma unroll
+  for (int j = 0; j < (NSUB > 0 ? NSUB : 8); j++) {
+    if (NSUB == 0 && j >= nSub)
+      break;
+    const double sin_phi = QX * finv;
+    if (CHECKED && fabs(sin_phi) > 1)
+      return false;
+    const double cos_phi = sqrt_fast(fma(-sin_phi, sin_phi, 1.0));
+    const double sa = __ldg(&d[BD_SA + j]), ca = __ldg(&d[BD_CA + j]);
+    const double sh = __ldg(&d[BD_SH + j]), ch = __ldg(&d[BD_CH + j]);
+    const double sine = fma(sa, cos_phi, ca * sin_phi);
+    const double cosi = fma(ca, cos_phi, -sa * sin_phi);
+    if (CHECKED && cosi == 0)
+      return false;
+    const double t = (rho0 + X) * rcp_fast(cosi);
+    QX = f * sine;
+    F = fma(t, sa * finv, F);
+    X = fma(t * __ldg(&d[BD_SH2 + j]), fma(sh, cos_phi, ch * sin_phi), X);
+    if (CHECKED)
+      done++;
+    if (j == nSub - 1)
+      break;
+    QX = fma(-__ldg(&d[BD_C2 + j]), X, QX - __ldg(&d[BD_C1 + j]));
+  }
+  return true;
+}
+
+template <int NSUB>
+__device__ __forceinline__ bool bend_dipole_fast(const double *__restrict__ d, int nSlices, int nSub_rt, double rho0,
+                                                 const trk_aperture *ap, bool aptilt, double apc, double aps,
+                                                 double &X, double &QX, double &Y, const double QY, const double D,
+                                                 double &dist, int &done) {
+  const int nSub = NSUB > 0 ? NSUB : nSub_rt;
+  const double opd = 1 + D;
+  const double f2 = opd * opd - QY * QY;
+  const double Y0 = Y;
+  double f = 0, finv = 0, F = 0;
+  if (f2 > 0) {
+    f = sqrt_fast(f2);
+    finv = rcp_fast(f);
+  }
+  bool ok = true;
+  done = 0;
+  for (int i = 0; i < nSlices; i++) {
+    if (ap && !check_aperture(X, Y0 + QY * F, ap, aptilt, apc, aps)) {
+      ok = false;
+      break;
+    }
+    if (!(f2 > 0)) {
+      ok = false;
+      break;
+    }
+    const double X0 = X, QX0 = QX, F0 = F;
+    dipole_slice<NSUB, false>(d, nSub, rho0, f, finv, X, QX, F, done);
+    if (!isfinite(X + QX + F)) {
+      /* a loss condition may have fired: redo the slice with the checks */
+      X = X0;
+      QX = QX0;
+      F = F0;
+      if (!dipole_slice<NSUB, true>(d, nSub, rho0, f, finv, X, QX, F, done)) {
+        ok = false;
+        break;
+      }
+      done -= nSub;
+    }
+    done += nSub;
+  }
+  Y = Y0 + QY * F;
+  dist = opd * F;
+  return ok;
+}
+#endif
 
 /* apply_edge_effects (src/csbend.c:4291-4333) */
 __device__ void edge_order2(double &x, double &xp, double &y, double &yp, double rho, double n, double beta,
@@ -449,6 +666,18 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
   bool ok = true;
   double dist = 0, dz_lost = 0;
   const double sl = __ldg(&d[BD_SLICE]);
+#if TRK_FAST
+  if (fmode == 0) {
+    int done = 0;
+    if (nSub == 4)
+      ok = bend_dipole_fast<4>(d, nSlices, nSub, rho0, ap, aptilt, apc, aps, X, QX, Y, QY, D, dist, done);
+    else
+      ok = bend_dipole_fast<0>(d, nSlices, nSub, rho0, ap, aptilt, apc, aps, X, QX, Y, QY, D, dist, done);
+    if (!ok) /* loss position: the drift substeps completed so far */
+      for (int k = 0; k < done; k++)
+        dz_lost += __ldg(&d[BD_DSH + k % nSub]);
+  } else
+#endif
   for (int i = 0; i < nSlices && ok; i++) {
     if (!check_aperture(X, Y, ap, aptilt, apc, aps)) {
       ok = false;
@@ -703,6 +932,269 @@ __device__ __forceinline__ bool op_rf(const trk_op *__restrict__ op, Part &p, do
   return true;
 }
 
+#if TRK_FAST
+/* OPK_MULT1 in the fast build: multipole_tracking2 for one normal multipole
+ * with no misalignment, steering or end drifts (src/multipole.c:660-1084),
+ * body unrolled by mult_body_fast.  The slope->momentum->slope round trip of
+ * the reference before the body (src/multipole.c:1190-1228) is an identity
+ * in exact arithmetic and is skipped. */
+__device__ __forceinline__ bool op_mult1_fast(const trk_op *__restrict__ op, Part &p, double Po, double z_start,
+                                              const trk_aperture *ap) {
+  const int n_parts = __ldg(&op->i[0]);
+  const int order = __ldg(&op->i[4]) & 0xff;
+  const int flags = __ldg(&op->i[6]);
+  const double *d = op->d;
+  const bool aptilt = (flags & MF_APTILT) != 0;
+  const double apc = __ldg(&d[MD_APC]), aps = __ldg(&d[MD_APS]);
+  double x = p.x, xp = p.xp, y = p.y, yp = p.yp, s = 0;
+  const double dp = p.dp;
+  double dzLoss = 0;
+  bool ok = !(isnan(x) || isnan(xp) || isnan(y) || isnan(yp) || fabs(x) > TRK_COORD_LIMIT ||
+              fabs(y) > TRK_COORD_LIMIT || fabs(xp) > TRK_SLOPE_LIMIT || fabs(yp) > TRK_SLOPE_LIMIT);
+  if (ok) {
+    const double r = (1 + dp) * rsqrt_fast(fma(yp, yp, fma(xp, xp, 1.0)));
+    double qx = xp * r, qy = yp * r;
+    int done = 0, rc;
+    if (order == 1)
+      rc = mult_body_fast<1>(d, n_parts, ap, aptilt, apc, aps, 0.0, 0.0, x, xp, y, yp, s, qx, qy, dp, done);
+    else if (order == 2)
+      rc = mult_body_fast<2>(d, n_parts, ap, aptilt, apc, aps, 0.0, 0.0, x, xp, y, yp, s, qx, qy, dp, done);
+    else
+      rc = mult_body_fast<3>(d, n_parts, ap, aptilt, apc, aps, 0.0, 0.0, x, xp, y, yp, s, qx, qy, dp, done);
+    if (rc) {
+      for (int k = 0; k < done; k++)
+        dzLoss += __ldg(&d[MD_DSH + (k & 3)]);
+      if (rc == 1) {
+        p.x = x;
+        p.y = y;
+      }
+      ok = false;
+    } else {
+      const double den = (1 + dp) * (1 + dp) - qx * qx - qy * qy;
+      if (!(den > 0)) {
+        for (int k = 0; k < done; k++)
+          dzLoss += __ldg(&d[MD_DSH + (k & 3)]);
+        ok = false;
+      } else {
+        const double ri = rsqrt_fast(den);
+        xp = qx * ri;
+        yp = qy * ri;
+        p.x = x;
+        p.xp = xp;
+        p.y = y;
+        p.yp = yp;
+        p.s += s;
+        p.dp = dp;
+        if (isnan(x) || isnan(xp) || isnan(y) || isnan(yp) || fabs(x) > TRK_COORD_LIMIT ||
+            fabs(y) > TRK_COORD_LIMIT || fabs(xp) > TRK_SLOPE_LIMIT || fabs(yp) > TRK_SLOPE_LIMIT) {
+          for (int k = 0; k < done; k++)
+            dzLoss += __ldg(&d[MD_DSH + (k & 3)]);
+          ok = false;
+        }
+      }
+    }
+  }
+  if (!ok) {
+    p.s = z_start + dzLoss;
+    p.dp = Po * (1 + p.dp);
+  }
+  return ok;
+}
+
+/* OPK_DIPOLE in the fast build: track_through_csbend for a pure dipole with
+ * no misalignment and no edge kick (src/csbend.c:654-1434), body by
+ * bend_dipole_fast. */
+__device__ __forceinline__ bool op_dipole_fast(const trk_op *__restrict__ op, Part &p, double Po, double z_start,
+                                               const trk_aperture *ap) {
+  const double *d = op->d;
+  const int nSlices = __ldg(&op->i[0]);
+  const double rho0 = __ldg(&d[BD_RHO0]);
+  const double D = p.dp;
+  const double r = (1 + D) * rsqrt_fast(fma(p.yp, p.yp, fma(p.xp, p.xp, 1.0)));
+  double X = p.x, Y = p.y, QX = p.xp * r;
+  const double QY = p.yp * r;
+  double dist = 0;
+  int done = 0;
+  bool ok = bend_dipole_fast<4>(d, nSlices, 4, rho0, ap, false, 1.0, 0.0, X, QX, Y, QY, D, dist, done);
+  double dz_lost = 0;
+  if (ok) {
+    dz_lost = nSlices * __ldg(&d[BD_SLICE]);
+    if (ap && !check_aperture(X, Y, ap, false, 1.0, 0.0))
+      ok = false;
+  } else
+    for (int k = 0; k < done; k++)
+      dz_lost += __ldg(&d[BD_DSH + (k & 3)]);
+  const double f = rsqrt_fast((1 + D) * (1 + D) - QX * QX - QY * QY);
+  p.x = X;
+  p.y = Y;
+  p.xp = QX * f;
+  p.yp = QY * f;
+  if (!ok) {
+    p.s = z_start + dz_lost;
+    p.dp = Po * (1 + D);
+    return false;
+  }
+  p.s += dist;
+  p.dp = D;
+  return true;
+}
+
+/* Two particles through one pure dipole with their substep chains
+ * interleaved: the body of each particle is a serial dependency chain
+ * (sqrt -> reciprocal -> update), so a thread that carries two independent
+ * chains keeps the FP64 pipe busier at the same occupancy.  Same arithmetic
+ * per particle as op_dipole_fast; a slice that produced a non-finite value is
+ * re-run for that particle with the reference's per-substep loss checks. */
+struct DipoleState {
+  double X, QX, F, QY, Y0, opd, f, finv;
+  double f2;
+  int done;
+  bool ok;
+};
+
+__device__ __forceinline__ void dipole_begin(DipoleState &q, const Part &p) {
+  q.opd = 1 + p.dp;
+  const double r = q.opd * rsqrt_fast(fma(p.yp, p.yp, fma(p.xp, p.xp, 1.0)));
+  q.X = p.x;
+  q.Y0 = p.y;
+  q.QX = p.xp * r;
+  q.QY = p.yp * r;
+  q.F = 0;
+  q.f2 = q.opd * q.opd - q.QY * q.QY;
+  q.f = 0;
+  q.finv = 0;
+  if (q.f2 > 0) {
+    q.f = sqrt_fast(q.f2);
+    q.finv = rcp_fast(q.f);
+  }
+  q.done = 0;
+}
+
+__device__ __forceinline__ void dipole_step(DipoleState &q, double rho0, double sa, double ca, double sh, double ch,
+                                            double sh2) {
+  const double sin_phi = q.QX * q.finv;
+  const double cos_phi = sqrt_fast(fma(-sin_phi, sin_phi, 1.0));
+  const double sine = fma(sa, cos_phi, ca * sin_phi);
+  const double cosi = fma(ca, cos_phi, -sa * sin_phi);
+  const double t = (rho0 + q.X) * rcp_fast(cosi);
+  q.QX = q.f * sine;
+  q.F = fma(t, sa * q.finv, q.F);
+  q.X = fma(t * sh2, fma(sh, cos_phi, ch * sin_phi), q.X);
+}
+
+__device__ __forceinline__ bool dipole_finish(DipoleState &q, Part &p, const double *__restrict__ d, int nSlices,
+                                              double Po, double z_start, const trk_aperture *ap) {
+  double dz_lost = 0;
+  const double Y = q.Y0 + q.QY * q.F;
+  bool ok = q.ok;
+  if (ok) {
+    dz_lost = nSlices * __ldg(&d[BD_SLICE]);
+    if (ap && !check_aperture(q.X, Y, ap, false, 1.0, 0.0))
+      ok = false;
+  } else
+    for (int k = 0; k < q.done; k++)
+      dz_lost += __ldg(&d[BD_DSH + (k & 3)]);
+  const double f = rsqrt_fast(q.opd * q.opd - q.QX * q.QX - q.QY * q.QY);
+  p.x = q.X;
+  p.y = Y;
+  p.xp = q.QX * f;
+  p.yp = q.QY * f;
+  if (!ok) {
+    p.s = z_start + dz_lost;
+    p.dp = Po * q.opd; /* Po * (1 + delta) */
+    return false;
+  }
+  p.s += q.opd * q.F;
+  return true;
+}
+
+/* one slice for one particle with the reference's loss checks (rare path) */
+__device__ __noinline__ void dipole_slice_checked(DipoleState &q, const double *__restrict__ d, double rho0) {
+  double X = q.X, QX = q.QX, F = q.F;
+  int done = q.done;
+  q.ok = dipole_slice<4, true>(d, 4, rho0, q.f, q.finv, X, QX, F, done);
+  q.X = X;
+  q.QX = QX;
+  q.F = F;
+  q.done = done;
+}
+
+__device__ __forceinline__ void op_dipole_fast2(const trk_op *__restrict__ op, Part &p0, Part &p1, bool &ok0,
+                                                bool &ok1, double Po, double z_start, const trk_aperture *ap) {
+  const double *d = op->d;
+  const int nSlices = __ldg(&op->i[0]);
+  const double rho0 = __ldg(&d[BD_RHO0]);
+  DipoleState q0, q1;
+  dipole_begin(q0, p0);
+  dipole_begin(q1, p1);
+  q0.ok = ok0;
+  q1.ok = ok1;
+  for (int i = 0; i < nSlices; i++) {
+    if (ap) {
+      if (q0.ok && !check_aperture(q0.X, q0.Y0 + q0.QY * q0.F, ap, false, 1.0, 0.0))
+        q0.ok = false;
+      if (q1.ok && !check_aperture(q1.X, q1.Y0 + q1.QY * q1.F, ap, false, 1.0, 0.0))
+        q1.ok = false;
+    }
+    if (!(q0.f2 > 0))
+      q0.ok = false;
+    if (!(q1.f2 > 0))
+      q1.ok = false;
+    if (!q0.ok && !q1.ok)
+      break;
+    const double X0a = q0.X, QX0a = q0.QX, F0a = q0.F;
+    const double X0b = q1.X, QX0b = q1.QX, F0b = q1.F;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const double sa = __ldg(&d[BD_SA + j]), ca = __ldg(&d[BD_CA + j]);
+      const double sh = __ldg(&d[BD_SH + j]), ch = __ldg(&d[BD_CH + j]);
+      const double sh2 = __ldg(&d[BD_SH2 + j]);
+      dipole_step(q0, rho0, sa, ca, sh, ch, sh2);
+      dipole_step(q1, rho0, sa, ca, sh, ch, sh2);
+      if (j == 3)
+        break;
+      const double c1 = __ldg(&d[BD_C1 + j]), c2 = __ldg(&d[BD_C2 + j]);
+      q0.QX = fma(-c2, q0.X, q0.QX - c1);
+      q1.QX = fma(-c2, q1.X, q1.QX - c1);
+    }
+    if (q0.ok) {
+      if (isfinite(q0.X + q0.QX + q0.F))
+        q0.done += 4;
+      else {
+        q0.X = X0a;
+        q0.QX = QX0a;
+        q0.F = F0a;
+        dipole_slice_checked(q0, d, rho0);
+      }
+    } else {
+      /* lost: keep the coordinates where the loss was found */
+      q0.X = X0a;
+      q0.QX = QX0a;
+      q0.F = F0a;
+    }
+    if (q1.ok) {
+      if (isfinite(q1.X + q1.QX + q1.F))
+        q1.done += 4;
+      else {
+        q1.X = X0b;
+        q1.QX = QX0b;
+        q1.F = F0b;
+        dipole_slice_checked(q1, d, rho0);
+      }
+    } else {
+      /* lost: keep the coordinates where the loss was found */
+      q1.X = X0b;
+      q1.QX = QX0b;
+      q1.F = F0b;
+    }
+  }
+  if (ok0)
+    ok0 = dipole_finish(q0, p0, d, nSlices, Po, z_start, ap);
+  if (ok1)
+    ok1 = dipole_finish(q1, p1, d, nSlices, Po, z_start, ap);
+}
+#endif
+
 /* ------------------------------------------------------ after-element */
 /* limit_amplitudes / elimit_amplitudes (src/limit_amplitudes.c:197-288,
  * 487-~620) for one particle; returns true if lost. */
@@ -823,6 +1315,7 @@ __device__ __forceinline__ void store_part(const TrackArgs &a, long i, const Par
 
 /* Track one particle through ops [ob, oe) for passes [pb, pe).  Returns
  * false if it was lost (loss recorded). */
+template <bool LEAN>
 __device__ __forceinline__ bool track_particle(const TrackArgs &a, Part &p, long i) {
   for (long pass = a.pass_begin; pass < a.pass_end; pass++) {
     const int var = (pass == a.fresh_pass) ? 0 : 1;
@@ -838,19 +1331,33 @@ __device__ __forceinline__ bool track_particle(const TrackArgs &a, Part &p, long
         op_drift(op, p);
         break;
       case OPK_EDRIFT:
-        exact_drift(p, __ldg(&op->d[DD_L]));
-        break;
       case OPK_RFDRIFT:
         exact_drift(p, __ldg(&op->d[DD_L]));
         break;
-      case OPK_MULT:
+      case OPK_MULT1:
+#if TRK_FAST
+        ok = op_mult1_fast(op, p, a.Po, z_start, ap_in);
+#else
         ok = op_mult(op, p, a.Po, z_start, ap_in);
+#endif
         break;
-      case OPK_BEND:
+      case OPK_DIPOLE:
+#if TRK_FAST
+        ok = op_dipole_fast(op, p, a.Po, z_start, ap_in);
+#else
         ok = op_bend(op, p, a.Po, z_start, ap_in, a.field);
+#endif
         break;
       case OPK_RF:
         ok = op_rf(op, p, a.Po, z_end, a.rf_phase);
+        break;
+      case OPK_MULT:
+        if (!LEAN)
+          ok = op_mult(op, p, a.Po, z_start, ap_in);
+        break;
+      case OPK_BEND:
+        if (!LEAN)
+          ok = op_bend(op, p, a.Po, z_start, ap_in, a.field);
         break;
       default:
         break;
@@ -875,17 +1382,116 @@ __device__ __forceinline__ bool track_particle(const TrackArgs &a, Part &p, long
   return true;
 }
 
-__global__ void __launch_bounds__(TRK_BLOCK) track_kernel(TrackArgs a) {
+/* Kernel variants (block size, minimum resident blocks per SM) trade
+ * registers against occupancy; trk_run.variant or the autotuner picks one. */
+template <int BLOCK, int MINB, bool LEAN>
+__global__ void __launch_bounds__(BLOCK, MINB) track_kernel(TrackArgs a) {
   const long stride = (long)gridDim.x * blockDim.x;
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
     if (a.lost_pass[i] >= 0)
       continue;
     Part p;
     load_part(a, i, p);
-    track_particle(a, p, i);
+    track_particle<LEAN>(a, p, i);
     store_part(a, i, p);
   }
 }
+
+#if TRK_FAST
+/* after-element filters and loss record of one particle (as in
+ * track_particle) */
+__device__ __forceinline__ bool after_element(const TrackArgs &a, const trk_op *__restrict__ op, int var, Part &p,
+                                              bool ok, long i, long pass) {
+  const double z_end = __ldg(&op->z_end);
+  if (ok && !__ldg(&op->no_aperture)) {
+    const int apo = __ldg(&op->ap_post[var]);
+    if (apo >= 0)
+      ok = !post_aperture(p, a.aps + apo, __ldg(&op->extrapolate), z_end, a.Po);
+  }
+  if (ok && (isinf(p.x) || isinf(p.y) || isnan(p.x) || isnan(p.y))) {
+    p.s = z_end;
+    p.dp = a.Po * (1 + p.dp);
+    ok = false;
+  }
+  if (!ok) {
+    a.lost_pass[i] = (int32_t)pass;
+    a.lost_elem[i] = __ldg(&op->elem);
+  }
+  return ok;
+}
+
+__device__ __forceinline__ bool lean_op(const TrackArgs &a, const trk_op *__restrict__ op, int kind, Part &p,
+                                        const trk_aperture *ap_in) {
+  const double z_start = __ldg(&op->z_start);
+  switch (kind) {
+  case OPK_DRIFT:
+    op_drift(op, p);
+    return true;
+  case OPK_EDRIFT:
+  case OPK_RFDRIFT:
+    exact_drift(p, __ldg(&op->d[DD_L]));
+    return true;
+  case OPK_MULT1:
+    return op_mult1_fast(op, p, a.Po, z_start, ap_in);
+  case OPK_DIPOLE:
+    return op_dipole_fast(op, p, a.Po, z_start, ap_in);
+  case OPK_RF:
+    return op_rf(op, p, a.Po, __ldg(&op->z_end), a.rf_phase);
+  default:
+    return true;
+  }
+}
+
+/* Two particles per thread (lean lattices, fast build): particles i and
+ * i + BLOCK of the block's tile. */
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) track_kernel2(TrackArgs a) {
+  const long tile = 2L * BLOCK;
+  for (long base = (long)blockIdx.x * tile; base < a.n; base += (long)gridDim.x * tile) {
+    const long i0 = base + threadIdx.x, i1 = i0 + BLOCK;
+    bool al0 = i0 < a.n && a.lost_pass[i0] < 0;
+    bool al1 = i1 < a.n && a.lost_pass[i1] < 0;
+    if (!al0 && !al1)
+      continue;
+    Part p0, p1;
+    if (al0)
+      load_part(a, i0, p0);
+    else
+      p0 = Part{0, 0, 0, 0, 0, 0};
+    if (al1)
+      load_part(a, i1, p1);
+    else
+      p1 = Part{0, 0, 0, 0, 0, 0};
+    const bool was0 = al0, was1 = al1;
+    for (long pass = a.pass_begin; pass < a.pass_end && (al0 || al1); pass++) {
+      const int var = (pass == a.fresh_pass) ? 0 : 1;
+      for (int k = a.op_begin; k < a.op_end && (al0 || al1); k++) {
+        const trk_op *op = a.ops + k;
+        const int kind = __ldg(&op->kind);
+        const int api = __ldg(&op->ap_in[var]);
+        const trk_aperture *ap_in = api >= 0 ? a.aps + api : nullptr;
+        bool ok0 = al0, ok1 = al1;
+        if (kind == OPK_DIPOLE) {
+          op_dipole_fast2(op, p0, p1, ok0, ok1, a.Po, __ldg(&op->z_start), ap_in);
+        } else {
+          if (al0)
+            ok0 = lean_op(a, op, kind, p0, ap_in);
+          if (al1)
+            ok1 = lean_op(a, op, kind, p1, ap_in);
+        }
+        if (al0)
+          al0 = after_element(a, op, var, p0, ok0, i0, pass);
+        if (al1)
+          al1 = after_element(a, op, var, p1, ok1, i1, pass);
+      }
+    }
+    if (was0)
+      store_part(a, i0, p0);
+    if (was1)
+      store_part(a, i1, p1);
+  }
+}
+#endif
 
 /* computeTimeCoordinatesOnly (src/trwake.c:519-527), rounded step by step
  * in both builds so the statistics, binning and kick kernels agree. */
@@ -1235,8 +1841,65 @@ __global__ void rotate_kernel(TrackArgs a, double ca, double sa) {
 }
 
 /* ------------------------------------------------------------- launchers */
-void launch_track(const TrackArgs &a, int grid, int block, cudaStream_t st) {
-  track_kernel<<<grid, block, 0, st>>>(a);
+int track_variant_block(int variant) {
+  switch (variant) {
+  case 2:
+    return 256;
+  case 3:
+    return 64;
+  default:
+    return 128;
+  }
+}
+
+template <bool LEAN>
+static void launch_track_t(const TrackArgs &a, int variant, int grid, int block, cudaStream_t st) {
+  switch (variant) {
+  case 1:
+    track_kernel<128, 4, LEAN><<<grid, block, 0, st>>>(a);
+    break;
+  case 2:
+    track_kernel<256, 2, LEAN><<<grid, block, 0, st>>>(a);
+    break;
+  case 3:
+    track_kernel<64, 8, LEAN><<<grid, block, 0, st>>>(a);
+    break;
+  case 4:
+    track_kernel<128, 5, LEAN><<<grid, block, 0, st>>>(a);
+    break;
+  default:
+    track_kernel<128, 1, LEAN><<<grid, block, 0, st>>>(a);
+    break;
+  }
+}
+
+void launch_track(const TrackArgs &a, int variant, bool lean, long n, int max_blocks, cudaStream_t st) {
+#if TRK_FAST
+  if (lean && (variant == 5 || variant == 6)) {
+    long g = (n + 2 * 128 - 1) / (2 * 128);
+    if (g < 1)
+      g = 1;
+    if (g > max_blocks)
+      g = max_blocks;
+    if (variant == 5)
+      track_kernel2<128, 3><<<(int)g, 128, 0, st>>>(a);
+    else
+      track_kernel2<128, 2><<<(int)g, 128, 0, st>>>(a);
+    return;
+  }
+#endif
+  if (variant >= 5)
+    variant = 1;
+  const int block = track_variant_block(variant);
+  long g = (n + block - 1) / block;
+  if (g < 1)
+    g = 1;
+  if (g > max_blocks)
+    g = max_blocks;
+  if (lean)
+    launch_track_t<true>(a, variant, (int)g, block, st);
+  else
+    launch_track_t<false>(a, variant, (int)g, block, st);
 }
 
 void launch_time_stats(const TimeStatsArgs &a, int grid, cudaStream_t st) {

@@ -92,7 +92,8 @@ struct WakeArgs {
 
 #define TRK_DECLARE_LAUNCHERS(NS)                                                                            \
   namespace NS {                                                                                             \
-  void launch_track(const TrackArgs &a, int grid, int block, cudaStream_t st);                               \
+  int track_variant_block(int variant);                                                                      \
+  void launch_track(const TrackArgs &a, int variant, bool lean, long n, int max_blocks, cudaStream_t st);    \
   void launch_time_stats(const TimeStatsArgs &a, int grid, cudaStream_t st);                                 \
   void launch_rf_fiducial(const double *stats, double omega, double t_reference, double *rf_phase, int slot, \
                           int *status, cudaStream_t st);                                                     \

@@ -26,7 +26,11 @@ enum trk_op_kind {
   OPK_RF = 5,     /* RFCA */
   OPK_WAKE = 6,   /* WAKE (collective: ends a fused segment) */
   OPK_TRWAKE = 7, /* TRWAKE (collective) */
-  OPK_RFDRIFT = 8 /* RFCA with VOLT=0: drift of length L */
+  OPK_RFDRIFT = 8, /* RFCA with VOLT=0: drift of length L */
+  OPK_MULT1 = 9,   /* KQUAD/KSEXT/KOCT with one normal multipole, 4th-order integrator, no
+                      misalignment, steering or end drifts (specialized fast-build body) */
+  OPK_DIPOLE = 10  /* CSBEND: pure dipole, 4th-order integrator, no misalignment, edge kicks
+                      that are exact no-ops (E=0, no fringe) or absent (specialized fast-build body) */
 };
 
 /* multipole flags (i[6]) */
@@ -130,6 +134,9 @@ typedef struct {
 #define BD_N 86       /* field index n = -b1/h for order-2 edges */
 #define BD_RHOINV 87  /* 1/rho0 (fast build) */
 #define BD_INVRHOA 88 /* 1/rho_actual (fast build) */
+#define BD_SH2 89     /* 8 values 2 sin(dsh/(2 rho0)) (fast build) */
+#define BD_C1 97      /* 8 values ds/rho_actual (fast build kick) */
+#define BD_C2 105     /* 8 values ds/(rho_actual rho0) (fast build kick) */
 /* i: 0 nSlices, 1 nSub, 2 field mode (0 dipole, 1 normal, 2 skew), 3 expansionOrder1,
  *    4 field pool offset, 5 edge1 mode, 6 edge2 mode, 7 flags */
 #define EDGE_NONE 0

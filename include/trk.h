@@ -123,9 +123,9 @@ typedef struct {
   long pass_offset;      /* index of the first pass (wake ramps, RF fiducial on pass 0) */
   int32_t fast_math;     /* 0: reference operation order, no FMA contraction (parity build);
                             1: transcendental-free CSBEND drift and FMA (fast build) */
-  int32_t block_size;    /* 0 = autotuned */
+  int32_t block_size;    /* unused, kept 0 (block shape comes with the variant) */
   int32_t compact_every; /* compact survivors every N passes in fused runs (0 = never) */
-  int32_t reserved;
+  int32_t variant;       /* tracking-kernel variant (block size x occupancy); -1 = autotuned choice */
 } trk_run;
 
 void trk_run_defaults(trk_run *run);

@@ -6,9 +6,9 @@ from elegant_b200 import Lattice, Tracker  # noqa: F401
 from oracle import pyoracle
 
 
-def gpu_run(tracker, lattice, beam, n_passes, p_central, fast, pass_offset=0):
+def gpu_run(tracker, lattice, beam, n_passes, p_central, fast, pass_offset=0, variant=-1):
     tracker.load(beam)
-    stats = tracker.track(lattice, n_passes, p_central, pass_offset=pass_offset, fast=fast)
+    stats = tracker.track(lattice, n_passes, p_central, pass_offset=pass_offset, fast=fast, variant=variant)
     n_left, out, lp, le = tracker.store(stride=7, with_loss=True)
     return n_left, out, lp, le, stats
 

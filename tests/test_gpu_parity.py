@@ -128,6 +128,28 @@ def test_fodo_ring_fast_one_turn(tracker):
     assert r["max_err"] < 2e-8, r
 
 
+@pytest.mark.parametrize("variant", range(7))
+def test_kernel_variants_fast_losses(tracker, variant):
+    """Every launch shape of the fast tracking kernel (one and two particles
+    per thread) against the oracle on a lossy ring: same survivors, same loss
+    pass and element, coordinates within the fast build's bound."""
+    lat = Lattice()
+    lat.add("MAXAMP", "AP", X_MAX=0.004, Y_MAX=0.003, ELLIPTICAL=1)
+    lat.extend(configs.c1_lattice(cells=4))
+    beam = configs.gaussian_beam(3001, seed=9, sigma_x=2e-3, sigma_xp=2e-4)
+    nl, g, lp, le, _ = gpu_run(tracker, lat, beam, 2, PC, fast=True, variant=variant)
+    with pyoracle.modes(exact_sums=True, cr_math=True):
+        rows, nlo, _ = oracle_run(lat, beam, 2, PC)
+    r = compare(g, rows, nl, nlo)
+    assert nlo < beam.shape[0]
+    assert r["same_survivors"] and r["max_err"] < 2e-8, r
+    o = rows[np.argsort(rows[:, 6])]
+    lost = o[:, 7] >= 0
+    gi = np.argsort(g[:, 6])
+    assert np.array_equal(lp[gi][lost], o[lost, 7].astype(np.int64))
+    assert np.array_equal(le[gi][lost], o[lost, 8].astype(np.int32))
+
+
 def test_losses_rect_aperture_exact(tracker):
     lat = Lattice()
     lat.add("MAXAMP", "AP", X_MAX=0.004, Y_MAX=0.003)
