@@ -84,7 +84,7 @@ struct trk_context {
   long perm_cap = 0;
   long passes_done = 0; /* passes tracked since the beam was loaded */
   long n_original = 0;  /* particles at the start of the run (do_tracking's nOriginal) */
-  int tuned_variant = 1; /* tracking-kernel variant used when trk_run.variant < 0 */
+  int tuned_variant = -1; /* tracking-kernel variant used when trk_run.variant < 0 (-1: by lattice class) */
   int last_launches = 0;
 };
 
@@ -814,8 +814,12 @@ int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, 
   const long p0 = run->pass_offset;
   const long fresh = ctx->passes_done == 0 ? p0 : -1;
   int variant = run->variant;
-  if (variant < 0 || variant > 6)
+  if (variant < 0 || variant >= TRK_N_VARIANTS)
     variant = ctx->tuned_variant;
+  if (variant < 0)
+    /* measured on B200: (128 threads, 6 blocks/SM) for lean lattices in the
+     * fast build (80 registers), (128, 4) otherwise */
+    variant = (fast && c.lean) ? 7 : 1;
   CUDA_TRY(cudaEventRecord(ctx->ev0, ctx->stream));
   if (ctx->np > 0 && run->n_passes > 0 && fresh >= 0) {
     screen_kernel<<<(int)((ctx->np + 255) / 256), 256, 0, ctx->stream>>>(

@@ -572,7 +572,7 @@ int compile_bend(const trk_lattice *l, int idx, double Po, trk_op *op, std::vect
   d[BD_RHOINV] = 1.0 / rho0;
   d[BD_INVRHOA] = 1.0 / rho_actual;
   for (int j = 0; j < nSub; j++) {
-    d[BD_SH2 + j] = 2 * d[BD_SH + j];
+    d[BD_OMC + j] = 2 * d[BD_SH + j] * d[BD_SH + j];
     d[BD_C1 + j] = d[BD_DS + j] * d[BD_INVRHOA];
     d[BD_C2 + j] = d[BD_C1 + j] * d[BD_RHOINV];
   }

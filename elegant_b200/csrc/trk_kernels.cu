@@ -18,10 +18,12 @@
  * boundaries need it, and no dense contraction exists for the tensor cores.
  */
 #include <cuda_runtime.h>
+#include <stddef.h>
 #include <stdint.h>
 
 #include "trk_constants.h"
 #include "trk_crmath.h"
+
 #include "trk_kernels.h"
 #include "trk_ops.h"
 
@@ -53,36 +55,39 @@ __device__ __forceinline__ double sqr(double v) { return v * v; }
 
 #if TRK_FAST
 /* Reciprocal and square root for the fast build: the hardware approximation
- * (about 20 correct bits) refined by Newton steps, y <- y(2 - xy) for 1/x
- * and y <- y(3 - x y^2)/2 for 1/sqrt(x), then one correction
- * s <- s + (x - s^2)/(2 sqrt x) for sqrt(x).  On B200 these agree with IEEE
- * 1/x and sqrt(x) to within an ulp; they skip the special-value paths, so
- * callers pass positive normal arguments. */
+ * y0 (about 20 correct bits) and one third-order correction from the series
+ *   1/x       = y0 / (1 - e)       = y0 (1 + e + e^2 + ...),   e = 1 - x y0
+ *   1/sqrt(x) = y0 (1 + r)^(-1/2)  = y0 (1 - r/2 + 3 r^2/8 - ...),  r = x y0^2 - 1
+ * truncated after the quadratic term (remainder ~e^3, r^3 ~ 2^-60), and
+ * sqrt(x) = (x y0)(1 + r)^(-1/2) with r formed from the rounded product
+ * x y0, so its rounding cancels to first order.  Results agree with IEEE
+ * 1/x and sqrt(x) to within an ulp.  There are no special-value paths:
+ * callers pass positive normal arguments, except that sqrt_fast returns 0
+ * for x <= 0 (as the reference's conditions need) and sqrt_nan returns NaN
+ * for x <= 0. */
 __device__ __forceinline__ double rcp_fast(double x) {
   double y;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-  double e = fma(-x, y, 1.0);
-  y = fma(y, e, y);
-  e = fma(-x, y, 1.0);
-  return fma(y, e, y);
+  const double e = fma(-x, y, 1.0);
+  return fma(y, fma(e, e, e), y);
 }
 
 __device__ __forceinline__ double rsqrt_fast(double x) {
   double y;
   asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-  const double h = 0.5 * x;
-  y = y * fma(-h * y, y, 1.5);
-  return y * fma(-h * y, y, 1.5);
+  const double r = fma(x * y, y, -1.0);
+  return fma(y, r * fma(0.375, r, -0.5), y);
 }
 
-__device__ __forceinline__ double sqrt_fast(double x) {
+__device__ __forceinline__ double sqrt_nan(double x) {
   double y;
   asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-  y = y * fma(-0.5 * x * y, y, 1.5);
   const double s = x * y;
-  const double e = fma(-s, s, x);
-  return x > 0 ? fma(e, 0.5 * y, s) : 0.0;
+  const double r = fma(s, y, -1.0);
+  return fma(s, r * fma(0.375, r, -0.5), s);
 }
+
+__device__ __forceinline__ double sqrt_fast(double x) { return x > 0 ? sqrt_nan(x) : 0.0; }
 
 #endif
 
@@ -450,43 +455,46 @@ __device__ __forceinline__ void bend_fields(int mode, int eo1, const double *__r
 
 #if TRK_FAST
 /* Body of a pure-dipole CSBEND in the fast build.  With no field gradient
- * QY and delta are constant through the body, so f = sqrt((1+delta)^2-QY^2)
- * and 1/f are formed once per bend, and Y and the path length grow by QY and
- * (1+delta) times the same factor each substep, so one running sum F of the
- * factors gives both.  The drift uses the angle-addition formulas with
- * tabulated sin/cos of the substep angle a = dsh/rho0 and two
- * cancellation-free identities:
- *   tan(a+phi) - tan(phi)     = sin(a) / (cos(a+phi) cos(phi))
- *   cos(phi)/cos(a+phi) - 1   = 2 sin(a/2+phi) sin(a/2) / cos(a+phi)
- * so with t = (rho0+X)/cos(a+phi): factor = t sin(a)/f and
- * X' = X + t 2 sin(a/2) sin(a/2+phi).  The kick is
- * QX -= ds (1 + X/rho0)/rho_actual.  Loss conditions are the reference's
- * (f<=0, |QX/f|>1, cos(a+phi)=0, aperture per slice); `done` counts the
- * completed drift substeps for the loss position. */
+ * QY and delta are constant through the body, so f^2 = (1+delta)^2 - QY^2 is
+ * formed once per bend, and Y and the path length grow by QY and (1+delta)
+ * times the same factor each substep, so one running sum F of the factors
+ * gives both.  The drift is written in f cos(phi) = sqrt(f^2 - QX^2) and
+ * f sin(phi) = QX, so no division by f is needed, with tabulated sin/cos of
+ * the substep angle a = dsh/rho0 and 1 - cos(a) = 2 sin^2(a/2) (no
+ * cancellation):
+ *   f cos(a+phi) = cos(a) f cos(phi) - sin(a) QX
+ *   QX'          = f sin(a+phi) = sin(a) f cos(phi) + cos(a) QX
+ *   u            = (rho0 + X) / (f cos(a+phi))
+ *   factor       = u sin(a)                          (= tan(a+phi)-tan(phi), times (rho0+X)cos(phi)/f)
+ *   X'           = X + u ((1-cos a) f cos(phi) + sin(a) QX)
+ * the last from cos(phi)/cos(a+phi) - 1 = 2 sin(a/2) sin(a/2+phi)/cos(a+phi).
+ * The kick is QX -= ds (1 + X/rho0)/rho_actual.  Loss conditions are the
+ * reference's (f<=0, |QX/f|>1, cos(a+phi)=0, aperture per slice); `done`
+ * counts the completed drift substeps for the loss position. */
+
 /* One slice of the dipole body; `checked` evaluates the reference's loss
  * conditions at every substep, otherwise non-finite values are left to
  * propagate and the caller re-runs the slice checked. */
 template <int NSUB, bool CHECKED>
-__device__ __forceinline__ bool dipole_slice(const double *__restrict__ d, int nSub, double rho0, double f,
-                                             double finv, double &X, double &QX, double &F, int &done) {
+__device__ __forceinline__ bool dipole_slice(const double *__restrict__ d, int nSub, double rho0, double f2,
+                                             double &X, double &QX, double &F, int &done) {
 #pragma unroll
   for (int j = 0; j < (NSUB > 0 ? NSUB : 8); j++) {
     if (NSUB == 0 && j >= nSub)
       break;
-    const double sin_phi = QX * finv;
-    if (CHECKED && fabs(sin_phi) > 1)
+    const double u2 = fma(-QX, QX, f2);
+    if (CHECKED && !(u2 >= 0)) /* |sin(phi)| = |QX/f| > 1 */
       return false;
-    const double cos_phi = sqrt_fast(fma(-sin_phi, sin_phi, 1.0));
+    const double fc = CHECKED ? sqrt_fast(u2) : sqrt_nan(u2);
     const double sa = __ldg(&d[BD_SA + j]), ca = __ldg(&d[BD_CA + j]);
-    const double sh = __ldg(&d[BD_SH + j]), ch = __ldg(&d[BD_CH + j]);
-    const double sine = fma(sa, cos_phi, ca * sin_phi);
-    const double cosi = fma(ca, cos_phi, -sa * sin_phi);
-    if (CHECKED && cosi == 0)
+    const double saq = sa * QX;
+    const double fcosi = fma(ca, fc, -saq);
+    if (CHECKED && fcosi == 0)
       return false;
-    const double t = (rho0 + X) * rcp_fast(cosi);
-    QX = f * sine;
-    F = fma(t, sa * finv, F);
-    X = fma(t * __ldg(&d[BD_SH2 + j]), fma(sh, cos_phi, ch * sin_phi), X);
+    const double u = (rho0 + X) * rcp_fast(fcosi);
+    QX = fma(sa, fc, ca * QX);
+    F = fma(u, sa, F);
+    X = fma(u, fma(__ldg(&d[BD_OMC + j]), fc, saq), X);
     if (CHECKED)
       done++;
     if (j == nSub - 1)
@@ -494,6 +502,28 @@ __device__ __forceinline__ bool dipole_slice(const double *__restrict__ d, int n
     QX = fma(-__ldg(&d[BD_C2 + j]), X, QX - __ldg(&d[BD_C1 + j]));
   }
   return true;
+}
+
+struct SliceState {
+  double X, QX, F;
+  int done;
+  bool ok;
+};
+
+/* The checked re-run of one slice, out of line so that the common path does
+ * not hold registers for it. */
+__device__ __noinline__ SliceState dipole_slice_redo(const double *__restrict__ d, int nSub, double rho0, double f2,
+                                                     double X, double QX, double F, int done) {
+  SliceState r;
+  if (nSub == 4)
+    r.ok = dipole_slice<4, true>(d, nSub, rho0, f2, X, QX, F, done);
+  else
+    r.ok = dipole_slice<0, true>(d, nSub, rho0, f2, X, QX, F, done);
+  r.X = X;
+  r.QX = QX;
+  r.F = F;
+  r.done = done;
+  return r;
 }
 
 template <int NSUB>
@@ -505,11 +535,7 @@ __device__ __forceinline__ bool bend_dipole_fast(const double *__restrict__ d, i
   const double opd = 1 + D;
   const double f2 = opd * opd - QY * QY;
   const double Y0 = Y;
-  double f = 0, finv = 0, F = 0;
-  if (f2 > 0) {
-    f = sqrt_fast(f2);
-    finv = rcp_fast(f);
-  }
+  double F = 0;
   bool ok = true;
   done = 0;
   for (int i = 0; i < nSlices; i++) {
@@ -521,14 +547,20 @@ __device__ __forceinline__ bool bend_dipole_fast(const double *__restrict__ d, i
       ok = false;
       break;
     }
+    /* re-read the substep constants every slice (L1 hits) rather than
+     * holding 20 doubles in registers across the slice loop */
+    const double *dd = d;
+    asm volatile("" : "+l"(dd));
     const double X0 = X, QX0 = QX, F0 = F;
-    dipole_slice<NSUB, false>(d, nSub, rho0, f, finv, X, QX, F, done);
+    dipole_slice<NSUB, false>(dd, nSub, rho0, f2, X, QX, F, done);
     if (!isfinite(X + QX + F)) {
       /* a loss condition may have fired: redo the slice with the checks */
-      X = X0;
-      QX = QX0;
-      F = F0;
-      if (!dipole_slice<NSUB, true>(d, nSub, rho0, f, finv, X, QX, F, done)) {
+      const SliceState r = dipole_slice_redo(dd, nSub, rho0, f2, X0, QX0, F0, done);
+      X = r.X;
+      QX = r.QX;
+      F = r.F;
+      done = r.done;
+      if (!r.ok) {
         ok = false;
         break;
       }
@@ -1046,8 +1078,7 @@ __device__ __forceinline__ bool op_dipole_fast(const trk_op *__restrict__ op, Pa
  * per particle as op_dipole_fast; a slice that produced a non-finite value is
  * re-run for that particle with the reference's per-substep loss checks. */
 struct DipoleState {
-  double X, QX, F, QY, Y0, opd, f, finv;
-  double f2;
+  double X, QX, F, QY, Y0, opd, f2;
   int done;
   bool ok;
 };
@@ -1061,25 +1092,16 @@ __device__ __forceinline__ void dipole_begin(DipoleState &q, const Part &p) {
   q.QY = p.yp * r;
   q.F = 0;
   q.f2 = q.opd * q.opd - q.QY * q.QY;
-  q.f = 0;
-  q.finv = 0;
-  if (q.f2 > 0) {
-    q.f = sqrt_fast(q.f2);
-    q.finv = rcp_fast(q.f);
-  }
   q.done = 0;
 }
 
-__device__ __forceinline__ void dipole_step(DipoleState &q, double rho0, double sa, double ca, double sh, double ch,
-                                            double sh2) {
-  const double sin_phi = q.QX * q.finv;
-  const double cos_phi = sqrt_fast(fma(-sin_phi, sin_phi, 1.0));
-  const double sine = fma(sa, cos_phi, ca * sin_phi);
-  const double cosi = fma(ca, cos_phi, -sa * sin_phi);
-  const double t = (rho0 + q.X) * rcp_fast(cosi);
-  q.QX = q.f * sine;
-  q.F = fma(t, sa * q.finv, q.F);
-  q.X = fma(t * sh2, fma(sh, cos_phi, ch * sin_phi), q.X);
+__device__ __forceinline__ void dipole_step(DipoleState &q, double rho0, double sa, double ca, double omc) {
+  const double fc = sqrt_nan(fma(-q.QX, q.QX, q.f2));
+  const double saq = sa * q.QX;
+  const double u = (rho0 + q.X) * rcp_fast(fma(ca, fc, -saq));
+  q.QX = fma(sa, fc, ca * q.QX);
+  q.F = fma(u, sa, q.F);
+  q.X = fma(u, fma(omc, fc, saq), q.X);
 }
 
 __device__ __forceinline__ bool dipole_finish(DipoleState &q, Part &p, const double *__restrict__ d, int nSlices,
@@ -1109,14 +1131,13 @@ __device__ __forceinline__ bool dipole_finish(DipoleState &q, Part &p, const dou
 }
 
 /* one slice for one particle with the reference's loss checks (rare path) */
-__device__ __noinline__ void dipole_slice_checked(DipoleState &q, const double *__restrict__ d, double rho0) {
-  double X = q.X, QX = q.QX, F = q.F;
-  int done = q.done;
-  q.ok = dipole_slice<4, true>(d, 4, rho0, q.f, q.finv, X, QX, F, done);
-  q.X = X;
-  q.QX = QX;
-  q.F = F;
-  q.done = done;
+__device__ __forceinline__ void dipole_slice_checked(DipoleState &q, const double *__restrict__ d, double rho0) {
+  const SliceState r = dipole_slice_redo(d, 4, rho0, q.f2, q.X, q.QX, q.F, q.done);
+  q.ok = r.ok;
+  q.X = r.X;
+  q.QX = r.QX;
+  q.F = r.F;
+  q.done = r.done;
 }
 
 __device__ __forceinline__ void op_dipole_fast2(const trk_op *__restrict__ op, Part &p0, Part &p1, bool &ok0,
@@ -1147,10 +1168,9 @@ __device__ __forceinline__ void op_dipole_fast2(const trk_op *__restrict__ op, P
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       const double sa = __ldg(&d[BD_SA + j]), ca = __ldg(&d[BD_CA + j]);
-      const double sh = __ldg(&d[BD_SH + j]), ch = __ldg(&d[BD_CH + j]);
-      const double sh2 = __ldg(&d[BD_SH2 + j]);
-      dipole_step(q0, rho0, sa, ca, sh, ch, sh2);
-      dipole_step(q1, rho0, sa, ca, sh, ch, sh2);
+      const double omc = __ldg(&d[BD_OMC + j]);
+      dipole_step(q0, rho0, sa, ca, omc);
+      dipole_step(q1, rho0, sa, ca, omc);
       if (j == 3)
         break;
       const double c1 = __ldg(&d[BD_C1 + j]), c2 = __ldg(&d[BD_C2 + j]);
@@ -1198,8 +1218,8 @@ __device__ __forceinline__ void op_dipole_fast2(const trk_op *__restrict__ op, P
 /* ------------------------------------------------------ after-element */
 /* limit_amplitudes / elimit_amplitudes (src/limit_amplitudes.c:197-288,
  * 487-~620) for one particle; returns true if lost. */
-__device__ __forceinline__ bool post_aperture(Part &p, const trk_aperture *__restrict__ ap, int extrapolate, double z,
-                                              double Po) {
+__device__ __forceinline__ bool post_aperture_body(Part &p, const trk_aperture *__restrict__ ap, int extrapolate,
+                                                   double z, double Po) {
   double xmax = ap->x_max, ymax = ap->y_max;
   if (ap->elliptical && xmax > 0 && ymax > 0) {
     if (isinf(p.x) || isinf(p.y) || isnan(p.x) || isnan(p.y)) {
@@ -1263,17 +1283,62 @@ __device__ __forceinline__ bool post_aperture(Part &p, const trk_aperture *__res
   return true;
 }
 
+/* True when the reference's after-element aperture test certainly keeps the
+ * particle (finite x, y inside the rectangle or ellipse, evaluated with the
+ * reference's arithmetic); anything else goes to post_aperture_full. */
+__device__ __forceinline__ bool post_aperture_inside(const Part &p, const trk_aperture *__restrict__ ap) {
+  const double xmax = __ldg(&ap->x_max), ymax = __ldg(&ap->y_max);
+  if (!(isfinite(p.x) && isfinite(p.y)))
+    return false;
+  if (__ldg(&ap->elliptical) && xmax > 0 && ymax > 0)
+    return (ipow_d(p.x, __ldg(&ap->xexp)) / __ldg(&ap->a2) + ipow_d(p.y, __ldg(&ap->yexp)) / __ldg(&ap->b2)) <= 1;
+  return (!(xmax > 0) || fabs(p.x) <= xmax) && (!(ymax > 0) || fabs(p.y) <= ymax);
+}
+
+struct PartLoss {
+  Part p;
+  int lost;
+};
+
+/* Out of line, with the particle passed and returned by value (a reference
+ * would pin the caller's coordinates in local memory): it only runs for
+ * particles that post_aperture_inside could not clear. */
+__device__ __noinline__ PartLoss post_aperture_full(Part p, const trk_aperture *__restrict__ ap, int extrapolate,
+                                                    double z, double Po) {
+  PartLoss r;
+  r.lost = post_aperture_body(p, ap, extrapolate, z, Po);
+  r.p = p;
+  return r;
+}
+
+__device__ __forceinline__ bool post_aperture(Part &p, const trk_aperture *__restrict__ ap, int extrapolate, double z,
+                                              double Po) {
+  if (post_aperture_inside(p, ap))
+    return false;
+  const PartLoss r = post_aperture_full(p, ap, extrapolate, z, Po);
+  p = r.p;
+  return r.lost != 0;
+}
+
 /* DRIF through its order-1/2 matrix (src/compute_matrices.c:391-413,
  * src/matrix.c:310-422): the structural zeros contribute only signed zeros
  * for finite input and NaN when any coordinate is not finite. */
 __device__ __forceinline__ void op_drift(const trk_op *__restrict__ op, Part &p) {
   const double L = __ldg(&op->d[DD_L]);
   const int order = __ldg(&op->i[0]);
+#if TRK_FAST
+  /* any non-finite coordinate makes x and y NaN, so the after-element filter
+   * records the loss here as the reference does */
+  const double nan_if = (p.s + p.dp) * 0.0;
+  p.x += nan_if;
+  p.y += nan_if;
+#else
   if (!(isfinite(p.x) && isfinite(p.xp) && isfinite(p.y) && isfinite(p.yp) && isfinite(p.s) && isfinite(p.dp))) {
     const double qnan = __longlong_as_double(0x7ff8000000000000ULL);
     p.x = p.xp = p.y = p.yp = p.s = p.dp = qnan;
     return;
   }
+#endif
   double xp = p.xp, yp = p.yp;
   double x1 = L * xp + p.x;
   double y1 = L * yp + p.y;
@@ -1315,18 +1380,59 @@ __device__ __forceinline__ void store_part(const TrackArgs &a, long i, const Par
 
 /* Track one particle through ops [ob, oe) for passes [pb, pe).  Returns
  * false if it was lost (loss recorded). */
+/* The per-element header fields every particle reads, fetched with three
+ * 16-byte loads (trk_op starts with 8 int32 fields; z_start and z_end follow
+ * at byte 64). */
+struct OpHead {
+  int kind, elem, ap_post, ap_in, extrapolate, no_aperture;
+  double z_start, z_end;
+};
+static_assert(offsetof(trk_op, z_start) == 64 && sizeof(trk_op) % 16 == 0, "trk_op header layout");
+
+__device__ __forceinline__ OpHead load_head(const trk_op *__restrict__ op, int var) {
+  const int4 h0 = __ldg(reinterpret_cast<const int4 *>(op));
+  const int4 h1 = __ldg(reinterpret_cast<const int4 *>(op) + 1);
+  const double2 z = __ldg(reinterpret_cast<const double2 *>(&op->z_start));
+  OpHead h;
+  h.kind = h0.x;
+  h.elem = h0.y;
+  h.ap_post = var ? h0.w : h0.z;
+  h.ap_in = var ? h1.y : h1.x;
+  h.extrapolate = h1.z;
+  h.no_aperture = h1.w;
+  h.z_start = z.x;
+  h.z_end = z.y;
+  return h;
+}
+
+/* After-element filters of do_tracking (src/do_tracking.c:2506-2524 MAXAMP
+ * aperture, :2675-2684 NaN/inf filter) and the loss record of one particle. */
+__device__ __forceinline__ bool after_element(const TrackArgs &a, const OpHead &h, Part &p, bool ok, long i,
+                                              long pass) {
+  if (ok && !h.no_aperture && h.ap_post >= 0)
+    ok = !post_aperture(p, a.aps + h.ap_post, h.extrapolate, h.z_end, a.Po);
+  if (ok && (isinf(p.x) || isinf(p.y) || isnan(p.x) || isnan(p.y))) {
+    p.s = h.z_end;
+    p.dp = a.Po * (1 + p.dp);
+    ok = false;
+  }
+  if (!ok) {
+    a.lost_pass[i] = (int32_t)pass;
+    a.lost_elem[i] = h.elem;
+  }
+  return ok;
+}
+
 template <bool LEAN>
 __device__ __forceinline__ bool track_particle(const TrackArgs &a, Part &p, long i) {
   for (long pass = a.pass_begin; pass < a.pass_end; pass++) {
     const int var = (pass == a.fresh_pass) ? 0 : 1;
     for (int k = a.op_begin; k < a.op_end; k++) {
       const trk_op *op = a.ops + k;
-      const int kind = __ldg(&op->kind);
-      const double z_start = __ldg(&op->z_start), z_end = __ldg(&op->z_end);
-      const int api = __ldg(&op->ap_in[var]);
-      const trk_aperture *ap_in = api >= 0 ? a.aps + api : nullptr;
+      const OpHead h = load_head(op, var);
+      const trk_aperture *ap_in = h.ap_in >= 0 ? a.aps + h.ap_in : nullptr;
       bool ok = true;
-      switch (kind) {
+      switch (h.kind) {
       case OPK_DRIFT:
         op_drift(op, p);
         break;
@@ -1336,47 +1442,34 @@ __device__ __forceinline__ bool track_particle(const TrackArgs &a, Part &p, long
         break;
       case OPK_MULT1:
 #if TRK_FAST
-        ok = op_mult1_fast(op, p, a.Po, z_start, ap_in);
+        ok = op_mult1_fast(op, p, a.Po, h.z_start, ap_in);
 #else
-        ok = op_mult(op, p, a.Po, z_start, ap_in);
+        ok = op_mult(op, p, a.Po, h.z_start, ap_in);
 #endif
         break;
       case OPK_DIPOLE:
 #if TRK_FAST
-        ok = op_dipole_fast(op, p, a.Po, z_start, ap_in);
+        ok = op_dipole_fast(op, p, a.Po, h.z_start, ap_in);
 #else
-        ok = op_bend(op, p, a.Po, z_start, ap_in, a.field);
+        ok = op_bend(op, p, a.Po, h.z_start, ap_in, a.field);
 #endif
         break;
       case OPK_RF:
-        ok = op_rf(op, p, a.Po, z_end, a.rf_phase);
+        ok = op_rf(op, p, a.Po, h.z_end, a.rf_phase);
         break;
       case OPK_MULT:
         if (!LEAN)
-          ok = op_mult(op, p, a.Po, z_start, ap_in);
+          ok = op_mult(op, p, a.Po, h.z_start, ap_in);
         break;
       case OPK_BEND:
         if (!LEAN)
-          ok = op_bend(op, p, a.Po, z_start, ap_in, a.field);
+          ok = op_bend(op, p, a.Po, h.z_start, ap_in, a.field);
         break;
       default:
         break;
       }
-      if (ok && !__ldg(&op->no_aperture)) {
-        const int apo = __ldg(&op->ap_post[var]);
-        if (apo >= 0)
-          ok = !post_aperture(p, a.aps + apo, __ldg(&op->extrapolate), z_end, a.Po);
-      }
-      if (ok && (isinf(p.x) || isinf(p.y) || isnan(p.x) || isnan(p.y))) {
-        p.s = z_end;
-        p.dp = a.Po * (1 + p.dp);
-        ok = false;
-      }
-      if (!ok) {
-        a.lost_pass[i] = (int32_t)pass;
-        a.lost_elem[i] = __ldg(&op->elem);
+      if (!after_element(a, h, p, ok, i, pass))
         return false;
-      }
     }
   }
   return true;
@@ -1398,32 +1491,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(TrackArgs a) {
 }
 
 #if TRK_FAST
-/* after-element filters and loss record of one particle (as in
- * track_particle) */
-__device__ __forceinline__ bool after_element(const TrackArgs &a, const trk_op *__restrict__ op, int var, Part &p,
-                                              bool ok, long i, long pass) {
-  const double z_end = __ldg(&op->z_end);
-  if (ok && !__ldg(&op->no_aperture)) {
-    const int apo = __ldg(&op->ap_post[var]);
-    if (apo >= 0)
-      ok = !post_aperture(p, a.aps + apo, __ldg(&op->extrapolate), z_end, a.Po);
-  }
-  if (ok && (isinf(p.x) || isinf(p.y) || isnan(p.x) || isnan(p.y))) {
-    p.s = z_end;
-    p.dp = a.Po * (1 + p.dp);
-    ok = false;
-  }
-  if (!ok) {
-    a.lost_pass[i] = (int32_t)pass;
-    a.lost_elem[i] = __ldg(&op->elem);
-  }
-  return ok;
-}
-
-__device__ __forceinline__ bool lean_op(const TrackArgs &a, const trk_op *__restrict__ op, int kind, Part &p,
+__device__ __forceinline__ bool lean_op(const TrackArgs &a, const trk_op *__restrict__ op, const OpHead &h, Part &p,
                                         const trk_aperture *ap_in) {
-  const double z_start = __ldg(&op->z_start);
-  switch (kind) {
+  const double z_start = h.z_start;
+  switch (h.kind) {
   case OPK_DRIFT:
     op_drift(op, p);
     return true;
@@ -1436,7 +1507,7 @@ __device__ __forceinline__ bool lean_op(const TrackArgs &a, const trk_op *__rest
   case OPK_DIPOLE:
     return op_dipole_fast(op, p, a.Po, z_start, ap_in);
   case OPK_RF:
-    return op_rf(op, p, a.Po, __ldg(&op->z_end), a.rf_phase);
+    return op_rf(op, p, a.Po, h.z_end, a.rf_phase);
   default:
     return true;
   }
@@ -1467,22 +1538,21 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel2(TrackArgs a) {
       const int var = (pass == a.fresh_pass) ? 0 : 1;
       for (int k = a.op_begin; k < a.op_end && (al0 || al1); k++) {
         const trk_op *op = a.ops + k;
-        const int kind = __ldg(&op->kind);
-        const int api = __ldg(&op->ap_in[var]);
-        const trk_aperture *ap_in = api >= 0 ? a.aps + api : nullptr;
+        const OpHead h = load_head(op, var);
+        const trk_aperture *ap_in = h.ap_in >= 0 ? a.aps + h.ap_in : nullptr;
         bool ok0 = al0, ok1 = al1;
-        if (kind == OPK_DIPOLE) {
-          op_dipole_fast2(op, p0, p1, ok0, ok1, a.Po, __ldg(&op->z_start), ap_in);
+        if (h.kind == OPK_DIPOLE) {
+          op_dipole_fast2(op, p0, p1, ok0, ok1, a.Po, h.z_start, ap_in);
         } else {
           if (al0)
-            ok0 = lean_op(a, op, kind, p0, ap_in);
+            ok0 = lean_op(a, op, h, p0, ap_in);
           if (al1)
-            ok1 = lean_op(a, op, kind, p1, ap_in);
+            ok1 = lean_op(a, op, h, p1, ap_in);
         }
         if (al0)
-          al0 = after_element(a, op, var, p0, ok0, i0, pass);
+          al0 = after_element(a, h, p0, ok0, i0, pass);
         if (al1)
-          al1 = after_element(a, op, var, p1, ok1, i1, pass);
+          al1 = after_element(a, h, p1, ok1, i1, pass);
       }
     }
     if (was0)
@@ -1844,6 +1914,7 @@ __global__ void rotate_kernel(TrackArgs a, double ca, double sa) {
 int track_variant_block(int variant) {
   switch (variant) {
   case 2:
+  case 8:
     return 256;
   case 3:
     return 64;
@@ -1867,6 +1938,12 @@ static void launch_track_t(const TrackArgs &a, int variant, int grid, int block,
   case 4:
     track_kernel<128, 5, LEAN><<<grid, block, 0, st>>>(a);
     break;
+  case 7:
+    track_kernel<128, 6, LEAN><<<grid, block, 0, st>>>(a);
+    break;
+  case 8:
+    track_kernel<256, 3, LEAN><<<grid, block, 0, st>>>(a);
+    break;
   default:
     track_kernel<128, 1, LEAN><<<grid, block, 0, st>>>(a);
     break;
@@ -1888,7 +1965,7 @@ void launch_track(const TrackArgs &a, int variant, bool lean, long n, int max_bl
     return;
   }
 #endif
-  if (variant >= 5)
+  if (variant == 5 || variant == 6 || variant < 0 || variant >= TRK_N_VARIANTS)
     variant = 1;
   const int block = track_variant_block(variant);
   long g = (n + block - 1) / block;

@@ -13,6 +13,12 @@
 
 #define TRK_BLOCK 128
 
+/* launch shapes of the tracking kernel (trk_run.variant):
+ * 0 (128 threads, 1 block/SM min), 1 (128, 4), 2 (256, 2), 3 (64, 8), 4 (128, 5),
+ * 5 and 6: two particles per thread (128, 3) / (128, 2), lean lattices in the fast build,
+ * 7 (128, 6), 8 (256, 3) */
+#define TRK_N_VARIANTS 9
+
 /* device status word bits (a kernel records a problem and returns; the host
  * turns the word into a trk_error after the launch sequence) */
 #define TRK_STATUS_LONG_BEAM 1      /* beam longer than the wake table (src/wake.c:134-140) */

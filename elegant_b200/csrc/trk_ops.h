@@ -134,7 +134,7 @@ typedef struct {
 #define BD_N 86       /* field index n = -b1/h for order-2 edges */
 #define BD_RHOINV 87  /* 1/rho0 (fast build) */
 #define BD_INVRHOA 88 /* 1/rho_actual (fast build) */
-#define BD_SH2 89     /* 8 values 2 sin(dsh/(2 rho0)) (fast build) */
+#define BD_OMC 89     /* 8 values 1 - cos(dsh/rho0) = 2 sin^2(dsh/(2 rho0)) (fast build) */
 #define BD_C1 97      /* 8 values ds/rho_actual (fast build kick) */
 #define BD_C2 105     /* 8 values ds/(rho_actual rho0) (fast build kick) */
 /* i: 0 nSlices, 1 nSub, 2 field mode (0 dipole, 1 normal, 2 skew), 3 expansionOrder1,
