@@ -37,6 +37,10 @@ sys.path.insert(0, ROOT)
 
 N_PARTICLES = 1_000_000
 WORKLOAD = "ring_rf_wake_fodo40_1e6"
+# DRAM bytes per particle of one tracking-kernel launch: 10.63 MB read + 1.8 KB
+# written at 2e5 particles (ncu; the coordinate writes stay in L2 and are
+# written back during later kernels)
+TRACK_DRAM_BYTES_PER_PARTICLE = 10.628e6 / 2e5
 
 
 def workload_config(n_particles):
@@ -207,6 +211,8 @@ def run_gpu(args, rank, world, local):
         step_ms = []
         effort = 0
         launches = 0
+        track_ms = 0.0
+        track_launches = 0
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
@@ -215,11 +221,13 @@ def run_gpu(args, rank, world, local):
             for k in range(args.steps):
                 with torch.cuda.stream(stream):
                     flush.fill_(float(k))
-                st = trk.track(lat, 1, configs.P_CENTRAL, pass_offset=pass_index, fast=fast)
+                st = trk.track(lat, 1, configs.P_CENTRAL, pass_offset=pass_index, fast=fast, time_kernels=True)
                 pass_index += 1
                 step_ms.append(st["device_ms"])
                 effort += st["particle_passes"]
                 launches += st["kernel_launches"]
+                track_ms += st["track_ms"]
+                track_launches += st["track_launches"]
             torch.cuda.synchronize()
             wall = time.perf_counter() - t_wall
         dev_s = sum(step_ms) / 1e3
@@ -235,27 +243,40 @@ def run_gpu(args, rank, world, local):
         value = effort / dev_s
         # end-to-end through the C ABI with host buffers
         pinned = torch.from_numpy(beam).pin_memory().numpy()
+        pinned_out = torch.empty(beam.shape, dtype=torch.float64).pin_memory().numpy()
         e2e_ms = []
-        for k in range(max(2, args.steps // 4)):
+        for k in range(max(3, args.steps // 2)):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             trk.load(pinned)
             st = trk.track(lat, 1, configs.P_CENTRAL, fast=fast)
-            trk.store(stride=7)
+            trk.store(stride=7, out=pinned_out)
             e2e_ms.append((time.perf_counter() - t0) * 1e3)
             e2e_eff = st["particle_passes"]
         e2e_value = e2e_eff / (np.median(e2e_ms) / 1e3) * world
     if rank != 0:
         return 0
-    # roofline: algorithmic FP64 flops per particle-turn
+    # roofline of the dominant kernel (the fused tracking kernel): algorithmic
+    # FP64 flops of the elements it runs (reference formulation, counted in
+    # oracle/flops.json) per launch, over its CUDA-event launch time
     peak = measure_fp64_peak(local)
     roof = None
-    if flops:
+    if flops and track_launches:
         fpt = flops["flops_per_particle_turn"][args.workload]
-        achieved = fpt * value / world / 1e12
+        if args.workload == "c2":
+            fpt -= flops["per_particle"]["WAKE"]["total"]  # the wake's per-particle work runs in the wake kernels
+        per_launch_flops = fpt * (effort / world) / track_launches
+        avg_launch_s = track_ms / track_launches / 1e3
+        achieved = per_launch_flops / avg_launch_s / 1e12
         roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak if peak else None, "traffic": None,
-                "flops_per_particle_turn": fpt, "peak_source": "measured in this run (dependent-FMA kernel)"}
+                "frac": achieved / peak if peak else None,
+                "traffic": TRACK_DRAM_BYTES_PER_PARTICLE * (effort / world) / track_launches,
+                "flops_per_particle_turn": fpt, "kernel": "track_kernel", "launches": track_launches,
+                "avg_launch_ms": avg_launch_s * 1e3,
+                "peak_source": "FP64 FMA peak measured in this run (independent dependent-FMA chains); "
+                               "MEASURED_PEAKS.json has no FP64 figure",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at 2e5 "
+                                  "particles, scaled by particles (profiles/track_kernel_ring_rf_wake.md)"}
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         cpu = cpu_baseline(cores=1)

@@ -41,12 +41,13 @@ class TrackingError(RuntimeError):
 class _Run(ctypes.Structure):
     _fields_ = [("p_central", ctypes.c_double), ("n_passes", ctypes.c_long), ("pass_offset", ctypes.c_long),
                 ("fast_math", ctypes.c_int32), ("block_size", ctypes.c_int32), ("compact_every", ctypes.c_int32),
-                ("variant", ctypes.c_int32)]
+                ("variant", ctypes.c_int32), ("time_kernels", ctypes.c_int32)]
 
 
 class _Stats(ctypes.Structure):
     _fields_ = [("n_total", ctypes.c_long), ("n_left", ctypes.c_long), ("particle_passes", ctypes.c_long),
-                ("device_ms", ctypes.c_double), ("kernel_launches", ctypes.c_long), ("p_central", ctypes.c_double)]
+                ("device_ms", ctypes.c_double), ("kernel_launches", ctypes.c_long), ("p_central", ctypes.c_double),
+                ("track_ms", ctypes.c_double), ("track_launches", ctypes.c_long)]
 
 
 _lib = None
@@ -243,8 +244,14 @@ class Tracker:
         self.np = np_
         _check(self.lib, self.lib.trk_beam_load_device(self.ctx, ctypes.c_void_p(ptr), np_, ld))
 
-    def store(self, stride=7, with_loss=False):
-        out = np.zeros((self.np, stride), dtype=np.float64)
+    def store(self, stride=7, with_loss=False, out=None):
+        """Beam rows back to the host (survivors first).  `out`, if given, is
+        a C-contiguous float64 (np, stride) array to fill (e.g. pinned
+        memory); otherwise a new array is returned."""
+        if out is None:
+            out = np.zeros((self.np, stride), dtype=np.float64)
+        elif out.shape != (self.np, stride) or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of shape (np, stride)")
         n_left = ctypes.c_long()
         if with_loss:
             lp = np.empty(self.np, dtype=np.int64)
@@ -279,7 +286,7 @@ class Tracker:
             self._lat_cache[key] = nat
         return nat[1]
 
-    def track(self, lattice, n_passes, p_central, pass_offset=0, fast=True, variant=-1):
+    def track(self, lattice, n_passes, p_central, pass_offset=0, fast=True, variant=-1, time_kernels=False):
         nat = self.native(lattice)
         run = _Run()
         self.lib.trk_run_defaults(ctypes.byref(run))
@@ -288,10 +295,12 @@ class Tracker:
         run.pass_offset = pass_offset
         run.fast_math = 1 if fast else 0
         run.variant = variant
+        run.time_kernels = 1 if time_kernels else 0
         st = _Stats()
         _check(self.lib, self.lib.trk_track(self.ctx, nat.ptr, ctypes.byref(run), ctypes.byref(st)))
         return Stats(n_total=st.n_total, n_left=st.n_left, particle_passes=st.particle_passes,
-                     device_ms=st.device_ms, kernel_launches=st.kernel_launches, p_central=st.p_central)
+                     device_ms=st.device_ms, kernel_launches=st.kernel_launches, p_central=st.p_central,
+                     track_ms=st.track_ms, track_launches=st.track_launches)
 
 
 def _lattice_signature(lat):

@@ -49,6 +49,7 @@ struct trk_context {
   int sm_count = 148;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> kev; /* start/stop pairs for trk_run.time_kernels */
   long np = 0, cap = 0;
   double *d_cols = nullptr; /* 7 columns x cap */
   int32_t *d_lost_pass = nullptr, *d_lost_elem = nullptr;
@@ -134,6 +135,19 @@ __global__ void soa_copy_kernel(const double *src, long ld, long np, double *col
     cols[c * cap + i] = src[c * ld + i];
   lost_pass[i] = -1;
   lost_elem[i] = -1;
+}
+
+/* reverse perm[nsel..np) in place (the partition writes rejected items in
+ * reverse order); nsel is read on the device */
+__global__ void reverse_tail_kernel(long *perm, const long *nsel_p, long np) {
+  const long nsel = *nsel_p;
+  const long m = np - nsel;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < m / 2; i += (long)gridDim.x * blockDim.x) {
+    const long a = nsel + i, b = np - 1 - i;
+    const long t = perm[a];
+    perm[a] = perm[b];
+    perm[b] = t;
+  }
 }
 
 __global__ void alive_flags_kernel(const int32_t *lost_pass, long np, char *flags, long *idx) {
@@ -642,6 +656,8 @@ void trk_context_destroy(trk_context *ctx) {
     cudaFree(w.Wy);
     cudaFree(w.state);
   }
+  for (cudaEvent_t e : ctx->kev)
+    cudaEventDestroy(e);
   if (ctx->ev0)
     cudaEventDestroy(ctx->ev0);
   if (ctx->ev1)
@@ -756,17 +772,9 @@ int trk_beam_store(trk_context *ctx, double *coord, long stride, long *n_left, l
     return rc;
   CUDA_TRY(cub::DevicePartition::Flagged(ctx->d_cub, tmp, d_idx, ctx->d_flags, ctx->d_perm, ctx->d_nsel, np,
                                          ctx->stream));
-  long nsel = 0;
-  CUDA_TRY(cudaMemcpyAsync(&nsel, ctx->d_nsel, sizeof(long), cudaMemcpyDeviceToHost, ctx->stream));
-  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   /* reverse the rejected tail so lost particles keep their original order */
-  std::vector<long> perm;
-  if (nsel < np) {
-    perm.resize(np - nsel);
-    CUDA_TRY(cudaMemcpy(perm.data(), ctx->d_perm + nsel, sizeof(long) * (np - nsel), cudaMemcpyDeviceToHost));
-    std::reverse(perm.begin(), perm.end());
-    CUDA_TRY(cudaMemcpy(ctx->d_perm + nsel, perm.data(), sizeof(long) * (np - nsel), cudaMemcpyHostToDevice));
-  }
+  reverse_tail_kernel<<<(int)((np / 2 + 255) / 256 + 1), 256, 0, ctx->stream>>>(ctx->d_perm, ctx->d_nsel, np);
+  CUDA_TRY(cudaGetLastError());
   if ((rc = ensure(&ctx->d_aos, ctx->aos_cap, (size_t)np * stride)))
     return rc;
   int32_t *d_out = nullptr;
@@ -790,9 +798,23 @@ int trk_beam_store(trk_context *ctx, double *coord, long stride, long *n_left, l
     }
     cudaFree(d_out);
   }
+  long nsel = 0;
+  CUDA_TRY(cudaMemcpyAsync(&nsel, ctx->d_nsel, sizeof(long), cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   if (n_left)
     *n_left = nsel;
+  return TRK_OK;
+}
+
+/* per-launch timing events for trk_run.time_kernels (created on demand,
+ * reused across calls) */
+#define TRK_MAX_TIMED 4096
+static int timing_events(trk_context *ctx, int pairs) {
+  while ((int)ctx->kev.size() < 2 * pairs) {
+    cudaEvent_t e;
+    CUDA_TRY(cudaEventCreate(&e));
+    ctx->kev.push_back(e);
+  }
   return TRK_OK;
 }
 
@@ -814,6 +836,7 @@ int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, 
   const long p0 = run->pass_offset;
   const long fresh = ctx->passes_done == 0 ? p0 : -1;
   int variant = run->variant;
+  int n_timed = 0;
   if (variant < 0 || variant >= TRK_N_VARIANTS)
     variant = ctx->tuned_variant;
   if (variant < 0)
@@ -852,10 +875,18 @@ int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, 
           ta.op_end = st.oe;
           ta.pass_begin = pass;
           ta.pass_end = pass + npass;
+          const bool timed = run->time_kernels && n_timed < TRK_MAX_TIMED;
+          if (timed) {
+            if ((rc = timing_events(ctx, n_timed + 1)))
+              return rc;
+            CUDA_TRY(cudaEventRecord(ctx->kev[2 * n_timed], ctx->stream));
+          }
           if (fast)
             trk_fast::launch_track(ta, variant, c.lean, ctx->np, max_blocks, ctx->stream);
           else
             trk_exact::launch_track(ta, variant, c.lean, ctx->np, max_blocks, ctx->stream);
+          if (timed)
+            CUDA_TRY(cudaEventRecord(ctx->kev[2 * n_timed++ + 1], ctx->stream));
           ctx->last_launches++;
         } else if (st.kind == 1) {
           const trk_op &op = c.ops[st.ob];
@@ -891,6 +922,12 @@ int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, 
     stats->n_total = ctx->np;
     stats->kernel_launches = ctx->last_launches;
     stats->p_central = Po;
+    for (int k = 0; k < n_timed; k++) {
+      float kms = 0;
+      CUDA_TRY(cudaEventElapsedTime(&kms, ctx->kev[2 * k], ctx->kev[2 * k + 1]));
+      stats->track_ms += kms;
+    }
+    stats->track_launches = n_timed;
     if (ctx->np > 0) {
       CUDA_TRY(cudaMemsetAsync(ctx->d_effort, 0, sizeof(long long), ctx->stream));
       effort_kernel<<<std::min(grid_for(ctx, ctx->np, 256), 1024), 256, 0, ctx->stream>>>(

@@ -76,7 +76,7 @@ __device__ __forceinline__ double rsqrt_fast(double x) {
   double y;
   asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
   const double r = fma(x * y, y, -1.0);
-  return fma(y, r * fma(0.375, r, -0.5), y);
+  return fma(y * r, fma(0.375, r, -0.5), y);
 }
 
 __device__ __forceinline__ double sqrt_nan(double x) {
@@ -84,7 +84,18 @@ __device__ __forceinline__ double sqrt_nan(double x) {
   asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
   const double s = x * y;
   const double r = fma(s, y, -1.0);
-  return fma(s, r * fma(0.375, r, -0.5), s);
+  return fma(s * r, fma(0.375, r, -0.5), s);
+}
+
+/* a / x with the reciprocal's correction applied to the quotient:
+ * a y0 (1 + e + e^2), e = 1 - x y0 (one dependent step shorter than
+ * a * rcp_fast(x)); NaN for x = 0. */
+__device__ __forceinline__ double div_fast(double a, double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  const double q = a * y;
+  const double e = fma(-x, y, 1.0);
+  return fma(q, fma(e, e, e), q);
 }
 
 __device__ __forceinline__ double sqrt_fast(double x) { return x > 0 ? sqrt_nan(x) : 0.0; }
@@ -491,7 +502,7 @@ __device__ __forceinline__ bool dipole_slice(const double *__restrict__ d, int n
     const double fcosi = fma(ca, fc, -saq);
     if (CHECKED && fcosi == 0)
       return false;
-    const double u = (rho0 + X) * rcp_fast(fcosi);
+    const double u = div_fast(rho0 + X, fcosi);
     QX = fma(sa, fc, ca * QX);
     F = fma(u, sa, F);
     X = fma(u, fma(__ldg(&d[BD_OMC + j]), fc, saq), X);
@@ -1098,7 +1109,7 @@ __device__ __forceinline__ void dipole_begin(DipoleState &q, const Part &p) {
 __device__ __forceinline__ void dipole_step(DipoleState &q, double rho0, double sa, double ca, double omc) {
   const double fc = sqrt_nan(fma(-q.QX, q.QX, q.f2));
   const double saq = sa * q.QX;
-  const double u = (rho0 + q.X) * rcp_fast(fma(ca, fc, -saq));
+  const double u = div_fast(rho0 + q.X, fma(ca, fc, -saq));
   q.QX = fma(sa, fc, ca * q.QX);
   q.F = fma(u, sa, q.F);
   q.X = fma(u, fma(omc, fc, saq), q.X);

@@ -126,6 +126,7 @@ typedef struct {
   int32_t block_size;    /* unused, kept 0 (block shape comes with the variant) */
   int32_t compact_every; /* compact survivors every N passes in fused runs (0 = never) */
   int32_t variant;       /* tracking-kernel variant (block size x occupancy); -1 = autotuned choice */
+  int32_t time_kernels;  /* 1: bracket every tracking-kernel launch with CUDA events (trk_stats.track_ms) */
 } trk_run;
 
 void trk_run_defaults(trk_run *run);
@@ -137,6 +138,8 @@ typedef struct {
   double device_ms;      /* device time of the tracking kernels (CUDA events) */
   long kernel_launches;  /* kernels launched by the library during the call */
   double p_central;      /* reference momentum after the run */
+  double track_ms;       /* with trk_run.time_kernels: summed device time of the tracking-kernel launches */
+  long track_launches;   /* with trk_run.time_kernels: tracking-kernel launches timed */
 } trk_stats;
 
 /* ------------------------------------------------------------- contexts */
