@@ -16,8 +16,10 @@ roofline: FP64 bound; achieved = algorithmic FP64 flops per particle-turn
         (counted on the reference formulation, oracle/flops.json) times
         particle-turns/s, against the FP64 peak measured in this run by a
         dependent-FMA kernel (MEASURED_PEAKS.json has no FP64 figure).
---impl reference: the oracle (CPU restatement of the reference's element
-        functions) on the host cores, process-parallel by particle shards.
+--impl reference: elegant's own tracking code compiled from the reference
+        sources (oracle/_ref/libref.so; the oracle restatement where that
+        was not built) on all host cores, process-parallel by particle
+        shards.
 Multi-GPU: one process per GPU; each rank tracks its own particle shard
 (weak scaling), the wake histogram and time statistics are all-reduced.
 """
@@ -106,31 +108,41 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
-def cpu_baseline(impl_reference=False, cores=None, sample_particles=2000, sample_turns=2):
-    """Time the oracle on the host: particle-turns/s on a bounded sample."""
+def _cpu_tracker():
+    """elegant's own tracking code (oracle/_ref/libref.so, built from the
+    reference sources) when present, else the oracle restatement."""
+    from oracle import pyoracle
+    if pyoracle.ref_available():
+        return pyoracle.track_ref, "reference"
+    pyoracle.load()
+    return pyoracle.track, "port"
+
+
+def cpu_baseline(cores=None, sample_particles=6000, sample_turns=3):
+    """Time the CPU tracking path on the host: particle-turns/s on a bounded
+    sample of the benchmark ring (same lattice, same beam distribution)."""
     from elegant_b200 import configs
     if cores is None:
         cores = 1
-    lat = configs.c2_lattice()
     if cores == 1:
-        from oracle import pyoracle
+        track, kind = _cpu_tracker()
+        lat = configs.c2_lattice()
         beam = configs.gaussian_beam(sample_particles, seed=1)
-        pyoracle.load()
         t0 = time.perf_counter()
-        _, _, eff = pyoracle.track(lat, beam, sample_turns, configs.P_CENTRAL)
+        _, _, eff = track(lat, beam, sample_turns, configs.P_CENTRAL)
         dt = time.perf_counter() - t0
-        return {"value": eff / dt, "unit": "particle-turns/s", "cores": 1, "kind": "port",
+        return {"value": eff / dt, "unit": "particle-turns/s", "cores": 1, "kind": kind,
                 "sample": f"{sample_particles} particles x {sample_turns} turns of the same lattice, 1 core"}
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     per = sample_particles
     with ctx.Pool(cores) as pool:
         args = [(per, sample_turns, 1 + k) for k in range(cores)]
-        pool.map(_oracle_shard, [(10, 1, 99)] * cores)  # warm the workers
+        kinds = pool.map(_oracle_shard, [(10, 1, 99)] * cores)  # warm the workers
         t0 = time.perf_counter()
         effs = pool.map(_oracle_shard, args)
         dt = time.perf_counter() - t0
-    return {"value": sum(effs) / dt, "unit": "particle-turns/s", "cores": cores, "kind": "port",
+    return {"value": sum(e for e, _ in effs) / dt, "unit": "particle-turns/s", "cores": cores, "kind": kinds[0][1],
             "sample": f"{cores} processes x {per} particles x {sample_turns} turns (particle shards; wake "
                       "histograms per shard)"}
 
@@ -139,28 +151,40 @@ def _oracle_shard(args):
     n, turns, seed = args
     sys.path.insert(0, ROOT)
     from elegant_b200 import configs
-    from oracle import pyoracle
+    track, kind = _cpu_tracker()
     lat = configs.c2_lattice()
     beam = configs.gaussian_beam(n, seed=seed)
-    _, _, eff = pyoracle.track(lat, beam, turns, configs.P_CENTRAL)
-    return eff
+    _, _, eff = track(lat, beam, turns, configs.P_CENTRAL)
+    return eff, kind
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the CPU tracking path on all host cores (one
+    process per core, particle shards), each step a bounded sample of the
+    benchmark ring; rank 0 only."""
     if rank != 0:
         return 0
+    import multiprocessing as mp
     cores = os.cpu_count() or 1
+    per, turns = 1000, 1
     steps = []
-    for _ in range(args.warmup):
-        cpu_baseline(cores=cores, sample_particles=200, sample_turns=1)
-    for _ in range(args.steps):
-        steps.append(cpu_baseline(cores=cores, sample_particles=1000, sample_turns=1))
-    v = float(np.mean([s["value"] for s in steps]))
+    with mp.get_context("spawn").Pool(cores) as pool:
+        kind = pool.map(_oracle_shard, [(10, 1, 99)] * cores)[0][1]
+        for k in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            effs = pool.map(_oracle_shard, [(per, turns, 1 + c) for c in range(cores)])
+            dt = time.perf_counter() - t0
+            if k >= args.warmup:
+                steps.append(sum(e for e, _ in effs) / dt)
+    v = float(np.mean(steps))
+    sample = (f"{cores} processes x {per} particles x {turns} turn of the same ring per step (particle shards; "
+              "wake histograms per shard)")
+    steps = [{"kind": kind, "sample": sample}]
     line = {"metric": "particle-turns/s", "value": v, "unit": "particle-turns/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian beam)",
             "config": workload_config(N_PARTICLES), "impl": "reference",
-            "cpu_baseline": {"value": v, "unit": "particle-turns/s", "cores": cores, "kind": "port",
+            "cpu_baseline": {"value": v, "unit": "particle-turns/s", "cores": cores, "kind": steps[0]["kind"],
                              "sample": steps[0]["sample"]},
             "e2e": {"value": v, "unit": "particle-turns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

@@ -306,6 +306,17 @@ int compile_mult(const trk_elem *e, double Po, trk_op *op) {
     op->d[MD_KX + st] = -xk * kf[st];
     op->d[MD_KY + st] = -yk * kf[st];
   }
+  /* multipole_tracking2 keeps one dzLoss for all particles of a call and
+   * integrate_kick_multipole_ordn resets it only after its entry checks
+   * (src/multipole.c:686, :1179-1186, :1232): a particle rejected at entry is
+   * recorded at z_start + the previous particle's dzLoss, which is this sum
+   * whenever that particle went through the body */
+  double dzfull = 0;
+  if (driftp != 0)
+    for (long k = 0; k < n_parts; k++)
+      for (int st = 0; st < nSub; st++)
+        dzfull += op->d[MD_DSH + st];
+  op->d[MD_DZFULL] = dzfull;
   if (KnL[0])
     flags |= MF_KNL0;
   if (KnL[1])

@@ -315,6 +315,9 @@ __device__ __forceinline__ bool op_mult(const trk_op *__restrict__ op, Part &p, 
     const double drift = __ldg(&d[MD_DRIFT]);
     if (isnan(x) || isnan(xp) || isnan(y) || isnan(yp) || fabs(x) > TRK_COORD_LIMIT || fabs(y) > TRK_COORD_LIMIT ||
         fabs(xp) > TRK_SLOPE_LIMIT || fabs(yp) > TRK_SLOPE_LIMIT) {
+      /* the reference records the previous particle's dzLoss here; taken
+       * as that of a particle that went through (MD_DZFULL) */
+      dzLoss = __ldg(&d[MD_DZFULL]);
       ok = false;
       goto done;
     }
@@ -398,6 +401,22 @@ __device__ __forceinline__ bool op_mult(const trk_op *__restrict__ op, Part &p, 
           ok = false;
           goto done;
         }
+#if !TRK_FAST
+        /* the radiation block's (1 + dp) divide/multiply round trip, entered
+         * for every kick with drift since isr_coef != 0 for Po > 0
+         * (src/multipole.c:1359-1389, :757-760); it can move qx, qy by an
+         * ulp.  The fast build leaves it out. */
+        if (drift != 0) {
+          qx /= (1 + dp);
+          qy /= (1 + dp);
+          qx *= (1 + dp);
+          qy *= (1 + dp);
+          if (!momenta_to_slopes(xp, yp, qx, qy, dp, expand)) {
+            ok = false;
+            goto done;
+          }
+        }
+#endif
       }
     }
     if (!check_aperture(x + mdx, y + mdy, ap, aptilt, apc, aps)) {
@@ -994,6 +1013,8 @@ __device__ __forceinline__ bool op_mult1_fast(const trk_op *__restrict__ op, Par
   double dzLoss = 0;
   bool ok = !(isnan(x) || isnan(xp) || isnan(y) || isnan(yp) || fabs(x) > TRK_COORD_LIMIT ||
               fabs(y) > TRK_COORD_LIMIT || fabs(xp) > TRK_SLOPE_LIMIT || fabs(yp) > TRK_SLOPE_LIMIT);
+  if (!ok)
+    dzLoss = __ldg(&d[MD_DZFULL]); /* as in op_mult */
   if (ok) {
     const double r = (1 + dp) * rsqrt_fast(fma(yp, yp, fma(xp, xp, 1.0)));
     double qx = xp * r, qy = yp * r;

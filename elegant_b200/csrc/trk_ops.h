@@ -95,6 +95,7 @@ typedef struct {
 #define MD_KY 50  /* 8 values -ykick*kickFrac */
 #define MD_DRIFT 58 /* drift per slice (nonzero test) */
 #define MD_COEF 59  /* expansion coefficients for orders 0..3 packed: order n at MD_COEF + n*(n+1)/2 */
+#define MD_DZFULL 70 /* dzLoss of a particle that went through the whole body (substep lengths summed in order) */
 /* i: 0 n_parts, 1 nSub, 2 expand, 3 maxOrder, 4 orders (o0 | o1<<8 | o2<<16), 5 skew bits, 6 flags */
 
 /* BEND */

@@ -126,3 +126,75 @@ def csbend_field_table(lattice, element):
                                            ctypes.byref(hn), ctypes.byref(hs)))
     nat.close()
     return Fx.reshape(11, 11), Fy.reshape(11, 11), eo1.value, hn.value, hs.value
+
+
+# ------------------------------------------------------------------------
+# oracle/_ref/libref.so: elegant's own tracking sources compiled from the
+# reference tree (oracle/ref/Makefile) and driven by oracle/ref/ref_driver.c.
+# Present only where the reference sources were available to build it.
+REF_LIB = os.path.join(HERE, "_ref", "libref.so")
+_ref = None
+
+
+def ref_available():
+    return os.path.exists(REF_LIB)
+
+
+def load_ref():
+    global _ref
+    if _ref is not None:
+        return _ref
+    if not ref_available():
+        raise FileNotFoundError(f"{REF_LIB} is not built (make -C oracle/ref with the reference sources present)")
+    lib = ctypes.CDLL(REF_LIB)
+    P, D, L, I = ctypes.c_void_p, ctypes.c_double, ctypes.c_long, ctypes.c_int
+    DP = ctypes.POINTER(ctypes.c_double)
+    lib.trk_last_error.restype = ctypes.c_char_p
+    lib.trk_lattice_create.argtypes = [ctypes.POINTER(P)]
+    lib.trk_lattice_destroy.argtypes = [P]
+    lib.trk_lattice_add.argtypes = [P, I, ctypes.c_char_p, ctypes.POINTER(I)]
+    lib.trk_lattice_set.argtypes = [P, I, ctypes.c_char_p, D]
+    lib.trk_lattice_set_wake.argtypes = [P, I, DP, DP, DP, L]
+    lib.trk_lattice_length.argtypes = [P]
+    lib.trk_param_count.argtypes = [I]
+    lib.trk_param_name.argtypes = [I, I]
+    lib.trk_param_name.restype = ctypes.c_char_p
+    lib.trk_param_default.argtypes = [I, I]
+    lib.trk_param_default.restype = D
+    lib.ref_track.argtypes = [P, DP, L, L, L, DP, ctypes.POINTER(_Result)]
+    lib.ref_set_cr_math.argtypes = [I]
+    lib.ref_set_exact_sums.argtypes = [I]
+    lib.ref_param_defaults.argtypes = [I, DP, I]
+    _ref = lib
+    return lib
+
+
+def track_ref(lattice, beam, n_passes, p_central, pass_offset=0, exact_sums=False, cr_math=False):
+    """As track(), through elegant's own element functions."""
+    lib = load_ref()
+    lib.ref_set_exact_sums(1 if exact_sums else 0)
+    lib.ref_set_cr_math(1 if cr_math else 0)
+    nat = lattice.native(lib)
+    rows = np.zeros((beam.shape[0], STRIDE), dtype=np.float64)
+    rows[:, :7] = beam[:, :7]
+    pc = ctypes.c_double(p_central)
+    res = _Result()
+    try:
+        _check(lib, lib.ref_track(nat.ptr, rows.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), rows.shape[0],
+                                  n_passes, pass_offset, ctypes.byref(pc), ctypes.byref(res)))
+    finally:
+        nat.close()
+        lib.ref_set_exact_sums(0)
+        lib.ref_set_cr_math(0)
+    return rows, res.n_left, res.particle_passes
+
+
+def ref_param_defaults(type_code):
+    """The reference's default of each parameter of the lattice tables
+    (NaN where the reference table lacks the name)."""
+    lib = load_ref()
+    out = np.zeros(64)
+    n = lib.ref_param_defaults(type_code, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 64)
+    if n < 0:
+        raise RuntimeError("bad type")
+    return out[:n]

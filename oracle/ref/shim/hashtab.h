@@ -1,0 +1,2 @@
+/* shim: see mdb.h */
+#include "mdb.h"

@@ -405,8 +405,12 @@ static long multipole_tracking2(double *coord, long n_part, const trk_elem *e, d
     exact_drift(coord, n_part, lEnd);
 
   long i_top = n_part - 1;
+  /* one dzLoss for the whole call, as in the reference (src/multipole.c:686):
+   * integrate_kick_multipole_ordn resets it only after its entry checks
+   * (:1179-1186, :1232), so a particle rejected there is recorded at
+   * z_start plus the previous particle's dzLoss */
+  double dzLoss = 0;
   for (long i_part = 0; i_part <= i_top; i_part++) {
-    double dzLoss = 0;
     if (!orc_integrate_kick_multipole(ROW(i_part), &m, Po, &ap, &dzLoss)) {
       swap_rows(ROW(i_part), ROW(i_top));
       ROW(i_top)[4] = z_start + dzLoss;

@@ -301,6 +301,18 @@ static int orc_integrate_kick_multipole(orc_r *coord, const orc_mult *m, double 
         orc_mkick(&qx, &qy, NULL, NULL, xpow, ypow, 0, -ykick * kickFrac[step], 1);
       if (!orc_momenta_to_slopes(&xp, &yp, qx, qy, dp, m->expand))
         return 0;
+      /* (rad_coef || isr_coef) && drift (src/multipole.c:1359-1389): isr_coef
+       * is nonzero whenever Po > 0 (negated when ISR is off, :757-760), so
+       * after every kick the momenta are divided by (1 + dp) and multiplied
+       * back, which can move them by an ulp, and the slopes are recomputed. */
+      if (drift) {
+        qx /= (1 + dp);
+        qy /= (1 + dp);
+        qx *= (1 + dp);
+        qy *= (1 + dp);
+        if (!orc_momenta_to_slopes(&xp, &yp, qx, qy, dp, m->expand))
+          return 0;
+      }
     }
   }
   (void)delta_qx;

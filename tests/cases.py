@@ -1,0 +1,43 @@
+"""Single-element lattices shared by the parity suites (GPU vs oracle,
+oracle vs the reference's own code)."""
+import math
+
+from elegant_b200 import Lattice
+
+
+def single(type_name, **params):
+    lat = Lattice()
+    lat.add(type_name, type_name, **params)
+    return lat
+
+
+ELEMENT_CASES = {
+    "drif": single("DRIF", L=1.3),
+    "drif_order1": single("DRIF", L=0.7, ORDER=1),
+    "edrift": single("EDRIFT", L=2.1),
+    "kquad": single("KQUAD", L=0.3, K1=1.2, N_KICKS=8),
+    "kquad_order2": single("KQUAD", L=0.3, K1=-1.1, N_SLICES=5, INTEGRATION_ORDER=2),
+    "kquad_order6": single("KQUAD", L=0.5, K1=0.8, N_SLICES=3, INTEGRATION_ORDER=6),
+    "kquad_misaligned": single("KQUAD", L=0.3, K1=1.2, N_KICKS=8, DX=1e-4, DY=-2e-4, DZ=1e-3, TILT=0.01),
+    "kquad_kicks_fse": single("KQUAD", L=0.4, K1=0.9, N_KICKS=12, HKICK=1e-5, VKICK=-2e-5, FSE=1e-3),
+    "kquad_leff": single("KQUAD", L=0.4, K1=0.9, N_KICKS=4, LEFFECTIVE=0.35),
+    "kquad_expand": single("KQUAD", L=0.3, K1=1.2, N_KICKS=8, EXPAND_HAMILTONIAN=1),
+    "ksext": single("KSEXT", L=0.2, K2=40.0, N_KICKS=4),
+    "ksext_k1j1": single("KSEXT", L=0.2, K2=-30.0, K1=0.01, J1=0.02, N_SLICES=2, TILT=0.1),
+    "koct": single("KOCT", L=0.2, K3=500.0),
+    "csbend": single("CSBEND", L=1.0, ANGLE=2 * math.pi / 80, N_KICKS=16),
+    "csbend_negative": single("CSBEND", L=1.0, ANGLE=-0.05, N_KICKS=8),
+    "csbend_k1": single("CSBEND", L=1.0, ANGLE=2 * math.pi / 280, K1=-0.4, N_KICKS=32),
+    "csbend_k1k2": single("CSBEND", L=0.8, ANGLE=0.03, K1=0.3, K2=5.0, N_SLICES=10),
+    "csbend_edges": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=0.03, N_SLICES=8),
+    "csbend_edges_fringe": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=0.03, HGAP=0.02, FINT=0.5, N_SLICES=8),
+    "csbend_edge_order2": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=0.03, EDGE_ORDER=2, K1=0.2, N_SLICES=8),
+    "csbend_edge3": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=0.03, EDGE1_EFFECTS=3, EDGE2_EFFECTS=3,
+                           N_SLICES=8),
+    "csbend_misaligned": single("CSBEND", L=1.0, ANGLE=0.05, DX=1e-4, DY=2e-4, DZ=-1e-4, TILT=0.02, N_SLICES=8),
+    "csbend_order6": single("CSBEND", L=1.0, ANGLE=0.05, N_SLICES=4, INTEGRATION_ORDER=6),
+    "rfca_thin": single("RFCA", L=0.0, VOLT=4e6, FREQ=352e6, PHASE=170.0),
+    "rfca_long": single("RFCA", L=0.5, VOLT=2e6, FREQ=500e6, PHASE=160.0, N_KICKS=5, END1_FOCUS=1, END2_FOCUS=1),
+    "rfca_tref": single("RFCA", L=0.0, VOLT=1e6, FREQ=352e6, PHASE=90.0, T_REFERENCE=1e-12),
+    "rfca_zero_volt": single("RFCA", L=0.3, VOLT=0.0),
+}
