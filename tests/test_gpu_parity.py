@@ -225,3 +225,32 @@ def test_trwake_exact_sums(tracker):
     assert r["same_survivors"]
     # transverse bin sums are FP64 atomics (order-dependent in the last bit)
     assert r["max_err"] < 1e-12, r
+
+
+@pytest.mark.skipif(not pyoracle.ref_available(), reason="oracle/_ref/libref.so not built")
+@pytest.mark.parametrize("lattice", ["fodo", "rf_wake", "lossy"])
+def test_parity_build_vs_reference_code(tracker, lattice):
+    """The parity build against elegant's own tracking code (compiled from the
+    reference sources, run with correctly rounded sin/cos/asin/tan and
+    double-double beam sums): bit-exact survivors, identical losses."""
+    if lattice == "fodo":
+        lat, passes = configs.c1_lattice(cells=4), 3
+        beam = configs.gaussian_beam(2000, seed=31)
+    elif lattice == "rf_wake":
+        lat, passes = configs.c2_lattice(cells=4, n_bins=400), 3
+        beam = configs.gaussian_beam(3000, seed=32)
+    else:
+        lat = Lattice()
+        lat.add("MAXAMP", "AP", X_MAX=0.004, Y_MAX=0.003, ELLIPTICAL=1)
+        lat.extend(configs.c2_lattice(cells=2, n_bins=200))
+        passes = 3
+        beam = configs.gaussian_beam(2000, seed=33, sigma_x=2e-3, sigma_xp=2e-4)
+    nl, g, lp, le, _ = gpu_run(tracker, lat, beam, passes, PC, fast=False)
+    rows, nlr, _ = pyoracle.track_ref(lat, beam, passes, PC, exact_sums=True, cr_math=True)
+    r = compare(g, rows, nl, nlr)
+    assert r["same_survivors"] and r["bit_exact"] and r["lost_equal"], r
+    o = rows[np.argsort(rows[:, 6])]
+    lost = o[:, 7] >= 0
+    gi = np.argsort(g[:, 6])
+    assert np.array_equal(lp[gi][lost], o[lost, 7].astype(np.int64))
+    assert np.array_equal(le[gi][lost], o[lost, 8].astype(np.int32))
