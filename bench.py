@@ -20,8 +20,10 @@ roofline: FP64 bound; achieved = algorithmic FP64 flops per particle-turn
         sources (oracle/_ref/libref.so; the oracle restatement where that
         was not built) on all host cores, process-parallel by particle
         shards.
-Multi-GPU: one process per GPU; each rank tracks its own particle shard
-(weak scaling), the wake histogram and time statistics are all-reduced.
+Multi-GPU: one process per GPU; each rank tracks its own particle shard of
+1e6 particles (weak scaling); the library's NCCL communicator exchanges the
+beam time statistics (all-gather) and the wake histogram (all-reduce) at the
+WAKE element of every turn, the RF fiducial statistics on the first pass.
 """
 import argparse
 import json
@@ -225,6 +227,14 @@ def run_gpu(args, rank, world, local):
     fast = not args.exact
     flops = load_flops()
     with Tracker(local) as trk:
+        if world > 1:
+            # the library's own NCCL communicator for the wake/RF exchanges
+            import elegant_b200
+            import torch.distributed as dist
+            uid = elegant_b200.nccl_unique_id() if rank == 0 else bytes(128)
+            t = torch.tensor(list(uid), dtype=torch.uint8, device=f"cuda:{local}")
+            dist.broadcast(t, 0)
+            trk.set_comm(bytes(t.cpu().tolist()), world, rank)
         trk.load(beam)
         pass_index = 0
         for _ in range(max(args.warmup, 3)):

@@ -61,6 +61,9 @@ def _declare(lib):
     DP = ctypes.POINTER(ctypes.c_double)
     sig = {
         "trk_last_error": (ctypes.c_char_p, []),
+        "trk_comm_get_unique_id": (I, [P]),
+        "trk_context_set_comm": (I, [P, P, I, I]),
+        "trk_context_comm": (I, [P, ctypes.POINTER(I), ctypes.POINTER(I)]),
         "trk_abi_version": (I, []),
         "trk_type_code": (I, [ctypes.c_char_p]),
         "trk_param_count": (I, [I]),
@@ -263,6 +266,12 @@ class Tracker:
         _check(self.lib, self.lib.trk_beam_store(self.ctx, _dptr(out), stride, ctypes.byref(n_left), None, None))
         return n_left.value, out
 
+    def set_comm(self, unique_id, nranks, rank):
+        """Join a sharded run: `unique_id` (128 bytes from nccl_unique_id() on
+        one rank) shared by all ranks; nranks <= 0 leaves it."""
+        buf = ctypes.create_string_buffer(bytes(unique_id), 128)
+        _check(self.lib, self.lib.trk_context_set_comm(self.ctx, buf, nranks, rank))
+
     def count(self):
         n = ctypes.c_long()
         _check(self.lib, self.lib.trk_beam_count(self.ctx, ctypes.byref(n)))
@@ -301,6 +310,14 @@ class Tracker:
         return Stats(n_total=st.n_total, n_left=st.n_left, particle_passes=st.particle_passes,
                      device_ms=st.device_ms, kernel_launches=st.kernel_launches, p_central=st.p_central,
                      track_ms=st.track_ms, track_launches=st.track_launches)
+
+
+def nccl_unique_id():
+    """128-byte NCCL id for Tracker.set_comm (call on one rank, share it)."""
+    lib = load_library()
+    buf = ctypes.create_string_buffer(128)
+    _check(lib, lib.trk_comm_get_unique_id(buf))
+    return buf.raw
 
 
 def _lattice_signature(lat):

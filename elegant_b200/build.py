@@ -55,6 +55,10 @@ def objects():
     o = os.path.join(BUILD, "trk_compile.o")
     out.append((src, o, ["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math"] + INC +
                 ["-c", src, "-o", o]))
+    src = os.path.join(CSRC, "trk_comm.cpp")
+    o = os.path.join(BUILD, "trk_comm.o")
+    out.append((src, o, ["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off"] + INC +
+                ["-I/usr/local/cuda/include", "-c", src, "-o", o]))
     src = os.path.join(CSRC, "trk_lattice.c")
     o = os.path.join(BUILD, "trk_lattice.o")
     out.append((src, o, ["gcc", "-std=gnu11", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math"] + INC +
@@ -75,7 +79,7 @@ def build(verbose=False):
             _run(cmd, verbose)
         objs.append(o)
     if _newer(LIB, objs):
-        _run([NVCC, "-shared", "-cudart", "static"] + ARCH + ["-o", LIB] + objs, verbose)
+        _run([NVCC, "-shared", "-cudart", "static"] + ARCH + ["-o", LIB] + objs + ["-ldl"], verbose)
     return LIB
 
 

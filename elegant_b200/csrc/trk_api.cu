@@ -21,6 +21,7 @@
 #include "trk.h"
 #include "trk_compile.h"
 #include "trk_constants.h"
+#include "trk_comm.h"
 #include "trk_kernels.h"
 #include "trk_lattice.h"
 
@@ -70,7 +71,10 @@ struct trk_context {
   double *d_part = nullptr; /* hi, lo, min, max per block */
   long long *d_part_n = nullptr;
   int part_cap = 0;
-  double *d_stats = nullptr; /* 4 doubles */
+  double *d_stats = nullptr; /* 6 doubles: sum, n, min, max, sum_hi, sum_lo */
+  trk_comm *comm = nullptr;  /* set for sharded runs (trk_context_set_comm) */
+  long long *d_i64 = nullptr; /* one int64 for count exchanges */
+  double *d_gather = nullptr; /* 6 doubles per rank */
   long long *d_effort = nullptr;
   /* wakes, keyed by op index */
   std::vector<std::pair<int, WakeBuffers>> wake_bufs;
@@ -85,6 +89,7 @@ struct trk_context {
   long perm_cap = 0;
   long passes_done = 0; /* passes tracked since the beam was loaded */
   long n_original = 0;  /* particles at the start of the run (do_tracking's nOriginal) */
+  long n_global = 0;    /* the same summed over the ranks of a sharded run */
   int tuned_variant = -1; /* tracking-kernel variant used when trk_run.variant < 0 (-1: by lattice class) */
   int last_launches = 0;
 };
@@ -397,6 +402,17 @@ int time_stats(trk_context *ctx, bool fast, int mode, double sOffset, double Po)
   else
     trk_exact::launch_time_stats(t, blocks, ctx->stream);
   ctx->last_launches += 2;
+  if (ctx->comm) {
+    /* every rank's {sum, n, min, max}, combined in rank order on each rank */
+    const int R = trk_comm_size(ctx->comm);
+    if ((rc = trk_comm_gather_f64(ctx->comm, ctx->d_stats, ctx->d_gather, 6, ctx->stream)))
+      return rc;
+    if (fast)
+      trk_fast::launch_stats_combine(ctx->d_gather, R, ctx->d_stats, ctx->stream);
+    else
+      trk_exact::launch_stats_combine(ctx->d_gather, R, ctx->d_stats, ctx->stream);
+    ctx->last_launches++;
+  }
   return TRK_OK;
 }
 
@@ -459,8 +475,8 @@ int run_wake(trk_context *ctx, bool fast, int opi, long pass, long fresh_pass, d
     /* CHARGE element (src/do_tracking.c:797-812) */
     const trk_elem *ce = &lat->e[charge_elem];
     double macro = 0;
-    if (ctx->n_original)
-      macro = TRK_P(ce, CHARGE_TOTAL) / ctx->n_original;
+    if (ctx->n_global)
+      macro = TRK_P(ce, CHARGE_TOTAL) / ctx->n_global;
     if (TRK_P(ce, CHARGE_PER_PARTICLE))
       macro = TRK_P(ce, CHARGE_PER_PARTICLE);
     a.macro_mode = 0;
@@ -520,9 +536,22 @@ int run_wake(trk_context *ctx, bool fast, int opi, long pass, long fresh_pass, d
   } else
     CUDA_TRY(cudaMemsetAsync(wb->counts, 0, sizeof(unsigned long long) * nb, ctx->stream));
   if (fast)
-    trk_fast::launch_wake(a, grid, ctx->stream);
+    trk_fast::launch_wake_bin(a, grid, ctx->stream);
   else
-    trk_exact::launch_wake(a, grid, ctx->stream);
+    trk_exact::launch_wake_bin(a, grid, ctx->stream);
+  if (ctx->comm) {
+    /* histogram sum over ranks (src/wake.c:226-233, src/trwake.c:195-204) */
+    if (w.transverse) {
+      if ((rc = trk_comm_sum_f64(ctx->comm, wb->hist_x, nb, ctx->stream)) ||
+          (rc = trk_comm_sum_f64(ctx->comm, wb->hist_y, nb, ctx->stream)))
+        return rc;
+    } else if ((rc = trk_comm_sum_u64(ctx->comm, wb->counts, nb, ctx->stream)))
+      return rc;
+  }
+  if (fast)
+    trk_fast::launch_wake_apply(a, grid, ctx->stream);
+  else
+    trk_exact::launch_wake_apply(a, grid, ctx->stream);
   ctx->last_launches += w.transverse ? 5 : 4;
   return TRK_OK;
 }
@@ -606,7 +635,7 @@ int trk_context_create(trk_context **out, int device) {
     ctx->sm_count = prop.multiProcessorCount;
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
-      cudaMalloc(&ctx->d_status, sizeof(int)) != cudaSuccess || cudaMalloc(&ctx->d_stats, 4 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&ctx->d_status, sizeof(int)) != cudaSuccess || cudaMalloc(&ctx->d_stats, 6 * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&ctx->d_effort, sizeof(long long)) != cudaSuccess) {
     trk_context_destroy(ctx);
     return trk_set_error(TRK_ERR_CUDA, "context set-up failed");
@@ -639,6 +668,9 @@ void trk_context_destroy(trk_context *ctx) {
   cudaFree(ctx->d_part);
   cudaFree(ctx->d_part_n);
   cudaFree(ctx->d_stats);
+  cudaFree(ctx->d_gather);
+  cudaFree(ctx->d_i64);
+  trk_comm_destroy(ctx->comm);
   cudaFree(ctx->d_effort);
   cudaFree(ctx->d_aos);
   cudaFree(ctx->d_cub);
@@ -681,6 +713,7 @@ int trk_beam_load(trk_context *ctx, const double *coord, long np, long stride) {
   ctx->np = np;
   reset_run_state(ctx);
   ctx->n_original = np;
+  ctx->n_global = np;
   if (np == 0)
     return TRK_OK;
   CUDA_TRY(cudaMemcpyAsync(ctx->d_aos, coord, sizeof(double) * np * stride, cudaMemcpyHostToDevice, ctx->stream));
@@ -700,6 +733,7 @@ int trk_beam_load_device(trk_context *ctx, const double *d_soa, long np, long ld
   ctx->np = np;
   reset_run_state(ctx);
   ctx->n_original = np;
+  ctx->n_global = np;
   if (np == 0)
     return TRK_OK;
   soa_copy_kernel<<<(int)((np + 255) / 256), 256, 0, ctx->stream>>>(d_soa, ld, np, ctx->d_cols, ctx->cap,
@@ -806,6 +840,42 @@ int trk_beam_store(trk_context *ctx, double *coord, long stride, long *n_left, l
   return TRK_OK;
 }
 
+static int ensure_i64(trk_context *ctx) {
+  if (!ctx->d_i64)
+    CUDA_TRY(cudaMalloc(&ctx->d_i64, sizeof(long long)));
+  return TRK_OK;
+}
+
+int trk_comm_get_unique_id(void *id128) { return trk_comm_unique_id(id128); }
+
+int trk_context_set_comm(trk_context *ctx, const void *id128, int nranks, int rank) {
+  if (!ctx)
+    return trk_set_error(TRK_ERR_ARG, "null context");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  trk_comm_destroy(ctx->comm);
+  ctx->comm = nullptr;
+  cudaFree(ctx->d_gather);
+  ctx->d_gather = nullptr;
+  if (nranks <= 0)
+    return TRK_OK;
+  int rc = trk_comm_create(&ctx->comm, id128, nranks, rank, ctx->device);
+  if (rc)
+    return rc;
+  CUDA_TRY(cudaMalloc(&ctx->d_gather, sizeof(double) * 6 * nranks));
+  return TRK_OK;
+}
+
+int trk_context_comm(const trk_context *ctx, int *rank, int *nranks) {
+  if (!ctx)
+    return trk_set_error(TRK_ERR_ARG, "null context");
+  if (rank)
+    *rank = trk_comm_rank(ctx->comm);
+  if (nranks)
+    *nranks = trk_comm_size(ctx->comm);
+  return TRK_OK;
+}
+
 /* per-launch timing events for trk_run.time_kernels (created on demand,
  * reused across calls) */
 #define TRK_MAX_TIMED 4096
@@ -849,7 +919,21 @@ int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, 
       ctx->d_cols, ctx->cap, ctx->d_lost_pass, ctx->d_lost_elem, ctx->np, p0, Po);
     ctx->last_launches++;
   }
-  if (ctx->np > 0 && run->n_passes > 0 && !c.ops.empty()) {
+  if (ctx->comm && fresh >= 0) {
+    /* total_nOriginal of a sharded run (src/do_tracking.c:1378-1381) */
+    long long n = ctx->n_original;
+    if ((rc = ensure_i64(ctx)))
+      return rc;
+    CUDA_TRY(cudaMemcpyAsync(ctx->d_i64, &n, sizeof(n), cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = trk_comm_sum_i64(ctx->comm, ctx->d_i64, 1, ctx->stream)))
+      return rc;
+    CUDA_TRY(cudaMemcpyAsync(&n, ctx->d_i64, sizeof(n), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    ctx->n_global = (long)n;
+  }
+  /* every rank of a sharded run takes the same collective steps, so a rank
+   * whose shard is empty still runs the schedule (its kernels see n = 0) */
+  if ((ctx->np > 0 || ctx->comm) && run->n_passes > 0 && !c.ops.empty()) {
     TrackArgs ta = track_args(ctx);
     ta.fresh_pass = fresh;
     ta.Po = Po;

@@ -1671,22 +1671,71 @@ __global__ void __launch_bounds__(TRK_BLOCK) time_stats_kernel(TimeStatsArgs a) 
 }
 
 /* Combine block partials in index order; write {sum, n, min, max}. */
-__global__ void time_stats_finish_kernel(TimeStatsArgs a, int nblocks) {
-  if (threadIdx.x != 0 || blockIdx.x != 0)
-    return;
+/* Sum of the block partials: 256 threads each add a strided subset in order,
+ * then a fixed-order tree; out = {sum, count, min, max, sum_hi, sum_lo} with
+ * sum the double-double total rounded once. */
+#define TRK_FINISH_THREADS 256
+__global__ void __launch_bounds__(TRK_FINISH_THREADS) time_stats_finish_kernel(TimeStatsArgs a, int nblocks) {
+  __shared__ double s_hi[TRK_FINISH_THREADS], s_lo[TRK_FINISH_THREADS], s_min[TRK_FINISH_THREADS],
+    s_max[TRK_FINISH_THREADS];
+  __shared__ long long s_n[TRK_FINISH_THREADS];
+  const int t = threadIdx.x;
   trkcr_dd acc = trkcr_make(0.0, 0.0);
   double tmin = 1.7976931348623157e308, tmax = -1.7976931348623157e308;
   long long n = 0;
-  for (int b = 0; b < nblocks; b++) {
+  for (int b = t; b < nblocks; b += TRK_FINISH_THREADS) {
     acc = trkcr_add(acc, trkcr_make(a.part_hi[b], a.part_lo[b]));
     tmin = fmin(tmin, a.part_min[b]);
     tmax = fmax(tmax, a.part_max[b]);
     n += a.part_n[b];
   }
-  a.out[0] = __dadd_rn(acc.hi, acc.lo);
-  a.out[1] = (double)n;
-  a.out[2] = tmin;
-  a.out[3] = tmax;
+  s_hi[t] = acc.hi;
+  s_lo[t] = acc.lo;
+  s_min[t] = tmin;
+  s_max[t] = tmax;
+  s_n[t] = n;
+  __syncthreads();
+  for (int w = TRK_FINISH_THREADS / 2; w > 0; w >>= 1) {
+    if (t < w) {
+      const trkcr_dd r = trkcr_add(trkcr_make(s_hi[t], s_lo[t]), trkcr_make(s_hi[t + w], s_lo[t + w]));
+      s_hi[t] = r.hi;
+      s_lo[t] = r.lo;
+      s_min[t] = fmin(s_min[t], s_min[t + w]);
+      s_max[t] = fmax(s_max[t], s_max[t + w]);
+      s_n[t] += s_n[t + w];
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    a.out[0] = __dadd_rn(s_hi[0], s_lo[0]);
+    a.out[1] = (double)s_n[0];
+    a.out[2] = s_min[0];
+    a.out[3] = s_max[0];
+    a.out[4] = s_hi[0];
+    a.out[5] = s_lo[0];
+  }
+}
+
+/* Combine the statistics all-gathered from `ranks` ranks (6 doubles each, as
+ * written by time_stats_finish_kernel) in rank order. */
+__global__ void stats_combine_kernel(const double *gathered, int ranks, double *out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0)
+    return;
+  trkcr_dd acc = trkcr_make(0.0, 0.0);
+  double n = 0, tmin = 1.7976931348623157e308, tmax = -1.7976931348623157e308;
+  for (int r = 0; r < ranks; r++) {
+    const double *g = gathered + 6 * r;
+    acc = trkcr_add(acc, trkcr_make(g[4], g[5]));
+    n += g[1];
+    tmin = fmin(tmin, g[2]);
+    tmax = fmax(tmax, g[3]);
+  }
+  out[0] = __dadd_rn(acc.hi, acc.lo);
+  out[1] = n;
+  out[2] = tmin;
+  out[3] = tmax;
+  out[4] = acc.hi;
+  out[5] = acc.lo;
 }
 
 /* RFCA fiducial: phase_fiducial = -omega * tmean (src/simple_rfca.c:412-445) */
@@ -2013,7 +2062,7 @@ void launch_track(const TrackArgs &a, int variant, bool lean, long n, int max_bl
 
 void launch_time_stats(const TimeStatsArgs &a, int grid, cudaStream_t st) {
   time_stats_kernel<<<grid, TRK_BLOCK, 0, st>>>(a);
-  time_stats_finish_kernel<<<1, 1, 0, st>>>(a, grid);
+  time_stats_finish_kernel<<<1, TRK_FINISH_THREADS, 0, st>>>(a, grid);
 }
 
 void launch_rf_fiducial(const double *stats, double omega, double t_reference, double *rf_phase, int slot,
@@ -2022,14 +2071,28 @@ void launch_rf_fiducial(const double *stats, double omega, double t_reference, d
 }
 
 void launch_wake(const WakeArgs &a, int grid, cudaStream_t st) {
+  launch_wake_bin(a, grid, st);
+  launch_wake_apply(a, grid, st);
+}
+
+/* geometry and histogram (the part before the cross-rank histogram sum) */
+void launch_wake_bin(const WakeArgs &a, int grid, cudaStream_t st) {
   wake_setup_kernel<<<1, 1, 0, st>>>(a);
   size_t smem = a.transverse ? 0 : (size_t)a.smem_bins * sizeof(unsigned int);
   wake_bin_kernel<<<grid, TRK_BLOCK, smem, st>>>(a);
+}
+
+/* convolution and kicks (after it) */
+void launch_wake_apply(const WakeArgs &a, int grid, cudaStream_t st) {
   int cb = (int)((a.max_bins + 1 + 127) / 128);
   wake_convolve_kernel<<<cb, 128, 0, st>>>(a, 0);
   if (a.transverse)
     wake_convolve_kernel<<<cb, 128, 0, st>>>(a, 1);
   wake_kick_kernel<<<grid, TRK_BLOCK, 0, st>>>(a);
+}
+
+void launch_stats_combine(const double *gathered, int ranks, double *out, cudaStream_t st) {
+  stats_combine_kernel<<<1, 1, 0, st>>>(gathered, ranks, out);
 }
 
 void launch_rotate(const TrackArgs &a, double ca, double sa, int grid, cudaStream_t st) {

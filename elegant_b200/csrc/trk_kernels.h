@@ -48,7 +48,7 @@ struct TimeStatsArgs {
   double Po, sOffset;
   double *part_hi, *part_lo, *part_min, *part_max;
   long long *part_n;
-  double *out;     /* {sum, n, min, max} */
+  double *out;     /* {sum, n, min, max, sum_hi, sum_lo} */
 };
 
 struct WakeState {
@@ -104,6 +104,9 @@ struct WakeArgs {
   void launch_rf_fiducial(const double *stats, double omega, double t_reference, double *rf_phase, int slot, \
                           int *status, cudaStream_t st);                                                     \
   void launch_wake(const WakeArgs &a, int grid, cudaStream_t st);                                            \
+  void launch_wake_bin(const WakeArgs &a, int grid, cudaStream_t st);                                        \
+  void launch_wake_apply(const WakeArgs &a, int grid, cudaStream_t st);                                      \
+  void launch_stats_combine(const double *gathered, int ranks, double *out, cudaStream_t st);                \
   void launch_rotate(const TrackArgs &a, double ca, double sa, int grid, cudaStream_t st);                   \
   cudaError_t set_coefficients(const double *coef10);                                                        \
   }

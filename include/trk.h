@@ -151,6 +151,21 @@ void trk_context_destroy(trk_context *ctx);
 /* The CUDA stream (cudaStream_t) all work of the context is ordered on. */
 void *trk_context_stream(trk_context *ctx);
 
+/* Sharded tracking across GPUs (one process per GPU, each rank holding its
+ * own block of particles), replacing Pelegant's MPI exchanges
+ * (src/wake.c:226-233, src/trwake.c:195-204, src/simple_rfca.c:222-230,
+ * src/findGlobalMinMax.c:10) with NCCL collectives on the context's stream:
+ * beam time statistics are all-gathered and combined in rank order, wake
+ * histograms summed, the CHARGE element's particle count summed.
+ * trk_comm_get_unique_id is called on one rank and its 128 bytes passed to
+ * every rank's trk_context_set_comm (nranks <= 0 removes the communicator;
+ * nranks = 1 runs the exchanges on a one-rank communicator).
+ * Every rank must then call trk_track with the same lattice and pass range.
+ * NCCL (libnccl.so.2) is loaded at run time; TRK_ERR_NCCL if it is absent. */
+int trk_comm_get_unique_id(void *id128);
+int trk_context_set_comm(trk_context *ctx, const void *id128, int nranks, int rank);
+int trk_context_comm(const trk_context *ctx, int *rank, int *nranks);
+
 /* Copy a host AoS beam (np particles, `stride` doubles each, stride >= 7,
  * column 6 = particle id) to the device SoA.  Replaces gpuBaseInit's copy
  * (src/do_tracking.c:411-414). */

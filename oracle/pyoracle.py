@@ -47,6 +47,7 @@ def load():
     lib.orc_track.argtypes = [P, DP, L, L, L, DP, ctypes.POINTER(_Result)]
     lib.orc_track_element.argtypes = [P, I, DP, L, L, DP, ctypes.POINTER(L)]
     lib.orc_csbend_field_table.argtypes = [P, I, DP, DP, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)]
+    lib.orc_set_collective.argtypes = [I, ctypes.c_void_p, ctypes.c_void_p]
     lib.orc_set_exact_sums.argtypes = [I]
     lib.orc_set_cr_math.argtypes = [I]
     for f in ('orc_cr_sin', 'orc_cr_cos', 'orc_cr_asin', 'orc_cr_tan'):
@@ -84,6 +85,35 @@ class modes:
     def __exit__(self, *exc):
         set_exact_sums(False)
         set_cr_math(False)
+
+
+_GATHER = ctypes.CFUNCTYPE(None, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.c_long)
+_SUM = ctypes.CFUNCTYPE(None, ctypes.POINTER(ctypes.c_double), ctypes.c_long)
+_collective_refs = None
+
+
+def set_collective(world, gather=None, allsum=None):
+    """Shard the oracle's collective steps over `world` ranks.  gather(send)
+    returns the concatenation of every rank's send array (numpy float64);
+    allsum(buf) returns the element-wise sum over ranks.  world <= 1 resets."""
+    global _collective_refs
+    lib = load()
+    if world <= 1:
+        lib.orc_set_collective(1, None, None)
+        _collective_refs = None
+        return
+
+    def g(send, recv, n):
+        out = gather(np.ctypeslib.as_array(send, shape=(n,)).copy())
+        np.ctypeslib.as_array(recv, shape=(world * n,))[:] = out
+
+    def sm(buf, n):
+        a = np.ctypeslib.as_array(buf, shape=(n,))
+        a[:] = allsum(a.copy())
+
+    _collective_refs = (_GATHER(g), _SUM(sm))
+    lib.orc_set_collective(world, ctypes.cast(_collective_refs[0], ctypes.c_void_p),
+                           ctypes.cast(_collective_refs[1], ctypes.c_void_p))
 
 
 def track(lattice, beam, n_passes, p_central, pass_offset=0):

@@ -904,6 +904,55 @@ static double kahan_plus(double sum, double b, double *error) {
   return t;
 }
 
+/* ------------------------------------------------------- sharded runs
+ * The particle-sharded decomposition the multi-GPU library uses, restated
+ * so it can be tested on CPU ranks: each rank tracks its own particles and
+ * exchanges only beam time statistics ({sum as double-double, count, min,
+ * max}, gathered and combined in rank order), the wake histograms (summed)
+ * and the CHARGE particle count (summed) -- Pelegant's exchanges
+ * (src/wake.c:226-233, src/trwake.c:195-204, src/simple_rfca.c:222-230,
+ * src/do_tracking.c:1378-1381). */
+static int orc_world = 1;
+static orc_gather_fn orc_gather_cb = NULL;
+static orc_sum_fn orc_sum_cb = NULL;
+
+void orc_set_collective(int world, orc_gather_fn gather, orc_sum_fn sum) {
+  orc_world = (world > 1 && gather && sum) ? world : 1;
+  orc_gather_cb = gather;
+  orc_sum_cb = sum;
+}
+
+/* {hi, lo} double-double sum, count, min, max of this rank -> of all ranks */
+static void shard_stats(double *hi, double *lo, double *n, double *tmin, double *tmax) {
+  if (orc_world <= 1)
+    return;
+  double send[6] = {*hi + *lo, *n, *tmin, *tmax, *hi, *lo};
+  double *recv = (double *)malloc(sizeof(double) * 6 * orc_world);
+  orc_gather_cb(send, recv, 6);
+  trkcr_dd acc = trkcr_make(0.0, 0.0);
+  double N = 0, mn = DBL_MAX, mx = -DBL_MAX;
+  for (int r = 0; r < orc_world; r++) {
+    const double *g = recv + 6 * r;
+    acc = trkcr_add(acc, trkcr_make(g[4], g[5]));
+    N += g[1];
+    if (g[2] < mn)
+      mn = g[2];
+    if (g[3] > mx)
+      mx = g[3];
+  }
+  free(recv);
+  *hi = acc.hi;
+  *lo = acc.lo;
+  *n = N;
+  *tmin = mn;
+  *tmax = mx;
+}
+
+static void shard_sum(double *buf, long n) {
+  if (orc_world > 1)
+    orc_sum_cb(buf, n);
+}
+
 /* beta_from_delta (src/do_tracking.c:95-98) */
 static double beta_from_delta(double p, double delta) {
   p *= 1 + delta;
@@ -919,7 +968,7 @@ static long rf_cavity(double *coord, long np, const trk_elem *e, orc_rf_state *r
   long nKicks;
   double omega, volt, tau, dtLight, phase, t0, To;
   (void)To;
-  if (np <= 0)
+  if (np <= 0 && orc_world <= 1)
     return np;
   if (TRK_P(e, RFCA_CHANGE_T) || TRK_P(e, RFCA_LINEARIZE) || TRK_P(e, RFCA_LOCK_PHASE) || TRK_P(e, RFCA_CHANGE_P0) ||
       TRK_P(e, RFCA_STANDING_WAVE)) {
@@ -966,6 +1015,17 @@ static long rf_cavity(double *coord, long np, const trk_elem *e, orc_rf_state *r
       }
       if (orc_exact_sums)
         tsum = hi + lo;
+      if (orc_world > 1) {
+        /* KahanParallel over ranks (src/simple_rfca.c:222-230) */
+        double dn = (double)nsum, mn = DBL_MAX, mx = -DBL_MAX;
+        if (!orc_exact_sums) {
+          hi = tsum;
+          lo = 0;
+        }
+        shard_stats(&hi, &lo, &dn, &mn, &mx);
+        tsum = hi + lo;
+        nsum = (long)dn;
+      }
       t0 = tsum / nsum;
     }
     rs->phase_fiducial = -omega * t0;
@@ -1109,23 +1169,20 @@ static int track_through_wake(double *coord, long np, const trk_elem *e, double 
     return 1;
   if (wake_table_setup(e, &dt, &i0, (int)TRK_P(e, WAKE_ACAUSAL_ALLOWED)))
     return 1;
-  /* set_up_wake (src/wake.c:340-372) */
-  if (chargeMacro)
-    ws->macroParticleCharge = *chargeMacro;
-  else if (i_pass == 0) {
-    ws->macroParticleCharge = 0;
-    if (np)
-      ws->macroParticleCharge = TRK_P(e, WAKE_CHARGE) / np;
-  }
   long rampPasses = (long)TRK_P(e, WAKE_RAMP_PASSES);
   if (i_pass >= rampPasses - 1)
     rampFactor = 1;
   else
     rampFactor = (i_pass + 1.0) / rampPasses;
-  if (np <= 0)
+  if (np <= 0 && orc_world <= 1) {
+    if (!chargeMacro && i_pass == 0)
+      ws->macroParticleCharge = 0;
+    else if (chargeMacro)
+      ws->macroParticleCharge = *chargeMacro;
     return 0;
-  double *time = (double *)malloc(sizeof(double) * np);
-  long *pbin = (long *)malloc(sizeof(long) * np);
+  }
+  double *time = (double *)malloc(sizeof(double) * (np > 0 ? np : 1));
+  long *pbin = (long *)malloc(sizeof(long) * (np > 0 ? np : 1));
   /* computeTimeCoordinatesOnly (src/trwake.c:519-527) */
   for (long ip = 0; ip < np; ip++) {
     double P = Po * (ROW(ip)[5] + 1);
@@ -1140,9 +1197,6 @@ static int track_through_wake(double *coord, long np, const trk_elem *e, double 
     else
       sum += time[ip];
   }
-  if (orc_exact_sums)
-    sum = sum + slo;
-  tmean = sum / np;
   tmin = DBL_MAX;
   tmax = -DBL_MAX;
   for (long ip = 0; ip < np; ip++) {
@@ -1150,6 +1204,19 @@ static int track_through_wake(double *coord, long np, const trk_elem *e, double 
       tmin = time[ip];
     if (time[ip] > tmax)
       tmax = time[ip];
+  }
+  double n_all = (double)np;
+  shard_stats(&sum, &slo, &n_all, &tmin, &tmax);
+  if (orc_exact_sums || orc_world > 1)
+    sum = sum + slo;
+  tmean = sum / n_all;
+  /* set_up_wake (src/wake.c:340-372) */
+  if (chargeMacro)
+    ws->macroParticleCharge = *chargeMacro;
+  else if (i_pass == 0) {
+    ws->macroParticleCharge = 0;
+    if (n_all)
+      ws->macroParticleCharge = TRK_P(e, WAKE_CHARGE) / n_all;
   }
   if ((tmax - tmin) > (e->wake_t[e->wake_points - 1] - e->wake_t[0]) && !TRK_P(e, WAKE_ALLOW_LONG_BEAM)) {
     free(time);
@@ -1180,6 +1247,7 @@ static int track_through_wake(double *coord, long np, const trk_elem *e, double 
     Itime[ib] += 1;
     pbin[ip] = ib;
   }
+  shard_sum(Itime, nb); /* src/wake.c:226-233 */
   Vtime[nb] = 0;
   convolve_arrays(Vtime, nb, Itime, nb, e->wake_w0, e->wake_points, i0);
   factor = ws->macroParticleCharge * TRK_PARTICLE_REL_SIGN * TRK_P(e, WAKE_FACTOR) * rampFactor;
@@ -1222,23 +1290,21 @@ static int track_through_trwake(double *coord, long np, const trk_elem *e, doubl
     return 1;
   if (wake_table_setup(e, &dt, &i0, (int)TRK_P(e, TRWAKE_ACAUSAL_ALLOWED)))
     return 1;
-  if (chargeMacro)
-    ws->macroParticleCharge = *chargeMacro;
-  else if (i_pass == 0) {
-    ws->macroParticleCharge = 0;
-    if (np)
-      ws->macroParticleCharge = TRK_P(e, TRWAKE_CHARGE) / np;
-  }
   long rampPasses = (long)TRK_P(e, TRWAKE_RAMP_PASSES);
   if (i_pass >= rampPasses - 1)
     rampFactor = 1;
   else
     rampFactor = (i_pass + 1.0) / rampPasses;
-  if (np <= 0)
+  if (np <= 0 && orc_world <= 1) {
+    if (chargeMacro)
+      ws->macroParticleCharge = *chargeMacro;
+    else if (i_pass == 0)
+      ws->macroParticleCharge = 0;
     return 0;
-  double *time = (double *)malloc(sizeof(double) * np);
-  long *pbin = (long *)malloc(sizeof(long) * np);
-  double *pz = (double *)calloc(np, sizeof(double));
+  }
+  double *time = (double *)malloc(sizeof(double) * (np > 0 ? np : 1));
+  long *pbin = (long *)malloc(sizeof(long) * (np > 0 ? np : 1));
+  double *pz = (double *)calloc(np > 0 ? np : 1, sizeof(double));
   for (long ip = 0; ip < np; ip++) {
     double P = Po * (ROW(ip)[5] + 1);
     time[ip] = ROW(ip)[4] * sqrt(orc_sqr(P) + 1) / (TRK_C_MKS * P);
@@ -1250,6 +1316,15 @@ static int track_through_trwake(double *coord, long np, const trk_elem *e, doubl
       tmin = time[ip];
     if (time[ip] > tmax)
       tmax = time[ip];
+  }
+  double shi = 0, slo = 0, n_all = (double)np;
+  shard_stats(&shi, &slo, &n_all, &tmin, &tmax);
+  if (chargeMacro)
+    ws->macroParticleCharge = *chargeMacro;
+  else if (i_pass == 0) {
+    ws->macroParticleCharge = 0;
+    if (n_all)
+      ws->macroParticleCharge = TRK_P(e, TRWAKE_CHARGE) / n_all;
   }
   if ((tmax - tmin) > (e->wake_t[e->wake_points - 1] - e->wake_t[0])) {
     free(time);
@@ -1303,6 +1378,8 @@ static int track_through_trwake(double *coord, long np, const trk_elem *e, doubl
     pbin[ip] = ib;
     pz[ip] = Po * (1 + c[5]) / sqrt(1 + orc_sqr(c[1]) + orc_sqr(c[3]));
   }
+  shard_sum(posItime[0], nb); /* src/trwake.c:195-204 */
+  shard_sum(posItime[1], nb);
   for (int plane = 0; plane < 2; plane++) {
     const double *W = plane ? e->wake_w1 : e->wake_w0;
     double factor = ws->macroParticleCharge * TRK_PARTICLE_REL_SIGN * TRK_P(e, TRWAKE_FACTOR);
@@ -1435,8 +1512,10 @@ static int run_state_init(const trk_lattice *l, long nOriginal, orc_run_state *r
       const trk_elem *e = &l->e[i];
       rs->have_charge = 1;
       rs->chargeMacro = 0;
-      if (nOriginal)
-        rs->chargeMacro = TRK_P(e, CHARGE_TOTAL) / nOriginal;
+      double nAll = (double)nOriginal;
+      shard_sum(&nAll, 1); /* total_nOriginal (src/do_tracking.c:1378-1381) */
+      if (nAll)
+        rs->chargeMacro = TRK_P(e, CHARGE_TOTAL) / nAll;
       if (TRK_P(e, CHARGE_PER_PARTICLE))
         rs->chargeMacro = TRK_P(e, CHARGE_PER_PARTICLE);
     }

@@ -45,6 +45,13 @@ double orc_cr_cos(double x);
 double orc_cr_asin(double x);
 double orc_cr_tan(double x);
 
+/* Sharded runs (test of the multi-GPU decomposition on CPU ranks): gather
+ * n doubles from every rank into recv[rank * n ...]; sum n doubles over
+ * ranks in place.  world <= 1 or NULL callbacks: a single process. */
+typedef void (*orc_gather_fn)(const double *send, double *recv, long n);
+typedef void (*orc_sum_fn)(double *buf, long n);
+void orc_set_collective(int world, orc_gather_fn gather, orc_sum_fn sum);
+
 /* Field-expansion table of a CSBEND as the oracle builds it (for tests):
  * Fx, Fy are 11x11 row-major, coefficient of x^i y^j at [i*11+j]. */
 int orc_csbend_field_table(const trk_lattice *lattice, int element, double *Fx, double *Fy, int *expansionOrder1,
