@@ -49,7 +49,8 @@ TRACK_DRAM_BYTES_PER_PARTICLE = 10.628e6 / 2e5
 
 def workload_config(n_particles):
     return {"workload": WORKLOAD, "particles_per_gpu": n_particles, "lattice": "40 FODO cells + KSEXT, RFCA, WAKE",
-            "wake_bins": 2000, "wake_points": 4096, "p_central": 13700.0, "l2": "flushed between timed steps"}
+            "wake_bins": 2000, "wake_points": 4096, "wake_dt_s": 5e-14, "charge_c": 1e-9, "p_central": 13700.0,
+            "l2": "flushed between timed steps"}
 
 
 def load_flops():

@@ -69,7 +69,7 @@ def resonator_wake(points=4096, dt=1e-12, f_r=20e9, r_over_q=1e3, q=5.0, seed=2,
     return t, W
 
 
-def c2_lattice(cells=40, with_rf=True, with_wake=True, n_bins=2000, wake_dt=1e-12, charge=1e-9, harmonic=329,
+def c2_lattice(cells=40, with_rf=True, with_wake=True, n_bins=2000, wake_dt=50e-15, charge=1e-9, harmonic=329,
                kq_errors=None, k2_errors=None):
     lat = Lattice()
     if with_wake:
