@@ -74,6 +74,8 @@ struct trk_context {
   double *d_stats = nullptr; /* 6 doubles: sum, n, min, max, sum_hi, sum_lo */
   trk_comm *comm = nullptr;  /* set for sharded runs (trk_context_set_comm) */
   long long *d_i64 = nullptr; /* one int64 for count exchanges */
+  double *d_matrix = nullptr; /* trk_track_matrix: C, R, T (168 doubles) */
+  size_t matrix_cap = 0;
   double *d_gather = nullptr; /* 6 doubles per rank */
   long long *d_effort = nullptr;
   /* wakes, keyed by op index */
@@ -286,10 +288,20 @@ TrackArgs track_args(trk_context *ctx) {
   return a;
 }
 
+int upload_compiled(trk_context *ctx);
+
 int upload_lattice(trk_context *ctx, const trk_lattice *lat, double Po) {
   int rc = trk_compile(lat, Po, ctx->comp);
   if (rc)
     return rc;
+  ctx->comp_src = lat;
+  return upload_compiled(ctx);
+}
+
+/* copy ctx->comp (ops, apertures, field tables) to the device and size the
+ * RF and wake buffers it needs */
+int upload_compiled(trk_context *ctx) {
+  int rc;
   CompiledLattice &c = ctx->comp;
   if ((rc = ensure(&ctx->d_ops, ctx->ops_cap, c.ops.size())))
     return rc;
@@ -351,7 +363,6 @@ int upload_lattice(trk_context *ctx, const trk_lattice *lat, double Po) {
     if (w.transverse)
       CUDA_TRY(cudaMemcpyAsync(wb->Wy, w.Wy, sizeof(double) * w.points, cudaMemcpyHostToDevice, ctx->stream));
   }
-  ctx->comp_src = lat;
   return TRK_OK;
 }
 
@@ -670,6 +681,7 @@ void trk_context_destroy(trk_context *ctx) {
   cudaFree(ctx->d_stats);
   cudaFree(ctx->d_gather);
   cudaFree(ctx->d_i64);
+  cudaFree(ctx->d_matrix);
   trk_comm_destroy(ctx->comm);
   cudaFree(ctx->d_effort);
   cudaFree(ctx->d_aos);
@@ -1029,14 +1041,202 @@ int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, 
   return TRK_OK;
 }
 
-int trk_track_element(trk_context *ctx, const trk_lattice *lattice, int element, long pass, double z_start,
-                      const trk_run *run, long *n_left) {
-  (void)z_start;
+static void default_elem(trk_elem &t, int type) {
+  std::memset(&t, 0, sizeof(t));
+  t.type = type;
+  for (int i = 0; i < trk_param_count(type); i++)
+    t.p[i] = trk_param_default(type, i);
+}
+
+int trk_track_element(trk_context *ctx, const trk_lattice *lattice, int element, long pass, int loss_element,
+                      double z_start, const trk_maxamp *maxamp, trk_element_state *state, const trk_run *run,
+                      long *n_left) {
   if (!ctx || !lattice || !run)
     return trk_set_error(TRK_ERR_ARG, "null argument");
   if (element < 0 || element >= lattice->n)
     return trk_set_error(TRK_ERR_ARG, "element index out of range");
-  return trk_set_error(TRK_ERR_UNSUPPORTED, "per-element tracking is provided by the elegant hook layer");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  const trk_elem *e = &lattice->e[element];
+  const bool wake = e->type == TRK_WAKE || e->type == TRK_TRWAKE;
+  const bool rf = e->type == TRK_RFCA;
+  if ((wake || rf) && !state)
+    return trk_set_error(TRK_ERR_ARG, "RFCA/WAKE/TRWAKE need an element state");
+  /* a private lattice: [MAXAMP of the caller's state] [CHARGE with the
+   * caller's macroparticle charge] element */
+  trk_elem tmp[3];
+  int n = 0;
+  if (maxamp) {
+    default_elem(tmp[n], TRK_MAXAMP);
+    TRK_P(&tmp[n], MAXAMP_X_MAX) = maxamp->x_max;
+    TRK_P(&tmp[n], MAXAMP_Y_MAX) = maxamp->y_max;
+    TRK_P(&tmp[n], MAXAMP_ELLIPTICAL) = maxamp->elliptical;
+    TRK_P(&tmp[n], MAXAMP_EXPONENT) = maxamp->exponent;
+    TRK_P(&tmp[n], MAXAMP_YEXPONENT) = maxamp->y_exponent;
+    n++;
+  }
+  if (wake) {
+    default_elem(tmp[n], TRK_CHARGE);
+    TRK_P(&tmp[n], CHARGE_PER_PARTICLE) = state->macro_charge;
+    n++;
+  }
+  tmp[n++] = *e;
+  trk_lattice L;
+  L.n = L.cap = n;
+  L.e = tmp;
+  const double Po = run->p_central;
+  if (!(Po > 0))
+    return trk_set_error(TRK_ERR_ARG, "p_central must be positive");
+  int rc = trk_compile(&L, Po, ctx->comp);
+  if (rc)
+    return rc;
+  CompiledLattice &c = ctx->comp;
+  int k = -1;
+  for (size_t i = 0; i < c.ops.size(); i++) {
+    trk_op &op = c.ops[i];
+    op.z_start += z_start;
+    op.z_end += z_start;
+    op.ap_post[0] = op.ap_post[1] = -1;
+    if (op.elem == n - 1) {
+      k = (int)i;
+      op.elem = loss_element;
+    }
+  }
+  ctx->comp_src = &L;
+  if ((rc = upload_compiled(ctx))) {
+    ctx->comp_src = nullptr;
+    return rc;
+  }
+  const bool fast = run->fast_math != 0;
+  int variant = run->variant;
+  if (variant < 0 || variant >= TRK_N_VARIANTS)
+    variant = (fast && c.lean) ? 7 : 1;
+  ctx->last_launches = 0;
+  if (k >= 0 && (ctx->np > 0 || ctx->comm)) {
+    const trk_op &op = c.ops[k];
+    if (wake) {
+      if ((rc = run_wake(ctx, fast, k, pass, -1, Po))) {
+        ctx->comp_src = nullptr;
+        return rc;
+      }
+    } else {
+      if (rf && op.kind == OPK_RF) {
+        const int slot = op.i[1];
+        if (state->rf_fiducial_seen) {
+          CUDA_TRY(cudaMemcpyAsync(ctx->d_rf_phase + slot, &state->rf_phase_fiducial, sizeof(double),
+                                   cudaMemcpyHostToDevice, ctx->stream));
+        } else {
+          /* findFiducialTime on the first call (src/simple_rfca.c:412-445) */
+          if ((rc = time_stats(ctx, fast, 1, op.d[RD_SOFF], Po))) {
+            ctx->comp_src = nullptr;
+            return rc;
+          }
+          if (fast)
+            trk_fast::launch_rf_fiducial(ctx->d_stats, op.d[RD_OMEGA], op.d[RD_TREF], ctx->d_rf_phase, slot,
+                                         ctx->d_status, ctx->stream);
+          else
+            trk_exact::launch_rf_fiducial(ctx->d_stats, op.d[RD_OMEGA], op.d[RD_TREF], ctx->d_rf_phase, slot,
+                                          ctx->d_status, ctx->stream);
+          CUDA_TRY(cudaMemcpyAsync(&state->rf_phase_fiducial, ctx->d_rf_phase + slot, sizeof(double),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+          CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+          state->rf_fiducial_seen = 1;
+        }
+      }
+      TrackArgs ta = track_args(ctx);
+      ta.fresh_pass = pass;
+      ta.Po = Po;
+      ta.element_only = 1;
+      ta.op_begin = k;
+      ta.op_end = k + 1;
+      ta.pass_begin = pass;
+      ta.pass_end = pass + 1;
+      if (fast)
+        trk_fast::launch_track(ta, variant, c.lean, ctx->np, ctx->sm_count * 256, ctx->stream);
+      else
+        trk_exact::launch_track(ta, variant, c.lean, ctx->np, ctx->sm_count * 256, ctx->stream);
+      ctx->last_launches++;
+    }
+    CUDA_TRY(cudaGetLastError());
+  }
+  ctx->comp_src = nullptr;
+  if ((rc = check_status(ctx)))
+    return rc;
+  return n_left ? trk_beam_count(ctx, n_left) : TRK_OK;
+}
+
+int trk_limit_amplitudes(trk_context *ctx, double x_max, double y_max, int elliptical, int exponent, int y_exponent,
+                         int extrapolate_z, double z, double p_central, long pass, int element, long *n_left) {
+  if (!ctx)
+    return trk_set_error(TRK_ERR_ARG, "null context");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  trk_aperture ap;
+  std::memset(&ap, 0, sizeof(ap));
+  ap.x_max = x_max;
+  ap.y_max = y_max;
+  ap.elliptical = elliptical;
+  ap.xexp = exponent;
+  ap.yexp = y_exponent ? y_exponent : exponent;
+  if (elliptical && (x_max || y_max)) {
+    /* elimit_amplitudes exits on a bad exponent (src/limit_amplitudes.c:523-538) */
+    if (exponent < 2 || exponent % 2 || (y_exponent && (y_exponent < 2 || y_exponent % 2)))
+      return trk_set_error(TRK_ERR_PHYSICS, "aperture exponent is not valid: give an even integer >= 2");
+  }
+  ap.valid = 1;
+  ap.a2 = ipow_h(x_max, ap.xexp);
+  ap.b2 = ipow_h(y_max, ap.yexp);
+  if (ctx->np > 0) {
+    TrackArgs ta = track_args(ctx);
+    ta.Po = p_central;
+    const int grid = grid_for(ctx, ctx->np, TRK_BLOCK);
+    trk_fast::launch_limit(ta, ap, 0, extrapolate_z, z, pass, element, grid, ctx->stream);
+    CUDA_TRY(cudaGetLastError());
+  }
+  return n_left ? trk_beam_count(ctx, n_left) : TRK_OK;
+}
+
+int trk_remove_invalid(trk_context *ctx, double z, double p_central, long pass, int element, long *n_left) {
+  if (!ctx)
+    return trk_set_error(TRK_ERR_ARG, "null context");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  if (ctx->np > 0) {
+    TrackArgs ta = track_args(ctx);
+    ta.Po = p_central;
+    trk_aperture ap;
+    std::memset(&ap, 0, sizeof(ap));
+    trk_fast::launch_limit(ta, ap, 1, 0, z, pass, element, grid_for(ctx, ctx->np, TRK_BLOCK), ctx->stream);
+    CUDA_TRY(cudaGetLastError());
+  }
+  return n_left ? trk_beam_count(ctx, n_left) : TRK_OK;
+}
+
+int trk_track_matrix(trk_context *ctx, int order, const double *C, const double *R, const double *T, int fast_math,
+                     long *n_left) {
+  if (!ctx || !C || !R || (order == 2 && !T))
+    return trk_set_error(TRK_ERR_ARG, "null argument");
+  if (order != 1 && order != 2)
+    return trk_set_error(TRK_ERR_UNSUPPORTED, "matrix order %d (1 or 2 supported)", order);
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  double h[6 + 36 + 126];
+  std::memcpy(h, C, sizeof(double) * 6);
+  std::memcpy(h + 6, R, sizeof(double) * 36);
+  if (order == 2)
+    std::memcpy(h + 42, T, sizeof(double) * 126);
+  else
+    std::memset(h + 42, 0, sizeof(double) * 126);
+  int rc;
+  if ((rc = ensure(&ctx->d_matrix, ctx->matrix_cap, 168)))
+    return rc;
+  CUDA_TRY(cudaMemcpyAsync(ctx->d_matrix, h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream));
+  if (ctx->np > 0) {
+    TrackArgs ta = track_args(ctx);
+    const int grid = grid_for(ctx, ctx->np, TRK_BLOCK);
+    if (fast_math)
+      trk_fast::launch_matrix(ta, ctx->d_matrix, order, grid, ctx->stream);
+    else
+      trk_exact::launch_matrix(ta, ctx->d_matrix, order, grid, ctx->stream);
+    CUDA_TRY(cudaGetLastError());
+  }
+  return n_left ? trk_beam_count(ctx, n_left) : TRK_OK;
 }
 
 int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int n_variants, const long *offsets,

@@ -69,23 +69,6 @@ bool rotation(double angle, double *c, double *s) {
   return true;
 }
 
-double ipow_h(double x, long p) {
-  if (p == 0)
-    return 1.0;
-  if (p == 1)
-    return x;
-  if (p == 2)
-    return x * x;
-  double h = 1.0, b = x;
-  long e = p < 0 ? -p : p;
-  while (e) {
-    if (e & 1)
-      h *= b;
-    b *= b;
-    e >>= 1;
-  }
-  return p < 0 ? 1.0 / h : h;
-}
 
 struct MaxampState {
   int idx = -1; /* aperture record, -1 none */
@@ -93,6 +76,21 @@ struct MaxampState {
 };
 
 } // namespace
+
+/* integer power by recursive squaring, the oracle's and the compiled SDDS
+ * shim's definition (src/multipole.c and src/limit_amplitudes.c call ipow) */
+double ipow_h(double x, long p) {
+  if (p == 0)
+    return 1.0;
+  if (p == 1)
+    return x;
+  if (p == 2)
+    return x * x;
+  if (p < 0)
+    return 1.0 / ipow_h(x, -p);
+  const double h = ipow_h(x, p / 2);
+  return (p & 1) ? h * h * x : h * h;
+}
 
 /* Field-expansion coefficients of a curved magnet from the recursion
  * Laplace's equation imposes in the curvilinear frame with curvature h

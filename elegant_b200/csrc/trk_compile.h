@@ -37,6 +37,7 @@ struct CompiledLattice {
 
 int trk_compile(const trk_lattice *l, double Po, CompiledLattice &out);
 void trk_expansion_coefficients(double *coef10);
+double ipow_h(double x, long p);
 extern "C" int trk_csbend_field_table(const double *b, const double *c, double h, int nonlinear, long expansionOrder,
                                       double *Fx, double *Fy, int *eo1, int *hasNormal, int *hasSkew);
 

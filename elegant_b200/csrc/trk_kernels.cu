@@ -1441,9 +1441,9 @@ __device__ __forceinline__ OpHead load_head(const trk_op *__restrict__ op, int v
  * aperture, :2675-2684 NaN/inf filter) and the loss record of one particle. */
 __device__ __forceinline__ bool after_element(const TrackArgs &a, const OpHead &h, Part &p, bool ok, long i,
                                               long pass) {
-  if (ok && !h.no_aperture && h.ap_post >= 0)
+  if (ok && !h.no_aperture && h.ap_post >= 0 && !a.element_only)
     ok = !post_aperture(p, a.aps + h.ap_post, h.extrapolate, h.z_end, a.Po);
-  if (ok && (isinf(p.x) || isinf(p.y) || isnan(p.x) || isnan(p.y))) {
+  if (ok && !a.element_only && (isinf(p.x) || isinf(p.y) || isnan(p.x) || isnan(p.y))) {
     p.s = h.z_end;
     p.dp = a.Po * (1 + p.dp);
     ok = false;
@@ -1960,7 +1960,7 @@ __global__ void __launch_bounds__(TRK_BLOCK) wake_kick_kernel(WakeArgs a) {
     bool lost = false;
     if (a.ap_post >= 0)
       lost = post_aperture(p, a.aps + a.ap_post, 0, a.z_end, a.Po);
-    if (!lost && (isinf(p.x) || isinf(p.y) || isnan(p.x) || isnan(p.y))) {
+    if (!lost && !a.element_only && (isinf(p.x) || isinf(p.y) || isnan(p.x) || isnan(p.y))) {
       p.s = a.z_end;
       p.dp = a.Po * (1 + p.dp);
       lost = true;
@@ -1987,6 +1987,71 @@ __global__ void rotate_kernel(TrackArgs a, double ca, double sa) {
     Part p;
     load_part(a, i, p);
     rotate(p, ca, sa);
+    store_part(a, i, p);
+  }
+}
+
+/* After-element filter on its own (limit_amplitudes / elimit_amplitudes,
+ * src/limit_amplitudes.c:197-288, 487-620): `ap` with x_max = y_max =
+ * DBL_MAX is the NaN filter.  mode 1: removeInvalidParticles
+ * (:289-331): a NaN coordinate or delta <= -1 loses the particle at z. */
+__global__ void limit_kernel(TrackArgs a, trk_aperture ap, int mode, int extrapolate, double z, long pass, int elem) {
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+    if (a.lost_pass[i] >= 0)
+      continue;
+    Part p;
+    load_part(a, i, p);
+    bool lost;
+    if (mode == 1) {
+      lost = isnan(p.x) || isnan(p.xp) || isnan(p.y) || isnan(p.yp) || isnan(p.s) || isnan(p.dp) || p.dp <= -1;
+      if (lost) {
+        p.s = z;
+        p.dp = a.Po * (1 + p.dp);
+      }
+    } else
+      lost = post_aperture_body(p, &ap, extrapolate, z, a.Po);
+    if (lost) {
+      store_part(a, i, p);
+      a.lost_pass[i] = (int32_t)pass;
+      a.lost_elem[i] = elem;
+    }
+  }
+}
+
+/* track_particles for a first- or second-order transport matrix
+ * (src/matrix.c:212-469 with TURBO_FASTMATTRACK=3): C[6], R[6][6] and the
+ * lower triangle T[i][j][k], k <= j, packed as 21 values per i, summed in the
+ * reference's order (i, j, k descending). */
+__global__ void matrix_kernel(TrackArgs a, const double *__restrict__ m, int order) {
+  const double *C = m, *R = m + 6, *T = m + 42;
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+    if (a.lost_pass[i] >= 0)
+      continue;
+    Part p;
+    load_part(a, i, p);
+    const double ini[6] = {p.x, p.xp, p.y, p.yp, p.s, p.dp};
+    double fin[6];
+    for (int r = 5; r >= 0; r--) {
+      double sum = __ldg(&C[r]);
+      for (int j = 5; j >= 0; j--) {
+        if (order >= 2) {
+          double sum1 = __ldg(&R[6 * r + j]);
+          for (int k = j; k >= 0; k--)
+            sum1 += __ldg(&T[21 * r + j * (j + 1) / 2 + k]) * ini[k];
+          sum += sum1 * ini[j];
+        } else
+          sum += __ldg(&R[6 * r + j]) * ini[j];
+      }
+      fin[r] = sum;
+    }
+    p.x = fin[0];
+    p.xp = fin[1];
+    p.y = fin[2];
+    p.yp = fin[3];
+    p.s = fin[4];
+    p.dp = fin[5];
     store_part(a, i, p);
   }
 }
@@ -2097,6 +2162,15 @@ void launch_stats_combine(const double *gathered, int ranks, double *out, cudaSt
 
 void launch_rotate(const TrackArgs &a, double ca, double sa, int grid, cudaStream_t st) {
   rotate_kernel<<<grid, TRK_BLOCK, 0, st>>>(a, ca, sa);
+}
+
+void launch_limit(const TrackArgs &a, const trk_aperture &ap, int mode, int extrapolate, double z, long pass, int elem,
+                  int grid, cudaStream_t st) {
+  limit_kernel<<<grid, TRK_BLOCK, 0, st>>>(a, ap, mode, extrapolate, z, pass, elem);
+}
+
+void launch_matrix(const TrackArgs &a, const double *m, int order, int grid, cudaStream_t st) {
+  matrix_kernel<<<grid, TRK_BLOCK, 0, st>>>(a, m, order);
 }
 
 cudaError_t set_coefficients(const double *coef10) {

@@ -37,6 +37,7 @@ struct TrackArgs {
   long pass_begin, pass_end;
   long fresh_pass; /* pass that sees the MAXAMP state of a fresh do_tracking call */
   double Po;
+  int element_only; /* 1: the element body only, no after-element aperture or NaN filter */
 };
 
 struct TimeStatsArgs {
@@ -94,6 +95,7 @@ struct WakeArgs {
   int ap_post;
   double z_end;
   int elem;
+  int element_only; /* 1: no NaN filter after the kick (per-element entry points) */
 };
 
 #define TRK_DECLARE_LAUNCHERS(NS)                                                                            \
@@ -108,6 +110,9 @@ struct WakeArgs {
   void launch_wake_apply(const WakeArgs &a, int grid, cudaStream_t st);                                      \
   void launch_stats_combine(const double *gathered, int ranks, double *out, cudaStream_t st);                \
   void launch_rotate(const TrackArgs &a, double ca, double sa, int grid, cudaStream_t st);                   \
+  void launch_limit(const TrackArgs &a, const trk_aperture &ap, int mode, int extrapolate, double z, long pass,  \
+                    int elem, int grid, cudaStream_t st);                                                    \
+  void launch_matrix(const TrackArgs &a, const double *m, int order, int grid, cudaStream_t st);             \
   cudaError_t set_coefficients(const double *coef10);                                                        \
   }
 

@@ -191,12 +191,58 @@ int trk_beam_count(trk_context *ctx, long *n_left);
  * *p_central is read and updated (RFCA CHANGE_P0, WAKE CHANGE_P0). */
 int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, trk_stats *stats);
 
-/* Same, through one element only (index `element` of the lattice), as the
- * reference's per-element hooks do; `pass` is the pass index and z_start the
- * arc length at the element entrance.  Survivors are compacted to the front
- * and *n_left updated, as the hooks' `long` return (src/multipole.c:701). */
-int trk_track_element(trk_context *ctx, const trk_lattice *lattice, int element, long pass,
-                      double z_start, const trk_run *run, long *n_left);
+/* ------------------------------------------------ per-element entry points
+ * What the reference's HAVE_GPU hooks call (src/multipole.c:698-709,
+ * src/csbend.c:689-701, src/csbend.c:3796-3800, src/simple_rfca.c:267-290,
+ * src/wake.c:47-56, src/trwake.c:43-50, src/limit_amplitudes.c:204-214,
+ * :296-300, :508-516, src/matrix.c:227-240): one element's body at a time,
+ * the after-element filters as separate calls, losses recorded with the
+ * given pass and element index.  *n_left receives the survivor count (the
+ * hooks' `long` return); the device beam keeps lost particles in place
+ * (trk_beam_store returns survivors first). */
+
+/* The sticky MAXAMP state that in-element aperture checks use (the `maxamp`
+ * argument of multipole_tracking2 / track_through_csbend). */
+typedef struct {
+  double x_max, y_max;
+  int32_t elliptical, exponent, y_exponent, reserved;
+} trk_maxamp;
+
+/* State of one element kept by the caller between calls: the RFCA fiducial
+ * phase (set on the first call, src/simple_rfca.c:412-471) and the
+ * macroparticle charge a WAKE/TRWAKE uses (CHARGE element, or the element's
+ * CHARGE / particles on pass 0: src/wake.c:346-372). */
+typedef struct {
+  double rf_phase_fiducial;
+  int32_t rf_fiducial_seen, reserved;
+  double macro_charge;
+} trk_element_state;
+
+/* Element `element` of `lattice` (any path type but MAXAMP/CHARGE/MARK, which
+ * do nothing here) on the surviving particles; z_start is the arc length at
+ * the element entrance; losses are recorded with `pass` and `loss_element`;
+ * maxamp may be NULL; state may be NULL for elements other than
+ * RFCA/WAKE/TRWAKE.  run supplies p_central, fast_math, variant. */
+int trk_track_element(trk_context *ctx, const trk_lattice *lattice, int element, long pass, int loss_element,
+                      double z_start, const trk_maxamp *maxamp, trk_element_state *state, const trk_run *run,
+                      long *n_left);
+
+/* limit_amplitudes / elimit_amplitudes (src/limit_amplitudes.c:197-288,
+ * 487-620) on the surviving particles; x_max = y_max = DBL_MAX is
+ * removeInvalidParticles' NaN/inf filter (:289-317).  Open sides (openCode)
+ * are not supported. */
+int trk_limit_amplitudes(trk_context *ctx, double x_max, double y_max, int elliptical, int exponent, int y_exponent,
+                         int extrapolate_z, double z, double p_central, long pass, int element, long *n_left);
+
+/* removeInvalidParticles (src/limit_amplitudes.c:289-331): particles with a
+ * NaN coordinate or delta <= -1 are lost at z. */
+int trk_remove_invalid(trk_context *ctx, double z, double p_central, long pass, int element, long *n_left);
+
+/* track_particles (src/matrix.c:212-469) for a first- or second-order matrix:
+ * C[6], R[36] row-major, T[6*21] with T[i][j][k] (k <= j) at i*21 + j(j+1)/2 + k
+ * (ignored for order 1). */
+int trk_track_matrix(trk_context *ctx, int order, const double *C, const double *R, const double *T, int fast_math,
+                     long *n_left);
 
 /* ------------------------------------------------------ batched ensembles */
 /* Track `n_variants` lattices that differ only in element parameter values

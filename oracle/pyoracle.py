@@ -228,3 +228,45 @@ def ref_param_defaults(type_code):
     if n < 0:
         raise RuntimeError("bad type")
     return out[:n]
+
+
+# oracle/_ref/libref_gpu.so: the same reference sources compiled with elegant's
+# HAVE_GPU hooks on, the hooks implemented over libtrkgpu.so
+# (elegant_b200/hooks/trk_elegant_hooks.c); needs a GPU to run.
+REF_GPU_LIB = os.path.join(HERE, "_ref", "libref_gpu.so")
+_refgpu = None
+
+
+def refgpu_available():
+    return os.path.exists(REF_GPU_LIB)
+
+
+def track_refgpu(lattice, beam, n_passes, p_central, pass_offset=0):
+    """As track_ref(), with every element going through elegant's GPU hooks
+    into the CUDA library (parity build).  Rows come back survivors first."""
+    global _refgpu
+    if _refgpu is None:
+        lib = ctypes.CDLL(REF_GPU_LIB)
+        P = ctypes.c_void_p
+        DP = ctypes.POINTER(ctypes.c_double)
+        L, I, D = ctypes.c_long, ctypes.c_int, ctypes.c_double
+        lib.trk_last_error.restype = ctypes.c_char_p
+        lib.trk_lattice_create.argtypes = [ctypes.POINTER(P)]
+        lib.trk_lattice_destroy.argtypes = [P]
+        lib.trk_lattice_add.argtypes = [P, I, ctypes.c_char_p, ctypes.POINTER(I)]
+        lib.trk_lattice_set.argtypes = [P, I, ctypes.c_char_p, D]
+        lib.trk_lattice_set_wake.argtypes = [P, I, DP, DP, DP, L]
+        lib.refgpu_track.argtypes = [P, DP, L, L, L, DP, ctypes.POINTER(_Result)]
+        _refgpu = lib
+    lib = _refgpu
+    nat = lattice.native(lib)
+    rows = np.zeros((beam.shape[0], STRIDE), dtype=np.float64)
+    rows[:, :7] = beam[:, :7]
+    pc = ctypes.c_double(p_central)
+    res = _Result()
+    try:
+        _check(lib, lib.refgpu_track(nat.ptr, rows.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), rows.shape[0],
+                                     n_passes, pass_offset, ctypes.byref(pc), ctypes.byref(res)))
+    finally:
+        nat.close()
+    return rows, res.n_left, res.particle_passes

@@ -25,6 +25,16 @@
 
 #include "trk_lattice.h"
 #include "trk_oracle.h"
+#ifdef REF_GPU_HOOKS
+/* built a second time with elegant's HAVE_GPU hooks on (oracle/_ref/libref_gpu.so):
+ * the same loop, with the beam on the device through the hooks of
+ * elegant_b200/hooks/trk_elegant_hooks.c, as do_tracking drives them
+ * (src/do_tracking.c:413, :925-931, :3177-3178) */
+#include "gpu_base.h"
+#define REF_ENTRY refgpu_track
+#else
+#define REF_ENTRY ref_track
+#endif
 
 VMATRIX *drift_matrix(double length, long order);
 void track_particles(double **final, VMATRIX *M, double **initial, long n_part);
@@ -223,6 +233,10 @@ static int build_beamline(const trk_lattice *l, ref_beamline *b) {
 }
 
 static void record_losses(double **coord, long nLeft, long nToTrack, long pass, long element, long *lp, long *le) {
+#ifdef REF_GPU_HOOKS
+  /* the device keeps the loss record; rows are not on the host here */
+  return;
+#endif
   for (long k = nLeft; k < nToTrack; k++) {
     long o = (long)coord[k][REF_ORIG];
     lp[o] = pass;
@@ -230,7 +244,7 @@ static void record_losses(double **coord, long nLeft, long nToTrack, long pass, 
   }
 }
 
-int ref_track(const trk_lattice *l, double *rows, long np, long n_passes, long pass_offset, double *P_central,
+int REF_ENTRY(const trk_lattice *l, double *rows, long np, long n_passes, long pass_offset, double *P_central,
               orc_result *result) {
   if (!l || (!rows && np) || !P_central)
     return TRK_ERR_ARG;
@@ -268,14 +282,25 @@ int ref_track(const trk_lattice *l, double *rows, long np, long n_passes, long p
   long elliptical = 0, maxampOpenCode = 0, maxampExponent = 2, maxampYExponent = 2;
   CHARGE *charge = NULL;
 
+#ifdef REF_GPU_HOOKS
+  gpuBaseInit(coord, np, NULL, NULL, 1);
+  trk_hooks_begin_pass(pass_offset);
+  getGpuBase()->elementOnGpu = 1;
+#endif
   nLeft = limit_amplitudes(coord, DBL_MAX, DBL_MAX, nToTrack, NULL, 0.0, *P_central, 0, 0, bl.n ? bl.el : NULL);
   record_losses(coord, nLeft, nToTrack, pass_offset, -1, lp, le);
   nToTrack = nLeft;
 
   for (long i_pass = pass_offset; i_pass < pass_offset + n_passes; i_pass++) {
     double z = 0, last_z = 0;
+#ifdef REF_GPU_HOOKS
+    trk_hooks_begin_pass(i_pass);
+#endif
     for (long ie = 0; ie < bl.n; ie++) {
       ELEMENT_LIST *eptr = &bl.el[ie];
+#ifdef REF_GPU_HOOKS
+      setElementGpuData(eptr);
+#endif
       last_z = z;
       if (entity_description[eptr->type].flags & HAS_LENGTH)
         z += ((DRIFT *)eptr->p_elem)->length;
@@ -350,6 +375,17 @@ int ref_track(const trk_lattice *l, double *rows, long np, long n_passes, long p
     }
     effort += nToTrack;
   }
+#ifdef REF_GPU_HOOKS
+  coord = forceParticlesToCpu("end of tracking");
+  const long *hook_le = trk_hooks_loss_elements();
+  for (long i = 0; i < np; i++) {
+    double *r = rows + (size_t)i * ORC_STRIDE;
+    memcpy(r, coord[i], 7 * sizeof(double));
+    r[7] = coord[i][lossPassIndex];
+    r[8] = hook_le[i];
+  }
+  gpuBaseDealloc();
+#else
   for (long i = 0; i < np; i++) {
     double *r = rows + (size_t)i * ORC_STRIDE;
     long o = (long)coord[i][REF_ORIG];
@@ -357,6 +393,7 @@ int ref_track(const trk_lattice *l, double *rows, long np, long n_passes, long p
     r[7] = lp[o];
     r[8] = le[o];
   }
+#endif
   if (result) {
     result->n_left = nToTrack;
     result->particle_passes = effort;
@@ -370,6 +407,7 @@ int ref_track(const trk_lattice *l, double *rows, long np, long n_passes, long p
   return TRK_OK;
 }
 
+#ifndef REF_GPU_HOOKS
 /* The reference's default of every parameter the lattice tables know, for
  * a test that the two tables agree: defaults[i] for parameter i of `type`
  * (trk_param_name order); returns the count or a negative error. */
@@ -394,3 +432,4 @@ int ref_param_defaults(int type, double *defaults, int max) {
   }
   return n;
 }
+#endif
