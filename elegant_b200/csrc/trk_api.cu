@@ -75,6 +75,7 @@ struct trk_context {
   trk_comm *comm = nullptr;  /* set for sharded runs (trk_context_set_comm) */
   long long *d_i64 = nullptr; /* one int64 for count exchanges */
   double *d_matrix = nullptr; /* trk_track_matrix: C, R, T (168 doubles) */
+  bool element_mode = false;  /* inside trk_track_element: element bodies only, no after-element filters */
   size_t matrix_cap = 0;
   double *d_gather = nullptr; /* 6 doubles per rank */
   long long *d_effort = nullptr;
@@ -540,6 +541,7 @@ int run_wake(trk_context *ctx, bool fast, int opi, long pass, long fresh_pass, d
   a.ap_post = op.ap_post[var];
   a.z_end = op.z_end;
   a.elem = op.elem;
+  a.element_only = ctx->element_mode ? 1 : 0;
   long nb = w.max_bins + 2;
   if (w.transverse) {
     CUDA_TRY(cudaMemsetAsync(wb->hist_x, 0, sizeof(double) * nb, ctx->stream));
@@ -1114,7 +1116,10 @@ int trk_track_element(trk_context *ctx, const trk_lattice *lattice, int element,
   if (k >= 0 && (ctx->np > 0 || ctx->comm)) {
     const trk_op &op = c.ops[k];
     if (wake) {
-      if ((rc = run_wake(ctx, fast, k, pass, -1, Po))) {
+      ctx->element_mode = true;
+      rc = run_wake(ctx, fast, k, pass, -1, Po);
+      ctx->element_mode = false;
+      if (rc) {
         ctx->comp_src = nullptr;
         return rc;
       }
@@ -1188,7 +1193,8 @@ int trk_limit_amplitudes(trk_context *ctx, double x_max, double y_max, int ellip
     TrackArgs ta = track_args(ctx);
     ta.Po = p_central;
     const int grid = grid_for(ctx, ctx->np, TRK_BLOCK);
-    trk_fast::launch_limit(ta, ap, 0, extrapolate_z, z, pass, element, grid, ctx->stream);
+    /* the reference's arithmetic (no FMA contraction in the extrapolation) */
+    trk_exact::launch_limit(ta, ap, 0, extrapolate_z, z, pass, element, grid, ctx->stream);
     CUDA_TRY(cudaGetLastError());
   }
   return n_left ? trk_beam_count(ctx, n_left) : TRK_OK;
@@ -1203,7 +1209,7 @@ int trk_remove_invalid(trk_context *ctx, double z, double p_central, long pass, 
     ta.Po = p_central;
     trk_aperture ap;
     std::memset(&ap, 0, sizeof(ap));
-    trk_fast::launch_limit(ta, ap, 1, 0, z, pass, element, grid_for(ctx, ctx->np, TRK_BLOCK), ctx->stream);
+    trk_exact::launch_limit(ta, ap, 1, 0, z, pass, element, grid_for(ctx, ctx->np, TRK_BLOCK), ctx->stream);
     CUDA_TRY(cudaGetLastError());
   }
   return n_left ? trk_beam_count(ctx, n_left) : TRK_OK;
