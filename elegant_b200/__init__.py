@@ -62,6 +62,7 @@ def _declare(lib):
     sig = {
         "trk_last_error": (ctypes.c_char_p, []),
         "trk_comm_get_unique_id": (I, [P]),
+        "trk_ensemble_variant": (I, [P]),
         "trk_context_set_comm": (I, [P, P, I, I]),
         "trk_context_comm": (I, [P, ctypes.POINTER(I), ctypes.POINTER(I)]),
         "trk_abi_version": (I, []),
@@ -266,6 +267,29 @@ class Tracker:
         _check(self.lib, self.lib.trk_beam_store(self.ctx, _dptr(out), stride, ctypes.byref(n_left), None, None))
         return n_left.value, out
 
+    def track_ensemble(self, lattices, counts, n_passes, p_central, pass_offset=0, fast=True, variant=-1):
+        """Track the loaded beam as len(lattices) variants: variant v owns the
+        next counts[v] particles (in load order).  The lattices must share
+        one element structure.  Returns the run statistics plus the launch
+        shape used ("variant")."""
+        nats = [self.native(lat) for lat in lattices]
+        arr = (ctypes.c_void_p * len(nats))(*[n.ptr.value for n in nats])
+        offs = np.concatenate([[0], np.cumsum(np.asarray(counts, dtype=np.int64))]).astype(np.int64)
+        run = _Run()
+        self.lib.trk_run_defaults(ctypes.byref(run))
+        run.p_central = p_central
+        run.n_passes = n_passes
+        run.pass_offset = pass_offset
+        run.fast_math = 1 if fast else 0
+        run.variant = variant
+        st = _Stats()
+        _check(self.lib, self.lib.trk_track_ensemble(
+            self.ctx, arr, len(nats),
+            offs.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), ctypes.byref(run), ctypes.byref(st)))
+        out = _stats_dict(st)
+        out["variant"] = self.lib.trk_ensemble_variant(self.ctx)
+        return out
+
     def set_comm(self, unique_id, nranks, rank):
         """Join a sharded run: `unique_id` (128 bytes from nccl_unique_id() on
         one rank) shared by all ranks; nranks <= 0 leaves it."""
@@ -310,6 +334,12 @@ class Tracker:
         return Stats(n_total=st.n_total, n_left=st.n_left, particle_passes=st.particle_passes,
                      device_ms=st.device_ms, kernel_launches=st.kernel_launches, p_central=st.p_central,
                      track_ms=st.track_ms, track_launches=st.track_launches)
+
+
+def _stats_dict(st):
+    return Stats(n_total=st.n_total, n_left=st.n_left, particle_passes=st.particle_passes,
+                 device_ms=st.device_ms, kernel_launches=st.kernel_launches, p_central=st.p_central,
+                 track_ms=st.track_ms, track_launches=st.track_launches)
 
 
 def nccl_unique_id():

@@ -73,11 +73,16 @@ def objects():
 
 def build(verbose=False):
     os.makedirs(BUILD, exist_ok=True)
-    objs = []
+    objs, todo = [], []
     for src, o, cmd in objects():
         if _newer(o, [src] + HEADERS):
-            _run(cmd, verbose)
+            todo.append(cmd)
         objs.append(o)
+    # the translation units are independent: compile them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(todo), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(_run, cmd, verbose) for cmd in todo]:
+            f.result()
     if _newer(LIB, objs):
         _run([NVCC, "-shared", "-cudart", "static"] + ARCH + ["-o", LIB] + objs + ["-ldl"], verbose)
     return LIB

@@ -76,6 +76,18 @@ struct trk_context {
   long long *d_i64 = nullptr; /* one int64 for count exchanges */
   double *d_matrix = nullptr; /* trk_track_matrix: C, R, T (168 doubles) */
   bool element_mode = false;  /* inside trk_track_element: element bodies only, no after-element filters */
+  long *d_ens_offsets = nullptr; /* ensemble variant offsets (n_variants + 1) */
+  size_t ens_offsets_cap = 0;
+  char *d_tune = nullptr;        /* autotuner's scratch copy of the beam */
+  size_t tune_cap = 0;
+  struct Tuned {
+    int nops;
+    long np;
+    bool lean, fast;
+    int variant;
+  };
+  std::vector<Tuned> ens_tuned;  /* autotuner choices */
+  int ens_last_variant = -1;
   size_t matrix_cap = 0;
   double *d_gather = nullptr; /* 6 doubles per rank */
   long long *d_effort = nullptr;
@@ -684,6 +696,8 @@ void trk_context_destroy(trk_context *ctx) {
   cudaFree(ctx->d_gather);
   cudaFree(ctx->d_i64);
   cudaFree(ctx->d_matrix);
+  cudaFree(ctx->d_ens_offsets);
+  cudaFree(ctx->d_tune);
   trk_comm_destroy(ctx->comm);
   cudaFree(ctx->d_effort);
   cudaFree(ctx->d_aos);
@@ -1245,16 +1259,221 @@ int trk_track_matrix(trk_context *ctx, int order, const double *C, const double 
   return n_left ? trk_beam_count(ctx, n_left) : TRK_OK;
 }
 
+/* ------------------------------------------------------------ ensembles */
+/* Launch shapes the autotuner tries (block size x resident blocks, see
+ * TRK_N_VARIANTS), timed on a scratch copy of the beam. */
+static const int k_tune_candidates[] = {1, 4, 7, 8};
+
+static int ensemble_launches(trk_context *ctx, const TrackArgs &base, int nv, int nops, int variant, bool lean,
+                             bool fast, long p0, long n_passes, long chunk) {
+  for (long pass = p0; pass < p0 + n_passes; pass += chunk) {
+    TrackArgs ta = base;
+    ta.op_begin = 0;
+    ta.op_end = nops;
+    ta.pass_begin = pass;
+    ta.pass_end = std::min(pass + chunk, p0 + n_passes);
+    if (fast)
+      trk_fast::launch_track_ensemble(ta, ctx->d_ens_offsets, nv, nops, variant, lean, ctx->np, ctx->sm_count * 256,
+                                      ctx->stream);
+    else
+      trk_exact::launch_track_ensemble(ta, ctx->d_ens_offsets, nv, nops, variant, lean, ctx->np,
+                                       ctx->sm_count * 256, ctx->stream);
+    ctx->last_launches++;
+  }
+  CUDA_TRY(cudaGetLastError());
+  return TRK_OK;
+}
+
+/* beam columns and loss arrays to / from the tuning scratch copy */
+static int beam_snapshot(trk_context *ctx, bool save) {
+  const size_t cols = sizeof(double) * 7 * ctx->cap, loss = sizeof(int32_t) * ctx->cap;
+  if (save) {
+    int rc;
+    if ((rc = ensure(&ctx->d_tune, ctx->tune_cap, cols + 2 * loss)))
+      return rc;
+  }
+  char *t = ctx->d_tune;
+  if (save) {
+    CUDA_TRY(cudaMemcpyAsync(t, ctx->d_cols, cols, cudaMemcpyDeviceToDevice, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(t + cols, ctx->d_lost_pass, loss, cudaMemcpyDeviceToDevice, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(t + cols + loss, ctx->d_lost_elem, loss, cudaMemcpyDeviceToDevice, ctx->stream));
+  } else {
+    CUDA_TRY(cudaMemcpyAsync(ctx->d_cols, t, cols, cudaMemcpyDeviceToDevice, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(ctx->d_lost_pass, t + cols, loss, cudaMemcpyDeviceToDevice, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(ctx->d_lost_elem, t + cols + loss, loss, cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  return TRK_OK;
+}
+
 int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int n_variants, const long *offsets,
                        const trk_run *run, trk_stats *stats) {
-  (void)ctx;
-  (void)lattices;
-  (void)n_variants;
-  (void)offsets;
-  (void)run;
-  (void)stats;
-  return trk_set_error(TRK_ERR_UNSUPPORTED, "ensembles not built yet");
+  if (!ctx || !lattices || !offsets || !run || n_variants < 1)
+    return trk_set_error(TRK_ERR_ARG, "bad ensemble arguments");
+  if (run->n_passes < 0)
+    return trk_set_error(TRK_ERR_ARG, "negative pass count");
+  if (offsets[0] != 0 || offsets[n_variants] != ctx->np)
+    return trk_set_error(TRK_ERR_ARG, "offsets must run from 0 to the loaded particle count (%ld)", ctx->np);
+  for (int v = 0; v < n_variants; v++)
+    if (!lattices[v] || offsets[v + 1] < offsets[v])
+      return trk_set_error(TRK_ERR_ARG, "variant %d: null lattice or decreasing offsets", v);
+  const trk_lattice *L0 = lattices[0];
+  for (int v = 0; v < n_variants; v++) {
+    if (lattices[v]->n != L0->n)
+      return trk_set_error(TRK_ERR_ARG, "variant %d has %d elements, variant 0 has %d", v, lattices[v]->n, L0->n);
+    for (int i = 0; i < L0->n; i++) {
+      const int t = lattices[v]->e[i].type;
+      if (t != L0->e[i].type)
+        return trk_set_error(TRK_ERR_ARG, "variant %d differs in the type of element %d", v, i);
+      if (t == TRK_WAKE || t == TRK_TRWAKE || t == TRK_RFCA)
+        return trk_set_error(TRK_ERR_UNSUPPORTED, "collective elements (RFCA, WAKE, TRWAKE) in an ensemble");
+    }
+  }
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  const double Po = run->p_central;
+  if (!(Po > 0))
+    return trk_set_error(TRK_ERR_ARG, "p_central must be positive");
+  /* one compiled record set per variant, concatenated; aperture and field
+   * indices shifted to the concatenated pools */
+  CompiledLattice all, c;
+  int rc = 0, nops = -1;
+  bool lean = true;
+  for (int v = 0; v < n_variants; v++) {
+    if ((rc = trk_compile(lattices[v], Po, c)))
+      return rc;
+    if (nops < 0)
+      nops = (int)c.ops.size();
+    else if ((int)c.ops.size() != nops)
+      return trk_set_error(TRK_ERR_ARG, "variant %d compiles to a different element sequence", v);
+    lean = lean && c.lean;
+    const int apo = (int)all.aps.size(), fo = (int)all.field.size();
+    for (trk_op op : c.ops) {
+      for (int k = 0; k < 2; k++) {
+        if (op.ap_post[k] >= 0)
+          op.ap_post[k] += apo;
+        if (op.ap_in[k] >= 0)
+          op.ap_in[k] += apo;
+      }
+      if (op.kind == OPK_BEND || op.kind == OPK_DIPOLE)
+        op.i[4] += fo;
+      all.ops.push_back(op);
+    }
+    all.aps.insert(all.aps.end(), c.aps.begin(), c.aps.end());
+    all.field.insert(all.field.end(), c.field.begin(), c.field.end());
+  }
+  all.lean = lean;
+  ctx->comp = all;
+  ctx->comp_src = nullptr;
+  if ((rc = upload_compiled(ctx)))
+    return rc;
+  if ((rc = ensure(&ctx->d_ens_offsets, ctx->ens_offsets_cap, (size_t)n_variants + 1)))
+    return rc;
+  CUDA_TRY(cudaMemcpyAsync(ctx->d_ens_offsets, offsets, sizeof(long) * (n_variants + 1), cudaMemcpyHostToDevice,
+                           ctx->stream));
+  const bool fast = run->fast_math != 0;
+  const long p0 = run->pass_offset;
+  const long fresh = ctx->passes_done == 0 ? p0 : -1;
+  const long chunk = 64;
+  ctx->last_launches = 0;
+  TrackArgs base = track_args(ctx);
+  base.fresh_pass = fresh;
+  base.Po = Po;
+
+  /* launch shape: the caller's, else the autotuner's choice for this
+   * (element count, particle count, build) */
+  int variant = run->variant;
+  if (!trk_fast::ensemble_variant_ok(variant)) {
+    variant = -1;
+    for (const auto &t : ctx->ens_tuned)
+      if (t.nops == nops && t.np == ctx->np && t.lean == lean && t.fast == fast)
+        variant = t.variant;
+  }
+  if (variant < 0 && ctx->np > 0 && nops > 0 && run->n_passes > 0) {
+    const long tune_passes = std::min<long>(run->n_passes, 2);
+    if ((rc = beam_snapshot(ctx, true)))
+      return rc;
+    float best = 0;
+    for (int cand : k_tune_candidates) {
+      if ((rc = beam_snapshot(ctx, false)))
+        return rc;
+      CUDA_TRY(cudaEventRecord(ctx->ev0, ctx->stream));
+      if ((rc = ensemble_launches(ctx, base, n_variants, nops, cand, lean, fast, p0, tune_passes, chunk)))
+        return rc;
+      CUDA_TRY(cudaEventRecord(ctx->ev1, ctx->stream));
+      CUDA_TRY(cudaEventSynchronize(ctx->ev1));
+      float ms = 0;
+      CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+      if (variant < 0 || ms < best) {
+        best = ms;
+        variant = cand;
+      }
+    }
+    if ((rc = beam_snapshot(ctx, false)))
+      return rc;
+    ctx->ens_tuned.push_back({nops, ctx->np, lean, fast, variant});
+    ctx->last_launches = 0;
+  }
+  if (variant < 0)
+    variant = 1;
+  ctx->ens_last_variant = variant;
+
+  CUDA_TRY(cudaEventRecord(ctx->ev0, ctx->stream));
+  if (ctx->np > 0 && run->n_passes > 0 && fresh >= 0) {
+    screen_kernel<<<(int)((ctx->np + 255) / 256), 256, 0, ctx->stream>>>(
+      ctx->d_cols, ctx->cap, ctx->d_lost_pass, ctx->d_lost_elem, ctx->np, p0, Po);
+    ctx->last_launches++;
+  }
+  if (ctx->np > 0 && run->n_passes > 0 && nops > 0) {
+    /* the chunked pass loop is captured once into a CUDA graph and replayed */
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    rc = ensemble_launches(ctx, base, n_variants, nops, variant, lean, fast, p0, run->n_passes, chunk);
+    cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+    if (rc)
+      return rc;
+    if (ce != cudaSuccess)
+      return trk_set_error(TRK_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    if (ce == cudaSuccess)
+      ce = cudaGraphLaunch(exec, ctx->stream);
+    if (exec)
+      cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess)
+      return trk_set_error(TRK_ERR_CUDA, "graph launch: %s", cudaGetErrorString(ce));
+  }
+  CUDA_TRY(cudaEventRecord(ctx->ev1, ctx->stream));
+  if ((rc = check_status(ctx)))
+    return rc;
+  ctx->passes_done += run->n_passes;
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    float ms = 0;
+    CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    stats->device_ms = ms;
+    stats->track_ms = ms;
+    stats->track_launches = ctx->last_launches;
+    stats->n_total = ctx->np;
+    stats->kernel_launches = ctx->last_launches;
+    stats->p_central = Po;
+    if (ctx->np > 0) {
+      CUDA_TRY(cudaMemsetAsync(ctx->d_effort, 0, sizeof(long long), ctx->stream));
+      effort_kernel<<<std::min(grid_for(ctx, ctx->np, 256), 1024), 256, 0, ctx->stream>>>(
+        ctx->d_lost_pass, ctx->np, p0, p0 + run->n_passes, (unsigned long long *)ctx->d_effort);
+      long long eff = 0;
+      CUDA_TRY(cudaMemcpyAsync(&eff, ctx->d_effort, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+      CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+      stats->particle_passes = eff;
+      long nl = 0;
+      if ((rc = trk_beam_count(ctx, &nl)))
+        return rc;
+      stats->n_left = nl;
+    }
+  }
+  return TRK_OK;
 }
+
+int trk_ensemble_variant(const trk_context *ctx) { return ctx ? ctx->ens_last_variant : -1; }
 
 int trk_adjoint(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, double centroid_weight,
                 double *loss, double *grad, int n_grad) {

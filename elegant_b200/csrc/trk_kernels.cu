@@ -1456,11 +1456,11 @@ __device__ __forceinline__ bool after_element(const TrackArgs &a, const OpHead &
 }
 
 template <bool LEAN>
-__device__ __forceinline__ bool track_particle(const TrackArgs &a, Part &p, long i) {
+__device__ __forceinline__ bool track_particle(const TrackArgs &a, const trk_op *__restrict__ ops, Part &p, long i) {
   for (long pass = a.pass_begin; pass < a.pass_end; pass++) {
     const int var = (pass == a.fresh_pass) ? 0 : 1;
     for (int k = a.op_begin; k < a.op_end; k++) {
-      const trk_op *op = a.ops + k;
+      const trk_op *op = ops + k;
       const OpHead h = load_head(op, var);
       const trk_aperture *ap_in = h.ap_in >= 0 ? a.aps + h.ap_in : nullptr;
       bool ok = true;
@@ -1515,9 +1515,23 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(TrackArgs a) {
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
     if (a.lost_pass[i] >= 0)
       continue;
+    const trk_op *ops = a.ops;
+    if (a.ens_offsets) {
+      /* ensemble: particle i runs the records of the variant v with
+       * offsets[v] <= i < offsets[v+1] (same structure, other values) */
+      int lo = 0, hi = a.ens_variants;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(&a.ens_offsets[mid]) <= i)
+          lo = mid;
+        else
+          hi = mid;
+      }
+      ops += (long)lo * a.ens_ops;
+    }
     Part p;
     load_part(a, i, p);
-    track_particle<LEAN>(a, p, i);
+    track_particle<LEAN>(a, ops, p, i);
     store_part(a, i, p);
   }
 }
@@ -2162,6 +2176,18 @@ void launch_stats_combine(const double *gathered, int ranks, double *out, cudaSt
 
 void launch_rotate(const TrackArgs &a, double ca, double sa, int grid, cudaStream_t st) {
   rotate_kernel<<<grid, TRK_BLOCK, 0, st>>>(a, ca, sa);
+}
+
+/* launch shapes an ensemble can use (the one-particle-per-thread kernels) */
+int ensemble_variant_ok(int variant) { return variant >= 0 && variant < TRK_N_VARIANTS && variant != 5 && variant != 6; }
+
+void launch_track_ensemble(const TrackArgs &a, const long *offsets, int n_variants, int ops_per_variant, int variant,
+                           bool lean, long n, int max_blocks, cudaStream_t st) {
+  TrackArgs e = a;
+  e.ens_offsets = offsets;
+  e.ens_variants = n_variants;
+  e.ens_ops = ops_per_variant;
+  launch_track(e, ensemble_variant_ok(variant) ? variant : 1, lean, n, max_blocks, st);
 }
 
 void launch_limit(const TrackArgs &a, const trk_aperture &ap, int mode, int extrapolate, double z, long pass, int elem,

@@ -38,6 +38,9 @@ struct TrackArgs {
   long fresh_pass; /* pass that sees the MAXAMP state of a fresh do_tracking call */
   double Po;
   int element_only; /* 1: the element body only, no after-element aperture or NaN filter */
+  /* ensembles: variant offsets (n_variants + 1), records per variant; null for one lattice */
+  const long *ens_offsets;
+  int ens_variants, ens_ops;
 };
 
 struct TimeStatsArgs {
@@ -113,6 +116,9 @@ struct WakeArgs {
   void launch_limit(const TrackArgs &a, const trk_aperture &ap, int mode, int extrapolate, double z, long pass,  \
                     int elem, int grid, cudaStream_t st);                                                    \
   void launch_matrix(const TrackArgs &a, const double *m, int order, int grid, cudaStream_t st);             \
+  int ensemble_variant_ok(int variant);                                                                      \
+  void launch_track_ensemble(const TrackArgs &a, const long *offsets, int n_variants, int ops_per_variant,   \
+                             int variant, bool lean, long n, int max_blocks, cudaStream_t st);              \
   cudaError_t set_coefficients(const double *coef10);                                                        \
   }
 

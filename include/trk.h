@@ -248,10 +248,19 @@ int trk_track_matrix(trk_context *ctx, int order, const double *C, const double 
 /* Track `n_variants` lattices that differ only in element parameter values
  * (error seeds, grids) in one launch.  `lattices` holds n_variants lattices of
  * identical structure; variant v owns particles [offsets[v], offsets[v+1]) of
- * the device beam.  Collective elements (WAKE, TRWAKE, RFCA fiducial) are not
- * allowed in ensembles. */
+ * the device beam (offsets[0] = 0, offsets[n_variants] = particles loaded).
+ * All passes run in chunked launches of the fused tracking kernel, captured
+ * into a CUDA graph; each particle reads its own variant's element records.
+ * Collective elements (WAKE, TRWAKE, RFCA) are not allowed in ensembles.
+ * The batched error-seed and dynamic-aperture studies of the reference run
+ * do_tracking once per variant (src/error.c, src/aperture_search.c:456). */
 int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int n_variants,
                        const long *offsets, const trk_run *run, trk_stats *stats);
+/* Launch shape (trk_run.variant value) the last trk_track_ensemble used: the
+ * caller's, or the autotuner's choice, which times each candidate shape on a
+ * scratch copy of the beam over the first passes of the first call for a
+ * given element count, particle count and build, and keeps the fastest. */
+int trk_ensemble_variant(const trk_context *ctx);
 
 /* ------------------------------------------------- allocation-free wake */
 /* No counterpart in the reference: elegant's WAKE (src/wake.c:23-304)
