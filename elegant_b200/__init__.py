@@ -94,6 +94,7 @@ def _declare(lib):
                                    ctypes.POINTER(_Stats)]),
         "trk_adjoint": (I, [P, P, ctypes.POINTER(_Run), D, DP, DP, I]),
         "trk_adjoint_param_count": (I, [P]),
+        "trk_objective": (I, [P, D, DP]),
     }
     for name, (res, args) in sig.items():
         if hasattr(lib, name):
@@ -289,6 +290,31 @@ class Tracker:
         out = _stats_dict(st)
         out["variant"] = self.lib.trk_ensemble_variant(self.ctx)
         return out
+
+    def adjoint(self, lattice, n_passes, p_central, centroid_weight=0.0, pass_offset=0, with_grad=True):
+        """Track the loaded beam n_passes passes and return (loss, gradient):
+        loss = mean(x^2 + y^2) + w (mean(x)^2 + mean(y)^2) over survivors,
+        gradient with respect to every KQUAD K1 and KSEXT K2 in lattice order
+        (reverse-mode adjoint on the device).  The beam is left at its final
+        state."""
+        nat = self.native(lattice)
+        n = _check(self.lib, self.lib.trk_adjoint_param_count(nat.ptr))
+        run = _Run()
+        self.lib.trk_run_defaults(ctypes.byref(run))
+        run.p_central = p_central
+        run.n_passes = n_passes
+        run.pass_offset = pass_offset
+        loss = ctypes.c_double()
+        g = np.zeros(max(n, 1))
+        _check(self.lib, self.lib.trk_adjoint(self.ctx, nat.ptr, ctypes.byref(run), centroid_weight, ctypes.byref(loss),
+                                              _dptr(g) if with_grad else None, n))
+        return loss.value, g[:n]
+
+    def objective(self, centroid_weight=0.0):
+        """The adjoint's loss function on the device beam as it is."""
+        v = ctypes.c_double()
+        _check(self.lib, self.lib.trk_objective(self.ctx, centroid_weight, ctypes.byref(v)))
+        return v.value
 
     def set_comm(self, unique_id, nranks, rank):
         """Join a sharded run: `unique_id` (128 bytes from nccl_unique_id() on

@@ -88,6 +88,12 @@ struct trk_context {
   };
   std::vector<Tuned> ens_tuned;  /* autotuner choices */
   int ens_last_variant = -1;
+  /* gradient runs: pass checkpoints, element entry states, adjoints */
+  double *d_adj_ck = nullptr, *d_adj_entry = nullptr, *d_adj_lam = nullptr, *d_adj_grad = nullptr;
+  double *d_adj_dk = nullptr, *d_adj_mom = nullptr;
+  int *d_adj_param = nullptr;
+  size_t adj_ck_cap = 0, adj_entry_cap = 0, adj_lam_cap = 0, adj_grad_cap = 0, adj_dk_cap = 0, adj_mom_cap = 0,
+         adj_param_cap = 0;
   size_t matrix_cap = 0;
   double *d_gather = nullptr; /* 6 doubles per rank */
   long long *d_effort = nullptr;
@@ -698,6 +704,13 @@ void trk_context_destroy(trk_context *ctx) {
   cudaFree(ctx->d_matrix);
   cudaFree(ctx->d_ens_offsets);
   cudaFree(ctx->d_tune);
+  cudaFree(ctx->d_adj_ck);
+  cudaFree(ctx->d_adj_entry);
+  cudaFree(ctx->d_adj_lam);
+  cudaFree(ctx->d_adj_grad);
+  cudaFree(ctx->d_adj_dk);
+  cudaFree(ctx->d_adj_mom);
+  cudaFree(ctx->d_adj_param);
   trk_comm_destroy(ctx->comm);
   cudaFree(ctx->d_effort);
   cudaFree(ctx->d_aos);
@@ -1475,16 +1488,218 @@ int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int
 
 int trk_ensemble_variant(const trk_context *ctx) { return ctx ? ctx->ens_last_variant : -1; }
 
+/* ------------------------------------------------------------- gradients */
+/* sums over surviving particles: x^2 + y^2, x, y, count */
+__global__ void adj_moments_kernel(const double *x, const double *y, const int32_t *lost, long n, double *out) {
+  double s2 = 0, sx = 0, sy = 0, c = 0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    if (lost[i] < 0) {
+      s2 += x[i] * x[i] + y[i] * y[i];
+      sx += x[i];
+      sy += y[i];
+      c += 1;
+    }
+  for (int off = 16; off > 0; off >>= 1) {
+    s2 += __shfl_xor_sync(0xffffffffu, s2, off);
+    sx += __shfl_xor_sync(0xffffffffu, sx, off);
+    sy += __shfl_xor_sync(0xffffffffu, sy, off);
+    c += __shfl_xor_sync(0xffffffffu, c, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(out, s2);
+    atomicAdd(out + 1, sx);
+    atomicAdd(out + 2, sy);
+    atomicAdd(out + 3, c);
+  }
+}
+
+/* lambda at the end of the run: dL/dx = (2 x + 2 w mean(x)) / N, same in y */
+__global__ void adj_seed_kernel(const double *x, const double *y, const int32_t *lost, long n, double *lam, double gx,
+                                double gy, double inv_n) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const bool act = lost[i] < 0;
+    lam[i] = act ? 2 * x[i] * inv_n + gx : 0;
+    lam[n + i] = 0;
+    lam[2 * n + i] = act ? 2 * y[i] * inv_n + gy : 0;
+    lam[3 * n + i] = 0;
+    lam[4 * n + i] = 0;
+  }
+}
+
+/* L = mean(x^2 + y^2) + w (mean(x)^2 + mean(y)^2) over survivors; also the
+ * means and the survivor count */
+static int objective(trk_context *ctx, double w, double *L, double *mx, double *my, double *count) {
+  int rc;
+  if ((rc = ensure(&ctx->d_adj_mom, ctx->adj_mom_cap, 4)))
+    return rc;
+  CUDA_TRY(cudaMemsetAsync(ctx->d_adj_mom, 0, 4 * sizeof(double), ctx->stream));
+  if (ctx->np > 0)
+    adj_moments_kernel<<<std::min(grid_for(ctx, ctx->np, 256), 1184), 256, 0, ctx->stream>>>(
+      ctx->d_cols, ctx->d_cols + 2 * ctx->cap, ctx->d_lost_pass, ctx->np, ctx->d_adj_mom);
+  double h[4];
+  CUDA_TRY(cudaMemcpyAsync(h, ctx->d_adj_mom, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (h[3] <= 0)
+    return trk_set_error(TRK_ERR_PHYSICS, "no surviving particles for the loss function");
+  *mx = h[1] / h[3];
+  *my = h[2] / h[3];
+  *count = h[3];
+  *L = h[0] / h[3] + w * (*mx * *mx + *my * *my);
+  return TRK_OK;
+}
+
+int trk_objective(trk_context *ctx, double centroid_weight, double *loss) {
+  if (!ctx || !loss)
+    return trk_set_error(TRK_ERR_ARG, "null argument");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  double mx, my, c;
+  return objective(ctx, centroid_weight, loss, &mx, &my, &c);
+}
+
+/* the parameter of an element and the derivative of its per-step kick
+ * strengths with respect to it (the element compiled with the parameter
+ * set to 1; kick strengths are linear in it) */
+static int param_derivative(const trk_elem *e, double Po, double *dk3) {
+  trk_elem t = *e;
+  const char *name = e->type == TRK_KQUAD ? "K1" : "K2";
+  const int pi = trk_param_index(e->type, name);
+  if (pi < 0)
+    return pi;
+  t.p[pi] = 1.0;
+  trk_lattice L;
+  L.n = L.cap = 1;
+  L.e = &t;
+  CompiledLattice c;
+  int rc = trk_compile(&L, Po, c);
+  if (rc)
+    return rc;
+  if (c.ops.size() != 1 || c.ops[0].kind != OPK_MULT1)
+    return trk_set_error(TRK_ERR_UNSUPPORTED, "%s: gradients need a single-order multipole without tilt, "
+                         "misalignment or steering", e->name);
+  for (int s = 0; s < 3; s++)
+    dk3[s] = c.ops[0].d[MD_KQ + s * 3];
+  return TRK_OK;
+}
+
 int trk_adjoint(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, double centroid_weight,
                 double *loss, double *grad, int n_grad) {
-  (void)ctx;
-  (void)lattice;
-  (void)run;
-  (void)centroid_weight;
-  (void)loss;
-  (void)grad;
-  (void)n_grad;
-  return trk_set_error(TRK_ERR_UNSUPPORTED, "adjoint not built yet");
+  if (!ctx || !lattice || !run)
+    return trk_set_error(TRK_ERR_ARG, "null argument");
+  const int n_params = trk_adjoint_param_count(lattice);
+  if (grad && n_grad != n_params)
+    return trk_set_error(TRK_ERR_ARG, "grad has %d entries, the lattice has %d parameters", n_grad, n_params);
+  if (run->n_passes < 1)
+    return trk_set_error(TRK_ERR_ARG, "at least one pass");
+  if (ctx->np <= 0)
+    return trk_set_error(TRK_ERR_STATE, "no beam loaded");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  const double Po = run->p_central;
+  int rc = upload_lattice(ctx, lattice, Po);
+  if (rc)
+    return rc;
+  const CompiledLattice &c = ctx->comp;
+  const int nops = (int)c.ops.size();
+  std::vector<int> op_param(std::max(nops, 1), -1);
+  std::vector<double> op_dk(3 * std::max(nops, 1), 0.0);
+  std::vector<int> param_of_elem(lattice->n, -1);
+  for (int i = 0, k = 0; i < lattice->n; i++)
+    if (lattice->e[i].type == TRK_KQUAD || lattice->e[i].type == TRK_KSEXT)
+      param_of_elem[i] = k++;
+  for (int k = 0; k < nops; k++) {
+    const trk_op &op = c.ops[k];
+    switch (op.kind) {
+    case OPK_NOP:
+    case OPK_DRIFT:
+    case OPK_EDRIFT:
+    case OPK_RFDRIFT:
+      break;
+    case OPK_MULT1:
+      if (op.i[0] * 3 > 48)
+        return trk_set_error(TRK_ERR_UNSUPPORTED, "multipole with more than 16 slices in a gradient run");
+      break;
+    case OPK_DIPOLE:
+      if (op.i[0] * 4 > 128)
+        return trk_set_error(TRK_ERR_UNSUPPORTED, "CSBEND with more than 32 slices in a gradient run");
+      break;
+    default:
+      return trk_set_error(TRK_ERR_UNSUPPORTED, "element %d: gradients cover DRIF, EDRIFT, KQUAD/KSEXT/KOCT "
+                           "(single order, no tilt or misalignment) and pure-dipole CSBEND", op.elem);
+    }
+    const int pe = (op.elem >= 0 && op.elem < lattice->n) ? param_of_elem[op.elem] : -1;
+    if (pe >= 0) {
+      if (op.kind != OPK_MULT1)
+        return trk_set_error(TRK_ERR_UNSUPPORTED, "element %d: gradients need a single-order multipole", op.elem);
+      op_param[k] = pe;
+      if ((rc = param_derivative(&lattice->e[op.elem], Po, &op_dk[3 * k])))
+        return rc;
+    }
+  }
+  const long np = ctx->np, T = run->n_passes;
+  if ((rc = ensure(&ctx->d_adj_ck, ctx->adj_ck_cap, (size_t)T * 4 * np)) ||
+      (rc = ensure(&ctx->d_adj_entry, ctx->adj_entry_cap, (size_t)std::max(nops, 1) * 4 * np)) ||
+      (rc = ensure(&ctx->d_adj_lam, ctx->adj_lam_cap, (size_t)5 * np)) ||
+      (rc = ensure(&ctx->d_adj_grad, ctx->adj_grad_cap, (size_t)std::max(n_params, 1))) ||
+      (rc = ensure(&ctx->d_adj_param, ctx->adj_param_cap, op_param.size())) ||
+      (rc = ensure(&ctx->d_adj_dk, ctx->adj_dk_cap, op_dk.size())))
+    return rc;
+  CUDA_TRY(cudaMemcpyAsync(ctx->d_adj_param, op_param.data(), sizeof(int) * op_param.size(), cudaMemcpyHostToDevice,
+                           ctx->stream));
+  CUDA_TRY(cudaMemcpyAsync(ctx->d_adj_dk, op_dk.data(), sizeof(double) * op_dk.size(), cudaMemcpyHostToDevice,
+                           ctx->stream));
+  CUDA_TRY(cudaMemsetAsync(ctx->d_adj_grad, 0, sizeof(double) * std::max(n_params, 1), ctx->stream));
+
+  /* forward, one pass per launch, the beam at the start of every pass kept */
+  const long p0 = run->pass_offset;
+  const long fresh = ctx->passes_done == 0 ? p0 : -1;
+  if (fresh >= 0)
+    screen_kernel<<<(int)((np + 255) / 256), 256, 0, ctx->stream>>>(ctx->d_cols, ctx->cap, ctx->d_lost_pass,
+                                                                    ctx->d_lost_elem, np, p0, Po);
+  TrackArgs ta = track_args(ctx);
+  ta.fresh_pass = fresh;
+  ta.Po = Po;
+  ta.op_begin = 0;
+  ta.op_end = nops;
+  const int col[4] = {0, 1, 2, 3};
+  for (long t = 0; t < T; t++) {
+    for (int q = 0; q < 4; q++)
+      CUDA_TRY(cudaMemcpyAsync(ctx->d_adj_ck + ((size_t)t * 4 + q) * np, ctx->d_cols + (size_t)col[q] * ctx->cap,
+                               sizeof(double) * np, cudaMemcpyDeviceToDevice, ctx->stream));
+    ta.pass_begin = p0 + t;
+    ta.pass_end = p0 + t + 1;
+    if (nops > 0)
+      trk_fast::launch_track(ta, (c.lean ? 7 : 1), c.lean, np, ctx->sm_count * 256, ctx->stream);
+  }
+  CUDA_TRY(cudaGetLastError());
+  ctx->passes_done += T;
+  double L, mx, my, cnt;
+  if ((rc = objective(ctx, centroid_weight, &L, &mx, &my, &cnt)))
+    return rc;
+  if (loss)
+    *loss = L;
+  if (!grad)
+    return TRK_OK;
+
+  /* reverse: seed, then per pass (last first) record the element entry
+   * states from the pass checkpoint and sweep the elements backwards */
+  adj_seed_kernel<<<std::min(grid_for(ctx, np, 256), 1184), 256, 0, ctx->stream>>>(
+    ctx->d_cols, ctx->d_cols + 2 * ctx->cap, ctx->d_lost_pass, np, ctx->d_adj_lam, 2 * centroid_weight * mx / cnt,
+    2 * centroid_weight * my / cnt, 1.0 / cnt);
+  AdjArgs g;
+  g.entry = ctx->d_adj_entry;
+  g.lam = ctx->d_adj_lam;
+  g.grad = ctx->d_adj_grad;
+  g.op_param = ctx->d_adj_param;
+  g.op_dk = ctx->d_adj_dk;
+  g.n_ops = nops;
+  for (long t = T - 1; t >= 0; t--) {
+    g.ck = ctx->d_adj_ck + (size_t)t * 4 * np;
+    trk_fast::launch_adjoint_record(ta, g, ctx->stream);
+    trk_fast::launch_adjoint_reverse(ta, g, ctx->stream);
+  }
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpyAsync(grad, ctx->d_adj_grad, sizeof(double) * n_params, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return check_status(ctx);
 }
 
 int trk_adjoint_param_count(const trk_lattice *lattice) {

@@ -19,6 +19,8 @@
  */
 #include <cuda_runtime.h>
 #include <stddef.h>
+
+#include <algorithm>
 #include <stdint.h>
 
 #include "trk_constants.h"
@@ -2070,6 +2072,310 @@ __global__ void matrix_kernel(TrackArgs a, const double *__restrict__ m, int ord
   }
 }
 
+#if TRK_FAST
+/* ------------------------------------------------------------- adjoint
+ * Reverse mode through the fast build's element maps.  The forward values
+ * inside an element are recomputed from its entry state (recorded per pass
+ * by adj_record_kernel) and the chain rule is applied backwards, operation
+ * by operation, to the adjoint (lambda) of x, x', y, y', delta.  Parameter
+ * sensitivities of the kick strengths are summed per warp and added to the
+ * gradient with one atomic per warp and element. */
+#define TRK_ADJ_MAX_KICKS 48  /* multipole: slices * 3 kicks */
+#define TRK_ADJ_MAX_STEPS 128 /* dipole: slices * 4 substeps */
+
+/* (sx, sy) = (qx, qy) / sqrt((1+delta)^2 - qx^2 - qy^2): adds the adjoint of
+ * qx, qy, delta given that of sx, sy */
+__device__ __forceinline__ void adj_m2s(double qx, double qy, double opd, double lsx, double lsy, double &lqx,
+                                        double &lqy, double &ldp) {
+  const double g = rsqrt_fast(opd * opd - qx * qx - qy * qy);
+  const double g3 = g * g * g;
+  lqx += lsx * (g + qx * qx * g3) + lsy * (qx * qy * g3);
+  lqy += lsx * (qx * qy * g3) + lsy * (g + qy * qy * g3);
+  ldp -= (lsx * qx + lsy * qy) * opd * g3;
+}
+
+/* (qx, qy) = (1+delta) (xp, yp) / sqrt(1 + xp^2 + yp^2): adjoint of xp, yp,
+ * delta given that of qx, qy */
+__device__ __forceinline__ void adj_s2m(double xp, double yp, double opd, double lqx, double lqy, double &lxp,
+                                        double &lyp, double &ldp) {
+  const double rs = rsqrt_fast(fma(yp, yp, fma(xp, xp, 1.0)));
+  const double rs3 = rs * rs * rs;
+  lxp += lqx * opd * (rs - xp * xp * rs3) - lqy * opd * xp * yp * rs3;
+  lyp += lqy * opd * (rs - yp * yp * rs3) - lqx * opd * xp * yp * rs3;
+  ldp += (lqx * xp + lqy * yp) * rs;
+}
+
+/* normal multipole field of order 1..3 with the fast build's coefficients:
+ * kick qx -= K Fy, qy += K Fx, and the partial derivatives */
+__device__ __forceinline__ void mult_field(int order, double x, double y, double &Fy, double &Fx, double &Fyx,
+                                           double &Fyy, double &Fxx, double &Fxy) {
+  if (order == 1) {
+    Fy = x;
+    Fx = y;
+    Fyx = 1;
+    Fyy = 0;
+    Fxx = 0;
+    Fxy = 1;
+  } else if (order == 2) {
+    Fy = 0.5 * (x * x - y * y);
+    Fx = x * y;
+    Fyx = x;
+    Fyy = -y;
+    Fxx = y;
+    Fxy = x;
+  } else {
+    const double x2 = x * x, y2 = y * y;
+    Fy = (x2 * x - 3 * x * y2) * (1.0 / 6);
+    Fx = (3 * x2 * y - y2 * y) * (1.0 / 6);
+    Fyx = 0.5 * (x2 - y2);
+    Fyy = -x * y;
+    Fxx = x * y;
+    Fxy = 0.5 * (x2 - y2);
+  }
+}
+
+/* adjoint of op_mult1_fast (the body of mult_body_fast); returns the
+ * sensitivity of the particle's contribution to the element's parameter */
+__device__ double adj_mult1(const trk_op *__restrict__ op, const double *__restrict__ dk, double x, double xp,
+                            double y, double yp, double dp, double &lx, double &lxp, double &ly, double &lyp,
+                            double &ldp) {
+  const double *d = op->d;
+  const int n_parts = __ldg(&op->i[0]);
+  const int order = __ldg(&op->i[4]) & 0xff;
+  const double opd = 1 + dp, opd2 = opd * opd;
+  double KX[TRK_ADJ_MAX_KICKS], KY[TRK_ADJ_MAX_KICKS], QX[TRK_ADJ_MAX_KICKS], QY[TRK_ADJ_MAX_KICKS];
+  const double r = opd * rsqrt_fast(fma(yp, yp, fma(xp, xp, 1.0)));
+  double qx = xp * r, qy = yp * r, sx = xp, sy = yp;
+  int nk = 0;
+  for (int i_kick = 0; i_kick < n_parts; i_kick++)
+    for (int step = 0; step < 4; step++) {
+      const double dsh = __ldg(&d[MD_DSH + step]);
+      x = fma(sx, dsh, x);
+      y = fma(sy, dsh, y);
+      if (step == 3)
+        break;
+      const double K = __ldg(&d[MD_KQ + step * 3]);
+      double Fy, Fx, a, b, c, e;
+      mult_field(order, x, y, Fy, Fx, a, b, c, e);
+      qx = fma(-K, Fy, qx);
+      qy = fma(K, Fx, qy);
+      const double rr = rsqrt_fast(opd2 - qx * qx - qy * qy);
+      sx = qx * rr;
+      sy = qy * rr;
+      KX[nk] = x;
+      KY[nk] = y;
+      QX[nk] = qx;
+      QY[nk] = qy;
+      nk++;
+    }
+  /* exit slopes from the final momenta */
+  double lqx = 0, lqy = 0, lsx = 0, lsy = 0, sens = 0;
+  adj_m2s(qx, qy, opd, lxp, lyp, lqx, lqy, ldp);
+  for (int i_kick = n_parts - 1; i_kick >= 0; i_kick--)
+    for (int step = 3; step >= 0; step--) {
+      if (step < 3) {
+        nk--;
+        adj_m2s(QX[nk], QY[nk], opd, lsx, lsy, lqx, lqy, ldp);
+        lsx = lsy = 0;
+        const double K = __ldg(&d[MD_KQ + step * 3]);
+        double Fy, Fx, Fyx, Fyy, Fxx, Fxy;
+        mult_field(order, KX[nk], KY[nk], Fy, Fx, Fyx, Fyy, Fxx, Fxy);
+        lx += K * (-Fyx * lqx + Fxx * lqy);
+        ly += K * (-Fyy * lqx + Fxy * lqy);
+        sens += (-Fy * lqx + Fx * lqy) * __ldg(&dk[step]);
+      }
+      const double dsh = __ldg(&d[MD_DSH + step]);
+      lsx += dsh * lx;
+      lsy += dsh * ly;
+    }
+  /* entry: the first drift used the incoming slopes; the momenta came from them */
+  double lxp_in = lsx, lyp_in = lsy;
+  adj_s2m(xp, yp, opd, lqx, lqy, lxp_in, lyp_in, ldp);
+  lxp = lxp_in;
+  lyp = lyp_in;
+  return sens;
+}
+
+/* adjoint of op_dipole_fast (bend_dipole_fast / dipole_slice) */
+__device__ void adj_dipole(const trk_op *__restrict__ op, double x, double xp, double y, double yp, double dp,
+                           double &lx, double &lxp, double &ly, double &lyp, double &ldp) {
+  const double *d = op->d;
+  const int nSlices = __ldg(&op->i[0]);
+  const double rho0 = __ldg(&d[BD_RHO0]);
+  const double opd = 1 + dp;
+  const double rs = rsqrt_fast(fma(yp, yp, fma(xp, xp, 1.0)));
+  const double QY = yp * opd * rs;
+  const double f2 = opd * opd - QY * QY;
+  double X = x, Q = xp * opd * rs, F = 0;
+  double SX[TRK_ADJ_MAX_STEPS], SQ[TRK_ADJ_MAX_STEPS];
+  int m = 0;
+  for (int i = 0; i < nSlices; i++)
+    for (int j = 0; j < 4; j++) {
+      SX[m] = X;
+      SQ[m] = Q;
+      m++;
+      const double sa = __ldg(&d[BD_SA + j]), ca = __ldg(&d[BD_CA + j]), omc = __ldg(&d[BD_OMC + j]);
+      const double fc = sqrt_nan(fma(-Q, Q, f2));
+      const double saq = sa * Q;
+      const double u = div_fast(rho0 + X, fma(ca, fc, -saq));
+      Q = fma(sa, fc, ca * Q);
+      F = fma(u, sa, F);
+      X = fma(u, fma(omc, fc, saq), X);
+      if (j < 3)
+        Q = fma(-__ldg(&d[BD_C2 + j]), X, Q - __ldg(&d[BD_C1 + j]));
+    }
+  /* exit: x = X, y = y0 + QY F, (xp, yp) = (Q, QY) / sqrt(opd^2 - Q^2 - QY^2) */
+  double lX = lx, lQ = 0, lQY = 0, lopd = 0, lF = QY * ly, lf2 = 0;
+  lQY += F * ly;
+  {
+    const double g = rsqrt_fast(opd * opd - Q * Q - QY * QY);
+    const double g3 = g * g * g;
+    lQ += lxp * (g + Q * Q * g3) + lyp * Q * QY * g3;
+    lQY += lyp * (g + QY * QY * g3) + lxp * Q * QY * g3;
+    lopd -= (lxp * Q + lyp * QY) * opd * g3;
+  }
+  for (int i = nSlices - 1; i >= 0; i--)
+    for (int j = 3; j >= 0; j--) {
+      if (j < 3)
+        lX -= __ldg(&d[BD_C2 + j]) * lQ;
+      m--;
+      const double Xs = SX[m], Qs = SQ[m];
+      const double sa = __ldg(&d[BD_SA + j]), ca = __ldg(&d[BD_CA + j]), omc = __ldg(&d[BD_OMC + j]);
+      const double fc = sqrt_nan(fma(-Qs, Qs, f2));
+      const double saq = sa * Qs;
+      const double fcosi = fma(ca, fc, -saq);
+      const double u = div_fast(rho0 + Xs, fcosi);
+      const double lu = lF * sa + lX * fma(omc, fc, saq);
+      double lfc = lQ * sa + lX * u * omc;
+      double lsaq = lX * u;
+      double lQs = lQ * ca;
+      double lXs = lX;
+      const double lfcosi = -lu * u / fcosi;
+      lXs += lu / fcosi;
+      lfc += ca * lfcosi;
+      lsaq -= lfcosi;
+      lQs += sa * lsaq;
+      const double lu2 = lfc / (2 * fc);
+      lf2 += lu2;
+      lQs -= 2 * Qs * lu2;
+      lX = lXs;
+      lQ = lQs;
+    }
+  lopd += 2 * opd * lf2;
+  lQY -= 2 * QY * lf2;
+  /* entry: X = x, (Q, QY) = opd (xp, yp) / sqrt(1 + xp^2 + yp^2) */
+  const double rs3 = rs * rs * rs;
+  lx = lX;
+  lxp = lQ * opd * (rs - xp * xp * rs3) - lQY * opd * xp * yp * rs3;
+  lyp = lQY * opd * (rs - yp * yp * rs3) - lQ * opd * xp * yp * rs3;
+  lopd += (lQ * xp + lQY * yp) * rs;
+  ldp += lopd;
+}
+
+/* forward pass from a checkpoint, recording every element's entry state */
+__global__ void adj_record_kernel(TrackArgs a, AdjArgs g) {
+  const long n = a.n, stride = (long)gridDim.x * blockDim.x;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    if (a.lost_pass[i] >= 0)
+      continue;
+    Part p;
+    p.x = g.ck[i];
+    p.xp = g.ck[n + i];
+    p.y = g.ck[2 * n + i];
+    p.yp = g.ck[3 * n + i];
+    p.s = 0;
+    p.dp = a.dp[i];
+    for (int k = 0; k < g.n_ops; k++) {
+      const trk_op *op = a.ops + k;
+      double *e = g.entry + (size_t)k * 4 * n;
+      e[i] = p.x;
+      e[n + i] = p.xp;
+      e[2 * n + i] = p.y;
+      e[3 * n + i] = p.yp;
+      switch (__ldg(&op->kind)) {
+      case OPK_DRIFT:
+        op_drift(op, p);
+        break;
+      case OPK_EDRIFT:
+      case OPK_RFDRIFT:
+        exact_drift(p, __ldg(&op->d[DD_L]));
+        break;
+      case OPK_MULT1:
+        op_mult1_fast(op, p, a.Po, 0.0, nullptr);
+        break;
+      case OPK_DIPOLE:
+        op_dipole_fast(op, p, a.Po, 0.0, nullptr);
+        break;
+      default:
+        break;
+      }
+    }
+  }
+}
+
+/* one pass backwards: lambda at the end of the pass -> at its start */
+__global__ void __launch_bounds__(128) adj_reverse_kernel(TrackArgs a, AdjArgs g) {
+  const long n = a.n;
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = i < n && a.lost_pass[i] < 0;
+  double lx = 0, lxp = 0, ly = 0, lyp = 0, ldp = 0, dp = 0;
+  if (act) {
+    lx = g.lam[i];
+    lxp = g.lam[n + i];
+    ly = g.lam[2 * n + i];
+    lyp = g.lam[3 * n + i];
+    ldp = g.lam[4 * n + i];
+    dp = a.dp[i];
+  }
+  for (int k = g.n_ops - 1; k >= 0; k--) {
+    const trk_op *op = a.ops + k;
+    double x = 0, xp = 0, y = 0, yp = 0;
+    if (act) {
+      const double *e = g.entry + (size_t)k * 4 * n;
+      x = e[i];
+      xp = e[n + i];
+      y = e[2 * n + i];
+      yp = e[3 * n + i];
+    }
+    double sens = 0;
+    switch (__ldg(&op->kind)) {
+    case OPK_DRIFT:
+    case OPK_EDRIFT:
+    case OPK_RFDRIFT: {
+      const double L = __ldg(&op->d[DD_L]);
+      lxp += L * lx;
+      lyp += L * ly;
+      break;
+    }
+    case OPK_MULT1:
+      sens = adj_mult1(op, g.op_dk + 3 * k, x, xp, y, yp, dp, lx, lxp, ly, lyp, ldp);
+      break;
+    case OPK_DIPOLE:
+      adj_dipole(op, x, xp, y, yp, dp, lx, lxp, ly, lyp, ldp);
+      break;
+    default:
+      break;
+    }
+    const int prm = __ldg(&g.op_param[k]);
+    if (prm >= 0) {
+      if (!act)
+        sens = 0;
+      for (int off = 16; off > 0; off >>= 1)
+        sens += __shfl_xor_sync(0xffffffffu, sens, off);
+      if ((threadIdx.x & 31) == 0 && sens != 0)
+        atomicAdd(&g.grad[prm], sens);
+    }
+  }
+  if (act) {
+    g.lam[i] = lx;
+    g.lam[n + i] = lxp;
+    g.lam[2 * n + i] = ly;
+    g.lam[3 * n + i] = lyp;
+    g.lam[4 * n + i] = ldp;
+  }
+}
+#endif
+
 /* ------------------------------------------------------------- launchers */
 int track_variant_block(int variant) {
   switch (variant) {
@@ -2188,6 +2494,28 @@ void launch_track_ensemble(const TrackArgs &a, const long *offsets, int n_varian
   e.ens_variants = n_variants;
   e.ens_ops = ops_per_variant;
   launch_track(e, ensemble_variant_ok(variant) ? variant : 1, lean, n, max_blocks, st);
+}
+
+void launch_adjoint_record(const TrackArgs &a, const AdjArgs &g, cudaStream_t st) {
+#if TRK_FAST
+  const long grid = std::min<long>((a.n + 127) / 128, 148L * 64);
+  adj_record_kernel<<<(int)std::max<long>(grid, 1), 128, 0, st>>>(a, g);
+#else
+  (void)a;
+  (void)g;
+  (void)st;
+#endif
+}
+
+void launch_adjoint_reverse(const TrackArgs &a, const AdjArgs &g, cudaStream_t st) {
+#if TRK_FAST
+  const long grid = (a.n + 127) / 128;
+  adj_reverse_kernel<<<(int)std::max<long>(grid, 1), 128, 0, st>>>(a, g);
+#else
+  (void)a;
+  (void)g;
+  (void)st;
+#endif
 }
 
 void launch_limit(const TrackArgs &a, const trk_aperture &ap, int mode, int extrapolate, double z, long pass, int elem,

@@ -101,6 +101,18 @@ struct WakeArgs {
   int element_only; /* 1: no NaN filter after the kick (per-element entry points) */
 };
 
+/* reverse-mode adjoint of the fast build's element maps (DRIF, EDRIFT,
+ * single-order multipoles, pure-dipole CSBEND) */
+struct AdjArgs {
+  const double *ck;      /* checkpoint of the pass being reversed: x, xp, y, yp columns of n */
+  double *entry;         /* element entry states: [op][4][n] */
+  double *lam;           /* adjoint of x, xp, y, yp, delta: 5 columns of n */
+  double *grad;          /* gradient accumulators, one per parameter */
+  const int *op_param;   /* parameter index of each op, -1 if none */
+  const double *op_dk;   /* per op: d(kick strength)/d(parameter) of kick steps 0..2 */
+  int n_ops;
+};
+
 #define TRK_DECLARE_LAUNCHERS(NS)                                                                            \
   namespace NS {                                                                                             \
   int track_variant_block(int variant);                                                                      \
@@ -117,6 +129,8 @@ struct WakeArgs {
                     int elem, int grid, cudaStream_t st);                                                    \
   void launch_matrix(const TrackArgs &a, const double *m, int order, int grid, cudaStream_t st);             \
   int ensemble_variant_ok(int variant);                                                                      \
+  void launch_adjoint_record(const TrackArgs &a, const AdjArgs &g, cudaStream_t st);                         \
+  void launch_adjoint_reverse(const TrackArgs &a, const AdjArgs &g, cudaStream_t st);                        \
   void launch_track_ensemble(const TrackArgs &a, const long *offsets, int n_variants, int ops_per_variant,   \
                              int variant, bool lean, long n, int max_blocks, cudaStream_t st);              \
   cudaError_t set_coefficients(const double *coef10);                                                        \

@@ -295,15 +295,26 @@ int trk_wake_noalloc(double *const *columns, int32_t *lost_pass, int32_t *lost_e
                      double factor, int interpolate, int allow_long_beam, long pass, int fast_math, void *stream);
 
 /* ------------------------------------------------------------- gradients */
-/* Reverse-mode adjoint through the fused element chain.  Loss function:
- *   L = mean_i (x_i^2 + y_i^2) + w_c * (mean_i x_i)^2 + (mean_i y_i)^2 )
- * over surviving particles after n_passes passes.  Parameters: the K1 of
- * every KQUAD and the K2 of every KSEXT, in lattice order (grad has
- * n_kquad + n_ksext entries).  Per-pass checkpoints of the beam are stored
- * on the device and each pass is recomputed during the reverse sweep.
- * The device beam is left at its final (forward) state. */
+/* Reverse-mode adjoint through the fused element chain (no counterpart in
+ * the reference, which offers only finite differences through repeated
+ * tracking).  Tracks the loaded beam n_passes passes (fast build), keeping
+ * the beam at the start of every pass on the device, then sweeps back pass
+ * by pass: each pass is recomputed from its checkpoint with every element's
+ * entry state recorded, and the elements' hand-written adjoints carry
+ * d(loss)/d(coordinates) backwards while the kick-strength sensitivities are
+ * summed into the gradient.  Loss function over the surviving particles:
+ *   loss = mean_i (x_i^2 + y_i^2) + w_c ((mean_i x_i)^2 + (mean_i y_i)^2)
+ * (particles lost during the run are left out: loss events are not
+ * differentiable).  Parameters: K1 of every KQUAD and K2 of every KSEXT, in
+ * lattice order.  Elements allowed: DRIF, EDRIFT, single-order
+ * KQUAD/KSEXT/KOCT without tilt or misalignment, pure-dipole CSBEND, MARK,
+ * MAXAMP.  grad may be NULL (loss only).  The device beam is left at its
+ * final state. */
 int trk_adjoint(trk_context *ctx, const trk_lattice *lattice, const trk_run *run,
                 double centroid_weight, double *loss, double *grad, int n_grad);
+/* The same loss function on the device beam as it is (for finite
+ * differences against trk_adjoint). */
+int trk_objective(trk_context *ctx, double centroid_weight, double *loss);
 /* Number of gradient parameters (KQUAD K1 + KSEXT K2) of a lattice. */
 int trk_adjoint_param_count(const trk_lattice *lattice);
 

@@ -1,0 +1,121 @@
+"""Reverse-mode gradients (trk_adjoint) of the tracked-beam objective
+mean(x^2+y^2) + w (mean(x)^2 + mean(y)^2) with respect to every KQUAD K1 and
+KSEXT K2, against central finite differences (h = 1e-7 relative) of the GPU
+tracking and of elegant's own compiled tracking code; relative gradient
+error <= 1e-6."""
+import numpy as np
+import pytest
+
+from elegant_b200 import Tracker, configs
+from elegant_b200.adjoint import get_parameters, make_autograd, set_parameters
+from oracle import pyoracle
+
+pytestmark = pytest.mark.gpu
+PC = configs.P_CENTRAL
+W = 0.7
+
+
+def _lattice(cells=2):
+    return configs.c2_lattice(cells=cells, with_rf=False, with_wake=False)
+
+
+def _beam(n=2000, seed=91):
+    b = configs.gaussian_beam(n, seed=seed, sigma_x=1e-3, sigma_xp=5e-5)
+    b[:, 0] += 2e-4  # an offset centroid so the centroid term matters
+    return b
+
+
+def _objective_rows(rows, w):
+    alive = rows[:, 7] < 0
+    x, y = rows[alive, 0], rows[alive, 2]
+    return np.mean(x * x + y * y) + w * (np.mean(x) ** 2 + np.mean(y) ** 2)
+
+
+def _rel_err(g, ref):
+    scale = np.maximum(np.abs(ref), 1e-3 * np.max(np.abs(ref)))
+    return np.max(np.abs(g - ref) / scale)
+
+
+def test_adjoint_matches_gpu_finite_differences():
+    lat, beam, passes = _lattice(), _beam(), 6
+    k0 = get_parameters(lat)
+    with Tracker(0) as trk:
+        trk.load(beam)
+        loss, grad = trk.adjoint(lat, passes, PC, W)
+        trk.load(beam)
+        trk.track(lat, passes, PC)
+        assert abs(trk.objective(W) - loss) <= 1e-14 * abs(loss)
+        fd = np.zeros_like(k0)
+        for p in range(len(k0)):
+            h = 1e-7 * abs(k0[p])
+            vals = []
+            for sgn in (1, -1):
+                k = k0.copy()
+                k[p] += sgn * h
+                set_parameters(lat, k)
+                trk.load(beam)
+                trk.track(lat, passes, PC)
+                vals.append(trk.objective(W))
+            fd[p] = (vals[0] - vals[1]) / (2 * h)
+        set_parameters(lat, k0)
+    assert len(grad) == 8 and np.all(np.isfinite(grad))
+    assert _rel_err(grad, fd) < 1e-6, (grad, fd)
+
+
+@pytest.mark.skipif(not pyoracle.ref_available(), reason="oracle/_ref/libref.so not built")
+def test_adjoint_matches_reference_code_finite_differences():
+    """Central differences of elegant's own tracking (compiled from the
+    reference sources, CPU) on a smaller beam; three parameters sampled.
+    The step is 1e-5 relative here: the reference's CSBEND drift forms
+    X = rho0 (f - 1) + f X, which turns each rounding of cos() into ~rho0 *
+    2^-53 of x, so its loss function carries noise that swamps a 1e-7 step
+    (the GPU formulation has no such cancellation and takes h = 1e-7)."""
+    lat, beam, passes = _lattice(cells=1), _beam(n=300, seed=92), 4
+    k0 = get_parameters(lat)
+    with Tracker(0) as trk:
+        trk.load(beam)
+        _, grad = trk.adjoint(lat, passes, PC, W)
+    for p in (0, 1, 2):
+        h = 1e-5 * abs(k0[p])
+        vals = []
+        for sgn in (1, -1):
+            k = k0.copy()
+            k[p] += sgn * h
+            set_parameters(lat, k)
+            rows, _, _ = pyoracle.track_ref(lat, beam, passes, PC)
+            vals.append(_objective_rows(rows, W))
+        set_parameters(lat, k0)
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(grad[p] - fd) <= 1e-6 * max(abs(fd), 1e-3 * np.max(np.abs(grad))), (p, grad[p], fd)
+
+
+def test_torch_autograd_wrapper():
+    import torch
+    lat, beam, passes = _lattice(cells=1), _beam(n=500, seed=93), 3
+    fn, trk = make_autograd(lat, beam, passes, PC, W)
+    try:
+        k = torch.tensor(get_parameters(lat), dtype=torch.float64, requires_grad=True)
+        loss = fn.apply(k)
+        loss.backward()
+        trk.load(beam)
+        l2, g2 = trk.adjoint(lat, passes, PC, W)
+    finally:
+        trk.close()
+    # sums over particles and parameter sensitivities use atomic adds: equal to rounding
+    assert abs(loss.item() - l2) <= 1e-13 * abs(l2)
+    assert np.allclose(k.grad.numpy(), g2, rtol=1e-11, atol=1e-11 * np.max(np.abs(g2)))
+
+
+def test_losses_are_left_out_and_elements_checked():
+    lat = _lattice(cells=1)
+    lat.add("MAXAMP", "AP", X_MAX=0.002, Y_MAX=0.002)
+    lat.elements.insert(0, lat.elements.pop())
+    beam = _beam(n=1000, seed=94)
+    with Tracker(0) as trk:
+        trk.load(beam)
+        loss, grad = trk.adjoint(lat, 3, PC, W)
+        assert trk.count() < 1000 and np.all(np.isfinite(grad))
+        rf = configs.c2_lattice(cells=1, with_wake=False)
+        trk.load(beam)
+        with pytest.raises(Exception):
+            trk.adjoint(rf, 2, PC, W)
