@@ -203,15 +203,127 @@ def main():
     ap.add_argument("--particles", type=int, default=N_PARTICLES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--exact", action="store_true", help="parity build instead of the fast build")
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2"],
-                    help="c2: ring with RF and wake (the benchmark); c1: plain FODO ring (profiling)")
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4"],
+                    help="c2: ring with RF and wake (the benchmark); c1: plain FODO ring (profiling); "
+                         "c3: batched error-seed ensemble on dynamic-aperture grids; c4: adjoint gradient "
+                         "against finite differences")
+    ap.add_argument("--variants", type=int, default=256, help="c3: lattice variants")
+    ap.add_argument("--turns", type=int, default=None, help="c3: 1024, c4: 64 unless given")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "c3":
+        return run_ensemble(args, rank)
+    if args.workload == "c4":
+        return run_gradient(args, rank)
     return run_gpu(args, rank, world, local)
+
+
+def run_ensemble(args, rank):
+    """Batched ensemble: `variants` error seeds of the FODO+sextupole ring
+    (rms dK1/K1 = 1e-3, dK2/K2 = 2e-3, 25 mm circular aperture), each with a
+    dynamic-aperture grid of U{1000..65536} particles (x in +-20 mm, y in
+    0..10 mm, delta = 0), all turns in one trk_track_ensemble call
+    (graph-captured, autotuned launch shape).  Metric: particle-turns/s of
+    the whole ensemble."""
+    import torch
+    from elegant_b200 import Tracker, configs
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(0)
+    turns = args.turns or 1024
+    rng = np.random.Generator(np.random.Philox(3))
+    counts = rng.integers(1000, 65537, args.variants)
+    lats = [configs.c3_variant(seed=v) for v in range(args.variants)]
+    first, beams = 1, []
+    for n in counts:
+        beams.append(configs.da_grid(int(n), first_id=first))
+        first += int(n)
+    beam = np.concatenate(beams)
+    with Tracker(0) as trk:
+        trk.load(beam)
+        warm = trk.track_ensemble(lats, counts, 4, configs.P_CENTRAL)  # autotunes
+        trk.load(beam)
+        torch.cuda.synchronize()
+        with ClockSampler(0) as clocks:
+            t0 = time.perf_counter()
+            st = trk.track_ensemble(lats, counts, turns, configs.P_CENTRAL)
+            wall = time.perf_counter() - t0
+    value = st["particle_passes"] / (st["device_ms"] / 1e3)
+    line = {"metric": "particle-turns/s", "value": value, "unit": "particle-turns/s", "n_gpus": 1, "steps": turns,
+            "warmup": 4, "ms_per_step": st["device_ms"] / turns, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded error seeds, dynamic-aperture grids)",
+            "config": {"workload": "ensemble_c3", "variants": args.variants, "particles": int(counts.sum()),
+                       "turns": turns, "aperture_m": 0.025, "survivors": st["n_left"]},
+            "build": "fast", "wall_s": wall, "launch_shape": st["variant"], "tuned_by": "autotuner",
+            "gpu_launches": st["kernel_launches"], "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_gradient(args, rank):
+    """Gradient of mean(x^2 + y^2) + (mean x)^2 + (mean y)^2 after `turns`
+    turns of 1e5 particles (the FODO configuration's Gaussian beam) on the
+    FODO+sextupole ring (RF and wake off) with
+    respect to all 80 KQUAD K1 and 80 KSEXT K2: the reverse-mode adjoint
+    against central finite differences (h = 1e-7 relative) with the same
+    GPU tracking.  Metric: finite-difference time over adjoint time."""
+    import torch
+    from elegant_b200 import Tracker, configs
+    from elegant_b200.adjoint import get_parameters, set_parameters
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(0)
+    turns = args.turns or 64
+    n = min(args.particles, 100_000)
+    lat = configs.c2_lattice(with_rf=False, with_wake=False)
+    beam = configs.gaussian_beam(n, seed=5)  # the FODO configuration's beam (x, y 100 um; x', y' 10 urad)
+    w = 1.0
+    k0 = get_parameters(lat)
+    with Tracker(0) as trk:
+        for _ in range(max(args.warmup, 1)):
+            trk.load(beam)
+            trk.adjoint(lat, turns, configs.P_CENTRAL, w)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        trk.load(beam)
+        loss, grad = trk.adjoint(lat, turns, configs.P_CENTRAL, w)
+        torch.cuda.synchronize()
+        t_adj = time.perf_counter() - t0
+        fd = np.zeros_like(k0)
+        t0 = time.perf_counter()
+        for p in range(len(k0)):
+            h = 1e-7 * abs(k0[p])
+            vals = []
+            for sgn in (1, -1):
+                k = k0.copy()
+                k[p] += sgn * h
+                set_parameters(lat, k)
+                trk.load(beam)
+                trk.track(lat, turns, configs.P_CENTRAL)
+                vals.append(trk.objective(w))
+            fd[p] = (vals[0] - vals[1]) / (2 * h)
+        torch.cuda.synchronize()
+        t_fd = time.perf_counter() - t0
+        set_parameters(lat, k0)
+    # norm-wise (largest difference over the largest component) and
+    # component-wise with a floor at 1e-3 of the largest component
+    err = float(np.max(np.abs(grad - fd)) / np.max(np.abs(fd)))
+    scale = np.maximum(np.abs(fd), 1e-3 * np.max(np.abs(fd)))
+    err_c = float(np.max(np.abs(grad - fd) / scale))
+    line = {"metric": "adjoint gradient speed-up over GPU finite differences", "value": t_fd / t_adj,
+            "unit": "x", "n_gpus": 1, "steps": 1, "warmup": max(args.warmup, 1), "ms_per_step": t_adj * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Gaussian beam)",
+            "config": {"workload": "gradient_c4", "particles": n, "turns": turns, "parameters": int(len(k0)),
+                       "centroid_weight": w, "fd_step_relative": 1e-7},
+            "adjoint_s": t_adj, "finite_difference_s": t_fd, "loss": loss,
+            "relative_gradient_error_vs_fd": err, "max_componentwise_relative_error_vs_fd": err_c, "build": "fast"}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def run_gpu(args, rank, world, local):
