@@ -250,6 +250,10 @@ __device__ __forceinline__ int mult_body_fast(const double *__restrict__ d, int 
                                               double &xp, double &y, double &yp, double &s, double &qx, double &qy,
                                               const double dp, int &done) {
   const double opd2 = (1 + dp) * (1 + dp);
+  /* path-length factor sqrt(1 + xp^2 + yp^2): once from the entry slopes,
+   * then (1+delta) / sqrt((1+delta)^2 - qx^2 - qy^2) from each slope update,
+   * which is the same quantity without another square root */
+  double sf = sqrt_fast(fma(yp, yp, fma(xp, xp, 1.0)));
   done = 0;
   for (int i_kick = 0; i_kick < n_parts; i_kick++) {
     if (ap && !check_aperture(x + mdx, y + mdy, ap, aptilt, apc, aps))
@@ -259,7 +263,7 @@ __device__ __forceinline__ int mult_body_fast(const double *__restrict__ d, int 
       const double dsh = __ldg(&d[MD_DSH + step]);
       x = fma(xp, dsh, x);
       y = fma(yp, dsh, y);
-      s = fma(dsh, sqrt_fast(fma(yp, yp, fma(xp, xp, 1.0))), s);
+      s = fma(dsh, sf, s);
       done++;
       if (step == 3)
         break;
@@ -281,6 +285,7 @@ __device__ __forceinline__ int mult_body_fast(const double *__restrict__ d, int 
       const double r = rsqrt_fast(den);
       xp = qx * r;
       yp = qy * r;
+      sf = (1 + dp) * r;
     }
   }
   if (ap && !check_aperture(x + mdx, y + mdy, ap, aptilt, apc, aps))
