@@ -20,6 +20,9 @@ roofline: FP64 bound; achieved = algorithmic FP64 flops per particle-turn
         sources (oracle/_ref/libref.so; the oracle restatement where that
         was not built) on all host cores, process-parallel by particle
         shards.
+--workload c5: the large ring (40 multi-bend-achromat cells of combined-
+        function CSBENDs, KQUADs, KSEXTs and KOCTs, with RFCA, WAKE and
+        TRWAKE on 4000 bins), 1e7 particles, same metric and keys.
 Multi-GPU: one process per GPU; each rank tracks its own particle shard of
 1e6 particles (weak scaling); the library's NCCL communicator exchanges the
 beam time statistics (all-gather) and the wake histogram (all-reduce) at the
@@ -40,17 +43,41 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_PARTICLES = 1_000_000
-WORKLOAD = "ring_rf_wake_fodo40_1e6"
 # DRAM bytes per particle of one tracking-kernel launch: 10.63 MB read + 1.8 KB
 # written at 2e5 particles (ncu; the coordinate writes stay in L2 and are
 # written back during later kernels)
 TRACK_DRAM_BYTES_PER_PARTICLE = 10.628e6 / 2e5
 
+WORKLOADS = {
+    "c1": {"workload": "ring_fodo40_1e6", "particles": 1_000_000,
+           "lattice": "40 FODO cells (KQUAD, CSBEND, DRIF)"},
+    "c2": {"workload": "ring_rf_wake_fodo40_1e6", "particles": 1_000_000,
+           "lattice": "40 FODO cells + KSEXT, RFCA, WAKE", "wake_bins": 2000, "wake_points": 4096,
+           "wake_dt_s": 5e-14, "charge_c": 1e-9},
+    "c5": {"workload": "mba_ring_rf_wake_trwake_1e7", "particles": 10_000_000,
+           "lattice": "40 MBA cells (7 CSBEND K1 N_KICKS=32, 12 KQUAD, 6 KSEXT, 2 KOCT, 27 DRIF) + RFCA, WAKE, "
+                      "TRWAKE", "wake_bins": 4000, "wake_points": 4096, "wake_dt_s": 2.5e-13, "charge_c": 1e-9,
+           "sigma_x_m": 30e-6},
+}
 
-def workload_config(n_particles):
-    return {"workload": WORKLOAD, "particles_per_gpu": n_particles, "lattice": "40 FODO cells + KSEXT, RFCA, WAKE",
-            "wake_bins": 2000, "wake_points": 4096, "wake_dt_s": 5e-14, "charge_c": 1e-9, "p_central": 13700.0,
-            "l2": "flushed between timed steps"}
+
+def workload_config(n_particles, workload="c2"):
+    cfg = dict(WORKLOADS[workload])
+    del cfg["particles"]
+    cfg.update({"particles_per_gpu": n_particles, "p_central": 13700.0, "l2": "flushed between timed steps"})
+    return cfg
+
+
+def workload_lattice(workload):
+    from elegant_b200 import configs
+    return {"c1": configs.c1_lattice, "c2": configs.c2_lattice, "c5": configs.c5_lattice}[workload]()
+
+
+def workload_beam(workload, n, seed=1, first_id=1):
+    from elegant_b200 import configs
+    if workload == "c5":
+        return configs.c5_beam(n, seed=seed, first_id=first_id)
+    return configs.gaussian_beam(n, seed=seed, first_id=first_id)
 
 
 def load_flops():
@@ -121,18 +148,17 @@ def _cpu_tracker():
     return pyoracle.track, "port"
 
 
-def cpu_baseline(cores=None, sample_particles=6000, sample_turns=3):
+def cpu_baseline(cores=None, sample_particles=6000, sample_turns=3, workload="c2"):
     """Time the CPU tracking path on the host: particle-turns/s on a bounded
     sample of the benchmark ring (same lattice, same beam distribution)."""
-    from elegant_b200 import configs
     if cores is None:
         cores = 1
     if cores == 1:
         track, kind = _cpu_tracker()
-        lat = configs.c2_lattice()
-        beam = configs.gaussian_beam(sample_particles, seed=1)
+        lat = workload_lattice(workload)
+        beam = workload_beam(workload, sample_particles, seed=1)
         t0 = time.perf_counter()
-        _, _, eff = track(lat, beam, sample_turns, configs.P_CENTRAL)
+        _, _, eff = track(lat, beam, sample_turns, 13700.0)
         dt = time.perf_counter() - t0
         return {"value": eff / dt, "unit": "particle-turns/s", "cores": 1, "kind": kind,
                 "sample": f"{sample_particles} particles x {sample_turns} turns of the same lattice, 1 core"}
@@ -140,8 +166,8 @@ def cpu_baseline(cores=None, sample_particles=6000, sample_turns=3):
     ctx = mp.get_context("spawn")
     per = sample_particles
     with ctx.Pool(cores) as pool:
-        args = [(per, sample_turns, 1 + k) for k in range(cores)]
-        kinds = pool.map(_oracle_shard, [(10, 1, 99)] * cores)  # warm the workers
+        args = [(per, sample_turns, 1 + k, workload) for k in range(cores)]
+        kinds = pool.map(_oracle_shard, [(10, 1, 99, workload)] * cores)  # warm the workers
         t0 = time.perf_counter()
         effs = pool.map(_oracle_shard, args)
         dt = time.perf_counter() - t0
@@ -151,13 +177,12 @@ def cpu_baseline(cores=None, sample_particles=6000, sample_turns=3):
 
 
 def _oracle_shard(args):
-    n, turns, seed = args
+    n, turns, seed, workload = args
     sys.path.insert(0, ROOT)
-    from elegant_b200 import configs
     track, kind = _cpu_tracker()
-    lat = configs.c2_lattice()
-    beam = configs.gaussian_beam(n, seed=seed)
-    _, _, eff = track(lat, beam, turns, configs.P_CENTRAL)
+    lat = workload_lattice(workload)
+    beam = workload_beam(workload, n, seed=seed)
+    _, _, eff = track(lat, beam, turns, 13700.0)
     return eff, kind
 
 
@@ -169,13 +194,14 @@ def run_reference(args, rank, world):
         return 0
     import multiprocessing as mp
     cores = os.cpu_count() or 1
-    per, turns = 1000, 1
+    workload = args.workload if args.workload in ("c1", "c5") else "c2"
+    per, turns = (100 if workload == "c5" else 1000), 1
     steps = []
     with mp.get_context("spawn").Pool(cores) as pool:
-        kind = pool.map(_oracle_shard, [(10, 1, 99)] * cores)[0][1]
+        kind = pool.map(_oracle_shard, [(10, 1, 99, workload)] * cores)[0][1]
         for k in range(args.warmup + args.steps):
             t0 = time.perf_counter()
-            effs = pool.map(_oracle_shard, [(per, turns, 1 + c) for c in range(cores)])
+            effs = pool.map(_oracle_shard, [(per, turns, 1 + c, workload) for c in range(cores)])
             dt = time.perf_counter() - t0
             if k >= args.warmup:
                 steps.append(sum(e for e, _ in effs) / dt)
@@ -186,7 +212,7 @@ def run_reference(args, rank, world):
     line = {"metric": "particle-turns/s", "value": v, "unit": "particle-turns/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian beam)",
-            "config": workload_config(N_PARTICLES), "impl": "reference",
+            "config": workload_config(WORKLOADS[workload]["particles"], workload), "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "particle-turns/s", "cores": cores, "kind": steps[0]["kind"],
                              "sample": steps[0]["sample"]},
             "e2e": {"value": v, "unit": "particle-turns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -200,11 +226,13 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--particles", type=int, default=N_PARTICLES)
+    ap.add_argument("--particles", type=int, default=None,
+                    help="particles per GPU (1e6 for c1/c2, 1e7 for c5, 1e5 for c4)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--exact", action="store_true", help="parity build instead of the fast build")
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4"],
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c2: ring with RF and wake (the benchmark); c1: plain FODO ring (profiling); "
+                         "c5: large MBA ring with RF, WAKE and TRWAKE, 1e7 particles; "
                          "c3: batched error-seed ensemble on dynamic-aperture grids; c4: adjoint gradient "
                          "against finite differences")
     ap.add_argument("--variants", type=int, default=256, help="c3: lattice variants")
@@ -278,7 +306,7 @@ def run_gradient(args, rank):
         return 0
     torch.cuda.set_device(0)
     turns = args.turns or 64
-    n = min(args.particles, 100_000)
+    n = min(args.particles or 100_000, 100_000)
     lat = configs.c2_lattice(with_rf=False, with_wake=False)
     beam = configs.gaussian_beam(n, seed=5)  # the FODO configuration's beam (x, y 100 um; x', y' 10 urad)
     w = 1.0
@@ -334,9 +362,9 @@ def run_gpu(args, rank, world, local):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    n = args.particles
-    lat = configs.c2_lattice() if args.workload == "c2" else configs.c1_lattice()
-    beam = configs.gaussian_beam(n, seed=1 + rank, first_id=1 + rank * n)
+    n = args.particles or WORKLOADS[args.workload]["particles"]
+    lat = workload_lattice(args.workload)
+    beam = workload_beam(args.workload, n, seed=1 + rank, first_id=1 + rank * n)
     fast = not args.exact
     flops = load_flops()
     with Tracker(local) as trk:
@@ -410,14 +438,15 @@ def run_gpu(args, rank, world, local):
     roof = None
     if flops and track_launches:
         fpt = flops["flops_per_particle_turn"][args.workload]
-        if args.workload == "c2":
-            fpt -= flops["per_particle"]["WAKE"]["total"]  # the wake's per-particle work runs in the wake kernels
+        # the wakes' per-particle work runs in the wake kernels
+        fpt -= {"c1": 0, "c2": 1, "c5": 2}[args.workload] * flops["per_particle"]["WAKE"]["total"]
         per_launch_flops = fpt * (effort / world) / track_launches
         avg_launch_s = track_ms / track_launches / 1e3
         achieved = per_launch_flops / avg_launch_s / 1e12
         roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak if peak else None,
-                "traffic": TRACK_DRAM_BYTES_PER_PARTICLE * (effort / world) / track_launches,
+                "traffic": (TRACK_DRAM_BYTES_PER_PARTICLE * (effort / world) / track_launches
+                            if args.workload == "c2" else None),
                 "flops_per_particle_turn": fpt, "kernel": "track_kernel", "launches": track_launches,
                 "avg_launch_ms": avg_launch_s * 1e3,
                 "peak_source": "FP64 FMA peak measured in this run (independent dependent-FMA chains); "
@@ -426,11 +455,12 @@ def run_gpu(args, rank, world, local):
                                   "particles, scaled by particles (profiles/track_kernel_ring_rf_wake.md)"}
     cpu = None
     if not args.no_cpu_baseline and world == 1:
-        cpu = cpu_baseline(cores=1)
+        cpu = (cpu_baseline(cores=1, sample_particles=1500, sample_turns=2, workload="c5") if args.workload == "c5"
+               else cpu_baseline(cores=1, workload=args.workload))
     line = {"metric": "particle-turns/s", "value": value, "unit": "particle-turns/s", "n_gpus": world,
             "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": dev_s * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded Gaussian beam, seeded resonator wake)", "config": workload_config(n),
+            "data": "synthetic (seeded Gaussian beam, seeded resonator wake)", "config": workload_config(n, args.workload),
             "build": "fast" if fast else "parity", "wall_s": wall,
             "e2e": {"value": e2e_value, "unit": "particle-turns/s", "h2d_bytes_per_step": int(n * 7 * 8),
                     "d2h_bytes_per_step": int(n * 7 * 8)},
