@@ -1366,7 +1366,7 @@ int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int
         if (op.ap_in[k] >= 0)
           op.ap_in[k] += apo;
       }
-      if (op.kind == OPK_BEND || op.kind == OPK_DIPOLE)
+      if (op.kind == OPK_BEND || op.kind == OPK_DIPOLE || op.kind == OPK_CFBEND)
         op.i[4] += fo;
       all.ops.push_back(op);
     }

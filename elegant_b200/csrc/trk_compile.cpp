@@ -828,12 +828,15 @@ int trk_compile(const trk_lattice *l, double Po, CompiledLattice &out) {
                            (op.i[5] == EDGE_LIN1 && op.d[BD_TE1] == 0 && op.d[BD_PSI1] == 0 && op.d[BD_LIM1] <= 0);
       const bool e2_noop = op.i[6] == EDGE_NONE ||
                            (op.i[6] == EDGE_LIN1 && op.d[BD_TE2] == 0 && op.d[BD_PSI2] == 0 && op.d[BD_LIM2] <= 0);
-      if (op.i[2] == 0 && op.i[1] == 4 && !(op.i[7] & BF_MISALIGN) && e1_noop && e2_noop)
+      const bool plain = op.i[1] == 4 && !(op.i[7] & (BF_MISALIGN | BF_APTILT)) && e1_noop && e2_noop;
+      if (plain && op.i[2] == 0)
         op.kind = OPK_DIPOLE;
+      else if (plain && op.i[2] == 1 && op.i[3] == 5)
+        op.kind = OPK_CFBEND;
     }
     if (op.kind != OPK_NOP && op.kind != OPK_DRIFT && op.kind != OPK_EDRIFT && op.kind != OPK_RFDRIFT &&
-        op.kind != OPK_MULT1 && op.kind != OPK_DIPOLE && op.kind != OPK_RF && op.kind != OPK_WAKE &&
-        op.kind != OPK_TRWAKE)
+        op.kind != OPK_MULT1 && op.kind != OPK_DIPOLE && op.kind != OPK_CFBEND && op.kind != OPK_RF &&
+        op.kind != OPK_WAKE && op.kind != OPK_TRWAKE)
       out.lean = false;
     if (e->type == TRK_MAXAMP)
       cur_maxamp = i;
@@ -848,7 +851,8 @@ int trk_compile(const trk_lattice *l, double Po, CompiledLattice &out) {
       const trk_aperture &a = out.aps[ap_of_elem[m]];
       bool active = a.x_max > 0 || a.y_max > 0;
       /* in-element checks (checkMultAperture) only matter with a positive limit */
-      if (active && (op.kind == OPK_MULT || op.kind == OPK_BEND || op.kind == OPK_MULT1 || op.kind == OPK_DIPOLE))
+      if (active && (op.kind == OPK_MULT || op.kind == OPK_BEND || op.kind == OPK_MULT1 || op.kind == OPK_DIPOLE ||
+                     op.kind == OPK_CFBEND))
         op.ap_in[v] = ap_of_elem[m];
       /* after-element limit if (x_max || y_max) (src/do_tracking.c:2508) */
       if (a.x_max || a.y_max)

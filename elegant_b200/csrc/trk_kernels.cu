@@ -609,6 +609,124 @@ __device__ __forceinline__ bool bend_dipole_fast(const double *__restrict__ d, i
   dist = opd * F;
   return ok;
 }
+
+/* Body of a combined-function CSBEND in the fast build: a normal-only field
+ * expansion of order 4 (K1 and/or K2; expansionOrder1 = 5).  The drift is
+ * the pure dipole's, with f^2 = (1+delta)^2 - QY^2 re-formed every substep
+ * because the kicks now change QY, and Y and the path length advanced by
+ * their own terms.  The field is computeCSBENDFields (src/csbend.c:99-172)
+ * regrouped by powers of y and evaluated in Horner form in x:
+ *   Fy = P0(x) + y^2 (P2(x) + y^2 P4),   Fx = y (Q1(x) + y^2 Q3(x)),
+ * with Pj, Qj the table columns j (terms i + j <= 4). */
+#define CF_T(T, i, j) __ldg(&(T)[(i) * 11 + (j)])
+__device__ __forceinline__ void cf_fields(const double *__restrict__ Fx_xy, const double *__restrict__ Fy_xy,
+                                          double x, double y, double &Fx, double &Fy) {
+  const double y2 = y * y;
+  const double p0 = fma(fma(fma(fma(CF_T(Fy_xy, 4, 0), x, CF_T(Fy_xy, 3, 0)), x, CF_T(Fy_xy, 2, 0)), x,
+                            CF_T(Fy_xy, 1, 0)),
+                        x, CF_T(Fy_xy, 0, 0));
+  const double p2 = fma(fma(CF_T(Fy_xy, 2, 2), x, CF_T(Fy_xy, 1, 2)), x, CF_T(Fy_xy, 0, 2));
+  Fy = fma(y2, fma(y2, CF_T(Fy_xy, 0, 4), p2), p0);
+  const double q1 = fma(fma(fma(CF_T(Fx_xy, 3, 1), x, CF_T(Fx_xy, 2, 1)), x, CF_T(Fx_xy, 1, 1)), x,
+                        CF_T(Fx_xy, 0, 1));
+  const double q3 = fma(CF_T(Fx_xy, 1, 3), x, CF_T(Fx_xy, 0, 3));
+  Fx = y * fma(y2, q3, q1);
+}
+#undef CF_T
+
+/* One slice (4 drift substeps, 3 kicks); `checked` as in dipole_slice. */
+template <bool CHECKED>
+__device__ __forceinline__ bool cf_slice(const double *__restrict__ d, const double *__restrict__ fxy, double rho0,
+                                         double opd, double &X, double &QX, double &Y, double &QY, double &dist,
+                                         int &done) {
+  const double opd2 = opd * opd;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const double f2 = fma(-QY, QY, opd2);
+    if (CHECKED && !(f2 > 0))
+      return false;
+    const double u2 = fma(-QX, QX, f2);
+    if (CHECKED && !(u2 >= 0)) /* |sin(phi)| = |QX/f| > 1 */
+      return false;
+    const double fc = CHECKED ? sqrt_fast(u2) : sqrt_nan(u2);
+    const double sa = __ldg(&d[BD_SA + j]), ca = __ldg(&d[BD_CA + j]);
+    const double saq = sa * QX;
+    const double fcosi = fma(ca, fc, -saq);
+    if (CHECKED && fcosi == 0)
+      return false;
+    const double u = div_fast(rho0 + X, fcosi);
+    const double fac = u * sa;
+    QX = fma(sa, fc, ca * QX);
+    Y = fma(QY, fac, Y);
+    dist = fma(fac, opd, dist);
+    X = fma(u, fma(__ldg(&d[BD_OMC + j]), fc, saq), X);
+    if (CHECKED)
+      done++;
+    if (j == 3)
+      break;
+    double Fx, Fy;
+    cf_fields(fxy, fxy + 121, X, Y, Fx, Fy);
+    const double w = fma(__ldg(&d[BD_C2 + j]), X, __ldg(&d[BD_C1 + j]));
+    QX = fma(-w, Fy, QX);
+    QY = fma(w, Fx, QY);
+  }
+  return true;
+}
+
+struct CfState {
+  double X, QX, Y, QY, dist;
+  int done;
+  bool ok;
+};
+
+__device__ __noinline__ CfState cf_slice_redo(const double *__restrict__ d, const double *__restrict__ fxy,
+                                              double rho0, double opd, double X, double QX, double Y, double QY,
+                                              double dist, int done) {
+  CfState r;
+  r.ok = cf_slice<true>(d, fxy, rho0, opd, X, QX, Y, QY, dist, done);
+  r.X = X;
+  r.QX = QX;
+  r.Y = Y;
+  r.QY = QY;
+  r.dist = dist;
+  r.done = done;
+  return r;
+}
+
+__device__ __forceinline__ bool bend_cf_fast(const double *__restrict__ d, const double *__restrict__ fxy,
+                                             int nSlices, double rho0, const trk_aperture *ap, double &X, double &QX,
+                                             double &Y, double &QY, const double D, double &dist, int &done) {
+  const double opd = 1 + D;
+  bool ok = true;
+  dist = 0;
+  done = 0;
+  for (int i = 0; i < nSlices; i++) {
+    if (ap && !check_aperture(X, Y, ap, false, 1.0, 0.0)) {
+      ok = false;
+      break;
+    }
+    const double *dd = d;
+    asm volatile("" : "+l"(dd));
+    const double X0 = X, QX0 = QX, Y0 = Y, QY0 = QY, S0 = dist;
+    cf_slice<false>(dd, fxy, rho0, opd, X, QX, Y, QY, dist, done);
+    if (!isfinite(X + QX + Y + QY + dist)) {
+      const CfState r = cf_slice_redo(dd, fxy, rho0, opd, X0, QX0, Y0, QY0, S0, done);
+      X = r.X;
+      QX = r.QX;
+      Y = r.Y;
+      QY = r.QY;
+      dist = r.dist;
+      done = r.done;
+      if (!r.ok) {
+        ok = false;
+        break;
+      }
+      done -= 4;
+    }
+    done += 4;
+  }
+  return ok;
+}
 #endif
 
 /* apply_edge_effects (src/csbend.c:4291-4333) */
@@ -1110,6 +1228,44 @@ __device__ __forceinline__ bool op_dipole_fast(const trk_op *__restrict__ op, Pa
   return true;
 }
 
+/* OPK_CFBEND in the fast build: track_through_csbend for a combined-function
+ * dipole (normal field expansion of order 4) with no misalignment and no edge
+ * kick (src/csbend.c:654-1434), body by bend_cf_fast. */
+__device__ __forceinline__ bool op_cfbend_fast(const trk_op *__restrict__ op, Part &p, double Po, double z_start,
+                                               const trk_aperture *ap, const double *__restrict__ field) {
+  const double *d = op->d;
+  const int nSlices = __ldg(&op->i[0]);
+  const double *fxy = field + __ldg(&op->i[4]);
+  const double rho0 = __ldg(&d[BD_RHO0]);
+  const double D = p.dp;
+  const double r = (1 + D) * rsqrt_fast(fma(p.yp, p.yp, fma(p.xp, p.xp, 1.0)));
+  double X = p.x, Y = p.y, QX = p.xp * r, QY = p.yp * r;
+  double dist = 0;
+  int done = 0;
+  bool ok = bend_cf_fast(d, fxy, nSlices, rho0, ap, X, QX, Y, QY, D, dist, done);
+  double dz_lost = 0;
+  if (ok) {
+    dz_lost = nSlices * __ldg(&d[BD_SLICE]);
+    if (ap && !check_aperture(X, Y, ap, false, 1.0, 0.0))
+      ok = false;
+  } else
+    for (int k = 0; k < done; k++)
+      dz_lost += __ldg(&d[BD_DSH + (k & 3)]);
+  const double f = rsqrt_fast((1 + D) * (1 + D) - QX * QX - QY * QY);
+  p.x = X;
+  p.y = Y;
+  p.xp = QX * f;
+  p.yp = QY * f;
+  if (!ok) {
+    p.s = z_start + dz_lost;
+    p.dp = Po * (1 + D);
+    return false;
+  }
+  p.s += dist;
+  p.dp = D;
+  return true;
+}
+
 /* Two particles through one pure dipole with their substep chains
  * interleaved: the body of each particle is a serial dependency chain
  * (sqrt -> reciprocal -> update), so a thread that carries two independent
@@ -1493,6 +1649,13 @@ __device__ __forceinline__ bool track_particle(const TrackArgs &a, const trk_op 
         ok = op_bend(op, p, a.Po, h.z_start, ap_in, a.field);
 #endif
         break;
+      case OPK_CFBEND:
+#if TRK_FAST
+        ok = op_cfbend_fast(op, p, a.Po, h.z_start, ap_in, a.field);
+#else
+        ok = op_bend(op, p, a.Po, h.z_start, ap_in, a.field);
+#endif
+        break;
       case OPK_RF:
         ok = op_rf(op, p, a.Po, h.z_end, a.rf_phase);
         break;
@@ -1559,6 +1722,8 @@ __device__ __forceinline__ bool lean_op(const TrackArgs &a, const trk_op *__rest
     return op_mult1_fast(op, p, a.Po, z_start, ap_in);
   case OPK_DIPOLE:
     return op_dipole_fast(op, p, a.Po, z_start, ap_in);
+  case OPK_CFBEND:
+    return op_cfbend_fast(op, p, a.Po, z_start, ap_in, a.field);
   case OPK_RF:
     return op_rf(op, p, a.Po, h.z_end, a.rf_phase);
   default:

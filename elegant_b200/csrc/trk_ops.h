@@ -29,8 +29,10 @@ enum trk_op_kind {
   OPK_RFDRIFT = 8, /* RFCA with VOLT=0: drift of length L */
   OPK_MULT1 = 9,   /* KQUAD/KSEXT/KOCT with one normal multipole, 4th-order integrator, no
                       misalignment, steering or end drifts (specialized fast-build body) */
-  OPK_DIPOLE = 10  /* CSBEND: pure dipole, 4th-order integrator, no misalignment, edge kicks
+  OPK_DIPOLE = 10, /* CSBEND: pure dipole, 4th-order integrator, no misalignment, edge kicks
                       that are exact no-ops (E=0, no fringe) or absent (specialized fast-build body) */
+  OPK_CFBEND = 11  /* CSBEND: combined function (normal field expansion of order 4: K1 and/or K2),
+                      otherwise as OPK_DIPOLE (specialized fast-build body) */
 };
 
 /* multipole flags (i[6]) */
