@@ -230,13 +230,14 @@ def main():
                     help="particles per GPU (1e6 for c1/c2, 1e7 for c5, 1e5 for c4)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--exact", action="store_true", help="parity build instead of the fast build")
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "c5grad"],
                     help="c2: ring with RF and wake (the benchmark); c1: plain FODO ring (profiling); "
-                         "c5: large MBA ring with RF, WAKE and TRWAKE, 1e7 particles; "
+                         "c5: large MBA ring with RF, WAKE and TRWAKE, 1e7 particles; c5grad: batched "
+                         "adjoint over 32 error seeds of the MBA ring against finite differences; "
                          "c3: batched error-seed ensemble on dynamic-aperture grids; c4: adjoint gradient "
                          "against finite differences")
     ap.add_argument("--variants", type=int, default=256, help="c3: lattice variants")
-    ap.add_argument("--turns", type=int, default=None, help="c3: 1024, c4: 64 unless given")
+    ap.add_argument("--turns", type=int, default=None, help="c3: 1024, c4: 64, c5grad: 8 unless given")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -247,6 +248,8 @@ def main():
         return run_ensemble(args, rank)
     if args.workload == "c4":
         return run_gradient(args, rank)
+    if args.workload == "c5grad":
+        return run_gradient_ensemble(args, rank)
     return run_gpu(args, rank, world, local)
 
 
@@ -350,6 +353,126 @@ def run_gradient(args, rank):
                        "centroid_weight": w, "fd_step_relative": 1e-7},
             "adjoint_s": t_adj, "finite_difference_s": t_fd, "loss": loss,
             "relative_gradient_error_vs_fd": err, "max_componentwise_relative_error_vs_fd": err_c, "build": "fast"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_gradient_ensemble(args, rank):
+    """Batched gradients on the large ring: 32 error seeds of the MBA ring
+    (RF and wakes off; seeded rms dK1/K1 = 1e-3 on every KQUAD, dK2/K2 =
+    2e-3 on every KSEXT), 1e5 particles split over the seeds, `turns` turns
+    (8 by default: over more turns a few particles of this seeded ring,
+    near the edge of its momentum acceptance, grow their sensitivities
+    exponentially, so the loss gradient is dominated by them and central
+    differences no longer resolve it); per seed the gradient of
+    mean(x^2 + y^2) + (mean x)^2 + (mean y)^2 with respect to its 480 K1 and
+    240 K2, all seeds in one trk_adjoint_ensemble call.  Finite differences
+    (h = 1e-7 relative; every seed perturbed at once, one trk_track_ensemble
+    run per sign, parameters updated in place with trk_lattice_set) are run
+    for a sample of the parameters and their time scaled to all 720 by the
+    parameter count (the cost is the same per parameter).  Metric: that
+    finite-difference time over the adjoint time."""
+    import ctypes
+
+    import torch
+    from elegant_b200 import Tracker, configs
+    from elegant_b200 import _Run, _Stats, _check
+    from elegant_b200.adjoint import PARAM_NAME, get_parameters, parameter_elements
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(0)
+    turns = args.turns or 8
+    seeds = 32
+    n = args.particles or 100_000
+    counts = np.full(seeds, n // seeds, dtype=np.int64)
+    counts[: n % seeds] += 1
+    lats, beams, first = [], [], 1
+    for v in range(seeds):
+        rng = np.random.Generator(np.random.Philox(1000 + v))
+        lats.append(configs.c5_lattice(with_rf=False, with_wake=False, kq_errors=rng.normal(0, 1e-3, (40, 12)),
+                                       k2_errors=rng.normal(0, 2e-3, (40, 6))))
+        beams.append(configs.c5_beam(int(counts[v]), seed=2000 + v, first_id=first))
+        first += int(counts[v])
+    beam = np.concatenate(beams)
+    bounds = np.concatenate([[0], np.cumsum(counts)])
+    offs = bounds.astype(np.int64)
+    w = 1.0
+    k0 = [get_parameters(lat) for lat in lats]
+    pidx = parameter_elements(lats[0])
+    n_par = len(k0[0])
+    sample = np.unique(np.linspace(0, n_par - 1, 24).astype(int))
+
+    def losses_from_store(trk):
+        nl, out, lp, le = trk.store(stride=7, with_loss=True)
+        ids = out[:, 6].astype(np.int64) - 1
+        alive = lp < 0
+        res = np.zeros(seeds)
+        for v in range(seeds):
+            m = alive & (ids >= bounds[v]) & (ids < bounds[v + 1])
+            x, y = out[m, 0], out[m, 2]
+            res[v] = np.mean(x * x + y * y) + w * (np.mean(x) ** 2 + np.mean(y) ** 2)
+        return res
+
+    with Tracker(0) as trk:
+        for _ in range(max(args.warmup, 1)):
+            trk.load(beam)
+            trk.adjoint_ensemble(lats, counts, turns, configs.P_CENTRAL, w)
+        torch.cuda.synchronize()
+        with ClockSampler(0) as clocks:
+            t0 = time.perf_counter()
+            trk.load(beam)
+            loss, grad = trk.adjoint_ensemble(lats, counts, turns, configs.P_CENTRAL, w)
+            torch.cuda.synchronize()
+            t_adj = time.perf_counter() - t0
+        # finite differences through the C ABI: native lattices built once,
+        # the perturbed parameter set in place
+        lib = trk.lib
+        nats = [trk.native(lat) for lat in lats]
+        arr = (ctypes.c_void_p * seeds)(*[nt.ptr.value for nt in nats])
+        run = _Run()
+        lib.trk_run_defaults(ctypes.byref(run))
+        run.p_central = configs.P_CENTRAL
+        run.n_passes = turns
+        st = _Stats()
+        fd = np.zeros((seeds, len(sample)))
+        dev_ms = 0.0
+        t0 = time.perf_counter()
+        for j, p in enumerate(sample):
+            e = pidx[p]
+            name = PARAM_NAME[lats[0].elements[e][0]].encode()
+            vals = []
+            for sgn in (1, -1):
+                for v in range(seeds):
+                    _check(lib, lib.trk_lattice_set(nats[v].ptr, e, name, k0[v][p] + sgn * 1e-7 * abs(k0[v][p])))
+                trk.load(beam)
+                _check(lib, lib.trk_track_ensemble(trk.ctx, arr, seeds,
+                                                   offs.ctypes.data_as(ctypes.POINTER(ctypes.c_long)),
+                                                   ctypes.byref(run), ctypes.byref(st)))
+                dev_ms += st.device_ms
+                vals.append(losses_from_store(trk))
+            for v in range(seeds):
+                _check(lib, lib.trk_lattice_set(nats[v].ptr, e, name, k0[v][p]))
+                fd[v, j] = (vals[0][v] - vals[1][v]) / (2 * 1e-7 * abs(k0[v][p]))
+        torch.cuda.synchronize()
+        t_fd_sample = time.perf_counter() - t0
+    scale = n_par / len(sample)
+    t_fd = t_fd_sample * scale
+    g = grad[:, sample]
+    err = float(np.max(np.abs(g - fd)) / np.max(np.abs(fd)))
+    line = {"metric": "adjoint gradient speed-up over GPU finite differences", "value": t_fd / t_adj,
+            "unit": "x", "n_gpus": 1, "steps": 1, "warmup": max(args.warmup, 1), "ms_per_step": t_adj * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded error seeds, seeded Gaussian beam)",
+            "config": {"workload": "gradient_ensemble_c5", "seeds": seeds, "particles": int(n), "turns": turns,
+                       "parameters_per_seed": n_par, "centroid_weight": w, "fd_step_relative": 1e-7,
+                       "fd_parameters_timed": int(len(sample))},
+            "adjoint_s": t_adj, "finite_difference_s": t_fd,
+            "finite_difference_device_s": dev_ms / 1e3 * scale,
+            "finite_difference_s_note": f"{len(sample)} parameters timed ({t_fd_sample:.2f} s wall), scaled by "
+                                        f"{n_par}/{len(sample)}; the device figure is the tracking kernels' time "
+                                        "alone",
+            "loss_mean": float(np.mean(loss)),
+            "relative_gradient_error_vs_fd": err, "clocks": clocks.summary(), "build": "fast"}
     print(json.dumps(line), flush=True)
     return 0
 

@@ -93,6 +93,7 @@ def _declare(lib):
         "trk_track_ensemble": (I, [P, ctypes.POINTER(P), I, ctypes.POINTER(L), ctypes.POINTER(_Run),
                                    ctypes.POINTER(_Stats)]),
         "trk_adjoint": (I, [P, P, ctypes.POINTER(_Run), D, DP, DP, I]),
+        "trk_adjoint_ensemble": (I, [P, ctypes.POINTER(P), I, ctypes.POINTER(L), ctypes.POINTER(_Run), D, DP, DP, I]),
         "trk_adjoint_param_count": (I, [P]),
         "trk_objective": (I, [P, D, DP]),
     }
@@ -309,6 +310,29 @@ class Tracker:
         _check(self.lib, self.lib.trk_adjoint(self.ctx, nat.ptr, ctypes.byref(run), centroid_weight, ctypes.byref(loss),
                                               _dptr(g) if with_grad else None, n))
         return loss.value, g[:n]
+
+    def adjoint_ensemble(self, lattices, counts, n_passes, p_central, centroid_weight=0.0, pass_offset=0,
+                         with_grad=True):
+        """The batched adjoint: the loaded beam tracked as len(lattices)
+        variants (variant v owns the next counts[v] particles) and, per
+        variant, (loss over its survivors, gradient with respect to its KQUAD
+        K1 and KSEXT K2 values).  Returns (losses[V], gradients[V, P])."""
+        nats = [self.native(lat) for lat in lattices]
+        arr = (ctypes.c_void_p * len(nats))(*[n.ptr.value for n in nats])
+        offs = np.concatenate([[0], np.cumsum(np.asarray(counts, dtype=np.int64))]).astype(np.int64)
+        n = _check(self.lib, self.lib.trk_adjoint_param_count(nats[0].ptr))
+        run = _Run()
+        self.lib.trk_run_defaults(ctypes.byref(run))
+        run.p_central = p_central
+        run.n_passes = n_passes
+        run.pass_offset = pass_offset
+        V = len(nats)
+        loss = np.zeros(V)
+        g = np.zeros(max(n * V, 1))
+        _check(self.lib, self.lib.trk_adjoint_ensemble(
+            self.ctx, arr, V, offs.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), ctypes.byref(run),
+            centroid_weight, _dptr(loss), _dptr(g) if with_grad else None, n * V))
+        return loss, g[:n * V].reshape(V, n)
 
     def objective(self, centroid_weight=0.0):
         """The adjoint's loss function on the device beam as it is."""

@@ -951,9 +951,7 @@ int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, 
   if (variant < 0 || variant >= TRK_N_VARIANTS)
     variant = ctx->tuned_variant;
   if (variant < 0)
-    /* measured on B200: (128 threads, 6 blocks/SM) for lean lattices in the
-     * fast build (80 registers), (128, 4) otherwise */
-    variant = (fast && c.lean) ? 7 : 1;
+    variant = trk_default_variant(fast, c);
   CUDA_TRY(cudaEventRecord(ctx->ev0, ctx->stream));
   if (ctx->np > 0 && run->n_passes > 0 && fresh >= 0) {
     screen_kernel<<<(int)((ctx->np + 255) / 256), 256, 0, ctx->stream>>>(
@@ -1138,7 +1136,7 @@ int trk_track_element(trk_context *ctx, const trk_lattice *lattice, int element,
   const bool fast = run->fast_math != 0;
   int variant = run->variant;
   if (variant < 0 || variant >= TRK_N_VARIANTS)
-    variant = (fast && c.lean) ? 7 : 1;
+    variant = trk_default_variant(fast, c);
   ctx->last_launches = 0;
   if (k >= 0 && (ctx->np > 0 || ctx->comm)) {
     const trk_op &op = c.ops[k];
@@ -1318,12 +1316,14 @@ static int beam_snapshot(trk_context *ctx, bool save) {
   return TRK_OK;
 }
 
-int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int n_variants, const long *offsets,
-                       const trk_run *run, trk_stats *stats) {
-  if (!ctx || !lattices || !offsets || !run || n_variants < 1)
+/* Checks an ensemble (same element types in every variant, no collective
+ * elements, offsets from 0 to the loaded particle count), compiles every
+ * variant and uploads the concatenated records and the variant offsets.
+ * Sets *nops_out to the records per variant and *lean_out. */
+static int prepare_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int n_variants, const long *offsets,
+                            double Po, int *nops_out, bool *lean_out) {
+  if (!ctx || !lattices || !offsets || n_variants < 1)
     return trk_set_error(TRK_ERR_ARG, "bad ensemble arguments");
-  if (run->n_passes < 0)
-    return trk_set_error(TRK_ERR_ARG, "negative pass count");
   if (offsets[0] != 0 || offsets[n_variants] != ctx->np)
     return trk_set_error(TRK_ERR_ARG, "offsets must run from 0 to the loaded particle count (%ld)", ctx->np);
   for (int v = 0; v < n_variants; v++)
@@ -1342,7 +1342,6 @@ int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int
     }
   }
   CUDA_TRY(cudaSetDevice(ctx->device));
-  const double Po = run->p_central;
   if (!(Po > 0))
     return trk_set_error(TRK_ERR_ARG, "p_central must be positive");
   /* one compiled record set per variant, concatenated; aperture and field
@@ -1358,6 +1357,7 @@ int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int
     else if ((int)c.ops.size() != nops)
       return trk_set_error(TRK_ERR_ARG, "variant %d compiles to a different element sequence", v);
     lean = lean && c.lean;
+    all.has_cfbend = all.has_cfbend || c.has_cfbend;
     const int apo = (int)all.aps.size(), fo = (int)all.field.size();
     for (trk_op op : c.ops) {
       for (int k = 0; k < 2; k++) {
@@ -1382,6 +1382,22 @@ int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int
     return rc;
   CUDA_TRY(cudaMemcpyAsync(ctx->d_ens_offsets, offsets, sizeof(long) * (n_variants + 1), cudaMemcpyHostToDevice,
                            ctx->stream));
+  *nops_out = nops;
+  *lean_out = lean;
+  return TRK_OK;
+}
+
+int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int n_variants, const long *offsets,
+                       const trk_run *run, trk_stats *stats) {
+  if (!run)
+    return trk_set_error(TRK_ERR_ARG, "bad ensemble arguments");
+  if (run->n_passes < 0)
+    return trk_set_error(TRK_ERR_ARG, "negative pass count");
+  const double Po = run->p_central;
+  int rc = 0, nops = 0;
+  bool lean = true;
+  if ((rc = prepare_ensemble(ctx, lattices, n_variants, offsets, Po, &nops, &lean)))
+    return rc;
   const bool fast = run->fast_math != 0;
   const long p0 = run->pass_offset;
   const long fresh = ctx->passes_done == 0 ? p0 : -1;
@@ -1489,62 +1505,105 @@ int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int
 int trk_ensemble_variant(const trk_context *ctx) { return ctx ? ctx->ens_last_variant : -1; }
 
 /* ------------------------------------------------------------- gradients */
-/* sums over surviving particles: x^2 + y^2, x, y, count */
-__global__ void adj_moments_kernel(const double *x, const double *y, const int32_t *lost, long n, double *out) {
-  double s2 = 0, sx = 0, sy = 0, c = 0;
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    if (lost[i] < 0) {
-      s2 += x[i] * x[i] + y[i] * y[i];
-      sx += x[i];
-      sy += y[i];
-      c += 1;
-    }
-  for (int off = 16; off > 0; off >>= 1) {
-    s2 += __shfl_xor_sync(0xffffffffu, s2, off);
-    sx += __shfl_xor_sync(0xffffffffu, sx, off);
-    sy += __shfl_xor_sync(0xffffffffu, sy, off);
-    c += __shfl_xor_sync(0xffffffffu, c, off);
+/* variant of particle i: offsets[v] <= i < offsets[v+1]; 0 without offsets */
+__device__ __forceinline__ int adj_variant(const long *offsets, int nv, long i) {
+  if (!offsets)
+    return 0;
+  int lo = 0, hi = nv;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (offsets[mid] <= i)
+      lo = mid;
+    else
+      hi = mid;
   }
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(out, s2);
-    atomicAdd(out + 1, sx);
-    atomicAdd(out + 2, sy);
-    atomicAdd(out + 3, c);
+  return lo;
+}
+
+/* sums over surviving particles per variant: x^2 + y^2, x, y, count
+ * (out[4 v .. 4 v + 3]) */
+__global__ void adj_moments_kernel(const double *x, const double *y, const int32_t *lost, long n,
+                                   const long *offsets, int nv, double *out) {
+  const long stride = (long)gridDim.x * blockDim.x;
+  /* every lane runs the same number of rounds so the warp shuffles see all
+   * 32 lanes */
+  const long rounds = (n + stride - 1) / stride;
+  for (long r = 0; r < rounds; r++) {
+    const long i = r * stride + (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double s2 = 0, sx = 0, sy = 0, c = 0;
+    int v = 0;
+    if (i < n) {
+      v = adj_variant(offsets, nv, i);
+      if (lost[i] < 0) {
+        s2 = x[i] * x[i] + y[i] * y[i];
+        sx = x[i];
+        sy = y[i];
+        c = 1;
+      }
+    } else if (n > 0) {
+      v = adj_variant(offsets, nv, n - 1);
+    }
+    const bool uniform = __all_sync(0xffffffffu, v == __shfl_sync(0xffffffffu, v, 0));
+    if (uniform) {
+      for (int off = 16; off > 0; off >>= 1) {
+        s2 += __shfl_xor_sync(0xffffffffu, s2, off);
+        sx += __shfl_xor_sync(0xffffffffu, sx, off);
+        sy += __shfl_xor_sync(0xffffffffu, sy, off);
+        c += __shfl_xor_sync(0xffffffffu, c, off);
+      }
+    }
+    if ((uniform ? (threadIdx.x & 31) == 0 : true) && c != 0) {
+      atomicAdd(out + 4 * v, s2);
+      atomicAdd(out + 4 * v + 1, sx);
+      atomicAdd(out + 4 * v + 2, sy);
+      atomicAdd(out + 4 * v + 3, c);
+    }
   }
 }
 
-/* lambda at the end of the run: dL/dx = (2 x + 2 w mean(x)) / N, same in y */
-__global__ void adj_seed_kernel(const double *x, const double *y, const int32_t *lost, long n, double *lam, double gx,
-                                double gy, double inv_n) {
+/* lambda at the end of the run: dL/dx = (2 x + 2 w mean(x)) / N, same in y,
+ * with coef[3 v .. 3 v + 2] = (2 w mean(x) / N, 2 w mean(y) / N, 1 / N) of
+ * the particle's variant */
+__global__ void adj_seed_kernel(const double *x, const double *y, const int32_t *lost, long n, double *lam,
+                                const long *offsets, int nv, const double *coef) {
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
     const bool act = lost[i] < 0;
-    lam[i] = act ? 2 * x[i] * inv_n + gx : 0;
+    const double *c = coef + 3 * adj_variant(offsets, nv, i);
+    lam[i] = act ? 2 * x[i] * c[2] + c[0] : 0;
     lam[n + i] = 0;
-    lam[2 * n + i] = act ? 2 * y[i] * inv_n + gy : 0;
+    lam[2 * n + i] = act ? 2 * y[i] * c[2] + c[1] : 0;
     lam[3 * n + i] = 0;
     lam[4 * n + i] = 0;
   }
 }
 
-/* L = mean(x^2 + y^2) + w (mean(x)^2 + mean(y)^2) over survivors; also the
- * means and the survivor count */
-static int objective(trk_context *ctx, double w, double *L, double *mx, double *my, double *count) {
+/* L_v = mean(x^2 + y^2) + w (mean(x)^2 + mean(y)^2) over the survivors of
+ * each variant (nv = 1 and offsets = null: the whole beam); mom receives
+ * (L, mean x, mean y, count) per variant */
+static int objective_variants(trk_context *ctx, double w, const long *d_offsets, int nv, std::vector<double> &mom) {
   int rc;
-  if ((rc = ensure(&ctx->d_adj_mom, ctx->adj_mom_cap, 4)))
+  if ((rc = ensure(&ctx->d_adj_mom, ctx->adj_mom_cap, (size_t)4 * nv)))
     return rc;
-  CUDA_TRY(cudaMemsetAsync(ctx->d_adj_mom, 0, 4 * sizeof(double), ctx->stream));
+  CUDA_TRY(cudaMemsetAsync(ctx->d_adj_mom, 0, 4 * sizeof(double) * nv, ctx->stream));
   if (ctx->np > 0)
     adj_moments_kernel<<<std::min(grid_for(ctx, ctx->np, 256), 1184), 256, 0, ctx->stream>>>(
-      ctx->d_cols, ctx->d_cols + 2 * ctx->cap, ctx->d_lost_pass, ctx->np, ctx->d_adj_mom);
-  double h[4];
-  CUDA_TRY(cudaMemcpyAsync(h, ctx->d_adj_mom, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+      ctx->d_cols, ctx->d_cols + 2 * ctx->cap, ctx->d_lost_pass, ctx->np, d_offsets, nv, ctx->d_adj_mom);
+  std::vector<double> h(4 * (size_t)nv);
+  CUDA_TRY(cudaMemcpyAsync(h.data(), ctx->d_adj_mom, sizeof(double) * h.size(), cudaMemcpyDeviceToHost,
+                           ctx->stream));
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  if (h[3] <= 0)
-    return trk_set_error(TRK_ERR_PHYSICS, "no surviving particles for the loss function");
-  *mx = h[1] / h[3];
-  *my = h[2] / h[3];
-  *count = h[3];
-  *L = h[0] / h[3] + w * (*mx * *mx + *my * *my);
+  mom.assign(4 * (size_t)nv, 0.0);
+  for (int v = 0; v < nv; v++) {
+    const double *q = &h[4 * (size_t)v];
+    if (q[3] <= 0)
+      return nv == 1 ? trk_set_error(TRK_ERR_PHYSICS, "no surviving particles for the loss function")
+                     : trk_set_error(TRK_ERR_PHYSICS, "variant %d: no surviving particles for the loss function", v);
+    const double mx = q[1] / q[3], my = q[2] / q[3];
+    mom[4 * v] = q[0] / q[3] + w * (mx * mx + my * my);
+    mom[4 * v + 1] = mx;
+    mom[4 * v + 2] = my;
+    mom[4 * v + 3] = q[3];
+  }
   return TRK_OK;
 }
 
@@ -1552,8 +1611,11 @@ int trk_objective(trk_context *ctx, double centroid_weight, double *loss) {
   if (!ctx || !loss)
     return trk_set_error(TRK_ERR_ARG, "null argument");
   CUDA_TRY(cudaSetDevice(ctx->device));
-  double mx, my, c;
-  return objective(ctx, centroid_weight, loss, &mx, &my, &c);
+  std::vector<double> mom;
+  int rc = objective_variants(ctx, centroid_weight, nullptr, 1, mom);
+  if (rc == TRK_OK)
+    *loss = mom[0];
+  return rc;
 }
 
 /* the parameter of an element and the derivative of its per-step kick
@@ -1581,26 +1643,37 @@ static int param_derivative(const trk_elem *e, double Po, double *dk3) {
   return TRK_OK;
 }
 
-int trk_adjoint(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, double centroid_weight,
-                double *loss, double *grad, int n_grad) {
-  if (!ctx || !lattice || !run)
+/* The adjoint run of one lattice (offsets = null: lattices[0]) or of an
+ * ensemble of nv lattices over the variant offsets. */
+static int adjoint_run(trk_context *ctx, const trk_lattice *const *lattices, int nv, const long *offsets,
+                       const trk_run *run, double centroid_weight, double *loss, double *grad, int n_grad) {
+  if (!ctx || !lattices || !lattices[0] || !run || nv < 1)
     return trk_set_error(TRK_ERR_ARG, "null argument");
+  const trk_lattice *lattice = lattices[0];
   const int n_params = trk_adjoint_param_count(lattice);
-  if (grad && n_grad != n_params)
-    return trk_set_error(TRK_ERR_ARG, "grad has %d entries, the lattice has %d parameters", n_grad, n_params);
+  if (grad && n_grad != n_params * nv)
+    return trk_set_error(TRK_ERR_ARG, "grad has %d entries, the run has %d parameters", n_grad, n_params * nv);
   if (run->n_passes < 1)
     return trk_set_error(TRK_ERR_ARG, "at least one pass");
   if (ctx->np <= 0)
     return trk_set_error(TRK_ERR_STATE, "no beam loaded");
   CUDA_TRY(cudaSetDevice(ctx->device));
   const double Po = run->p_central;
-  int rc = upload_lattice(ctx, lattice, Po);
-  if (rc)
-    return rc;
+  const bool ensemble = offsets != nullptr;
+  int rc = 0, nops = 0;
+  bool lean = true;
+  if (ensemble) {
+    if ((rc = prepare_ensemble(ctx, lattices, nv, offsets, Po, &nops, &lean)))
+      return rc;
+  } else {
+    if ((rc = upload_lattice(ctx, lattice, Po)))
+      return rc;
+    nops = (int)ctx->comp.ops.size();
+    lean = ctx->comp.lean;
+  }
   const CompiledLattice &c = ctx->comp;
-  const int nops = (int)c.ops.size();
   std::vector<int> op_param(std::max(nops, 1), -1);
-  std::vector<double> op_dk(3 * std::max(nops, 1), 0.0);
+  std::vector<double> op_dk(3 * (size_t)nv * std::max(nops, 1), 0.0);
   std::vector<int> param_of_elem(lattice->n, -1);
   for (int i = 0, k = 0; i < lattice->n; i++)
     if (lattice->e[i].type == TRK_KQUAD || lattice->e[i].type == TRK_KSEXT)
@@ -1618,27 +1691,31 @@ int trk_adjoint(trk_context *ctx, const trk_lattice *lattice, const trk_run *run
         return trk_set_error(TRK_ERR_UNSUPPORTED, "multipole with more than 16 slices in a gradient run");
       break;
     case OPK_DIPOLE:
-      if (op.i[0] * 4 > 128)
+    case OPK_CFBEND:
+      if (op.i[0] > 32)
         return trk_set_error(TRK_ERR_UNSUPPORTED, "CSBEND with more than 32 slices in a gradient run");
       break;
     default:
       return trk_set_error(TRK_ERR_UNSUPPORTED, "element %d: gradients cover DRIF, EDRIFT, KQUAD/KSEXT/KOCT "
-                           "(single order, no tilt or misalignment) and pure-dipole CSBEND", op.elem);
+                           "(single order, no tilt or misalignment) and CSBEND (pure dipole or K1/K2 "
+                           "expansion, no misalignment or edge kick)", op.elem);
     }
     const int pe = (op.elem >= 0 && op.elem < lattice->n) ? param_of_elem[op.elem] : -1;
     if (pe >= 0) {
       if (op.kind != OPK_MULT1)
         return trk_set_error(TRK_ERR_UNSUPPORTED, "element %d: gradients need a single-order multipole", op.elem);
       op_param[k] = pe;
-      if ((rc = param_derivative(&lattice->e[op.elem], Po, &op_dk[3 * k])))
-        return rc;
+      for (int v = 0; v < nv; v++)
+        if ((rc = param_derivative(&lattices[v]->e[op.elem], Po, &op_dk[3 * ((size_t)v * nops + k)])))
+          return rc;
     }
   }
   const long np = ctx->np, T = run->n_passes;
+  const size_t n_grad_all = (size_t)n_params * nv;
   if ((rc = ensure(&ctx->d_adj_ck, ctx->adj_ck_cap, (size_t)T * 4 * np)) ||
       (rc = ensure(&ctx->d_adj_entry, ctx->adj_entry_cap, (size_t)std::max(nops, 1) * 4 * np)) ||
       (rc = ensure(&ctx->d_adj_lam, ctx->adj_lam_cap, (size_t)5 * np)) ||
-      (rc = ensure(&ctx->d_adj_grad, ctx->adj_grad_cap, (size_t)std::max(n_params, 1))) ||
+      (rc = ensure(&ctx->d_adj_grad, ctx->adj_grad_cap, std::max<size_t>(n_grad_all, 1))) ||
       (rc = ensure(&ctx->d_adj_param, ctx->adj_param_cap, op_param.size())) ||
       (rc = ensure(&ctx->d_adj_dk, ctx->adj_dk_cap, op_dk.size())))
     return rc;
@@ -1646,7 +1723,6 @@ int trk_adjoint(trk_context *ctx, const trk_lattice *lattice, const trk_run *run
                            ctx->stream));
   CUDA_TRY(cudaMemcpyAsync(ctx->d_adj_dk, op_dk.data(), sizeof(double) * op_dk.size(), cudaMemcpyHostToDevice,
                            ctx->stream));
-  CUDA_TRY(cudaMemsetAsync(ctx->d_adj_grad, 0, sizeof(double) * std::max(n_params, 1), ctx->stream));
 
   /* forward, one pass per launch, the beam at the start of every pass kept */
   const long p0 = run->pass_offset;
@@ -1659,31 +1735,48 @@ int trk_adjoint(trk_context *ctx, const trk_lattice *lattice, const trk_run *run
   ta.Po = Po;
   ta.op_begin = 0;
   ta.op_end = nops;
-  const int col[4] = {0, 1, 2, 3};
+  const long *d_off = ensemble ? ctx->d_ens_offsets : nullptr;
+  const int shape = trk_default_variant(true, c);
   for (long t = 0; t < T; t++) {
     for (int q = 0; q < 4; q++)
-      CUDA_TRY(cudaMemcpyAsync(ctx->d_adj_ck + ((size_t)t * 4 + q) * np, ctx->d_cols + (size_t)col[q] * ctx->cap,
+      CUDA_TRY(cudaMemcpyAsync(ctx->d_adj_ck + ((size_t)t * 4 + q) * np, ctx->d_cols + (size_t)q * ctx->cap,
                                sizeof(double) * np, cudaMemcpyDeviceToDevice, ctx->stream));
     ta.pass_begin = p0 + t;
     ta.pass_end = p0 + t + 1;
-    if (nops > 0)
-      trk_fast::launch_track(ta, (c.lean ? 7 : 1), c.lean, np, ctx->sm_count * 256, ctx->stream);
+    if (nops > 0) {
+      if (ensemble)
+        trk_fast::launch_track_ensemble(ta, d_off, nv, nops, shape, lean, np, ctx->sm_count * 256, ctx->stream);
+      else
+        trk_fast::launch_track(ta, shape, lean, np, ctx->sm_count * 256, ctx->stream);
+    }
   }
   CUDA_TRY(cudaGetLastError());
   ctx->passes_done += T;
-  double L, mx, my, cnt;
-  if ((rc = objective(ctx, centroid_weight, &L, &mx, &my, &cnt)))
+  std::vector<double> mom;
+  if ((rc = objective_variants(ctx, centroid_weight, d_off, nv, mom)))
     return rc;
   if (loss)
-    *loss = L;
+    for (int v = 0; v < nv; v++)
+      loss[v] = mom[4 * v];
   if (!grad)
     return TRK_OK;
 
   /* reverse: seed, then per pass (last first) record the element entry
    * states from the pass checkpoint and sweep the elements backwards */
+  std::vector<double> coef(3 * (size_t)nv);
+  for (int v = 0; v < nv; v++) {
+    const double cnt = mom[4 * v + 3];
+    coef[3 * v] = 2 * centroid_weight * mom[4 * v + 1] / cnt;
+    coef[3 * v + 1] = 2 * centroid_weight * mom[4 * v + 2] / cnt;
+    coef[3 * v + 2] = 1.0 / cnt;
+  }
+  /* the seed coefficients go to the moments buffer (4 per variant), whose
+   * contents are no longer needed */
+  CUDA_TRY(cudaMemcpyAsync(ctx->d_adj_mom, coef.data(), sizeof(double) * coef.size(), cudaMemcpyHostToDevice,
+                           ctx->stream));
   adj_seed_kernel<<<std::min(grid_for(ctx, np, 256), 1184), 256, 0, ctx->stream>>>(
-    ctx->d_cols, ctx->d_cols + 2 * ctx->cap, ctx->d_lost_pass, np, ctx->d_adj_lam, 2 * centroid_weight * mx / cnt,
-    2 * centroid_weight * my / cnt, 1.0 / cnt);
+    ctx->d_cols, ctx->d_cols + 2 * ctx->cap, ctx->d_lost_pass, np, ctx->d_adj_lam, d_off, nv, ctx->d_adj_mom);
+  CUDA_TRY(cudaMemsetAsync(ctx->d_adj_grad, 0, sizeof(double) * std::max<size_t>(n_grad_all, 1), ctx->stream));
   AdjArgs g;
   g.entry = ctx->d_adj_entry;
   g.lam = ctx->d_adj_lam;
@@ -1691,15 +1784,35 @@ int trk_adjoint(trk_context *ctx, const trk_lattice *lattice, const trk_run *run
   g.op_param = ctx->d_adj_param;
   g.op_dk = ctx->d_adj_dk;
   g.n_ops = nops;
+  g.n_params = n_params;
+  if (ensemble) {
+    ta.ens_offsets = d_off;
+    ta.ens_variants = nv;
+    ta.ens_ops = nops;
+  }
   for (long t = T - 1; t >= 0; t--) {
     g.ck = ctx->d_adj_ck + (size_t)t * 4 * np;
     trk_fast::launch_adjoint_record(ta, g, ctx->stream);
     trk_fast::launch_adjoint_reverse(ta, g, ctx->stream);
   }
   CUDA_TRY(cudaGetLastError());
-  CUDA_TRY(cudaMemcpyAsync(grad, ctx->d_adj_grad, sizeof(double) * n_params, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaMemcpyAsync(grad, ctx->d_adj_grad, sizeof(double) * n_grad_all, cudaMemcpyDeviceToHost,
+                           ctx->stream));
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return check_status(ctx);
+}
+
+int trk_adjoint(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, double centroid_weight,
+                double *loss, double *grad, int n_grad) {
+  const trk_lattice *one[1] = {lattice};
+  return adjoint_run(ctx, one, 1, nullptr, run, centroid_weight, loss, grad, n_grad);
+}
+
+int trk_adjoint_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int n_variants, const long *offsets,
+                         const trk_run *run, double centroid_weight, double *loss, double *grad, int n_grad) {
+  if (!offsets)
+    return trk_set_error(TRK_ERR_ARG, "null offsets");
+  return adjoint_run(ctx, lattices, n_variants, offsets, run, centroid_weight, loss, grad, n_grad);
 }
 
 int trk_adjoint_param_count(const trk_lattice *lattice) {

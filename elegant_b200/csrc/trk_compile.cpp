@@ -831,8 +831,10 @@ int trk_compile(const trk_lattice *l, double Po, CompiledLattice &out) {
       const bool plain = op.i[1] == 4 && !(op.i[7] & (BF_MISALIGN | BF_APTILT)) && e1_noop && e2_noop;
       if (plain && op.i[2] == 0)
         op.kind = OPK_DIPOLE;
-      else if (plain && op.i[2] == 1 && op.i[3] == 5)
+      else if (plain && op.i[2] == 1 && op.i[3] == 5) {
         op.kind = OPK_CFBEND;
+        out.has_cfbend = true;
+      }
     }
     if (op.kind != OPK_NOP && op.kind != OPK_DRIFT && op.kind != OPK_EDRIFT && op.kind != OPK_RFDRIFT &&
         op.kind != OPK_MULT1 && op.kind != OPK_DIPOLE && op.kind != OPK_CFBEND && op.kind != OPK_RF &&

@@ -33,7 +33,18 @@ struct CompiledLattice {
   int n_mult = 0;
   double total_length = 0;
   bool lean = true; /* every op has a kind the lean kernel variant handles */
+  bool has_cfbend = false; /* some op is a combined-function CSBEND (OPK_CFBEND) */
 };
+
+/* Launch shape of the tracking kernel when the caller names none, measured on
+ * B200 (fast build): (128 threads, 6 blocks/SM; 80 registers) for lean
+ * lattices, (128, 5; 102 registers) for lean lattices with combined-function
+ * bends, whose body spills at 80 registers, and (128, 4) otherwise. */
+inline int trk_default_variant(bool fast, const CompiledLattice &c) {
+  if (fast && c.lean)
+    return c.has_cfbend ? 4 : 7;
+  return 1;
+}
 
 int trk_compile(const trk_lattice *l, double Po, CompiledLattice &out);
 void trk_expansion_coefficients(double *coef10);

@@ -1677,6 +1677,20 @@ __device__ __forceinline__ bool track_particle(const TrackArgs &a, const trk_op 
   return true;
 }
 
+/* Ensemble variant v of particle i: offsets[v] <= i < offsets[v+1] (the
+ * variants hold the same element structure with other values). */
+__device__ __forceinline__ int ens_variant(const long *__restrict__ offsets, int n_variants, long i) {
+  int lo = 0, hi = n_variants;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(&offsets[mid]) <= i)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
 /* Kernel variants (block size, minimum resident blocks per SM) trade
  * registers against occupancy; trk_run.variant or the autotuner picks one. */
 template <int BLOCK, int MINB, bool LEAN>
@@ -1686,19 +1700,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(TrackArgs a) {
     if (a.lost_pass[i] >= 0)
       continue;
     const trk_op *ops = a.ops;
-    if (a.ens_offsets) {
-      /* ensemble: particle i runs the records of the variant v with
-       * offsets[v] <= i < offsets[v+1] (same structure, other values) */
-      int lo = 0, hi = a.ens_variants;
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (__ldg(&a.ens_offsets[mid]) <= i)
-          lo = mid;
-        else
-          hi = mid;
-      }
-      ops += (long)lo * a.ens_ops;
-    }
+    if (a.ens_offsets) /* ensemble: the records of this particle's variant */
+      ops += (long)ens_variant(a.ens_offsets, a.ens_variants, i) * a.ens_ops;
     Part p;
     load_part(a, i, p);
     track_particle<LEAN>(a, ops, p, i);
@@ -2442,6 +2445,152 @@ __device__ void adj_dipole(const trk_op *__restrict__ op, double x, double xp, d
   ldp += lopd;
 }
 
+#define TRK_ADJ_MAX_SLICES 32 /* combined-function bend: slices */
+
+/* partial derivatives of the cf_fields expansion at (x, y) */
+#define CF_T(T, i, j) __ldg(&(T)[(i) * 11 + (j)])
+__device__ __forceinline__ void cf_fields_d(const double *__restrict__ Fx_xy, const double *__restrict__ Fy_xy,
+                                            double x, double y, double &Fyx, double &Fyy, double &Fxx,
+                                            double &Fxy) {
+  const double y2 = y * y;
+  const double dp0 = fma(fma(fma(4 * CF_T(Fy_xy, 4, 0), x, 3 * CF_T(Fy_xy, 3, 0)), x, 2 * CF_T(Fy_xy, 2, 0)), x,
+                         CF_T(Fy_xy, 1, 0));
+  const double p2 = fma(fma(CF_T(Fy_xy, 2, 2), x, CF_T(Fy_xy, 1, 2)), x, CF_T(Fy_xy, 0, 2));
+  const double dp2 = fma(2 * CF_T(Fy_xy, 2, 2), x, CF_T(Fy_xy, 1, 2));
+  Fyx = fma(y2, dp2, dp0);
+  Fyy = 2 * y * fma(2 * y2, CF_T(Fy_xy, 0, 4), p2);
+  const double q1 = fma(fma(fma(CF_T(Fx_xy, 3, 1), x, CF_T(Fx_xy, 2, 1)), x, CF_T(Fx_xy, 1, 1)), x,
+                        CF_T(Fx_xy, 0, 1));
+  const double dq1 = fma(fma(3 * CF_T(Fx_xy, 3, 1), x, 2 * CF_T(Fx_xy, 2, 1)), x, CF_T(Fx_xy, 1, 1));
+  const double q3 = fma(CF_T(Fx_xy, 1, 3), x, CF_T(Fx_xy, 0, 3));
+  Fxx = y * fma(y2, CF_T(Fx_xy, 1, 3), dq1);
+  Fxy = fma(3 * y2, q3, q1);
+}
+#undef CF_T
+
+/* one drift substep j of cf_slice (no path length) */
+__device__ __forceinline__ void cf_drift(const double *__restrict__ d, int j, double rho0, double opd2, double &X,
+                                         double &QX, double &Y, const double QY) {
+  const double fc = sqrt_nan(fma(-QX, QX, fma(-QY, QY, opd2)));
+  const double sa = __ldg(&d[BD_SA + j]), ca = __ldg(&d[BD_CA + j]);
+  const double saq = sa * QX;
+  const double u = div_fast(rho0 + X, fma(ca, fc, -saq));
+  QX = fma(sa, fc, ca * QX);
+  Y = fma(QY, u * sa, Y);
+  X = fma(u, fma(__ldg(&d[BD_OMC + j]), fc, saq), X);
+}
+
+/* adjoint of op_cfbend_fast (bend_cf_fast / cf_slice): the entry state of
+ * every slice is kept, and each slice's four substeps are recomputed from it
+ * while the slices are reversed */
+__device__ void adj_cfbend(const trk_op *__restrict__ op, const double *__restrict__ field, double x, double xp,
+                           double y, double yp, double dp, double &lx, double &lxp, double &ly, double &lyp,
+                           double &ldp) {
+  const double *d = op->d;
+  const double *fx = field + __ldg(&op->i[4]);
+  const double *fy = fx + 121;
+  const int nSlices = __ldg(&op->i[0]);
+  const double rho0 = __ldg(&d[BD_RHO0]);
+  const double opd = 1 + dp, opd2 = opd * opd;
+  const double r = opd * rsqrt_fast(fma(yp, yp, fma(xp, xp, 1.0)));
+  double X = x, QX = xp * r, Y = y, QY = yp * r;
+  double CX[TRK_ADJ_MAX_SLICES], CQX[TRK_ADJ_MAX_SLICES], CY[TRK_ADJ_MAX_SLICES], CQY[TRK_ADJ_MAX_SLICES];
+  for (int i = 0; i < nSlices; i++) {
+    CX[i] = X;
+    CQX[i] = QX;
+    CY[i] = Y;
+    CQY[i] = QY;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      cf_drift(d, j, rho0, opd2, X, QX, Y, QY);
+      if (j == 3)
+        break;
+      double Fx, Fy;
+      cf_fields(fx, fy, X, Y, Fx, Fy);
+      const double w = fma(__ldg(&d[BD_C2 + j]), X, __ldg(&d[BD_C1 + j]));
+      QX = fma(-w, Fy, QX);
+      QY = fma(w, Fx, QY);
+    }
+  }
+  /* exit: x = X, y = Y, (xp, yp) = (QX, QY) / sqrt(opd^2 - QX^2 - QY^2) */
+  double lX = lx, lY = ly, lQX = 0, lQY = 0, lopd = 0;
+  adj_m2s(QX, QY, opd, lxp, lyp, lQX, lQY, lopd);
+  for (int i = nSlices - 1; i >= 0; i--) {
+    /* substep entry states of slice i (and the kick positions) */
+    double sX[5], sQX[4], sY[5], sQY[4];
+    X = CX[i];
+    QX = CQX[i];
+    Y = CY[i];
+    QY = CQY[i];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      sX[j] = X;
+      sQX[j] = QX;
+      sY[j] = Y;
+      sQY[j] = QY;
+      cf_drift(d, j, rho0, opd2, X, QX, Y, QY);
+      sX[j + 1] = X;
+      sY[j + 1] = Y;
+      if (j == 3)
+        break;
+      double Fx, Fy;
+      cf_fields(fx, fy, X, Y, Fx, Fy);
+      const double w = fma(__ldg(&d[BD_C2 + j]), X, __ldg(&d[BD_C1 + j]));
+      QX = fma(-w, Fy, QX);
+      QY = fma(w, Fx, QY);
+    }
+#pragma unroll
+    for (int j = 3; j >= 0; j--) {
+      if (j < 3) {
+        /* kick at (X1, Y1) = (sX[j+1], sY[j+1]): QX -= w Fy, QY += w Fx */
+        const double X1 = sX[j + 1], Y1 = sY[j + 1];
+        const double c2 = __ldg(&d[BD_C2 + j]);
+        const double w = fma(c2, X1, __ldg(&d[BD_C1 + j]));
+        double Fx, Fy, Fyx, Fyy, Fxx, Fxy;
+        cf_fields(fx, fy, X1, Y1, Fx, Fy);
+        cf_fields_d(fx, fy, X1, Y1, Fyx, Fyy, Fxx, Fxy);
+        const double lw = fma(-lQX, Fy, lQY * Fx);
+        lX += lw * c2 + w * fma(-lQX, Fyx, lQY * Fxx);
+        lY += w * fma(-lQX, Fyy, lQY * Fxy);
+      }
+      /* drift from (Xs, QXs, Ys, QYs): X' = Xs + u (omc fc + sa QXs),
+       * QX' = sa fc + ca QXs, Y' = Ys + QYs u sa, with
+       * fc = sqrt(opd^2 - QYs^2 - QXs^2), u = (rho0 + Xs) / (ca fc - sa QXs) */
+      const double Xs = sX[j], QXs = sQX[j], QYs = sQY[j];
+      const double sa = __ldg(&d[BD_SA + j]), ca = __ldg(&d[BD_CA + j]), omc = __ldg(&d[BD_OMC + j]);
+      const double fc = sqrt_nan(fma(-QXs, QXs, fma(-QYs, QYs, opd2)));
+      const double saq = sa * QXs;
+      const double fcosi = fma(ca, fc, -saq);
+      const double u = div_fast(rho0 + Xs, fcosi);
+      lQY += lY * u * sa;
+      const double lu = lY * QYs * sa + lX * fma(omc, fc, saq);
+      double lfc = lX * u * omc + lQX * sa;
+      double lsaq = lX * u;
+      double lQXs = lQX * ca;
+      double lXs = lX;
+      const double lfcosi = -lu * u / fcosi;
+      lXs += lu / fcosi;
+      lfc += ca * lfcosi;
+      lsaq -= lfcosi;
+      lQXs += sa * lsaq;
+      const double lu2 = lfc / (2 * fc);
+      lQXs -= 2 * QXs * lu2;
+      lopd += 2 * opd * lu2;
+      lQY -= 2 * QYs * lu2;
+      lX = lXs;
+      lQX = lQXs;
+    }
+  }
+  /* entry: X = x, Y = y, (QX, QY) = opd (xp, yp) / sqrt(1 + xp^2 + yp^2) */
+  lx = lX;
+  ly = lY;
+  double lxp_in = 0, lyp_in = 0;
+  adj_s2m(xp, yp, opd, lQX, lQY, lxp_in, lyp_in, ldp);
+  lxp = lxp_in;
+  lyp = lyp_in;
+  ldp += lopd;
+}
+
 /* forward pass from a checkpoint, recording every element's entry state */
 __global__ void adj_record_kernel(TrackArgs a, AdjArgs g) {
   const long n = a.n, stride = (long)gridDim.x * blockDim.x;
@@ -2455,8 +2604,11 @@ __global__ void adj_record_kernel(TrackArgs a, AdjArgs g) {
     p.yp = g.ck[3 * n + i];
     p.s = 0;
     p.dp = a.dp[i];
+    const trk_op *ops = a.ops;
+    if (a.ens_offsets)
+      ops += (long)ens_variant(a.ens_offsets, a.ens_variants, i) * a.ens_ops;
     for (int k = 0; k < g.n_ops; k++) {
-      const trk_op *op = a.ops + k;
+      const trk_op *op = ops + k;
       double *e = g.entry + (size_t)k * 4 * n;
       e[i] = p.x;
       e[n + i] = p.xp;
@@ -2476,6 +2628,9 @@ __global__ void adj_record_kernel(TrackArgs a, AdjArgs g) {
       case OPK_DIPOLE:
         op_dipole_fast(op, p, a.Po, 0.0, nullptr);
         break;
+      case OPK_CFBEND:
+        op_cfbend_fast(op, p, a.Po, 0.0, nullptr, a.field);
+        break;
       default:
         break;
       }
@@ -2489,6 +2644,13 @@ __global__ void __launch_bounds__(128) adj_reverse_kernel(TrackArgs a, AdjArgs g
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const bool act = i < n && a.lost_pass[i] < 0;
   double lx = 0, lxp = 0, ly = 0, lyp = 0, ldp = 0, dp = 0;
+  /* variant of this particle (ensembles); lanes past the end take the last
+   * particle's, so a warp of one variant stays uniform */
+  int v = 0;
+  if (a.ens_offsets && n > 0)
+    v = ens_variant(a.ens_offsets, a.ens_variants, i < n ? i : n - 1);
+  const trk_op *ops = a.ops + (long)v * a.ens_ops;
+  const bool warp_uniform = __all_sync(0xffffffffu, v == __shfl_sync(0xffffffffu, v, 0));
   if (act) {
     lx = g.lam[i];
     lxp = g.lam[n + i];
@@ -2498,7 +2660,7 @@ __global__ void __launch_bounds__(128) adj_reverse_kernel(TrackArgs a, AdjArgs g
     dp = a.dp[i];
   }
   for (int k = g.n_ops - 1; k >= 0; k--) {
-    const trk_op *op = a.ops + k;
+    const trk_op *op = ops + k;
     double x = 0, xp = 0, y = 0, yp = 0;
     if (act) {
       const double *e = g.entry + (size_t)k * 4 * n;
@@ -2518,10 +2680,13 @@ __global__ void __launch_bounds__(128) adj_reverse_kernel(TrackArgs a, AdjArgs g
       break;
     }
     case OPK_MULT1:
-      sens = adj_mult1(op, g.op_dk + 3 * k, x, xp, y, yp, dp, lx, lxp, ly, lyp, ldp);
+      sens = adj_mult1(op, g.op_dk + 3 * ((long)v * g.n_ops + k), x, xp, y, yp, dp, lx, lxp, ly, lyp, ldp);
       break;
     case OPK_DIPOLE:
       adj_dipole(op, x, xp, y, yp, dp, lx, lxp, ly, lyp, ldp);
+      break;
+    case OPK_CFBEND:
+      adj_cfbend(op, a.field, x, xp, y, yp, dp, lx, lxp, ly, lyp, ldp);
       break;
     default:
       break;
@@ -2530,10 +2695,14 @@ __global__ void __launch_bounds__(128) adj_reverse_kernel(TrackArgs a, AdjArgs g
     if (prm >= 0) {
       if (!act)
         sens = 0;
-      for (int off = 16; off > 0; off >>= 1)
-        sens += __shfl_xor_sync(0xffffffffu, sens, off);
-      if ((threadIdx.x & 31) == 0 && sens != 0)
-        atomicAdd(&g.grad[prm], sens);
+      if (warp_uniform) {
+        for (int off = 16; off > 0; off >>= 1)
+          sens += __shfl_xor_sync(0xffffffffu, sens, off);
+        if ((threadIdx.x & 31) == 0 && sens != 0)
+          atomicAdd(&g.grad[(long)v * g.n_params + prm], sens);
+      } else if (sens != 0) {
+        atomicAdd(&g.grad[(long)v * g.n_params + prm], sens);
+      }
     }
   }
   if (act) {

@@ -109,8 +109,9 @@ struct AdjArgs {
   double *lam;           /* adjoint of x, xp, y, yp, delta: 5 columns of n */
   double *grad;          /* gradient accumulators, one per parameter */
   const int *op_param;   /* parameter index of each op, -1 if none */
-  const double *op_dk;   /* per op: d(kick strength)/d(parameter) of kick steps 0..2 */
-  int n_ops;
+  const double *op_dk;   /* per variant and op: d(kick strength)/d(parameter) of kick steps 0..2 */
+  int n_ops;             /* ops per variant */
+  int n_params;          /* parameters per variant (grad holds n_variants x n_params) */
 };
 
 #define TRK_DECLARE_LAUNCHERS(NS)                                                                            \

@@ -307,11 +307,19 @@ int trk_wake_noalloc(double *const *columns, int32_t *lost_pass, int32_t *lost_e
  * (particles lost during the run are left out: loss events are not
  * differentiable).  Parameters: K1 of every KQUAD and K2 of every KSEXT, in
  * lattice order.  Elements allowed: DRIF, EDRIFT, single-order
- * KQUAD/KSEXT/KOCT without tilt or misalignment, pure-dipole CSBEND, MARK,
- * MAXAMP.  grad may be NULL (loss only).  The device beam is left at its
- * final state. */
+ * KQUAD/KSEXT/KOCT without tilt or misalignment, CSBEND (pure dipole, or a
+ * K1/K2 field expansion) without misalignment or edge kick, MARK, MAXAMP.
+ * grad may be NULL (loss only).  The device beam is left at its final state. */
 int trk_adjoint(trk_context *ctx, const trk_lattice *lattice, const trk_run *run,
                 double centroid_weight, double *loss, double *grad, int n_grad);
+/* The batched form: n_variants lattices of one structure (error seeds) over
+ * particle ranges [offsets[v], offsets[v+1]) of the loaded beam, as in
+ * trk_track_ensemble, in one forward and one reverse sweep.  loss[v] is
+ * variant v's loss over its own survivors; grad[v * P + p] its gradient
+ * with respect to parameter p (P = trk_adjoint_param_count of a variant;
+ * n_grad = n_variants * P). */
+int trk_adjoint_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int n_variants, const long *offsets,
+                         const trk_run *run, double centroid_weight, double *loss, double *grad, int n_grad);
 /* The same loss function on the device beam as it is (for finite
  * differences against trk_adjoint). */
 int trk_objective(trk_context *ctx, double centroid_weight, double *loss);

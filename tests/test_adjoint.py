@@ -119,3 +119,96 @@ def test_losses_are_left_out_and_elements_checked():
         trk.load(beam)
         with pytest.raises(Exception):
             trk.adjoint(rf, 2, PC, W)
+
+
+def _gpu_fd(trk, lat, beam, passes, w, params=None, rel=1e-7):
+    k0 = get_parameters(lat)
+    fd = np.zeros_like(k0)
+    for p in (range(len(k0)) if params is None else params):
+        h = rel * abs(k0[p])
+        vals = []
+        for sgn in (1, -1):
+            k = k0.copy()
+            k[p] += sgn * h
+            set_parameters(lat, k)
+            trk.load(beam)
+            trk.track(lat, passes, PC)
+            vals.append(trk.objective(w))
+        fd[p] = (vals[0] - vals[1]) / (2 * h)
+    set_parameters(lat, k0)
+    return fd
+
+
+def _mba(cells=1, **kw):
+    return configs.c5_lattice(cells=cells, with_rf=False, with_wake=False, **kw)
+
+
+def test_adjoint_through_combined_function_bends():
+    """The MBA cell: combined-function CSBENDs (K1 field expansion), strong
+    quadrupoles, sextupoles and octupoles; gradient w.r.t. its 12 K1 and 6
+    K2 against GPU central differences."""
+    lat, passes = _mba(), 6
+    beam = configs.c5_beam(3000, seed=93)
+    beam[:, 0] += 5e-5
+    with Tracker(0) as trk:
+        trk.load(beam)
+        loss, grad = trk.adjoint(lat, passes, PC, W)
+        trk.load(beam)
+        trk.track(lat, passes, PC)
+        assert abs(trk.objective(W) - loss) <= 1e-14 * abs(loss)
+        fd = _gpu_fd(trk, lat, beam, passes, W)
+    assert len(grad) == 18 and np.all(np.isfinite(grad))
+    assert np.linalg.norm(grad - fd) / np.linalg.norm(fd) < 1e-6, (grad, fd)
+    assert _rel_err(grad, fd) < 1e-5, (grad, fd)
+
+
+def test_adjoint_ensemble_equals_separate_adjoints():
+    """Four error seeds of the MBA cell with uneven particle counts in one
+    batched call: each variant's loss and gradient equal its own adjoint run
+    (to the order of the atomic sums)."""
+    counts = [700, 1300, 64, 950]
+    rng = np.random.Generator(np.random.Philox(94))
+    lats, beams, first = [], [], 1
+    for v, n in enumerate(counts):
+        kq = rng.normal(0, 1e-3, (1, 12))
+        k2 = rng.normal(0, 2e-3, (1, 6))
+        lats.append(_mba(kq_errors=kq, k2_errors=k2))
+        b = configs.c5_beam(n, seed=95 + v, first_id=first)
+        b[:, 0] += 5e-5
+        beams.append(b)
+        first += n
+    passes = 5
+    with Tracker(0) as trk:
+        trk.load(np.concatenate(beams))
+        losses, grads = trk.adjoint_ensemble(lats, counts, passes, PC, W)
+        for v, (lat, b) in enumerate(zip(lats, beams)):
+            trk.load(b)
+            loss, grad = trk.adjoint(lat, passes, PC, W)
+            assert abs(losses[v] - loss) <= 1e-13 * abs(loss), (v, losses[v], loss)
+            assert np.max(np.abs(grads[v] - grad)) <= 1e-10 * np.max(np.abs(grad)), v
+    assert grads.shape == (4, 18)
+    assert np.max(np.abs(grads[0] - grads[1])) > 0  # the variants differ
+
+
+def test_adjoint_ensemble_vs_finite_differences():
+    """The batched gradient of one variant against central differences of
+    that variant tracked alone."""
+    counts = [800, 1200]
+    lats = [_mba(kq_errors=np.full((1, 12), 1e-3 * s), k2_errors=np.full((1, 6), -2e-3 * s)) for s in (1, -1)]
+    beams = [configs.c5_beam(800, seed=96), configs.c5_beam(1200, seed=97, first_id=801)]
+    passes = 4
+    with Tracker(0) as trk:
+        trk.load(np.concatenate(beams))
+        _, grads = trk.adjoint_ensemble(lats, counts, passes, PC, W)
+        fd = _gpu_fd(trk, lats[1], beams[1], passes, W)
+    assert np.linalg.norm(grads[1] - fd) / np.linalg.norm(fd) < 1e-6, (grads[1], fd)
+
+
+def test_adjoint_rejects_misaligned_bend():
+    lat = _mba()
+    i = next(k for k, e in enumerate(lat.elements) if e[0] == "CSBEND")
+    lat.elements[i][2]["DX"] = 1e-4
+    with Tracker(0) as trk:
+        trk.load(configs.c5_beam(100, seed=98))
+        with pytest.raises(RuntimeError):
+            trk.adjoint(lat, 2, PC, W)
