@@ -44,6 +44,26 @@ class _Run(ctypes.Structure):
                 ("variant", ctypes.c_int32), ("time_kernels", ctypes.c_int32)]
 
 
+class BeamSums(ctypes.Structure):
+    """trk_beam_sums: elegant's BEAM_SUMS with its BEAM_SUMS2 (index 6 = time)."""
+    _fields_ = [("centroid", ctypes.c_double * 7), ("sigma", (ctypes.c_double * 7) * 7),
+                ("sigman", (ctypes.c_double * 7) * 7), ("maxabs", ctypes.c_double * 7),
+                ("min", ctypes.c_double * 7), ("max", ctypes.c_double * 7), ("n_part", ctypes.c_long),
+                ("p0", ctypes.c_double), ("charge", ctypes.c_double)]
+
+    @classmethod
+    def zeroed(cls):
+        """As zero_beam_sums leaves a BEAM_SUMS (src/compute_centroids.c:264-284)."""
+        s = cls()
+        for j in range(7):
+            s.min[j] = 1.7976931348623157e308
+            s.max[j] = -1.7976931348623157e308
+        return s
+
+
+SUMS_SPARSE, SUMS_NOMINMAX, SUMS_EXACT_NORMEMIT, SUMS_SECOND_ORDER = 0x1, 0x2, 0x4, 0x8
+
+
 class _Stats(ctypes.Structure):
     _fields_ = [("n_total", ctypes.c_long), ("n_left", ctypes.c_long), ("particle_passes", ctypes.c_long),
                 ("device_ms", ctypes.c_double), ("kernel_launches", ctypes.c_long), ("p_central", ctypes.c_double),
@@ -93,6 +113,10 @@ def _declare(lib):
         "trk_track_ensemble": (I, [P, ctypes.POINTER(P), I, ctypes.POINTER(L), ctypes.POINTER(_Run),
                                    ctypes.POINTER(_Stats)]),
         "trk_adjoint": (I, [P, P, ctypes.POINTER(_Run), D, DP, DP, I]),
+        "trk_beam_centroids": (I, [P, DP, ctypes.POINTER(L)]),
+        "trk_accumulate_beam_sums": (I, [P, ctypes.POINTER(BeamSums), D, D, DP, D, D, L, L, ctypes.c_uint]),
+        "trk_match_energy": (I, [P, DP, I]),
+        "trk_sort_by_id": (I, [P]),
         "trk_adjoint_ensemble": (I, [P, ctypes.POINTER(P), I, ctypes.POINTER(L), ctypes.POINTER(_Run), D, DP, DP, I]),
         "trk_adjoint_param_count": (I, [P]),
         "trk_objective": (I, [P, D, DP]),
@@ -333,6 +357,32 @@ class Tracker:
             self.ctx, arr, V, offs.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), ctypes.byref(run),
             centroid_weight, _dptr(loss), _dptr(g) if with_grad else None, n * V))
         return loss, g[:n * V].reshape(V, n)
+
+    def centroids(self):
+        """compute_centroids of the surviving particles: (centroid[6], count)."""
+        c = np.zeros(6)
+        n = ctypes.c_long()
+        _check(self.lib, self.lib.trk_beam_centroids(self.ctx, _dptr(c), ctypes.byref(n)))
+        return c, n.value
+
+    def accumulate_beam_sums(self, sums, p_central, mp_charge=0.0, time=None, t_min=0.0, t_max=0.0, start_pid=-1,
+                             end_pid=-1, flags=SUMS_SECOND_ORDER):
+        """accumulate_beam_sums of the surviving particles into `sums` (BeamSums)."""
+        tv = None if time is None else np.ascontiguousarray(time, dtype=np.float64)
+        _check(self.lib, self.lib.trk_accumulate_beam_sums(self.ctx, ctypes.byref(sums), p_central, mp_charge,
+                                                           None if tv is None else _dptr(tv), t_min, t_max,
+                                                           start_pid, end_pid, flags))
+        return sums
+
+    def match_energy(self, p_central, change_beam=0):
+        """do_match_energy on the device beam; returns the (new) central momentum."""
+        pc = ctypes.c_double(p_central)
+        _check(self.lib, self.lib.trk_match_energy(self.ctx, ctypes.byref(pc), int(change_beam)))
+        return pc.value
+
+    def sort_by_id(self):
+        """Survivors in increasing particle ID (lost particles after them)."""
+        _check(self.lib, self.lib.trk_sort_by_id(self.ctx))
 
     def objective(self, centroid_weight=0.0):
         """The adjoint's loss function on the device beam as it is."""

@@ -63,6 +63,9 @@ def objects():
     o = os.path.join(BUILD, "trk_lattice.o")
     out.append((src, o, ["gcc", "-std=gnu11", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math"] + INC +
                 ["-c", src, "-o", o]))
+    src = os.path.join(CSRC, "trk_observe.cu")
+    o = os.path.join(BUILD, "trk_observe.o")
+    out.append((src, o, nv_common + ["-fmad=false", "-c", src, "-o", o]))
     for extra in ("trk_noalloc.cu", "trk_hooks.cu"):
         src = os.path.join(CSRC, extra)
         if os.path.exists(src):

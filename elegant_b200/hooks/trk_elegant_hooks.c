@@ -17,6 +17,10 @@
  *   gpu_track_through_trwake     TRWAKE                  (src/trwake.c:46)
  *   gpu_limit_amplitudes, gpu_elimit_amplitudes, gpu_removeInvalidParticles
  *                                after-element filters   (src/limit_amplitudes.c:207, :510, :298)
+ *   gpu_compute_centroids, gpu_accumulate_beam_sums
+ *                                beam observers          (src/compute_centroids.c:64-76, :313-327)
+ *   gpu_collect_trajectory_data, gpu_do_match_energy, sortByPID
+ *                                whole-beam steps        (src/do_tracking.c:2598, :3404, :943)
  *
  * Element parameters are read from elegant's element structures through
  * elegant's own parameter tables (entity_description[], by name), so the
@@ -33,7 +37,9 @@
 #include "track.h"
 
 #include "gpu_base.h"
+#include "gpu_compute_centroids.h"
 #include "gpu_csbend.h"
+#include "gpu_funcs.h"
 #include "gpu_limit_amplitudes.h"
 #include "gpu_matrix.h"
 #include "gpu_multipole.h"
@@ -444,4 +450,68 @@ long gpu_elliptical_collimator(ECOL *ecol, long np, double **accepted, double z,
 }
 long gpu_beam_scraper(SCRAPER *scraper, long np, double **accepted, double z, double Po) {
   return outside("SCRAPER");
+}
+
+/* ------------------------------------------------- whole-beam observers */
+void gpu_compute_centroids(double *centroid, long n_part) {
+  long n = 0;
+  (void)n_part;
+  check(trk_beam_centroids(g_ctx, centroid, &n), "trk_beam_centroids");
+}
+
+void gpu_accumulate_beam_sums(BEAM_SUMS *sums, long n_part, double p_central, double mp_charge, double *timeValue,
+                              double tMin, double tMax, long startPID, long endPID, unsigned long flags) {
+  (void)n_part;
+  if (timeValue)
+    bombElegant("gpu_accumulate_beam_sums: caller-supplied time coordinates are not supported on the GPU path", NULL);
+  trk_beam_sums s;
+  memset(&s, 0, sizeof(s));
+  memcpy(s.centroid, sums->centroid, sizeof(s.centroid));
+  unsigned int f = 0;
+  if (flags & BEAM_SUMS_SPARSE)
+    f |= TRK_SUMS_SPARSE;
+  if (flags & BEAM_SUMS_NOMINMAX)
+    f |= TRK_SUMS_NOMINMAX;
+  if (exactNormalizedEmittance)
+    f |= TRK_SUMS_EXACT_NORMEMIT;
+  if (sums->beamSums2) {
+    f |= TRK_SUMS_SECOND_ORDER;
+    memcpy(s.sigma, sums->beamSums2->sigma, sizeof(s.sigma));
+    memcpy(s.sigman, sums->beamSums2->sigman, sizeof(s.sigman));
+    memcpy(s.maxabs, sums->beamSums2->maxabs, sizeof(s.maxabs));
+    memcpy(s.min, sums->beamSums2->min, sizeof(s.min));
+    memcpy(s.max, sums->beamSums2->max, sizeof(s.max));
+  }
+  s.n_part = sums->n_part;
+  s.p0 = sums->p0;
+  s.charge = sums->charge;
+  check(trk_accumulate_beam_sums(g_ctx, &s, p_central, mp_charge, NULL, tMin, tMax, startPID, endPID, f),
+        "trk_accumulate_beam_sums");
+  memcpy(sums->centroid, s.centroid, sizeof(s.centroid));
+  if (sums->beamSums2) {
+    memcpy(sums->beamSums2->sigma, s.sigma, sizeof(s.sigma));
+    memcpy(sums->beamSums2->sigman, s.sigman, sizeof(s.sigman));
+    memcpy(sums->beamSums2->maxabs, s.maxabs, sizeof(s.maxabs));
+    memcpy(sums->beamSums2->min, s.min, sizeof(s.min));
+    memcpy(sums->beamSums2->max, s.max, sizeof(s.max));
+  }
+  sums->n_part = s.n_part;
+  sums->p0 = s.p0;
+  sums->charge = s.charge;
+}
+
+void gpu_do_match_energy(long np, double *P_central, long change_beam) {
+  (void)np;
+  check(trk_match_energy(g_ctx, P_central, (int)change_beam), "trk_match_energy");
+}
+
+void gpu_collect_trajectory_data(double *centroid, long n) {
+  long m = 0;
+  (void)n;
+  check(trk_beam_centroids(g_ctx, centroid, &m), "trk_beam_centroids");
+}
+
+void sortByPID(long n) {
+  (void)n;
+  check(trk_sort_by_id(g_ctx), "trk_sort_by_id");
 }

@@ -244,6 +244,53 @@ int trk_remove_invalid(trk_context *ctx, double z, double p_central, long pass, 
 int trk_track_matrix(trk_context *ctx, int order, const double *C, const double *R, const double *T, int fast_math,
                      long *n_left);
 
+/* ------------------------------------------------------- beam observers */
+/* Whole-beam readings and operations between elements, on the device beam
+ * (survivors only), so observers do not force the beam to the host.  Sums
+ * the reference forms with Kahan's summation are formed in double-double. */
+
+/* compute_centroids (src/compute_centroids.c:53-160): means of x, x', y, y',
+ * s, delta over the surviving particles (all zero with none); *n (may be
+ * NULL) receives their count.  Also the trajectory centroids of do_tracking
+ * (src/do_tracking.c:2585-2610). */
+int trk_beam_centroids(trk_context *ctx, double *centroid, long *n);
+
+/* The reference's BEAM_SUMS with its BEAM_SUMS2 (src/track.h:281-297);
+ * index 6 is the time coordinate.  Zero it (and set min to +DBL_MAX, max to
+ * -DBL_MAX) before the first accumulation, as zero_beam_sums does. */
+typedef struct {
+  double centroid[7];
+  double sigma[7][7];
+  double sigman[7][7];
+  double maxabs[7], min[7], max[7];
+  long n_part;
+  double p0;
+  double charge;
+} trk_beam_sums;
+#define TRK_SUMS_SPARSE 0x1u         /* BEAM_SUMS_SPARSE: diagonal blocks and dispersive terms only */
+#define TRK_SUMS_NOMINMAX 0x2u       /* BEAM_SUMS_NOMINMAX */
+#define TRK_SUMS_EXACT_NORMEMIT 0x4u /* exactNormalizedEmittance: sigman with px, py */
+#define TRK_SUMS_SECOND_ORDER 0x8u   /* the BEAM_SUMS2 part is kept (sigma, min, max, maxabs) */
+/* accumulate_beam_sums (src/compute_centroids.c:286-461): adds the surviving
+ * particles with start_pid <= id <= end_pid (both < 0: all) and, if
+ * t_min < t_max, t_min <= t <= t_max, to *sums.  time_value (host, one per
+ * loaded particle in load order) replaces the computed time coordinates
+ * when not NULL. */
+int trk_accumulate_beam_sums(trk_context *ctx, trk_beam_sums *sums, double p_central, double mp_charge,
+                             const double *time_value, double t_min, double t_max, long start_pid, long end_pid,
+                             unsigned int flags);
+
+/* do_match_energy (src/do_tracking.c:3376-3546): change_beam = 0 moves
+ * *p_central to the survivors' mean momentum and rescales delta;
+ * change_beam = 1 shifts every momentum so the mean is *p_central, keeping
+ * each particle's time of flight. */
+int trk_match_energy(trk_context *ctx, double *p_central, int change_beam);
+
+/* The particle-ID sort of do_tracking (src/do_tracking.c:935-950, sortByPID
+ * on the GPU path): survivors in increasing ID, lost particles after them in
+ * their present order. */
+int trk_sort_by_id(trk_context *ctx);
+
 /* ------------------------------------------------------ batched ensembles */
 /* Track `n_variants` lattices that differ only in element parameter values
  * (error seeds, grids) in one launch.  `lattices` holds n_variants lattices of

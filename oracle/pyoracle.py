@@ -270,3 +270,111 @@ def track_refgpu(lattice, beam, n_passes, p_central, pass_offset=0):
     finally:
         nat.close()
     return rows, res.n_left, res.particle_passes
+
+
+# ------------------------------------------------------------ beam observers
+class BeamSums(ctypes.Structure):
+    """The layout of orc_beam_sums / trk_beam_sums / elegant's BEAM_SUMS(2)."""
+    _fields_ = [("centroid", ctypes.c_double * 7), ("sigma", (ctypes.c_double * 7) * 7),
+                ("sigman", (ctypes.c_double * 7) * 7), ("maxabs", ctypes.c_double * 7),
+                ("min", ctypes.c_double * 7), ("max", ctypes.c_double * 7), ("n_part", ctypes.c_long),
+                ("p0", ctypes.c_double), ("charge", ctypes.c_double)]
+
+
+def zero_beam_sums():
+    """Fresh sums as zero_beam_sums leaves them (src/compute_centroids.c:264-284)."""
+    s = BeamSums()
+    for j in range(7):
+        s.min[j] = 1.7976931348623157e308
+        s.max[j] = -1.7976931348623157e308
+    return s
+
+
+def sums_dict(s):
+    return {"centroid": np.array(s.centroid[:]), "sigma": np.array([r[:] for r in s.sigma]),
+            "sigman": np.array([r[:] for r in s.sigman]), "maxabs": np.array(s.maxabs[:]),
+            "min": np.array(s.min[:]), "max": np.array(s.max[:]), "n_part": s.n_part, "p0": s.p0,
+            "charge": s.charge}
+
+
+def _rows(beam):
+    rows = np.zeros((beam.shape[0], STRIDE), dtype=np.float64)
+    rows[:, :7] = beam[:, :7]
+    return rows
+
+
+def beam_centroids(beam):
+    """compute_centroids on the rows of `beam` (all survivors)."""
+    lib = load()
+    lib.orc_beam_centroids.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.c_long, ctypes.POINTER(ctypes.c_double)]
+    rows = _rows(beam)
+    c = np.zeros(6)
+    lib.orc_beam_centroids(rows.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), rows.shape[0],
+                           c.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    return c
+
+
+def accumulate_beam_sums(beam, sums, p_central, mp_charge=0.0, time=None, t_min=0.0, t_max=0.0, start_pid=-1,
+                         end_pid=-1, flags=0x8):
+    """accumulate_beam_sums on the rows of `beam` into `sums` (BeamSums)."""
+    lib = load()
+    DP = ctypes.POINTER(ctypes.c_double)
+    lib.orc_accumulate_beam_sums.argtypes = [DP, ctypes.c_long, ctypes.POINTER(BeamSums), ctypes.c_double,
+                                             ctypes.c_double, DP, ctypes.c_double, ctypes.c_double, ctypes.c_long,
+                                             ctypes.c_long, ctypes.c_uint]
+    rows = _rows(beam)
+    tv = None if time is None else np.ascontiguousarray(time, dtype=np.float64)
+    lib.orc_accumulate_beam_sums(rows.ctypes.data_as(DP), rows.shape[0], ctypes.byref(sums), p_central, mp_charge,
+                                 None if tv is None else tv.ctypes.data_as(DP), t_min, t_max, start_pid, end_pid,
+                                 flags)
+    return sums
+
+
+def match_energy(beam, p_central, change_beam):
+    """do_match_energy on the rows of `beam`; returns (beam, p_central)."""
+    lib = load()
+    DP = ctypes.POINTER(ctypes.c_double)
+    lib.orc_match_energy.argtypes = [DP, ctypes.c_long, DP, ctypes.c_int]
+    rows = _rows(beam)
+    pc = ctypes.c_double(p_central)
+    lib.orc_match_energy(rows.ctypes.data_as(DP), rows.shape[0], ctypes.byref(pc), int(change_beam))
+    out = beam.copy()
+    out[:, :7] = rows[:, :7]
+    return out, pc.value
+
+
+def _observe(lib, fn, beam, p_central, mp_charge, flags, start_pid, end_pid, t_min, t_max, repeats):
+    DP = ctypes.POINTER(ctypes.c_double)
+    f = getattr(lib, fn)
+    f.argtypes = [DP, ctypes.c_long, ctypes.c_double, ctypes.c_double, ctypes.c_uint, ctypes.c_long, ctypes.c_long,
+                  ctypes.c_double, ctypes.c_double, ctypes.c_int, DP, ctypes.POINTER(BeamSums)]
+    rows = _rows(beam)
+    c = np.zeros(6)
+    s = BeamSums()
+    _check(lib, f(rows.ctypes.data_as(DP), rows.shape[0], p_central, mp_charge, flags, start_pid, end_pid, t_min,
+                  t_max, repeats, c.ctypes.data_as(DP), ctypes.byref(s)))
+    return c, s
+
+
+def observe_ref(beam, p_central, mp_charge=0.0, flags=0x8, start_pid=-1, end_pid=-1, t_min=0.0, t_max=0.0,
+                repeats=1, exact_sums=False):
+    """elegant's own compute_centroids and accumulate_beam_sums (libref.so)
+    on the rows of `beam`: (centroid[6], BeamSums after `repeats`
+    accumulations from zero_beam_sums)."""
+    lib = load_ref()
+    lib.ref_set_exact_sums(1 if exact_sums else 0)
+    try:
+        return _observe(lib, "ref_observe", beam, p_central, mp_charge, flags, start_pid, end_pid, t_min, t_max,
+                        repeats)
+    finally:
+        lib.ref_set_exact_sums(0)
+
+
+def observe_refgpu(beam, p_central, mp_charge=0.0, flags=0x8, start_pid=-1, end_pid=-1, t_min=0.0, t_max=0.0,
+                   repeats=1):
+    """As observe_ref(), with the calls going through elegant's GPU hooks
+    into the CUDA library (libref_gpu.so)."""
+    lib = ctypes.CDLL(REF_GPU_LIB)
+    lib.trk_last_error.restype = ctypes.c_char_p
+    return _observe(lib, "refgpu_observe", beam, p_central, mp_charge, flags, start_pid, end_pid, t_min, t_max,
+                    repeats)

@@ -31,9 +31,12 @@
  * elegant_b200/hooks/trk_elegant_hooks.c, as do_tracking drives them
  * (src/do_tracking.c:413, :925-931, :3177-3178) */
 #include "gpu_base.h"
+#include "gpu_compute_centroids.h"
 #define REF_ENTRY refgpu_track
+#define REF_OBSERVE refgpu_observe
 #else
 #define REF_ENTRY ref_track
+#define REF_OBSERVE ref_observe
 #endif
 
 VMATRIX *drift_matrix(double length, long order);
@@ -404,6 +407,59 @@ int REF_ENTRY(const trk_lattice *l, double *rows, long np, long n_passes, long p
   free(lp);
   free(le);
   free_beamline(&bl);
+  return TRK_OK;
+}
+
+/* elegant's compute_centroids and accumulate_beam_sums (src/compute_centroids.c)
+ * on np surviving rows (ORC_STRIDE layout), the sums starting from
+ * zero_beam_sums and accumulated `repeats` times; flags: bits 0..2 are the
+ * reference's BEAM_SUMS_SPARSE/NOMINMAX/EXACTEMIT (EXACTEMIT sets
+ * exactNormalizedEmittance), bit 3 keeps the BEAM_SUMS2 part.  In the hook
+ * build the beam is handed to the device first (gpuBaseInit) and the calls
+ * go through the GPU hooks, as do_tracking's observers do on the GPU path. */
+int REF_OBSERVE(const double *rows, long np, double Po, double mp_charge, unsigned flags, long startPID, long endPID,
+                double tMin, double tMax, int repeats, double *centroid, orc_beam_sums *out) {
+  totalPropertiesPerParticle = REF_ROW;
+  sizeOfParticle = REF_ROW * sizeof(double);
+  double *buf = (double *)calloc((size_t)(np > 0 ? np : 1) * REF_ROW, sizeof(double));
+  double **coord = (double **)calloc(np > 0 ? np : 1, sizeof(double *));
+  for (long i = 0; i < np; i++) {
+    coord[i] = buf + (size_t)i * REF_ROW;
+    memcpy(coord[i], rows + (size_t)i * ORC_STRIDE, 7 * sizeof(double));
+    coord[i][7] = -1;
+  }
+  BEAM_SUMS sums;
+  BEAM_SUMS2 sums2;
+  memset(&sums, 0, sizeof(sums));
+  memset(&sums2, 0, sizeof(sums2));
+  sums.beamSums2 = (flags & 8u) ? &sums2 : NULL;
+  zero_beam_sums(&sums, 1);
+  exactNormalizedEmittance = (flags & 4u) ? 1 : 0;
+#ifdef REF_GPU_HOOKS
+  gpuBaseInit(coord, np, NULL, NULL, 1);
+  getGpuBase()->elementOnGpu = 1;
+#endif
+  compute_centroids(centroid, coord, np);
+  for (int r = 0; r < repeats; r++)
+    accumulate_beam_sums(&sums, coord, np, Po, mp_charge, NULL, tMin, tMax, startPID, endPID, flags & 7u);
+#ifdef REF_GPU_HOOKS
+  gpuBaseDealloc();
+#endif
+  exactNormalizedEmittance = 0;
+  memset(out, 0, sizeof(*out));
+  memcpy(out->centroid, sums.centroid, sizeof(out->centroid));
+  if (sums.beamSums2) {
+    memcpy(out->sigma, sums2.sigma, sizeof(out->sigma));
+    memcpy(out->sigman, sums2.sigman, sizeof(out->sigman));
+    memcpy(out->maxabs, sums2.maxabs, sizeof(out->maxabs));
+    memcpy(out->min, sums2.min, sizeof(out->min));
+    memcpy(out->max, sums2.max, sizeof(out->max));
+  }
+  out->n_part = sums.n_part;
+  out->p0 = sums.p0;
+  out->charge = sums.charge;
+  free(buf);
+  free(coord);
   return TRK_OK;
 }
 

@@ -1600,3 +1600,194 @@ int orc_track_element(const trk_lattice *l, int element, double *coord, long np,
   run_state_free(&rs);
   return rc;
 }
+
+/* ------------------------------------------------------ beam observers
+ * On rows of ORC_STRIDE doubles, survivors first (np of them).  Kahan sums
+ * of the reference become double-double sums in exact-sums mode, as above. */
+
+/* compute_centroids (src/compute_centroids.c:53-160, serial branch) */
+void orc_beam_centroids(const double *coord, long np, double *centroid) {
+  double sum[6], error[6], lo[6];
+  for (int c = 0; c < 6; c++)
+    sum[c] = centroid[c] = error[c] = lo[c] = 0;
+  for (long i = 0; i < np; i++)
+    for (int c = 0; c < 6; c++) {
+      const double v = coord[(size_t)i * ORC_STRIDE + c];
+      if (orc_exact_sums)
+        dd_acc(&sum[c], &lo[c], v);
+      else
+        sum[c] = kahan_plus(sum[c], v, &error[c]);
+    }
+  if (np)
+    for (int c = 0; c < 6; c++)
+      centroid[c] = sum[c] / np;
+}
+
+/* computeTimeCoordinates' per-particle time (src/trwake.c:533-548) */
+static double orc_time(const double *r, double Po) {
+  const double P = Po * (r[5] + 1);
+  return r[4] * sqrt(P * P + 1) / (TRK_C_MKS * P);
+}
+
+/* accumulate_beam_sums (src/compute_centroids.c:286-461, the serial
+ * version): sums of the chosen particles folded into *s.  The sigma sums
+ * are the reference's in-line Kahan sums (not switchable to double-double
+ * there either); only the centroid sums follow the exact-sums mode. */
+void orc_accumulate_beam_sums(const double *coord, long np, orc_beam_sums *s, double Po, double mp_charge,
+                              const double *time_value, double tMin, double tMax, long startPID, long endPID,
+                              unsigned flags) {
+  static const short sparse[7][7] = {{1, 1, 0, 0, 0, 1, 0}, {0, 1, 0, 0, 0, 1, 0}, {0, 0, 1, 1, 0, 1, 0},
+                                     {0, 0, 0, 1, 0, 1, 0}, {0, 0, 0, 0, 1, 1, 1}, {0, 0, 0, 0, 0, 1, 0},
+                                     {0, 0, 0, 0, 0, 0, 1}};
+  const int second = (flags & 0x8u) != 0, exact_emit = (flags & 0x4u) != 0;
+  double *t = (double *)malloc(sizeof(double) * (np > 0 ? np : 1));
+  short *chosen = (short *)malloc(sizeof(short) * (np > 0 ? np : 1));
+  double *pz = exact_emit ? (double *)malloc(sizeof(double) * (np > 0 ? np : 1)) : NULL;
+  for (long i = 0; i < np; i++) {
+    const double *r = coord + (size_t)i * ORC_STRIDE;
+    t[i] = time_value ? time_value[i] : orc_time(r, Po);
+    if (pz)
+      pz[i] = Po * (1 + r[5]) / sqrt(1 + r[1] * r[1] + r[3] * r[3]);
+  }
+  if (!s->n_part)
+    s->p0 = Po;
+  long npCount = 0;
+  if (np) {
+    for (long i = 0; i < np; i++) {
+      const double id = coord[(size_t)i * ORC_STRIDE + 6];
+      chosen[i] = ((startPID < 0 && endPID < 0) || (id >= startPID && id <= endPID)) &&
+                  (tMin >= tMax || (t[i] >= tMin && t[i] <= tMax));
+      npCount += chosen[i];
+    }
+    if (!(flags & 0x2u) && second)
+      for (int c = 0; c < 6; c++) {
+        if (c == 4)
+          continue;
+        for (long i = 0; i < np; i++)
+          if (chosen[i]) {
+            const double v = coord[(size_t)i * ORC_STRIDE + c];
+            if (fabs(v) > s->maxabs[c])
+              s->maxabs[c] = fabs(v);
+            if (v > s->max[c])
+              s->max[c] = v;
+            if (v < s->min[c])
+              s->min[c] = v;
+          }
+      }
+    double cen[7], cenn[7];
+    for (int c = 0; c < 7; c++) {
+      double err = 0, errn = 0, lo = 0, lon = 0;
+      cen[c] = cenn[c] = 0;
+      for (long i = 0; i < np; i++)
+        if (chosen[i]) {
+          const double *r = coord + (size_t)i * ORC_STRIDE;
+          if (exact_emit && (c == 1 || c == 3)) {
+            if (orc_exact_sums)
+              dd_acc(&cenn[c], &lon, r[c] * pz[i]);
+            else
+              cenn[c] = kahan_plus(cenn[c], r[c] * pz[i], &errn);
+          }
+          const double v = c < 6 ? r[c] : t[i];
+          if (orc_exact_sums)
+            dd_acc(&cen[c], &lo, v);
+          else
+            cen[c] = kahan_plus(cen[c], v, &err);
+        }
+      if (npCount) {
+        s->centroid[c] = (s->centroid[c] * s->n_part + cen[c]) / (s->n_part + npCount);
+        cen[c] /= npCount;
+        cenn[c] /= npCount;
+      }
+    }
+    for (int c = 0; c < 7; c++)
+      if (c != 1 && c != 3)
+        cenn[c] = cen[c];
+    for (long i = 0; i < np; i++)
+      t[i] -= cen[6];
+    if (!(flags & 0x2u) && second)
+      for (long i = 0; i < np; i++)
+        if (chosen[i]) {
+          double v = coord[(size_t)i * ORC_STRIDE + 4] - cen[4];
+          if (fabs(v) > s->maxabs[4])
+            s->maxabs[4] = fabs(v);
+          if (v > s->max[4])
+            s->max[4] = v;
+          if (v < s->min[4])
+            s->min[4] = v;
+          v = t[i];
+          if (fabs(v) > s->maxabs[6])
+            s->maxabs[6] = fabs(v);
+          if (v > s->max[6])
+            s->max[6] = v;
+          if (v < s->min[6])
+            s->min[6] = v;
+        }
+    if (second)
+      for (int a = 0; a < 7; a++)
+        for (int b = a; b < 7; b++) {
+          double Sij = 0, Sijn = 0, e = 0, en = 0;
+          if ((flags & 0x1u) && !sparse[a][b]) {
+            s->sigma[b][a] = s->sigma[a][b] = 0;
+            s->sigman[b][a] = s->sigman[a][b] = 0;
+            continue;
+          }
+          for (long i = 0; i < np; i++)
+            if (chosen[i]) {
+              const double *r = coord + (size_t)i * ORC_STRIDE;
+              const double bv = (a < 6 ? r[a] - cen[a] : t[i]) * (b < 6 ? r[b] - cen[b] : t[i]);
+              /* in-line Kahan (src/compute_centroids.c:424-436) */
+              double Y = bv + e, old = Sij;
+              Sij += Y;
+              e = Y - (Sij - old);
+              if (exact_emit) {
+                const double bn = (r[a] * (a == 1 || a == 3 ? pz[i] : 1) - cenn[a]) * (r[b] * (b == 1 || b == 3 ? pz[i] : 1));
+                double Yn = bn + en, oldn = Sijn;
+                Sijn += Yn;
+                en = Yn - (Sijn - oldn);
+              }
+            }
+          s->sigma[b][a] = (s->sigma[a][b] = (s->sigma[a][b] * s->n_part + Sij) / (s->n_part + npCount));
+          if (exact_emit)
+            s->sigman[b][a] = (s->sigman[a][b] = (s->sigman[a][b] * s->n_part + Sijn) / (s->n_part + npCount));
+        }
+  }
+  s->charge = mp_charge * npCount;
+  s->n_part += npCount;
+  free(t);
+  free(chosen);
+  free(pz);
+}
+
+/* do_match_energy (src/do_tracking.c:3376-3546, the serial branches) */
+void orc_match_energy(double *coord, long np, double *P_central, int change_beam) {
+  if (!np)
+    return;
+  double P_average = 0, error = 0, lo = 0;
+  for (long i = 0; i < np; i++) {
+    const double v = (*P_central) * (1 + coord[(size_t)i * ORC_STRIDE + 5]);
+    if (orc_exact_sums)
+      dd_acc(&P_average, &lo, v);
+    else
+      P_average = kahan_plus(P_average, v, &error);
+  }
+  P_average /= np;
+  if (!change_beam) {
+    if (fabs(P_average - (*P_central)) / (*P_central) > 1e-14) {
+      const double dp = (*P_central - P_average) / P_average;
+      const double dr = (*P_central) / P_average;
+      for (long i = 0; i < np; i++)
+        coord[(size_t)i * ORC_STRIDE + 5] = dp + coord[(size_t)i * ORC_STRIDE + 5] * dr;
+      *P_central = P_average;
+    }
+  } else {
+    const double dP_centroid = *P_central - P_average;
+    for (long i = 0; i < np; i++) {
+      double *r = coord + (size_t)i * ORC_STRIDE;
+      double P = (1 + r[5]) * (*P_central);
+      const double tt = r[4] / (P / sqrt(P * P + 1));
+      P += dP_centroid;
+      r[5] = (P - *P_central) / (*P_central);
+      r[4] = tt * (P / sqrt(P * P + 1));
+    }
+  }
+}

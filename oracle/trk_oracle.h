@@ -57,6 +57,22 @@ void orc_set_collective(int world, orc_gather_fn gather, orc_sum_fn sum);
 int orc_csbend_field_table(const trk_lattice *lattice, int element, double *Fx, double *Fy, int *expansionOrder1,
                            int *hasNormal, int *hasSkew);
 
+/* Beam observers on rows of ORC_STRIDE doubles, survivors first (np). */
+typedef struct {
+  double centroid[7];
+  double sigma[7][7];
+  double sigman[7][7];
+  double maxabs[7], min[7], max[7];
+  long n_part;
+  double p0;
+  double charge;
+} orc_beam_sums;
+void orc_beam_centroids(const double *coord, long np, double *centroid);
+void orc_accumulate_beam_sums(const double *coord, long np, orc_beam_sums *sums, double p_central, double mp_charge,
+                              const double *time_value, double t_min, double t_max, long start_pid, long end_pid,
+                              unsigned flags);
+void orc_match_energy(double *coord, long np, double *p_central, int change_beam);
+
 #ifdef __cplusplus
 }
 #endif
