@@ -64,6 +64,13 @@ class BeamSums(ctypes.Structure):
 SUMS_SPARSE, SUMS_NOMINMAX, SUMS_EXACT_NORMEMIT, SUMS_SECOND_ORDER = 0x1, 0x2, 0x4, 0x8
 
 
+class _ApertureSearch(ctypes.Structure):
+    _fields_ = [("lines", ctypes.c_int32), ("full_plane", ctypes.c_int32), ("slope_mode", ctypes.c_int32),
+                ("n_splits", ctypes.c_int32), ("nx", ctypes.c_long), ("xmax", ctypes.c_double),
+                ("ymax", ctypes.c_double), ("xpmax", ctypes.c_double), ("ypmax", ctypes.c_double),
+                ("split_fraction", ctypes.c_double), ("orbit", ctypes.c_double * 6)]
+
+
 class _Stats(ctypes.Structure):
     _fields_ = [("n_total", ctypes.c_long), ("n_left", ctypes.c_long), ("particle_passes", ctypes.c_long),
                 ("device_ms", ctypes.c_double), ("kernel_launches", ctypes.c_long), ("p_central", ctypes.c_double),
@@ -117,6 +124,8 @@ def _declare(lib):
         "trk_accumulate_beam_sums": (I, [P, ctypes.POINTER(BeamSums), D, D, DP, D, D, L, L, ctypes.c_uint]),
         "trk_match_energy": (I, [P, DP, I]),
         "trk_sort_by_id": (I, [P]),
+        "trk_aperture_search_lines": (I, [P, ctypes.POINTER(P), I, ctypes.POINTER(_ApertureSearch),
+                                          ctypes.POINTER(_Run), DP, DP, DP, DP, DP, DP, DP, DP]),
         "trk_adjoint_ensemble": (I, [P, ctypes.POINTER(P), I, ctypes.POINTER(L), ctypes.POINTER(_Run), D, DP, DP, I]),
         "trk_adjoint_param_count": (I, [P]),
         "trk_objective": (I, [P, D, DP]),
@@ -379,6 +388,41 @@ class Tracker:
         pc = ctypes.c_double(p_central)
         _check(self.lib, self.lib.trk_match_energy(self.ctx, ctypes.byref(pc), int(change_beam)))
         return pc.value
+
+    def aperture_search_lines(self, lattices, p_central, n_passes, lines, nx, xmax, ymax, n_splits=0,
+                              split_fraction=0.5, full_plane=0, slope_mode=0, xpmax=0.0, ypmax=0.0, orbit=None,
+                              fast=True, variant=-1):
+        """elegant's line-mode aperture search for one lattice or a list of
+        error-seed lattices, every point of a sweep in one launch.  Returns a
+        dict of (variants, lines) arrays x_limit, y_limit, x_clipped,
+        y_clipped, x_lost, y_lost, s_lost and area (variants,).  The loaded
+        beam is replaced."""
+        lats = lattices if isinstance(lattices, (list, tuple)) else [lattices]
+        nats = [self.native(lat) for lat in lats]
+        arr = (ctypes.c_void_p * len(nats))(*[n.ptr.value for n in nats])
+        S = _ApertureSearch()
+        S.lines, S.full_plane, S.slope_mode, S.n_splits = lines, full_plane, slope_mode, n_splits
+        S.nx, S.xmax, S.ymax, S.xpmax, S.ypmax = nx, xmax, ymax, xpmax, ypmax
+        S.split_fraction = split_fraction
+        for k, v in enumerate(np.zeros(6) if orbit is None else orbit):
+            S.orbit[k] = float(v)
+        run = _Run()
+        self.lib.trk_run_defaults(ctypes.byref(run))
+        run.p_central = p_central
+        run.n_passes = n_passes
+        run.fast_math = 1 if fast else 0
+        run.variant = variant
+        V = len(nats)
+        out = {k: np.zeros(V * lines) for k in ("x_limit", "y_limit", "x_clipped", "y_clipped", "x_lost", "y_lost",
+                                                 "s_lost")}
+        area = np.zeros(V)
+        _check(self.lib, self.lib.trk_aperture_search_lines(
+            self.ctx, arr, V, ctypes.byref(S), ctypes.byref(run), _dptr(out["x_limit"]), _dptr(out["y_limit"]),
+            _dptr(out["x_clipped"]), _dptr(out["y_clipped"]), _dptr(out["x_lost"]), _dptr(out["y_lost"]),
+            _dptr(out["s_lost"]), _dptr(area)))
+        res = {k: v.reshape(V, lines) for k, v in out.items()}
+        res["area"] = area
+        return res
 
     def sort_by_id(self):
         """Survivors in increasing particle ID (lost particles after them)."""

@@ -55,6 +55,10 @@ def objects():
     o = os.path.join(BUILD, "trk_compile.o")
     out.append((src, o, ["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math"] + INC +
                 ["-c", src, "-o", o]))
+    src = os.path.join(CSRC, "trk_aperture.cpp")
+    o = os.path.join(BUILD, "trk_aperture.o")
+    out.append((src, o, ["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math"] + INC +
+                ["-c", src, "-o", o]))
     src = os.path.join(CSRC, "trk_comm.cpp")
     o = os.path.join(BUILD, "trk_comm.o")
     out.append((src, o, ["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off"] + INC +

@@ -291,6 +291,35 @@ int trk_match_energy(trk_context *ctx, double *p_central, int change_beam);
  * their present order. */
 int trk_sort_by_id(trk_context *ctx);
 
+/* ----------------------------------------------------- aperture search */
+/* The line modes of elegant's aperture search (one-, two-, three- and
+ * n-line: do_aperture_search_line, src/aperture_search.c:985-1234). */
+typedef struct {
+  int32_t lines;          /* 1, 2, 3 (fixed directions) or more (evenly spread over the half or full plane) */
+  int32_t full_plane;     /* lines spread over 2 pi instead of pi */
+  int32_t slope_mode;     /* search in x', y' instead of x, y */
+  int32_t n_splits;       /* refinement sweeps after the first */
+  long nx;                /* points of the first sweep along each line (>= 2) */
+  double xmax, ymax;      /* extent of the first sweep (positions) */
+  double xpmax, ypmax;    /* extent of the first sweep (slopes, slope_mode) */
+  double split_fraction;  /* step reduction per refinement sweep, in (0, 1) */
+  double orbit[6];        /* added to every particle (offset_by_orbit; zeros otherwise) */
+} trk_aperture_search;
+/* For each of n_variants lattices (error seeds; one lattice: n_variants = 1)
+ * the largest surviving point along every line after run->n_passes passes,
+ * the search the reference does particle by particle, with every point of a
+ * sweep of every line and variant tracked in one launch.  Outputs, per
+ * variant v and line l at [v * lines + l]: x_limit, y_limit (the surviving
+ * point); x_clipped, y_clipped (the same after the reference's island
+ * clipping, trimApertureSearchResult); x_lost, y_lost, s_lost (the last
+ * loss seen on the line, DBL_MAX if none); area[v] (0 if the origin is lost
+ * or lines = 1).  Any output but x_limit, y_limit may be NULL.  The loaded
+ * beam is replaced. */
+int trk_aperture_search_lines(trk_context *ctx, const trk_lattice *const *lattices, int n_variants,
+                              const trk_aperture_search *search, const trk_run *run, double *x_limit,
+                              double *y_limit, double *x_clipped, double *y_clipped, double *x_lost, double *y_lost,
+                              double *s_lost, double *area);
+
 /* ------------------------------------------------------ batched ensembles */
 /* Track `n_variants` lattices that differ only in element parameter values
  * (error seeds, grids) in one launch.  `lattices` holds n_variants lattices of

@@ -378,3 +378,98 @@ def observe_refgpu(beam, p_central, mp_charge=0.0, flags=0x8, start_pid=-1, end_
     lib.trk_last_error.restype = ctypes.c_char_p
     return _observe(lib, "refgpu_observe", beam, p_central, mp_charge, flags, start_pid, end_pid, t_min, t_max,
                     repeats)
+
+
+# ------------------------------------------------------------ aperture search
+def aperture_search_lines(lattice, p_central, n_passes, lines, nx, xmax, ymax, n_splits=0, split_fraction=0.5,
+                          full_plane=0, slope_mode=0, xpmax=0.0, ypmax=0.0, orbit=None, area_fn=None):
+    """do_aperture_search_line (src/aperture_search.c:985-1234) restated
+    serially: one particle at a time along each line, each sweep stopping at
+    the first loss, tracked by the oracle.  Returns dict with x_limit,
+    y_limit, x_lost, y_lost, s_lost per line, origin_stable, and, if
+    area_fn is given (the trimming routine), the clipped limits and area."""
+    import math
+    orbit = np.zeros(6) if orbit is None else np.asarray(orbit, dtype=np.float64)
+    if lines == 1:
+        dxf, dyf = [1.0], [1.0]
+    elif lines == 2:
+        dxf, dyf = [-1.0, 1.0], [1.0, 1.0]
+    elif lines == 3:
+        dxf, dyf = [0.0, 1 / math.sqrt(2), 1.0], [1.0, 1 / math.sqrt(2), 0.0]
+    else:
+        dtheta = (math.pi if full_plane == 0 else 2 * math.pi) / (lines - 1)
+        dxf = [math.sin(-math.pi / 2 + dtheta * k) for k in range(lines)]
+        dyf = [math.cos(-math.pi / 2 + dtheta * k) for k in range(lines)]
+        dxf = [0.0 if abs(v) < 1e-6 else v for v in dxf]
+        dyf = [0.0 if abs(v) < 1e-6 else v for v in dyf]
+    big = 1.7976931348623157e308
+    origin_stable = False
+    xlim, ylim, xl_, yl_, sl_ = [], [], [], [], []
+    for line in range(lines):
+        if dxf[line] > 0:
+            xs = ys = -1.0
+        else:
+            ys = -1.0
+            xs = 1.0
+        xl = yl = sl = big
+        for split in range(n_splits + 1):
+            if split == 0:
+                ex, ey = (xpmax, ypmax) if slope_mode else (xmax, ymax)
+                dx = ex / (nx - 1) * dxf[line]
+                dy = ey / (nx - 1) * dyf[line]
+                x0 = y0 = 0.0
+                steps = nx
+            else:
+                x0, y0 = xs, ys
+                dx *= split_fraction
+                dy *= split_fraction
+                x0 += dx
+                y0 += dy
+                steps = max(1, int(1 / split_fraction - 0.5))
+            for index in range(steps):
+                if index != 0 or split != 0 or not origin_stable:
+                    b = np.zeros((1, 7))
+                    b[0, :6] = orbit
+                    if not slope_mode:
+                        b[0, 0] = index * dx + x0 + orbit[0]
+                        b[0, 2] = index * dy + y0 + orbit[2]
+                    else:
+                        b[0, 1] = index * dx + x0 + orbit[1]
+                        b[0, 3] = index * dy + y0 + orbit[3]
+                    b[0, 6] = 1
+                    rows, n_left, _ = track(lattice, b, n_passes, p_central)
+                    if n_left != 1:
+                        xl, yl, sl = rows[0, 0], rows[0, 2], rows[0, 4]
+                        break
+                if index == 0 and split == 0:
+                    origin_stable = True
+                xk, yk = x0 + index * dx, y0 + index * dy
+                if dxf[line]:
+                    if (dxf[line] > 0 and xs < xk) or (dxf[line] < 0 and xs > xk):
+                        xs, ys = xk, yk
+                elif ys < yk:
+                    xs, ys = xk, yk
+        xlim.append(xs)
+        ylim.append(ys)
+        xl_.append(xl)
+        yl_.append(yl)
+        sl_.append(sl)
+    out = {"x_limit": np.array(xlim), "y_limit": np.array(ylim), "x_lost": np.array(xl_), "y_lost": np.array(yl_),
+           "s_lost": np.array(sl_), "origin_stable": origin_stable, "dxf": np.array(dxf), "dyf": np.array(dyf)}
+    if area_fn is not None:
+        xc, yc = out["x_limit"].copy(), out["y_limit"].copy()
+        out["area"] = area_fn(xc, yc, out["dxf"], out["dyf"], full_plane) if origin_stable and lines > 1 else 0.0
+        out["x_clipped"], out["y_clipped"] = xc, yc
+    return out
+
+
+def trim_aperture_ref(x, y, dxf, dyf, full_plane):
+    """elegant's own trimApertureSearchResult (libref.so), clipping x, y in place."""
+    lib = load_ref()
+    DP = ctypes.POINTER(ctypes.c_double)
+    lib.trimApertureSearchResult.argtypes = [ctypes.c_long, DP, DP, DP, DP, ctypes.c_long]
+    lib.trimApertureSearchResult.restype = ctypes.c_double
+    dxf = np.ascontiguousarray(dxf, dtype=np.float64)
+    dyf = np.ascontiguousarray(dyf, dtype=np.float64)
+    return lib.trimApertureSearchResult(len(x), x.ctypes.data_as(DP), y.ctypes.data_as(DP), dxf.ctypes.data_as(DP),
+                                        dyf.ctypes.data_as(DP), int(full_plane))
