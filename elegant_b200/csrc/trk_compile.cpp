@@ -162,14 +162,17 @@ int compile_mult(const trk_elem *e, double Po, trk_op *op) {
   double KnL[3] = {0, 0, 0}, drift, tilt, dx, dy, dz, xkick = 0, ykick = 0, lEnd = 0;
   int order[3] = {0, 0, 0}, skew[3] = {0, 0, 0}, integ, expand;
   long n_kicks, nSlices;
-  int doEndDrift = 0;
+  int doEndDrift = 0, synch_rad = 0;
+  double elem_length = 0;
   double cfac = TRK_E_MKS / (TRK_ME_MKS * TRK_C_MKS * Po);
   switch (e->type) {
   case TRK_KQUAD: {
-    if (TRK_P(e, KQUAD_SYNCH_RAD) || TRK_P(e, KQUAD_ISR) || TRK_P(e, KQUAD_EDGE1_EFFECTS) ||
-        TRK_P(e, KQUAD_EDGE2_EFFECTS) || TRK_P(e, KQUAD_RADIAL) || TRK_P(e, KQUAD_MALIGN_METHOD))
-      return trk_set_error(TRK_ERR_UNSUPPORTED, "KQUAD %s: radiation, fringe, RADIAL and MALIGN_METHOD!=0 are not on this path",
+    if (TRK_P(e, KQUAD_ISR) || TRK_P(e, KQUAD_EDGE1_EFFECTS) || TRK_P(e, KQUAD_EDGE2_EFFECTS) ||
+        TRK_P(e, KQUAD_RADIAL) || TRK_P(e, KQUAD_MALIGN_METHOD))
+      return trk_set_error(TRK_ERR_UNSUPPORTED, "KQUAD %s: ISR, fringe, RADIAL and MALIGN_METHOD!=0 are not on this path",
                            e->name);
+    synch_rad = TRK_P(e, KQUAD_SYNCH_RAD) != 0;
+    elem_length = TRK_P(e, KQUAD_L);
     nSlices = (long)TRK_P(e, KQUAD_N_SLICES);
     n_kicks = (long)TRK_P(e, KQUAD_N_KICKS);
     expand = (int)TRK_P(e, KQUAD_EXPAND_HAMILTONIAN);
@@ -196,8 +199,10 @@ int compile_mult(const trk_elem *e, double Po, trk_op *op) {
     break;
   }
   case TRK_KSEXT:
-    if (TRK_P(e, KSEXT_SYNCH_RAD) || TRK_P(e, KSEXT_ISR) || TRK_P(e, KSEXT_MALIGN_METHOD))
-      return trk_set_error(TRK_ERR_UNSUPPORTED, "KSEXT %s: radiation and MALIGN_METHOD!=0 are not on this path", e->name);
+    if (TRK_P(e, KSEXT_ISR) || TRK_P(e, KSEXT_MALIGN_METHOD))
+      return trk_set_error(TRK_ERR_UNSUPPORTED, "KSEXT %s: ISR and MALIGN_METHOD!=0 are not on this path", e->name);
+    synch_rad = TRK_P(e, KSEXT_SYNCH_RAD) != 0;
+    elem_length = TRK_P(e, KSEXT_L);
     n_kicks = (long)TRK_P(e, KSEXT_N_KICKS);
     nSlices = (long)TRK_P(e, KSEXT_N_SLICES);
     expand = (int)TRK_P(e, KSEXT_EXPAND_HAMILTONIAN);
@@ -226,8 +231,10 @@ int compile_mult(const trk_elem *e, double Po, trk_op *op) {
     }
     break;
   case TRK_KOCT:
-    if (TRK_P(e, KOCT_SYNCH_RAD) || TRK_P(e, KOCT_ISR) || TRK_P(e, KOCT_MALIGN_METHOD))
-      return trk_set_error(TRK_ERR_UNSUPPORTED, "KOCT %s: radiation and MALIGN_METHOD!=0 are not on this path", e->name);
+    if (TRK_P(e, KOCT_ISR) || TRK_P(e, KOCT_MALIGN_METHOD))
+      return trk_set_error(TRK_ERR_UNSUPPORTED, "KOCT %s: ISR and MALIGN_METHOD!=0 are not on this path", e->name);
+    synch_rad = TRK_P(e, KOCT_SYNCH_RAD) != 0;
+    elem_length = TRK_P(e, KOCT_L);
     n_kicks = (long)TRK_P(e, KOCT_N_KICKS);
     nSlices = (long)TRK_P(e, KOCT_N_SLICES);
     expand = (int)TRK_P(e, KOCT_EXPAND_HAMILTONIAN);
@@ -325,6 +332,20 @@ int compile_mult(const trk_elem *e, double Po, trk_op *op) {
     flags |= MF_XKICK;
   if (yk)
     flags |= MF_YKICK;
+  /* classical radiation: rad_coef = e^2 Po^3 / (6 pi eps0 c^2 m), zero for
+   * elements shorter than 1e-6 m (src/multipole.c:755-763) */
+  if (synch_rad && !(elem_length < 1e-6)) {
+    const double rad_coef = (TRK_E_MKS * TRK_E_MKS) * (Po * Po * Po) /
+                            (6 * TRK_PI * TRK_EPSILON_O * (TRK_C_MKS * TRK_C_MKS) * TRK_ME_MKS);
+    if (rad_coef) {
+      flags |= MF_RAD;
+      op->d[MD_RAD] = rad_coef;
+      op->d[MD_XKR] = xk;
+      op->d[MD_YKR] = yk;
+      for (int st = 0; st < nSub && st < 8; st++)
+        op->d[MD_KFRAC + st] = kf[st];
+    }
+  }
   op->i[6] = flags;
   return TRK_OK;
 }
@@ -397,10 +418,10 @@ int edge_mode(int on, int effects, int edge_order, const char *name) {
 /* set-up of track_through_csbend (src/csbend.c:654-1078) */
 int compile_bend(const trk_lattice *l, int idx, double Po, trk_op *op, std::vector<double> &field) {
   const trk_elem *e = &l->e[idx];
-  if (TRK_P(e, CSBEND_SYNCH_RAD) || TRK_P(e, CSBEND_ISR) || TRK_P(e, CSBEND_REFERENCE_CORRECTION) ||
-      TRK_P(e, CSBEND_FSE_CORRECTION) || TRK_P(e, CSBEND_MALIGN_METHOD) || TRK_P(e, CSBEND_EXPAND_HAMILTONIAN))
+  if (TRK_P(e, CSBEND_ISR) || TRK_P(e, CSBEND_REFERENCE_CORRECTION) || TRK_P(e, CSBEND_FSE_CORRECTION) ||
+      TRK_P(e, CSBEND_MALIGN_METHOD) || TRK_P(e, CSBEND_EXPAND_HAMILTONIAN))
     return trk_set_error(TRK_ERR_UNSUPPORTED,
-                         "CSBEND %s: radiation, REFERENCE_CORRECTION, FSE_CORRECTION, MALIGN_METHOD!=0 and "
+                         "CSBEND %s: ISR, REFERENCE_CORRECTION, FSE_CORRECTION, MALIGN_METHOD!=0 and "
                          "EXPAND_HAMILTONIAN are not on this path",
                          e->name);
   const double L = TRK_P(e, CSBEND_L), ANGLE = TRK_P(e, CSBEND_ANGLE);
@@ -558,6 +579,15 @@ int compile_bend(const trk_lattice *l, int idx, double Po, trk_op *op, std::vect
     flags |= BF_ISR_ROUNDTRIP; /* isrConstant < 0 but nonzero (src/csbend.c:931-934) */
   if (dx || dy || dz || ttilt || etilt)
     flags |= BF_MISALIGN;
+  /* classical radiation (src/csbend.c:953-959) */
+  if (TRK_P(e, CSBEND_SYNCH_RAD)) {
+    const double rad_coef = (TRK_E_MKS * TRK_E_MKS) * (Po * Po * Po) * ((1 + fse) * (1 + fse)) /
+                            (6 * TRK_PI * TRK_EPSILON_O * (TRK_C_MKS * TRK_C_MKS) * TRK_ME_MKS * (rho0 * rho0));
+    if (rad_coef) {
+      flags |= BF_RAD;
+      d[BD_RAD] = rad_coef;
+    }
+  }
   const double rt = -tilt;
   if (rt) {
     flags |= BF_APTILT;
@@ -821,14 +851,14 @@ int trk_compile(const trk_lattice *l, double Po, CompiledLattice &out) {
       const int f = op.i[6];
       const int o = op.i[4] & 0xff;
       if (op.i[1] == 4 && !op.i[2] && op.d[MD_DRIFT] != 0 && o >= 1 && o <= 3 && !(op.i[5] & 1) &&
-          !(f & (MF_KNL1 | MF_KNL2 | MF_XKICK | MF_YKICK | MF_OFFSET | MF_TILT | MF_ENDDRIFT)))
+          !(f & (MF_KNL1 | MF_KNL2 | MF_XKICK | MF_YKICK | MF_OFFSET | MF_TILT | MF_ENDDRIFT | MF_RAD)))
         op.kind = OPK_MULT1;
     } else if (op.kind == OPK_BEND) {
       const bool e1_noop = op.i[5] == EDGE_NONE ||
                            (op.i[5] == EDGE_LIN1 && op.d[BD_TE1] == 0 && op.d[BD_PSI1] == 0 && op.d[BD_LIM1] <= 0);
       const bool e2_noop = op.i[6] == EDGE_NONE ||
                            (op.i[6] == EDGE_LIN1 && op.d[BD_TE2] == 0 && op.d[BD_PSI2] == 0 && op.d[BD_LIM2] <= 0);
-      const bool plain = op.i[1] == 4 && !(op.i[7] & (BF_MISALIGN | BF_APTILT)) && e1_noop && e2_noop;
+      const bool plain = op.i[1] == 4 && !(op.i[7] & (BF_MISALIGN | BF_APTILT | BF_RAD)) && e1_noop && e2_noop;
       if (plain && op.i[2] == 0)
         op.kind = OPK_DIPOLE;
       else if (plain && op.i[2] == 1 && op.i[3] == 5) {

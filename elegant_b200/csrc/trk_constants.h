@@ -22,6 +22,8 @@
 #define TRK_PIx2 6.283185307179586476925287
 #define TRK_PIo2 1.570796326794896619231322
 #define TRK_PARTICLE_REL_SIGN 1.0           /* electrons */
+#define TRK_MU_O (4 * TRK_PI * 1e-7)        /* vacuum permeability, as the SDDS constants define it */
+#define TRK_EPSILON_O (1 / (TRK_MU_O * TRK_C_MKS * TRK_C_MKS))
 
 /* Loss limits on |x|,|y| and |x'|,|y'| inside kick elements (src/track.h:1250-1251,
  * global_settings.c:61-62 defaults). */

@@ -195,7 +195,7 @@ __device__ __forceinline__ bool momenta_to_slopes(double &xp, double &yp, double
  * orders on this path, with the reference's term order and coefficients
  * (src/multipole.h:76-146). */
 __device__ __forceinline__ void mkick(double &qx, double &qy, double x, double y, int order, double K, int skew,
-                                      const double *coef) {
+                                      const double *coef, double *dqx = nullptr, double *dqy = nullptr) {
   double sFx, sFy;
   switch (order) {
   case 0:
@@ -233,6 +233,10 @@ __device__ __forceinline__ void mkick(double &qx, double &qy, double x, double y
   }
   qx -= K * sFy;
   qy += K * sFx;
+  if (dqx) { /* the kick returned for the radiation field (src/multipole.h:416-419) */
+    *dqx -= K * sFy;
+    *dqy += K * sFx;
+  }
 }
 
 __device__ __constant__ double c_coef[10]; /* expansion coefficients, orders 0..3 at n(n+1)/2 */
@@ -348,7 +352,7 @@ __device__ __forceinline__ bool op_mult(const trk_op *__restrict__ op, Part &p, 
     }
 #if TRK_FAST
     if (nSub == 4 && !expand && drift != 0 && (orders & 0xff) >= 1 && (orders & 0xff) <= 3 && !(skews & 1) &&
-        !(flags & (MF_KNL1 | MF_KNL2 | MF_XKICK | MF_YKICK))) {
+        !(flags & (MF_KNL1 | MF_KNL2 | MF_XKICK | MF_YKICK | MF_RAD))) {
       int done = 0, rc;
       const int o = orders & 0xff;
       if (o == 1)
@@ -394,12 +398,17 @@ __device__ __forceinline__ bool op_mult(const trk_op *__restrict__ op, Part &p, 
         }
         if (step == nSub - 1)
           break; /* kickFrac of the last substep is 0 for orders 2, 4, 6 */
+        double dqx = 0, dqy = 0;
+        const bool rad = (flags & MF_RAD) != 0;
         if (flags & MF_KNL0)
-          mkick(qx, qy, x, y, orders & 0xff, __ldg(&d[MD_KQ + step * 3 + 0]), skews & 1, c_coef);
+          mkick(qx, qy, x, y, orders & 0xff, __ldg(&d[MD_KQ + step * 3 + 0]), skews & 1, c_coef, rad ? &dqx : nullptr,
+                &dqy);
         if (flags & MF_KNL1)
-          mkick(qx, qy, x, y, (orders >> 8) & 0xff, __ldg(&d[MD_KQ + step * 3 + 1]), (skews >> 1) & 1, c_coef);
+          mkick(qx, qy, x, y, (orders >> 8) & 0xff, __ldg(&d[MD_KQ + step * 3 + 1]), (skews >> 1) & 1, c_coef,
+                rad ? &dqx : nullptr, &dqy);
         if (flags & MF_KNL2)
-          mkick(qx, qy, x, y, (orders >> 16) & 0xff, __ldg(&d[MD_KQ + step * 3 + 2]), (skews >> 2) & 1, c_coef);
+          mkick(qx, qy, x, y, (orders >> 16) & 0xff, __ldg(&d[MD_KQ + step * 3 + 2]), (skews >> 2) & 1, c_coef,
+                rad ? &dqx : nullptr, &dqy);
         if (flags & MF_XKICK)
           mkick(qx, qy, x, y, 0, __ldg(&d[MD_KX + step]), 0, c_coef);
         if (flags & MF_YKICK)
@@ -407,6 +416,28 @@ __device__ __forceinline__ bool op_mult(const trk_op *__restrict__ op, Part &p, 
         if (!momenta_to_slopes(xp, yp, qx, qy, dp, expand)) {
           ok = false;
           goto done;
+        }
+        if (rad && drift != 0) {
+          /* classical radiation after the kick (src/multipole.c:1359-1389):
+           * the field from the returned kick, dp -= rad_coef (1+dp)^2 F^2 ds */
+          qx /= (1 + dp);
+          qy /= (1 + dp);
+          const double deltaFactor = sqr(1 + dp);
+          const double kfs = __ldg(&d[MD_KFRAC + step]);
+          dqx /= kfs;
+          dqy /= kfs;
+          const double xkr = __ldg(&d[MD_XKR]), ykr = __ldg(&d[MD_YKR]);
+          const double F2 = sqr(dqx / drift - xkr / drift) + sqr(dqy / drift + ykr / drift);
+          double dsFactor = sqrt(1 + sqr(xp) + sqr(yp));
+          dsFactor *= drift * kfs;
+          dp -= __ldg(&d[MD_RAD]) * deltaFactor * F2 * dsFactor;
+          qx *= (1 + dp);
+          qy *= (1 + dp);
+          if (!momenta_to_slopes(xp, yp, qx, qy, dp, expand)) {
+            ok = false;
+            goto done;
+          }
+          continue;
         }
 #if !TRK_FAST
         /* the radiation block's (1 + dp) divide/multiply round trip, entered
@@ -443,7 +474,13 @@ __device__ __forceinline__ bool op_mult(const trk_op *__restrict__ op, Part &p, 
     p.xp = xp;
     p.y = y;
     p.yp = yp;
-    p.s += s;
+    if (flags & MF_RAD) {
+      /* the path length rescaled to the new velocity (src/multipole.c:1437-1441) */
+      const double p0 = Po * (1 + p.dp), p1 = Po * (1 + dp);
+      const double beta0 = p0 / sqrt(sqr(p0) + 1), beta1 = p1 / sqrt(sqr(p1) + 1);
+      p.s = beta1 * (p.s / beta0 + 2 * s / (beta0 + beta1));
+    } else
+      p.s += s;
     p.dp = dp;
     if (isnan(x) || isnan(xp) || isnan(y) || isnan(yp) || fabs(x) > TRK_COORD_LIMIT || fabs(y) > TRK_COORD_LIMIT ||
         fabs(xp) > TRK_SLOPE_LIMIT || fabs(yp) > TRK_SLOPE_LIMIT)
@@ -815,9 +852,7 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
   const double apc = __ldg(&d[BD_APC]), aps = __ldg(&d[BD_APS]);
 
   double x, xp, y, yp, s, dp;
-#if !TRK_FAST
   double dp0;
-#endif
   if (flags & BF_MISALIGN) {
     const double dxi = __ldg(&d[BD_DXI]), dyi = __ldg(&d[BD_DYI]), dzi = __ldg(&d[BD_DZI]);
     p.s += dzi * sqrt(1 + sqr(p.xp) + sqr(p.yp));
@@ -835,9 +870,7 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
   }
   s = p.s;
   dp = p.dp;
-#if !TRK_FAST
   dp0 = p.dp;
-#endif
   const double nidx = __ldg(&d[BD_N]);
   if (edge1)
     bend_edge(edge1, d, BD_E1, -1, rho_a, nidx, x, xp, y, yp, dp);
@@ -854,7 +887,7 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
   double dist = 0, dz_lost = 0;
   const double sl = __ldg(&d[BD_SLICE]);
 #if TRK_FAST
-  if (fmode == 0) {
+  if (fmode == 0 && !(flags & BF_RAD)) { /* the radiating dipole takes the general body */
     int done = 0;
     if (nSub == 4)
       ok = bend_dipole_fast<4>(d, nSlices, nSub, rho0, ap, aptilt, apc, aps, X, QX, Y, QY, D, dist, done);
@@ -952,6 +985,23 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
 #else
       QX += -ds * (1 + X / rho0) * Fy / rho_a;
       QY += ds * (1 + X / rho0) * Fx / rho_a;
+#endif
+      if (flags & BF_RAD) {
+        /* classical radiation after the kick (src/csbend.c:1627-1656) */
+        const double hX = 1 + X * __ldg(&d[BD_RHOINV]);
+        const double f = hX / sqrt(sqr(1 + D) - sqr(QX) - sqr(QY));
+        const double xpr = QX * f, ypr = QY * f;
+        const double dsFactor = sqrt(sqr(hX) + sqr(xpr) + sqr(ypr));
+        const double F2 = sqr(Fx) + sqr(Fy);
+        const double deltaFactor = sqr(1 + D);
+        QX /= (1 + D);
+        QY /= (1 + D);
+        D -= __ldg(&d[BD_RAD]) * deltaFactor * F2 * ds * dsFactor;
+        QX *= (1 + D);
+        QY *= (1 + D);
+        continue;
+      }
+#if !TRK_FAST
       if (flags & BF_ISR_ROUNDTRIP) {
         QX /= (1 + D);
         QY /= (1 + D);
@@ -985,7 +1035,11 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
     return false;
   }
 #if TRK_FAST
-  s += S;
+  if (flags & BF_RAD) {
+    const double p0 = Po * (1 + dp0), p1 = Po * (1 + D);
+    s = p1 / sqrt(sqr(p1) + 1) * s / (p0 / sqrt(sqr(p0) + 1)) + S;
+  } else
+    s += S;
 #else
   if (flags & BF_ISR_ROUNDTRIP) {
     double p0 = Po * (1 + dp0);

@@ -45,11 +45,13 @@ enum trk_op_kind {
 #define MF_KNL1 64
 #define MF_KNL2 128
 #define MF_APTILT 256 /* aperture check rotates by -TILT */
+#define MF_RAD 512    /* classical synchrotron radiation (SYNCH_RAD) */
 
 /* bend flags (i[7]) */
 #define BF_ISR_ROUNDTRIP 1 /* reference's (1+DPoP) divide/multiply round trip */
 #define BF_MISALIGN 2      /* entry/exit offsets or tilt not all zero */
 #define BF_APTILT 4
+#define BF_RAD 8 /* classical synchrotron radiation (SYNCH_RAD) */
 
 /* RF flags (i[3]) */
 #define RF_SAME_DGAMMA 1
@@ -98,6 +100,10 @@ typedef struct {
 #define MD_DRIFT 58 /* drift per slice (nonzero test) */
 #define MD_COEF 59  /* expansion coefficients for orders 0..3 packed: order n at MD_COEF + n*(n+1)/2 */
 #define MD_DZFULL 70 /* dzLoss of a particle that went through the whole body (substep lengths summed in order) */
+#define MD_KFRAC 71  /* 8 kick fractions of the integrator (radiation) */
+#define MD_RAD 79    /* rad_coef (src/multipole.c:755-756) */
+#define MD_XKR 80    /* xkick / n_parts, ykick / n_parts (radiation field strength) */
+#define MD_YKR 81
 /* i: 0 n_parts, 1 nSub, 2 expand, 3 maxOrder, 4 orders (o0 | o1<<8 | o2<<16), 5 skew bits, 6 flags */
 
 /* BEND */
@@ -140,6 +146,7 @@ typedef struct {
 #define BD_OMC 89     /* 8 values 1 - cos(dsh/rho0) = 2 sin^2(dsh/(2 rho0)) (fast build) */
 #define BD_C1 97      /* 8 values ds/rho_actual (fast build kick) */
 #define BD_C2 105     /* 8 values ds/(rho_actual rho0) (fast build kick) */
+#define BD_RAD 113    /* rad_coef (src/csbend.c:956-959) */
 /* i: 0 nSlices, 1 nSub, 2 field mode (0 dipole, 1 normal, 2 skew), 3 expansionOrder1,
  *    4 field pool offset, 5 edge1 mode, 6 edge2 mode, 7 flags */
 #define EDGE_NONE 0

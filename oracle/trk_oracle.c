@@ -370,6 +370,25 @@ static long multipole_tracking2(double *coord, long n_part, const trk_elem *e, d
     return n_part;
   }
   (void)lEffective;
+  {
+    /* SYNCH_RAD: rad_coef = e^2 Po^3 / (6 pi eps0 c^2 m), dropped for
+     * elements shorter than 1e-6 m (src/multipole.c:755-763) */
+    int synch = 0;
+    double length = 0;
+    if (e->type == TRK_KQUAD) {
+      synch = TRK_P(e, KQUAD_SYNCH_RAD) != 0;
+      length = TRK_P(e, KQUAD_L);
+    } else if (e->type == TRK_KSEXT) {
+      synch = TRK_P(e, KSEXT_SYNCH_RAD) != 0;
+      length = TRK_P(e, KSEXT_L);
+    } else {
+      synch = TRK_P(e, KOCT_SYNCH_RAD) != 0;
+      length = TRK_P(e, KOCT_L);
+    }
+    if (synch && !(length < 1e-6))
+      m.rad_coef = (TRK_E_MKS * TRK_E_MKS) * (Po * Po * Po) /
+                   (6 * TRK_PI * TRK_EPSILON_O * (TRK_C_MKS * TRK_C_MKS) * TRK_ME_MKS);
+  }
   if (m.integ_order != 2 && m.integ_order != 4 && m.integ_order != 6) {
     *err = 1;
     return n_part;
@@ -564,8 +583,8 @@ static int csbend_setup(const trk_lattice *l, int idx, double Po, orc_csbend_set
   const trk_elem *e = &l->e[idx];
   double b[9], c[9];
   memset(S, 0, sizeof(*S));
-  if (TRK_P(e, CSBEND_SYNCH_RAD) || TRK_P(e, CSBEND_ISR) || TRK_P(e, CSBEND_REFERENCE_CORRECTION) ||
-      TRK_P(e, CSBEND_FSE_CORRECTION) || TRK_P(e, CSBEND_MALIGN_METHOD) || TRK_P(e, CSBEND_EXPAND_HAMILTONIAN))
+  if (TRK_P(e, CSBEND_ISR) || TRK_P(e, CSBEND_REFERENCE_CORRECTION) || TRK_P(e, CSBEND_FSE_CORRECTION) ||
+      TRK_P(e, CSBEND_MALIGN_METHOD) || TRK_P(e, CSBEND_EXPAND_HAMILTONIAN))
     return 1;
   if (TRK_P(e, CSBEND_ANGLE) == 0) {
     S->is_drift = 1;
@@ -654,6 +673,10 @@ static int csbend_setup(const trk_lattice *l, int idx, double Po, orc_csbend_set
   /* isrConstant is nonzero (negative) whenever Po>0 even with ISR=0
    * (src/csbend.c:931-934), which enables the (1+DPoP) round trip */
   S->bd.isr_or_rad = Po > 0;
+  /* SYNCH_RAD (src/csbend.c:953-959) */
+  if (TRK_P(e, CSBEND_SYNCH_RAD))
+    S->bd.rad_coef = (TRK_E_MKS * TRK_E_MKS) * (Po * Po * Po) * ((1 + S->fse) * (1 + S->fse)) /
+                     (6 * TRK_PI * TRK_EPSILON_O * (TRK_C_MKS * TRK_C_MKS) * TRK_ME_MKS * (S->bd.rho0 * S->bd.rho0));
   csbend_field_table(&S->bd, b, c, S->h, (int)TRK_P(e, CSBEND_NONLINEAR), (long)TRK_P(e, CSBEND_EXPANSION_ORDER));
 
   double ttilt = S->tilt + S->etilt;

@@ -222,6 +222,7 @@ typedef struct {
   int integ_order;
   int expand;
   int maxOrder;
+  double rad_coef; /* classical radiation (SYNCH_RAD), 0 without */
 } orc_mult;
 
 /* integrate_kick_multipole_ordn (src/multipole.c:1099-1456) with
@@ -248,7 +249,7 @@ static int orc_integrate_kick_multipole(orc_r *coord, const orc_mult *m, double 
   s = 0;
   dp = coord[5];
   p = Po * (1 + dp);
-  (void)p;
+  orc_r beta0 = p / ORC_SQRT(orc_sqr(p) + 1);
 
   if (ORC_ISNAN(x) || ORC_ISNAN(xp) || ORC_ISNAN(y) || ORC_ISNAN(yp))
     return 0;
@@ -305,7 +306,25 @@ static int orc_integrate_kick_multipole(orc_r *coord, const orc_mult *m, double 
        * is nonzero whenever Po > 0 (negated when ISR is off, :757-760), so
        * after every kick the momenta are divided by (1 + dp) and multiplied
        * back, which can move them by an ulp, and the slopes are recomputed. */
-      if (drift) {
+      if (drift && m->rad_coef) {
+        /* the radiation block with SYNCH_RAD (src/multipole.c:1359-1389):
+         * field from the returned kick, dp -= rad_coef (1+dp)^2 F^2 ds */
+        qx /= (1 + dp);
+        qy /= (1 + dp);
+        orc_r deltaFactor = orc_sqr(1 + dp);
+        delta_qx /= kickFrac[step];
+        delta_qy /= kickFrac[step];
+        orc_r F2 = orc_sqr(delta_qx / drift - xkick / drift) + orc_sqr(delta_qy / drift + ykick / drift);
+        delta_qx = 0;
+        delta_qy = 0;
+        orc_r dsFactor = ORC_SQRT(1 + orc_sqr(xp) + orc_sqr(yp));
+        dsFactor *= drift * kickFrac[step];
+        dp -= m->rad_coef * deltaFactor * F2 * dsFactor;
+        qx *= (1 + dp);
+        qy *= (1 + dp);
+        if (!orc_momenta_to_slopes(&xp, &yp, qx, qy, dp, m->expand))
+          return 0;
+      } else if (drift) {
         qx /= (1 + dp);
         qy /= (1 + dp);
         qx *= (1 + dp);
@@ -328,7 +347,13 @@ static int orc_integrate_kick_multipole(orc_r *coord, const orc_mult *m, double 
   coord[1] = xp;
   coord[2] = y;
   coord[3] = yp;
-  coord[4] += s;
+  if (m->rad_coef) {
+    /* the path length rescaled to the new velocity (src/multipole.c:1437-1441) */
+    p = Po * (1 + dp);
+    orc_r beta1 = p / ORC_SQRT(orc_sqr(p) + 1);
+    coord[4] = beta1 * (coord[4] / beta0 + 2 * s / (beta0 + beta1));
+  } else
+    coord[4] += s;
   coord[5] = dp;
   if (ORC_ISNAN(x) || ORC_ISNAN(xp) || ORC_ISNAN(y) || ORC_ISNAN(yp))
     return 0;
@@ -348,6 +373,7 @@ typedef struct {
   int expansionOrder1;
   double Fx_xy[11][11], Fy_xy[11][11];
   int isr_or_rad; /* (rad_coef || isrConstant) in the reference: true for Po>0 */
+  double rad_coef; /* classical radiation (SYNCH_RAD), 0 without */
 } orc_bend;
 
 /* computeCSBENDFields (src/csbend.c:99-172) */
@@ -433,7 +459,20 @@ static int orc_integrate_csbend(orc_r *Qf, const orc_r *Qi, const orc_bend *b, c
       orc_csbend_fields(b, &Fx, &Fy, Qf[0], Qf[2]);
       Qf[1] += -ds * (1 + Qf[0] / rho0) * Fy / b->rho_actual;
       Qf[3] += ds * (1 + Qf[0] / rho0) * Fx / b->rho_actual;
-      if (b->isr_or_rad) {
+      if (b->isr_or_rad && b->rad_coef) {
+        /* src/csbend.c:1627-1656 with SYNCH_RAD */
+        orc_r f = (1 + Qf[0] * (1. / rho0)) / ORC_SQRT(orc_sqr(1 + Qf[5]) - orc_sqr(Qf[1]) - orc_sqr(Qf[3]));
+        orc_r xp = Qf[1] * f;
+        orc_r yp = Qf[3] * f;
+        orc_r dsFactor = ORC_SQRT(orc_sqr(1 + Qf[0] * (1. / rho0)) + orc_sqr(xp) + orc_sqr(yp));
+        orc_r F2 = orc_sqr(Fx) + orc_sqr(Fy);
+        orc_r deltaFactor = orc_sqr(1 + Qf[5]);
+        Qf[1] /= (1 + Qf[5]);
+        Qf[3] /= (1 + Qf[5]);
+        Qf[5] -= b->rad_coef * deltaFactor * F2 * ds * dsFactor;
+        Qf[1] *= (1 + Qf[5]);
+        Qf[3] *= (1 + Qf[5]);
+      } else if (b->isr_or_rad) {
         /* src/csbend.c:1628-1656: with SYNCH_RAD=0 and ISR=0 the reference
          * still divides and re-multiplies QX, QY by (1+DPoP) */
         Qf[1] /= (1 + Qf[5]);

@@ -36,6 +36,12 @@ ELEMENT_CASES = {
                            N_SLICES=8),
     "csbend_misaligned": single("CSBEND", L=1.0, ANGLE=0.05, DX=1e-4, DY=2e-4, DZ=-1e-4, TILT=0.02, N_SLICES=8),
     "csbend_order6": single("CSBEND", L=1.0, ANGLE=0.05, N_SLICES=4, INTEGRATION_ORDER=6),
+    "kquad_rad": single("KQUAD", L=0.3, K1=1.2, N_KICKS=8, SYNCH_RAD=1),
+    "kquad_rad_kicks": single("KQUAD", L=0.4, K1=-0.9, N_KICKS=12, HKICK=2e-5, VKICK=-1e-5, SYNCH_RAD=1),
+    "ksext_rad": single("KSEXT", L=0.2, K2=40.0, N_KICKS=4, SYNCH_RAD=1),
+    "koct_rad": single("KOCT", L=0.2, K3=500.0, SYNCH_RAD=1),
+    "csbend_rad": single("CSBEND", L=1.0, ANGLE=2 * math.pi / 80, N_KICKS=16, SYNCH_RAD=1),
+    "csbend_k1_rad": single("CSBEND", L=1.0, ANGLE=2 * math.pi / 280, K1=-0.4, N_KICKS=32, SYNCH_RAD=1),
     "rfca_thin": single("RFCA", L=0.0, VOLT=4e6, FREQ=352e6, PHASE=170.0),
     "rfca_long": single("RFCA", L=0.5, VOLT=2e6, FREQ=500e6, PHASE=160.0, N_KICKS=5, END1_FOCUS=1, END2_FOCUS=1),
     "rfca_tref": single("RFCA", L=0.0, VOLT=1e6, FREQ=352e6, PHASE=90.0, T_REFERENCE=1e-12),
