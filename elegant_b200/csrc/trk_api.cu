@@ -1005,9 +1005,9 @@ int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, 
             CUDA_TRY(cudaEventRecord(ctx->kev[2 * n_timed], ctx->stream));
           }
           if (fast)
-            trk_fast::launch_track(ta, variant, c.lean, ctx->np, max_blocks, ctx->stream);
+            trk_fast::launch_track(ta, variant, trk_lean_flavor(c), ctx->np, max_blocks, ctx->stream);
           else
-            trk_exact::launch_track(ta, variant, c.lean, ctx->np, max_blocks, ctx->stream);
+            trk_exact::launch_track(ta, variant, trk_lean_flavor(c), ctx->np, max_blocks, ctx->stream);
           if (timed)
             CUDA_TRY(cudaEventRecord(ctx->kev[2 * n_timed++ + 1], ctx->stream));
           ctx->last_launches++;
@@ -1181,9 +1181,9 @@ int trk_track_element(trk_context *ctx, const trk_lattice *lattice, int element,
       ta.pass_begin = pass;
       ta.pass_end = pass + 1;
       if (fast)
-        trk_fast::launch_track(ta, variant, c.lean, ctx->np, ctx->sm_count * 256, ctx->stream);
+        trk_fast::launch_track(ta, variant, trk_lean_flavor(c), ctx->np, ctx->sm_count * 256, ctx->stream);
       else
-        trk_exact::launch_track(ta, variant, c.lean, ctx->np, ctx->sm_count * 256, ctx->stream);
+        trk_exact::launch_track(ta, variant, trk_lean_flavor(c), ctx->np, ctx->sm_count * 256, ctx->stream);
       ctx->last_launches++;
     }
     CUDA_TRY(cudaGetLastError());
@@ -1275,7 +1275,7 @@ int trk_track_matrix(trk_context *ctx, int order, const double *C, const double 
  * TRK_N_VARIANTS), timed on a scratch copy of the beam. */
 static const int k_tune_candidates[] = {1, 4, 7, 8};
 
-static int ensemble_launches(trk_context *ctx, const TrackArgs &base, int nv, int nops, int variant, bool lean,
+static int ensemble_launches(trk_context *ctx, const TrackArgs &base, int nv, int nops, int variant, int lean,
                              bool fast, long p0, long n_passes, long chunk) {
   for (long pass = p0; pass < p0 + n_passes; pass += chunk) {
     TrackArgs ta = base;
@@ -1425,7 +1425,8 @@ int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int
       if ((rc = beam_snapshot(ctx, false)))
         return rc;
       CUDA_TRY(cudaEventRecord(ctx->ev0, ctx->stream));
-      if ((rc = ensemble_launches(ctx, base, n_variants, nops, cand, lean, fast, p0, tune_passes, chunk)))
+      if ((rc = ensemble_launches(ctx, base, n_variants, nops, cand, trk_lean_flavor(ctx->comp), fast, p0, tune_passes,
+                                  chunk)))
         return rc;
       CUDA_TRY(cudaEventRecord(ctx->ev1, ctx->stream));
       CUDA_TRY(cudaEventSynchronize(ctx->ev1));
@@ -1456,7 +1457,8 @@ int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    rc = ensemble_launches(ctx, base, n_variants, nops, variant, lean, fast, p0, run->n_passes, chunk);
+    rc = ensemble_launches(ctx, base, n_variants, nops, variant, trk_lean_flavor(ctx->comp), fast, p0, run->n_passes,
+                           chunk);
     cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
     if (rc)
       return rc;
@@ -1745,9 +1747,10 @@ static int adjoint_run(trk_context *ctx, const trk_lattice *const *lattices, int
     ta.pass_end = p0 + t + 1;
     if (nops > 0) {
       if (ensemble)
-        trk_fast::launch_track_ensemble(ta, d_off, nv, nops, shape, lean, np, ctx->sm_count * 256, ctx->stream);
+        trk_fast::launch_track_ensemble(ta, d_off, nv, nops, shape, trk_lean_flavor(c), np, ctx->sm_count * 256,
+                                        ctx->stream);
       else
-        trk_fast::launch_track(ta, shape, lean, np, ctx->sm_count * 256, ctx->stream);
+        trk_fast::launch_track(ta, shape, trk_lean_flavor(c), np, ctx->sm_count * 256, ctx->stream);
     }
   }
   CUDA_TRY(cudaGetLastError());

@@ -40,6 +40,10 @@ struct CompiledLattice {
  * B200 (fast build): (128 threads, 6 blocks/SM; 80 registers) for lean
  * lattices, (128, 5; 102 registers) for lean lattices with combined-function
  * bends, whose body spills at 80 registers, and (128, 4) otherwise. */
+/* lean kernel flavour of a compiled lattice: 0 general, 1 lean, 2 lean with
+ * combined-function bends */
+inline int trk_lean_flavor(const CompiledLattice &c) { return c.lean ? (c.has_cfbend ? 2 : 1) : 0; }
+
 inline int trk_default_variant(bool fast, const CompiledLattice &c) {
   if (fast && c.lean)
     return c.has_cfbend ? 4 : 7;

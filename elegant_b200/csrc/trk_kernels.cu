@@ -1672,7 +1672,11 @@ __device__ __forceinline__ bool after_element(const TrackArgs &a, const OpHead &
   return ok;
 }
 
-template <bool LEAN>
+/* LEAN: 0 every element kind; 1 the kinds of lean lattices (no general
+ * multipole or bend bodies); 2 as 1 plus combined-function bends, a flavour
+ * of its own because their body, inlined into the loop, costs lattices
+ * without them 3 % (register allocation of the whole loop) */
+template <int LEAN>
 __device__ __forceinline__ bool track_particle(const TrackArgs &a, const trk_op *__restrict__ ops, Part &p, long i) {
   for (long pass = a.pass_begin; pass < a.pass_end; pass++) {
     const int var = (pass == a.fresh_pass) ? 0 : 1;
@@ -1705,7 +1709,8 @@ __device__ __forceinline__ bool track_particle(const TrackArgs &a, const trk_op 
         break;
       case OPK_CFBEND:
 #if TRK_FAST
-        ok = op_cfbend_fast(op, p, a.Po, h.z_start, ap_in, a.field);
+        if (LEAN != 1)
+          ok = op_cfbend_fast(op, p, a.Po, h.z_start, ap_in, a.field);
 #else
         ok = op_bend(op, p, a.Po, h.z_start, ap_in, a.field);
 #endif
@@ -1747,7 +1752,7 @@ __device__ __forceinline__ int ens_variant(const long *__restrict__ offsets, int
 
 /* Kernel variants (block size, minimum resident blocks per SM) trade
  * registers against occupancy; trk_run.variant or the autotuner picks one. */
-template <int BLOCK, int MINB, bool LEAN>
+template <int BLOCK, int MINB, int LEAN>
 __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(TrackArgs a) {
   const long stride = (long)gridDim.x * blockDim.x;
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
@@ -2782,7 +2787,7 @@ int track_variant_block(int variant) {
   }
 }
 
-template <bool LEAN>
+template <int LEAN>
 static void launch_track_t(const TrackArgs &a, int variant, int grid, int block, cudaStream_t st) {
   switch (variant) {
   case 1:
@@ -2809,7 +2814,7 @@ static void launch_track_t(const TrackArgs &a, int variant, int grid, int block,
   }
 }
 
-void launch_track(const TrackArgs &a, int variant, bool lean, long n, int max_blocks, cudaStream_t st) {
+void launch_track(const TrackArgs &a, int variant, int lean, long n, int max_blocks, cudaStream_t st) {
 #if TRK_FAST
   if (lean && (variant == 5 || variant == 6)) {
     long g = (n + 2 * 128 - 1) / (2 * 128);
@@ -2832,10 +2837,16 @@ void launch_track(const TrackArgs &a, int variant, bool lean, long n, int max_bl
     g = 1;
   if (g > max_blocks)
     g = max_blocks;
+#if TRK_FAST
+  if (lean == 2)
+    launch_track_t<2>(a, variant, (int)g, block, st);
+  else if (lean)
+#else
   if (lean)
-    launch_track_t<true>(a, variant, (int)g, block, st);
+#endif
+    launch_track_t<1>(a, variant, (int)g, block, st);
   else
-    launch_track_t<false>(a, variant, (int)g, block, st);
+    launch_track_t<0>(a, variant, (int)g, block, st);
 }
 
 void launch_time_stats(const TimeStatsArgs &a, int grid, cudaStream_t st) {
@@ -2881,7 +2892,7 @@ void launch_rotate(const TrackArgs &a, double ca, double sa, int grid, cudaStrea
 int ensemble_variant_ok(int variant) { return variant >= 0 && variant < TRK_N_VARIANTS && variant != 5 && variant != 6; }
 
 void launch_track_ensemble(const TrackArgs &a, const long *offsets, int n_variants, int ops_per_variant, int variant,
-                           bool lean, long n, int max_blocks, cudaStream_t st) {
+                           int lean, long n, int max_blocks, cudaStream_t st) {
   TrackArgs e = a;
   e.ens_offsets = offsets;
   e.ens_variants = n_variants;

@@ -117,7 +117,7 @@ struct AdjArgs {
 #define TRK_DECLARE_LAUNCHERS(NS)                                                                            \
   namespace NS {                                                                                             \
   int track_variant_block(int variant);                                                                      \
-  void launch_track(const TrackArgs &a, int variant, bool lean, long n, int max_blocks, cudaStream_t st);    \
+  void launch_track(const TrackArgs &a, int variant, int lean, long n, int max_blocks, cudaStream_t st);     \
   void launch_time_stats(const TimeStatsArgs &a, int grid, cudaStream_t st);                                 \
   void launch_rf_fiducial(const double *stats, double omega, double t_reference, double *rf_phase, int slot, \
                           int *status, cudaStream_t st);                                                     \
@@ -133,7 +133,7 @@ struct AdjArgs {
   void launch_adjoint_record(const TrackArgs &a, const AdjArgs &g, cudaStream_t st);                         \
   void launch_adjoint_reverse(const TrackArgs &a, const AdjArgs &g, cudaStream_t st);                        \
   void launch_track_ensemble(const TrackArgs &a, const long *offsets, int n_variants, int ops_per_variant,   \
-                             int variant, bool lean, long n, int max_blocks, cudaStream_t st);              \
+                             int variant, int lean, long n, int max_blocks, cudaStream_t st);               \
   cudaError_t set_coefficients(const double *coef10);                                                        \
   }
 
