@@ -47,6 +47,9 @@ N_PARTICLES = 1_000_000
 # written at 2e5 particles (ncu; the coordinate writes stay in L2 and are
 # written back during later kernels)
 TRACK_DRAM_BYTES_PER_PARTICLE = 10.628e6 / 2e5
+# the same for the MBA ring (C5): 110.67 MB read + 120.53 MB written at 2e6 particles (ncu,
+# profiles/track_kernel_mba_ring.md)
+TRACK_DRAM_BYTES_PER_PARTICLE_C5 = (110.67e6 + 120.53e6) / 2e6
 
 WORKLOADS = {
     "c1": {"workload": "ring_fodo40_1e6", "particles": 1_000_000,
@@ -568,14 +571,18 @@ def run_gpu(args, rank, world, local):
         achieved = per_launch_flops / avg_launch_s / 1e12
         roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak if peak else None,
-                "traffic": (TRACK_DRAM_BYTES_PER_PARTICLE * (effort / world) / track_launches
-                            if args.workload == "c2" else None),
+                "traffic": ({"c2": TRACK_DRAM_BYTES_PER_PARTICLE, "c5": TRACK_DRAM_BYTES_PER_PARTICLE_C5}
+                            [args.workload] * (effort / world) / track_launches
+                            if args.workload in ("c2", "c5") else None),
                 "flops_per_particle_turn": fpt, "kernel": "track_kernel", "launches": track_launches,
                 "avg_launch_ms": avg_launch_s * 1e3,
                 "peak_source": "FP64 FMA peak measured in this run (independent dependent-FMA chains); "
                                "MEASURED_PEAKS.json has no FP64 figure",
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at 2e5 "
-                                  "particles, scaled by particles (profiles/track_kernel_ring_rf_wake.md)"}
+                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at 2e5 "
+                                   "particles, scaled by particles (profiles/track_kernel_ring_rf_wake.md)"
+                                   if args.workload != "c5" else
+                                   "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at 2e6 "
+                                   "particles, scaled by particles (profiles/track_kernel_mba_ring.md)")}
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         cpu = (cpu_baseline(cores=1, sample_particles=1500, sample_turns=2, workload="c5") if args.workload == "c5"
