@@ -41,7 +41,7 @@ class TrackingError(RuntimeError):
 class _Run(ctypes.Structure):
     _fields_ = [("p_central", ctypes.c_double), ("n_passes", ctypes.c_long), ("pass_offset", ctypes.c_long),
                 ("fast_math", ctypes.c_int32), ("block_size", ctypes.c_int32), ("compact_every", ctypes.c_int32),
-                ("variant", ctypes.c_int32), ("time_kernels", ctypes.c_int32)]
+                ("variant", ctypes.c_int32), ("time_kernels", ctypes.c_int32), ("isr_seed", ctypes.c_uint64)]
 
 
 class BeamSums(ctypes.Structure):
@@ -463,7 +463,8 @@ class Tracker:
             self._lat_cache[key] = nat
         return nat[1]
 
-    def track(self, lattice, n_passes, p_central, pass_offset=0, fast=True, variant=-1, time_kernels=False):
+    def track(self, lattice, n_passes, p_central, pass_offset=0, fast=True, variant=-1, time_kernels=False,
+              isr_seed=0):
         nat = self.native(lattice)
         run = _Run()
         self.lib.trk_run_defaults(ctypes.byref(run))
@@ -472,6 +473,7 @@ class Tracker:
         run.pass_offset = pass_offset
         run.fast_math = 1 if fast else 0
         run.variant = variant
+        run.isr_seed = isr_seed
         run.time_kernels = 1 if time_kernels else 0
         st = _Stats()
         _check(self.lib, self.lib.trk_track(self.ctx, nat.ptr, ctypes.byref(run), ctypes.byref(st)))

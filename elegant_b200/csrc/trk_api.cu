@@ -304,6 +304,8 @@ TrackArgs track_args(trk_context *ctx) {
   a.field = ctx->d_field;
   a.rf_phase = ctx->d_rf_phase;
   a.n = ctx->np;
+  a.id = c + 6 * cap;
+  a.isr_limit = 3.0; /* srGaussianLimit's default (src/track_data.c:65) */
   return a;
 }
 
@@ -976,6 +978,7 @@ int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, 
     TrackArgs ta = track_args(ctx);
     ta.fresh_pass = fresh;
     ta.Po = Po;
+    ta.isr_seed = run->isr_seed;
     const int max_blocks = ctx->sm_count * 256;
     std::vector<Step> steps;
     long pass = p0;
@@ -1175,6 +1178,7 @@ int trk_track_element(trk_context *ctx, const trk_lattice *lattice, int element,
       TrackArgs ta = track_args(ctx);
       ta.fresh_pass = pass;
       ta.Po = Po;
+      ta.isr_seed = run->isr_seed;
       ta.element_only = 1;
       ta.op_begin = k;
       ta.op_end = k + 1;
@@ -1406,6 +1410,7 @@ int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int
   TrackArgs base = track_args(ctx);
   base.fresh_pass = fresh;
   base.Po = Po;
+  base.isr_seed = run->isr_seed;
 
   /* launch shape: the caller's, else the autotuner's choice for this
    * (element count, particle count, build) */

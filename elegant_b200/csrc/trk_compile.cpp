@@ -162,16 +162,18 @@ int compile_mult(const trk_elem *e, double Po, trk_op *op) {
   double KnL[3] = {0, 0, 0}, drift, tilt, dx, dy, dz, xkick = 0, ykick = 0, lEnd = 0;
   int order[3] = {0, 0, 0}, skew[3] = {0, 0, 0}, integ, expand;
   long n_kicks, nSlices;
-  int doEndDrift = 0, synch_rad = 0;
+  int doEndDrift = 0, synch_rad = 0, isr = 0, isr1 = 1;
   double elem_length = 0;
   double cfac = TRK_E_MKS / (TRK_ME_MKS * TRK_C_MKS * Po);
   switch (e->type) {
   case TRK_KQUAD: {
-    if (TRK_P(e, KQUAD_ISR) || TRK_P(e, KQUAD_EDGE1_EFFECTS) || TRK_P(e, KQUAD_EDGE2_EFFECTS) ||
-        TRK_P(e, KQUAD_RADIAL) || TRK_P(e, KQUAD_MALIGN_METHOD))
-      return trk_set_error(TRK_ERR_UNSUPPORTED, "KQUAD %s: ISR, fringe, RADIAL and MALIGN_METHOD!=0 are not on this path",
+    if (TRK_P(e, KQUAD_EDGE1_EFFECTS) || TRK_P(e, KQUAD_EDGE2_EFFECTS) || TRK_P(e, KQUAD_RADIAL) ||
+        TRK_P(e, KQUAD_MALIGN_METHOD))
+      return trk_set_error(TRK_ERR_UNSUPPORTED, "KQUAD %s: fringe, RADIAL and MALIGN_METHOD!=0 are not on this path",
                            e->name);
     synch_rad = TRK_P(e, KQUAD_SYNCH_RAD) != 0;
+    isr = TRK_P(e, KQUAD_ISR) != 0;
+    isr1 = TRK_P(e, KQUAD_ISR1PART) != 0;
     elem_length = TRK_P(e, KQUAD_L);
     nSlices = (long)TRK_P(e, KQUAD_N_SLICES);
     n_kicks = (long)TRK_P(e, KQUAD_N_KICKS);
@@ -199,9 +201,11 @@ int compile_mult(const trk_elem *e, double Po, trk_op *op) {
     break;
   }
   case TRK_KSEXT:
-    if (TRK_P(e, KSEXT_ISR) || TRK_P(e, KSEXT_MALIGN_METHOD))
-      return trk_set_error(TRK_ERR_UNSUPPORTED, "KSEXT %s: ISR and MALIGN_METHOD!=0 are not on this path", e->name);
+    if (TRK_P(e, KSEXT_MALIGN_METHOD))
+      return trk_set_error(TRK_ERR_UNSUPPORTED, "KSEXT %s: MALIGN_METHOD!=0 is not on this path", e->name);
     synch_rad = TRK_P(e, KSEXT_SYNCH_RAD) != 0;
+    isr = TRK_P(e, KSEXT_ISR) != 0;
+    isr1 = TRK_P(e, KSEXT_ISR1PART) != 0;
     elem_length = TRK_P(e, KSEXT_L);
     n_kicks = (long)TRK_P(e, KSEXT_N_KICKS);
     nSlices = (long)TRK_P(e, KSEXT_N_SLICES);
@@ -231,9 +235,11 @@ int compile_mult(const trk_elem *e, double Po, trk_op *op) {
     }
     break;
   case TRK_KOCT:
-    if (TRK_P(e, KOCT_ISR) || TRK_P(e, KOCT_MALIGN_METHOD))
-      return trk_set_error(TRK_ERR_UNSUPPORTED, "KOCT %s: ISR and MALIGN_METHOD!=0 are not on this path", e->name);
+    if (TRK_P(e, KOCT_MALIGN_METHOD))
+      return trk_set_error(TRK_ERR_UNSUPPORTED, "KOCT %s: MALIGN_METHOD!=0 is not on this path", e->name);
     synch_rad = TRK_P(e, KOCT_SYNCH_RAD) != 0;
+    isr = TRK_P(e, KOCT_ISR) != 0;
+    isr1 = TRK_P(e, KOCT_ISR1PART) != 0;
     elem_length = TRK_P(e, KOCT_L);
     n_kicks = (long)TRK_P(e, KOCT_N_KICKS);
     nSlices = (long)TRK_P(e, KOCT_N_SLICES);
@@ -334,16 +340,27 @@ int compile_mult(const trk_elem *e, double Po, trk_op *op) {
     flags |= MF_YKICK;
   /* classical radiation: rad_coef = e^2 Po^3 / (6 pi eps0 c^2 m), zero for
    * elements shorter than 1e-6 m (src/multipole.c:755-763) */
-  if (synch_rad && !(elem_length < 1e-6)) {
-    const double rad_coef = (TRK_E_MKS * TRK_E_MKS) * (Po * Po * Po) /
-                            (6 * TRK_PI * TRK_EPSILON_O * (TRK_C_MKS * TRK_C_MKS) * TRK_ME_MKS);
-    if (rad_coef) {
+  /* and incoherent radiation: isr_coef = r_e sqrt(55/(24 sqrt 3) Po^5 137.0359895)
+   * (src/multipole.c:757-760) */
+  if ((synch_rad || isr) && !(elem_length < 1e-6)) {
+    const double rad_coef = synch_rad ? (TRK_E_MKS * TRK_E_MKS) * (Po * Po * Po) /
+                                          (6 * TRK_PI * TRK_EPSILON_O * (TRK_C_MKS * TRK_C_MKS) * TRK_ME_MKS)
+                                      : 0.0;
+    const double isr_coef = isr ? TRK_RE_MKS * std::sqrt(55.0 / (24 * std::sqrt(3.0)) * ipow_h(Po, 5) * 137.0359895)
+                                : 0.0;
+    if (rad_coef || isr_coef > 0) {
       flags |= MF_RAD;
       op->d[MD_RAD] = rad_coef;
       op->d[MD_XKR] = xk;
       op->d[MD_YKR] = yk;
       for (int st = 0; st < nSub && st < 8; st++)
         op->d[MD_KFRAC + st] = kf[st];
+      if (isr_coef > 0) {
+        flags |= MF_ISR;
+        op->d[MD_ISR] = isr_coef;
+        if (!isr1)
+          flags |= MF_ISR1OFF;
+      }
     }
   }
   op->i[6] = flags;
@@ -418,10 +435,10 @@ int edge_mode(int on, int effects, int edge_order, const char *name) {
 /* set-up of track_through_csbend (src/csbend.c:654-1078) */
 int compile_bend(const trk_lattice *l, int idx, double Po, trk_op *op, std::vector<double> &field) {
   const trk_elem *e = &l->e[idx];
-  if (TRK_P(e, CSBEND_ISR) || TRK_P(e, CSBEND_REFERENCE_CORRECTION) || TRK_P(e, CSBEND_FSE_CORRECTION) ||
-      TRK_P(e, CSBEND_MALIGN_METHOD) || TRK_P(e, CSBEND_EXPAND_HAMILTONIAN))
+  if (TRK_P(e, CSBEND_REFERENCE_CORRECTION) || TRK_P(e, CSBEND_FSE_CORRECTION) || TRK_P(e, CSBEND_MALIGN_METHOD) ||
+      TRK_P(e, CSBEND_EXPAND_HAMILTONIAN))
     return trk_set_error(TRK_ERR_UNSUPPORTED,
-                         "CSBEND %s: ISR, REFERENCE_CORRECTION, FSE_CORRECTION, MALIGN_METHOD!=0 and "
+                         "CSBEND %s: REFERENCE_CORRECTION, FSE_CORRECTION, MALIGN_METHOD!=0 and "
                          "EXPAND_HAMILTONIAN are not on this path",
                          e->name);
   const double L = TRK_P(e, CSBEND_L), ANGLE = TRK_P(e, CSBEND_ANGLE);
@@ -586,6 +603,18 @@ int compile_bend(const trk_lattice *l, int idx, double Po, trk_op *op, std::vect
     if (rad_coef) {
       flags |= BF_RAD;
       d[BD_RAD] = rad_coef;
+    }
+  }
+  /* incoherent radiation: isrConstant (src/csbend.c:961-964) */
+  if (TRK_P(e, CSBEND_ISR)) {
+    const double ra = std::fabs(rho_actual);
+    const double isr_constant =
+      TRK_RE_MKS * std::sqrt(55.0 / (24 * std::sqrt(3.0)) * ipow_h(Po, 5) * 137.0359895 / (ra * ra * ra));
+    if (isr_constant > 0) {
+      flags |= BF_RAD | BF_ISR;
+      d[BD_ISR] = isr_constant;
+      if (TRK_P(e, CSBEND_ISR1PART) == 0)
+        flags |= BF_ISR1OFF;
     }
   }
   const double rt = -tilt;

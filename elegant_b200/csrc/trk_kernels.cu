@@ -25,6 +25,7 @@
 
 #include "trk_constants.h"
 #include "trk_crmath.h"
+#include "trk_philox.h"
 
 #include "trk_kernels.h"
 #include "trk_ops.h"
@@ -298,9 +299,19 @@ __device__ __forceinline__ int mult_body_fast(const double *__restrict__ d, int 
 }
 #endif
 
+/* what an incoherent-radiation deviate is keyed by: the run's seed, the
+ * particle ID, the pass and the element (op index); `single`: one particle
+ * is tracked (ISR1PART=0 then turns ISR off, src/multipole.c:758) */
+struct IsrKey {
+  unsigned long long seed;
+  unsigned int id, pass, elem;
+  double limit;
+  bool single;
+};
+
 /* multipole_tracking2 + integrate_kick_multipole_ordn (src/multipole.c:660-1456) */
 __device__ __forceinline__ bool op_mult(const trk_op *__restrict__ op, Part &p, double Po, double z_start,
-                                        const trk_aperture *ap) {
+                                        const trk_aperture *ap, const IsrKey *isr = nullptr) {
   const int n_parts = __ldg(&op->i[0]);
   const int nSub = __ldg(&op->i[1]);
   const int expand = __ldg(&op->i[2]);
@@ -429,8 +440,17 @@ __device__ __forceinline__ bool op_mult(const trk_op *__restrict__ op, Part &p, 
           const double xkr = __ldg(&d[MD_XKR]), ykr = __ldg(&d[MD_YKR]);
           const double F2 = sqr(dqx / drift - xkr / drift) + sqr(dqy / drift + ykr / drift);
           double dsFactor = sqrt(1 + sqr(xp) + sqr(yp));
+          const double dsISRFactor = dsFactor * drift / (nSub - 1);
           dsFactor *= drift * kfs;
-          dp -= __ldg(&d[MD_RAD]) * deltaFactor * F2 * dsFactor;
+          const double rad_coef = __ldg(&d[MD_RAD]);
+          if (rad_coef != 0)
+            dp -= rad_coef * deltaFactor * F2 * dsFactor;
+          if ((flags & MF_ISR) && isr && !(isr->single && (flags & MF_ISR1OFF))) {
+            /* quantum excitation (src/multipole.c:1380-1381) */
+            const double g = trk_isr_gauss(isr->seed, isr->id, isr->pass, isr->elem, (unsigned)(i_kick * 8 + step),
+                                           isr->limit);
+            dp -= __ldg(&d[MD_ISR]) * deltaFactor * pow(F2, 0.75) * sqrt(dsISRFactor) * g;
+          }
           qx *= (1 + dp);
           qy *= (1 + dp);
           if (!momenta_to_slopes(xp, yp, qx, qy, dp, expand)) {
@@ -474,7 +494,7 @@ __device__ __forceinline__ bool op_mult(const trk_op *__restrict__ op, Part &p, 
     p.xp = xp;
     p.y = y;
     p.yp = yp;
-    if (flags & MF_RAD) {
+    if (__ldg(&d[MD_RAD]) != 0) {
       /* the path length rescaled to the new velocity (src/multipole.c:1437-1441) */
       const double p0 = Po * (1 + p.dp), p1 = Po * (1 + dp);
       const double beta0 = p0 / sqrt(sqr(p0) + 1), beta1 = p1 / sqrt(sqr(p1) + 1);
@@ -836,7 +856,8 @@ __device__ __forceinline__ void bend_edge(int mode, const double *__restrict__ d
 /* track_through_csbend (src/csbend.c:654-1434) with integrate_csbend_ordn
  * (src/csbend.c:1459-1720); no radiation, MALIGN_METHOD=0. */
 __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, double Po, double z_start,
-                                        const trk_aperture *ap, const double *__restrict__ field) {
+                                        const trk_aperture *ap, const double *__restrict__ field,
+                                        const IsrKey *isr = nullptr) {
   const double *d = op->d;
   const int nSlices = __ldg(&op->i[0]);
   const int nSub = __ldg(&op->i[1]);
@@ -994,9 +1015,18 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
         const double dsFactor = sqrt(sqr(hX) + sqr(xpr) + sqr(ypr));
         const double F2 = sqr(Fx) + sqr(Fy);
         const double deltaFactor = sqr(1 + D);
+        const double dsISR = sl / (nSub - 1);
         QX /= (1 + D);
         QY /= (1 + D);
-        D -= __ldg(&d[BD_RAD]) * deltaFactor * F2 * ds * dsFactor;
+        const double rad_coef = __ldg(&d[BD_RAD]);
+        if (rad_coef != 0)
+          D -= rad_coef * deltaFactor * F2 * ds * dsFactor;
+        if ((flags & BF_ISR) && isr && !(isr->single && (flags & BF_ISR1OFF))) {
+          /* quantum excitation (src/csbend.c:1649-1651) */
+          const double g =
+            trk_isr_gauss(isr->seed, isr->id, isr->pass, isr->elem, (unsigned)(i * 8 + j), isr->limit);
+          D -= __ldg(&d[BD_ISR]) * deltaFactor * pow(F2, 0.75) * sqrt(dsISR * dsFactor) * g;
+        }
         QX *= (1 + D);
         QY *= (1 + D);
         continue;
@@ -1719,12 +1749,20 @@ __device__ __forceinline__ bool track_particle(const TrackArgs &a, const trk_op 
         ok = op_rf(op, p, a.Po, h.z_end, a.rf_phase);
         break;
       case OPK_MULT:
-        if (!LEAN)
-          ok = op_mult(op, p, a.Po, h.z_start, ap_in);
-        break;
       case OPK_BEND:
-        if (!LEAN)
-          ok = op_bend(op, p, a.Po, h.z_start, ap_in, a.field);
+        if (!LEAN) {
+          IsrKey key;
+          key.seed = a.isr_seed;
+          key.id = (unsigned int)(long long)__ldg(&a.id[i]);
+          key.pass = (unsigned int)pass;
+          key.elem = (unsigned int)k;
+          key.limit = a.isr_limit;
+          key.single = a.n == 1;
+          if (h.kind == OPK_MULT)
+            ok = op_mult(op, p, a.Po, h.z_start, ap_in, &key);
+          else
+            ok = op_bend(op, p, a.Po, h.z_start, ap_in, a.field, &key);
+        }
         break;
       default:
         break;

@@ -41,6 +41,11 @@ struct TrackArgs {
   /* ensembles: variant offsets (n_variants + 1), records per variant; null for one lattice */
   const long *ens_offsets;
   int ens_variants, ens_ops;
+  /* incoherent synchrotron radiation: particle IDs (the deviates are keyed
+   * by ID), the run's seed and the truncation of the normal deviates */
+  const double *id;
+  unsigned long long isr_seed;
+  double isr_limit;
 };
 
 struct TimeStatsArgs {

@@ -45,13 +45,17 @@ enum trk_op_kind {
 #define MF_KNL1 64
 #define MF_KNL2 128
 #define MF_APTILT 256 /* aperture check rotates by -TILT */
-#define MF_RAD 512    /* classical synchrotron radiation (SYNCH_RAD) */
+#define MF_RAD 512    /* radiation block after each kick (SYNCH_RAD and/or ISR) */
+#define MF_ISR 1024   /* incoherent synchrotron radiation (ISR) */
+#define MF_ISR1OFF 2048 /* ISR1PART=0: no ISR when a single particle is tracked */
 
 /* bend flags (i[7]) */
 #define BF_ISR_ROUNDTRIP 1 /* reference's (1+DPoP) divide/multiply round trip */
 #define BF_MISALIGN 2      /* entry/exit offsets or tilt not all zero */
 #define BF_APTILT 4
-#define BF_RAD 8 /* classical synchrotron radiation (SYNCH_RAD) */
+#define BF_RAD 8       /* radiation block after each kick (SYNCH_RAD and/or ISR) */
+#define BF_ISR 16      /* incoherent synchrotron radiation (ISR) */
+#define BF_ISR1OFF 32  /* ISR1PART=0: no ISR when a single particle is tracked */
 
 /* RF flags (i[3]) */
 #define RF_SAME_DGAMMA 1
@@ -104,6 +108,7 @@ typedef struct {
 #define MD_RAD 79    /* rad_coef (src/multipole.c:755-756) */
 #define MD_XKR 80    /* xkick / n_parts, ykick / n_parts (radiation field strength) */
 #define MD_YKR 81
+#define MD_ISR 82    /* isr_coef (src/multipole.c:757) */
 /* i: 0 n_parts, 1 nSub, 2 expand, 3 maxOrder, 4 orders (o0 | o1<<8 | o2<<16), 5 skew bits, 6 flags */
 
 /* BEND */
@@ -147,6 +152,7 @@ typedef struct {
 #define BD_C1 97      /* 8 values ds/rho_actual (fast build kick) */
 #define BD_C2 105     /* 8 values ds/(rho_actual rho0) (fast build kick) */
 #define BD_RAD 113    /* rad_coef (src/csbend.c:956-959) */
+#define BD_ISR 114    /* isrConstant (src/csbend.c:961) */
 /* i: 0 nSlices, 1 nSub, 2 field mode (0 dipole, 1 normal, 2 skew), 3 expansionOrder1,
  *    4 field pool offset, 5 edge1 mode, 6 edge2 mode, 7 flags */
 #define EDGE_NONE 0

@@ -46,6 +46,7 @@
   X(KQUAD_SYNCH_RAD, "SYNCH_RAD", 0.0)             \
   X(KQUAD_INTEGRATION_ORDER, "INTEGRATION_ORDER", 4.0) \
   X(KQUAD_ISR, "ISR", 0.0)                         \
+  X(KQUAD_ISR1PART, "ISR1PART", 1.0)               \
   X(KQUAD_EDGE1_EFFECTS, "EDGE1_EFFECTS", 0.0)     \
   X(KQUAD_EDGE2_EFFECTS, "EDGE2_EFFECTS", 0.0)     \
   X(KQUAD_LEFFECTIVE, "LEFFECTIVE", 0.0)           \
@@ -76,6 +77,7 @@
   X(KSEXT_SYNCH_RAD, "SYNCH_RAD", 0.0)             \
   X(KSEXT_INTEGRATION_ORDER, "INTEGRATION_ORDER", 4.0) \
   X(KSEXT_ISR, "ISR", 0.0)                         \
+  X(KSEXT_ISR1PART, "ISR1PART", 1.0)               \
   X(KSEXT_EXPAND_HAMILTONIAN, "EXPAND_HAMILTONIAN", 0.0) \
   X(KSEXT_MALIGN_METHOD, "MALIGN_METHOD", 0.0)
 
@@ -96,6 +98,7 @@
   X(KOCT_INTEGRATION_ORDER, "INTEGRATION_ORDER", 4.0) \
   X(KOCT_SYNCH_RAD, "SYNCH_RAD", 0.0)              \
   X(KOCT_ISR, "ISR", 0.0)                          \
+  X(KOCT_ISR1PART, "ISR1PART", 1.0)                \
   X(KOCT_EXPAND_HAMILTONIAN, "EXPAND_HAMILTONIAN", 0.0) \
   X(KOCT_MALIGN_METHOD, "MALIGN_METHOD", 0.0)
 
@@ -151,6 +154,7 @@
   X(CSBEND_B7, "B7", 0.0)                          \
   X(CSBEND_B8, "B8", 0.0)                          \
   X(CSBEND_ISR, "ISR", 0.0)                        \
+  X(CSBEND_ISR1PART, "ISR1PART", 1.0)              \
   X(CSBEND_REFERENCE_CORRECTION, "REFERENCE_CORRECTION", 0.0) \
   X(CSBEND_FSE_CORRECTION, "FSE_CORRECTION", 0.0)  \
   X(CSBEND_MALIGN_METHOD, "MALIGN_METHOD", 0.0)

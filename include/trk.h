@@ -127,6 +127,8 @@ typedef struct {
   int32_t compact_every; /* compact survivors every N passes in fused runs (0 = never) */
   int32_t variant;       /* tracking-kernel variant (block size x occupancy); -1 = autotuned choice */
   int32_t time_kernels;  /* 1: bracket every tracking-kernel launch with CUDA events (trk_stats.track_ms) */
+  uint64_t isr_seed;     /* seed of the incoherent-radiation (ISR) deviates; each deviate is a function of
+                            (seed, particle ID, pass, element, kick), so runs repeat exactly */
 } trk_run;
 
 void trk_run_defaults(trk_run *run);

@@ -49,6 +49,7 @@ def load():
     lib.orc_csbend_field_table.argtypes = [P, I, DP, DP, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)]
     lib.orc_set_collective.argtypes = [I, ctypes.c_void_p, ctypes.c_void_p]
     lib.orc_set_exact_sums.argtypes = [I]
+    lib.orc_set_isr_seed.argtypes = [ctypes.c_ulonglong]
     lib.orc_set_cr_math.argtypes = [I]
     for f in ('orc_cr_sin', 'orc_cr_cos', 'orc_cr_asin', 'orc_cr_tan'):
         getattr(lib, f).argtypes = [D]
@@ -473,3 +474,8 @@ def trim_aperture_ref(x, y, dxf, dyf, full_plane):
     dyf = np.ascontiguousarray(dyf, dtype=np.float64)
     return lib.trimApertureSearchResult(len(x), x.ctypes.data_as(DP), y.ctypes.data_as(DP), dxf.ctypes.data_as(DP),
                                         dyf.ctypes.data_as(DP), int(full_plane))
+
+
+def set_isr_seed(seed):
+    """Seed of the oracle's incoherent-radiation deviates (as trk_run.isr_seed)."""
+    load().orc_set_isr_seed(int(seed))

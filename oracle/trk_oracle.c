@@ -388,6 +388,22 @@ static long multipole_tracking2(double *coord, long n_part, const trk_elem *e, d
     if (synch && !(length < 1e-6))
       m.rad_coef = (TRK_E_MKS * TRK_E_MKS) * (Po * Po * Po) /
                    (6 * TRK_PI * TRK_EPSILON_O * (TRK_C_MKS * TRK_C_MKS) * TRK_ME_MKS);
+    /* ISR: isr_coef = r_e sqrt(55/(24 sqrt 3) Po^5 137.0359895) (src/multipole.c:757-763) */
+    int isr = 0, isr1 = 1;
+    if (e->type == TRK_KQUAD) {
+      isr = TRK_P(e, KQUAD_ISR) != 0;
+      isr1 = TRK_P(e, KQUAD_ISR1PART) != 0;
+    } else if (e->type == TRK_KSEXT) {
+      isr = TRK_P(e, KSEXT_ISR) != 0;
+      isr1 = TRK_P(e, KSEXT_ISR1PART) != 0;
+    } else {
+      isr = TRK_P(e, KOCT_ISR) != 0;
+      isr1 = TRK_P(e, KOCT_ISR1PART) != 0;
+    }
+    if (isr && !(length < 1e-6)) {
+      m.isr_coef = TRK_RE_MKS * sqrt(55.0 / (24 * sqrt(3.0)) * orc_ipow(Po, 5) * 137.0359895);
+      m.isr1off = !isr1;
+    }
   }
   if (m.integ_order != 2 && m.integ_order != 4 && m.integ_order != 6) {
     *err = 1;
@@ -583,8 +599,8 @@ static int csbend_setup(const trk_lattice *l, int idx, double Po, orc_csbend_set
   const trk_elem *e = &l->e[idx];
   double b[9], c[9];
   memset(S, 0, sizeof(*S));
-  if (TRK_P(e, CSBEND_ISR) || TRK_P(e, CSBEND_REFERENCE_CORRECTION) || TRK_P(e, CSBEND_FSE_CORRECTION) ||
-      TRK_P(e, CSBEND_MALIGN_METHOD) || TRK_P(e, CSBEND_EXPAND_HAMILTONIAN))
+  if (TRK_P(e, CSBEND_REFERENCE_CORRECTION) || TRK_P(e, CSBEND_FSE_CORRECTION) || TRK_P(e, CSBEND_MALIGN_METHOD) ||
+      TRK_P(e, CSBEND_EXPAND_HAMILTONIAN))
     return 1;
   if (TRK_P(e, CSBEND_ANGLE) == 0) {
     S->is_drift = 1;
@@ -674,6 +690,12 @@ static int csbend_setup(const trk_lattice *l, int idx, double Po, orc_csbend_set
    * (src/csbend.c:931-934), which enables the (1+DPoP) round trip */
   S->bd.isr_or_rad = Po > 0;
   /* SYNCH_RAD (src/csbend.c:953-959) */
+  if (TRK_P(e, CSBEND_ISR)) {
+    /* isrConstant (src/csbend.c:961-964) */
+    const double ra = fabs(S->rho_actual);
+    S->bd.isr_constant = TRK_RE_MKS * sqrt(55.0 / (24 * sqrt(3.0)) * orc_ipow(Po, 5) * 137.0359895 / (ra * ra * ra));
+    S->bd.isr1off = TRK_P(e, CSBEND_ISR1PART) == 0;
+  }
   if (TRK_P(e, CSBEND_SYNCH_RAD))
     S->bd.rad_coef = (TRK_E_MKS * TRK_E_MKS) * (Po * Po * Po) * ((1 + S->fse) * (1 + S->fse)) /
                      (6 * TRK_PI * TRK_EPSILON_O * (TRK_C_MKS * TRK_C_MKS) * TRK_ME_MKS * (S->bd.rho0 * S->bd.rho0));
@@ -829,6 +851,7 @@ static long track_through_csbend(double *coord, long n_part, const trk_lattice *
     Qi[4] = 0;
     Qi[5] = dp;
     orc_to_dipole_canonical(Qi);
+    orc_isr.id = (uint32_t)(long long)c[6];
     int lost = !orc_integrate_csbend(Qf, Qi, &S.bd, &ap, &dz_lost);
     orc_from_dipole_canonical(Qf);
     if (lost) {
@@ -904,6 +927,7 @@ typedef struct {
  * GPU path computes, for bit-level checks of the downstream arithmetic. */
 static int orc_exact_sums = 0;
 void orc_set_exact_sums(int on) { orc_exact_sums = on; }
+void orc_set_isr_seed(unsigned long long seed) { orc_isr.seed = seed; }
 void orc_set_cr_math(int on) { orc_cr_math = on; }
 double orc_cr_sin(double x) { return trkcr_sin(x); }
 double orc_cr_cos(double x) { return trkcr_cos(x); }
@@ -1467,6 +1491,8 @@ static int track_one_element(const trk_lattice *l, int idx, double *coord, long 
   const trk_elem *e = &l->e[idx];
   long nLeft = nToTrack;
   int err = 0;
+  orc_isr.pass = (uint32_t)i_pass;
+  orc_isr.elem = (uint32_t)idx;
   switch (e->type) {
   case TRK_MARK:
   case TRK_CHARGE:
@@ -1556,6 +1582,7 @@ int orc_track(const trk_lattice *l, double *coord, long np, long n_passes, long 
   int rc;
   if (!l || (!coord && np) || !p_central)
     return TRK_ERR_ARG;
+  orc_isr.single = np == 1;
   if ((rc = run_state_init(l, np, &rs)))
     return rc;
   for (long ip = 0; ip < np; ip++) {

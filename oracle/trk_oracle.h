@@ -38,6 +38,10 @@ int orc_track_element(const trk_lattice *lattice, int element, double *coord, lo
  * rounded once (the GPU path's value) for bit-level checks. */
 void orc_set_exact_sums(int on);
 
+/* Seed of the incoherent-radiation deviates (ISR), drawn as the library
+ * draws them (elegant_b200/csrc/trk_philox.h). */
+void orc_set_isr_seed(unsigned long long seed);
+
 /* 0: libm sin/cos/asin; 1: correctly rounded ones (what the GPU parity build computes). */
 void orc_set_cr_math(int on);
 double orc_cr_sin(double x);

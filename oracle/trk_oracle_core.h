@@ -15,8 +15,20 @@
 #define TRK_ORACLE_CORE_H
 
 #include <math.h>
+#include <stdint.h>
 #include "trk_constants.h"
 #include "trk_crmath.h"
+#include "trk_philox.h"
+
+/* what an incoherent-radiation deviate is keyed by (the library draws the
+ * same deviates): the run's seed, the particle ID, the pass, the element
+ * index; `single`: one particle tracked (ISR1PART=0 then turns ISR off) */
+typedef struct {
+  uint64_t seed;
+  uint32_t id, pass, elem;
+  int single;
+} orc_isr_key;
+static orc_isr_key orc_isr;
 
 /* 0: the C library's sin/cos/asin (as the reference links them);
  * 1: correctly rounded double-double evaluations (trk_crmath.h), the values a
@@ -223,6 +235,8 @@ typedef struct {
   int expand;
   int maxOrder;
   double rad_coef; /* classical radiation (SYNCH_RAD), 0 without */
+  double isr_coef; /* incoherent radiation (ISR), 0 without */
+  int isr1off;     /* ISR1PART=0 */
 } orc_mult;
 
 /* integrate_kick_multipole_ordn (src/multipole.c:1099-1456) with
@@ -306,7 +320,7 @@ static int orc_integrate_kick_multipole(orc_r *coord, const orc_mult *m, double 
        * is nonzero whenever Po > 0 (negated when ISR is off, :757-760), so
        * after every kick the momenta are divided by (1 + dp) and multiplied
        * back, which can move them by an ulp, and the slopes are recomputed. */
-      if (drift && m->rad_coef) {
+      if (drift && (m->rad_coef || m->isr_coef > 0)) {
         /* the radiation block with SYNCH_RAD (src/multipole.c:1359-1389):
          * field from the returned kick, dp -= rad_coef (1+dp)^2 F^2 ds */
         qx /= (1 + dp);
@@ -318,8 +332,16 @@ static int orc_integrate_kick_multipole(orc_r *coord, const orc_mult *m, double 
         delta_qx = 0;
         delta_qy = 0;
         orc_r dsFactor = ORC_SQRT(1 + orc_sqr(xp) + orc_sqr(yp));
+        orc_r dsISRFactor = dsFactor * drift / (nSubsteps - 1);
         dsFactor *= drift * kickFrac[step];
-        dp -= m->rad_coef * deltaFactor * F2 * dsFactor;
+        if (m->rad_coef)
+          dp -= m->rad_coef * deltaFactor * F2 * dsFactor;
+        if (m->isr_coef > 0 && !(orc_isr.single && m->isr1off)) {
+          /* src/multipole.c:1380-1381, with the library's deviates */
+          const double g = trk_isr_gauss(orc_isr.seed, (uint32_t)(long long)ORC_VAL(coord[6]), orc_isr.pass,
+                                         orc_isr.elem, (uint32_t)(i_kick * 8 + step), 3.0);
+          dp -= m->isr_coef * deltaFactor * pow(ORC_VAL(F2), 0.75) * ORC_SQRT(dsISRFactor) * g;
+        }
         qx *= (1 + dp);
         qy *= (1 + dp);
         if (!orc_momenta_to_slopes(&xp, &yp, qx, qy, dp, m->expand))
@@ -374,6 +396,8 @@ typedef struct {
   double Fx_xy[11][11], Fy_xy[11][11];
   int isr_or_rad; /* (rad_coef || isrConstant) in the reference: true for Po>0 */
   double rad_coef; /* classical radiation (SYNCH_RAD), 0 without */
+  double isr_constant; /* incoherent radiation (ISR), 0 without */
+  int isr1off;         /* ISR1PART=0 */
 } orc_bend;
 
 /* computeCSBENDFields (src/csbend.c:99-172) */
@@ -459,7 +483,7 @@ static int orc_integrate_csbend(orc_r *Qf, const orc_r *Qi, const orc_bend *b, c
       orc_csbend_fields(b, &Fx, &Fy, Qf[0], Qf[2]);
       Qf[1] += -ds * (1 + Qf[0] / rho0) * Fy / b->rho_actual;
       Qf[3] += ds * (1 + Qf[0] / rho0) * Fx / b->rho_actual;
-      if (b->isr_or_rad && b->rad_coef) {
+      if (b->isr_or_rad && (b->rad_coef || b->isr_constant > 0)) {
         /* src/csbend.c:1627-1656 with SYNCH_RAD */
         orc_r f = (1 + Qf[0] * (1. / rho0)) / ORC_SQRT(orc_sqr(1 + Qf[5]) - orc_sqr(Qf[1]) - orc_sqr(Qf[3]));
         orc_r xp = Qf[1] * f;
@@ -467,9 +491,17 @@ static int orc_integrate_csbend(orc_r *Qf, const orc_r *Qi, const orc_bend *b, c
         orc_r dsFactor = ORC_SQRT(orc_sqr(1 + Qf[0] * (1. / rho0)) + orc_sqr(xp) + orc_sqr(yp));
         orc_r F2 = orc_sqr(Fx) + orc_sqr(Fy);
         orc_r deltaFactor = orc_sqr(1 + Qf[5]);
+        double dsISR = s / (nSubsteps - 1);
         Qf[1] /= (1 + Qf[5]);
         Qf[3] /= (1 + Qf[5]);
-        Qf[5] -= b->rad_coef * deltaFactor * F2 * ds * dsFactor;
+        if (b->rad_coef)
+          Qf[5] -= b->rad_coef * deltaFactor * F2 * ds * dsFactor;
+        if (b->isr_constant > 0 && !(orc_isr.single && b->isr1off)) {
+          /* src/csbend.c:1649-1651, with the library's deviates */
+          const double g =
+            trk_isr_gauss(orc_isr.seed, orc_isr.id, orc_isr.pass, orc_isr.elem, (uint32_t)(i * 8 + j), 3.0);
+          Qf[5] -= b->isr_constant * deltaFactor * pow(ORC_VAL(F2), 0.75) * ORC_SQRT(dsISR * dsFactor) * g;
+        }
         Qf[1] *= (1 + Qf[5]);
         Qf[3] *= (1 + Qf[5]);
       } else if (b->isr_or_rad) {
