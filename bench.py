@@ -57,6 +57,9 @@ WORKLOADS = {
     "c2": {"workload": "ring_rf_wake_fodo40_1e6", "particles": 1_000_000,
            "lattice": "40 FODO cells + KSEXT, RFCA, WAKE", "wake_bins": 2000, "wake_points": 4096,
            "wake_dt_s": 5e-14, "charge_c": 1e-9},
+    "rad": {"workload": "ring_rf_wake_fodo40_radiation_1e6", "particles": 1_000_000,
+            "lattice": "40 FODO cells + KSEXT, RFCA, WAKE; SYNCH_RAD=1 and ISR=1 on every KQUAD, KSEXT, CSBEND",
+            "wake_bins": 2000, "wake_points": 4096, "wake_dt_s": 5e-14, "charge_c": 1e-9},
     "c5": {"workload": "mba_ring_rf_wake_trwake_1e7", "particles": 10_000_000,
            "lattice": "40 MBA cells (7 CSBEND K1 N_KICKS=32, 12 KQUAD, 6 KSEXT, 2 KOCT, 27 DRIF) + RFCA, WAKE, "
                       "TRWAKE", "wake_bins": 4000, "wake_points": 4096, "wake_dt_s": 2.5e-13, "charge_c": 1e-9,
@@ -73,6 +76,13 @@ def workload_config(n_particles, workload="c2"):
 
 def workload_lattice(workload):
     from elegant_b200 import configs
+    if workload == "rad":
+        lat = configs.c2_lattice()
+        for e in lat.elements:
+            if e[0] in ("KQUAD", "KSEXT", "CSBEND"):
+                e[2]["SYNCH_RAD"] = 1.0
+                e[2]["ISR"] = 1.0
+        return lat
     return {"c1": configs.c1_lattice, "c2": configs.c2_lattice, "c5": configs.c5_lattice}[workload]()
 
 
@@ -233,10 +243,13 @@ def main():
                     help="particles per GPU (1e6 for c1/c2, 1e7 for c5, 1e5 for c4)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--exact", action="store_true", help="parity build instead of the fast build")
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "c5grad"],
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "c5grad", "rad", "observe",
+                                                       "da"],
                     help="c2: ring with RF and wake (the benchmark); c1: plain FODO ring (profiling); "
                          "c5: large MBA ring with RF, WAKE and TRWAKE, 1e7 particles; c5grad: batched "
-                         "adjoint over 32 error seeds of the MBA ring against finite differences; "
+                         "adjoint over 32 error seeds of the MBA ring against finite differences; rad: c2 with "
+                         "SYNCH_RAD and ISR on every magnet; observe: beam sums of 1e7 particles (HBM); da: "
+                         "dynamic-aperture line search over 256 error seeds; "
                          "c3: batched error-seed ensemble on dynamic-aperture grids; c4: adjoint gradient "
                          "against finite differences")
     ap.add_argument("--variants", type=int, default=256, help="c3: lattice variants")
@@ -253,6 +266,10 @@ def main():
         return run_gradient(args, rank)
     if args.workload == "c5grad":
         return run_gradient_ensemble(args, rank)
+    if args.workload == "observe":
+        return run_observe(args, rank)
+    if args.workload == "da":
+        return run_da(args, rank)
     return run_gpu(args, rank, world, local)
 
 
@@ -480,6 +497,104 @@ def run_gradient_ensemble(args, rank):
     return 0
 
 
+def _measured_hbm_gbs():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            v = json.load(f).get("hbm_gbs")
+            if v:
+                return float(v), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback (earlier measurement on this pool)"
+
+
+def run_observe(args, rank):
+    """Beam observers on the device beam: trk_accumulate_beam_sums (centroids,
+    7x7 second moments, extremes; elegant's accumulate_beam_sums) on 1e7
+    particles of the MBA ring's beam.  HBM-bound: two passes over x, x', y,
+    y', s, delta, id and the loss word, 60 B per particle each.  Metric:
+    particles summed per second; roofline in GB/s against the measured HBM
+    copy bandwidth."""
+    import torch
+    from elegant_b200 import BeamSums, SUMS_SECOND_ORDER, Tracker, configs
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(0)
+    n = args.particles or 10_000_000
+    beam = configs.c5_beam(n, seed=1)
+    with Tracker(0) as trk:
+        trk.load(beam)
+        stream = torch.cuda.ExternalStream(trk.stream(), device="cuda:0")
+        for _ in range(max(args.warmup, 3)):
+            trk.accumulate_beam_sums(BeamSums.zeroed(), configs.P_CENTRAL, flags=SUMS_SECOND_ORDER)
+        ms = []
+        with ClockSampler(0) as clocks:
+            for _ in range(args.steps):
+                s = BeamSums.zeroed()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                trk.accumulate_beam_sums(s, configs.P_CENTRAL, flags=SUMS_SECOND_ORDER)
+                e1.record(stream)
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+        c_ms = []
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            trk.centroids()
+            e1.record(stream)
+            e1.synchronize()
+            c_ms.append(e0.elapsed_time(e1))
+    t = float(np.median(ms)) / 1e3
+    tc = float(np.median(c_ms)) / 1e3
+    peak, src = _measured_hbm_gbs()
+    algo = 2 * 60.0 * n
+    line = {"metric": "beam sums (accumulate_beam_sums) particles/s", "value": n / t, "unit": "particles/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": t * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Gaussian beam)",
+            "config": {"workload": "observe_beam_sums_1e7", "particles": n, "second_order": True},
+            "roofline": {"bound": "hbm", "achieved": algo / t / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": algo / t / 1e9 / peak, "traffic": None, "peak_source": src,
+                         "bytes_per_particle": 120},
+            "centroids_ms": tc * 1e3, "centroids_gbs": 60.0 * n / tc / 1e9, "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_da(args, rank):
+    """Dynamic-aperture line search over error seeds (trk_aperture_search_lines):
+    256 seeds of the FODO+sextupole ring with its 25 mm aperture, 11 lines of
+    41 points to 20 mm x 10 mm, two refinement sweeps, `turns` turns.  Metric:
+    particle-turns/s of the whole search (every tracked point x turns over the
+    search's wall time, host logic included)."""
+    import torch
+    from elegant_b200 import Tracker, configs
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(0)
+    turns = args.turns or 1024
+    seeds = min(args.variants, 256)
+    lats = [configs.c3_variant(seed=v) for v in range(seeds)]
+    kw = dict(lines=11, nx=41, xmax=0.02, ymax=0.01, n_splits=2, split_fraction=0.5)
+    points = seeds * kw["lines"] * (kw["nx"] + 2 * max(1, int(1 / kw["split_fraction"] - 0.5)))
+    with Tracker(0) as trk:
+        trk.aperture_search_lines(lats, configs.P_CENTRAL, 4, **kw)  # autotune, warm
+        torch.cuda.synchronize()
+        with ClockSampler(0) as clocks:
+            t0 = time.perf_counter()
+            r = trk.aperture_search_lines(lats, configs.P_CENTRAL, turns, **kw)
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
+    line = {"metric": "aperture-search particle-turns/s", "value": points * turns / wall, "unit": "particle-turns/s",
+            "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": wall * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded error seeds)",
+            "config": {"workload": "da_search_256x11_lines", "seeds": seeds, "turns": turns, **kw,
+                       "points_tracked": points},
+            "search_s": wall, "mean_area_m2": float(np.mean(r["area"])), "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_gpu(args, rank, world, local):
     import torch
     from elegant_b200 import Tracker, configs
@@ -563,9 +678,10 @@ def run_gpu(args, rank, world, local):
     peak = measure_fp64_peak(local)
     roof = None
     if flops and track_launches:
-        fpt = flops["flops_per_particle_turn"][args.workload]
+        # the radiating ring is counted as the plain one (the radiation's own flops are not counted)
+        fpt = flops["flops_per_particle_turn"]["c2" if args.workload == "rad" else args.workload]
         # the wakes' per-particle work runs in the wake kernels
-        fpt -= {"c1": 0, "c2": 1, "c5": 2}[args.workload] * flops["per_particle"]["WAKE"]["total"]
+        fpt -= {"c1": 0, "c2": 1, "rad": 1, "c5": 2}[args.workload] * flops["per_particle"]["WAKE"]["total"]
         per_launch_flops = fpt * (effort / world) / track_launches
         avg_launch_s = track_ms / track_launches / 1e3
         achieved = per_launch_flops / avg_launch_s / 1e12
@@ -584,7 +700,9 @@ def run_gpu(args, rank, world, local):
                                    "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at 2e6 "
                                    "particles, scaled by particles (profiles/track_kernel_mba_ring.md)")}
     cpu = None
-    if not args.no_cpu_baseline and world == 1:
+    # no CPU leg for the radiating ring: the reference's ISR deviates come from the SDDS toolkit's
+    # generator, which is not in the reference tree
+    if not args.no_cpu_baseline and world == 1 and args.workload != "rad":
         cpu = (cpu_baseline(cores=1, sample_particles=1500, sample_turns=2, workload="c5") if args.workload == "c5"
                else cpu_baseline(cores=1, workload=args.workload))
     line = {"metric": "particle-turns/s", "value": value, "unit": "particle-turns/s", "n_gpus": world,
