@@ -28,6 +28,7 @@
 
 #ifdef __CUDACC__
 #define TRKCR_FN __device__ __forceinline__
+#define TRKCR_SLOW static __device__ __noinline__
 #define TRKCR_CONST __device__ __constant__ const
 #define TRKCR_ADD(a, b) __dadd_rn((a), (b))
 #define TRKCR_SUB(a, b) __dsub_rn((a), (b))
@@ -40,6 +41,7 @@
 #include <math.h>
 /* host build: compile with -ffp-contract=off so each operation rounds once */
 #define TRKCR_FN static inline
+#define TRKCR_SLOW static
 #define TRKCR_CONST static const
 #define TRKCR_ADD(a, b) ((a) + (b))
 #define TRKCR_SUB(a, b) ((a) - (b))
@@ -216,7 +218,7 @@ TRKCR_FN trkcr_dd trkcr_cos_dd(double x) {
   }
 }
 
-TRKCR_FN double trkcr_sin(double x) {
+TRKCR_SLOW double trkcr_sin_slow(double x) {
   if (x == 0.0)
     return x;
   if (!isfinite(x))
@@ -225,15 +227,164 @@ TRKCR_FN double trkcr_sin(double x) {
   return TRKCR_ADD(v.hi, v.lo);
 }
 
-TRKCR_FN double trkcr_cos(double x) {
+TRKCR_SLOW double trkcr_cos_slow(double x) {
   if (!isfinite(x))
     return x - x;
   trkcr_dd v = trkcr_cos_dd(x);
   return TRKCR_ADD(v.hi, v.lo);
 }
 
-/* tan = sin/cos with a double-double quotient */
-TRKCR_FN double trkcr_tan(double x) {
+/*
+ * Fast paths for small arguments (|x| <= 2^-5, the CSBEND substep angles and
+ * slopes), after Ziv's strategy: evaluate the function as hi + L with a
+ * rigorous bound e on |f(x) - (hi + L)|, and return RN(hi + L) when
+ * RN(hi + L + e) == RN(hi + L - e), i.e. when every value the true result
+ * can take rounds the same way.  Otherwise the caller takes the
+ * double-double path above.  The bound is a few times 2^-100 |x|, so the
+ * test fails only for arguments whose result lies within that distance of
+ * a rounding boundary (about one call in 2^20 or fewer).
+ *
+ * The leading correction (x^3/6 for sin and asin, x^2/2 for cos) is formed
+ * exactly or to ~2^-104 relative with error-free products; the rest of the
+ * series, c2 (at most 2^-27 |x| for sin and asin, 2^-22 for cos), in plain
+ * double.  Error budget, written into e:
+ *   2^-49 |c2|        the plain-double tail (at most 7 roundings, 2^-50.2
+ *                     relative, from the rounded powers, coefficients and
+ *                     Horner steps) and its truncation (below 2^-62 |c2|);
+ *   2^-100 |x|        the leading correction's low part (below 2^-103 |x^3|);
+ *   2^-51 |L|         the roundings of L and of L +- e in the test itself.
+ * Each term carries a factor of two or more over the error it covers, which
+ * also absorbs the roundings of e's own sum.
+ * Arguments below 2^-26 (2^-27 for cos) return x (1) directly: the first
+ * correction is then under half an ulp.
+ */
+#define TRKCR_SMALL 0x1p-5
+
+TRKCR_FN int trkcr_round_test(double hi, double L, double e, double *out) {
+  const double u = TRKCR_ADD(hi, TRKCR_ADD(L, e));
+  const double v = TRKCR_ADD(hi, TRKCR_SUB(L, e));
+  *out = u;
+  return u == v;
+}
+
+/* x + sgn*x^3/6 + x^5 P(x^2) split as hi + L, with the error bound; sgn is
+ * -1 for sin, +1 for asin */
+TRKCR_FN double trkcr_odd_small(double x, double sgn, double c2, double zh, double zl, double th, double tl,
+                                double *L, double *e) {
+  const double S1h = 0x1.5555555555555p-3, S1l = 0x1.5555555555555p-57; /* 1/6 */
+  /* x^3 = th + tl + zl x, |zl x| rounding below 2^-106 |x^3| */
+  const double t_lo = TRKCR_ADD(tl, TRKCR_MUL(zl, x));
+  const double c1h = TRKCR_MUL(sgn, TRKCR_MUL(th, S1h));
+  const double e1 = TRKCR_FMA(sgn * th, S1h, -c1h);
+  const double c1l = TRKCR_ADD(e1, TRKCR_MUL(sgn, TRKCR_ADD(TRKCR_MUL(th, S1l), TRKCR_MUL(t_lo, S1h))));
+  const double lo = TRKCR_ADD(c1l, c2);
+  const double sh = TRKCR_ADD(x, c1h);
+  const double sl = TRKCR_SUB(c1h, TRKCR_SUB(sh, x));
+  *L = TRKCR_ADD(sl, lo);
+  *e = TRKCR_ADD(TRKCR_ADD(TRKCR_MUL(0x1p-49, fabs(c2)), TRKCR_MUL(0x1p-100, fabs(x))),
+                 TRKCR_MUL(0x1p-51, fabs(*L)));
+  return sh;
+}
+
+/* sin x as hi + L within e, for 2^-26 <= |x| <= 2^-5, from zh + zl = x^2 */
+TRKCR_FN double trkcr_sin_parts(double x, double zh, double zl, double *L, double *e) {
+  const double th = TRKCR_MUL(zh, x);
+  const double tl = TRKCR_FMA(zh, x, -th);
+  /* x^5 (1/120 - z/5040 + z^2/362880 - z^3/39916800) */
+  double P = TRKCR_FMA(zh, -0x1.ae64567f544e4p-26, 0x1.71de3a556c734p-19);
+  P = TRKCR_FMA(zh, P, -0x1.a01a01a01a01ap-13);
+  P = TRKCR_FMA(zh, P, 0x1.1111111111111p-7);
+  const double c2 = TRKCR_MUL(TRKCR_MUL(th, zh), P);
+  return trkcr_odd_small(x, -1.0, c2, zh, zl, th, tl, L, e);
+}
+
+/* cos x as hi + L within e, for 2^-27 <= |x| <= 2^-5, from zh + zl = x^2:
+ * cos = (1 - zh/2) + (-zl/2 + zh^2 Q(zh)),
+ * Q = 1/24 - z/720 + z^2/40320 - z^3/3628800 + z^4/479001600 (first omitted
+ * term z^7/14! below 2^-106); the tail's error (the rounded zh^2, the
+ * dropped 2 zh zl, Q's roundings) stays under 2^-50.5 |zh^2 Q|, covered by
+ * 2^-48 (|t| + |zl|) */
+TRKCR_FN double trkcr_cos_parts(double zh, double zl, double *L, double *e) {
+  const double ah = TRKCR_SUB(1.0, TRKCR_MUL(0.5, zh));
+  const double al = TRKCR_SUB(TRKCR_SUB(1.0, ah), TRKCR_MUL(0.5, zh));
+  double Q = TRKCR_FMA(zh, 0x1.1eed8eff8d898p-29, -0x1.27e4fb7789f5cp-22);
+  Q = TRKCR_FMA(zh, Q, 0x1.a01a01a01a01ap-16);
+  Q = TRKCR_FMA(zh, Q, -0x1.6c16c16c16c17p-10);
+  Q = TRKCR_FMA(zh, Q, 0x1.5555555555555p-5);
+  const double t = TRKCR_FMA(TRKCR_MUL(zh, zh), Q, TRKCR_MUL(-0.5, zl));
+  *L = TRKCR_ADD(al, t);
+  *e = TRKCR_ADD(TRKCR_ADD(TRKCR_MUL(0x1p-48, TRKCR_ADD(fabs(t), fabs(zl))), TRKCR_MUL(0x1p-51, fabs(*L))),
+                 0x1p-110);
+  return ah;
+}
+
+/* correctly rounded sin of |x| <= 2^-5, or 0 when the rounding test fails */
+TRKCR_FN int trkcr_sin_small(double x, double *s) {
+  if (fabs(x) < 0x1p-26) {
+    *s = x;
+    return 1;
+  }
+  double L, e;
+  const double zh = TRKCR_MUL(x, x);
+  const double hi = trkcr_sin_parts(x, zh, TRKCR_FMA(x, x, -zh), &L, &e);
+  return trkcr_round_test(hi, L, e, s);
+}
+
+/* correctly rounded cos of |x| <= 2^-5, or 0 when the rounding test fails */
+TRKCR_FN int trkcr_cos_small(double x, double *c) {
+  if (fabs(x) < 0x1p-27) {
+    *c = 1.0;
+    return 1;
+  }
+  double L, e;
+  const double zh = TRKCR_MUL(x, x);
+  const double hi = trkcr_cos_parts(zh, TRKCR_FMA(x, x, -zh), &L, &e);
+  return trkcr_round_test(hi, L, e, c);
+}
+
+TRKCR_FN double trkcr_sin(double x) {
+  double s;
+  if (fabs(x) <= TRKCR_SMALL && trkcr_sin_small(x, &s))
+    return s;
+  return trkcr_sin_slow(x);
+}
+
+TRKCR_FN double trkcr_cos(double x) {
+  double c;
+  if (fabs(x) <= TRKCR_SMALL && trkcr_cos_small(x, &c))
+    return c;
+  return trkcr_cos_slow(x);
+}
+
+/* sin and cos of one argument (the CSBEND drift needs both): x^2 formed once */
+TRKCR_FN void trkcr_sincos(double x, double *s, double *c) {
+  const double ax = fabs(x);
+  if (ax <= TRKCR_SMALL) {
+    if (ax < 0x1p-27) {
+      *s = x;
+      *c = 1.0;
+      return;
+    }
+    double L, e, so, co;
+    const double zh = TRKCR_MUL(x, x);
+    const double zl = TRKCR_FMA(x, x, -zh);
+    int ok = 1;
+    if (ax < 0x1p-26)
+      so = x;
+    else
+      ok = trkcr_round_test(trkcr_sin_parts(x, zh, zl, &L, &e), L, e, &so);
+    if (ok && trkcr_round_test(trkcr_cos_parts(zh, zl, &L, &e), L, e, &co)) {
+      *s = so;
+      *c = co;
+      return;
+    }
+  }
+  *s = trkcr_sin_slow(x);
+  *c = trkcr_cos_slow(x);
+}
+
+/* tan = sin/cos with a double-double quotient (bend edges only: not inlined) */
+TRKCR_SLOW double trkcr_tan(double x) {
   if (x == 0.0)
     return x;
   if (!isfinite(x))
@@ -248,7 +399,7 @@ TRKCR_FN double trkcr_tan(double x) {
   return TRKCR_ADD(q.hi, q.lo);
 }
 
-TRKCR_FN double trkcr_asin(double y) {
+TRKCR_SLOW double trkcr_asin_slow(double y) {
   if (y == 0.0 || fabs(y) >= 1.0 || isnan(y))
     return TRKCR_ASIN(y);
   double a0 = TRKCR_ASIN(y);
@@ -259,6 +410,35 @@ TRKCR_FN double trkcr_asin(double y) {
   double delta = TRKCR_DIV(num, c);
   trkcr_dd a = trkcr_two_sum(a0, delta);
   return TRKCR_ADD(a.hi, a.lo);
+}
+
+/* asin(y) = y + y^3/6 + y^5 R(y^2), R = sum_{n>=2} (2n)!/(4^n (n!)^2 (2n+1)) z^(n-2):
+ * 3/40, 5/112, 35/1152, 63/2816, 231/13312, 143/10240; the first omitted
+ * term (6435/557056 y^17) is below 2^-62 |y^5 R| for |y| <= 2^-5 */
+TRKCR_FN double trkcr_asin_parts(double y, double zh, double zl, double *L, double *e) {
+  const double th = TRKCR_MUL(zh, y);
+  const double tl = TRKCR_FMA(zh, y, -th);
+  double R = TRKCR_FMA(zh, 143.0 / 10240.0, 231.0 / 13312.0);
+  R = TRKCR_FMA(zh, R, 63.0 / 2816.0);
+  R = TRKCR_FMA(zh, R, 35.0 / 1152.0);
+  R = TRKCR_FMA(zh, R, 5.0 / 112.0);
+  R = TRKCR_FMA(zh, R, 3.0 / 40.0);
+  const double c2 = TRKCR_MUL(TRKCR_MUL(th, zh), R);
+  return trkcr_odd_small(y, 1.0, c2, zh, zl, th, tl, L, e);
+}
+
+TRKCR_FN double trkcr_asin(double y) {
+  const double ay = fabs(y);
+  if (ay <= TRKCR_SMALL) {
+    if (ay < 0x1p-26)
+      return y;
+    double L, e, out;
+    const double zh = TRKCR_MUL(y, y);
+    const double hi = trkcr_asin_parts(y, zh, TRKCR_FMA(y, y, -zh), &L, &e);
+    if (trkcr_round_test(hi, L, e, &out))
+      return out;
+  }
+  return trkcr_asin_slow(y);
 }
 
 #endif

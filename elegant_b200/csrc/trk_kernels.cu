@@ -40,12 +40,14 @@
 #define M_COS(x) cos(x)
 #define M_ASIN(x) asin(x)
 #define M_TAN(x) tan(x)
+#define M_SINCOS(x, s, c) sincos((x), (s), (c))
 #else
 #define TRK_NS trk_exact
 #define M_SIN(x) trkcr_sin(x)
 #define M_COS(x) trkcr_cos(x)
 #define M_ASIN(x) trkcr_asin(x)
 #define M_TAN(x) trkcr_tan(x)
+#define M_SINCOS(x, s, c) trkcr_sincos((x), (s), (c))
 #endif
 
 namespace TRK_NS {
@@ -974,8 +976,8 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
       double sin_phi = QX / f;
       double phi = M_ASIN(sin_phi);
       const double arg = __ldg(&d[BD_ARG + j]);
-      double sine = M_SIN(arg + phi);
-      double cosi = M_COS(arg + phi);
+      double sine, cosi;
+      M_SINCOS(arg + phi, &sine, &cosi);
       if (cosi == 0) {
         ok = false;
         break;

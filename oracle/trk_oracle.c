@@ -933,6 +933,26 @@ double orc_cr_sin(double x) { return trkcr_sin(x); }
 double orc_cr_cos(double x) { return trkcr_cos(x); }
 double orc_cr_asin(double x) { return trkcr_asin(x); }
 double orc_cr_tan(double x) { return trkcr_tan(x); }
+/* the double-double evaluations behind the fast paths, and the fast paths'
+ * parts (hi, L, error bound e; returns the rounding test's verdict), for the
+ * tests of the fast paths' error bounds */
+double orc_cr_slow(int kind, double x) {
+  return kind == 0 ? trkcr_sin_slow(x) : kind == 1 ? trkcr_cos_slow(x) : trkcr_asin_slow(x);
+}
+int orc_cr_parts(int kind, double x, double *out) {
+  double L, e, hi, r;
+  const double zh = x * x, zl = fma(x, x, -zh);
+  if (kind == 0)
+    hi = trkcr_sin_parts(x, zh, zl, &L, &e);
+  else if (kind == 1)
+    hi = trkcr_cos_parts(zh, zl, &L, &e);
+  else
+    hi = trkcr_asin_parts(x, zh, zl, &L, &e);
+  out[0] = hi;
+  out[1] = L;
+  out[2] = e;
+  return trkcr_round_test(hi, L, e, &r);
+}
 
 static void dd_acc(double *hi, double *lo, double v) {
   double s = *hi + v, bb = s - *hi, e = (*hi - (s - bb)) + (v - bb);

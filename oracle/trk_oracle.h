@@ -48,6 +48,8 @@ double orc_cr_sin(double x);
 double orc_cr_cos(double x);
 double orc_cr_asin(double x);
 double orc_cr_tan(double x);
+double orc_cr_slow(int kind, double x);
+int orc_cr_parts(int kind, double x, double *out);
 
 /* Sharded runs (test of the multi-GPU decomposition on CPU ranks): gather
  * n doubles from every rank into recv[rank * n ...]; sum n doubles over
