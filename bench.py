@@ -6,6 +6,18 @@ function on 2000 bins, CHARGE 1 nC), 1e6 particles from a seeded Gaussian
 beam.  One step is one pass (turn) of the whole beam.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                  [--build both|parity|fast]
+
+Two builds of one kernel source are timed in the same run:
+  parity (the headline `value`): the reference's operation sequence without
+        FMA contraction and with correctly rounded sin/cos/asin; bit-exact
+        with elegant's own tracking code run with a correctly rounded libm;
+  fast (`fast_build`): FMA contraction and transcendental-free CSBEND and
+        multipole bodies; within a few 1e-8 of the reference after one turn.
+Each carries `accuracy`: its measured error against elegant's own tracking
+code on the benchmark rings as configured (committed fixtures written by the
+reference: 1e4 particles x 1 and 100 turns of the FODO ring, 4000 particles x
+1 and 10 turns of this ring).
 
 value : particle-turns/s with the beam resident on the device; each step is
         timed with CUDA events on the tracking stream, the L2 is flushed
@@ -47,8 +59,7 @@ N_PARTICLES = 1_000_000
 # written at 2e5 particles (ncu; the coordinate writes stay in L2 and are
 # written back during later kernels)
 TRACK_DRAM_BYTES_PER_PARTICLE = 10.628e6 / 2e5
-# the same for the MBA ring (C5): 110.67 MB read + 120.53 MB written at 2e6 particles (ncu,
-# profiles/track_kernel_mba_ring.md)
+# the same for the MBA ring: 110.67 MB read + 120.53 MB written at 2e6 particles (ncu)
 TRACK_DRAM_BYTES_PER_PARTICLE_C5 = (110.67e6 + 120.53e6) / 2e6
 
 WORKLOADS = {
@@ -181,28 +192,35 @@ def cpu_baseline(cores=None, sample_particles=6000, sample_turns=3, workload="c2
     with ctx.Pool(cores) as pool:
         args = [(per, sample_turns, 1 + k, workload) for k in range(cores)]
         kinds = pool.map(_oracle_shard, [(10, 1, 99, workload)] * cores)  # warm the workers
-        t0 = time.perf_counter()
-        effs = pool.map(_oracle_shard, args)
-        dt = time.perf_counter() - t0
-    return {"value": sum(e for e, _ in effs) / dt, "unit": "particle-turns/s", "cores": cores, "kind": kinds[0][1],
+        res = pool.map(_oracle_shard, args)
+        dt = max(r[2] for r in res)
+    return {"value": sum(r[0] for r in res) / dt, "unit": "particle-turns/s", "cores": cores, "kind": kinds[0][1],
             "sample": f"{cores} processes x {per} particles x {sample_turns} turns (particle shards; wake "
                       "histograms per shard)"}
 
 
 def _oracle_shard(args):
+    """One shard of the CPU leg: builds its lattice and beam, then times the
+    tracking call alone.  Returns (particle-turns, kind, seconds)."""
     n, turns, seed, workload = args
     sys.path.insert(0, ROOT)
     track, kind = _cpu_tracker()
     lat = workload_lattice(workload)
     beam = workload_beam(workload, n, seed=seed)
+    t0 = time.perf_counter()
     _, _, eff = track(lat, beam, turns, 13700.0)
-    return eff, kind
+    return eff, kind, time.perf_counter() - t0
 
 
 def run_reference(args, rank, world):
     """The reference arm: the CPU tracking path on all host cores (one
     process per core, particle shards), each step a bounded sample of the
-    benchmark ring; rank 0 only."""
+    benchmark ring; rank 0 only.  Each shard times its own tracking call
+    (lattice and beam set-up outside the timed region); a step's time is the
+    slowest shard's.  Shards run elegant's serial build, which bins and
+    convolves its own wake histogram (Pelegant would sum the shards'
+    histograms with one MPI_Allreduce per wake, src/wake.c:226-233; the
+    work per shard is the same)."""
     if rank != 0:
         return 0
     import multiprocessing as mp
@@ -213,21 +231,19 @@ def run_reference(args, rank, world):
     with mp.get_context("spawn").Pool(cores) as pool:
         kind = pool.map(_oracle_shard, [(10, 1, 99, workload)] * cores)[0][1]
         for k in range(args.warmup + args.steps):
-            t0 = time.perf_counter()
-            effs = pool.map(_oracle_shard, [(per, turns, 1 + c, workload) for c in range(cores)])
-            dt = time.perf_counter() - t0
+            res = pool.map(_oracle_shard, [(per, turns, 1 + c, workload) for c in range(cores)])
+            dt = max(r[2] for r in res)
             if k >= args.warmup:
-                steps.append(sum(e for e, _ in effs) / dt)
+                steps.append(sum(r[0] for r in res) / dt)
     v = float(np.mean(steps))
     sample = (f"{cores} processes x {per} particles x {turns} turn of the same ring per step (particle shards; "
-              "wake histograms per shard)")
-    steps = [{"kind": kind, "sample": sample}]
+              "wake histograms per shard); tracking calls timed, set-up excluded")
     line = {"metric": "particle-turns/s", "value": v, "unit": "particle-turns/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian beam)",
             "config": workload_config(WORKLOADS[workload]["particles"], workload), "impl": "reference",
-            "cpu_baseline": {"value": v, "unit": "particle-turns/s", "cores": cores, "kind": steps[0]["kind"],
-                             "sample": steps[0]["sample"]},
+            "cpu_baseline": {"value": v, "unit": "particle-turns/s", "cores": cores, "kind": kind,
+                             "sample": sample},
             "e2e": {"value": v, "unit": "particle-turns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -242,7 +258,10 @@ def main():
     ap.add_argument("--particles", type=int, default=None,
                     help="particles per GPU (1e6 for c1/c2, 1e7 for c5, 1e5 for c4)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--exact", action="store_true", help="parity build instead of the fast build")
+    ap.add_argument("--exact", action="store_true", help="the parity build alone (same as --build parity)")
+    ap.add_argument("--build", default="both", choices=["both", "parity", "fast"],
+                    help="both: the parity build (bit-exact with the reference's arithmetic under a correctly "
+                         "rounded libm) is the headline value and the fast build is reported beside it")
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "c5grad", "rad", "observe",
                                                        "da"],
                     help="c2: ring with RF and wake (the benchmark); c1: plain FODO ring (profiling); "
@@ -595,6 +614,136 @@ def run_da(args, rank):
     return 0
 
 
+def _timed_turns(trk, lat, fast, steps, warmup, pass_index, flush, stream, world, local):
+    """Warm-up turns, then `steps` timed turns of the resident beam (CUDA
+    events on the tracking stream, L2 flushed between steps outside the
+    events).  Returns the measurements and the next pass index."""
+    import torch
+    from elegant_b200 import configs
+    for _ in range(max(warmup, 3)):
+        trk.track(lat, 1, configs.P_CENTRAL, pass_offset=pass_index, fast=fast)
+        pass_index += 1
+    step_ms, effort, launches, track_ms, track_launches = [], 0, 0, 0.0, 0
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        t_wall = time.perf_counter()
+        for k in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(k))
+            st = trk.track(lat, 1, configs.P_CENTRAL, pass_offset=pass_index, fast=fast, time_kernels=True)
+            pass_index += 1
+            step_ms.append(st["device_ms"])
+            effort += st["particle_passes"]
+            launches += st["kernel_launches"]
+            track_ms += st["track_ms"]
+            track_launches += st["track_launches"]
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t_wall
+    dev_s = sum(step_ms) / 1e3
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([dev_s, float(effort)], dtype=torch.float64, device=f"cuda:{local}")
+        dmax = t[:1].clone()
+        dist.all_reduce(dmax, op=dist.ReduceOp.MAX)
+        dsum = t[1:].clone()
+        dist.all_reduce(dsum, op=dist.ReduceOp.SUM)
+        dev_s = float(dmax.item())
+        effort = float(dsum.item())
+    return {"value": effort / dev_s, "dev_s": dev_s, "effort": effort, "launches": launches, "track_ms": track_ms,
+            "track_launches": track_launches, "wall": wall, "clocks": clocks.summary()}, pass_index
+
+
+def _e2e(trk, lat, fast, beam, steps, world):
+    """The same metric through the C ABI with host buffers: each step loads
+    the beam from pinned host memory, tracks one turn and stores it back."""
+    import torch
+    from elegant_b200 import configs
+    pinned = torch.from_numpy(beam).pin_memory().numpy()
+    pinned_out = torch.empty(beam.shape, dtype=torch.float64).pin_memory().numpy()
+    e2e_ms, eff = [], 0
+    for _ in range(max(3, steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        trk.load(pinned)
+        st = trk.track(lat, 1, configs.P_CENTRAL, fast=fast)
+        trk.store(stride=7, out=pinned_out)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        eff = st["particle_passes"]
+    n = beam.shape[0]
+    return {"value": eff / (np.median(e2e_ms) / 1e3) * world, "unit": "particle-turns/s",
+            "h2d_bytes_per_step": int(n * 7 * 8), "d2h_bytes_per_step": int(n * 7 * 8)}
+
+
+def _roofline(m, workload, world, peak, flops):
+    """FP64 roofline of the fused tracking kernel: algorithmic flops of the
+    elements it runs (reference formulation, oracle/flops.json) per launch
+    over its CUDA-event launch time."""
+    if not flops or not m["track_launches"]:
+        return None
+    # the radiating ring is counted as the plain one (the radiation's own flops are not counted)
+    fpt = flops["flops_per_particle_turn"]["c2" if workload == "rad" else workload]
+    # the wakes' per-particle work runs in the wake kernels
+    fpt -= {"c1": 0, "c2": 1, "rad": 1, "c5": 2}[workload] * flops["per_particle"]["WAKE"]["total"]
+    per_launch_flops = fpt * (m["effort"] / world) / m["track_launches"]
+    avg_launch_s = m["track_ms"] / m["track_launches"] / 1e3
+    achieved = per_launch_flops / avg_launch_s / 1e12
+    traffic = {"c2": TRACK_DRAM_BYTES_PER_PARTICLE, "c5": TRACK_DRAM_BYTES_PER_PARTICLE_C5}.get(workload)
+    return {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak if peak else None,
+            "traffic": traffic * (m["effort"] / world) / m["track_launches"] if traffic else None,
+            "flops_per_particle_turn": fpt, "kernel": "track_kernel", "launches": m["track_launches"],
+            "avg_launch_ms": avg_launch_s * 1e3,
+            "peak_source": "FP64 FMA peak measured in this run (independent dependent-FMA chains); "
+                           "MEASURED_PEAKS.json has no FP64 figure",
+            "traffic_source": (None if not traffic else
+                               "ncu dram__bytes_read.sum + dram__bytes_write.sum of one fast-build launch at "
+                               + ("2e5" if workload == "c2" else "2e6") + " particles, scaled by particles")}
+
+
+LONG_FIXTURES = os.path.join(ROOT, "tests", "golden", "long_tracks.npz")
+
+
+def accuracy(local, fast):
+    """Error of one build against elegant's own tracking code on the
+    benchmark rings as configured, from the committed fixtures the
+    reference wrote (tests/golden/long_tracks.npz): the FODO ring with 1e4
+    particles after 1 and 100 turns, the RF + wake ring (2000 bins) with
+    4000 particles after 1 and 10 turns.  Per coordinate |gpu - ref| /
+    max(|ref|, sigma_c) over the reference's survivors, against the
+    reference in the parity arithmetic (correctly rounded libm) and in its
+    own (glibc libm); plus whether the survivor sets are identical."""
+    from elegant_b200 import Tracker, configs
+    if not os.path.exists(LONG_FIXTURES):
+        return None
+    gold = np.load(LONG_FIXTURES)
+    cases = {"fodo40_1e4": ("c1", configs.c1_lattice, lambda: configs.gaussian_beam(10_000, seed=1), (1, 100)),
+             "ring_rf_wake_4e3": ("c2", configs.c2_lattice, lambda: configs.gaussian_beam(4000, seed=7), (1, 10))}
+    out = {}
+    with Tracker(local) as trk:  # no communicator: a one-GPU run on every rank that asks
+        for name, (ring, mk_lat, mk_beam, turn_list) in cases.items():
+            lat, beam = mk_lat(), mk_beam()
+            for turns in turn_list:
+                trk.load(beam)
+                trk.track(lat, turns, configs.P_CENTRAL, fast=fast)
+                n_left, g, lp, le = trk.store(stride=7, with_loss=True)
+                order = np.argsort(g[:, 6], kind="stable")
+                g, lp = g[order], lp[order]
+                res = {}
+                for mode in ("parity_arith", "reference_arith"):
+                    key = f"{ring}/turns{turns}/{mode}"
+                    ref, loss = gold[key + "/coords"], gold[key + "/loss"]
+                    alive = loss[:, 0] < 0
+                    sig = np.std(ref[alive, :6], axis=0)
+                    d = np.abs(g[alive, :6] - ref[alive, :6]) / np.maximum(np.abs(ref[alive, :6]), sig)
+                    res[mode] = {"max_err": float(d.max()), "bit_exact": bool(np.array_equal(g[alive, :6],
+                                                                                              ref[alive, :6])),
+                                 "same_survivors": bool(np.array_equal(lp < 0, alive))}
+                out[f"{name}_{turns}turn" + ("s" if turns > 1 else "")] = res
+    return out
+
+
 def run_gpu(args, rank, world, local):
     import torch
     from elegant_b200 import Tracker, configs
@@ -606,8 +755,10 @@ def run_gpu(args, rank, world, local):
     n = args.particles or WORKLOADS[args.workload]["particles"]
     lat = workload_lattice(args.workload)
     beam = workload_beam(args.workload, n, seed=1 + rank, first_id=1 + rank * n)
-    fast = not args.exact
+    builds = {"parity": ["parity"], "fast": ["fast"], "both": ["parity", "fast"]}[
+        "parity" if args.exact else args.build]
     flops = load_flops()
+    res = {}
     with Tracker(local) as trk:
         if world > 1:
             # the library's own NCCL communicator for the wake/RF exchanges
@@ -617,106 +768,50 @@ def run_gpu(args, rank, world, local):
             t = torch.tensor(list(uid), dtype=torch.uint8, device=f"cuda:{local}")
             dist.broadcast(t, 0)
             trk.set_comm(bytes(t.cpu().tolist()), world, rank)
-        trk.load(beam)
-        pass_index = 0
-        for _ in range(max(args.warmup, 3)):
-            trk.track(lat, 1, configs.P_CENTRAL, pass_offset=pass_index, fast=fast)
-            pass_index += 1
         flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
         stream = torch.cuda.ExternalStream(trk.stream(), device=f"cuda:{local}")
-        step_ms = []
-        effort = 0
-        launches = 0
-        track_ms = 0.0
-        track_launches = 0
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
-        with ClockSampler(local) as clocks:
-            t_wall = time.perf_counter()
-            for k in range(args.steps):
-                with torch.cuda.stream(stream):
-                    flush.fill_(float(k))
-                st = trk.track(lat, 1, configs.P_CENTRAL, pass_offset=pass_index, fast=fast, time_kernels=True)
-                pass_index += 1
-                step_ms.append(st["device_ms"])
-                effort += st["particle_passes"]
-                launches += st["kernel_launches"]
-                track_ms += st["track_ms"]
-                track_launches += st["track_launches"]
-            torch.cuda.synchronize()
-            wall = time.perf_counter() - t_wall
-        dev_s = sum(step_ms) / 1e3
-        if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([dev_s, float(effort)], dtype=torch.float64, device=f"cuda:{local}")
-            dmax = t[:1].clone()
-            dist.all_reduce(dmax, op=dist.ReduceOp.MAX)
-            dsum = t[1:].clone()
-            dist.all_reduce(dsum, op=dist.ReduceOp.SUM)
-            dev_s = float(dmax.item())
-            effort = float(dsum.item())
-        value = effort / dev_s
-        # end-to-end through the C ABI with host buffers
-        pinned = torch.from_numpy(beam).pin_memory().numpy()
-        pinned_out = torch.empty(beam.shape, dtype=torch.float64).pin_memory().numpy()
-        e2e_ms = []
-        for k in range(max(3, args.steps // 2)):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            trk.load(pinned)
-            st = trk.track(lat, 1, configs.P_CENTRAL, fast=fast)
-            trk.store(stride=7, out=pinned_out)
-            e2e_ms.append((time.perf_counter() - t0) * 1e3)
-            e2e_eff = st["particle_passes"]
-        e2e_value = e2e_eff / (np.median(e2e_ms) / 1e3) * world
+        for b in builds:
+            fast = b == "fast"
+            trk.load(beam)
+            m, _ = _timed_turns(trk, lat, fast, args.steps, args.warmup, 0, flush, stream, world, local)
+            m["e2e"] = _e2e(trk, lat, fast, beam, args.steps // 2, world)
+            res[b] = m
+        del flush
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
     if rank != 0:
         return 0
-    # roofline of the dominant kernel (the fused tracking kernel): algorithmic
-    # FP64 flops of the elements it runs (reference formulation, counted in
-    # oracle/flops.json) per launch, over its CUDA-event launch time
     peak = measure_fp64_peak(local)
-    roof = None
-    if flops and track_launches:
-        # the radiating ring is counted as the plain one (the radiation's own flops are not counted)
-        fpt = flops["flops_per_particle_turn"]["c2" if args.workload == "rad" else args.workload]
-        # the wakes' per-particle work runs in the wake kernels
-        fpt -= {"c1": 0, "c2": 1, "rad": 1, "c5": 2}[args.workload] * flops["per_particle"]["WAKE"]["total"]
-        per_launch_flops = fpt * (effort / world) / track_launches
-        avg_launch_s = track_ms / track_launches / 1e3
-        achieved = per_launch_flops / avg_launch_s / 1e12
-        roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak if peak else None,
-                "traffic": ({"c2": TRACK_DRAM_BYTES_PER_PARTICLE, "c5": TRACK_DRAM_BYTES_PER_PARTICLE_C5}
-                            [args.workload] * (effort / world) / track_launches
-                            if args.workload in ("c2", "c5") else None),
-                "flops_per_particle_turn": fpt, "kernel": "track_kernel", "launches": track_launches,
-                "avg_launch_ms": avg_launch_s * 1e3,
-                "peak_source": "FP64 FMA peak measured in this run (independent dependent-FMA chains); "
-                               "MEASURED_PEAKS.json has no FP64 figure",
-                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at 2e5 "
-                                   "particles, scaled by particles (profiles/track_kernel_ring_rf_wake.md)"
-                                   if args.workload != "c5" else
-                                   "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at 2e6 "
-                                   "particles, scaled by particles (profiles/track_kernel_mba_ring.md)")}
+    acc = {b: accuracy(local, b == "fast") for b in builds} if world == 1 else None
     cpu = None
     # no CPU leg for the radiating ring: the reference's ISR deviates come from the SDDS toolkit's
     # generator, which is not in the reference tree
     if not args.no_cpu_baseline and world == 1 and args.workload != "rad":
         cpu = (cpu_baseline(cores=1, sample_particles=1500, sample_turns=2, workload="c5") if args.workload == "c5"
                else cpu_baseline(cores=1, workload=args.workload))
-    line = {"metric": "particle-turns/s", "value": value, "unit": "particle-turns/s", "n_gpus": world,
-            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": dev_s * 1e3 / args.steps,
+    head = builds[0]
+    m = res[head]
+    line = {"metric": "particle-turns/s", "value": m["value"], "unit": "particle-turns/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": m["dev_s"] * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded Gaussian beam, seeded resonator wake)", "config": workload_config(n, args.workload),
-            "build": "fast" if fast else "parity", "wall_s": wall,
-            "e2e": {"value": e2e_value, "unit": "particle-turns/s", "h2d_bytes_per_step": int(n * 7 * 8),
-                    "d2h_bytes_per_step": int(n * 7 * 8)},
-            "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks.summary()}
+            "data": "synthetic (seeded Gaussian beam, seeded resonator wake)",
+            "config": workload_config(n, args.workload), "build": head, "wall_s": m["wall"], "e2e": m["e2e"],
+            "gpu_launches": m["launches"], "roofline": _roofline(m, args.workload, world, peak, flops),
+            "cpu_baseline": cpu, "clocks": m["clocks"]}
+    if acc and acc.get(head):
+        line["accuracy"] = acc[head]
+        line["accuracy_metric"] = ("max over surviving particles and coordinates of |gpu - ref| / max(|ref|, "
+                                   "sigma_c) against elegant's own tracking code (fixtures written by it): "
+                                   "parity_arith = with a correctly rounded libm, reference_arith = with glibc's")
+    for b in builds[1:]:
+        mb = res[b]
+        line[f"{b}_build"] = {"value": mb["value"], "ms_per_step": mb["dev_s"] * 1e3 / args.steps,
+                              "e2e": mb["e2e"], "gpu_launches": mb["launches"],
+                              "roofline": _roofline(mb, args.workload, world, peak, flops),
+                              "accuracy": acc.get(b) if acc else None, "clocks": mb["clocks"]}
     print(json.dumps(line), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
     return 0
 
 

@@ -36,13 +36,17 @@ def loss_and_grad(tracker, lattice, beam, n_passes, p_central, centroid_weight=0
     return tracker.adjoint(lattice, n_passes, p_central, centroid_weight)
 
 
-def make_autograd(lattice, beam, n_passes, p_central, centroid_weight=0.0, device=0):
+def make_autograd(lattice, beam, n_passes, p_central, centroid_weight=0.0, device=0, tracker=None):
     """A torch.autograd.Function whose forward maps the parameter vector to
     the objective (tracking on the GPU) and whose backward returns the
-    adjoint gradient."""
+    adjoint gradient, and the Tracker it tracks with.  Pass `tracker` to
+    track with one of your own; otherwise a new Tracker is created, and the
+    caller owns it: close it (tracker.close(), or use it in a with block)
+    when the function is no longer needed."""
     import torch
 
-    tracker = Tracker(device)
+    if tracker is None:
+        tracker = Tracker(device)
 
     class TrackedLoss(torch.autograd.Function):
         @staticmethod

@@ -70,11 +70,9 @@ def objects():
     src = os.path.join(CSRC, "trk_observe.cu")
     o = os.path.join(BUILD, "trk_observe.o")
     out.append((src, o, nv_common + ["-fmad=false", "-c", src, "-o", o]))
-    for extra in ("trk_noalloc.cu", "trk_hooks.cu"):
-        src = os.path.join(CSRC, extra)
-        if os.path.exists(src):
-            o = os.path.join(BUILD, extra.replace(".cu", ".o"))
-            out.append((src, o, nv_common + ["-c", src, "-o", o]))
+    src = os.path.join(CSRC, "trk_noalloc.cu")
+    o = os.path.join(BUILD, "trk_noalloc.o")
+    out.append((src, o, nv_common + ["-c", src, "-o", o]))
     return out
 
 

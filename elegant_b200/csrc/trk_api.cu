@@ -113,7 +113,44 @@ struct trk_context {
   long n_global = 0;    /* the same summed over the ranks of a sharded run */
   int tuned_variant = -1; /* tracking-kernel variant used when trk_run.variant < 0 (-1: by lattice class) */
   int last_launches = 0;
+  /* device scratch of the beam observers (trk_observe.cu), keyed by call
+   * site and slot, grown on demand, freed with the context */
+  struct ScratchSlot {
+    int site, slot;
+    void *p;
+    size_t bytes;
+  };
+  std::vector<ScratchSlot> obs_scratch;
 };
+
+/* Observer scratch of a context: `bytes` of device memory for (site, slot),
+ * reused between calls and grown when a call needs more.  The observers
+ * synchronize their stream before returning, so a buffer is idle whenever
+ * a new call asks for it. */
+int trk_context_scratch(trk_context *ctx, int site, int slot, size_t bytes, void **out) {
+  for (trk_context::ScratchSlot &e : ctx->obs_scratch)
+    if (e.site == site && e.slot == slot) {
+      if (e.bytes < bytes) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(e.p);
+        e.p = nullptr;
+        e.bytes = 0;
+        cudaError_t er = cudaMalloc(&e.p, bytes);
+        if (er != cudaSuccess)
+          return trk_set_error(TRK_ERR_CUDA, "cudaMalloc: %s", cudaGetErrorString(er));
+        e.bytes = bytes;
+      }
+      *out = e.p;
+      return TRK_OK;
+    }
+  void *q = nullptr;
+  cudaError_t er = cudaMalloc(&q, bytes);
+  if (er != cudaSuccess)
+    return trk_set_error(TRK_ERR_CUDA, "cudaMalloc: %s", cudaGetErrorString(er));
+  ctx->obs_scratch.push_back({site, slot, q, bytes});
+  *out = q;
+  return TRK_OK;
+}
 
 namespace {
 
@@ -713,6 +750,9 @@ void trk_context_destroy(trk_context *ctx) {
   cudaFree(ctx->d_adj_dk);
   cudaFree(ctx->d_adj_mom);
   cudaFree(ctx->d_adj_param);
+  for (trk_context::ScratchSlot &e : ctx->obs_scratch)
+    cudaFree(e.p);
+  ctx->obs_scratch.clear();
   trk_comm_destroy(ctx->comm);
   cudaFree(ctx->d_effort);
   cudaFree(ctx->d_aos);

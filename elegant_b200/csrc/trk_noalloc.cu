@@ -44,7 +44,8 @@ constexpr size_t kOffCounts = 0;
 constexpr size_t kOffV = align256(kOffCounts + sizeof(unsigned long long) * (kMaxBins + 2));
 constexpr size_t kOffState = align256(kOffV + sizeof(double) * (kMaxBins + 2));
 constexpr size_t kOffStats = align256(kOffState + sizeof(WakeState));
-constexpr size_t kOffPart = align256(kOffStats + sizeof(double) * 4);
+/* time statistics: sum, count, min, max, sum_hi, sum_lo (time_stats_finish_kernel) */
+constexpr size_t kOffPart = align256(kOffStats + sizeof(double) * 6);
 constexpr size_t kOffPartN = align256(kOffPart + sizeof(double) * 4 * kMaxBlocks);
 constexpr size_t kOffStatus = align256(kOffPartN + sizeof(long long) * kMaxBlocks);
 constexpr size_t kBytes = align256(kOffStatus + sizeof(int));
@@ -121,10 +122,13 @@ extern "C" int trk_wake_noalloc(double *const *columns, int32_t *lost_pass, int3
   if (rc)
     return rc;
   cudaStream_t st = (cudaStream_t)stream;
-  const int blocks = (int)std::max(1L, std::min((np + kChunk - 1) / kChunk, (long)sms * 8));
-  if (blocks > kMaxBlocks)
-    return trk_set_error(TRK_ERR_ARG, "trk_wake_noalloc: %d reduction blocks exceed the static %d", blocks,
-                         kMaxBlocks);
+  /* the time-statistics reduction takes the block count trk_track takes
+   * (one block per 4096 particles, at most 8 per SM), capped at the static
+   * partials' size: on a GPU with more than 148 SMs a large beam then uses
+   * fewer blocks than trk_track, and its mean time may differ in the last
+   * bit */
+  const int blocks =
+    (int)std::max(1L, std::min(std::min((np + kChunk - 1) / kChunk, (long)sms * 8), (long)kMaxBlocks));
   unsigned long long *counts = (unsigned long long *)(base + kOffCounts);
   double *V = (double *)(base + kOffV);
   WakeState *state = (WakeState *)(base + kOffState);

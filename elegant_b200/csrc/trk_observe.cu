@@ -36,6 +36,9 @@
       return trk_set_error(TRK_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_));                                  \
   } while (0)
 
+/* observer scratch held by the context (defined in trk_api.cu) */
+int trk_context_scratch(trk_context *ctx, int site, int slot, size_t bytes, void **out);
+
 namespace {
 
 constexpr int OBS_THREADS = 128;
@@ -365,6 +368,7 @@ struct Ctx {
   long n;
   int device;
   cudaStream_t st;
+  trk_context *ctx;
 };
 
 int context_beam(trk_context *ctx, Ctx &c) {
@@ -374,6 +378,7 @@ int context_beam(trk_context *ctx, Ctx &c) {
   if (rc)
     return rc;
   c.st = (cudaStream_t)trk_context_stream(ctx);
+  c.ctx = ctx;
   c.device = -1;
   if (c.n > 0) {
     cudaPointerAttributes at;
@@ -393,48 +398,23 @@ Beam beam_of(const Ctx &c) {
   return b;
 }
 
-/* Device scratch of the observers, kept between calls (grow-only, one set
- * per stream, call site and slot, held until the process exits): a
- * cudaMalloc/cudaFree pair per call would cost more than the reductions
- * themselves, and cudaFree synchronizes the device.  Every call ends with a
- * stream synchronization before it returns, so the next call on the same
- * stream may reuse the buffers. */
-struct CacheEntry {
-  cudaStream_t st;
-  int site, slot;
-  void *p;
-  size_t bytes;
-};
-static std::vector<CacheEntry> g_scratch;
-
+/* Device scratch of the observers, kept between calls in the context that
+ * owns the beam (trk_context_scratch, trk_api.cu; freed by
+ * trk_context_destroy): a cudaMalloc/cudaFree pair per call would cost more
+ * than the reductions themselves, and cudaFree synchronizes the device.
+ * Every call ends with a stream synchronization before it returns, so the
+ * next call on the same context may reuse the buffers. */
 struct Scratch {
-  cudaStream_t st;
+  trk_context *ctx;
   int site, slot = 0;
-  Scratch(cudaStream_t s, int site_) : st(s), site(site_) {}
+  Scratch(trk_context *c, int site_) : ctx(c), site(site_) {}
   template <typename T>
   int get(T **out, size_t count) {
-    const size_t bytes = sizeof(T) * std::max<size_t>(count, 1);
-    for (CacheEntry &e : g_scratch)
-      if (e.st == st && e.site == site && e.slot == slot) {
-        if (e.bytes < bytes) {
-          cudaStreamSynchronize(st);
-          cudaFree(e.p);
-          e.p = nullptr;
-          cudaError_t er = cudaMalloc(&e.p, bytes);
-          if (er != cudaSuccess)
-            return trk_set_error(TRK_ERR_CUDA, "cudaMalloc: %s", cudaGetErrorString(er));
-          e.bytes = bytes;
-        }
-        *out = (T *)e.p;
-        slot++;
-        return TRK_OK;
-      }
-    void *q = nullptr;
-    cudaError_t er = cudaMalloc(&q, bytes);
-    if (er != cudaSuccess)
-      return trk_set_error(TRK_ERR_CUDA, "cudaMalloc: %s", cudaGetErrorString(er));
-    g_scratch.push_back({st, site, slot, q, bytes});
-    *out = (T *)q;
+    void *p = nullptr;
+    int rc = trk_context_scratch(ctx, site, slot, sizeof(T) * std::max<size_t>(count, 1), &p);
+    if (rc)
+      return rc;
+    *out = (T *)p;
     slot++;
     return TRK_OK;
   }
@@ -443,7 +423,7 @@ struct Scratch {
 /* pass-1 totals on the host: 9 rounded sums, count, 5 x (min, max, maxabs) */
 int pass1(const Ctx &c, const Select &s, int pz_mode, double sums[9], double &count, double mm[15]) {
   const int nb = (int)((c.n + OBS_CHUNK - 1) / OBS_CHUNK);
-  Scratch sc(c.st, 1);
+  Scratch sc(c.ctx, 1);
   double *part, *out;
   signed char *ops;
   int rc;
@@ -520,7 +500,7 @@ int trk_accumulate_beam_sums(trk_context *ctx, trk_beam_sums *sums, double p_cen
     return rc;
   double np_count = 0;
   if (alive > 0) {
-    Scratch sc(c.st, 2);
+    Scratch sc(c.ctx, 2);
     Select s;
     s.Po = p_central;
     s.tmin = t_min;
@@ -639,7 +619,7 @@ int trk_match_energy(trk_context *ctx, double *p_central, int change_beam) {
     return TRK_OK;
   const double Po = *p_central;
   const int nb = (int)((c.n + OBS_CHUNK - 1) / OBS_CHUNK);
-  Scratch sc(c.st, 4);
+  Scratch sc(c.ctx, 4);
   double *part, *out;
   signed char *ops;
   if ((rc = sc.get(&part, (size_t)nb * 3)) || (rc = sc.get(&out, 3)) || (rc = sc.get(&ops, 1)))
@@ -682,7 +662,7 @@ int trk_sort_by_id(trk_context *ctx) {
   if (c.n <= 1)
     return TRK_OK;
   const long n = c.n;
-  Scratch sc(c.st, 5);
+  Scratch sc(c.ctx, 5);
   long long *k0, *k1;
   long *i0, *i1;
   if ((rc = sc.get(&k0, n)) || (rc = sc.get(&k1, n)) || (rc = sc.get(&i0, n)) || (rc = sc.get(&i1, n)))

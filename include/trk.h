@@ -364,7 +364,11 @@ int trk_ensemble_variant(const trk_context *ctx);
  *   macro_charge   charge per macroparticle (C); factor = WAKE FACTOR
  *   fast_math      0 parity build, 1 fast build; stream = cudaStream_t
  * Returns TRK_ERR_PHYSICS if the beam is longer than the wake (unless
- * allow_long_beam), TRK_ERR_ARG for sizes beyond the static limits. */
+ * allow_long_beam), TRK_ERR_ARG for sizes beyond the static limits.  The
+ * beam-time reduction uses trk_track's block count (one block per 4096
+ * particles, at most 8 per SM) capped at TRK_NOALLOC_MAX_BLOCKS; the result
+ * equals trk_track's bit for bit while the two block counts agree (always
+ * on GPUs of up to 148 SMs). */
 #define TRK_NOALLOC_MAX_BINS 8192
 #define TRK_NOALLOC_MAX_BLOCKS 1184
 #define TRK_NOALLOC_SCRATCH_BYTES (256 * 1024)

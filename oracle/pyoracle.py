@@ -176,7 +176,7 @@ def load_ref():
     if _ref is not None:
         return _ref
     if not ref_available():
-        raise FileNotFoundError(f"{REF_LIB} is not built (make -C oracle/ref with the reference sources present)")
+        raise FileNotFoundError(f"{REF_LIB} is not built (make -C oracle/ref REF=<reference tree>)")
     lib = ctypes.CDLL(REF_LIB)
     P, D, L, I = ctypes.c_void_p, ctypes.c_double, ctypes.c_long, ctypes.c_int
     DP = ctypes.POINTER(ctypes.c_double)

@@ -4,7 +4,7 @@ loss element of small seeded beams tracked by elegant's own tracking code
 oracle/ref/Makefile), in the reference's arithmetic and in the parity
 build's (correctly rounded libm, double-double sums).
 
-    make -C oracle/ref && python tests/golden/make_golden.py
+    make -C oracle/ref REF=<reference tree> && python tests/golden/make_golden.py
 
 The fixtures let the oracle be checked against the reference where the
 reference sources (and so libref.so) are not available."""

@@ -19,7 +19,7 @@ pytestmark = pytest.mark.gpu
 
 PC = configs.P_CENTRAL
 CHARGE = 1e-9
-N_BINS = 2000
+MAX_BINS = 8192  # TRK_NOALLOC_MAX_BINS in include/trk.h
 
 
 def _declare(lib):
@@ -37,10 +37,10 @@ def _beam(n):
     return b
 
 
-def _reference_path(beam, t, W, fast):
+def _reference_path(beam, t, W, fast, n_bins):
     lat = Lattice()
     lat.add("CHARGE", "Q", TOTAL=CHARGE)
-    i = lat.add("WAKE", "W", N_BINS=N_BINS, ALLOW_LONG_BEAM=1)
+    i = lat.add("WAKE", "W", N_BINS=n_bins, ALLOW_LONG_BEAM=1)
     lat.set_wake(i, t, W)
     with Tracker(0) as trk:
         trk.load(beam)
@@ -49,15 +49,17 @@ def _reference_path(beam, t, W, fast):
     return n_left, out
 
 
+@pytest.mark.parametrize("n_bins", [2000, MAX_BINS])
 @pytest.mark.parametrize("fast", [True, False])
-def test_wake_noalloc_matches_allocating_path(fast):
+def test_wake_noalloc_matches_allocating_path(fast, n_bins):
+    import torch
     lib = load_library()
     f = _declare(lib)
     n = 200_000
     beam = _beam(n)
     t, W = configs.resonator_wake(points=4096, dt=1e-12)
     dt = (t[-1] - t[0]) / (len(t) - 1)  # the spacing the allocating path derives from the table
-    n_ref, ref = _reference_path(beam, t, W, fast)
+    n_ref, ref = _reference_path(beam, t, W, fast, n_bins)
     ref = ref[np.argsort(ref[:, 6])]
 
     # Device memory for the caller's beam and wake table comes from two other
@@ -74,9 +76,17 @@ def test_wake_noalloc_matches_allocating_path(fast):
             cols, npart, loss = holder.columns()
             assert npart == n
             colptr = (ctypes.c_void_p * 6)(*cols[:6])
-            rc = f(colptr, loss[0], loss[1], n, PC, wcols[0], len(W), dt, N_BINS, CHARGE / n, 1.0, 0, 1, 0,
+            torch.cuda.synchronize()
+            free0 = torch.cuda.mem_get_info(0)[0]
+            rc = f(colptr, loss[0], loss[1], n, PC, wcols[0], len(W), dt, n_bins, CHARGE / n, 1.0, 0, 1, 0,
                    1 if fast else 0, holder.stream())
             assert rc == 0, lib.trk_last_error()
+            torch.cuda.synchronize()
+            if call == 1:
+                # the defining property: the call took no device memory
+                # (the first call on a device only looks up the static
+                # array's address, which allocates nothing either)
+                assert torch.cuda.mem_get_info(0)[0] == free0
             n_left, out = holder.store()
             out = out[np.argsort(out[:, 6])]
             assert n_left == n_ref
