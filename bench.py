@@ -292,13 +292,46 @@ def main():
     return run_gpu(args, rank, world, local)
 
 
+def _ensemble_cpu_shard(args):
+    """One variant of the ensemble on the CPU (reference code): a sample of
+    its dynamic-aperture grid, tracked `turns` turns; the tracking call
+    alone is timed.  Returns (particle-turns, kind, seconds)."""
+    v, n, turns = args
+    sys.path.insert(0, ROOT)
+    from elegant_b200 import configs
+    track, kind = _cpu_tracker()
+    lat = configs.c3_variant(seed=v)
+    beam = configs.da_grid(n)
+    t0 = time.perf_counter()
+    _, _, eff = track(lat, beam, turns, configs.P_CENTRAL)
+    return eff, kind, time.perf_counter() - t0
+
+
+def ensemble_cpu_baseline(variants=16, per_variant=256, turns=8):
+    """The ensemble's CPU baseline: `variants` error seeds, each a sample of
+    `per_variant` points of its grid tracked `turns` turns by the
+    reference's code, one process per variant on the host cores; the
+    slowest process's tracking time is the step time."""
+    import multiprocessing as mp
+    cores = min(os.cpu_count() or 1, variants)
+    with mp.get_context("spawn").Pool(cores) as pool:
+        pool.map(_ensemble_cpu_shard, [(0, 8, 1)] * cores)  # warm the workers
+        res = pool.map(_ensemble_cpu_shard, [(v, per_variant, turns) for v in range(variants)])
+    # variants run `variants / cores` rounds deep on `cores` processes: the
+    # time is the summed work over the cores
+    dt = sum(r[2] for r in res) / cores
+    return {"value": sum(r[0] for r in res) / dt, "unit": "particle-turns/s", "cores": cores, "kind": res[0][1],
+            "sample": f"{variants} error seeds x {per_variant} grid points x {turns} turns of the same ring "
+                      f"(one process per seed on {cores} cores)"}
+
+
 def run_ensemble(args, rank):
     """Batched ensemble: `variants` error seeds of the FODO+sextupole ring
     (rms dK1/K1 = 1e-3, dK2/K2 = 2e-3, 25 mm circular aperture), each with a
     dynamic-aperture grid of U{1000..65536} particles (x in +-20 mm, y in
     0..10 mm, delta = 0), all turns in one trk_track_ensemble call
-    (graph-captured, autotuned launch shape).  Metric: particle-turns/s of
-    the whole ensemble."""
+    (graph-captured, autotuned launch shape, survivors compacted every 64
+    passes).  Metric: particle-turns/s of the whole ensemble."""
     import torch
     from elegant_b200 import Tracker, configs
     if rank != 0:
@@ -313,23 +346,37 @@ def run_ensemble(args, rank):
         beams.append(configs.da_grid(int(n), first_id=first))
         first += int(n)
     beam = np.concatenate(beams)
+    fast = args.build != "parity" and not args.exact  # the fast build unless the parity build is asked for
     with Tracker(0) as trk:
         trk.load(beam)
-        warm = trk.track_ensemble(lats, counts, 4, configs.P_CENTRAL)  # autotunes
+        trk.track_ensemble(lats, counts, 4, configs.P_CENTRAL, fast=fast)  # autotunes
         trk.load(beam)
         torch.cuda.synchronize()
         with ClockSampler(0) as clocks:
             t0 = time.perf_counter()
-            st = trk.track_ensemble(lats, counts, turns, configs.P_CENTRAL)
+            st = trk.track_ensemble(lats, counts, turns, configs.P_CENTRAL, fast=fast)
             wall = time.perf_counter() - t0
     value = st["particle_passes"] / (st["device_ms"] / 1e3)
+    flops = load_flops()
+    roof = None
+    if flops:
+        per = flops["per_particle"]
+        fpt = flops["flops_per_particle_turn"]["c2"] - per["RFCA_L0"]["total"] - per["WAKE"]["total"]
+        peak = measure_fp64_peak(0)
+        achieved = fpt * value / 1e12
+        roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak if peak else None, "traffic": None, "flops_per_particle_turn": fpt,
+                "kernel": "track_kernel (ensemble graph, compaction kernels included in the time)",
+                "peak_source": "FP64 FMA peak measured in this run (independent dependent-FMA chains)"}
+    cpu = None if args.no_cpu_baseline else ensemble_cpu_baseline()
     line = {"metric": "particle-turns/s", "value": value, "unit": "particle-turns/s", "n_gpus": 1, "steps": turns,
             "warmup": 4, "ms_per_step": st["device_ms"] / turns, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded error seeds, dynamic-aperture grids)",
             "config": {"workload": "ensemble_c3", "variants": args.variants, "particles": int(counts.sum()),
-                       "turns": turns, "aperture_m": 0.025, "survivors": st["n_left"]},
-            "build": "fast", "wall_s": wall, "launch_shape": st["variant"], "tuned_by": "autotuner",
-            "gpu_launches": st["kernel_launches"], "clocks": clocks.summary()}
+                       "turns": turns, "aperture_m": 0.025, "survivors": st["n_left"], "compact_every": 64},
+            "build": "fast" if fast else "parity", "wall_s": wall, "launch_shape": st["variant"],
+            "tuned_by": "autotuner", "gpu_launches": st["kernel_launches"], "roofline": roof, "cpu_baseline": cpu,
+            "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
     return 0
 

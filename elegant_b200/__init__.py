@@ -80,6 +80,19 @@ class _Stats(ctypes.Structure):
 _lib = None
 
 
+_SUM_F64 = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_size_t)
+_SUM_U64 = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64), ctypes.c_size_t)
+_SUM_I64 = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.c_size_t)
+_GATHER_F64 = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                               ctypes.POINTER(ctypes.c_double), ctypes.c_size_t)
+
+
+class _Exchange(ctypes.Structure):
+    """trk_exchange: the caller's host-side collectives (include/trk.h)."""
+    _fields_ = [("user", ctypes.c_void_p), ("sum_f64", _SUM_F64), ("sum_u64", _SUM_U64), ("sum_i64", _SUM_I64),
+                ("gather_f64", _GATHER_F64)]
+
+
 def _declare(lib):
     P = ctypes.c_void_p
     D = ctypes.c_double
@@ -91,6 +104,7 @@ def _declare(lib):
         "trk_comm_get_unique_id": (I, [P]),
         "trk_ensemble_variant": (I, [P]),
         "trk_context_set_comm": (I, [P, P, I, I]),
+        "trk_context_set_exchange": (I, [P, P, I, I]),
         "trk_context_comm": (I, [P, ctypes.POINTER(I), ctypes.POINTER(I)]),
         "trk_abi_version": (I, []),
         "trk_type_code": (I, [ctypes.c_char_p]),
@@ -302,11 +316,13 @@ class Tracker:
         _check(self.lib, self.lib.trk_beam_store(self.ctx, _dptr(out), stride, ctypes.byref(n_left), None, None))
         return n_left.value, out
 
-    def track_ensemble(self, lattices, counts, n_passes, p_central, pass_offset=0, fast=True, variant=-1):
+    def track_ensemble(self, lattices, counts, n_passes, p_central, pass_offset=0, fast=True, variant=-1,
+                       compact_every=None):
         """Track the loaded beam as len(lattices) variants: variant v owns the
         next counts[v] particles (in load order).  The lattices must share
-        one element structure.  Returns the run statistics plus the launch
-        shape used ("variant")."""
+        one element structure.  compact_every: passes between survivor
+        compactions (0 = never; None = the library default, 64).  Returns the
+        run statistics plus the launch shape used ("variant")."""
         nats = [self.native(lat) for lat in lattices]
         arr = (ctypes.c_void_p * len(nats))(*[n.ptr.value for n in nats])
         offs = np.concatenate([[0], np.cumsum(np.asarray(counts, dtype=np.int64))]).astype(np.int64)
@@ -317,6 +333,8 @@ class Tracker:
         run.pass_offset = pass_offset
         run.fast_math = 1 if fast else 0
         run.variant = variant
+        if compact_every is not None:
+            run.compact_every = compact_every
         st = _Stats()
         _check(self.lib, self.lib.trk_track_ensemble(
             self.ctx, arr, len(nats),
@@ -440,6 +458,33 @@ class Tracker:
         buf = ctypes.create_string_buffer(bytes(unique_id), 128)
         _check(self.lib, self.lib.trk_context_set_comm(self.ctx, buf, nranks, rank))
 
+    def set_exchange(self, sum_f64, sum_u64, sum_i64, gather_f64, nranks, rank):
+        """Join a sharded run whose collectives the caller performs on host
+        arrays (an MPI or gloo host): sum_f64/sum_u64/sum_i64(a) sum the
+        numpy array `a` element-wise over the ranks in place;
+        gather_f64(send, recv) fills recv (nranks * len(send)) with every
+        rank's send in rank order.  nranks <= 0 leaves the run."""
+        def wrap_sum(fn, dtype):
+            def cb(_user, buf, n):
+                try:
+                    fn(np.ctypeslib.as_array(buf, shape=(n,)) if n else np.zeros(0, dtype))
+                    return 0
+                except Exception:  # the library reports the failure as TRK_ERR_NCCL
+                    return 1
+            return cb
+
+        def cb_gather(_user, send, recv, n):
+            try:
+                gather_f64(np.ctypeslib.as_array(send, shape=(n,)), np.ctypeslib.as_array(recv, shape=(n * nranks,)))
+                return 0
+            except Exception:
+                return 1
+
+        ex = _Exchange(None, _SUM_F64(wrap_sum(sum_f64, np.float64)), _SUM_U64(wrap_sum(sum_u64, np.uint64)),
+                       _SUM_I64(wrap_sum(sum_i64, np.int64)), _GATHER_F64(cb_gather))
+        self._exchange = ex  # the library holds the pointer while the exchange is set
+        _check(self.lib, self.lib.trk_context_set_exchange(self.ctx, ctypes.byref(ex), nranks, rank))
+
     def count(self):
         n = ctypes.c_long()
         _check(self.lib, self.lib.trk_beam_count(self.ctx, ctypes.byref(n)))
@@ -464,10 +509,15 @@ class Tracker:
         return nat[1]
 
     def track(self, lattice, n_passes, p_central, pass_offset=0, fast=True, variant=-1, time_kernels=False,
-              isr_seed=0):
+              isr_seed=0, compact_every=None):
+        """Track the loaded beam n_passes passes (trk_track).  compact_every:
+        passes between survivor compactions in fused multi-pass runs (0 =
+        never; None = the library default, 64)."""
         nat = self.native(lattice)
         run = _Run()
         self.lib.trk_run_defaults(ctypes.byref(run))
+        if compact_every is not None:
+            run.compact_every = compact_every
         run.p_central = p_central
         run.n_passes = n_passes
         run.pass_offset = pass_offset

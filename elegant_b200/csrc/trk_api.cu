@@ -26,6 +26,7 @@
 #include "trk_lattice.h"
 
 #include <cub/device/device_partition.cuh>
+#include <cub/device/device_select.cuh>
 
 #define CUDA_TRY(call)                                                                                       \
   do {                                                                                                       \
@@ -108,6 +109,14 @@ struct trk_context {
   long *d_nsel = nullptr;
   char *d_flags = nullptr;
   long perm_cap = 0;
+  /* survivor compaction (trk_run.compact_every): index list, its length,
+   * flags and identity indices for the selection, and the selection's
+   * scratch */
+  long *d_live = nullptr, *d_live_n = nullptr, *d_live_idx = nullptr;
+  char *d_live_flags = nullptr;
+  long live_cap = 0;
+  void *d_live_cub = nullptr;
+  size_t live_cub_cap = 0;
   long passes_done = 0; /* passes tracked since the beam was loaded */
   long n_original = 0;  /* particles at the start of the run (do_tracking's nOriginal) */
   long n_global = 0;    /* the same summed over the ranks of a sharded run */
@@ -122,6 +131,12 @@ struct trk_context {
   };
   std::vector<ScratchSlot> obs_scratch;
 };
+
+/* survivor compaction (defined with the ensemble launches) */
+extern "C" {
+static int prepare_live(trk_context *ctx);
+static int compact_live(trk_context *ctx);
+}
 
 /* Observer scratch of a context: `bytes` of device memory for (site, slot),
  * reused between calls and grown when a call needs more.  The observers
@@ -219,6 +234,14 @@ __global__ void alive_flags_kernel(const int32_t *lost_pass, long np, char *flag
     return;
   flags[i] = lost_pass[i] < 0;
   idx[i] = i;
+}
+
+/* survivors' indices for compaction: flags[i] = alive, idx[i] = i */
+__global__ void live_flags_kernel(const int32_t *lost_pass, long np, char *flags, long *idx) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (long)gridDim.x * blockDim.x) {
+    flags[i] = lost_pass[i] < 0;
+    idx[i] = i;
+  }
 }
 
 __global__ void gather_aos_kernel(const double *cols, long cap, const long *perm, long np, long stride, double *aos,
@@ -684,6 +707,7 @@ void trk_run_defaults(trk_run *run) {
   run->n_passes = 1;
   run->fast_math = 1;
   run->variant = -1;
+  run->compact_every = 64;
 }
 
 int trk_context_create(trk_context **out, int device) {
@@ -750,6 +774,11 @@ void trk_context_destroy(trk_context *ctx) {
   cudaFree(ctx->d_adj_dk);
   cudaFree(ctx->d_adj_mom);
   cudaFree(ctx->d_adj_param);
+  cudaFree(ctx->d_live);
+  cudaFree(ctx->d_live_n);
+  cudaFree(ctx->d_live_idx);
+  cudaFree(ctx->d_live_flags);
+  cudaFree(ctx->d_live_cub);
   for (trk_context::ScratchSlot &e : ctx->obs_scratch)
     cudaFree(e.p);
   ctx->obs_scratch.clear();
@@ -931,6 +960,24 @@ static int ensure_i64(trk_context *ctx) {
 
 int trk_comm_get_unique_id(void *id128) { return trk_comm_unique_id(id128); }
 
+int trk_context_set_exchange(trk_context *ctx, const trk_exchange *ex, int nranks, int rank) {
+  if (!ctx)
+    return trk_set_error(TRK_ERR_ARG, "null context");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  trk_comm_destroy(ctx->comm);
+  ctx->comm = nullptr;
+  cudaFree(ctx->d_gather);
+  ctx->d_gather = nullptr;
+  if (nranks <= 0)
+    return TRK_OK;
+  int rc = trk_comm_create_exchange(&ctx->comm, ex, nranks, rank);
+  if (rc)
+    return rc;
+  CUDA_TRY(cudaMalloc(&ctx->d_gather, sizeof(double) * 6 * nranks));
+  return TRK_OK;
+}
+
 int trk_context_set_comm(trk_context *ctx, const void *id128, int nranks, int rank) {
   if (!ctx)
     return trk_set_error(TRK_ERR_ARG, "null context");
@@ -1028,13 +1075,21 @@ int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, 
       pass_steps(c, fid, steps);
       bool simple = steps.size() == 1 && steps[0].kind == 0;
       long npass = 1;
+      bool compact = false;
       if (simple) {
-        /* merge passes while the schedule stays one full segment */
+        /* merge passes while the schedule stays one full segment (the
+         * first pass's fresh MAXAMP state is selected inside the kernel);
+         * with compaction, compact_every passes per launch */
         npass = pend - pass;
-        if (fresh >= 0 && pass == fresh && npass > 1) {
-          /* first pass uses the fresh MAXAMP state; still one launch */
+        if (run->compact_every > 0 && ctx->np > 0 && !ctx->comm && npass > 1) {
+          compact = true;
+          npass = std::min<long>(npass, run->compact_every);
+          if ((rc = prepare_live(ctx)) || (rc = compact_live(ctx)))
+            return rc;
         }
       }
+      ta.live = compact ? ctx->d_live : nullptr;
+      ta.live_n = compact ? ctx->d_live_n : nullptr;
       for (const Step &st : steps) {
         if (st.kind == 0) {
           ta.op_begin = st.ob;
@@ -1317,12 +1372,65 @@ int trk_track_matrix(trk_context *ctx, int order, const double *C, const double 
 /* ------------------------------------------------------------ ensembles */
 /* Launch shapes the autotuner tries (block size x resident blocks, see
  * TRK_N_VARIANTS), timed on a scratch copy of the beam. */
+/* Survivor compaction: buffers and selection scratch sized for the loaded
+ * beam (outside any stream capture), then compact_live() writes the
+ * ascending indices of the particles still alive into d_live and their
+ * number into *d_live_n, on the stream (capturable: no host sync, fixed
+ * sizes).  The tracking kernels then walk d_live instead of the whole beam,
+ * so lost particles no longer hold lanes of the warps. */
+static int prepare_live(trk_context *ctx) {
+  const long np = ctx->np;
+  if (np > ctx->live_cap) {
+    cudaFree(ctx->d_live);
+    cudaFree(ctx->d_live_idx);
+    cudaFree(ctx->d_live_flags);
+    ctx->d_live = ctx->d_live_idx = nullptr;
+    ctx->d_live_flags = nullptr;
+    ctx->live_cap = 0;
+    CUDA_TRY(cudaMalloc(&ctx->d_live, sizeof(long) * np));
+    CUDA_TRY(cudaMalloc(&ctx->d_live_idx, sizeof(long) * np));
+    CUDA_TRY(cudaMalloc(&ctx->d_live_flags, np));
+    ctx->live_cap = np;
+  }
+  if (!ctx->d_live_n)
+    CUDA_TRY(cudaMalloc(&ctx->d_live_n, sizeof(long)));
+  size_t tmp = 0;
+  CUDA_TRY(cub::DeviceSelect::Flagged(nullptr, tmp, ctx->d_live_idx, ctx->d_live_flags, ctx->d_live, ctx->d_live_n,
+                                      np, ctx->stream));
+  if (tmp > ctx->live_cub_cap) {
+    cudaFree(ctx->d_live_cub);
+    ctx->d_live_cub = nullptr;
+    ctx->live_cub_cap = 0;
+    CUDA_TRY(cudaMalloc(&ctx->d_live_cub, tmp));
+    ctx->live_cub_cap = tmp;
+  }
+  return TRK_OK;
+}
+
+static int compact_live(trk_context *ctx) {
+  const long np = ctx->np;
+  live_flags_kernel<<<grid_for(ctx, np, 256), 256, 0, ctx->stream>>>(ctx->d_lost_pass, np, ctx->d_live_flags,
+                                                                      ctx->d_live_idx);
+  size_t tmp = ctx->live_cub_cap;
+  CUDA_TRY(cub::DeviceSelect::Flagged(ctx->d_live_cub, tmp, ctx->d_live_idx, ctx->d_live_flags, ctx->d_live,
+                                      ctx->d_live_n, np, ctx->stream));
+  ctx->last_launches += 2;
+  return TRK_OK;
+}
+
 static const int k_tune_candidates[] = {1, 4, 7, 8};
 
 static int ensemble_launches(trk_context *ctx, const TrackArgs &base, int nv, int nops, int variant, int lean,
-                             bool fast, long p0, long n_passes, long chunk) {
+                             bool fast, long p0, long n_passes, long chunk, bool compact) {
   for (long pass = p0; pass < p0 + n_passes; pass += chunk) {
     TrackArgs ta = base;
+    if (compact) {
+      int rc = compact_live(ctx);
+      if (rc)
+        return rc;
+      ta.live = ctx->d_live;
+      ta.live_n = ctx->d_live_n;
+    }
     ta.op_begin = 0;
     ta.op_end = nops;
     ta.pass_begin = pass;
@@ -1445,7 +1553,11 @@ int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int
   const bool fast = run->fast_math != 0;
   const long p0 = run->pass_offset;
   const long fresh = ctx->passes_done == 0 ? p0 : -1;
-  const long chunk = 64;
+  /* passes per launch: compact_every when compacting, else 64 */
+  const bool compact = run->compact_every > 0 && ctx->np > 0;
+  const long chunk = compact ? run->compact_every : 64;
+  if (compact && (rc = prepare_live(ctx)))
+    return rc;
   ctx->last_launches = 0;
   TrackArgs base = track_args(ctx);
   base.fresh_pass = fresh;
@@ -1471,7 +1583,7 @@ int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int
         return rc;
       CUDA_TRY(cudaEventRecord(ctx->ev0, ctx->stream));
       if ((rc = ensemble_launches(ctx, base, n_variants, nops, cand, trk_lean_flavor(ctx->comp), fast, p0, tune_passes,
-                                  chunk)))
+                                  chunk, compact)))
         return rc;
       CUDA_TRY(cudaEventRecord(ctx->ev1, ctx->stream));
       CUDA_TRY(cudaEventSynchronize(ctx->ev1));
@@ -1503,7 +1615,7 @@ int trk_track_ensemble(trk_context *ctx, const trk_lattice *const *lattices, int
     cudaGraphExec_t exec = nullptr;
     CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     rc = ensemble_launches(ctx, base, n_variants, nops, variant, trk_lean_flavor(ctx->comp), fast, p0, run->n_passes,
-                           chunk);
+                           chunk, compact);
     cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
     if (rc)
       return rc;

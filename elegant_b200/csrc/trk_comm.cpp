@@ -10,6 +10,7 @@
 #include <dlfcn.h>
 #include <mutex>
 #include <nccl.h>
+#include <vector>
 
 #include "trk_lattice.h"
 
@@ -63,7 +64,49 @@ int nccl_err(ncclResult_t r, const char *what) {
 struct trk_comm {
   ncclComm_t comm = nullptr;
   int rank = 0, size = 1;
+  /* host-exchange communicators: the caller's collectives and a staging
+   * buffer (8-byte words) */
+  const trk_exchange *ex = nullptr;
+  std::vector<unsigned long long> host;
 };
+
+namespace {
+
+/* device buffer -> host, the caller's collective, host -> device */
+int stage_out(trk_comm *c, const void *dev, size_t bytes, size_t words, cudaStream_t st) {
+  if (c->host.size() < words)
+    c->host.resize(words);
+  if (cudaMemcpyAsync(c->host.data(), dev, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return trk_set_error(TRK_ERR_CUDA, "host exchange: device-to-host copy failed");
+  return TRK_OK;
+}
+
+int stage_in(trk_comm *c, void *dev, size_t bytes, cudaStream_t st) {
+  /* synchronous so the host buffer can be reused by the next exchange */
+  if (cudaMemcpyAsync(dev, c->host.data(), bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return trk_set_error(TRK_ERR_CUDA, "host exchange: host-to-device copy failed");
+  return TRK_OK;
+}
+
+int ex_rc(int r, const char *what) {
+  return r == 0 ? TRK_OK : trk_set_error(TRK_ERR_NCCL, "host exchange %s returned %d", what, r);
+}
+
+} // namespace
+
+int trk_comm_create_exchange(trk_comm **out, const trk_exchange *ex, int nranks, int rank) {
+  if (!out || !ex || !ex->sum_f64 || !ex->sum_u64 || !ex->sum_i64 || !ex->gather_f64 || nranks < 1 || rank < 0 ||
+      rank >= nranks)
+    return trk_set_error(TRK_ERR_ARG, "bad host-exchange arguments (nranks=%d, rank=%d)", nranks, rank);
+  trk_comm *c = new trk_comm();
+  c->rank = rank;
+  c->size = nranks;
+  c->ex = ex;
+  *out = c;
+  return TRK_OK;
+}
 
 int trk_comm_unique_id(void *out128) {
   if (!out128)
@@ -112,17 +155,49 @@ int trk_comm_rank(const trk_comm *c) { return c ? c->rank : 0; }
 int trk_comm_size(const trk_comm *c) { return c ? c->size : 1; }
 
 int trk_comm_sum_f64(trk_comm *c, double *buf, size_t n, cudaStream_t st) {
+  if (c->ex) {
+    int rc = stage_out(c, buf, sizeof(double) * n, n, st);
+    if (rc || (rc = ex_rc(c->ex->sum_f64(c->ex->user, (double *)c->host.data(), n), "sum_f64")))
+      return rc;
+    return stage_in(c, buf, sizeof(double) * n, st);
+  }
   return nccl_err(g_nccl.allReduce(buf, buf, n, ncclFloat64, ncclSum, c->comm, st), "ncclAllReduce(f64)");
 }
 
 int trk_comm_sum_u64(trk_comm *c, unsigned long long *buf, size_t n, cudaStream_t st) {
+  if (c->ex) {
+    int rc = stage_out(c, buf, sizeof(uint64_t) * n, n, st);
+    if (rc || (rc = ex_rc(c->ex->sum_u64(c->ex->user, (uint64_t *)c->host.data(), n), "sum_u64")))
+      return rc;
+    return stage_in(c, buf, sizeof(uint64_t) * n, st);
+  }
   return nccl_err(g_nccl.allReduce(buf, buf, n, ncclUint64, ncclSum, c->comm, st), "ncclAllReduce(u64)");
 }
 
 int trk_comm_sum_i64(trk_comm *c, long long *buf, size_t n, cudaStream_t st) {
+  if (c->ex) {
+    int rc = stage_out(c, buf, sizeof(int64_t) * n, n, st);
+    if (rc || (rc = ex_rc(c->ex->sum_i64(c->ex->user, (int64_t *)c->host.data(), n), "sum_i64")))
+      return rc;
+    return stage_in(c, buf, sizeof(int64_t) * n, st);
+  }
   return nccl_err(g_nccl.allReduce(buf, buf, n, ncclInt64, ncclSum, c->comm, st), "ncclAllReduce(i64)");
 }
 
 int trk_comm_gather_f64(trk_comm *c, const double *send, double *recv, size_t n, cudaStream_t st) {
+  if (c->ex) {
+    /* host layout: [send (n)] [recv (size * n)] */
+    const size_t words = n * (1 + (size_t)c->size);
+    int rc = stage_out(c, send, sizeof(double) * n, words, st);
+    if (rc)
+      return rc;
+    double *h = (double *)c->host.data();
+    if ((rc = ex_rc(c->ex->gather_f64(c->ex->user, h, h + n, n), "gather_f64")))
+      return rc;
+    if (cudaMemcpyAsync(recv, h + n, sizeof(double) * n * c->size, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      return trk_set_error(TRK_ERR_CUDA, "host exchange: host-to-device copy failed");
+    return TRK_OK;
+  }
   return nccl_err(g_nccl.allGather(send, recv, n, ncclFloat64, c->comm, st), "ncclAllGather(f64)");
 }

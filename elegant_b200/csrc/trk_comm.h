@@ -21,10 +21,15 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 
+#include "trk.h"
+
 struct trk_comm;
 
 /* 0 on success; message in trk_last_error() otherwise */
 int trk_comm_create(trk_comm **out, const void *unique_id, int nranks, int rank, int device);
+/* a communicator over the caller's host-side collectives (trk_exchange in
+ * trk.h): device buffers are staged through host memory around each call */
+int trk_comm_create_exchange(trk_comm **out, const trk_exchange *ex, int nranks, int rank);
 void trk_comm_destroy(trk_comm *c);
 int trk_comm_rank(const trk_comm *c);
 int trk_comm_size(const trk_comm *c);

@@ -37,16 +37,19 @@ struct CompiledLattice {
 };
 
 /* Launch shape of the tracking kernel when the caller names none, measured on
- * B200 (fast build): (128 threads, 6 blocks/SM; 80 registers) for lean
+ * B200: fast build (128 threads, 6 blocks/SM; 80 registers) for lean
  * lattices, (128, 5; 102 registers) for lean lattices with combined-function
- * bends, whose body spills at 80 registers, and (128, 4) otherwise. */
+ * bends, whose body spills at 80 registers; parity build (128, 6) for lean
+ * lattices without combined-function bends (the FODO ring with RF and wake:
+ * 94.6 ms per turn of 1e6 particles against 104.6 ms at (128, 4) and
+ * 95.6 ms at (256, 3)); (128, 4) otherwise. */
 /* lean kernel flavour of a compiled lattice: 0 general, 1 lean, 2 lean with
  * combined-function bends */
 inline int trk_lean_flavor(const CompiledLattice &c) { return c.lean ? (c.has_cfbend ? 2 : 1) : 0; }
 
 inline int trk_default_variant(bool fast, const CompiledLattice &c) {
-  if (fast && c.lean)
-    return c.has_cfbend ? 4 : 7;
+  if (c.lean && (fast || !c.has_cfbend))
+    return fast && c.has_cfbend ? 4 : 7;
   return 1;
 }
 

@@ -342,45 +342,126 @@ TRKCR_FN int trkcr_cos_small(double x, double *c) {
   return trkcr_round_test(hi, L, e, c);
 }
 
-TRKCR_FN double trkcr_sin(double x) {
+/*
+ * Tiny arguments (2^-27 <= |x| <= 2^-7, the CSBEND substep angles and most
+ * slopes): the correction to the leading term (x for sin and asin, 1 for
+ * cos) is formed in plain double, with a rigorous relative error bound, and
+ * the same rounding test decides.  With |x| <= 2^-7 the correction is at
+ * most 2^-15.4 |x| (sin, asin) or 2^-15 (cos), so a relative error of
+ * 2^-50 in it is a few 2^-66 of the result: the test then fails for about
+ * one call in 2^13 (cos near |x| = 2^-7) to far fewer (smaller |x|), and
+ * the caller takes the next path.
+ *
+ * Error budget of the correction c (sin, asin: c = x^3 P(x^2); cos:
+ * c = x^2 Q(x^2), result 1 - c): x^2 rounded (2^-53), x^3 or the final
+ * product rounded (2^-53 each), P or Q rounded (2^-53 from its last FMA and
+ * 2^-53.4 from its leading coefficient; the other terms are scaled by
+ * x^2 <= 2^-14), truncation of the series (below 2^-56 relative): in all
+ * below 2^-50.7 |c|.  The test widens c by e = 2^-49 |c|, which covers that
+ * error and the rounding of c +- e.
+ * Series: sin  P = -1/6 + z/120 - z^2/5040          (next: z^3/9!, 2^-58 rel.)
+ *         asin P = 1/6 + 3z/40 + 5z^2/112 + 35z^3/1152 + 63z^4/2816
+ *                                                    (next: 231 z^5/13312)
+ *         cos  Q = 1/2 - z/24 + z^2/720              (next: z^3/8!, 2^-56 rel.)
+ */
+#define TRKCR_TINY 0x1p-7
+
+TRKCR_FN int trkcr_tiny_test(double lead, double c, double *out) {
+  const double ac = fabs(c);
+  const double u = TRKCR_ADD(lead, TRKCR_FMA(ac, 0x1p-49, c));
+  const double v = TRKCR_ADD(lead, TRKCR_FMA(-ac, 0x1p-49, c));
+  *out = u;
+  return u == v;
+}
+
+/* the corrections: sin x = x + c, cos x = 1 + c, asin y = y + c */
+TRKCR_FN double trkcr_sin_tiny_c(double x, double z) {
+  double P = TRKCR_FMA(z, -0x1.a01a01a01a01ap-13, 0x1.1111111111111p-7);
+  P = TRKCR_FMA(z, P, -0x1.5555555555555p-3);
+  return TRKCR_MUL(TRKCR_MUL(x, z), P);
+}
+
+TRKCR_FN double trkcr_cos_tiny_c(double z) {
+  double Q = TRKCR_FMA(z, 0x1.6c16c16c16c17p-10, -0x1.5555555555555p-5);
+  Q = TRKCR_FMA(z, Q, 0.5);
+  return -TRKCR_MUL(z, Q);
+}
+
+TRKCR_FN double trkcr_asin_tiny_c(double y, double z) {
+  double P = TRKCR_FMA(z, 63.0 / 2816.0, 35.0 / 1152.0);
+  P = TRKCR_FMA(z, P, 5.0 / 112.0);
+  P = TRKCR_FMA(z, P, 3.0 / 40.0);
+  P = TRKCR_FMA(z, P, 0x1.5555555555555p-3);
+  return TRKCR_MUL(TRKCR_MUL(y, z), P);
+}
+
+/* sin x, 2^-26 <= |x| <= 2^-7, z = RN(x^2) */
+TRKCR_FN int trkcr_sin_tiny(double x, double z, double *s) { return trkcr_tiny_test(x, trkcr_sin_tiny_c(x, z), s); }
+
+/* cos x, 2^-27 <= |x| <= 2^-7, z = RN(x^2) */
+TRKCR_FN int trkcr_cos_tiny(double z, double *c) { return trkcr_tiny_test(1.0, trkcr_cos_tiny_c(z), c); }
+
+/* asin y, 2^-26 <= |y| <= 2^-7, z = RN(y^2) */
+TRKCR_FN int trkcr_asin_tiny(double y, double z, double *a) {
+  return trkcr_tiny_test(y, trkcr_asin_tiny_c(y, z), a);
+}
+
+/* the paths of |x| <= 2^-5 after the tiny one: double-double correction,
+ * then the full double-double evaluation */
+TRKCR_SLOW double trkcr_sin_mid(double x) {
   double s;
   if (fabs(x) <= TRKCR_SMALL && trkcr_sin_small(x, &s))
     return s;
   return trkcr_sin_slow(x);
 }
 
-TRKCR_FN double trkcr_cos(double x) {
+TRKCR_SLOW double trkcr_cos_mid(double x) {
   double c;
   if (fabs(x) <= TRKCR_SMALL && trkcr_cos_small(x, &c))
     return c;
   return trkcr_cos_slow(x);
 }
 
+TRKCR_FN double trkcr_sin(double x) {
+  const double ax = fabs(x);
+  if (ax < 0x1p-26)
+    return x;
+  double s;
+  if (ax <= TRKCR_TINY && trkcr_sin_tiny(x, TRKCR_MUL(x, x), &s))
+    return s;
+  return trkcr_sin_mid(x);
+}
+
+TRKCR_FN double trkcr_cos(double x) {
+  const double ax = fabs(x);
+  if (ax < 0x1p-27)
+    return 1.0;
+  double c;
+  if (ax <= TRKCR_TINY && trkcr_cos_tiny(TRKCR_MUL(x, x), &c))
+    return c;
+  return trkcr_cos_mid(x);
+}
+
 /* sin and cos of one argument (the CSBEND drift needs both): x^2 formed once */
 TRKCR_FN void trkcr_sincos(double x, double *s, double *c) {
   const double ax = fabs(x);
-  if (ax <= TRKCR_SMALL) {
-    if (ax < 0x1p-27) {
-      *s = x;
-      *c = 1.0;
-      return;
-    }
-    double L, e, so, co;
-    const double zh = TRKCR_MUL(x, x);
-    const double zl = TRKCR_FMA(x, x, -zh);
-    int ok = 1;
-    if (ax < 0x1p-26)
-      so = x;
-    else
-      ok = trkcr_round_test(trkcr_sin_parts(x, zh, zl, &L, &e), L, e, &so);
-    if (ok && trkcr_round_test(trkcr_cos_parts(zh, zl, &L, &e), L, e, &co)) {
-      *s = so;
-      *c = co;
-      return;
-    }
+  if (ax < 0x1p-27) {
+    *s = x;
+    *c = 1.0;
+    return;
   }
-  *s = trkcr_sin_slow(x);
-  *c = trkcr_cos_slow(x);
+  if (ax <= TRKCR_TINY) {
+    const double z = TRKCR_MUL(x, x);
+    if (ax < 0x1p-26)
+      *s = x;
+    else if (!trkcr_sin_tiny(x, z, s))
+      *s = trkcr_sin_mid(x);
+    if (!trkcr_cos_tiny(z, c))
+      *c = trkcr_cos_mid(x);
+    return;
+  }
+  *s = trkcr_sin_mid(x);
+  *c = trkcr_cos_mid(x);
 }
 
 /* tan = sin/cos with a double-double quotient (bend edges only: not inlined) */
@@ -427,11 +508,9 @@ TRKCR_FN double trkcr_asin_parts(double y, double zh, double zl, double *L, doub
   return trkcr_odd_small(y, 1.0, c2, zh, zl, th, tl, L, e);
 }
 
-TRKCR_FN double trkcr_asin(double y) {
+TRKCR_SLOW double trkcr_asin_mid(double y) {
   const double ay = fabs(y);
   if (ay <= TRKCR_SMALL) {
-    if (ay < 0x1p-26)
-      return y;
     double L, e, out;
     const double zh = TRKCR_MUL(y, y);
     const double hi = trkcr_asin_parts(y, zh, TRKCR_FMA(y, y, -zh), &L, &e);
@@ -439,6 +518,16 @@ TRKCR_FN double trkcr_asin(double y) {
       return out;
   }
   return trkcr_asin_slow(y);
+}
+
+TRKCR_FN double trkcr_asin(double y) {
+  const double ay = fabs(y);
+  if (ay < 0x1p-26)
+    return y;
+  double a;
+  if (ay <= TRKCR_TINY && trkcr_asin_tiny(y, TRKCR_MUL(y, y), &a))
+    return a;
+  return trkcr_asin_mid(y);
 }
 
 #endif

@@ -523,6 +523,103 @@ done:
 }
 
 /* ---------------------------------------------------------------- CSBEND */
+#if !TRK_FAST
+/* RN(a/b) given y ~ 1/b with relative error below 2^-50 (a reciprocal
+ * rounded once, on the host or by __drcp_rn): q0 = RN(a y), the residual
+ * r = RN(a - b q0) by one FMA and t = RN(r y) ~ (a - b q0)/b to within
+ * 2^-49.7 relative; a/b = q0 + (a - b q0)/b, so when q0 + t +- 2^-48 |t|
+ * round to the same double that double is RN(a/b).  Otherwise (one call in
+ * ~2^45, or a zero, non-finite or tiny quotient) the full IEEE division. */
+__device__ __forceinline__ double div_rn_by(double a, double b, double y) {
+  const double q0 = __dmul_rn(a, y);
+  const double t = __dmul_rn(__fma_rn(-b, q0, a), y);
+  const double at = fabs(t);
+  const double hi = __dadd_rn(q0, __fma_rn(at, 0x1p-48, t));
+  const double lo = __dadd_rn(q0, __fma_rn(-at, 0x1p-48, t));
+  if (hi == lo && fabs(hi) > 0x1p-900)
+    return hi;
+  return __ddiv_rn(a, b);
+}
+
+/* Body of a pure-dipole CSBEND in the parity build: integrate_csbend_ordn
+ * (src/csbend.c:1561-1660) with Fx = 0, Fy = 1 and no radiation, every
+ * operation rounded as the reference rounds it, with these shortcuts that
+ * change no result:
+ *  - 1 + delta is constant through the body, and so is f = sqrt((1+delta)^2
+ *    - QY^2) while QY^2 rounds to the same double (QY moves only by the
+ *    (1+delta) divide/multiply round trip, by an ulp at most): f and its
+ *    reciprocal are re-formed only when QY^2 changes;
+ *  - divisions by f, rho0, rho_actual and 1 + delta use a reciprocal formed
+ *    once (div_rn_by: the IEEE quotient, certified);
+ *  - the kick's Fx term, ((ds (1 + X/rho0)) 0)/rho_actual, is a signed zero
+ *    (or NaN), formed by multiplying by 1/rho_actual instead of dividing;
+ *  - dz_lost is summed only for a lost particle, from the substeps done.
+ * Loss conditions, their order and the state left at a loss are the
+ * reference's: aperture at the start of each slice, f <= 0, |QX/f| > 1 and
+ * cos(dsh/rho0 + phi) == 0 before any coordinate of the substep changes. */
+__device__ __forceinline__ bool bend_dipole_exact(const double *__restrict__ d, int nSlices, int nSub, double rho0,
+                                                  bool roundtrip, const trk_aperture *ap, bool aptilt, double apc,
+                                                  double aps, double &X, double &QX, double &Y, double &QY,
+                                                  const double D, double &dist, int &done) {
+  const double opd = __dadd_rn(1.0, D);
+  const double opd2 = __dmul_rn(opd, opd);
+  const double yopd = __drcp_rn(opd);
+  const double yrho0 = __ldg(&d[BD_RHOINV]);
+  const double rho_a = __ldg(&d[BD_RHOA]), yrho_a = __ldg(&d[BD_INVRHOA]);
+  double qy2 = __dmul_rn(QY, QY);
+  double f2 = __dsub_rn(opd2, qy2);
+  double f = __dsqrt_rn(f2);
+  double yf = __drcp_rn(f);
+  done = 0;
+  for (int i = 0; i < nSlices; i++) {
+    if (!check_aperture(X, Y, ap, aptilt, apc, aps))
+      return false;
+    for (int j = 0; j < nSub; j++) {
+      if (f2 <= 0)
+        return false;
+      const double sin_phi = div_rn_by(QX, f, yf);
+      if (fabs(sin_phi) > 1)
+        return false;
+      const double phi = trkcr_asin(sin_phi);
+      double sine, cosi;
+      trkcr_sincos(__dadd_rn(__ldg(&d[BD_ARG + j]), phi), &sine, &cosi);
+      if (cosi == 0)
+        return false;
+      const double tang = __ddiv_rn(sine, cosi);
+      const double cos_phi = trkcr_cos(phi);
+      QX = __dmul_rn(f, sine);
+      const double a3 = div_rn_by(__dmul_rn(__dadd_rn(rho0, X), cos_phi), f, yf);
+      const double factor = __dmul_rn(a3, __dsub_rn(tang, __ddiv_rn(sin_phi, cos_phi)));
+      Y = __dadd_rn(Y, __dmul_rn(QY, factor));
+      dist = __dadd_rn(dist, __dmul_rn(factor, opd));
+      done++;
+      const double fr = __ddiv_rn(cos_phi, cosi);
+      X = __dadd_rn(__dmul_rn(rho0, __dsub_rn(fr, 1.0)), __dmul_rn(fr, X));
+      if (j == nSub - 1)
+        break;
+      /* kick: QX += -ds (1 + X/rho0) Fy / rho_a, QY += ds (1 + X/rho0) Fx / rho_a */
+      const double ds = __ldg(&d[BD_DS + j]);
+      const double w = __dmul_rn(ds, __dadd_rn(1.0, div_rn_by(X, rho0, yrho0)));
+      QX = __dadd_rn(QX, div_rn_by(-w, rho_a, yrho_a));
+      QY = __dadd_rn(QY, __dmul_rn(__dmul_rn(w, 0.0), yrho_a));
+      if (roundtrip) {
+        /* QX /= (1 + delta); QY /= ...; QX *= (1 + delta); QY *= ... */
+        QX = __dmul_rn(div_rn_by(QX, opd, yopd), opd);
+        QY = __dmul_rn(div_rn_by(QY, opd, yopd), opd);
+      }
+      const double q2 = __dmul_rn(QY, QY);
+      if (q2 != qy2) {
+        qy2 = q2;
+        f2 = __dsub_rn(opd2, qy2);
+        f = __dsqrt_rn(f2);
+        yf = __drcp_rn(f);
+      }
+    }
+  }
+  return true;
+}
+#endif
+
 /* computeCSBENDFields (src/csbend.c:99-172): y powers are formed on the fly
  * (the same products as the reference's yp[] table) so nothing is indexed
  * in local memory. */
@@ -909,18 +1006,21 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
   bool ok = true;
   double dist = 0, dz_lost = 0;
   const double sl = __ldg(&d[BD_SLICE]);
-#if TRK_FAST
   if (fmode == 0 && !(flags & BF_RAD)) { /* the radiating dipole takes the general body */
     int done = 0;
+#if TRK_FAST
     if (nSub == 4)
       ok = bend_dipole_fast<4>(d, nSlices, nSub, rho0, ap, aptilt, apc, aps, X, QX, Y, QY, D, dist, done);
     else
       ok = bend_dipole_fast<0>(d, nSlices, nSub, rho0, ap, aptilt, apc, aps, X, QX, Y, QY, D, dist, done);
+#else
+    ok = bend_dipole_exact(d, nSlices, nSub, rho0, (flags & BF_ISR_ROUNDTRIP) != 0, ap, aptilt, apc, aps, X, QX, Y,
+                           QY, D, dist, done);
+#endif
     if (!ok) /* loss position: the drift substeps completed so far */
       for (int k = 0; k < done; k++)
         dz_lost += __ldg(&d[BD_DSH + k % nSub]);
   } else
-#endif
   for (int i = 0; i < nSlices && ok; i++) {
     if (!check_aperture(X, Y, ap, aptilt, apc, aps)) {
       ok = false;
@@ -1795,7 +1895,9 @@ __device__ __forceinline__ int ens_variant(const long *__restrict__ offsets, int
 template <int BLOCK, int MINB, int LEAN>
 __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(TrackArgs a) {
   const long stride = (long)gridDim.x * blockDim.x;
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+  const long n = a.live ? __ldg(a.live_n) : a.n;
+  for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+    const long i = a.live ? __ldg(&a.live[k]) : k;
     if (a.lost_pass[i] >= 0)
       continue;
     const trk_op *ops = a.ops;
@@ -1838,10 +1940,13 @@ __device__ __forceinline__ bool lean_op(const TrackArgs &a, const trk_op *__rest
 template <int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) track_kernel2(TrackArgs a) {
   const long tile = 2L * BLOCK;
-  for (long base = (long)blockIdx.x * tile; base < a.n; base += (long)gridDim.x * tile) {
-    const long i0 = base + threadIdx.x, i1 = i0 + BLOCK;
-    bool al0 = i0 < a.n && a.lost_pass[i0] < 0;
-    bool al1 = i1 < a.n && a.lost_pass[i1] < 0;
+  const long n = a.live ? __ldg(a.live_n) : a.n;
+  for (long base = (long)blockIdx.x * tile; base < n; base += (long)gridDim.x * tile) {
+    const long k0 = base + threadIdx.x, k1 = k0 + BLOCK;
+    const long i0 = k0 < n && a.live ? __ldg(&a.live[k0]) : k0;
+    const long i1 = k1 < n && a.live ? __ldg(&a.live[k1]) : k1;
+    bool al0 = k0 < n && a.lost_pass[i0] < 0;
+    bool al1 = k1 < n && a.lost_pass[i1] < 0;
     if (!al0 && !al1)
       continue;
     Part p0, p1;

@@ -46,6 +46,10 @@ struct TrackArgs {
   const double *id;
   unsigned long long isr_seed;
   double isr_limit;
+  /* survivor compaction: when `live` is set the kernel tracks particles
+   * live[0 .. *live_n) (indices into the beam, ascending) instead of 0..n */
+  const long *live;
+  const long *live_n;
 };
 
 struct TimeStatsArgs {

@@ -124,7 +124,9 @@ typedef struct {
   int32_t fast_math;     /* 0: reference operation order, no FMA contraction (parity build);
                             1: transcendental-free CSBEND drift and FMA (fast build) */
   int32_t block_size;    /* unused, kept 0 (block shape comes with the variant) */
-  int32_t compact_every; /* compact survivors every N passes in fused runs (0 = never) */
+  int32_t compact_every; /* fused multi-pass runs (one-segment lattices, ensembles): track the survivors
+                            compacted into an index list, re-formed every N passes, so lost particles
+                            hold no lanes (0 = never; trk_run_defaults sets 64) */
   int32_t variant;       /* tracking-kernel variant (block size x occupancy); -1 = autotuned choice */
   int32_t time_kernels;  /* 1: bracket every tracking-kernel launch with CUDA events (trk_stats.track_ms) */
   uint64_t isr_seed;     /* seed of the incoherent-radiation (ISR) deviates; each deviate is a function of
@@ -167,6 +169,28 @@ void *trk_context_stream(trk_context *ctx);
 int trk_comm_get_unique_id(void *id128);
 int trk_context_set_comm(trk_context *ctx, const void *id128, int nranks, int rank);
 int trk_context_comm(const trk_context *ctx, int *rank, int *nranks);
+
+/* The same sharded run over the caller's own host-side collectives instead
+ * of NCCL: the route of a Pelegant-style host that already runs MPI (the
+ * reference's MPI_Allreduce / MPI_Allgather over host buffers,
+ * src/wake.c:226-233, src/trwake.c:195-204, src/simple_rfca.c:222-230)
+ * and has no NCCL.  At each exchange the library copies the device buffer
+ * to host memory, synchronizes the context's stream, calls the callback
+ * (which must perform the collective over all ranks and return 0, or
+ * nonzero to fail the call with TRK_ERR_NCCL), and copies the result back.
+ * The callbacks are called from the thread that drives the context, in the
+ * same order on every rank.  `ex` must stay valid while it is set;
+ * trk_context_set_comm (either form) replaces it. */
+typedef struct {
+  void *user;
+  /* in-place element-wise sum over ranks of n values */
+  int (*sum_f64)(void *user, double *buf, size_t n);
+  int (*sum_u64)(void *user, uint64_t *buf, size_t n);
+  int (*sum_i64)(void *user, int64_t *buf, size_t n);
+  /* recv[r * n + k] = rank r's send[k] */
+  int (*gather_f64)(void *user, const double *send, double *recv, size_t n);
+} trk_exchange;
+int trk_context_set_exchange(trk_context *ctx, const trk_exchange *ex, int nranks, int rank);
 
 /* Copy a host AoS beam (np particles, `stride` doubles each, stride >= 7,
  * column 6 = particle id) to the device SoA.  Replaces gpuBaseInit's copy

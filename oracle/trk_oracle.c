@@ -954,6 +954,93 @@ int orc_cr_parts(int kind, double x, double *out) {
   return trkcr_round_test(hi, L, e, &r);
 }
 
+/* Self-test of the tiered correctly rounded functions: n arguments drawn
+ * uniformly from [lo, hi] (log_mag: magnitudes log-uniform in [lo, hi],
+ * random sign), each function against its double-double evaluation
+ * (trkcr_*_slow, ~2^-100 relative).  Returns the number of disagreements;
+ * *tiny_hits counts the calls whose tiny-argument test accepted and
+ * *max_rel the largest relative error of the tiny path's correction
+ * (against the double-double value minus the leading term), which the
+ * tiny path's rounding test assumes to be below 2^-50.7. */
+static unsigned long long orc_splitmix(unsigned long long *st) {
+  unsigned long long z = (*st += 0x9e3779b97f4a7c15ULL);
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+long orc_cr_selftest(int kind, double lo, double hi, int log_mag, long n, unsigned long long seed, long *tiny_hits,
+                     double *max_rel) {
+  unsigned long long st = seed;
+  long bad = 0, hits = 0;
+  double mrel = 0;
+  for (long k = 0; k < n; k++) {
+    const double u = (double)(orc_splitmix(&st) >> 11) * 0x1p-53;
+    double x;
+    if (log_mag) {
+      x = exp(log(lo) + u * (log(hi) - log(lo)));
+      if (orc_splitmix(&st) & 1)
+        x = -x;
+    } else
+      x = lo + u * (hi - lo);
+    double got, want, t;
+    const double z = x * x, ax = fabs(x);
+    if (kind <= 2 && ax >= 0x1p-26 && ax <= TRKCR_TINY) {
+      /* the exact correction from the double-double value (hi - lead is
+       * exact: hi and the lead are within a factor of two) */
+      trkcr_dd v;
+      double lead, c;
+      if (kind == 0) {
+        v = trkcr_sin_dd(x);
+        lead = x;
+        c = trkcr_sin_tiny_c(x, z);
+      } else if (kind == 1) {
+        v = trkcr_cos_dd(x);
+        lead = 1.0;
+        c = trkcr_cos_tiny_c(z);
+      } else {
+        const double a0 = asin(x);
+        const trkcr_dd sa = trkcr_sin_dd(a0);
+        /* asin x = a0 + (x - sin a0)/cos a0 to ~2^-100 */
+        const double d = ((x - sa.hi) - sa.lo) / cos(a0);
+        v = trkcr_two_sum(a0, d);
+        lead = x;
+        c = trkcr_asin_tiny_c(x, z);
+      }
+      const double ce = (v.hi - lead) + v.lo;
+      const double rel = fabs(c - ce) / fabs(ce);
+      if (rel > mrel)
+        mrel = rel;
+    }
+    if (kind == 0) {
+      got = trkcr_sin(x);
+      want = trkcr_sin_slow(x);
+      hits += ax >= 0x1p-26 && ax <= TRKCR_TINY && trkcr_sin_tiny(x, z, &t);
+    } else if (kind == 1) {
+      got = trkcr_cos(x);
+      want = trkcr_cos_slow(x);
+      hits += ax >= 0x1p-27 && ax <= TRKCR_TINY && trkcr_cos_tiny(z, &t);
+    } else if (kind == 2) {
+      got = trkcr_asin(x);
+      want = trkcr_asin_slow(x);
+      hits += ax >= 0x1p-26 && ax <= TRKCR_TINY && trkcr_asin_tiny(x, z, &t);
+    } else {
+      double s, c;
+      trkcr_sincos(x, &s, &c);
+      got = s - trkcr_sin_slow(x);
+      want = c - trkcr_cos_slow(x);
+      bad += !(got == 0 && want == 0);
+      continue;
+    }
+    if (!(got == want) && !(got != got && want != want))
+      bad++;
+  }
+  if (tiny_hits)
+    *tiny_hits = hits;
+  if (max_rel)
+    *max_rel = mrel;
+  return bad;
+}
+
 static void dd_acc(double *hi, double *lo, double v) {
   double s = *hi + v, bb = s - *hi, e = (*hi - (s - bb)) + (v - bb);
   e += *lo;

@@ -84,3 +84,22 @@ def test_correct_rounding(kind, lo, hi):
     xs = rng.uniform(lo, hi, 150)
     bad = [x for x in xs if f(float(x)) != float(ex(float(x)))]
     assert not bad, f"{kind}: {len(bad)} of {len(xs)} not correctly rounded, e.g. {bad[:3]}"
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2, 3])
+@pytest.mark.parametrize("lo,hi,log_mag", [(2.0 ** -30, 2.0 ** -7, 1), (-2.0 ** -7, 2.0 ** -7, 0),
+                                           (2.0 ** -7, 2.0 ** -5, 1), (-0.05, 0.05, 0)])
+def test_tiered_paths_agree_with_double_double(kind, lo, hi, log_mag):
+    """The tiny- and small-argument paths (plain-double and double-double
+    corrections behind a rounding test) against the full double-double
+    evaluation on 1e6 arguments per range (kind 3: sin and cos of one
+    argument together), and the tiny path's correction within the relative
+    error its rounding test assumes (2^-50.7; the test widens by 2^-49)."""
+    import ctypes
+    lib = pyoracle.load()
+    hits, mrel = ctypes.c_long(), ctypes.c_double()
+    bad = lib.orc_cr_selftest(kind, lo, hi, log_mag, 1_000_000, 4242 + kind, ctypes.byref(hits), ctypes.byref(mrel))
+    assert bad == 0
+    assert mrel.value < 2.0 ** -50.7
+    if hi <= 2.0 ** -7 and kind < 3:
+        assert hits.value > 0.8 * 1_000_000  # the tiny path takes nearly every call

@@ -106,3 +106,32 @@ def test_ensemble_rejects_mixed_structures_and_wakes():
             trk.track_ensemble([configs.c2_lattice(cells=1, n_bins=50)] * 2, [10, 10], 1, PC)
         with pytest.raises(TrackingError):
             trk.track_ensemble(lats, [10, 5], 1, PC)
+
+
+@pytest.mark.parametrize("fast", [True, False])
+def test_compaction_changes_no_result(fast):
+    """Survivor compaction (trk_run.compact_every) only changes which lanes
+    track which particles: an ensemble and a fused multi-pass run give the
+    same bits with compaction every 3 passes, every 64 (the default) and
+    never."""
+    counts = [400, 700, 0, 250]
+    lats, beams = _variants(counts)
+    beam = np.concatenate(beams)
+    passes = 10
+    outs = []
+    with Tracker(0) as trk:
+        for every in (0, 3, None):
+            trk.load(beam)
+            st = trk.track_ensemble(lats, counts, passes, PC, fast=fast, compact_every=every)
+            outs.append((st, trk.store(stride=7, with_loss=True)))
+        for every in (0, 3):
+            trk.load(beams[0])
+            st = trk.track(lats[0], passes, PC, fast=fast, compact_every=every)
+            outs.append((st, trk.store(stride=7, with_loss=True)))
+    for (st_a, a), (st_b, b) in [(outs[0], outs[1]), (outs[0], outs[2]), (outs[3], outs[4])]:
+        assert a[0] == b[0] and st_a["particle_passes"] == st_b["particle_passes"]
+        ia, ib = np.argsort(a[1][:, 6]), np.argsort(b[1][:, 6])
+        same = (a[1][ia] == b[1][ib]) | (np.isnan(a[1][ia]) & np.isnan(b[1][ib]))
+        assert same.all()
+        assert np.array_equal(a[2][ia], b[2][ib]) and np.array_equal(a[3][ia], b[3][ib])
+    assert 0 < outs[0][1][0] < sum(counts)
