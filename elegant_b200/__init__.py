@@ -107,6 +107,7 @@ def _declare(lib):
         "trk_context_set_exchange": (I, [P, P, I, I]),
         "trk_context_comm": (I, [P, ctypes.POINTER(I), ctypes.POINTER(I)]),
         "trk_abi_version": (I, []),
+        "trk_test_fail_allocation": (I, [I]),
         "trk_type_code": (I, [ctypes.c_char_p]),
         "trk_param_count": (I, [I]),
         "trk_param_name": (ctypes.c_char_p, [I, I]),

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -132,6 +133,11 @@ struct trk_context {
   std::vector<ScratchSlot> obs_scratch;
 };
 
+/* Passes per launch when compacting: 1, 2, 4, ... up to compact_every,
+ * so particles lost in the first turns (most of a dynamic-aperture grid's
+ * outer points) free their lanes early, then every compact_every passes. */
+static long compact_chunk(long k, long every) { return k >= 30 ? every : std::min<long>(every, 1L << k); }
+
 /* survivor compaction (defined with the ensemble launches) */
 extern "C" {
 static int prepare_live(trk_context *ctx);
@@ -177,6 +183,20 @@ int grid_for(const trk_context *ctx, long n, int block) {
   return (int)std::min(g, cap);
 }
 
+/* Test hook (trk_test_fail_allocation): the number of growing allocations
+ * still to succeed before one is refused; negative = never refuse. */
+static std::atomic<int> g_fail_alloc_after{-1};
+
+/* true when the hook refuses this allocation (it then disarms itself) */
+static bool alloc_refused() {
+  int v = g_fail_alloc_after.load();
+  while (v >= 0) {
+    if (g_fail_alloc_after.compare_exchange_weak(v, v - 1))
+      return v == 0;
+  }
+  return false;
+}
+
 template <typename T> int ensure(T **p, size_t &cap, size_t need) {
   if (need <= cap && *p)
     return TRK_OK;
@@ -184,6 +204,10 @@ template <typename T> int ensure(T **p, size_t &cap, size_t need) {
     cudaFree(*p);
   *p = nullptr;
   size_t n = std::max(need, (size_t)1);
+  if (alloc_refused()) {
+    cap = 0;
+    return trk_set_error(TRK_ERR_NOMEM, "cudaMalloc of %zu bytes refused (test hook)", n * sizeof(T));
+  }
   cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
   if (e != cudaSuccess) {
     cap = 0;
@@ -329,6 +353,8 @@ int ensure_beam(trk_context *ctx, long np) {
   ctx->d_lost_pass = ctx->d_lost_elem = nullptr;
   ctx->cap = 0;
   long cap = std::max(np, 1L);
+  if (alloc_refused())
+    return trk_set_error(TRK_ERR_NOMEM, "device beam allocation for %ld particles refused (test hook)", np);
   if (cudaMalloc(&ctx->d_cols, sizeof(double) * 7 * cap) != cudaSuccess ||
       cudaMalloc(&ctx->d_lost_pass, sizeof(int32_t) * cap) != cudaSuccess ||
       cudaMalloc(&ctx->d_lost_elem, sizeof(int32_t) * cap) != cudaSuccess)
@@ -699,6 +725,11 @@ int check_status(trk_context *ctx) {
 /* ======================================================================= C ABI */
 extern "C" {
 
+int trk_test_fail_allocation(int after) {
+  g_fail_alloc_after.store(after < 0 ? -1 : after);
+  return TRK_OK;
+}
+
 void trk_run_defaults(trk_run *run) {
   if (!run)
     return;
@@ -817,6 +848,8 @@ int trk_beam_load(trk_context *ctx, const double *coord, long np, long stride) {
   if (!ctx || (np > 0 && !coord) || np < 0 || stride < 7)
     return trk_set_error(TRK_ERR_ARG, "bad beam (np=%ld, stride=%ld)", np, stride);
   CUDA_TRY(cudaSetDevice(ctx->device));
+  /* the previous beam is gone from here on: a failed load leaves no beam */
+  ctx->np = ctx->n_original = ctx->n_global = 0;
   int rc = ensure_beam(ctx, np);
   if (rc)
     return rc;
@@ -839,6 +872,7 @@ int trk_beam_load_device(trk_context *ctx, const double *d_soa, long np, long ld
   if (!ctx || (np > 0 && !d_soa) || np < 0 || ld < np)
     return trk_set_error(TRK_ERR_ARG, "bad device beam (np=%ld, ld=%ld)", np, ld);
   CUDA_TRY(cudaSetDevice(ctx->device));
+  ctx->np = ctx->n_original = ctx->n_global = 0;
   int rc = ensure_beam(ctx, np);
   if (rc)
     return rc;
@@ -1070,6 +1104,7 @@ int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, 
     std::vector<Step> steps;
     long pass = p0;
     const long pend = p0 + run->n_passes;
+    long n_compact = 0;
     while (pass < pend) {
       std::vector<int> fid = ctx->rf_fid_done;
       pass_steps(c, fid, steps);
@@ -1083,7 +1118,7 @@ int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, 
         npass = pend - pass;
         if (run->compact_every > 0 && ctx->np > 0 && !ctx->comm && npass > 1) {
           compact = true;
-          npass = std::min<long>(npass, run->compact_every);
+          npass = std::min<long>(npass, compact_chunk(n_compact++, run->compact_every));
           if ((rc = prepare_live(ctx)) || (rc = compact_live(ctx)))
             return rc;
         }
@@ -1421,8 +1456,10 @@ static int compact_live(trk_context *ctx) {
 static const int k_tune_candidates[] = {1, 4, 7, 8};
 
 static int ensemble_launches(trk_context *ctx, const TrackArgs &base, int nv, int nops, int variant, int lean,
-                             bool fast, long p0, long n_passes, long chunk, bool compact) {
+                             bool fast, long p0, long n_passes, long every, bool compact) {
+  long k = 0, chunk;
   for (long pass = p0; pass < p0 + n_passes; pass += chunk) {
+    chunk = compact ? compact_chunk(k++, every) : every;
     TrackArgs ta = base;
     if (compact) {
       int rc = compact_live(ctx);

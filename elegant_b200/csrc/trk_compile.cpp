@@ -428,7 +428,11 @@ int edge_mode(int on, int effects, int edge_order, const char *name) {
     return edge_order <= 1 ? EDGE_LIN1 : EDGE_LIN2;
   if (effects == 3)
     return EDGE_SYMP;
-  trk_set_error(TRK_ERR_UNSUPPORTED, "CSBEND %s: EDGE_EFFECTS=%d is not on this path (0, 1, 3 are)", name, effects);
+  if (effects == 2)
+    return edge_order <= 1 ? EDGE_HWANG1 : EDGE_HWANG2;
+  if (effects == 4)
+    return EDGE_HWANGL;
+  trk_set_error(TRK_ERR_UNSUPPORTED, "CSBEND %s: EDGE_EFFECTS=%d is not on this path (0 to 4 are)", name, effects);
   return -1;
 }
 
@@ -542,6 +546,12 @@ int compile_bend(const trk_lattice *l, int idx, double Po, trk_op *op, std::vect
   int m2 = edge_mode(ed2, (int)TRK_P(e, CSBEND_EDGE2_EFFECTS), eo, e->name);
   if (m1 < 0 || m2 < 0)
     return TRK_ERR_UNSUPPORTED;
+  if (eo > 1 && (TRK_P(e, CSBEND_EDGE1_EFFECTS) == 2 || TRK_P(e, CSBEND_EDGE2_EFFECTS) == 2) &&
+      TRK_P(e, CSBEND_HGAP) == 0)
+    return trk_set_error(TRK_ERR_PHYSICS, /* src/csbend.c:711-712 */
+                         "CSBEND %s has EDGE_ORDER>1 and EDGE[12]_EFFECTS==2, but HGAP=0. This gives undefined "
+                         "results.",
+                         e->name);
   op->i[5] = m1;
   op->i[6] = m2;
   double *d = op->d;
@@ -636,6 +646,16 @@ int compile_bend(const trk_lattice *l, int idx, double Po, trk_op *op, std::vect
   d[BD_LIM2] = lim2;
   d[BD_HE2] = he2;
   d[BD_SE2] = 1. / std::cos(e2);
+  /* Hwang fringes: the values dipoleFringeKHwang / ...RLindberg form per call
+   * (src/csbend.c:4360-4363, :4443-4446); FINT1/FINT2 where >= 0, else FINT
+   * (src/csbend.c:1150, :1329) */
+  d[BD_FS1] = std::sin(e1);
+  d[BD_FC1] = std::cos(e1);
+  d[BD_FS2] = std::sin(e2);
+  d[BD_FC2] = std::cos(e2);
+  d[BD_FF1] = TRK_P(e, CSBEND_FINT1) >= 0 ? TRK_P(e, CSBEND_FINT1) : TRK_P(e, CSBEND_FINT);
+  d[BD_FF2] = TRK_P(e, CSBEND_FINT2) >= 0 ? TRK_P(e, CSBEND_FINT2) : TRK_P(e, CSBEND_FINT);
+  d[BD_GAP] = 2 * TRK_P(e, CSBEND_HGAP);
   d[BD_N] = n;
   d[BD_RHOINV] = 1.0 / rho0;
   d[BD_INVRHOA] = 1.0 / rho_actual;

@@ -37,6 +37,9 @@
 #define TRKCR_FMA(a, b, c) __fma_rn((a), (b), (c))
 #define TRKCR_ASIN(x) asin(x)
 #define TRKCR_COS(x) cos(x)
+#define TRKCR_EXP(x) exp(x)
+#define TRKCR_LDEXP(x, k) ldexp((x), (k))
+#define TRKCR_HIWORD(x) ((unsigned)__double2hiint(x))
 #else
 #include <math.h>
 /* host build: compile with -ffp-contract=off so each operation rounds once */
@@ -50,6 +53,16 @@
 #define TRKCR_FMA(a, b, c) fma((a), (b), (c))
 #define TRKCR_ASIN(x) asin(x)
 #define TRKCR_COS(x) cos(x)
+#define TRKCR_EXP(x) exp(x)
+#define TRKCR_LDEXP(x, k) ldexp((x), (k))
+#include <stdint.h>
+#include <string.h>
+static inline unsigned trkcr_hiword(double x) {
+  uint64_t b;
+  memcpy(&b, &x, sizeof b);
+  return (unsigned)(b >> 32);
+}
+#define TRKCR_HIWORD(x) trkcr_hiword(x)
 #endif
 
 typedef struct {
@@ -528,6 +541,104 @@ TRKCR_FN double trkcr_asin(double y) {
   if (ay <= TRKCR_TINY && trkcr_asin_tiny(y, TRKCR_MUL(y, y), &a))
     return a;
   return trkcr_asin_mid(y);
+}
+
+/*
+ * exp, correctly rounded for |x| <= 700 (the CSBEND Hwang-Lindberg fringe
+ * takes exp of a small product per particle, src/csbend.c:4466, :4506).
+ * Tiny |x| <= 2^-7: exp x = (1 + x) + x^2 P(x), P = 1/2 + x/6 + ... +
+ * x^6/8! (next term x^9/9!, below 2^-66 of x^2/2); 1 + x is
+ * split exactly (sh + sl), the rest L = sl + x^2 P in plain double with
+ * error below 2^-51.4 |x^2 P| + 2^-53 |L|, and the rounding test widens L
+ * by 2^-49 |x^2 P| + 2^-52 |L|.  Otherwise: x = k ln2 + r with ln2 in three
+ * parts, exp(r/256) by its Taylor series in double-double, squared eight
+ * times, times 2^k (~2^-92 relative); beyond |x| > 700 the library's exp.
+ */
+TRKCR_CONST double trkcr_exp_c[13][2] = {
+  {0x1.0000000000000p+0, 0x0.0p+0},           {0x1.0000000000000p+0, 0x0.0p+0},
+  {0x1.0000000000000p-1, 0x0.0p+0},           {0x1.5555555555555p-3, 0x1.5555555555555p-57},
+  {0x1.5555555555555p-5, 0x1.5555555555555p-59}, {0x1.1111111111111p-7, 0x1.1111111111111p-63},
+  {0x1.6c16c16c16c17p-10, -0x1.f49f49f49f49fp-65}, {0x1.a01a01a01a01ap-13, 0x1.a01a01a01a01ap-73},
+  {0x1.a01a01a01a01ap-16, 0x1.a01a01a01a01ap-76}, {0x1.71de3a556c734p-19, -0x1.c154f8ddc6c00p-73},
+  {0x1.27e4fb7789f5cp-22, 0x1.cbbc05b4fa99ap-76}, {0x1.ae64567f544e4p-26, -0x1.c062e06d1f209p-80},
+  {0x1.1eed8eff8d898p-29, -0x1.2aec959e14c06p-83},
+};
+#define TRKCR_LN2_1 0x1.62e42fefa39efp-1
+#define TRKCR_LN2_2 0x1.abc9e3b39803fp-56
+#define TRKCR_LN2_3 0x1.7b57a079a1934p-111
+#define TRKCR_INVLN2 0x1.71547652b82fep+0
+
+/* exp x as a double-double, |x| <= 700 */
+TRKCR_FN trkcr_dd trkcr_exp_dd(double x) {
+  const double k = rint(TRKCR_MUL(x, TRKCR_INVLN2));
+  trkcr_dd a = trkcr_two_prod(k, TRKCR_LN2_1);
+  trkcr_dd r = trkcr_two_sum(x, -a.hi);
+  r = trkcr_add(r, trkcr_make(-a.lo, 0.0));
+  trkcr_dd b = trkcr_two_prod(k, TRKCR_LN2_2);
+  r = trkcr_add(r, trkcr_make(-b.hi, -b.lo));
+  r = trkcr_add(r, trkcr_make(-TRKCR_MUL(k, TRKCR_LN2_3), 0.0));
+  r.hi = TRKCR_MUL(r.hi, 0x1p-8);
+  r.lo = TRKCR_MUL(r.lo, 0x1p-8);
+  trkcr_dd p = trkcr_make(trkcr_exp_c[12][0], trkcr_exp_c[12][1]);
+  for (int i = 11; i >= 0; i--)
+    p = trkcr_add(trkcr_mul(p, r), trkcr_make(trkcr_exp_c[i][0], trkcr_exp_c[i][1]));
+  for (int i = 0; i < 8; i++)
+    p = trkcr_mul(p, p);
+  return trkcr_make(TRKCR_LDEXP(p.hi, (int)k), TRKCR_LDEXP(p.lo, (int)k));
+}
+
+/* the x^2 P(x) of the tiny path */
+TRKCR_FN double trkcr_exp_tiny_t(double x) {
+  double P = TRKCR_FMA(x, 0x1.a01a01a01a01ap-16, 0x1.a01a01a01a01ap-13);
+  P = TRKCR_FMA(x, P, 0x1.6c16c16c16c17p-10);
+  P = TRKCR_FMA(x, P, 0x1.1111111111111p-7);
+  P = TRKCR_FMA(x, P, 0x1.5555555555555p-5);
+  P = TRKCR_FMA(x, P, 0x1.5555555555555p-3);
+  P = TRKCR_FMA(x, P, 0.5);
+  return TRKCR_MUL(TRKCR_MUL(x, x), P);
+}
+
+TRKCR_SLOW double trkcr_exp_slow(double x) {
+  if (!(fabs(x) <= 700.0))
+    return TRKCR_EXP(x);
+  const trkcr_dd v = trkcr_exp_dd(x);
+  return TRKCR_ADD(v.hi, v.lo);
+}
+
+TRKCR_FN double trkcr_exp(double x) {
+  if (fabs(x) <= TRKCR_TINY) {
+    if (x == 0.0)
+      return 1.0;
+    const double sh = TRKCR_ADD(1.0, x);
+    const double sl = TRKCR_ADD(TRKCR_SUB(1.0, sh), x);
+    const double t = trkcr_exp_tiny_t(x);
+    const double L = TRKCR_ADD(sl, t);
+    const double e = TRKCR_FMA(fabs(t), 0x1p-49, TRKCR_MUL(fabs(L), 0x1p-52));
+    const double u = TRKCR_ADD(sh, TRKCR_ADD(L, e)), v = TRKCR_ADD(sh, TRKCR_SUB(L, e));
+    if (u == v)
+      return u;
+  }
+  return trkcr_exp_slow(x);
+}
+
+/*
+ * RN(a/b) from y = RN(1/b), the correctly rounded reciprocal of b (formed
+ * once for a divisor used many times): q0 = RN(a y) is within 1.5 ulp of
+ * a/b; one FMA correction q1 = RN(q0 + (a - b q0) y) leaves it within an
+ * ulp (its error is ~(2u)^2 relative plus the final rounding); a second,
+ * q2 = RN(q1 + (a - b q1) y), with the residual exact because q1 is
+ * faithful, is RN(a/b) by Markstein's theorem (P. Markstein, IBM J. Res.
+ * Dev. 34 (1990) 111; the basis of FMA division on IA-64).  The theorem
+ * assumes no underflow or overflow in the intermediates: quotients outside
+ * [2^-958, 2^960) in magnitude (and zeros, infinities, NaNs) take the IEEE
+ * division, so signed zeros and special values are the IEEE ones.
+ */
+TRKCR_FN double trkcr_div_rcp(double a, double b, double y) {
+  const double q0 = TRKCR_MUL(a, y);
+  const double q1 = TRKCR_FMA(TRKCR_FMA(-b, q0, a), y, q0);
+  const double q2 = TRKCR_FMA(TRKCR_FMA(-b, q1, a), y, q1);
+  const unsigned e = (TRKCR_HIWORD(q0) >> 20) & 0x7ffu;
+  return (e - 65u < 1918u) ? q2 : TRKCR_DIV(a, b);
 }
 
 #endif

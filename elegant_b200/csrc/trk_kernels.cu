@@ -41,6 +41,7 @@
 #define M_ASIN(x) asin(x)
 #define M_TAN(x) tan(x)
 #define M_SINCOS(x, s, c) sincos((x), (s), (c))
+#define M_EXP(x) exp(x)
 #else
 #define TRK_NS trk_exact
 #define M_SIN(x) trkcr_sin(x)
@@ -48,6 +49,7 @@
 #define M_ASIN(x) trkcr_asin(x)
 #define M_TAN(x) trkcr_tan(x)
 #define M_SINCOS(x, s, c) trkcr_sincos((x), (s), (c))
+#define M_EXP(x) trkcr_exp(x)
 #endif
 
 namespace TRK_NS {
@@ -524,23 +526,6 @@ done:
 
 /* ---------------------------------------------------------------- CSBEND */
 #if !TRK_FAST
-/* RN(a/b) given y ~ 1/b with relative error below 2^-50 (a reciprocal
- * rounded once, on the host or by __drcp_rn): q0 = RN(a y), the residual
- * r = RN(a - b q0) by one FMA and t = RN(r y) ~ (a - b q0)/b to within
- * 2^-49.7 relative; a/b = q0 + (a - b q0)/b, so when q0 + t +- 2^-48 |t|
- * round to the same double that double is RN(a/b).  Otherwise (one call in
- * ~2^45, or a zero, non-finite or tiny quotient) the full IEEE division. */
-__device__ __forceinline__ double div_rn_by(double a, double b, double y) {
-  const double q0 = __dmul_rn(a, y);
-  const double t = __dmul_rn(__fma_rn(-b, q0, a), y);
-  const double at = fabs(t);
-  const double hi = __dadd_rn(q0, __fma_rn(at, 0x1p-48, t));
-  const double lo = __dadd_rn(q0, __fma_rn(-at, 0x1p-48, t));
-  if (hi == lo && fabs(hi) > 0x1p-900)
-    return hi;
-  return __ddiv_rn(a, b);
-}
-
 /* Body of a pure-dipole CSBEND in the parity build: integrate_csbend_ordn
  * (src/csbend.c:1561-1660) with Fx = 0, Fy = 1 and no radiation, every
  * operation rounded as the reference rounds it, with these shortcuts that
@@ -549,8 +534,10 @@ __device__ __forceinline__ double div_rn_by(double a, double b, double y) {
  *    - QY^2) while QY^2 rounds to the same double (QY moves only by the
  *    (1+delta) divide/multiply round trip, by an ulp at most): f and its
  *    reciprocal are re-formed only when QY^2 changes;
- *  - divisions by f, rho0, rho_actual and 1 + delta use a reciprocal formed
- *    once (div_rn_by: the IEEE quotient, certified);
+ *  - divisions by f, rho0, rho_actual and 1 + delta use their correctly
+ *    rounded reciprocals, formed once (trkcr_div_rcp: Markstein's two FMA
+ *    corrections give the IEEE quotient for five FP64 operations, about a
+ *    third of an IEEE division's cost on B200);
  *  - the kick's Fx term, ((ds (1 + X/rho0)) 0)/rho_actual, is a signed zero
  *    (or NaN), formed by multiplying by 1/rho_actual instead of dividing;
  *  - dz_lost is summed only for a lost particle, from the substeps done.
@@ -577,7 +564,7 @@ __device__ __forceinline__ bool bend_dipole_exact(const double *__restrict__ d, 
     for (int j = 0; j < nSub; j++) {
       if (f2 <= 0)
         return false;
-      const double sin_phi = div_rn_by(QX, f, yf);
+      const double sin_phi = trkcr_div_rcp(QX, f, yf);
       if (fabs(sin_phi) > 1)
         return false;
       const double phi = trkcr_asin(sin_phi);
@@ -588,7 +575,7 @@ __device__ __forceinline__ bool bend_dipole_exact(const double *__restrict__ d, 
       const double tang = __ddiv_rn(sine, cosi);
       const double cos_phi = trkcr_cos(phi);
       QX = __dmul_rn(f, sine);
-      const double a3 = div_rn_by(__dmul_rn(__dadd_rn(rho0, X), cos_phi), f, yf);
+      const double a3 = trkcr_div_rcp(__dmul_rn(__dadd_rn(rho0, X), cos_phi), f, yf);
       const double factor = __dmul_rn(a3, __dsub_rn(tang, __ddiv_rn(sin_phi, cos_phi)));
       Y = __dadd_rn(Y, __dmul_rn(QY, factor));
       dist = __dadd_rn(dist, __dmul_rn(factor, opd));
@@ -599,13 +586,13 @@ __device__ __forceinline__ bool bend_dipole_exact(const double *__restrict__ d, 
         break;
       /* kick: QX += -ds (1 + X/rho0) Fy / rho_a, QY += ds (1 + X/rho0) Fx / rho_a */
       const double ds = __ldg(&d[BD_DS + j]);
-      const double w = __dmul_rn(ds, __dadd_rn(1.0, div_rn_by(X, rho0, yrho0)));
-      QX = __dadd_rn(QX, div_rn_by(-w, rho_a, yrho_a));
+      const double w = __dmul_rn(ds, __dadd_rn(1.0, trkcr_div_rcp(X, rho0, yrho0)));
+      QX = __dadd_rn(QX, trkcr_div_rcp(-w, rho_a, yrho_a));
       QY = __dadd_rn(QY, __dmul_rn(__dmul_rn(w, 0.0), yrho_a));
       if (roundtrip) {
         /* QX /= (1 + delta); QY /= ...; QX *= (1 + delta); QY *= ... */
-        QX = __dmul_rn(div_rn_by(QX, opd, yopd), opd);
-        QY = __dmul_rn(div_rn_by(QY, opd, yopd), opd);
+        QX = __dmul_rn(trkcr_div_rcp(QX, opd, yopd), opd);
+        QY = __dmul_rn(trkcr_div_rcp(QY, opd, yopd), opd);
       }
       const double q2 = __dmul_rn(QY, QY);
       if (q2 != qy2) {
@@ -918,6 +905,135 @@ __device__ void edge_order2(double &x, double &xp, double &y, double &yp, double
 }
 
 /* edge kick of track_through_csbend (src/csbend.c:1126-1204, 1306-1382) */
+/* K. Hwang's dipole fringe (dipoleFringeKHwang, src/csbend.c:4336-4408) in
+ * dipole canonical coordinates, each expression in the reference's operation
+ * order; sec, tan, sin, cos of the edge angle come from the element record */
+#define FR_P2(v) ((v) * (v))
+#define FR_P3(v) ((v) * (v) * (v))
+__device__ __noinline__ void fringe_hwang(double &x, double &px, double &y, double &py, double dp, double rho,
+                                          double inFringe, bool second_order, double sec_edge, double tan_edge,
+                                          double sin_edge, double cos_edge, double gap, double fint, double Rhe) {
+  const double k0 = FR_P2(TRK_PI) / 6., k2 = fint, k3 = 1.0 * 1. / 6., k4 = -1.0 * FR_P2(TRK_PI) / 3., k5 = 0.0,
+               k6 = -1.0;
+  const double x0 = x, px0 = px, y0 = y, py0 = py, dp0 = dp;
+  double dx = 0, dpx = 0, dy = 0, dpy = 0;
+  if (second_order) {
+    dx = inFringe * FR_P2(sec_edge) * FR_P2(gap) * k0 / rho / (1 + dp0) +
+         inFringe * FR_P2(x0) * FR_P2(tan_edge) / 2 / rho / (1 + dp0) -
+         inFringe * FR_P2(y0) * FR_P2(sec_edge) / 2 / rho / (1 + dp0);
+    dy = -inFringe * x0 * y0 * FR_P2(tan_edge) / rho / (1 + dp0);
+    if (inFringe == -1.) {
+      dpx = -1. * FR_P3(sec_edge) * sin_edge * FR_P2(gap) * k0 / rho / rho / (1 + dp0) + tan_edge * x0 / rho +
+            FR_P2(y0) / 2 * (2 * FR_P3(tan_edge)) / FR_P2(rho) / (1 + dp0) +
+            FR_P2(y0) / 2 * (tan_edge) / FR_P2(rho) / (1 + dp0) -
+            inFringe * (x0 * px0 - y0 * py0) * FR_P2(tan_edge) / rho / (1 + dp0) +
+            k4 * FR_P2(sin_edge) * FR_P2(gap) / 2 / FR_P3(cos_edge) / rho * Rhe -
+            k5 * x0 * sin_edge * gap / FR_P3(cos_edge) / rho * Rhe +
+            k6 * (y0 * y0 - x0 * x0) / 2 / FR_P3(cos_edge) / rho * Rhe;
+      dpy = -1. * tan_edge * y0 / rho + k2 * y0 * (1 + FR_P2(sin_edge)) * gap / (1 + dp0) / FR_P2(rho) / FR_P3(cos_edge) +
+            inFringe * (x0 * py0 + y0 * px0) * FR_P2(tan_edge) / rho / (1 + dp0) +
+            inFringe * y0 * px0 / rho / (1 + dp0) +
+            k3 * FR_P3(y0) * (2. / 3. / cos_edge - 4. / 3. / FR_P3(cos_edge)) / (1 + dp0) / rho / rho / gap +
+            k6 * x0 * y0 / FR_P3(cos_edge) / rho * Rhe;
+    } else {
+      dpx = tan_edge * x0 / rho - FR_P2(y0) / 2 * (1 * FR_P3(tan_edge)) / FR_P2(rho) / (1 + dp0) -
+            FR_P2(x0) / 2 * (1 * FR_P3(tan_edge)) / FR_P2(rho) / (1 + dp0) -
+            inFringe * (x0 * px0 - y0 * py0) * FR_P2(tan_edge) / rho / (1 + dp0) +
+            k4 * FR_P2(sin_edge) * FR_P2(gap) / 2 / FR_P3(cos_edge) / rho * Rhe -
+            k5 * x0 * sin_edge * gap / FR_P3(cos_edge) / rho * Rhe +
+            k6 * (y0 * y0 - x0 * x0) / 2 / FR_P3(cos_edge) / rho * Rhe;
+      dpy = -1. * tan_edge * y0 / rho + k2 * y0 * (1 + FR_P2(sin_edge)) * gap / (1 + dp0) / FR_P2(rho) / FR_P3(cos_edge) +
+            inFringe * (x0 * py0 + y0 * px0) * FR_P2(tan_edge) / rho / (1 + dp0) +
+            inFringe * y0 * px0 / rho / (1 + dp0) + x0 * y0 * FR_P2(sec_edge) * tan_edge / FR_P2(rho) / (1 + dp0) +
+            k3 * FR_P3(y0) * (2. / 3. / cos_edge - 4. / 3. / FR_P3(cos_edge)) / (1 + dp0) / rho / rho / gap -
+            k5 * y0 * sin_edge * gap / FR_P3(cos_edge) / rho * Rhe + k6 * x0 * y0 / FR_P3(cos_edge) / rho * Rhe;
+    }
+  } else {
+    dx = inFringe * FR_P2(sec_edge) * FR_P2(gap) * k0 / rho / (1 + dp0);
+    if (inFringe == -1.) {
+      dpx = -1. * FR_P3(sec_edge) * sin_edge * FR_P2(gap) * k0 / rho / rho / (1 + dp0) + tan_edge * x0 / rho +
+            k4 * FR_P2(sin_edge) * FR_P2(gap) / 2 / FR_P3(cos_edge) / rho * Rhe -
+            k5 * x0 * sin_edge * gap / FR_P3(cos_edge) / rho * Rhe;
+      dpy = -1. * tan_edge * y0 / rho + k2 * y0 * (1 + FR_P2(sin_edge)) * gap / (1 + dp0) / FR_P2(rho) / FR_P3(cos_edge);
+    } else {
+      dpx = tan_edge * x0 / rho + k4 * FR_P2(sin_edge) * FR_P2(gap) / 2 / FR_P3(cos_edge) / rho * Rhe -
+            k5 * x0 * sin_edge * gap / FR_P3(cos_edge) / rho * Rhe;
+      dpy = -1. * tan_edge * y0 / rho + k2 * y0 * (1 + FR_P2(sin_edge)) * gap / (1 + dp0) / FR_P2(rho) / FR_P3(cos_edge) -
+            k5 * y0 * sin_edge * gap / FR_P3(cos_edge) / rho * Rhe;
+    }
+  }
+  x = x0 + dx;
+  px = px0 + dpx;
+  y = y0 + dy;
+  py = py0 + dpy;
+}
+
+/* the same symplectified by R. Lindberg (dipoleFringeKHwangRLindberg,
+ * src/csbend.c:4413-4520): five maps in sequence */
+__device__ __noinline__ void fringe_hwang_lindberg(double &x, double &px, double &y, double &py, double dp, double rho,
+                                                   double inFringe, double sec_edge, double tan_edge, double sin_edge,
+                                                   double cos_edge, double gap, double fint, double Rhe) {
+  const double k0 = FR_P2(TRK_PI) / 6., k2 = fint, k3 = 1.0 * 1. / 6., k4 = -1.0 * FR_P2(TRK_PI) / 3., k5 = 0.0,
+               k6 = -1.0;
+  const double rho2 = FR_P2(rho);
+  const double x0 = x, px0 = px, y0 = y, py0 = py, dp0 = dp;
+  const double sec2_edge = FR_P2(sec_edge), cos3_edge = FR_P3(cos_edge), tan2_edge = FR_P2(tan_edge),
+               tan3_edge = FR_P3(tan_edge);
+  double x1, px1, y1, py1, x2, px2, x3, py3, px4, y4, py4, t1, t2;
+  if (inFringe == -1) {
+    x1 = x0;
+    px1 = px0 + tan_edge / rho * x0 + tan_edge / (2 * rho2 * (1 + dp0)) * FR_P2(y0) -
+          tan3_edge / (rho2 * (1 + dp0)) * FR_P2(x0) - gap * k5 * sin_edge * Rhe / (rho * cos3_edge) * x0 +
+          k6 * sec2_edge * Rhe / (2 * rho) * (FR_P2(y0) - FR_P2(x0));
+    y1 = y0;
+    py1 = py0 - tan_edge / rho * y0 + tan_edge / (rho2 * (1 + dp0)) * x0 * y0 +
+          gap * k2 * (1 + FR_P2(sin_edge)) / (rho2 * (1 + dp0) * cos3_edge) * y0 +
+          2 * k3 * (FR_P2(cos_edge) - 2) / (3 * gap * rho2 * cos3_edge) * FR_P3(y0) +
+          gap * k5 * sin_edge * Rhe / (rho * cos3_edge) * y0 + k6 * FR_P3(sec_edge) * Rhe / rho * x0 * y0;
+    t1 = (1 + tan2_edge / (2 * rho * (1 + dp0)) * x1);
+    x2 = x1 / t1;
+    px2 = px1 * FR_P2(t1);
+    t1 = sec2_edge / (rho * (1 + dp0));
+    x3 = x2 + t1 / 2 * FR_P2(y1);
+    py3 = py1 - t1 * y1 * px2;
+    t1 = tan2_edge / (rho * (1 + dp0));
+    t2 = M_EXP(t1 * x3);
+    px4 = px2 - t1 * y1 * py3;
+    y4 = y1 * t2;
+    py4 = py3 / t2;
+    t1 = FR_P2(gap) * k0 * sec2_edge / (rho * (1 + dp0));
+    x = x3 - t1;
+    px = px4 - t1 * tan_edge / rho + FR_P2(gap) * k4 * FR_P2(sin_edge) * Rhe / (2 * rho * cos3_edge);
+  } else {
+    x1 = x0;
+    px1 = px0 + tan_edge / rho * x0 + tan3_edge / (2 * rho2 * (1 + dp0)) * FR_P2(y0) +
+          tan3_edge / (2 * rho2 * (1 + dp0)) * FR_P2(x0) - gap * k5 * sin_edge * Rhe / (rho * cos3_edge) * x0 +
+          k6 * sec2_edge * Rhe / (2 * rho) * (FR_P2(y0) - FR_P2(x0));
+    y1 = y0;
+    py1 = py0 - tan_edge / rho * y0 + tan3_edge / (rho2 * (1 + dp0)) * x0 * y0 +
+          gap * k2 * (1 + FR_P2(sin_edge)) / (rho2 * (1 + dp0) * cos3_edge) * y0 +
+          2 * k3 * (FR_P2(cos_edge) - 2) / (3 * gap * rho2 * cos3_edge) * FR_P3(y0) +
+          gap * k5 * sin_edge * Rhe / (rho * cos3_edge) * y0 + k6 * FR_P3(sec_edge) * Rhe / rho * x0 * y0;
+    t1 = (1 - tan2_edge / (2 * rho * (1 + dp0)) * x1);
+    x2 = x1 / t1;
+    px2 = px1 * FR_P2(t1);
+    t1 = sec2_edge / (rho * (1 + dp0));
+    x3 = x2 - t1 / 2 * FR_P2(y1);
+    py3 = py1 + t1 * y1 * px2;
+    t1 = -tan2_edge / (rho * (1 + dp0));
+    t2 = M_EXP(t1 * x3);
+    px4 = px2 - t1 * y1 * py3;
+    y4 = y1 * t2;
+    py4 = py3 / t2;
+    x = x3 + FR_P2(gap) * k0 * sec2_edge / (rho * (1 + dp0));
+    px = px4 + FR_P2(gap) * k4 * FR_P2(sin_edge) * Rhe / (2 * rho * cos3_edge);
+  }
+  y = y4;
+  py = py4;
+}
+#undef FR_P2
+#undef FR_P3
+
 __device__ __forceinline__ void bend_edge(int mode, const double *__restrict__ d, int base, int which, double rho_a,
                                           double nidx, double &x, double &xp, double &y, double &yp, double dp) {
   const double e = __ldg(&d[base + 0]), te = __ldg(&d[base + 1]), psi = __ldg(&d[base + 2]);
@@ -949,6 +1065,21 @@ __device__ __forceinline__ void bend_edge(int mode, const double *__restrict__ d
     f = 1 / sqrt(sqr(1 + dp) - sqr(Q1) - sqr(Q3));
     xp = Q1 * f;
     yp = Q3 * f;
+  } else if (mode == EDGE_HWANG1 || mode == EDGE_HWANG2 || mode == EDGE_HWANGL) {
+    /* in dipole canonical coordinates (src/csbend.c:1139-1182, :1319-1359;
+     * convert{To,From}DipoleCanonicalCoordinates, :1436-1457) */
+    double f = (1 + dp) / sqrt(1 + sqr(xp) + sqr(yp));
+    double px = xp * f, py = yp * f;
+    const int k = which < 0 ? 0 : 1;
+    const double sn = __ldg(&d[BD_FS1 + 3 * k]), cs = __ldg(&d[BD_FC1 + 3 * k]), fint = __ldg(&d[BD_FF1 + 3 * k]);
+    const double gap = __ldg(&d[BD_GAP]);
+    if (mode == EDGE_HWANGL)
+      fringe_hwang_lindberg(x, px, y, py, dp, rho_a, (double)which, secb, te, sn, cs, gap, fint, he);
+    else
+      fringe_hwang(x, px, y, py, dp, rho_a, (double)which, mode == EDGE_HWANG2, secb, te, sn, cs, gap, fint, he);
+    f = 1 / sqrt(sqr(1 + dp) - sqr(px) - sqr(py));
+    xp = px * f;
+    yp = py * f;
   }
 }
 

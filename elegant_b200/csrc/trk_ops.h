@@ -72,7 +72,7 @@ typedef struct {
   int32_t no_aperture; /* NO_APERTURE element class (MARK, CHARGE) */
   int32_t i[8];
   double z_start, z_end;
-  double d[120];
+  double d[128];
 } trk_op;
 
 /* after-element / in-element aperture from the sticky MAXAMP state */
@@ -153,12 +153,25 @@ typedef struct {
 #define BD_C2 105     /* 8 values ds/(rho_actual rho0) (fast build kick) */
 #define BD_RAD 113    /* rad_coef (src/csbend.c:956-959) */
 #define BD_ISR 114    /* isrConstant (src/csbend.c:961) */
+/* Hwang fringes (EDGE_EFFECTS 2 and 4): sin and cos of each edge angle, its
+ * FINT, and the full gap 2 HGAP (sec and tan are BD_SE1/2, BD_TE1/2, the
+ * pole-face curvature BD_HE1/2) */
+#define BD_FS1 115
+#define BD_FC1 116
+#define BD_FF1 117
+#define BD_FS2 118
+#define BD_FC2 119
+#define BD_FF2 120
+#define BD_GAP 121
 /* i: 0 nSlices, 1 nSub, 2 field mode (0 dipole, 1 normal, 2 skew), 3 expansionOrder1,
  *    4 field pool offset, 5 edge1 mode, 6 edge2 mode, 7 flags */
 #define EDGE_NONE 0
 #define EDGE_LIN1 1 /* EDGE_EFFECTS=1, EDGE_ORDER<=1 */
 #define EDGE_LIN2 2 /* EDGE_EFFECTS=1, EDGE_ORDER>=2 (apply_edge_effects) */
 #define EDGE_SYMP 3 /* EDGE_EFFECTS=3 */
+#define EDGE_HWANG1 4 /* EDGE_EFFECTS=2, EDGE_ORDER<=1 (dipoleFringeKHwang, linear terms) */
+#define EDGE_HWANG2 5 /* EDGE_EFFECTS=2, EDGE_ORDER>=2 */
+#define EDGE_HWANGL 6 /* EDGE_EFFECTS=4 (dipoleFringeKHwangRLindberg) */
 
 /* RF */
 #define RD_OMEGA 0

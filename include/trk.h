@@ -135,6 +135,13 @@ typedef struct {
 
 void trk_run_defaults(trk_run *run);
 
+/* Test hook, no counterpart in the reference: the next `after` growing
+ * device allocations of the library succeed and the one after them is
+ * refused as if cudaMalloc had failed (TRK_ERR_NOMEM, nothing allocated);
+ * the hook then disarms.  after < 0 disarms it.  Process-wide.  Lets tests
+ * check that a failed call leaves its context usable. */
+int trk_test_fail_allocation(int after);
+
 typedef struct {
   long n_total;          /* particles loaded */
   long n_left;           /* survivors after the run */

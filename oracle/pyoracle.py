@@ -53,6 +53,8 @@ def load():
     lib.orc_set_cr_math.argtypes = [I]
     lib.orc_cr_selftest.argtypes = [I, D, D, I, L, ctypes.c_ulonglong, ctypes.POINTER(L), DP]
     lib.orc_cr_selftest.restype = L
+    lib.orc_div_rcp_selftest.argtypes = [L, ctypes.c_ulonglong]
+    lib.orc_div_rcp_selftest.restype = L
     for f in ('orc_cr_sin', 'orc_cr_cos', 'orc_cr_asin', 'orc_cr_tan'):
         getattr(lib, f).argtypes = [D]
         getattr(lib, f).restype = D

@@ -1,6 +1,6 @@
 /*
  * TEST INFRASTRUCTURE (oracle/ref): force-included into elegant's sources so
- * that their sin/cos/asin/tan calls go through oracle/ref/shim_impl.c, which
+ * that their sin/cos/asin/tan/exp calls go through oracle/ref/shim_impl.c, which
  * can switch them to correctly rounded versions.  math.h is included first
  * so its own declarations keep the real names.
  */
@@ -11,8 +11,10 @@ double ref_sin(double x);
 double ref_cos(double x);
 double ref_asin(double x);
 double ref_tan(double x);
+double ref_exp(double x);
 #define sin(x) ref_sin(x)
 #define cos(x) ref_cos(x)
 #define asin(x) ref_asin(x)
 #define tan(x) ref_tan(x)
+#define exp(x) ref_exp(x)
 #endif

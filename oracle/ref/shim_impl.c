@@ -33,6 +33,7 @@ double ref_sin(double x) { return ref_cr_math ? trkcr_sin(x) : sin(x); }
 double ref_cos(double x) { return ref_cr_math ? trkcr_cos(x) : cos(x); }
 double ref_asin(double x) { return ref_cr_math ? trkcr_asin(x) : asin(x); }
 double ref_tan(double x) { return ref_cr_math ? trkcr_tan(x) : tan(x); }
+double ref_exp(double x) { return ref_cr_math ? trkcr_exp(x) : exp(x); }
 
 /* ----------------------------------------------------- SDDS mdbmth helpers */
 double ipow(double x, long p) {

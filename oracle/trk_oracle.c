@@ -15,6 +15,7 @@
 #include <float.h>
 #include <math.h>
 #include <stdlib.h>
+#include <stdint.h>
 #include <string.h>
 
 #include "trk_lattice.h"
@@ -532,6 +533,7 @@ typedef struct {
   orc_bend bd;
   double angle, e1, e2, tilt, etilt, rho0, h, n, fse, rho_actual;
   double psi1, psi2, e1_kick_limit, e2_kick_limit, he1, he2;
+  double hgap, fint1, fint2; /* fringe: HGAP and FINT1/FINT2 (FINT where negative) */
   double cos_ttilt, sin_ttilt, dcoord_etilt[6];
   double dxi, dyi, dzi, dxf, dyf, dzf;
   int edge1, edge2, edge_order, edge1_effects, edge2_effects;
@@ -671,6 +673,9 @@ static int csbend_setup(const trk_lattice *l, int idx, double Po, orc_csbend_set
   double hgap = TRK_P(e, CSBEND_HGAP);
   double fint1 = TRK_P(e, CSBEND_FINT1) >= 0 ? TRK_P(e, CSBEND_FINT1) : TRK_P(e, CSBEND_FINT);
   double fint2 = TRK_P(e, CSBEND_FINT2) >= 0 ? TRK_P(e, CSBEND_FINT2) : TRK_P(e, CSBEND_FINT);
+  S->hgap = hgap;
+  S->fint1 = fint1;
+  S->fint2 = fint2;
   double Kg1 = 2 * hgap * fint1 * SIGN(rho0);
   S->psi1 = Kg1 / fabs(S->rho_actual) / cos(S->e1) * (1 + orc_sqr(sin(S->e1)));
   double Kg2 = 2 * hgap * fint2 * SIGN(rho0);
@@ -733,7 +738,10 @@ static int csbend_setup(const trk_lattice *l, int idx, double Po, orc_csbend_set
   for (int k = 0; k < 2; k++) {
     int eff = k ? S->edge2_effects : S->edge1_effects;
     int on = k ? S->edge2 : S->edge1;
-    if (on && eff != 0 && eff != 1 && eff != 3)
+    if (on && eff != 0 && eff != 1 && eff != 2 && eff != 3 && eff != 4)
+      return 1;
+    /* EDGE_ORDER > 1 with Hwang's fringe needs HGAP (src/csbend.c:711-712) */
+    if (eff == 2 && S->edge_order > 1 && S->hgap == 0)
       return 1;
   }
   return 0;
@@ -792,6 +800,159 @@ static void simple_dipole_edge_kick(double *xp, double *yp, double x, double y, 
   *yp = Qi[3];
 }
 
+/* dipoleFringeKHwang (src/csbend.c:4336-4408): K. Hwang's dipole fringe in
+ * dipole canonical coordinates, inFringe = -1 entrance, +1 exit */
+static void fringe_hwang(double *Qf, const double *Qi, double rho, double inFringe, long edgeOrder, double edge,
+                         double gap, double fint, double Rhe) {
+  double dx, dpx, dy, dpy, tan_edge, sin_edge, sec_edge, cos_edge, x0, px0, y0, py0, dp0;
+  const double k0 = orc_sqr(TRK_PI) / 6., k2 = fint, k3 = 1.0 * 1. / 6., k4 = -1.0 * orc_sqr(TRK_PI) / 3., k5 = 0.0,
+               k6 = -1.0;
+  x0 = Qi[0];
+  px0 = Qi[1];
+  y0 = Qi[2];
+  py0 = Qi[3];
+  dp0 = Qi[5];
+  dx = dpx = dy = dpy = 0;
+  sec_edge = 1. / cos(edge);
+  tan_edge = tan(edge);
+  sin_edge = sin(edge);
+  cos_edge = cos(edge);
+#define P2(v) ((v) * (v))
+#define P3(v) ((v) * (v) * (v))
+  if (edgeOrder > 1) {
+    if (inFringe == -1.) {
+      dx = inFringe * P2(sec_edge) * P2(gap) * k0 / rho / (1 + dp0) + inFringe * P2(x0) * P2(tan_edge) / 2 / rho / (1 + dp0) -
+           inFringe * P2(y0) * P2(sec_edge) / 2 / rho / (1 + dp0);
+      dy = -inFringe * x0 * y0 * P2(tan_edge) / rho / (1 + dp0);
+      dpx = -1. * P3(sec_edge) * sin_edge * P2(gap) * k0 / rho / rho / (1 + dp0) + tan_edge * x0 / rho +
+            P2(y0) / 2 * (2 * P3(tan_edge)) / P2(rho) / (1 + dp0) + P2(y0) / 2 * (tan_edge) / P2(rho) / (1 + dp0) -
+            inFringe * (x0 * px0 - y0 * py0) * P2(tan_edge) / rho / (1 + dp0) +
+            k4 * P2(sin_edge) * P2(gap) / 2 / P3(cos_edge) / rho * Rhe - k5 * x0 * sin_edge * gap / P3(cos_edge) / rho * Rhe +
+            k6 * (y0 * y0 - x0 * x0) / 2 / P3(cos_edge) / rho * Rhe;
+      dpy = -1. * tan_edge * y0 / rho + k2 * y0 * (1 + P2(sin_edge)) * gap / (1 + dp0) / P2(rho) / P3(cos_edge) +
+            inFringe * (x0 * py0 + y0 * px0) * P2(tan_edge) / rho / (1 + dp0) + inFringe * y0 * px0 / rho / (1 + dp0) +
+            k3 * P3(y0) * (2. / 3. / cos_edge - 4. / 3. / P3(cos_edge)) / (1 + dp0) / rho / rho / gap +
+            k6 * x0 * y0 / P3(cos_edge) / rho * Rhe;
+    }
+    if (inFringe == 1.) {
+      dx = inFringe * P2(sec_edge) * P2(gap) * k0 / rho / (1 + dp0) + inFringe * P2(x0) * P2(tan_edge) / 2 / rho / (1 + dp0) -
+           inFringe * P2(y0) * P2(sec_edge) / 2 / rho / (1 + dp0);
+      dy = -inFringe * x0 * y0 * P2(tan_edge) / rho / (1 + dp0);
+      dpx = tan_edge * x0 / rho - P2(y0) / 2 * (1 * P3(tan_edge)) / P2(rho) / (1 + dp0) -
+            P2(x0) / 2 * (1 * P3(tan_edge)) / P2(rho) / (1 + dp0) - inFringe * (x0 * px0 - y0 * py0) * P2(tan_edge) / rho / (1 + dp0) +
+            k4 * P2(sin_edge) * P2(gap) / 2 / P3(cos_edge) / rho * Rhe - k5 * x0 * sin_edge * gap / P3(cos_edge) / rho * Rhe +
+            k6 * (y0 * y0 - x0 * x0) / 2 / P3(cos_edge) / rho * Rhe;
+      dpy = -1. * tan_edge * y0 / rho + k2 * y0 * (1 + P2(sin_edge)) * gap / (1 + dp0) / P2(rho) / P3(cos_edge) +
+            inFringe * (x0 * py0 + y0 * px0) * P2(tan_edge) / rho / (1 + dp0) + inFringe * y0 * px0 / rho / (1 + dp0) +
+            x0 * y0 * P2(sec_edge) * tan_edge / P2(rho) / (1 + dp0) +
+            k3 * P3(y0) * (2. / 3. / cos_edge - 4. / 3. / P3(cos_edge)) / (1 + dp0) / rho / rho / gap -
+            k5 * y0 * sin_edge * gap / P3(cos_edge) / rho * Rhe + k6 * x0 * y0 / P3(cos_edge) / rho * Rhe;
+    }
+  } else {
+    if (inFringe == -1.) {
+      dx = inFringe * P2(sec_edge) * P2(gap) * k0 / rho / (1 + dp0);
+      dy = 0;
+      dpx = -1. * P3(sec_edge) * sin_edge * P2(gap) * k0 / rho / rho / (1 + dp0) + tan_edge * x0 / rho +
+            k4 * P2(sin_edge) * P2(gap) / 2 / P3(cos_edge) / rho * Rhe - k5 * x0 * sin_edge * gap / P3(cos_edge) / rho * Rhe;
+      dpy = -1. * tan_edge * y0 / rho + k2 * y0 * (1 + P2(sin_edge)) * gap / (1 + dp0) / P2(rho) / P3(cos_edge);
+    }
+    if (inFringe == 1.) {
+      dx = inFringe * P2(sec_edge) * P2(gap) * k0 / rho / (1 + dp0);
+      dy = 0;
+      dpx = tan_edge * x0 / rho + k4 * P2(sin_edge) * P2(gap) / 2 / P3(cos_edge) / rho * Rhe -
+            k5 * x0 * sin_edge * gap / P3(cos_edge) / rho * Rhe;
+      dpy = -1. * tan_edge * y0 / rho + k2 * y0 * (1 + P2(sin_edge)) * gap / (1 + dp0) / P2(rho) / P3(cos_edge) -
+            k5 * y0 * sin_edge * gap / P3(cos_edge) / rho * Rhe;
+    }
+  }
+  Qf[0] = x0 + dx;
+  Qf[1] = px0 + dpx;
+  Qf[2] = y0 + dy;
+  Qf[3] = py0 + dpy;
+  Qf[5] = Qi[5];
+}
+
+/* dipoleFringeKHwangRLindberg (src/csbend.c:4413-4520): the symplectic form */
+static void fringe_hwang_lindberg(double *Qf, const double *Qi, double rho, double inFringe, double edge, double gap,
+                                  double fint, double Rhe) {
+  const double k0 = orc_sqr(TRK_PI) / 6., k2 = fint, k3 = 1.0 * 1. / 6., k4 = -1.0 * orc_sqr(TRK_PI) / 3., k5 = 0.0,
+               k6 = -1.0;
+  const double rho2 = orc_sqr(rho);
+  const double x0 = Qi[0], px0 = Qi[1], y0 = Qi[2], py0 = Qi[3], dp0 = Qi[5];
+  const double sec_edge = 1. / cos(edge), tan_edge = tan(edge), sin_edge = sin(edge), cos_edge = cos(edge);
+  const double sec2_edge = P2(sec_edge), cos3_edge = P3(cos_edge), tan2_edge = P2(tan_edge), tan3_edge = P3(tan_edge);
+  double x1, px1, y1, py1, x2, px2, y2, py2, x3, px3, y3, py3, x4, px4, y4, py4, x5, px5, y5, py5, t1, t2;
+  if (inFringe == -1) {
+    x1 = x0;
+    px1 = px0 + tan_edge / rho * x0 + tan_edge / (2 * rho2 * (1 + dp0)) * orc_sqr(y0) -
+          tan3_edge / (rho2 * (1 + dp0)) * orc_sqr(x0) - gap * k5 * sin_edge * Rhe / (rho * cos3_edge) * x0 +
+          k6 * sec2_edge * Rhe / (2 * rho) * (orc_sqr(y0) - orc_sqr(x0));
+    y1 = y0;
+    py1 = py0 - tan_edge / rho * y0 + tan_edge / (rho2 * (1 + dp0)) * x0 * y0 +
+          gap * k2 * (1 + orc_sqr(sin_edge)) / (rho2 * (1 + dp0) * cos3_edge) * y0 +
+          2 * k3 * (orc_sqr(cos_edge) - 2) / (3 * gap * rho2 * cos3_edge) * P3(y0) +
+          gap * k5 * sin_edge * Rhe / (rho * cos3_edge) * y0 + k6 * P3(sec_edge) * Rhe / rho * x0 * y0;
+    t1 = (1 + tan2_edge / (2 * rho * (1 + dp0)) * x1);
+    x2 = x1 / t1;
+    px2 = px1 * orc_sqr(t1);
+    y2 = y1;
+    py2 = py1;
+    t1 = sec2_edge / (rho * (1 + dp0));
+    x3 = x2 + t1 / 2 * orc_sqr(y2);
+    px3 = px2;
+    y3 = y2;
+    py3 = py2 - t1 * y2 * px2;
+    t1 = tan2_edge / (rho * (1 + dp0));
+    t2 = orc_exp_sel(t1 * x3);
+    x4 = x3;
+    px4 = px3 - t1 * y3 * py3;
+    y4 = y3 * t2;
+    py4 = py3 / t2;
+    t1 = orc_sqr(gap) * k0 * sec2_edge / (rho * (1 + dp0));
+    x5 = x4 - t1;
+    px5 = px4 - t1 * tan_edge / rho + orc_sqr(gap) * k4 * orc_sqr(sin_edge) * Rhe / (2 * rho * cos3_edge);
+    y5 = y4;
+    py5 = py4;
+  } else {
+    x1 = x0;
+    px1 = px0 + tan_edge / rho * x0 + tan3_edge / (2 * rho2 * (1 + dp0)) * orc_sqr(y0) +
+          tan3_edge / (2 * rho2 * (1 + dp0)) * orc_sqr(x0) - gap * k5 * sin_edge * Rhe / (rho * cos3_edge) * x0 +
+          k6 * sec2_edge * Rhe / (2 * rho) * (orc_sqr(y0) - orc_sqr(x0));
+    y1 = y0;
+    py1 = py0 - tan_edge / rho * y0 + tan3_edge / (rho2 * (1 + dp0)) * x0 * y0 +
+          gap * k2 * (1 + orc_sqr(sin_edge)) / (rho2 * (1 + dp0) * cos3_edge) * y0 +
+          2 * k3 * (orc_sqr(cos_edge) - 2) / (3 * gap * rho2 * cos3_edge) * P3(y0) +
+          gap * k5 * sin_edge * Rhe / (rho * cos3_edge) * y0 + k6 * P3(sec_edge) * Rhe / rho * x0 * y0;
+    t1 = (1 - tan2_edge / (2 * rho * (1 + dp0)) * x1);
+    x2 = x1 / t1;
+    px2 = px1 * orc_sqr(t1);
+    y2 = y1;
+    py2 = py1;
+    t1 = sec2_edge / (rho * (1 + dp0));
+    x3 = x2 - t1 / 2 * orc_sqr(y2);
+    px3 = px2;
+    y3 = y2;
+    py3 = py2 + t1 * y2 * px2;
+    t1 = -tan2_edge / (rho * (1 + dp0));
+    t2 = orc_exp_sel(t1 * x3);
+    x4 = x3;
+    px4 = px3 - t1 * y3 * py3;
+    y4 = y3 * t2;
+    py4 = py3 / t2;
+    x5 = x4 + orc_sqr(gap) * k0 * sec2_edge / (rho * (1 + dp0));
+    px5 = px4 + orc_sqr(gap) * k4 * orc_sqr(sin_edge) * Rhe / (2 * rho * cos3_edge);
+    y5 = y4;
+    py5 = py4;
+  }
+#undef P2
+#undef P3
+  Qf[0] = x5;
+  Qf[1] = px5;
+  Qf[2] = y5;
+  Qf[3] = py5;
+  Qf[5] = dp0;
+}
+
 static void csbend_edge(const orc_csbend_setup *S, int which, double *x, double *xp, double *y, double *yp,
                         double dp) {
   int eff = which < 0 ? S->edge1_effects : S->edge2_effects;
@@ -811,6 +972,30 @@ static void csbend_edge(const orc_csbend_setup *S, int which, double *x, double 
     apply_edge_effects(x, xp, y, yp, rho, S->n, e, he, psi * (1 + dp), which);
   } else if (eff == 3) {
     simple_dipole_edge_kick(xp, yp, *x, *y, dp, S->rho_actual, e, psi, lim);
+  } else if (eff == 2 || eff == 4) {
+    /* in dipole canonical coordinates (src/csbend.c:1139-1182, :1319-1359) */
+    double Qi[6], Qf[6];
+    Qi[0] = *x;
+    Qi[1] = *xp;
+    Qi[2] = *y;
+    Qi[3] = *yp;
+    Qi[4] = 0;
+    Qi[5] = dp;
+    double f = (1 + Qi[5]) / sqrt(1 + orc_sqr(Qi[1]) + orc_sqr(Qi[3]));
+    Qi[1] *= f;
+    Qi[3] *= f;
+    const double fint = which < 0 ? S->fint1 : S->fint2;
+    if (eff == 2)
+      fringe_hwang(Qf, Qi, S->rho_actual, (double)which, S->edge_order, e, 2 * S->hgap, fint, he);
+    else
+      fringe_hwang_lindberg(Qf, Qi, S->rho_actual, (double)which, e, 2 * S->hgap, fint, he);
+    f = 1 / sqrt(orc_sqr(1 + Qf[5]) - orc_sqr(Qf[1]) - orc_sqr(Qf[3]));
+    Qf[1] *= f;
+    Qf[3] *= f;
+    *x = Qf[0];
+    *xp = Qf[1];
+    *y = Qf[2];
+    *yp = Qf[3];
   }
 }
 
@@ -933,6 +1118,7 @@ double orc_cr_sin(double x) { return trkcr_sin(x); }
 double orc_cr_cos(double x) { return trkcr_cos(x); }
 double orc_cr_asin(double x) { return trkcr_asin(x); }
 double orc_cr_tan(double x) { return trkcr_tan(x); }
+double orc_cr_exp(double x) { return trkcr_exp(x); }
 /* the double-double evaluations behind the fast paths, and the fast paths'
  * parts (hi, L, error bound e; returns the rounding test's verdict), for the
  * tests of the fast paths' error bounds */
@@ -957,7 +1143,8 @@ int orc_cr_parts(int kind, double x, double *out) {
 /* Self-test of the tiered correctly rounded functions: n arguments drawn
  * uniformly from [lo, hi] (log_mag: magnitudes log-uniform in [lo, hi],
  * random sign), each function against its double-double evaluation
- * (trkcr_*_slow, ~2^-100 relative).  Returns the number of disagreements;
+ * (trkcr_*_slow, ~2^-100 relative; kind 3: sin and cos together, kind 4:
+ * exp).  Returns the number of disagreements;
  * *tiny_hits counts the calls whose tiny-argument test accepted and
  * *max_rel the largest relative error of the tiny path's correction
  * (against the double-double value minus the leading term), which the
@@ -984,6 +1171,15 @@ long orc_cr_selftest(int kind, double lo, double hi, int log_mag, long n, unsign
       x = lo + u * (hi - lo);
     double got, want, t;
     const double z = x * x, ax = fabs(x);
+    if (kind == 4 && ax >= 0x1p-12 && ax <= TRKCR_TINY) {
+      /* the tiny path's x^2 P(x) against exp - 1 - x from the double-double
+       * (whose absolute accuracy, ~2^-100, resolves x^2 P to 2^-75 here) */
+      const trkcr_dd v = trkcr_exp_dd(x);
+      const double ce = ((v.hi - 1.0) - x) + v.lo;
+      const double rel = fabs(trkcr_exp_tiny_t(x) - ce) / fabs(ce);
+      if (rel > mrel)
+        mrel = rel;
+    }
     if (kind <= 2 && ax >= 0x1p-26 && ax <= TRKCR_TINY) {
       /* the exact correction from the double-double value (hi - lead is
        * exact: hi and the lead are within a factor of two) */
@@ -1023,6 +1219,9 @@ long orc_cr_selftest(int kind, double lo, double hi, int log_mag, long n, unsign
       got = trkcr_asin(x);
       want = trkcr_asin_slow(x);
       hits += ax >= 0x1p-26 && ax <= TRKCR_TINY && trkcr_asin_tiny(x, z, &t);
+    } else if (kind == 4) {
+      got = trkcr_exp(x);
+      want = trkcr_exp_slow(x);
     } else {
       double s, c;
       trkcr_sincos(x, &s, &c);
@@ -1038,6 +1237,40 @@ long orc_cr_selftest(int kind, double lo, double hi, int log_mag, long n, unsign
     *tiny_hits = hits;
   if (max_rel)
     *max_rel = mrel;
+  return bad;
+}
+
+/* Self-test of trkcr_div_rcp (the parity build's division by a divisor
+ * with a precomputed correctly rounded reciprocal) against the IEEE
+ * quotient: n random pairs over 2^-20..2^20 with random signs, one in four
+ * divisors with a run of trailing ones, one in four dividends placed on a
+ * rounding midpoint of the quotient, and zeros.  Returns disagreements. */
+long orc_div_rcp_selftest(long n, unsigned long long seed) {
+  unsigned long long st = seed;
+  long bad = 0;
+  for (long k = 0; k < n; k++) {
+    const unsigned long long r1 = orc_splitmix(&st), r2 = orc_splitmix(&st), r3 = orc_splitmix(&st);
+    double a = ldexp(1.0 + (double)(r1 >> 12) * 0x1p-52, (int)(r3 % 41) - 20);
+    double b = ldexp(1.0 + (double)(r2 >> 12) * 0x1p-52, (int)((r3 >> 8) % 41) - 20);
+    if (r3 & (1ULL << 20))
+      a = -a;
+    if (r3 & (1ULL << 21))
+      b = -b;
+    if ((k & 3) == 1) {
+      uint64_t bits;
+      memcpy(&bits, &b, 8);
+      bits |= (1ULL << 52) - (1ULL << ((r3 >> 24) % 9));
+      memcpy(&b, &bits, 8);
+    } else if ((k & 3) == 2) {
+      const double q = a / b, m = q + (nextafter(q, INFINITY) - q) / 2;
+      a = m * b;
+    } else if ((k & 1023) == 3) {
+      a = (r3 & 1) ? 0.0 : -0.0;
+    }
+    const double got = trkcr_div_rcp(a, b, 1.0 / b), want = a / b;
+    if (memcmp(&got, &want, 8) != 0)
+      bad++;
+  }
   return bad;
 }
 

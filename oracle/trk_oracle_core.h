@@ -38,6 +38,7 @@ static inline double orc_sin_sel(double x) { return orc_cr_math ? trkcr_sin(x) :
 static inline double orc_cos_sel(double x) { return orc_cr_math ? trkcr_cos(x) : cos(x); }
 static inline double orc_asin_sel(double x) { return orc_cr_math ? trkcr_asin(x) : asin(x); }
 static inline double orc_tan_sel(double x) { return orc_cr_math ? trkcr_tan(x) : tan(x); }
+static inline double orc_exp_sel(double x) { return orc_cr_math ? trkcr_exp(x) : exp(x); }
 
 #ifndef ORC_R
 #define ORC_R double

@@ -34,6 +34,15 @@ ELEMENT_CASES = {
     "csbend_edge_order2": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=0.03, EDGE_ORDER=2, K1=0.2, N_SLICES=8),
     "csbend_edge3": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=0.03, EDGE1_EFFECTS=3, EDGE2_EFFECTS=3,
                            N_SLICES=8),
+    "csbend_hwang": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=0.03, HGAP=0.02, FINT=0.5, H1=0.3, H2=-0.2,
+                           EDGE1_EFFECTS=2, EDGE2_EFFECTS=2, N_SLICES=8),
+    "csbend_hwang_order2": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=0.03, HGAP=0.02, FINT1=0.45, FINT2=0.55,
+                                  H1=0.3, H2=-0.2, EDGE1_EFFECTS=2, EDGE2_EFFECTS=2, EDGE_ORDER=2, K1=0.2,
+                                  N_SLICES=8),
+    "csbend_hwang_lindberg": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=0.03, HGAP=0.025, FINT=0.5, H1=0.3,
+                                    H2=-0.2, EDGE1_EFFECTS=4, EDGE2_EFFECTS=4, N_SLICES=8),
+    "csbend_hwang_negative": single("CSBEND", L=1.0, ANGLE=-0.06, E1=0.02, E2=0.05, HGAP=0.02, FINT=0.6,
+                                    EDGE1_EFFECTS=4, EDGE2_EFFECTS=2, N_SLICES=8),
     "csbend_misaligned": single("CSBEND", L=1.0, ANGLE=0.05, DX=1e-4, DY=2e-4, DZ=-1e-4, TILT=0.02, N_SLICES=8),
     "csbend_order6": single("CSBEND", L=1.0, ANGLE=0.05, N_SLICES=4, INTEGRATION_ORDER=6),
     "kquad_rad": single("KQUAD", L=0.3, K1=1.2, N_KICKS=8, SYNCH_RAD=1),

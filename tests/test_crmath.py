@@ -86,7 +86,7 @@ def test_correct_rounding(kind, lo, hi):
     assert not bad, f"{kind}: {len(bad)} of {len(xs)} not correctly rounded, e.g. {bad[:3]}"
 
 
-@pytest.mark.parametrize("kind", [0, 1, 2, 3])
+@pytest.mark.parametrize("kind", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("lo,hi,log_mag", [(2.0 ** -30, 2.0 ** -7, 1), (-2.0 ** -7, 2.0 ** -7, 0),
                                            (2.0 ** -7, 2.0 ** -5, 1), (-0.05, 0.05, 0)])
 def test_tiered_paths_agree_with_double_double(kind, lo, hi, log_mag):
@@ -101,5 +101,45 @@ def test_tiered_paths_agree_with_double_double(kind, lo, hi, log_mag):
     bad = lib.orc_cr_selftest(kind, lo, hi, log_mag, 1_000_000, 4242 + kind, ctypes.byref(hits), ctypes.byref(mrel))
     assert bad == 0
     assert mrel.value < 2.0 ** -50.7
-    if hi <= 2.0 ** -7 and kind < 3:
+    if hi <= 2.0 ** -7 and kind < 3 and log_mag == 0:
         assert hits.value > 0.8 * 1_000_000  # the tiny path takes nearly every call
+
+
+def test_division_with_precomputed_reciprocal_is_ieee():
+    """trkcr_div_rcp (Markstein's two FMA corrections from RN(1/b)) against
+    the IEEE quotient on 4e6 pairs, a quarter of them on rounding midpoints
+    of the quotient and a quarter with divisors of many trailing ones."""
+    lib = pyoracle.load()
+    assert lib.orc_div_rcp_selftest(4_000_000, 99) == 0
+
+
+def test_exp_correctly_rounded():
+    """trkcr_exp (the Hwang-Lindberg fringe's per-particle exp) against
+    120-digit values, on its tiny and general paths."""
+    lib = pyoracle.load()
+    lib.orc_cr_exp.argtypes = [ctypes_double()]
+    lib.orc_cr_exp.restype = ctypes_double()
+    rng = np.random.Generator(np.random.Philox(8))
+    xs = np.concatenate([rng.uniform(-2.0 ** -7, 2.0 ** -7, 200), rng.uniform(-30, 30, 100)])
+    bad = [x for x in xs if lib.orc_cr_exp(float(x)) != float(dexp(float(x)))]
+    assert not bad, bad[:3]
+
+
+def ctypes_double():
+    import ctypes
+    return ctypes.c_double
+
+
+def dexp(x):
+    x = Decimal(x)
+    n = int((x / Decimal(2).ln()).to_integral_value())
+    r = x - n * Decimal(2).ln()
+    t = s = Decimal(1)
+    k = 1
+    while True:
+        t = t * r / k
+        k += 1
+        if abs(t) < Decimal(10) ** -125:
+            break
+        s += t
+    return s * (Decimal(2) ** n)
