@@ -9,10 +9,12 @@
  */
 #include <cmath>
 #include <cstring>
+#include <utility>
 #include <vector>
 
 #include "trk_compile.h"
 #include "trk_constants.h"
+#include "trk_crmath.h"
 #include "trk_lattice.h"
 
 namespace {
@@ -158,6 +160,63 @@ int trk_csbend_field_table(const double *b, const double *c, double h, int nonli
 
 namespace {
 
+/* quadPartialFringeMatrix (src/fringe.c:231-275): the 2x2 blocks
+ * {R00, R01, R10, R11, R22, R23, R32, R33} of one linear fringe part; the
+ * exponentials correctly rounded, as the parity build's arithmetic is */
+static void quad_partial_fringe(double *R, double K1, long inFringe, const double *fi, long part) {
+  double J1x, J2x, J3x, J1y, J2y, J3y;
+  const double K1sqr = K1 * K1;
+  if (part == 1) {
+    J1x = inFringe * (K1 * fi[1] - 2 * K1sqr * fi[3] / 3. - K1sqr * fi[0] * fi[2] / 2);
+    J2x = inFringe * K1 * fi[2];
+    J3x = inFringe * K1sqr * (fi[2] + fi[4] + fi[0] * fi[1]);
+    J1y = inFringe * (-K1 * fi[1] - 2 * K1sqr * fi[3] / 3. - K1sqr * fi[0] * fi[2] / 2);
+  } else {
+    J1x = inFringe * (K1 * fi[1] + K1sqr * fi[0] * fi[2] / 2);
+    J2x = inFringe * K1 * fi[2];
+    J3x = inFringe * K1sqr * (fi[4] - fi[0] * fi[1]);
+    J1y = inFringe * (-K1 * fi[1] + K1sqr * fi[0] * fi[2] / 2);
+  }
+  J2y = -J2x;
+  J3y = J3x;
+  const double ex = trkcr_exp(J1x), ey = trkcr_exp(J1y);
+  R[0] = ex;
+  R[1] = J2x / ex;
+  R[2] = ex * J3x;
+  R[3] = (1 + J2x * J3x) / ex;
+  R[4] = ey;
+  R[5] = J2y / ey;
+  R[6] = ey * J3y;
+  R[7] = (1 + J2y * J3y) / ey;
+}
+
+/* the two linear parts quadFringe applies at one edge (src/fringe.c:47-90):
+ * M1 from the I-m integrals, M2 from the I+m ones, diagonal entries swapped
+ * and the parts exchanged at an entrance, inverted for a backward magnet */
+static void quad_fringe_matrices(double K1, const double *fint_m, const double *fint_p, int backtrack, int inFringe,
+                          double *M1, double *M2) {
+  quad_partial_fringe(M1, K1, 1, fint_m, 1);
+  quad_partial_fringe(M2, K1, 1, fint_p, 2);
+  if (inFringe * (backtrack ? -1 : 1) == -1) {
+    std::swap(M1[0], M1[3]);
+    std::swap(M1[4], M1[7]);
+    std::swap(M2[0], M2[3]);
+    std::swap(M2[4], M2[7]);
+    for (int k = 0; k < 8; k++)
+      std::swap(M1[k], M2[k]);
+  }
+  if (backtrack) {
+    for (double *M : {M1, M2}) {
+      std::swap(M[0], M[3]);
+      std::swap(M[4], M[7]);
+      M[1] *= -1;
+      M[2] *= -1;
+      M[5] *= -1;
+      M[6] *= -1;
+    }
+  }
+}
+
 int compile_mult(const trk_elem *e, double Po, trk_op *op) {
   double KnL[3] = {0, 0, 0}, drift, tilt, dx, dy, dz, xkick = 0, ykick = 0, lEnd = 0;
   int order[3] = {0, 0, 0}, skew[3] = {0, 0, 0}, integ, expand;
@@ -167,9 +226,8 @@ int compile_mult(const trk_elem *e, double Po, trk_op *op) {
   double cfac = TRK_E_MKS / (TRK_ME_MKS * TRK_C_MKS * Po);
   switch (e->type) {
   case TRK_KQUAD: {
-    if (TRK_P(e, KQUAD_EDGE1_EFFECTS) || TRK_P(e, KQUAD_EDGE2_EFFECTS) || TRK_P(e, KQUAD_RADIAL) ||
-        TRK_P(e, KQUAD_MALIGN_METHOD))
-      return trk_set_error(TRK_ERR_UNSUPPORTED, "KQUAD %s: fringe, RADIAL and MALIGN_METHOD!=0 are not on this path",
+    if (TRK_P(e, KQUAD_RADIAL) || TRK_P(e, KQUAD_MALIGN_METHOD))
+      return trk_set_error(TRK_ERR_UNSUPPORTED, "KQUAD %s: RADIAL and MALIGN_METHOD!=0 are not on this path",
                            e->name);
     synch_rad = TRK_P(e, KQUAD_SYNCH_RAD) != 0;
     isr = TRK_P(e, KQUAD_ISR) != 0;
@@ -362,6 +420,24 @@ int compile_mult(const trk_elem *e, double Po, trk_op *op) {
           flags |= MF_ISR1OFF;
       }
     }
+  }
+  /* KQUAD hard-edge fringe (src/multipole.c:999-1006, :1054-1061; src/fringe.c) */
+  if (e->type == TRK_KQUAD) {
+    for (int edge = 0; edge < 2; edge++) {
+      const int eff = (int)(edge ? TRK_P(e, KQUAD_EDGE2_EFFECTS) : TRK_P(e, KQUAD_EDGE1_EFFECTS));
+      if (eff <= 0)
+        continue;
+      flags |= edge ? MF_FRINGE2 : MF_FRINGE1;
+      double *fr = op->d + (edge ? MD_FR2 : MD_FR1);
+      const int linear = (int)(edge ? TRK_P(e, KQUAD_EDGE2_LINEAR) : TRK_P(e, KQUAD_EDGE1_LINEAR));
+      if (linear)
+        quad_fringe_matrices(TRK_P(e, KQUAD_K1), &TRK_P(e, KQUAD_I0M), &TRK_P(e, KQUAD_I0P), TRK_P(e, KQUAD_L) < 0,
+                             edge ? 1 : -1, fr, fr + 8);
+      fr[16] = edge ? TRK_P(e, KQUAD_EDGE2_NONLINEAR_FACTOR) : TRK_P(e, KQUAD_EDGE1_NONLINEAR_FACTOR);
+      fr[17] = eff;
+      fr[18] = linear;
+    }
+    op->d[MD_FRK1] = TRK_P(e, KQUAD_K1);
   }
   op->i[6] = flags;
   return TRK_OK;
@@ -900,7 +976,8 @@ int trk_compile(const trk_lattice *l, double Po, CompiledLattice &out) {
       const int f = op.i[6];
       const int o = op.i[4] & 0xff;
       if (op.i[1] == 4 && !op.i[2] && op.d[MD_DRIFT] != 0 && o >= 1 && o <= 3 && !(op.i[5] & 1) &&
-          !(f & (MF_KNL1 | MF_KNL2 | MF_XKICK | MF_YKICK | MF_OFFSET | MF_TILT | MF_ENDDRIFT | MF_RAD)))
+          !(f & (MF_KNL1 | MF_KNL2 | MF_XKICK | MF_YKICK | MF_OFFSET | MF_TILT | MF_ENDDRIFT | MF_RAD | MF_FRINGE1 |
+                 MF_FRINGE2)))
         op.kind = OPK_MULT1;
     } else if (op.kind == OPK_BEND) {
       const bool e1_noop = op.i[5] == EDGE_NONE ||

@@ -27,6 +27,8 @@
 #include "trk_crmath.h"
 #include "trk_philox.h"
 
+#include <cfloat>
+
 #include "trk_kernels.h"
 #include "trk_ops.h"
 
@@ -313,6 +315,125 @@ struct IsrKey {
   bool single;
 };
 
+/* quadFringe (src/fringe.c:25-219) on one particle: slopes to momenta, the
+ * first linear part, the nonlinear generator of order |higherOrder| (2:
+ * leading, 3: higher), the second linear part, the path-length change,
+ * momenta back to slopes; `fr` holds the edge's M1, M2, nonlinear factor,
+ * higherOrder and linear flag (compile_mult), each expression in the
+ * reference's operation order. */
+__device__ __noinline__ void quad_fringe(Part &p, const double *__restrict__ fr, double K1, int inFringe) {
+  const double nonlinearFactor = __ldg(&fr[16]);
+  const int higherOrder = (int)__ldg(&fr[17]);
+  const bool linear = __ldg(&fr[18]) != 0;
+  const double delta = p.dp;
+  double x, px, y, py, v1, v3, a, dx = 0, dpx = 0, dy = 0, dpy = 0, ds = 0;
+  {
+    const double xp = p.xp, yp = p.yp;
+    const double denom = sqrt(1 + sqr(xp) + sqr(yp));
+    v1 = (1 + delta) * xp / denom;
+    v3 = (1 + delta) * yp / denom;
+  }
+  if (linear) {
+    x = __ldg(&fr[0]) * p.x + __ldg(&fr[1]) * v1;
+    px = __ldg(&fr[2]) * p.x + __ldg(&fr[3]) * v1;
+    y = __ldg(&fr[4]) * p.y + __ldg(&fr[5]) * v3;
+    py = __ldg(&fr[6]) * p.y + __ldg(&fr[7]) * v3;
+  } else {
+    x = p.x;
+    px = v1;
+    y = p.y;
+    py = v3;
+  }
+  a = -inFringe * K1 / (12 * (1 + delta));
+  const int ho = higherOrder < 0 ? -higherOrder : higherOrder;
+  if (ho > 1) {
+    double xpow[9], ypow[9];
+    xpow[0] = ypow[0] = 1;
+    if (ho > 2) {
+      double apow[4];
+      apow[0] = 1;
+#pragma unroll
+      for (int i = 1; i < 9; i++) {
+        xpow[i] = xpow[i - 1] * x;
+        ypow[i] = ypow[i - 1] * y;
+      }
+#pragma unroll
+      for (int i = 1; i < 4; i++)
+        apow[i] = apow[i - 1] * a;
+      dpx = (a * (12 * a * (-4 * py * x * y + px * (xpow[2] - 5 * ypow[2])) * (xpow[2] - ypow[2]) -
+                  24 * (-2 * py * x * y + px * (xpow[2] + ypow[2])) +
+                  4 * apow[2] *
+                    (-2 * py * x * y * (3 * xpow[4] + 50 * xpow[2] * ypow[2] - 21 * ypow[4]) +
+                     px * (xpow[6] + 75 * xpow[4] * ypow[2] - 105 * xpow[2] * ypow[4] - 35 * ypow[6])) +
+                  3 * apow[3] *
+                    (-8 * py * x * y * (xpow[6] - 27 * xpow[4] * ypow[2] + 83 * xpow[2] * ypow[4] + 7 * ypow[6]) +
+                     px * (xpow[8] - 108 * xpow[6] * ypow[2] + 830 * xpow[4] * ypow[4] + 196 * xpow[2] * ypow[6] +
+                           105 * ypow[8])))) /
+            8;
+      dpy = (a * (-8 * px * x * y *
+                    (6 - 6 * a * (xpow[2] - ypow[2]) + apow[2] * (21 * xpow[4] - 50 * xpow[2] * ypow[2] - 3 * ypow[4]) +
+                     3 * apow[3] * (7 * xpow[6] + 83 * xpow[4] * ypow[2] - 27 * xpow[2] * ypow[4] + ypow[6])) +
+                  py * (315 * apow[3] * xpow[8] + 28 * apow[2] * xpow[6] * (5 + 21 * a * ypow[2]) +
+                        30 * a * xpow[4] * (2 + 14 * a * ypow[2] + 83 * apow[2] * ypow[4]) +
+                        ypow[2] * (24 + 12 * a * ypow[2] - 4 * apow[2] * ypow[4] + 3 * apow[3] * ypow[6]) -
+                        12 * xpow[2] * (-2 + 6 * a * ypow[2] + 25 * apow[2] * ypow[4] + 27 * apow[3] * ypow[6])))) /
+            8;
+      if (higherOrder > 0) {
+        dx = (a * x *
+              (8 * (xpow[2] + 3 * ypow[2]) +
+               4 * apow[2] * (5 * xpow[6] + 21 * xpow[4] * ypow[2] - 25 * xpow[2] * ypow[4] - ypow[6]) +
+               apow[3] * (35 * xpow[8] + 84 * xpow[6] * ypow[2] + 498 * xpow[4] * ypow[4] - 108 * xpow[2] * ypow[6] +
+                          3 * ypow[8]) +
+               12 * a * sqr(xpow[2] - ypow[2]))) /
+             8;
+        dy = (a * y *
+              (-8 * (3 * xpow[2] + ypow[2]) +
+               4 * apow[2] * (xpow[6] + 25 * xpow[4] * ypow[2] - 21 * xpow[2] * ypow[4] - 5 * ypow[6]) +
+               apow[3] * (3 * xpow[8] - 108 * xpow[6] * ypow[2] + 498 * xpow[4] * ypow[4] + 84 * xpow[2] * ypow[6] +
+                          35 * ypow[8]) +
+               12 * a * sqr(xpow[2] - ypow[2]))) /
+             8;
+      }
+    } else {
+#pragma unroll
+      for (int i = 1; i < 4; i++) {
+        xpow[i] = xpow[i - 1] * x;
+        ypow[i] = ypow[i - 1] * y;
+      }
+      dpx = 3 * a * (-px * xpow[2] + 2 * py * x * y - px * ypow[2]);
+      dpy = 3 * a * (py * xpow[2] - 2 * px * x * y + py * ypow[2]);
+      if (higherOrder > 0) {
+        dx = a * (xpow[3] + 3 * x * ypow[2]);
+        dy = a * (-3 * xpow[2] * y - ypow[3]);
+      }
+    }
+    ds = (a / (1 + delta)) * (3 * py * y * xpow[2] - px * xpow[3] - 3 * px * x * ypow[2] + py * ypow[3]);
+  }
+  x += nonlinearFactor * dx;
+  px += nonlinearFactor * dpx;
+  y += nonlinearFactor * dy;
+  py += nonlinearFactor * dpy;
+  if (linear) {
+    p.x = __ldg(&fr[8]) * x + __ldg(&fr[9]) * px;
+    v1 = __ldg(&fr[10]) * x + __ldg(&fr[11]) * px;
+    p.y = __ldg(&fr[12]) * y + __ldg(&fr[13]) * py;
+    v3 = __ldg(&fr[14]) * y + __ldg(&fr[15]) * py;
+  } else {
+    p.x = x;
+    v1 = px;
+    p.y = y;
+    v3 = py;
+  }
+  p.s -= nonlinearFactor * ds;
+  double denom = sqr(1 + delta) - sqr(v1) - sqr(v3);
+  if (denom > 0) {
+    denom = sqrt(denom);
+    p.xp = v1 / denom;
+    p.yp = v3 / denom;
+  } else
+    p.xp = p.yp = DBL_MAX;
+}
+
 /* multipole_tracking2 + integrate_kick_multipole_ordn (src/multipole.c:660-1456) */
 __device__ __forceinline__ bool op_mult(const trk_op *__restrict__ op, Part &p, double Po, double z_start,
                                         const trk_aperture *ap, const IsrKey *isr = nullptr) {
@@ -331,6 +452,8 @@ __device__ __forceinline__ bool op_mult(const trk_op *__restrict__ op, Part &p, 
     rotate(p, __ldg(&d[MD_TC]), __ldg(&d[MD_TS]));
   if (flags & MF_ENDDRIFT)
     exact_drift(p, __ldg(&d[MD_LEND]));
+  if (flags & MF_FRINGE1) /* KQUAD entrance fringe (src/multipole.c:999-1006) */
+    quad_fringe(p, d + MD_FR1, __ldg(&d[MD_FRK1]), -1);
 
   bool ok = true;
   double dzLoss = 0;
@@ -515,6 +638,10 @@ done:
     p.s = z_start + dzLoss;
     p.dp = Po * (1 + p.dp);
   }
+  /* KQUAD exit fringe, lost particles included as in the reference
+   * (src/multipole.c:1054-1061 runs it over all n_part rows) */
+  if (flags & MF_FRINGE2)
+    quad_fringe(p, d + MD_FR2, __ldg(&d[MD_FRK1]), 1);
   if (flags & MF_ENDDRIFT)
     exact_drift(p, __ldg(&d[MD_LEND]));
   if (flags & MF_TILT)

@@ -48,6 +48,8 @@ enum trk_op_kind {
 #define MF_RAD 512    /* radiation block after each kick (SYNCH_RAD and/or ISR) */
 #define MF_ISR 1024   /* incoherent synchrotron radiation (ISR) */
 #define MF_ISR1OFF 2048 /* ISR1PART=0: no ISR when a single particle is tracked */
+#define MF_FRINGE1 4096 /* KQUAD entrance fringe (EDGE1_EFFECTS > 0) */
+#define MF_FRINGE2 8192 /* KQUAD exit fringe (EDGE2_EFFECTS > 0) */
 
 /* bend flags (i[7]) */
 #define BF_ISR_ROUNDTRIP 1 /* reference's (1+DPoP) divide/multiply round trip */
@@ -109,6 +111,14 @@ typedef struct {
 #define MD_XKR 80    /* xkick / n_parts, ykick / n_parts (radiation field strength) */
 #define MD_YKR 81
 #define MD_ISR 82    /* isr_coef (src/multipole.c:757) */
+/* KQUAD fringe, per edge (entrance at MD_FR1, exit at MD_FR2): the linear
+ * parts M1 and M2 as they apply to that edge (R00 R01 R10 R11 R22 R23 R32
+ * R33 each), the nonlinear factor, EDGE_EFFECTS (higherOrder), EDGE_LINEAR;
+ * K1 at MD_FRK1 */
+#define MD_FR1 83
+#define MD_FR2 102
+#define MD_FRLEN 19
+#define MD_FRK1 121
 /* i: 0 n_parts, 1 nSub, 2 expand, 3 maxOrder, 4 orders (o0 | o1<<8 | o2<<16), 5 skew bits, 6 flags */
 
 /* BEND */

@@ -52,7 +52,21 @@
   X(KQUAD_LEFFECTIVE, "LEFFECTIVE", 0.0)           \
   X(KQUAD_RADIAL, "RADIAL", 0.0)                   \
   X(KQUAD_EXPAND_HAMILTONIAN, "EXPAND_HAMILTONIAN", 0.0) \
-  X(KQUAD_MALIGN_METHOD, "MALIGN_METHOD", 0.0)
+  X(KQUAD_MALIGN_METHOD, "MALIGN_METHOD", 0.0)     \
+  X(KQUAD_I0P, "I0P", 0.0)                         \
+  X(KQUAD_I1P, "I1P", 0.0)                         \
+  X(KQUAD_I2P, "I2P", 0.0)                         \
+  X(KQUAD_I3P, "I3P", 0.0)                         \
+  X(KQUAD_LAMBDA2P, "LAMBDA2P", 0.0)               \
+  X(KQUAD_I0M, "I0M", 0.0)                         \
+  X(KQUAD_I1M, "I1M", 0.0)                         \
+  X(KQUAD_I2M, "I2M", 0.0)                         \
+  X(KQUAD_I3M, "I3M", 0.0)                         \
+  X(KQUAD_LAMBDA2M, "LAMBDA2M", 0.0)               \
+  X(KQUAD_EDGE1_LINEAR, "EDGE1_LINEAR", 1.0)       \
+  X(KQUAD_EDGE2_LINEAR, "EDGE2_LINEAR", 1.0)       \
+  X(KQUAD_EDGE1_NONLINEAR_FACTOR, "EDGE1_NONLINEAR_FACTOR", 1.0) \
+  X(KQUAD_EDGE2_NONLINEAR_FACTOR, "EDGE2_NONLINEAR_FACTOR", 1.0)
 
 #define TRK_PARAMS_KSEXT(X)                        \
   X(KSEXT_L, "L", 0.0)                             \
@@ -258,6 +272,6 @@ enum {
 };
 #undef TRK_ENUM_ENTRY
 
-#define TRK_MAX_PARAMS 64
+#define TRK_MAX_PARAMS 128
 
 #endif

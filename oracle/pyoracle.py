@@ -228,8 +228,8 @@ def ref_param_defaults(type_code):
     """The reference's default of each parameter of the lattice tables
     (NaN where the reference table lacks the name)."""
     lib = load_ref()
-    out = np.zeros(64)
-    n = lib.ref_param_defaults(type_code, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 64)
+    out = np.zeros(128)
+    n = lib.ref_param_defaults(type_code, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 128)
     if n < 0:
         raise RuntimeError("bad type")
     return out[:n]

@@ -288,6 +288,183 @@ static void rotate_beam(double *coord, long np, double angle) {
 /* ------------------------------------------------------------ multipoles */
 /* multipole_tracking2 (src/multipole.c:660-1084) for KQUAD, KSEXT, KOCT,
  * MALIGN_METHOD=0, no radiation, no fringe, no error multipoles. */
+/* quadPartialFringeMatrix (src/fringe.c:231-275): the 2x2 blocks of one
+ * linear fringe part, R = {R00, R01, R10, R11, R22, R23, R32, R33} */
+static void quad_partial_fringe_matrix(double *R, double K1, long inFringe, const double *fringeInt, long part) {
+  double J1x, J2x, J3x, J1y, J2y, J3y, K1sqr, expJ1x, expJ1y;
+  K1sqr = orc_sqr(K1);
+  if (part == 1) {
+    J1x = inFringe * (K1 * fringeInt[1] - 2 * K1sqr * fringeInt[3] / 3. - K1sqr * fringeInt[0] * fringeInt[2] / 2);
+    J2x = inFringe * K1 * fringeInt[2];
+    J3x = inFringe * K1sqr * (fringeInt[2] + fringeInt[4] + fringeInt[0] * fringeInt[1]);
+    J1y = inFringe * (-K1 * fringeInt[1] - 2 * K1sqr * fringeInt[3] / 3. - K1sqr * fringeInt[0] * fringeInt[2] / 2);
+    J2y = -J2x;
+    J3y = J3x;
+  } else {
+    J1x = inFringe * (K1 * fringeInt[1] + K1sqr * fringeInt[0] * fringeInt[2] / 2);
+    J2x = inFringe * K1 * fringeInt[2];
+    J3x = inFringe * K1sqr * (fringeInt[4] - fringeInt[0] * fringeInt[1]);
+    J1y = inFringe * (-K1 * fringeInt[1] + K1sqr * fringeInt[0] * fringeInt[2] / 2);
+    J2y = -J2x;
+    J3y = J3x;
+  }
+  expJ1x = R[0] = orc_exp_sel(J1x);
+  R[1] = J2x / expJ1x;
+  R[2] = expJ1x * J3x;
+  R[3] = (1 + J2x * J3x) / expJ1x;
+  expJ1y = R[4] = orc_exp_sel(J1y);
+  R[5] = J2y / expJ1y;
+  R[6] = expJ1y * J3y;
+  R[7] = (1 + J2y * J3y) / expJ1y;
+}
+
+#define ORC_SWAP(a, b)                                                                                             \
+  do {                                                                                                             \
+    double t_ = (a);                                                                                               \
+    (a) = (b);                                                                                                     \
+    (b) = t_;                                                                                                      \
+  } while (0)
+
+/* quadFringe (src/fringe.c:25-219): KQUAD hard-edge fringe, linear parts
+ * from the fringe integrals and the leading (|higherOrder| = 2) or higher
+ * (3) order nonlinear generator, on every row of coord */
+static void quad_fringe(double *coord, long np, double K1, const double *fringeIntM, const double *fringeIntP,
+                        int backtrack, int inFringe, int higherOrder, int linearFlag, double nonlinearFactor) {
+  double M1[8], M2[8];
+  if (linearFlag) {
+    quad_partial_fringe_matrix(M1, K1, 1, fringeIntM, 1);
+    quad_partial_fringe_matrix(M2, K1, 1, fringeIntP, 2);
+    if (inFringe * (backtrack ? -1 : 1) == -1) {
+      ORC_SWAP(M1[0], M1[3]);
+      ORC_SWAP(M1[4], M1[7]);
+      ORC_SWAP(M2[0], M2[3]);
+      ORC_SWAP(M2[4], M2[7]);
+      for (int k = 0; k < 8; k++)
+        ORC_SWAP(M1[k], M2[k]);
+    }
+    if (backtrack) {
+      ORC_SWAP(M1[0], M1[3]);
+      ORC_SWAP(M1[4], M1[7]);
+      M1[1] *= -1;
+      M1[2] *= -1;
+      M1[5] *= -1;
+      M1[6] *= -1;
+      ORC_SWAP(M2[0], M2[3]);
+      ORC_SWAP(M2[4], M2[7]);
+      M2[1] *= -1;
+      M2[2] *= -1;
+      M2[5] *= -1;
+      M2[6] *= -1;
+    }
+  }
+  for (long ip = 0; ip < np; ip++) {
+    double *vec = ROW(ip);
+    double x, px, y, py, delta, xp, yp, denom, a, dx, dpx, dy, dpy, ds;
+    delta = vec[5];
+    xp = vec[1];
+    yp = vec[3];
+    denom = sqrt(1 + orc_sqr(xp) + orc_sqr(yp));
+    vec[1] = (1 + delta) * xp / denom;
+    vec[3] = (1 + delta) * yp / denom;
+    if (linearFlag) {
+      x = M1[0] * vec[0] + M1[1] * vec[1];
+      px = M1[2] * vec[0] + M1[3] * vec[1];
+      y = M1[4] * vec[2] + M1[5] * vec[3];
+      py = M1[6] * vec[2] + M1[7] * vec[3];
+    } else {
+      x = vec[0];
+      px = vec[1];
+      y = vec[2];
+      py = vec[3];
+    }
+    a = -inFringe * K1 / (12 * (1 + delta));
+    dx = dpx = dy = dpy = ds = 0;
+    if (abs(higherOrder) > 1) {
+      double xpow[9], ypow[9], apow[4];
+      xpow[0] = ypow[0] = apow[0] = 1;
+      if (abs(higherOrder) > 2) {
+        for (int i = 1; i < 9; i++) {
+          xpow[i] = xpow[i - 1] * x;
+          ypow[i] = ypow[i - 1] * y;
+        }
+        for (int i = 1; i < 4; i++)
+          apow[i] = apow[i - 1] * a;
+        dpx = (a * (12 * a * (-4 * py * x * y + px * (xpow[2] - 5 * ypow[2])) * (xpow[2] - ypow[2]) -
+                    24 * (-2 * py * x * y + px * (xpow[2] + ypow[2])) +
+                    4 * apow[2] *
+                      (-2 * py * x * y * (3 * xpow[4] + 50 * xpow[2] * ypow[2] - 21 * ypow[4]) +
+                       px * (xpow[6] + 75 * xpow[4] * ypow[2] - 105 * xpow[2] * ypow[4] - 35 * ypow[6])) +
+                    3 * apow[3] *
+                      (-8 * py * x * y * (xpow[6] - 27 * xpow[4] * ypow[2] + 83 * xpow[2] * ypow[4] + 7 * ypow[6]) +
+                       px * (xpow[8] - 108 * xpow[6] * ypow[2] + 830 * xpow[4] * ypow[4] + 196 * xpow[2] * ypow[6] +
+                             105 * ypow[8])))) /
+              8;
+        dpy = (a * (-8 * px * x * y *
+                      (6 - 6 * a * (xpow[2] - ypow[2]) + apow[2] * (21 * xpow[4] - 50 * xpow[2] * ypow[2] - 3 * ypow[4]) +
+                       3 * apow[3] * (7 * xpow[6] + 83 * xpow[4] * ypow[2] - 27 * xpow[2] * ypow[4] + ypow[6])) +
+                    py * (315 * apow[3] * xpow[8] + 28 * apow[2] * xpow[6] * (5 + 21 * a * ypow[2]) +
+                          30 * a * xpow[4] * (2 + 14 * a * ypow[2] + 83 * apow[2] * ypow[4]) +
+                          ypow[2] * (24 + 12 * a * ypow[2] - 4 * apow[2] * ypow[4] + 3 * apow[3] * ypow[6]) -
+                          12 * xpow[2] * (-2 + 6 * a * ypow[2] + 25 * apow[2] * ypow[4] + 27 * apow[3] * ypow[6])))) /
+              8;
+        if (higherOrder > 0) {
+          dx = (a * x *
+                (8 * (xpow[2] + 3 * ypow[2]) +
+                 4 * apow[2] * (5 * xpow[6] + 21 * xpow[4] * ypow[2] - 25 * xpow[2] * ypow[4] - ypow[6]) +
+                 apow[3] * (35 * xpow[8] + 84 * xpow[6] * ypow[2] + 498 * xpow[4] * ypow[4] - 108 * xpow[2] * ypow[6] +
+                            3 * ypow[8]) +
+                 12 * a * orc_sqr(xpow[2] - ypow[2]))) /
+               8;
+          dy = (a * y *
+                (-8 * (3 * xpow[2] + ypow[2]) +
+                 4 * apow[2] * (xpow[6] + 25 * xpow[4] * ypow[2] - 21 * xpow[2] * ypow[4] - 5 * ypow[6]) +
+                 apow[3] * (3 * xpow[8] - 108 * xpow[6] * ypow[2] + 498 * xpow[4] * ypow[4] + 84 * xpow[2] * ypow[6] +
+                            35 * ypow[8]) +
+                 12 * a * orc_sqr(xpow[2] - ypow[2]))) /
+               8;
+        }
+      } else {
+        for (int i = 1; i < 4; i++) {
+          xpow[i] = xpow[i - 1] * x;
+          ypow[i] = ypow[i - 1] * y;
+        }
+        dpx = 3 * a * (-px * xpow[2] + 2 * py * x * y - px * ypow[2]);
+        dpy = 3 * a * (py * xpow[2] - 2 * px * x * y + py * ypow[2]);
+        if (higherOrder > 0) {
+          dx = a * (xpow[3] + 3 * x * ypow[2]);
+          dy = a * (-3 * xpow[2] * y - ypow[3]);
+        }
+      }
+      ds = (a / (1 + delta)) * (3 * py * y * xpow[2] - px * xpow[3] - 3 * px * x * ypow[2] + py * ypow[3]);
+    }
+    x += nonlinearFactor * dx;
+    px += nonlinearFactor * dpx;
+    y += nonlinearFactor * dy;
+    py += nonlinearFactor * dpy;
+    if (linearFlag) {
+      vec[0] = M2[0] * x + M2[1] * px;
+      vec[1] = M2[2] * x + M2[3] * px;
+      vec[2] = M2[4] * y + M2[5] * py;
+      vec[3] = M2[6] * y + M2[7] * py;
+    } else {
+      vec[0] = x;
+      vec[1] = px;
+      vec[2] = y;
+      vec[3] = py;
+    }
+    vec[4] -= nonlinearFactor * ds;
+    px = vec[1];
+    py = vec[3];
+    denom = orc_sqr(1 + delta) - orc_sqr(px) - orc_sqr(py);
+    if (denom > 0) {
+      denom = sqrt(denom);
+      vec[1] = px / denom;
+      vec[3] = py / denom;
+    } else
+      vec[1] = vec[3] = DBL_MAX;
+  }
+}
+
 static long multipole_tracking2(double *coord, long n_part, const trk_elem *e, double Po, double z_start,
                                 const orc_maxamp *st, int *err) {
   orc_mult m;
@@ -439,6 +616,11 @@ static long multipole_tracking2(double *coord, long n_part, const trk_elem *e, d
     rotate_beam(coord, n_part, tilt);
   if (doEndDrift)
     exact_drift(coord, n_part, lEnd);
+  /* KQUAD entrance fringe (src/multipole.c:999-1006) */
+  if (e->type == TRK_KQUAD && TRK_P(e, KQUAD_EDGE1_EFFECTS) > 0)
+    quad_fringe(coord, n_part, TRK_P(e, KQUAD_K1), &TRK_P(e, KQUAD_I0M), &TRK_P(e, KQUAD_I0P), TRK_P(e, KQUAD_L) < 0,
+                -1, (int)TRK_P(e, KQUAD_EDGE1_EFFECTS), (int)TRK_P(e, KQUAD_EDGE1_LINEAR),
+                TRK_P(e, KQUAD_EDGE1_NONLINEAR_FACTOR));
 
   long i_top = n_part - 1;
   /* one dzLoss for the whole call, as in the reference (src/multipole.c:686):
@@ -455,6 +637,11 @@ static long multipole_tracking2(double *coord, long n_part, const trk_elem *e, d
       i_part--;
     }
   }
+  /* KQUAD exit fringe, on every row, lost ones included (src/multipole.c:1054-1061) */
+  if (e->type == TRK_KQUAD && TRK_P(e, KQUAD_EDGE2_EFFECTS) > 0)
+    quad_fringe(coord, n_part, TRK_P(e, KQUAD_K1), &TRK_P(e, KQUAD_I0M), &TRK_P(e, KQUAD_I0P), TRK_P(e, KQUAD_L) < 0,
+                1, (int)TRK_P(e, KQUAD_EDGE2_EFFECTS), (int)TRK_P(e, KQUAD_EDGE2_LINEAR),
+                TRK_P(e, KQUAD_EDGE2_NONLINEAR_FACTOR));
   if (doEndDrift)
     exact_drift(coord, n_part, lEnd);
   if (dx || dy || dz || tilt) {

@@ -11,6 +11,17 @@ def single(type_name, **params):
     return lat
 
 
+QUAD_FRINGE_INTEGRALS = dict(I0P=0.01, I1P=2e-5, I2P=1e-7, I3P=5e-10, LAMBDA2P=3e-7, I0M=0.012, I1M=-1.5e-5,
+                             I2M=8e-8, I3M=-4e-10, LAMBDA2M=2e-7)
+
+
+def _lossy_fringe_quad():
+    lat = Lattice()
+    lat.add("MAXAMP", "AP", X_MAX=0.0012, Y_MAX=0.001, ELLIPTICAL=1)
+    lat.add("KQUAD", "QF", L=0.5, K1=2.5, N_KICKS=8, EDGE1_EFFECTS=2, EDGE2_EFFECTS=3, **QUAD_FRINGE_INTEGRALS)
+    return lat
+
+
 ELEMENT_CASES = {
     "drif": single("DRIF", L=1.3),
     "drif_order1": single("DRIF", L=0.7, ORDER=1),
@@ -21,6 +32,14 @@ ELEMENT_CASES = {
     "kquad_misaligned": single("KQUAD", L=0.3, K1=1.2, N_KICKS=8, DX=1e-4, DY=-2e-4, DZ=1e-3, TILT=0.01),
     "kquad_kicks_fse": single("KQUAD", L=0.4, K1=0.9, N_KICKS=12, HKICK=1e-5, VKICK=-2e-5, FSE=1e-3),
     "kquad_leff": single("KQUAD", L=0.4, K1=0.9, N_KICKS=4, LEFFECTIVE=0.35),
+    "kquad_fringe_linear": single("KQUAD", L=0.3, K1=1.2, N_KICKS=8, EDGE1_EFFECTS=1, EDGE2_EFFECTS=1,
+                                  **QUAD_FRINGE_INTEGRALS),
+    "kquad_fringe_order2": single("KQUAD", L=0.3, K1=-1.4, N_KICKS=8, EDGE1_EFFECTS=2, EDGE2_EFFECTS=2,
+                                  **QUAD_FRINGE_INTEGRALS),
+    "kquad_fringe_order3": single("KQUAD", L=0.4, K1=2.0, N_KICKS=8, EDGE1_EFFECTS=3, EDGE2_EFFECTS=3,
+                                  EDGE2_LINEAR=0, EDGE1_NONLINEAR_FACTOR=0.8, LEFFECTIVE=0.35, DX=1e-4,
+                                  **QUAD_FRINGE_INTEGRALS),
+    "kquad_fringe_lossy": _lossy_fringe_quad(),
     "kquad_expand": single("KQUAD", L=0.3, K1=1.2, N_KICKS=8, EXPAND_HAMILTONIAN=1),
     "ksext": single("KSEXT", L=0.2, K2=40.0, N_KICKS=4),
     "ksext_k1j1": single("KSEXT", L=0.2, K2=-30.0, K1=0.01, J1=0.02, N_SLICES=2, TILT=0.1),
