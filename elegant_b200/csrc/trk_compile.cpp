@@ -516,10 +516,10 @@ int edge_mode(int on, int effects, int edge_order, const char *name) {
 int compile_bend(const trk_lattice *l, int idx, double Po, trk_op *op, std::vector<double> &field) {
   const trk_elem *e = &l->e[idx];
   if (TRK_P(e, CSBEND_REFERENCE_CORRECTION) || TRK_P(e, CSBEND_FSE_CORRECTION) || TRK_P(e, CSBEND_MALIGN_METHOD) ||
-      TRK_P(e, CSBEND_EXPAND_HAMILTONIAN))
+      TRK_P(e, CSBEND_EXPAND_HAMILTONIAN) || TRK_P(e, CSBEND_USE_RAD_DIST))
     return trk_set_error(TRK_ERR_UNSUPPORTED,
-                         "CSBEND %s: REFERENCE_CORRECTION, FSE_CORRECTION, MALIGN_METHOD!=0 and "
-                         "EXPAND_HAMILTONIAN are not on this path",
+                         "CSBEND %s: REFERENCE_CORRECTION, FSE_CORRECTION, MALIGN_METHOD!=0, EXPAND_HAMILTONIAN and "
+                         "USE_RAD_DIST (photon-based radiation) are not on this path",
                          e->name);
   const double L = TRK_P(e, CSBEND_L), ANGLE = TRK_P(e, CSBEND_ANGLE);
   if (ANGLE == 0) {
@@ -539,6 +539,16 @@ int compile_bend(const trk_lattice *l, int idx, double Po, trk_op *op, std::vect
     b[i] = TRK_P(e, CSBEND_USE_BN) ? e->p[P_CSBEND_B1 + i - 1] : e->p[P_CSBEND_K1 + i - 1] * rho0;
   for (int j = 0; j < 9; j++)
     c[j] = 0;
+  /* fractional field errors fn, gn at XREFERENCE (src/csbend.c:824-848) */
+  if (TRK_P(e, CSBEND_XREFERENCE) > 0) {
+    const double xr = TRK_P(e, CSBEND_XREFERENCE);
+    double term = 1 / xr;
+    for (int i = 0; i < 8; i++) {
+      b[i + 1] += e->p[P_CSBEND_F1 + i] * term;
+      c[i + 1] += e->p[P_CSBEND_G1 + i] * term;
+      term *= (i + 2) / xr;
+    }
+  }
   const double fse_ = TRK_P(e, CSBEND_FSE), fseD = TRK_P(e, CSBEND_FSE_DIPOLE), fseQ = TRK_P(e, CSBEND_FSE_QUADRUPOLE);
   b[1] *= (1 + fse_ + fseQ) / (1 + fse_ + fseD);
   c[1] *= (1 + fse_ + fseQ) / (1 + fse_ + fseD);
@@ -798,6 +808,10 @@ int compile_wake(const trk_elem *e, trk_op *op, CompiledWake &w) {
     return trk_set_error(TRK_ERR_UNSUPPORTED, "%s: SMOOTHING is not on this path", e->name);
   if (!tr && TRK_P(e, WAKE_CHANGE_P0))
     return trk_set_error(TRK_ERR_UNSUPPORTED, "WAKE %s: CHANGE_P0 is not on this path", e->name);
+  if ((tr ? TRK_P(e, TRWAKE_START_BUNCH) : TRK_P(e, WAKE_START_BUNCH)) >= 0 ||
+      (tr ? TRK_P(e, TRWAKE_END_BUNCH) : TRK_P(e, WAKE_END_BUNCH)) >= 0)
+    return trk_set_error(TRK_ERR_UNSUPPORTED, "%s: START_BUNCH/END_BUNCH (bunched-beam mode) are not on this path",
+                         e->name);
   long nbins = (long)(tr ? TRK_P(e, TRWAKE_N_BINS) : TRK_P(e, WAKE_N_BINS));
   if (nbins < 2 && nbins != 0)
     return trk_set_error(TRK_ERR_PHYSICS, "n_bins must be >=2 or else 0 (autoscale) for WAKE element %s", e->name);

@@ -44,6 +44,7 @@ static const trk_param_def defs_wake[] = {TRK_PARAMS_WAKE(TRK_DEF_ENTRY)};
 static const trk_param_def defs_trwake[] = {TRK_PARAMS_TRWAKE(TRK_DEF_ENTRY)};
 static const trk_param_def defs_maxamp[] = {TRK_PARAMS_MAXAMP(TRK_DEF_ENTRY)};
 static const trk_param_def defs_charge[] = {TRK_PARAMS_CHARGE(TRK_DEF_ENTRY)};
+static const trk_param_def defs_mark[] = {TRK_PARAMS_MARK(TRK_DEF_ENTRY)};
 #undef TRK_DEF_ENTRY
 
 typedef struct {
@@ -53,7 +54,7 @@ typedef struct {
 } trk_type_def;
 
 static const trk_type_def type_defs[TRK_N_TYPES] = {
-  {"MARK", NULL, 0},
+  {"MARK", defs_mark, P_MARK_COUNT_},
   {"DRIF", defs_drif, P_DRIF_COUNT_},
   {"EDRIFT", defs_edrift, P_EDRIFT_COUNT_},
   {"KQUAD", defs_kquad, P_KQUAD_COUNT_},

@@ -66,7 +66,19 @@
   X(KQUAD_EDGE1_LINEAR, "EDGE1_LINEAR", 1.0)       \
   X(KQUAD_EDGE2_LINEAR, "EDGE2_LINEAR", 1.0)       \
   X(KQUAD_EDGE1_NONLINEAR_FACTOR, "EDGE1_NONLINEAR_FACTOR", 1.0) \
-  X(KQUAD_EDGE2_NONLINEAR_FACTOR, "EDGE2_NONLINEAR_FACTOR", 1.0)
+  X(KQUAD_EDGE2_NONLINEAR_FACTOR, "EDGE2_NONLINEAR_FACTOR", 1.0) \
+  X(KQUAD_HSTEERING, "HSTEERING", 0.0) \
+  X(KQUAD_VSTEERING, "VSTEERING", 0.0) \
+  X(KQUAD_SYSTEMATIC_MULTIPOLE_FACTOR, "SYSTEMATIC_MULTIPOLE_FACTOR", 1.0) \
+  X(KQUAD_RANDOM_MULTIPOLE_FACTOR, "RANDOM_MULTIPOLE_FACTOR", 1.0) \
+  X(KQUAD_STEERING_MULTIPOLE_FACTOR, "STEERING_MULTIPOLE_FACTOR", 1.0) \
+  X(KQUAD_MIN_NORMAL_ORDER, "MIN_NORMAL_ORDER", -1.0) \
+  X(KQUAD_MIN_SKEW_ORDER, "MIN_SKEW_ORDER", -1.0) \
+  X(KQUAD_MAX_NORMAL_ORDER, "MAX_NORMAL_ORDER", -1.0) \
+  X(KQUAD_MAX_SKEW_ORDER, "MAX_SKEW_ORDER", -1.0) \
+  X(KQUAD_SQRT_ORDER, "SQRT_ORDER", 0.0) \
+  X(KQUAD_SR_IN_ORDINARY_MATRIX, "SR_IN_ORDINARY_MATRIX", 0.0) \
+  X(KQUAD_TRACKING_MATRIX, "TRACKING_MATRIX", 0.0)
 
 #define TRK_PARAMS_KSEXT(X)                        \
   X(KSEXT_L, "L", 0.0)                             \
@@ -93,7 +105,17 @@
   X(KSEXT_ISR, "ISR", 0.0)                         \
   X(KSEXT_ISR1PART, "ISR1PART", 1.0)               \
   X(KSEXT_EXPAND_HAMILTONIAN, "EXPAND_HAMILTONIAN", 0.0) \
-  X(KSEXT_MALIGN_METHOD, "MALIGN_METHOD", 0.0)
+  X(KSEXT_MALIGN_METHOD, "MALIGN_METHOD", 0.0) \
+  X(KSEXT_HSTEERING, "HSTEERING", 0.0) \
+  X(KSEXT_VSTEERING, "VSTEERING", 0.0) \
+  X(KSEXT_SYSTEMATIC_MULTIPOLE_FACTOR, "SYSTEMATIC_MULTIPOLE_FACTOR", 1.0) \
+  X(KSEXT_RANDOM_MULTIPOLE_FACTOR, "RANDOM_MULTIPOLE_FACTOR", 1.0) \
+  X(KSEXT_STEERING_MULTIPOLE_FACTOR, "STEERING_MULTIPOLE_FACTOR", 1.0) \
+  X(KSEXT_MIN_NORMAL_ORDER, "MIN_NORMAL_ORDER", -1.0) \
+  X(KSEXT_MIN_SKEW_ORDER, "MIN_SKEW_ORDER", -1.0) \
+  X(KSEXT_MAX_NORMAL_ORDER, "MAX_NORMAL_ORDER", -1.0) \
+  X(KSEXT_MAX_SKEW_ORDER, "MAX_SKEW_ORDER", -1.0) \
+  X(KSEXT_SQRT_ORDER, "SQRT_ORDER", 0.0)
 
 #define TRK_PARAMS_KOCT(X)                         \
   X(KOCT_L, "L", 0.0)                              \
@@ -114,7 +136,8 @@
   X(KOCT_ISR, "ISR", 0.0)                          \
   X(KOCT_ISR1PART, "ISR1PART", 1.0)                \
   X(KOCT_EXPAND_HAMILTONIAN, "EXPAND_HAMILTONIAN", 0.0) \
-  X(KOCT_MALIGN_METHOD, "MALIGN_METHOD", 0.0)
+  X(KOCT_MALIGN_METHOD, "MALIGN_METHOD", 0.0) \
+  X(KOCT_SQRT_ORDER, "SQRT_ORDER", 0.0)
 
 #define TRK_PARAMS_CSBEND(X)                       \
   X(CSBEND_L, "L", 0.0)                            \
@@ -171,7 +194,48 @@
   X(CSBEND_ISR1PART, "ISR1PART", 1.0)              \
   X(CSBEND_REFERENCE_CORRECTION, "REFERENCE_CORRECTION", 0.0) \
   X(CSBEND_FSE_CORRECTION, "FSE_CORRECTION", 0.0)  \
-  X(CSBEND_MALIGN_METHOD, "MALIGN_METHOD", 0.0)
+  X(CSBEND_MALIGN_METHOD, "MALIGN_METHOD", 0.0) \
+  X(CSBEND_FRINGE1K0, "FRINGE1K0", 0.0) \
+  X(CSBEND_FRINGE1K1, "FRINGE1K1", 0.0) \
+  X(CSBEND_FRINGE1K2, "FRINGE1K2", 0.0) \
+  X(CSBEND_FRINGE1K3, "FRINGE1K3", 0.0) \
+  X(CSBEND_FRINGE1K4, "FRINGE1K4", 0.0) \
+  X(CSBEND_FRINGE1K5, "FRINGE1K5", 0.0) \
+  X(CSBEND_FRINGE1K6, "FRINGE1K6", 0.0) \
+  X(CSBEND_FRINGE2K0, "FRINGE2K0", 0.0) \
+  X(CSBEND_FRINGE2K1, "FRINGE2K1", 0.0) \
+  X(CSBEND_FRINGE2K2, "FRINGE2K2", 0.0) \
+  X(CSBEND_FRINGE2K3, "FRINGE2K3", 0.0) \
+  X(CSBEND_FRINGE2K4, "FRINGE2K4", 0.0) \
+  X(CSBEND_FRINGE2K5, "FRINGE2K5", 0.0) \
+  X(CSBEND_FRINGE2K6, "FRINGE2K6", 0.0) \
+  X(CSBEND_EPITCH, "EPITCH", 0.0) \
+  X(CSBEND_EYAW, "EYAW", 0.0) \
+  X(CSBEND_SR_IN_ORDINARY_MATRIX, "SR_IN_ORDINARY_MATRIX", 0.0) \
+  X(CSBEND_XREFERENCE, "XREFERENCE", 0.0) \
+  X(CSBEND_F1, "F1", 0.0) \
+  X(CSBEND_F2, "F2", 0.0) \
+  X(CSBEND_F3, "F3", 0.0) \
+  X(CSBEND_F4, "F4", 0.0) \
+  X(CSBEND_F5, "F5", 0.0) \
+  X(CSBEND_F6, "F6", 0.0) \
+  X(CSBEND_F7, "F7", 0.0) \
+  X(CSBEND_F8, "F8", 0.0) \
+  X(CSBEND_G1, "G1", 0.0) \
+  X(CSBEND_G2, "G2", 0.0) \
+  X(CSBEND_G3, "G3", 0.0) \
+  X(CSBEND_G4, "G4", 0.0) \
+  X(CSBEND_G5, "G5", 0.0) \
+  X(CSBEND_G6, "G6", 0.0) \
+  X(CSBEND_G7, "G7", 0.0) \
+  X(CSBEND_G8, "G8", 0.0) \
+  X(CSBEND_SQRT_ORDER, "SQRT_ORDER", 0.0) \
+  X(CSBEND_USE_RAD_DIST, "USE_RAD_DIST", 0.0) \
+  X(CSBEND_ADD_OPENING_ANGLE, "ADD_OPENING_ANGLE", 1.0) \
+  X(CSBEND_PHOTON_LOW_ENERGY_CUTOFF, "PHOTON_LOW_ENERGY_CUTOFF", 0.0) \
+  X(CSBEND_TRACKING_MATRIX, "TRACKING_MATRIX", 0.0) \
+  X(CSBEND_XSTEERING, "XSTEERING", 0.0) \
+  X(CSBEND_YSTEERING, "YSTEERING", 0.0)
 
 #define TRK_PARAMS_RFCA(X)                         \
   X(RFCA_L, "L", 0.0)                              \
@@ -202,7 +266,11 @@
   X(WAKE_ALLOW_LONG_BEAM, "ALLOW_LONG_BEAM", 0.0)  \
   X(WAKE_RAMP_PASSES, "RAMP_PASSES", 0.0)          \
   X(WAKE_BUNCHED_BEAM_MODE, "BUNCHED_BEAM_MODE", 1.0) \
-  X(WAKE_ACAUSAL_ALLOWED, "ACAUSAL_ALLOWED", 0.0)
+  X(WAKE_ACAUSAL_ALLOWED, "ACAUSAL_ALLOWED", 0.0) \
+  X(WAKE_SG_HALFWIDTH, "SG_HALFWIDTH", 4.0) \
+  X(WAKE_SG_ORDER, "SG_ORDER", 1.0) \
+  X(WAKE_START_BUNCH, "START_BUNCH", -1.0) \
+  X(WAKE_END_BUNCH, "END_BUNCH", -1.0)
 
 #define TRK_PARAMS_TRWAKE(X)                       \
   X(TRWAKE_CHARGE, "CHARGE", 0.0)                  \
@@ -221,7 +289,11 @@
   X(TRWAKE_Y_PROBE_EXPONENT, "Y_PROBE_EXPONENT", 0.0) \
   X(TRWAKE_RAMP_PASSES, "RAMP_PASSES", 0.0)        \
   X(TRWAKE_BUNCHED_BEAM_MODE, "BUNCHED_BEAM_MODE", 1.0) \
-  X(TRWAKE_ACAUSAL_ALLOWED, "ACAUSAL_ALLOWED", 0.0)
+  X(TRWAKE_ACAUSAL_ALLOWED, "ACAUSAL_ALLOWED", 0.0) \
+  X(TRWAKE_SG_HALFWIDTH, "SG_HALFWIDTH", 4.0) \
+  X(TRWAKE_SG_ORDER, "SG_ORDER", 1.0) \
+  X(TRWAKE_START_BUNCH, "START_BUNCH", -1.0) \
+  X(TRWAKE_END_BUNCH, "END_BUNCH", -1.0)
 
 #define TRK_PARAMS_MAXAMP(X)                       \
   X(MAXAMP_X_MAX, "X_MAX", 0.0)                    \
@@ -234,9 +306,15 @@
   X(CHARGE_TOTAL, "TOTAL", 0.0)                    \
   X(CHARGE_PER_PARTICLE, "PER_PARTICLE", 0.0)
 
-#define TRK_PARAMS_MARK(X)
+#define TRK_PARAMS_MARK(X)                         \
+  X(MARK_DX, "DX", 0.0)                            \
+  X(MARK_DY, "DY", 0.0)                            \
+  X(MARK_FITPOINT, "FITPOINT", 0.0)
 
 #define TRK_ENUM_ENTRY(e, n, d) P_##e,
+enum {
+  TRK_PARAMS_MARK(TRK_ENUM_ENTRY) P_MARK_COUNT_
+};
 enum {
   TRK_PARAMS_DRIF(TRK_ENUM_ENTRY) P_DRIF_COUNT_
 };

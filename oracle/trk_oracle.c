@@ -789,7 +789,7 @@ static int csbend_setup(const trk_lattice *l, int idx, double Po, orc_csbend_set
   double b[9], c[9];
   memset(S, 0, sizeof(*S));
   if (TRK_P(e, CSBEND_REFERENCE_CORRECTION) || TRK_P(e, CSBEND_FSE_CORRECTION) || TRK_P(e, CSBEND_MALIGN_METHOD) ||
-      TRK_P(e, CSBEND_EXPAND_HAMILTONIAN))
+      TRK_P(e, CSBEND_EXPAND_HAMILTONIAN) || TRK_P(e, CSBEND_USE_RAD_DIST))
     return 1;
   if (TRK_P(e, CSBEND_ANGLE) == 0) {
     S->is_drift = 1;
@@ -810,6 +810,16 @@ static int csbend_setup(const trk_lattice *l, int idx, double Po, orc_csbend_set
   }
   for (int j = 0; j < 9; j++)
     c[j] = 0;
+  /* fractional field errors fn, gn at XREFERENCE (src/csbend.c:824-848) */
+  if (TRK_P(e, CSBEND_XREFERENCE) > 0) {
+    const double xr = TRK_P(e, CSBEND_XREFERENCE);
+    double term = 1 / xr;
+    for (int i = 0; i < 8; i++) {
+      b[i + 1] += e->p[P_CSBEND_F1 + i] * term;
+      c[i + 1] += e->p[P_CSBEND_G1 + i] * term;
+      term *= (i + 2) / xr;
+    }
+  }
   double fse_ = TRK_P(e, CSBEND_FSE), fseD = TRK_P(e, CSBEND_FSE_DIPOLE), fseQ = TRK_P(e, CSBEND_FSE_QUADRUPOLE);
   b[1] *= (1 + fse_ + fseQ) / (1 + fse_ + fseD);
   c[1] *= (1 + fse_ + fseQ) / (1 + fse_ + fseD);

@@ -62,6 +62,11 @@ ELEMENT_CASES = {
                                     H2=-0.2, EDGE1_EFFECTS=4, EDGE2_EFFECTS=4, N_SLICES=8),
     "csbend_hwang_negative": single("CSBEND", L=1.0, ANGLE=-0.06, E1=0.02, E2=0.05, HGAP=0.02, FINT=0.6,
                                     EDGE1_EFFECTS=4, EDGE2_EFFECTS=2, N_SLICES=8),
+    "csbend_xreference": single("CSBEND", L=1.0, ANGLE=0.06, XREFERENCE=0.02, F1=1e-3, F2=-2e-3, F3=5e-4, G1=4e-4,
+                                G2=-1e-4, N_SLICES=8, EPITCH=1e-3, EYAW=-2e-3, XSTEERING=1, SQRT_ORDER=2,
+                                FRINGE1K0=0.1, TRACKING_MATRIX=2),
+    "kquad_inert_params": single("KQUAD", L=0.3, K1=1.2, N_KICKS=8, HSTEERING=1, VSTEERING=1, SQRT_ORDER=1,
+                                 SYSTEMATIC_MULTIPOLE_FACTOR=2, MIN_NORMAL_ORDER=2, TRACKING_MATRIX=3),
     "csbend_misaligned": single("CSBEND", L=1.0, ANGLE=0.05, DX=1e-4, DY=2e-4, DZ=-1e-4, TILT=0.02, N_SLICES=8),
     "csbend_order6": single("CSBEND", L=1.0, ANGLE=0.05, N_SLICES=4, INTEGRATION_ORDER=6),
     "kquad_rad": single("KQUAD", L=0.3, K1=1.2, N_KICKS=8, SYNCH_RAD=1),
