@@ -243,6 +243,7 @@ class _NativeLattice:
                                                          _dptr(Wy) if Wy is not None else None, len(tt)))
         except Exception:
             lib.trk_lattice_destroy(self.ptr)
+            self.ptr = ctypes.c_void_p()  # destroyed: close() and __del__ must not free it again
             raise
 
     def close(self):

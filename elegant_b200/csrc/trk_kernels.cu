@@ -2832,8 +2832,15 @@ __device__ double adj_mult1(const trk_op *__restrict__ op, const double *__restr
 }
 
 /* adjoint of op_dipole_fast (bend_dipole_fast / dipole_slice) */
+/* The adjoint of the pure-dipole body; with dk (the bend's field
+ * derivative tables, dF/dK1 at dk and dF/dK2 at dk + 242) it also returns
+ * the sensitivities to the bend's K1 and K2 at K1 = K2 = 0: each kick
+ * QX -= w Fy, QY += w Fx changes by -w dFy, +w dFx per unit K, weighted by
+ * the adjoints of QX and QY after the kick (QY's running adjoint collects
+ * the later drifts' shares as the sweep goes back). */
 __device__ void adj_dipole(const trk_op *__restrict__ op, double x, double xp, double y, double yp, double dp,
-                           double &lx, double &lxp, double &ly, double &lyp, double &ldp) {
+                           double &lx, double &lxp, double &ly, double &lyp, double &ldp,
+                           const double *__restrict__ dk = nullptr, double *sk = nullptr) {
   const double *d = op->d;
   const int nSlices = __ldg(&op->i[0]);
   const double rho0 = __ldg(&d[BD_RHO0]);
@@ -2842,12 +2849,13 @@ __device__ void adj_dipole(const trk_op *__restrict__ op, double x, double xp, d
   const double QY = yp * opd * rs;
   const double f2 = opd * opd - QY * QY;
   double X = x, Q = xp * opd * rs, F = 0;
-  double SX[TRK_ADJ_MAX_STEPS], SQ[TRK_ADJ_MAX_STEPS];
+  double SX[TRK_ADJ_MAX_STEPS], SQ[TRK_ADJ_MAX_STEPS], SF[TRK_ADJ_MAX_STEPS];
   int m = 0;
   for (int i = 0; i < nSlices; i++)
     for (int j = 0; j < 4; j++) {
       SX[m] = X;
       SQ[m] = Q;
+      SF[m] = F;
       m++;
       const double sa = __ldg(&d[BD_SA + j]), ca = __ldg(&d[BD_CA + j]), omc = __ldg(&d[BD_OMC + j]);
       const double fc = sqrt_nan(fma(-Q, Q, f2));
@@ -2859,9 +2867,9 @@ __device__ void adj_dipole(const trk_op *__restrict__ op, double x, double xp, d
       if (j < 3)
         Q = fma(-__ldg(&d[BD_C2 + j]), X, Q - __ldg(&d[BD_C1 + j]));
     }
+  const int nsteps = m;
   /* exit: x = X, y = y0 + QY F, (xp, yp) = (Q, QY) / sqrt(opd^2 - Q^2 - QY^2) */
   double lX = lx, lQ = 0, lQY = 0, lopd = 0, lF = QY * ly, lf2 = 0;
-  lQY += F * ly;
   {
     const double g = rsqrt_fast(opd * opd - Q * Q - QY * QY);
     const double g3 = g * g * g;
@@ -2869,10 +2877,23 @@ __device__ void adj_dipole(const trk_op *__restrict__ op, double x, double xp, d
     lQY += lyp * (g + QY * QY * g3) + lxp * Q * QY * g3;
     lopd -= (lxp * Q + lyp * QY) * opd * g3;
   }
+  double sk1 = 0, sk2 = 0;
   for (int i = nSlices - 1; i >= 0; i--)
     for (int j = 3; j >= 0; j--) {
-      if (j < 3)
-        lX -= __ldg(&d[BD_C2 + j]) * lQ;
+      if (j < 3) {
+        const double c2 = __ldg(&d[BD_C2 + j]);
+        if (dk) {
+          /* the kick at the end of drift j: position X1, Y1 = y + QY F1 */
+          const double X1 = m < nsteps ? SX[m] : X, Y1 = fma(QY, m < nsteps ? SF[m] : F, y);
+          const double w = fma(c2, X1, __ldg(&d[BD_C1 + j]));
+          double dFx, dFy;
+          cf_fields(dk, dk + 121, X1, Y1, dFx, dFy);
+          sk1 += w * (lQY * dFx - lQ * dFy);
+          cf_fields(dk + 242, dk + 363, X1, Y1, dFx, dFy);
+          sk2 += w * (lQY * dFx - lQ * dFy);
+        }
+        lX -= c2 * lQ;
+      }
       m--;
       const double Xs = SX[m], Qs = SQ[m];
       const double sa = __ldg(&d[BD_SA + j]), ca = __ldg(&d[BD_CA + j]), omc = __ldg(&d[BD_OMC + j]);
@@ -2892,12 +2913,17 @@ __device__ void adj_dipole(const trk_op *__restrict__ op, double x, double xp, d
       lQs += sa * lsaq;
       const double lu2 = lfc / (2 * fc);
       lf2 += lu2;
+      /* this drift's share of QY's adjoint: Y grows by QY u sa, f2 holds -QY^2 */
+      lQY += ly * u * sa - 2 * QY * lu2;
       lQs -= 2 * Qs * lu2;
       lX = lXs;
       lQ = lQs;
     }
   lopd += 2 * opd * lf2;
-  lQY -= 2 * QY * lf2;
+  if (sk) {
+    sk[0] = sk1;
+    sk[1] = sk2;
+  }
   /* entry: X = x, (Q, QY) = opd (xp, yp) / sqrt(1 + xp^2 + yp^2) */
   const double rs3 = rs * rs * rs;
   lx = lX;

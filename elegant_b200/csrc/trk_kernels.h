@@ -119,6 +119,8 @@ struct AdjArgs {
   double *grad;          /* gradient accumulators, one per parameter */
   const int *op_param;   /* parameter index of each op, -1 if none */
   const double *op_dk;   /* per variant and op: d(kick strength)/d(parameter) of kick steps 0..2 */
+  const int *op_dfield;  /* per op: offset in dfield of a CSBEND's field derivatives (-1 none) */
+  const double *dfield;  /* d(Fx, Fy)/dK1 and d(Fx, Fy)/dK2 tables, 4 x 121 doubles per CSBEND op */
   int n_ops;             /* ops per variant */
   int n_params;          /* parameters per variant (grad holds n_variants x n_params) */
 };
