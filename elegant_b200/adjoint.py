@@ -1,8 +1,8 @@
 """Gradients of tracked-beam objectives through the C ABI's reverse-mode
 adjoint (trk_adjoint), with a torch.autograd.Function wrapper.
 
-The parameters are the K1 of every KQUAD and the K2 of every KSEXT of a
-lattice, in lattice order; the objective is
+The parameters are, in lattice order, the K1 of every KQUAD, the K2 of every
+KSEXT and the K1 and K2 of every CSBEND; the objective is
     mean(x^2 + y^2) + w (mean(x)^2 + mean(y)^2)
 over the particles that survive n_passes passes.
 """
@@ -10,25 +10,36 @@ import numpy as np
 
 from . import Tracker
 
-PARAM_NAME = {"KQUAD": "K1", "KSEXT": "K2"}
+PARAM_NAMES = {"KQUAD": ("K1",), "KSEXT": ("K2",), "CSBEND": ("K1", "K2")}
+# finite-difference step scale of each name where the value itself is zero
+PARAM_SCALE = {"K1": 1.0, "K2": 10.0}
+
+
+def parameter_list(lattice):
+    """(element index, parameter name) of every gradient entry, in order."""
+    return [(i, n) for i, (t, _, _, _) in enumerate(lattice.elements) for n in PARAM_NAMES.get(t, ())]
 
 
 def parameter_elements(lattice):
-    """Element indices of the gradient parameters, in gradient order."""
-    return [i for i, (t, _, _, _) in enumerate(lattice.elements) if t in PARAM_NAME]
+    """Element index of every gradient entry (a CSBEND appears twice)."""
+    return [i for i, _ in parameter_list(lattice)]
 
 
 def get_parameters(lattice):
-    return np.array([lattice.elements[i][2].get(PARAM_NAME[lattice.elements[i][0]], 0.0)
-                     for i in parameter_elements(lattice)])
+    return np.array([lattice.elements[i][2].get(n, 0.0) for i, n in parameter_list(lattice)])
 
 
 def set_parameters(lattice, values):
-    idx = parameter_elements(lattice)
-    if len(idx) != len(values):
-        raise ValueError(f"{len(values)} values for {len(idx)} parameters")
-    for i, v in zip(idx, values):
-        lattice.elements[i][2][PARAM_NAME[lattice.elements[i][0]]] = float(v)
+    plist = parameter_list(lattice)
+    if len(plist) != len(values):
+        raise ValueError(f"{len(values)} values for {len(plist)} parameters")
+    for (i, n), v in zip(plist, values):
+        lattice.elements[i][2][n] = float(v)
+
+
+def fd_step(name, value, rel=1e-7):
+    """Central-difference step: rel x |value|, or rel x the name's scale for a zero value."""
+    return rel * (abs(value) if value != 0 else PARAM_SCALE.get(name, 1.0))
 
 
 def loss_and_grad(tracker, lattice, beam, n_passes, p_central, centroid_weight=0.0):

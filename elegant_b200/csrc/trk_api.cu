@@ -94,6 +94,9 @@ struct trk_context {
   double *d_adj_ck = nullptr, *d_adj_entry = nullptr, *d_adj_lam = nullptr, *d_adj_grad = nullptr;
   double *d_adj_dk = nullptr, *d_adj_mom = nullptr;
   int *d_adj_param = nullptr;
+  int *d_adj_dfo = nullptr;        /* per op: offset of a CSBEND's field derivative tables */
+  double *d_adj_dfield = nullptr;  /* the tables */
+  size_t adj_dfo_cap = 0, adj_dfield_cap = 0;
   size_t adj_ck_cap = 0, adj_entry_cap = 0, adj_lam_cap = 0, adj_grad_cap = 0, adj_dk_cap = 0, adj_mom_cap = 0,
          adj_param_cap = 0;
   size_t matrix_cap = 0;
@@ -805,6 +808,8 @@ void trk_context_destroy(trk_context *ctx) {
   cudaFree(ctx->d_adj_dk);
   cudaFree(ctx->d_adj_mom);
   cudaFree(ctx->d_adj_param);
+  cudaFree(ctx->d_adj_dfo);
+  cudaFree(ctx->d_adj_dfield);
   cudaFree(ctx->d_live);
   cudaFree(ctx->d_live_n);
   cudaFree(ctx->d_live_idx);
@@ -1839,6 +1844,38 @@ static int param_derivative(const trk_elem *e, double Po, double *dk3) {
   return TRK_OK;
 }
 
+/* d(Fx, Fy)/dK1 and d(Fx, Fy)/dK2 of a CSBEND's field expansion, as 4 x 121
+ * doubles (Fx, Fy per unit K1, then per unit K2).  The expansion is linear
+ * in b[] (trk_csbend_field_table), and b1 = K1 (L/ANGLE) (1+FSE+FSE_Q)/
+ * (1+FSE+FSE_D), b2 = K2 (L/ANGLE) (1+FSE)/(1+FSE+FSE_D), odd b's flipped
+ * for ANGLE < 0 (compile_bend): the tables are the expansion of those unit
+ * b's without the constant dipole and steering terms, to the order the
+ * element's own expansion takes. */
+static int csbend_field_derivatives(const trk_elem *e, double *out) {
+  const double L = TRK_P(e, CSBEND_L), ANGLE = TRK_P(e, CSBEND_ANGLE);
+  const double fse = TRK_P(e, CSBEND_FSE), fseD = TRK_P(e, CSBEND_FSE_DIPOLE), fseQ = TRK_P(e, CSBEND_FSE_QUADRUPOLE);
+  const double rho = std::fabs(L / ANGLE);
+  for (int q = 0; q < 2; q++) {
+    double b[9] = {0}, c[9] = {0};
+    if (q == 0)
+      b[1] = (L / ANGLE) * ((1 + fse + fseQ) / (1 + fse + fseD)) * (ANGLE < 0 ? -1 : 1);
+    else
+      b[2] = (L / ANGLE) * ((1 + fse) / (1 + fse + fseD));
+    long order = (long)TRK_P(e, CSBEND_EXPANSION_ORDER);
+    if (order == 0)
+      order = 4; /* the automatic order with K1 and/or K2 (i + 2 < 4 for i <= 2) */
+    if (order != 4)
+      return trk_set_error(TRK_ERR_UNSUPPORTED, "CSBEND gradients need EXPANSION_ORDER 0 or 4");
+    int eo1, hn, hs;
+    double *Fx = out + 242 * q, *Fy = Fx + 121;
+    if (trk_csbend_field_table(b, c, 1 / rho, (int)TRK_P(e, CSBEND_NONLINEAR), order, Fx, Fy, &eo1, &hn, &hs))
+      return trk_set_error(TRK_ERR_UNSUPPORTED, "CSBEND expansion order too high");
+    Fx[0] = 0;
+    Fy[0] = 0;
+  }
+  return TRK_OK;
+}
+
 /* The adjoint run of one lattice (offsets = null: lattices[0]) or of an
  * ensemble of nv lattices over the variant offsets. */
 static int adjoint_run(trk_context *ctx, const trk_lattice *const *lattices, int nv, const long *offsets,
@@ -1871,9 +1908,17 @@ static int adjoint_run(trk_context *ctx, const trk_lattice *const *lattices, int
   std::vector<int> op_param(std::max(nops, 1), -1);
   std::vector<double> op_dk(3 * (size_t)nv * std::max(nops, 1), 0.0);
   std::vector<int> param_of_elem(lattice->n, -1);
-  for (int i = 0, k = 0; i < lattice->n; i++)
-    if (lattice->e[i].type == TRK_KQUAD || lattice->e[i].type == TRK_KSEXT)
+  for (int i = 0, k = 0; i < lattice->n; i++) {
+    const int t = lattice->e[i].type;
+    if (t == TRK_KQUAD || t == TRK_KSEXT)
       param_of_elem[i] = k++;
+    else if (t == TRK_CSBEND) { /* K1 at k, K2 at k + 1 */
+      param_of_elem[i] = k;
+      k += 2;
+    }
+  }
+  std::vector<int> op_dfield(std::max(nops, 1), -1);
+  std::vector<double> dfield;
   for (int k = 0; k < nops; k++) {
     const trk_op &op = c.ops[k];
     switch (op.kind) {
@@ -1897,7 +1942,27 @@ static int adjoint_run(trk_context *ctx, const trk_lattice *const *lattices, int
                            "expansion, no misalignment or edge kick)", op.elem);
     }
     const int pe = (op.elem >= 0 && op.elem < lattice->n) ? param_of_elem[op.elem] : -1;
-    if (pe >= 0) {
+    if (pe >= 0 && lattice->e[op.elem].type == TRK_CSBEND) {
+      /* K1 and K2 of a bend: the kicks' field derivatives (a zero-angle
+       * CSBEND is a drift, and USE_BN ignores K: zero gradient) */
+      if (op.kind != OPK_DIPOLE && op.kind != OPK_CFBEND)
+        continue;
+      const trk_elem *e0 = &lattices[0]->e[op.elem];
+      if (TRK_P(e0, CSBEND_USE_BN))
+        continue;
+      static const int same[] = {P_CSBEND_L, P_CSBEND_ANGLE, P_CSBEND_FSE, P_CSBEND_FSE_DIPOLE,
+                                 P_CSBEND_FSE_QUADRUPOLE, P_CSBEND_NONLINEAR, P_CSBEND_EXPANSION_ORDER};
+      for (int v = 1; v < nv; v++)
+        for (int q : same)
+          if (lattices[v]->e[op.elem].p[q] != e0->p[q])
+            return trk_set_error(TRK_ERR_UNSUPPORTED, "element %d: CSBEND gradients need the variants to share "
+                                 "L, ANGLE, FSE* and the expansion settings", op.elem);
+      op_param[k] = pe;
+      op_dfield[k] = (int)dfield.size();
+      dfield.resize(dfield.size() + 4 * 121);
+      if ((rc = csbend_field_derivatives(e0, dfield.data() + op_dfield[k])))
+        return rc;
+    } else if (pe >= 0) {
       if (op.kind != OPK_MULT1)
         return trk_set_error(TRK_ERR_UNSUPPORTED, "element %d: gradients need a single-order multipole", op.elem);
       op_param[k] = pe;
@@ -1913,8 +1978,15 @@ static int adjoint_run(trk_context *ctx, const trk_lattice *const *lattices, int
       (rc = ensure(&ctx->d_adj_lam, ctx->adj_lam_cap, (size_t)5 * np)) ||
       (rc = ensure(&ctx->d_adj_grad, ctx->adj_grad_cap, std::max<size_t>(n_grad_all, 1))) ||
       (rc = ensure(&ctx->d_adj_param, ctx->adj_param_cap, op_param.size())) ||
-      (rc = ensure(&ctx->d_adj_dk, ctx->adj_dk_cap, op_dk.size())))
+      (rc = ensure(&ctx->d_adj_dk, ctx->adj_dk_cap, op_dk.size())) ||
+      (rc = ensure(&ctx->d_adj_dfo, ctx->adj_dfo_cap, op_dfield.size())) ||
+      (rc = ensure(&ctx->d_adj_dfield, ctx->adj_dfield_cap, std::max<size_t>(dfield.size(), 1))))
     return rc;
+  CUDA_TRY(cudaMemcpyAsync(ctx->d_adj_dfo, op_dfield.data(), sizeof(int) * op_dfield.size(), cudaMemcpyHostToDevice,
+                           ctx->stream));
+  if (!dfield.empty())
+    CUDA_TRY(cudaMemcpyAsync(ctx->d_adj_dfield, dfield.data(), sizeof(double) * dfield.size(),
+                             cudaMemcpyHostToDevice, ctx->stream));
   CUDA_TRY(cudaMemcpyAsync(ctx->d_adj_param, op_param.data(), sizeof(int) * op_param.size(), cudaMemcpyHostToDevice,
                            ctx->stream));
   CUDA_TRY(cudaMemcpyAsync(ctx->d_adj_dk, op_dk.data(), sizeof(double) * op_dk.size(), cudaMemcpyHostToDevice,
@@ -1980,6 +2052,8 @@ static int adjoint_run(trk_context *ctx, const trk_lattice *const *lattices, int
   g.grad = ctx->d_adj_grad;
   g.op_param = ctx->d_adj_param;
   g.op_dk = ctx->d_adj_dk;
+  g.op_dfield = ctx->d_adj_dfo;
+  g.dfield = ctx->d_adj_dfield;
   g.n_ops = nops;
   g.n_params = n_params;
   if (ensemble) {
@@ -2016,9 +2090,12 @@ int trk_adjoint_param_count(const trk_lattice *lattice) {
   if (!lattice)
     return trk_set_error(TRK_ERR_ARG, "null lattice");
   int n = 0;
-  for (int i = 0; i < lattice->n; i++)
+  for (int i = 0; i < lattice->n; i++) {
     if (lattice->e[i].type == TRK_KQUAD || lattice->e[i].type == TRK_KSEXT)
       n++;
+    else if (lattice->e[i].type == TRK_CSBEND)
+      n += 2;
+  }
   return n;
 }
 

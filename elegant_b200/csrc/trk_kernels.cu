@@ -2973,7 +2973,7 @@ __device__ __forceinline__ void cf_drift(const double *__restrict__ d, int j, do
  * while the slices are reversed */
 __device__ void adj_cfbend(const trk_op *__restrict__ op, const double *__restrict__ field, double x, double xp,
                            double y, double yp, double dp, double &lx, double &lxp, double &ly, double &lyp,
-                           double &ldp) {
+                           double &ldp, const double *__restrict__ dk = nullptr, double *sk = nullptr) {
   const double *d = op->d;
   const double *fx = field + __ldg(&op->i[4]);
   const double *fy = fx + 121;
@@ -3001,7 +3001,7 @@ __device__ void adj_cfbend(const trk_op *__restrict__ op, const double *__restri
     }
   }
   /* exit: x = X, y = Y, (xp, yp) = (QX, QY) / sqrt(opd^2 - QX^2 - QY^2) */
-  double lX = lx, lY = ly, lQX = 0, lQY = 0, lopd = 0;
+  double lX = lx, lY = ly, lQX = 0, lQY = 0, lopd = 0, sk1 = 0, sk2 = 0;
   adj_m2s(QX, QY, opd, lxp, lyp, lQX, lQY, lopd);
   for (int i = nSlices - 1; i >= 0; i--) {
     /* substep entry states of slice i (and the kick positions) */
@@ -3040,6 +3040,13 @@ __device__ void adj_cfbend(const trk_op *__restrict__ op, const double *__restri
         const double lw = fma(-lQX, Fy, lQY * Fx);
         lX += lw * c2 + w * fma(-lQX, Fyx, lQY * Fxx);
         lY += w * fma(-lQX, Fyy, lQY * Fxy);
+        if (dk) { /* d(kick)/dK1, d(kick)/dK2 with the adjoints after the kick */
+          double dFx, dFy;
+          cf_fields(dk, dk + 121, X1, Y1, dFx, dFy);
+          sk1 += w * (lQY * dFx - lQX * dFy);
+          cf_fields(dk + 242, dk + 363, X1, Y1, dFx, dFy);
+          sk2 += w * (lQY * dFx - lQX * dFy);
+        }
       }
       /* drift from (Xs, QXs, Ys, QYs): X' = Xs + u (omc fc + sa QXs),
        * QX' = sa fc + ca QXs, Y' = Ys + QYs u sa, with
@@ -3068,6 +3075,10 @@ __device__ void adj_cfbend(const trk_op *__restrict__ op, const double *__restri
       lX = lXs;
       lQX = lQXs;
     }
+  }
+  if (sk) {
+    sk[0] = sk1;
+    sk[1] = sk2;
   }
   /* entry: X = x, Y = y, (QX, QY) = opd (xp, yp) / sqrt(1 + xp^2 + yp^2) */
   lx = lX;
@@ -3157,7 +3168,11 @@ __global__ void __launch_bounds__(128) adj_reverse_kernel(TrackArgs a, AdjArgs g
       y = e[2 * n + i];
       yp = e[3 * n + i];
     }
-    double sens = 0;
+    double sens = 0, sk[2] = {0, 0};
+    const int prm = __ldg(&g.op_param[k]);
+    const int dfo = g.op_dfield ? __ldg(&g.op_dfield[k]) : -1;
+    const double *dk = (prm >= 0 && dfo >= 0) ? g.dfield + dfo : nullptr;
+    bool two = false;
     switch (__ldg(&op->kind)) {
     case OPK_DRIFT:
     case OPK_EDRIFT:
@@ -3171,25 +3186,30 @@ __global__ void __launch_bounds__(128) adj_reverse_kernel(TrackArgs a, AdjArgs g
       sens = adj_mult1(op, g.op_dk + 3 * ((long)v * g.n_ops + k), x, xp, y, yp, dp, lx, lxp, ly, lyp, ldp);
       break;
     case OPK_DIPOLE:
-      adj_dipole(op, x, xp, y, yp, dp, lx, lxp, ly, lyp, ldp);
+      adj_dipole(op, x, xp, y, yp, dp, lx, lxp, ly, lyp, ldp, dk, sk);
+      two = dk != nullptr;
       break;
     case OPK_CFBEND:
-      adj_cfbend(op, a.field, x, xp, y, yp, dp, lx, lxp, ly, lyp, ldp);
+      adj_cfbend(op, a.field, x, xp, y, yp, dp, lx, lxp, ly, lyp, ldp, dk, sk);
+      two = dk != nullptr;
       break;
     default:
       break;
     }
-    const int prm = __ldg(&g.op_param[k]);
     if (prm >= 0) {
-      if (!act)
-        sens = 0;
-      if (warp_uniform) {
-        for (int off = 16; off > 0; off >>= 1)
-          sens += __shfl_xor_sync(0xffffffffu, sens, off);
-        if ((threadIdx.x & 31) == 0 && sens != 0)
-          atomicAdd(&g.grad[(long)v * g.n_params + prm], sens);
-      } else if (sens != 0) {
-        atomicAdd(&g.grad[(long)v * g.n_params + prm], sens);
+      /* one parameter (multipole K) or two (CSBEND K1, K2 at prm, prm + 1) */
+      for (int q = 0; q < (two ? 2 : 1); q++) {
+        double sv = two ? sk[q] : sens;
+        if (!act)
+          sv = 0;
+        if (warp_uniform) {
+          for (int off = 16; off > 0; off >>= 1)
+            sv += __shfl_xor_sync(0xffffffffu, sv, off);
+          if ((threadIdx.x & 31) == 0 && sv != 0)
+            atomicAdd(&g.grad[(long)v * g.n_params + prm + q], sv);
+        } else if (sv != 0) {
+          atomicAdd(&g.grad[(long)v * g.n_params + prm + q], sv);
+        }
       }
     }
   }

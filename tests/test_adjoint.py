@@ -1,13 +1,14 @@
 """Reverse-mode gradients (trk_adjoint) of the tracked-beam objective
-mean(x^2+y^2) + w (mean(x)^2 + mean(y)^2) with respect to every KQUAD K1 and
-KSEXT K2, against central finite differences (h = 1e-7 relative) of the GPU
-tracking and of elegant's own compiled tracking code; relative gradient
-error <= 1e-6."""
+mean(x^2+y^2) + w (mean(x)^2 + mean(y)^2) with respect to every KQUAD K1,
+KSEXT K2 and CSBEND K1 and K2, against central finite differences (h = 1e-7
+relative; 1e-7 m^-2 and 1e-6 m^-3 absolute for a bend's zero K1 and K2) of
+the GPU tracking and of elegant's own compiled tracking code; relative
+gradient error <= 1e-6."""
 import numpy as np
 import pytest
 
 from elegant_b200 import Tracker, configs
-from elegant_b200.adjoint import get_parameters, make_autograd, set_parameters
+from elegant_b200.adjoint import fd_step, get_parameters, make_autograd, parameter_list, set_parameters
 from oracle import pyoracle
 
 pytestmark = pytest.mark.gpu
@@ -38,27 +39,16 @@ def _rel_err(g, ref):
 
 def test_adjoint_matches_gpu_finite_differences():
     lat, beam, passes = _lattice(), _beam(), 6
-    k0 = get_parameters(lat)
     with Tracker(0) as trk:
         trk.load(beam)
         loss, grad = trk.adjoint(lat, passes, PC, W)
         trk.load(beam)
         trk.track(lat, passes, PC)
         assert abs(trk.objective(W) - loss) <= 1e-14 * abs(loss)
-        fd = np.zeros_like(k0)
-        for p in range(len(k0)):
-            h = 1e-7 * abs(k0[p])
-            vals = []
-            for sgn in (1, -1):
-                k = k0.copy()
-                k[p] += sgn * h
-                set_parameters(lat, k)
-                trk.load(beam)
-                trk.track(lat, passes, PC)
-                vals.append(trk.objective(W))
-            fd[p] = (vals[0] - vals[1]) / (2 * h)
-        set_parameters(lat, k0)
-    assert len(grad) == 8 and np.all(np.isfinite(grad))
+        fd = _gpu_fd(trk, lat, beam, passes, W)
+    # 4 KQUAD K1, 4 KSEXT K2, 4 CSBEND (K1, K2)
+    names = [n for _, n in parameter_list(lat)]
+    assert len(grad) == 16 and names.count("K1") == 8 and np.all(np.isfinite(grad))
     assert _rel_err(grad, fd) < 1e-6, (grad, fd)
 
 
@@ -72,11 +62,13 @@ def test_adjoint_matches_reference_code_finite_differences():
     (the GPU formulation has no such cancellation and takes h = 1e-7)."""
     lat, beam, passes = _lattice(cells=1), _beam(n=300, seed=92), 4
     k0 = get_parameters(lat)
+    plist = parameter_list(lat)
+    bend = [i for i, (e, _) in enumerate(plist) if lat.elements[e][0] == "CSBEND"]
     with Tracker(0) as trk:
         trk.load(beam)
         _, grad = trk.adjoint(lat, passes, PC, W)
-    for p in (0, 1, 2):
-        h = 1e-5 * abs(k0[p])
+    for p in (0, 1, bend[0], bend[1]):
+        h = fd_step(plist[p][1], k0[p], rel=1e-5)
         vals = []
         for sgn in (1, -1):
             k = k0.copy()
@@ -123,9 +115,10 @@ def test_losses_are_left_out_and_elements_checked():
 
 def _gpu_fd(trk, lat, beam, passes, w, params=None, rel=1e-7):
     k0 = get_parameters(lat)
+    names = [n for _, n in parameter_list(lat)]
     fd = np.zeros_like(k0)
     for p in (range(len(k0)) if params is None else params):
-        h = rel * abs(k0[p])
+        h = fd_step(names[p], k0[p], rel)
         vals = []
         for sgn in (1, -1):
             k = k0.copy()
@@ -145,8 +138,8 @@ def _mba(cells=1, **kw):
 
 def test_adjoint_through_combined_function_bends():
     """The MBA cell: combined-function CSBENDs (K1 field expansion), strong
-    quadrupoles, sextupoles and octupoles; gradient w.r.t. its 12 K1 and 6
-    K2 against GPU central differences."""
+    quadrupoles, sextupoles and octupoles; gradient w.r.t. its 12 KQUAD K1,
+    6 KSEXT K2 and 7 CSBEND (K1, K2) against GPU central differences."""
     lat, passes = _mba(), 6
     beam = configs.c5_beam(3000, seed=93)
     beam[:, 0] += 5e-5
@@ -157,7 +150,7 @@ def test_adjoint_through_combined_function_bends():
         trk.track(lat, passes, PC)
         assert abs(trk.objective(W) - loss) <= 1e-14 * abs(loss)
         fd = _gpu_fd(trk, lat, beam, passes, W)
-    assert len(grad) == 18 and np.all(np.isfinite(grad))
+    assert len(grad) == 32 and np.all(np.isfinite(grad))
     assert np.linalg.norm(grad - fd) / np.linalg.norm(fd) < 1e-6, (grad, fd)
     assert _rel_err(grad, fd) < 1e-5, (grad, fd)
 
@@ -186,7 +179,7 @@ def test_adjoint_ensemble_equals_separate_adjoints():
             loss, grad = trk.adjoint(lat, passes, PC, W)
             assert abs(losses[v] - loss) <= 1e-13 * abs(loss), (v, losses[v], loss)
             assert np.max(np.abs(grads[v] - grad)) <= 1e-10 * np.max(np.abs(grad)), v
-    assert grads.shape == (4, 18)
+    assert grads.shape == (4, 32)
     assert np.max(np.abs(grads[0] - grads[1])) > 0  # the variants differ
 
 
