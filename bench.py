@@ -646,9 +646,9 @@ def run_observe(args, rank):
     """Beam observers on the device beam: trk_accumulate_beam_sums (centroids,
     7x7 second moments, extremes; elegant's accumulate_beam_sums) on 1e7
     particles of the MBA ring's beam.  HBM-bound: two passes over x, x', y,
-    y', s, delta, id and the loss word, 60 B per particle each.  Metric:
-    particles summed per second; roofline in GB/s against the measured HBM
-    copy bandwidth."""
+    y', s, delta and the loss word (the ID column only with an ID window),
+    52 B per particle each.  Metric: particles summed per second; roofline in
+    GB/s against the measured HBM copy bandwidth."""
     import torch
     from elegant_b200 import BeamSums, SUMS_SECOND_ORDER, Tracker, configs
     if rank != 0:
@@ -682,16 +682,17 @@ def run_observe(args, rank):
     t = float(np.median(ms)) / 1e3
     tc = float(np.median(c_ms)) / 1e3
     peak, src = _measured_hbm_gbs()
-    algo = 2 * 60.0 * n
+    algo = 2 * 52.0 * n
     line = {"metric": "beam sums (accumulate_beam_sums) particles/s", "value": n / t, "unit": "particles/s",
             "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": t * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded Gaussian beam)",
-            "config": {"workload": "observe_beam_sums_1e7", "particles": n, "second_order": True},
+            "config": {"workload": "observe_beam_sums_1e7", "particles": n, "second_order": True,
+                       "l2": "beam columns larger than L2 (no flush needed)"},
             "roofline": {"bound": "hbm", "achieved": algo / t / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": algo / t / 1e9 / peak, "traffic": None, "peak_source": src,
-                         "bytes_per_particle": 120},
-            "centroids_ms": tc * 1e3, "centroids_gbs": 60.0 * n / tc / 1e9, "clocks": clocks.summary()}
+                         "bytes_per_particle": 104},
+            "centroids_ms": tc * 1e3, "centroids_gbs": 52.0 * n / tc / 1e9, "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
     return 0
 

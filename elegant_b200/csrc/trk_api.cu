@@ -355,7 +355,9 @@ int ensure_beam(trk_context *ctx, long np) {
   ctx->d_cols = nullptr;
   ctx->d_lost_pass = ctx->d_lost_elem = nullptr;
   ctx->cap = 0;
-  long cap = std::max(np, 1L);
+  /* a multiple of 32 entries: every column starts 256-byte aligned and the
+   * beam-sum tiles may round their bulk copies up to 16 bytes inside it */
+  const long cap = (std::max(np, 1L) + 31) / 32 * 32;
   if (alloc_refused())
     return trk_set_error(TRK_ERR_NOMEM, "device beam allocation for %ld particles refused (test hook)", np);
   if (cudaMalloc(&ctx->d_cols, sizeof(double) * 7 * cap) != cudaSuccess ||

@@ -79,128 +79,247 @@ __device__ trkcr_dd block_dd_sum(trkcr_dd v, double *sh) {
   return t;
 }
 
-__device__ double block_min(double v, double *sh) {
-  for (int off = 16; off > 0; off >>= 1)
-    v = fmin(v, __shfl_down_sync(0xffffffffu, v, off));
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0)
-    sh[threadIdx.x >> 5] = v;
-  __syncthreads();
-  double t = OBS_BIG;
-  if (threadIdx.x == 0)
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++)
-      t = fmin(t, sh[w]);
-  return t;
-}
-
-__device__ double block_max(double v, double *sh) {
-  for (int off = 16; off > 0; off >>= 1)
-    v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0)
-    sh[threadIdx.x >> 5] = v;
-  __syncthreads();
-  double t = -OBS_BIG;
-  if (threadIdx.x == 0)
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++)
-      t = fmax(t, sh[w]);
-  return t;
-}
-
 /* selection of accumulate_beam_sums (src/compute_centroids.c:346-354) */
 struct Select {
   double Po, tmin, tmax;
   long start_pid, end_pid;
+  int pid_window;     /* start_pid or end_pid given */
   const double *time; /* caller's time coordinates, or null */
 };
 
-__device__ __forceinline__ bool chosen(const Beam &b, const Select &s, long i, double &t) {
-  if (b.lost[i] >= 0)
-    return false;
-  t = s.time ? s.time[i] : time_of(s.Po, b.c[5][i], b.c[4][i]);
-  const double id = b.c[6][i];
-  return ((s.start_pid < 0 && s.end_pid < 0) || (id >= s.start_pid && id <= s.end_pid)) &&
-         (s.tmin >= s.tmax || (t >= s.tmin && t <= s.tmax));
+/* Beam sums.  The beam is cut into chunks of SUM_CHUNK particles, and every
+ * chunk gets its own partial, so the partials do not depend on the grid or on
+ * which block sums which chunk.  Within a block a thread keeps, per sum, a
+ * running double and the plain sum of the exact errors of its additions
+ * (Knuth's TwoSum): a compensated sum whose error is of order u^2 per term.
+ * The lanes then combine their pairs as double-double values in a fixed order
+ * (a butterfly that leaves value v in lane v), the warps in index order, and
+ * the chunks in chunk order, so every total is the double-double of the exact
+ * sum of the rounded terms to about 2^-100 relative, rounded once at the end.
+ * Particles that are lost or outside the windows add +0.0 and leave the sums
+ * unchanged.
+ *
+ * Data movement: persistent blocks take chunks from a counter, and a ring of
+ * SUM_STAGES tiles of SUM_TILE particles in shared memory is filled by 1-D
+ * bulk copies (cp.async.bulk, from this device's own beam columns) that
+ * complete on an mbarrier per stage; the copies of the next tiles stream
+ * while the threads sum the current one.  Bulk copies need 16-byte aligned
+ * sources and sizes: the beam columns are SUM_TILE-aligned slices of arrays
+ * whose stride (the beam capacity) is a multiple of 32 entries, and a tile's
+ * copy is rounded up to whole 16-byte units inside that capacity. */
+constexpr int SUM_THREADS = 128;
+constexpr int SUM_WARPS = SUM_THREADS / 32;
+constexpr int SUM_TILE = 512;
+constexpr int SUM_STAGES = 2;
+constexpr long SUM_CHUNK = 8192;
+/* resident blocks per SM: pass 2 keeps 56 running sums per thread */
+template <int PASS> constexpr int sum_blocks_per_sm() { return PASS == 1 ? 3 : 2; }
+/* a stage: 6 coordinates, ID, caller's time (doubles), loss word (int32) */
+constexpr int STAGE_BYTES = SUM_TILE * (8 * 8 + 4);
+constexpr int SUM_SMEM = SUM_STAGES * STAGE_BYTES;
+constexpr int COMBINE_THREADS = 1024;
+/* a bulk copy that has not completed after this long is reported as an error */
+constexpr unsigned long long SUM_WAIT_NS = 2000000000ull;
+
+/* kernel variants: the time coordinate is needed; the ID column is read;
+ * the pz-normalized sums (pass 1: x' pz, y' pz; pass 2: sigman) */
+enum { SF_TIME = 1, SF_ID = 2, SF_PZ = 4 };
+
+/* status word of the sums kernels */
+enum { SUM_STATUS_OK = 0, SUM_STATUS_COPY_TIMEOUT = 1 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
 }
 
-/* Pass 1 of the beam sums, one chunk per block.  Per chunk: double-double
- * sums of x, x', y, y', s, delta, t (and of x' pz, y' pz when `pz_mode`),
- * the count, and min / max / max |.| of x, x', y, y', delta.  Layout of a
- * block's partial (P1 doubles): [0..17] 9 sums as (hi, lo), [18] count,
- * [19..33] (min, max, maxabs) for coordinates 0, 1, 2, 3, 5. */
-constexpr int P1 = 34;
-__global__ void __launch_bounds__(OBS_THREADS) sums_pass1(Beam b, Select s, int pz_mode, double *part) {
-  __shared__ double sh[2 * (OBS_THREADS / 32)];
-  const long lo = (long)blockIdx.x * OBS_CHUNK, hi = min(b.n, lo + OBS_CHUNK);
-  trkcr_dd acc[9];
-  for (int k = 0; k < 9; k++)
-    acc[k] = trkcr_make(0.0, 0.0);
-  double cnt = 0, mn[5], mx[5], ma[5];
-  for (int k = 0; k < 5; k++) {
-    mn[k] = OBS_BIG;
-    mx[k] = -OBS_BIG;
-    ma[k] = 0;
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile("{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+               "selp.u32 %0, 1, 0, p;\n\t}"
+               : "=r"(ok)
+               : "r"(smem_addr(bar)), "r"(parity)
+               : "memory");
+  return ok != 0;
+}
+
+/* wait for the phase of `parity` to complete, for SUM_WAIT_NS at most */
+__device__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+  if (mbar_test(bar, parity))
+    return true;
+  const unsigned long long t0 = global_ns();
+  for (long k = 0; k < (1L << 28); k++) {
+    if (mbar_test(bar, parity))
+      return true;
+    if (global_ns() - t0 > SUM_WAIT_NS)
+      return false;
+    __nanosleep(32);
   }
-  for (long i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-    double t;
-    if (!chosen(b, s, i, t))
-      continue;
-    for (int k = 0; k < 6; k++)
-      acc[k] = trkcr_add(acc[k], trkcr_make(b.c[k][i], 0.0));
-    acc[6] = trkcr_add(acc[6], trkcr_make(t, 0.0));
-    if (pz_mode) {
-      /* pz = p_central (1 + delta) / sqrt(1 + x'^2 + y'^2) (src/compute_centroids.c:338-342) */
-      const double xp = b.c[1][i], yp = b.c[3][i];
-      const double pz = __ddiv_rn(__dmul_rn(s.Po, __dadd_rn(1.0, b.c[5][i])),
-                                  __dsqrt_rn(__dadd_rn(__dadd_rn(1.0, __dmul_rn(xp, xp)), __dmul_rn(yp, yp))));
-      acc[7] = trkcr_add(acc[7], trkcr_make(__dmul_rn(xp, pz), 0.0));
-      acc[8] = trkcr_add(acc[8], trkcr_make(__dmul_rn(yp, pz), 0.0));
+  return false;
+}
+
+/* one 1-D bulk copy global -> shared, completing on `bar` */
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                 smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void csum_add(double &s, double &e, double x) {
+  const double t = __dadd_rn(s, x);
+  const double bb = __dsub_rn(t, s);
+  e = __dadd_rn(e, __dadd_rn(__dsub_rn(s, __dsub_rn(t, bb)), __dsub_rn(x, bb)));
+  s = t;
+}
+
+/* Lane butterfly over NP (a power of two <= 32) double-double values: steps
+ * with distance >= NP add all values across the lane pair, the others keep
+ * half of the values and add the partner's copy of that half.  Afterwards
+ * lane L holds value L % NP in h[0], l[0].  Both lanes of a pair add the
+ * lower lane's value first, so the result does not depend on the lane. */
+template <int NP>
+__device__ __forceinline__ void warp_dd_scatter(double (&h)[NP], double (&l)[NP]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int m = 16; m >= NP; m >>= 1) {
+    const bool up = (lane & m) != 0;
+#pragma unroll
+    for (int i = 0; i < NP; i++) {
+      const double rh = __shfl_xor_sync(0xffffffffu, h[i], m), rl = __shfl_xor_sync(0xffffffffu, l[i], m);
+      const trkcr_dd s = trkcr_add(trkcr_make(up ? rh : h[i], up ? rl : l[i]),
+                                   trkcr_make(up ? h[i] : rh, up ? l[i] : rl));
+      h[i] = s.hi;
+      l[i] = s.lo;
     }
-    cnt += 1;
-    const int cols[5] = {0, 1, 2, 3, 5};
-    for (int k = 0; k < 5; k++) {
-      const double v = b.c[cols[k]][i];
-      mn[k] = fmin(mn[k], v);
-      mx[k] = fmax(mx[k], v);
-      ma[k] = fmax(ma[k], fabs(v));
-    }
   }
-  double *out = part + (size_t)blockIdx.x * P1;
-  for (int k = 0; k < 9; k++) {
-    const trkcr_dd t = block_dd_sum(acc[k], sh);
-    if (threadIdx.x == 0) {
-      out[2 * k] = t.hi;
-      out[2 * k + 1] = t.lo;
-    }
-  }
-  {
-    const trkcr_dd t = block_dd_sum(trkcr_make(cnt, 0.0), sh);
-    if (threadIdx.x == 0)
-      out[18] = t.hi;
-  }
-  for (int k = 0; k < 5; k++) {
-    const double a = block_min(mn[k], sh), c = block_max(mx[k], sh), d = block_max(ma[k], sh);
-    if (threadIdx.x == 0) {
-      out[19 + 3 * k] = a;
-      out[20 + 3 * k] = c;
-      out[21 + 3 * k] = d;
+#pragma unroll
+  for (int m = (NP < 32 ? NP / 2 : 16); m >= 1; m >>= 1) {
+    const bool up = (lane & m) != 0;
+#pragma unroll
+    for (int i = 0; i < m; i++) {
+      const double sh = up ? h[i] : h[i + m], sl = up ? l[i] : l[i + m];
+      const double kh = up ? h[i + m] : h[i], kl = up ? l[i + m] : l[i];
+      const double rh = __shfl_xor_sync(0xffffffffu, sh, m), rl = __shfl_xor_sync(0xffffffffu, sl, m);
+      const trkcr_dd s = trkcr_add(trkcr_make(up ? rh : kh, up ? rl : kl), trkcr_make(up ? kh : rh, up ? kl : rl));
+      h[i] = s.hi;
+      l[i] = s.lo;
     }
   }
 }
 
-/* Pass 2: second moments about the centroids.  Per chunk: double-double
- * sums of (c_i - m_i)(c_j - m_j), i <= j over x, x', y, y', s, delta, t
- * (28 pairs, in row order), of the normalized products when `pz_mode`
- * (src/compute_centroids.c:418-420, as written there: the second factor is
- * not centered and index 6 reads the particle ID column), and min / max /
- * max |.| of s - m_s and t - m_t.  Block partial: [0..55] sigma (hi, lo),
- * [56..111] sigman, [112..117] (min, max, maxabs) of s and t. */
-constexpr int P2 = 118;
-struct Moments {
-  double m[7];  /* centroids (t: time centroid) */
-  double mn[7]; /* centroids of the normalized coordinates */
-  int sparse;
+/* the block's NV double-double totals from the threads' compensated sums
+ * (s, e) -> out[2v], out[2v + 1]; `sh` holds 2 NV SUM_WARPS doubles */
+template <int NV, int NP>
+__device__ __forceinline__ void block_dd_totals(double (&s)[NP], double (&e)[NP], double *sh, double *out) {
+#pragma unroll
+  for (int v = 0; v < NP; v++) {
+    const trkcr_dd t = trkcr_two_sum(s[v], e[v]);
+    s[v] = t.hi;
+    e[v] = t.lo;
+  }
+  warp_dd_scatter<NP>(s, e);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane < NV) {
+    sh[2 * (warp * NV + lane)] = s[0];
+    sh[2 * (warp * NV + lane) + 1] = e[0];
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    const int v = threadIdx.x;
+    trkcr_dd t = trkcr_make(sh[2 * v], sh[2 * v + 1]);
+    for (int w = 1; w < SUM_WARPS; w++)
+      t = trkcr_add(t, trkcr_make(sh[2 * (w * NV + v)], sh[2 * (w * NV + v) + 1]));
+    out[2 * v] = t.hi;
+    out[2 * v + 1] = t.lo;
+  }
+  __syncthreads();
+}
+
+/* the block's extremes: value v is a minimum when bit v of `min_mask` is set,
+ * else a maximum; `sh` holds NV SUM_WARPS doubles */
+template <int NV>
+__device__ __forceinline__ void block_extremes(double (&x)[NV], unsigned min_mask, double *sh, double *out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int v = 0; v < NV; v++) {
+    const bool is_min = (min_mask >> v) & 1u;
+    for (int off = 16; off > 0; off >>= 1) {
+      const double o = __shfl_down_sync(0xffffffffu, x[v], off);
+      x[v] = is_min ? fmin(x[v], o) : fmax(x[v], o);
+    }
+    if (lane == 0)
+      sh[warp * NV + v] = x[v];
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    const int v = threadIdx.x;
+    const bool is_min = (min_mask >> v) & 1u;
+    double t = sh[v];
+    for (int w = 1; w < SUM_WARPS; w++)
+      t = is_min ? fmin(t, sh[w * NV + v]) : fmax(t, sh[w * NV + v]);
+    out[v] = t;
+  }
+  __syncthreads();
+}
+
+/* the block's count of a per-thread integer -> out[0] */
+__device__ __forceinline__ void block_count(int n, int *sh, double *out) {
+  n = __reduce_add_sync(0xffffffffu, n);
+  if ((threadIdx.x & 31) == 0)
+    sh[threadIdx.x >> 5] = n;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long t = 0;
+    for (int w = 0; w < SUM_WARPS; w++)
+      t += sh[w];
+    out[0] = (double)t;
+  }
+  __syncthreads();
+}
+
+/* one particle's columns, read from a staged tile */
+struct Row {
+  double v[6], id, t;
+  int32_t lost;
 };
+
+/* the time coordinate and the selection of one loaded particle */
+template <int F>
+__device__ __forceinline__ bool select_row(const Select &s, Row &r) {
+  bool ok = r.lost < 0;
+  if (F & SF_TIME) {
+    if (!s.time)
+      r.t = time_of(s.Po, r.v[5], r.v[4]);
+    ok = ok && (s.tmin >= s.tmax || (r.t >= s.tmin && r.t <= s.tmax));
+  }
+  if ((F & SF_ID) && s.pid_window)
+    ok = ok && r.id >= s.start_pid && r.id <= s.end_pid;
+  return ok;
+}
+
+/* pz = p_central (1 + delta) / sqrt(1 + x'^2 + y'^2) (src/compute_centroids.c:338-342) */
+__device__ __forceinline__ double pz_of(double Po, const Row &r) {
+  const double xp = r.v[1], yp = r.v[3];
+  return __ddiv_rn(__dmul_rn(Po, __dadd_rn(1.0, r.v[5])),
+                   __dsqrt_rn(__dadd_rn(__dadd_rn(1.0, __dmul_rn(xp, xp)), __dmul_rn(yp, yp))));
+}
 
 /* the pairs BEAM_SUMS_SPARSE keeps: diagonal blocks and dispersive
  * correlations (src/compute_centroids.c:301-308) */
@@ -212,96 +331,318 @@ struct Moments {
 __constant__ signed char k_sparse[7][7] = OBS_SPARSE;
 static const signed char k_sparse_host[7][7] = OBS_SPARSE;
 
-__global__ void __launch_bounds__(OBS_THREADS) sums_pass2(Beam b, Select s, Moments M, int pz_mode, double *part) {
-  __shared__ double sh[2 * (OBS_THREADS / 32)];
-  const long lo = (long)blockIdx.x * OBS_CHUNK, hi = min(b.n, lo + OBS_CHUNK);
-  double *out = part + (size_t)blockIdx.x * P2;
-  double smn = OBS_BIG, smx = -OBS_BIG, sma = 0, tmn = OBS_BIG, tmx = -OBS_BIG, tma = 0;
-  /* one pair at a time keeps the per-thread state small; the chunk is read
-   * from L1/L2 again for each pair */
-  int pair = 0;
-  for (int i = 0; i < 7; i++)
-    for (int j = i; j < 7; j++, pair++) {
-      trkcr_dd acc = trkcr_make(0.0, 0.0), accn = trkcr_make(0.0, 0.0);
-      const bool skip = M.sparse && !k_sparse[i][j];
-      if (!skip)
-        for (long p = lo + threadIdx.x; p < hi; p += blockDim.x) {
-          double t;
-          if (!chosen(b, s, p, t))
-            continue;
-          const double tc = __dsub_rn(t, M.m[6]);
-          const double di = i < 6 ? __dsub_rn(b.c[i][p], M.m[i]) : tc;
-          const double dj = j < 6 ? __dsub_rn(b.c[j][p], M.m[j]) : tc;
-          acc = trkcr_add(acc, trkcr_make(__dmul_rn(di, dj), 0.0));
-          if (pz_mode) {
-            const double xp = b.c[1][p], yp = b.c[3][p];
-            const double pz = __ddiv_rn(__dmul_rn(s.Po, __dadd_rn(1.0, b.c[5][p])),
-                                        __dsqrt_rn(__dadd_rn(__dadd_rn(1.0, __dmul_rn(xp, xp)), __dmul_rn(yp, yp))));
-            const double ui = (i == 1 || i == 3) ? __dmul_rn(b.c[i][p], pz) : b.c[i][p];
-            const double uj = (j == 1 || j == 3) ? __dmul_rn(b.c[j][p], pz) : b.c[j][p];
-            accn = trkcr_add(accn, trkcr_make(__dmul_rn(__dsub_rn(ui, M.mn[i]), uj), 0.0));
-          }
-          if (pair == 0) {
-            const double ds = __dsub_rn(b.c[4][p], M.m[4]);
-            smn = fmin(smn, ds);
-            smx = fmax(smx, ds);
-            sma = fmax(sma, fabs(ds));
-            tmn = fmin(tmn, tc);
-            tmx = fmax(tmx, tc);
-            tma = fmax(tma, fabs(tc));
-          }
-        }
-      else if (pair == 0)
-        for (long p = lo + threadIdx.x; p < hi; p += blockDim.x) {
-          double t;
-          if (!chosen(b, s, p, t))
-            continue;
-          const double tc = __dsub_rn(t, M.m[6]);
-          const double ds = __dsub_rn(b.c[4][p], M.m[4]);
-          smn = fmin(smn, ds);
-          smx = fmax(smx, ds);
-          sma = fmax(sma, fabs(ds));
-          tmn = fmin(tmn, tc);
-          tmx = fmax(tmx, tc);
-          tma = fmax(tma, fabs(tc));
-        }
-      const trkcr_dd r = block_dd_sum(acc, sh);
-      const trkcr_dd rn = block_dd_sum(accn, sh);
-      if (threadIdx.x == 0) {
-        out[2 * pair] = r.hi;
-        out[2 * pair + 1] = r.lo;
-        out[56 + 2 * pair] = rn.hi;
-        out[57 + 2 * pair] = rn.lo;
-      }
+/* centroids of pass 1 (m) and of the normalized coordinates (mn) */
+__device__ __forceinline__ void moments_of(const double *tot1, double m[7], double mn[7]) {
+  const double count = tot1[18];
+#pragma unroll
+  for (int k = 0; k < 7; k++) {
+    m[k] = __dadd_rn(tot1[2 * k], tot1[2 * k + 1]);
+    mn[k] = 0.0;
+  }
+  mn[1] = __dadd_rn(tot1[14], tot1[15]);
+  mn[3] = __dadd_rn(tot1[16], tot1[17]);
+  if (count > 0)
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+      m[k] = __ddiv_rn(m[k], count);
+      mn[k] = __ddiv_rn(mn[k], count);
     }
-  const double v[6] = {block_min(smn, sh), block_max(smx, sh), block_max(sma, sh),
-                       block_min(tmn, sh), block_max(tmx, sh), block_max(tma, sh)};
-  if (threadIdx.x == 0)
-    for (int k = 0; k < 6; k++)
-      out[112 + k] = v[k];
+#pragma unroll
+  for (int k = 0; k < 7; k++)
+    if (k != 1 && k != 3)
+      mn[k] = m[k];
 }
 
-/* Combine the block partials in block order: `n_dd` double-double pairs at
- * the front, then `n_plain` values combined with `ops` (0 sum, 1 min, 2 max)
- * per value; one block, thread k owns value k. */
-__global__ void combine_partials(const double *part, int nblocks, int stride, int n_dd, int n_plain,
-                                 const signed char *ops, double *out) {
-  const int k = threadIdx.x;
-  if (k < n_dd) {
-    trkcr_dd acc = trkcr_make(0.0, 0.0);
-    for (int b = 0; b < nblocks; b++)
-      acc = trkcr_add(acc, trkcr_make(part[(size_t)b * stride + 2 * k], part[(size_t)b * stride + 2 * k + 1]));
-    out[2 * k] = acc.hi;
-    out[2 * k + 1] = acc.lo;
-  } else if (k < n_dd + n_plain) {
-    const int q = 2 * n_dd + (k - n_dd);
-    const int op = ops[k - n_dd];
-    double acc = op == 0 ? 0.0 : (op == 1 ? OBS_BIG : -OBS_BIG);
-    for (int b = 0; b < nblocks; b++) {
-      const double v = part[(size_t)b * stride + q];
-      acc = op == 0 ? __dadd_rn(acc, v) : (op == 1 ? fmin(acc, v) : fmax(acc, v));
+/* the ring of staged tiles: an mbarrier per stage and the tile it holds
+ * (chunk -1: no work left) */
+struct Ring {
+  uint64_t bar[SUM_STAGES];
+  long chunk[SUM_STAGES];
+  int tile[SUM_STAGES];
+  int fail;
+};
+
+/* tiles of chunk c */
+__device__ __forceinline__ int tiles_of(long c, long n) {
+  const long lo = c * SUM_CHUNK, hi = min(n, lo + SUM_CHUNK);
+  return (int)((hi - lo + SUM_TILE - 1) / SUM_TILE);
+}
+
+/* the issuing thread's position in its stream of tiles */
+struct Producer {
+  long chunk, issued;
+  int tile, ntiles;
+};
+
+/* Issue the next tile of the block's stream into `stage` (thread 0).  A new
+ * chunk is taken from the counter when the current one is used up; past the
+ * last chunk the stage gets an end mark and a plain arrival instead. */
+template <int F>
+__device__ void issue_tile(Ring &r, unsigned char *smem, int stage, Producer &p, const Beam &b, const Select &s,
+                           int *next_chunk, long nchunks) {
+  if (p.tile == p.ntiles) {
+    if (p.chunk < nchunks)
+      p.chunk = atomicAdd(next_chunk, 1);
+    p.tile = 0;
+    p.ntiles = p.chunk < nchunks ? tiles_of(p.chunk, b.n) : 0;
+  }
+  if (p.chunk >= nchunks) {
+    r.chunk[stage] = -1;
+    mbar_arrive(&r.bar[stage]);
+    return;
+  }
+  unsigned char *st = smem + (size_t)stage * STAGE_BYTES;
+  const long start = p.chunk * SUM_CHUNK + (long)p.tile * SUM_TILE;
+  const int cnt = (int)min((long)SUM_TILE, b.n - start);
+  /* whole 16-byte units: 2 doubles, 4 loss words (inside the capacity) */
+  const unsigned bd = (unsigned)((cnt + 1) & ~1) * 8u, bl = (unsigned)((cnt + 3) & ~3) * 4u;
+  const bool time = (F & SF_TIME) && s.time;
+  r.chunk[stage] = p.chunk;
+  r.tile[stage] = p.tile;
+  mbar_arrive_expect_tx(&r.bar[stage], bd * (6u + ((F & SF_ID) ? 1u : 0u) + (time ? 1u : 0u)) + bl);
+  for (int k = 0; k < 6; k++)
+    bulk_load(st + (size_t)k * SUM_TILE * 8, b.c[k] + start, bd, &r.bar[stage]);
+  if (F & SF_ID)
+    bulk_load(st + (size_t)6 * SUM_TILE * 8, b.c[6] + start, bd, &r.bar[stage]);
+  if (time)
+    bulk_load(st + (size_t)7 * SUM_TILE * 8, s.time + start, bd, &r.bar[stage]);
+  bulk_load(st + (size_t)8 * SUM_TILE * 8, b.lost + start, bl, &r.bar[stage]);
+  p.tile++;
+  p.issued++;
+}
+
+/* P1 / P2: the block partial layouts of the two passes (doubles per chunk) */
+constexpr int P1 = 35;
+constexpr unsigned P1_MIN_MASK = 0x2492u; /* plain values 1, 4, 7, 10, 13: the minima */
+constexpr unsigned P1_MAX_MASK = 0xDB6Cu; /* plain values 2, 3, 5, 6, ..., 14, 15 */
+constexpr int P2 = 118;
+constexpr unsigned P2_MIN_MASK = 0x9u; /* plain values 0 and 3 */
+constexpr unsigned P2_MAX_MASK = 0x36u;
+
+/* The beam-sum passes, one partial per chunk.
+ *
+ * Pass 1 (PASS = 1): sums of x, x', y, y', s, delta, t (SF_TIME) and of
+ * x' pz, y' pz (SF_PZ), the count of selected particles, min / max / max |.|
+ * of x, x', y, y', delta, and the count of surviving particles.  Partial (P1
+ * doubles): [0..17] 9 sums as (hi, lo), [18] count, [19..33] (min, max,
+ * maxabs) for coordinates 0, 1, 2, 3, 5, [34] survivors.
+ *
+ * Pass 2 (PASS = 2): second moments about the centroids, which each block
+ * forms from the combined pass-1 totals `tot1` as the host forms them
+ * (src/compute_centroids.c:357-385).  Sums of (c_i - m_i)(c_j - m_j), i <= j
+ * over x, x', y, y', s, delta, t (28 pairs, in row order), and min / max /
+ * max |.| of s - m_s and t - m_t; or, with SF_PZ, the sums of the normalized
+ * products (src/compute_centroids.c:418-420, as written there: the second
+ * factor is not centered and index 6 reads the particle ID column).  Partial
+ * (P2 doubles): [0..55] sigma (hi, lo), [56..111] sigman, [112..117] (min,
+ * max, maxabs) of s and t.  The pass without SF_PZ writes zeros to the sigman
+ * part unless `pz_pass` says the SF_PZ pass follows.
+ *
+ * `status` gets SUM_STATUS_COPY_TIMEOUT when a staged copy did not complete
+ * in time; the block then waits (bounded) for its copies in flight and
+ * returns. */
+template <int PASS, int F>
+__global__ void __launch_bounds__(SUM_THREADS, sum_blocks_per_sm<PASS>())
+  beam_sums(Beam b, Select s, const double *tot1, int sparse, int pz_pass, int *next_chunk, int *status,
+            double *part) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ Ring r;
+  __shared__ double red[2 * 28 * SUM_WARPS];
+  __shared__ int redc[SUM_WARPS];
+  constexpr int NP = PASS == 1 ? 16 : 32; /* butterfly width */
+  constexpr int NX = PASS == 1 ? 15 : 6;  /* extremes */
+  __shared__ double sm_m[7], sm_mn[7];
+  const long nchunks = (b.n + SUM_CHUNK - 1) / SUM_CHUNK;
+  if (PASS == 2 && threadIdx.x == 0)
+    moments_of(tot1, sm_m, sm_mn);
+  const double *m = sm_m, *mn = sm_mn;
+  double S[NP], E[NP], X[NX];
+  int cnt = 0, alive = 0;
+  auto reset = [&]() {
+#pragma unroll
+    for (int k = 0; k < NP; k++)
+      S[k] = E[k] = 0.0;
+#pragma unroll
+    for (int k = 0; k < NX; k++)
+      X[k] = (k % 3 == 0) ? OBS_BIG : ((k % 3 == 1) ? -OBS_BIG : 0.0);
+    cnt = alive = 0;
+  };
+  reset();
+  Producer p;
+  p.chunk = -1;
+  p.issued = 0;
+  p.tile = p.ntiles = 0;
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < SUM_STAGES; k++)
+      mbar_init(&r.bar[k], 1);
+    r.fail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int k = 0; k < SUM_STAGES; k++)
+      issue_tile<F>(r, smem, k, p, b, s, next_chunk, nchunks);
+  long it = 0;
+  for (;; it++) {
+    const int stage = (int)(it % SUM_STAGES);
+    const bool ok = mbar_wait(&r.bar[stage], (unsigned)((it / SUM_STAGES) & 1));
+    long chunk = -1;
+    int tile = 0;
+    if (ok) {
+      chunk = r.chunk[stage];
+      tile = r.tile[stage];
+    } else {
+      r.fail = 1;
     }
-    out[q] = acc;
+    if (ok && chunk >= 0) {
+      const double *col = (const double *)(smem + (size_t)stage * STAGE_BYTES);
+      const int32_t *lost = (const int32_t *)(col + 8 * SUM_TILE);
+      const long start = chunk * SUM_CHUNK + (long)tile * SUM_TILE;
+      const int n_tile = (int)min((long)SUM_TILE, b.n - start);
+      for (int q = threadIdx.x; q < n_tile; q += SUM_THREADS) {
+        Row w;
+        w.lost = lost[q];
+#pragma unroll
+        for (int k = 0; k < 6; k++)
+          w.v[k] = col[k * SUM_TILE + q];
+        w.id = (F & SF_ID) ? col[6 * SUM_TILE + q] : 0.0;
+        w.t = ((F & SF_TIME) && s.time) ? col[7 * SUM_TILE + q] : 0.0;
+        const bool sel = select_row<F>(s, w);
+        if constexpr (PASS == 1) {
+          alive += w.lost < 0;
+          cnt += sel;
+#pragma unroll
+          for (int k = 0; k < 6; k++)
+            csum_add(S[k], E[k], sel ? w.v[k] : 0.0);
+          if (F & SF_TIME)
+            csum_add(S[6], E[6], sel ? w.t : 0.0);
+          if (F & SF_PZ) {
+            const double pz = pz_of(s.Po, w);
+            csum_add(S[7], E[7], sel ? __dmul_rn(w.v[1], pz) : 0.0);
+            csum_add(S[8], E[8], sel ? __dmul_rn(w.v[3], pz) : 0.0);
+          }
+          const int cols[5] = {0, 1, 2, 3, 5};
+#pragma unroll
+          for (int k = 0; k < 5; k++) {
+            const double v = w.v[cols[k]];
+            X[3 * k] = fmin(X[3 * k], sel ? v : OBS_BIG);
+            X[3 * k + 1] = fmax(X[3 * k + 1], sel ? v : -OBS_BIG);
+            X[3 * k + 2] = fmax(X[3 * k + 2], sel ? fabs(v) : 0.0);
+          }
+        } else if constexpr (!(F & SF_PZ)) {
+          double d[7];
+#pragma unroll
+          for (int k = 0; k < 6; k++)
+            d[k] = __dsub_rn(w.v[k], m[k]);
+          d[6] = __dsub_rn(w.t, m[6]);
+          int pair = 0;
+#pragma unroll
+          for (int a = 0; a < 7; a++)
+#pragma unroll
+            for (int c = a; c < 7; c++, pair++)
+              if (!sparse || k_sparse[a][c])
+                csum_add(S[pair], E[pair], sel ? __dmul_rn(d[a], d[c]) : 0.0);
+          X[0] = fmin(X[0], sel ? d[4] : OBS_BIG);
+          X[1] = fmax(X[1], sel ? d[4] : -OBS_BIG);
+          X[2] = fmax(X[2], sel ? fabs(d[4]) : 0.0);
+          X[3] = fmin(X[3], sel ? d[6] : OBS_BIG);
+          X[4] = fmax(X[4], sel ? d[6] : -OBS_BIG);
+          X[5] = fmax(X[5], sel ? fabs(d[6]) : 0.0);
+        } else {
+          const double pz = pz_of(s.Po, w);
+          double u[7];
+#pragma unroll
+          for (int k = 0; k < 6; k++)
+            u[k] = (k == 1 || k == 3) ? __dmul_rn(w.v[k], pz) : w.v[k];
+          u[6] = w.id;
+          int pair = 0;
+#pragma unroll
+          for (int a = 0; a < 7; a++)
+#pragma unroll
+            for (int c = a; c < 7; c++, pair++)
+              if (!sparse || k_sparse[a][c])
+                csum_add(S[pair], E[pair], sel ? __dmul_rn(__dsub_rn(u[a], mn[a]), u[c]) : 0.0);
+        }
+      }
+    }
+    /* the stage is consumed; failures and the end of the work are seen by
+     * every thread after this barrier */
+    __syncthreads();
+    if (r.fail || chunk < 0)
+      break;
+    if (threadIdx.x == 0) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue_tile<F>(r, smem, stage, p, b, s, next_chunk, nchunks);
+    }
+    if (tile == tiles_of(chunk, b.n) - 1) {
+      /* the chunk is complete: its partial */
+      if constexpr (PASS == 1) {
+        double *out = part + (size_t)chunk * P1;
+        block_dd_totals<9, NP>(S, E, red, out);
+        block_count(cnt, redc, out + 18);
+        block_extremes<NX>(X, 0x1249u, red, out + 19);
+        block_count(alive, redc, out + 34);
+      } else if constexpr (!(F & SF_PZ)) {
+        double *out = part + (size_t)chunk * P2;
+        block_dd_totals<28, NP>(S, E, red, out);
+        block_extremes<NX>(X, 0x9u, red, out + 112);
+        if (!pz_pass)
+          for (int k = threadIdx.x; k < 56; k += SUM_THREADS)
+            out[56 + k] = 0.0;
+      } else {
+        block_dd_totals<28, NP>(S, E, red, part + (size_t)chunk * P2 + 56);
+      }
+      reset();
+    }
+  }
+  if (r.fail && threadIdx.x == 0) {
+    /* copies still in flight land before the block's shared memory is
+     * released: wait for them too, again for a bounded time */
+    for (long t = it + 1; t < p.issued; t++)
+      mbar_wait(&r.bar[t % SUM_STAGES], (unsigned)((t / SUM_STAGES) & 1));
+    if (!mbar_test(&r.bar[it % SUM_STAGES], (unsigned)((it / SUM_STAGES) & 1)))
+      mbar_wait(&r.bar[it % SUM_STAGES], (unsigned)((it / SUM_STAGES) & 1));
+    atomicExch(status, SUM_STATUS_COPY_TIMEOUT);
+  }
+}
+
+/* Combine the block partials in block order: `n_dd` double-double values at
+ * the front, then `n_plain` values, plain value k a minimum when bit k of
+ * `min_mask` is set, a maximum when bit k of `max_mask` is set, else a sum.
+ * One warp per value: lane l takes blocks l, l + 32, ... in order and the
+ * lanes combine in a fixed tree. */
+__global__ void __launch_bounds__(COMBINE_THREADS)
+  combine_partials(const double *part, int nblocks, int stride, int n_dd, int n_plain, unsigned min_mask,
+                   unsigned max_mask, double *out) {
+  const int lane = threadIdx.x & 31;
+  for (int v = threadIdx.x >> 5; v < n_dd + n_plain; v += COMBINE_THREADS / 32) {
+    if (v < n_dd) {
+      trkcr_dd acc = trkcr_make(0.0, 0.0);
+      for (int b = lane; b < nblocks; b += 32)
+        acc = trkcr_add(acc, trkcr_make(part[(size_t)b * stride + 2 * v], part[(size_t)b * stride + 2 * v + 1]));
+      for (int off = 16; off > 0; off >>= 1) {
+        const double h = __shfl_down_sync(0xffffffffu, acc.hi, off), l = __shfl_down_sync(0xffffffffu, acc.lo, off);
+        acc = trkcr_add(acc, trkcr_make(h, l));
+      }
+      if (lane == 0) {
+        out[2 * v] = acc.hi;
+        out[2 * v + 1] = acc.lo;
+      }
+    } else {
+      const int k = v - n_dd, q = 2 * n_dd + k;
+      const int op = ((min_mask >> k) & 1u) ? 1 : (((max_mask >> k) & 1u) ? 2 : 0);
+      double acc = op == 0 ? 0.0 : (op == 1 ? OBS_BIG : -OBS_BIG);
+      for (int b = lane; b < nblocks; b += 32) {
+        const double x = part[(size_t)b * stride + q];
+        acc = op == 0 ? __dadd_rn(acc, x) : (op == 1 ? fmin(acc, x) : fmax(acc, x));
+      }
+      for (int off = 16; off > 0; off >>= 1) {
+        const double x = __shfl_down_sync(0xffffffffu, acc, off);
+        acc = op == 0 ? __dadd_rn(acc, x) : (op == 1 ? fmin(acc, x) : fmax(acc, x));
+      }
+      if (lane == 0)
+        out[q] = acc;
+    }
   }
 }
 
@@ -420,32 +761,63 @@ struct Scratch {
   }
 };
 
-/* pass-1 totals on the host: 9 rounded sums, count, 5 x (min, max, maxabs) */
-int pass1(const Ctx &c, const Select &s, int pz_mode, double sums[9], double &count, double mm[15]) {
-  const int nb = (int)((c.n + OBS_CHUNK - 1) / OBS_CHUNK);
-  Scratch sc(c.ctx, 1);
-  double *part, *out;
-  signed char *ops;
+/* one pass of the beam sums into the chunk partials `part`; `counter` and
+ * `status` are device ints the caller has zeroed */
+template <int PASS, int F>
+int launch_sums(const Ctx &c, const Select &s, const double *tot1, int sparse, int pz_pass, int *counter,
+                int *status, double *part) {
+  auto kernel = beam_sums<PASS, F>;
+  OBS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SUM_SMEM));
+  int sms = 0;
+  OBS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device));
+  const long nchunks = (c.n + SUM_CHUNK - 1) / SUM_CHUNK;
+  const int grid = (int)std::max(1L, std::min<long>(nchunks, (long)sms * sum_blocks_per_sm<PASS>()));
+  kernel<<<grid, SUM_THREADS, SUM_SMEM, c.st>>>(beam_of(c), s, tot1, sparse, pz_pass, counter, status, part);
+  OBS_CUDA(cudaGetLastError());
+  return TRK_OK;
+}
+
+int blocks_of(const Ctx &c) { return (int)((c.n + SUM_CHUNK - 1) / SUM_CHUNK); }
+
+/* pass 1 on the device: chunk partials, then their combination into tot1;
+ * `ctl` (4 ints: chunk counters of the passes, status) is zeroed here */
+int enqueue_pass1(const Ctx &c, Scratch &sc, const Select &s, int F, double **tot1, int **ctl) {
+  const int nb = blocks_of(c);
+  double *part;
   int rc;
-  if ((rc = sc.get(&part, (size_t)nb * P1)) || (rc = sc.get(&out, P1)) || (rc = sc.get(&ops, 16)))
+  if ((rc = sc.get(&part, (size_t)nb * P1)) || (rc = sc.get(tot1, P1)) || (rc = sc.get(ctl, 4)))
     return rc;
-  signed char h_ops[16] = {0};
-  for (int k = 0; k < 5; k++) {
-    h_ops[1 + 3 * k] = 1;
-    h_ops[2 + 3 * k] = 2;
-    h_ops[3 + 3 * k] = 2;
+  OBS_CUDA(cudaMemsetAsync(*ctl, 0, 4 * sizeof(int), c.st));
+  switch (F) {
+  case 0:
+    rc = launch_sums<1, 0>(c, s, nullptr, 0, 0, *ctl, *ctl + 3, part);
+    break;
+  case SF_TIME:
+    rc = launch_sums<1, SF_TIME>(c, s, nullptr, 0, 0, *ctl, *ctl + 3, part);
+    break;
+  case SF_TIME | SF_ID:
+    rc = launch_sums<1, SF_TIME | SF_ID>(c, s, nullptr, 0, 0, *ctl, *ctl + 3, part);
+    break;
+  case SF_TIME | SF_PZ:
+    rc = launch_sums<1, SF_TIME | SF_PZ>(c, s, nullptr, 0, 0, *ctl, *ctl + 3, part);
+    break;
+  case SF_TIME | SF_ID | SF_PZ:
+    rc = launch_sums<1, SF_TIME | SF_ID | SF_PZ>(c, s, nullptr, 0, 0, *ctl, *ctl + 3, part);
+    break;
+  default:
+    return trk_set_error(TRK_ERR_ARG, "beam sums: no pass-1 variant %d", F);
   }
-  OBS_CUDA(cudaMemcpyAsync(ops, h_ops, sizeof(h_ops), cudaMemcpyHostToDevice, c.st));
-  sums_pass1<<<nb, OBS_THREADS, 0, c.st>>>(beam_of(c), s, pz_mode, part);
-  combine_partials<<<1, 64, 0, c.st>>>(part, nb, P1, 9, 16, ops, out);
-  double h[P1];
-  OBS_CUDA(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, c.st));
-  OBS_CUDA(cudaStreamSynchronize(c.st));
-  for (int k = 0; k < 9; k++)
-    sums[k] = h[2 * k] + h[2 * k + 1];
-  count = h[18];
-  for (int k = 0; k < 15; k++)
-    mm[k] = h[19 + k];
+  if (rc)
+    return rc;
+  combine_partials<<<1, COMBINE_THREADS, 0, c.st>>>(part, nb, P1, 9, 17, P1_MIN_MASK, P1_MAX_MASK, *tot1);
+  OBS_CUDA(cudaGetLastError());
+  return TRK_OK;
+}
+
+/* the status word of the passes, after the stream has been synchronized */
+int sums_status(int status) {
+  if (status == SUM_STATUS_COPY_TIMEOUT)
+    return trk_set_error(TRK_ERR_CUDA, "beam sums: a staged copy of the beam did not complete");
   return TRK_OK;
 }
 
@@ -470,13 +842,22 @@ int trk_beam_centroids(trk_context *ctx, double *centroid, long *n) {
   s.Po = 1.0;
   s.tmin = s.tmax = 0;
   s.start_pid = s.end_pid = -1;
+  s.pid_window = 0;
   s.time = nullptr;
-  double sums[9], count, mm[15];
-  if ((rc = pass1(c, s, 0, sums, count, mm)))
+  Scratch sc(c.ctx, 1);
+  double *tot, h[P1];
+  int *ctl, status = 0;
+  if ((rc = enqueue_pass1(c, sc, s, 0, &tot, &ctl)))
     return rc;
+  OBS_CUDA(cudaMemcpyAsync(h, tot, sizeof(h), cudaMemcpyDeviceToHost, c.st));
+  OBS_CUDA(cudaMemcpyAsync(&status, ctl + 3, sizeof(int), cudaMemcpyDeviceToHost, c.st));
+  OBS_CUDA(cudaStreamSynchronize(c.st));
+  if ((rc = sums_status(status)))
+    return rc;
+  const double count = h[18];
   if (count > 0)
     for (int k = 0; k < 6; k++)
-      centroid[k] = sums[k] / count;
+      centroid[k] = (h[2 * k] + h[2 * k + 1]) / count;
   if (n)
     *n = (long)count;
   return TRK_OK;
@@ -495,11 +876,8 @@ int trk_accumulate_beam_sums(trk_context *ctx, trk_beam_sums *sums, double p_cen
   const int pz_mode = (flags & TRK_SUMS_EXACT_NORMEMIT) ? 1 : 0;
   if (!sums->n_part)
     sums->p0 = p_central;
-  long alive = 0;
-  if ((rc = trk_beam_count(ctx, &alive)))
-    return rc;
   double np_count = 0;
-  if (alive > 0) {
+  if (c.n > 0) {
     Scratch sc(c.ctx, 2);
     Select s;
     s.Po = p_central;
@@ -507,82 +885,87 @@ int trk_accumulate_beam_sums(trk_context *ctx, trk_beam_sums *sums, double p_cen
     s.tmax = t_max;
     s.start_pid = start_pid;
     s.end_pid = end_pid;
+    s.pid_window = start_pid >= 0 || end_pid >= 0;
     s.time = nullptr;
     if (time_value) {
       /* the caller's time coordinates, one per loaded particle */
       double *d_time;
-      if ((rc = sc.get(&d_time, (size_t)c.n)))
+      if ((rc = sc.get(&d_time, (size_t)(c.n + 31) / 32 * 32)))
         return rc;
       OBS_CUDA(cudaMemcpyAsync(d_time, time_value, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.st));
       s.time = d_time;
     }
-    double sum[9], mm[15];
-    if ((rc = pass1(c, s, pz_mode, sum, np_count, mm)))
+    /* the whole computation is queued on the device: pass 2 forms the
+     * centroids from pass 1's totals itself, and the host waits once */
+    const int id = s.pid_window ? SF_ID : 0;
+    double *tot1, *tot2 = nullptr;
+    int *ctl, status = 0;
+    if ((rc = enqueue_pass1(c, sc, s, SF_TIME | id | (pz_mode ? SF_PZ : 0), &tot1, &ctl)))
       return rc;
-    if (!(flags & TRK_SUMS_NOMINMAX) && second) {
-      const int cols[5] = {0, 1, 2, 3, 5};
-      for (int k = 0; k < 5; k++) {
-        const int i = cols[k];
-        if (np_count > 0) {
-          if (mm[3 * k + 2] > sums->maxabs[i])
-            sums->maxabs[i] = mm[3 * k + 2];
-          if (mm[3 * k + 1] > sums->max[i])
-            sums->max[i] = mm[3 * k + 1];
-          if (mm[3 * k] < sums->min[i])
-            sums->min[i] = mm[3 * k];
-        }
-      }
-    }
-    /* centroids of this beam, folded into the running ones
-     * (src/compute_centroids.c:357-385) */
-    double cen[7], cenn[7];
-    for (int i = 0; i < 7; i++) {
-      cen[i] = sum[i];
-      cenn[i] = 0;
-    }
-    cenn[1] = sum[7];
-    cenn[3] = sum[8];
-    if (np_count > 0)
-      for (int i = 0; i < 7; i++) {
-        sums->centroid[i] = (sums->centroid[i] * sums->n_part + cen[i]) / (sums->n_part + np_count);
-        cen[i] /= np_count;
-        cenn[i] /= np_count;
-      }
-    for (int i = 0; i < 7; i++)
-      if (i != 1 && i != 3)
-        cenn[i] = cen[i];
+    double h1[P1], h[P2];
     if (second) {
-      const int nb = (int)((c.n + OBS_CHUNK - 1) / OBS_CHUNK);
-      double *part, *out;
-      signed char *ops;
-      if ((rc = sc.get(&part, (size_t)nb * P2)) || (rc = sc.get(&out, P2)) || (rc = sc.get(&ops, 8)))
+      const int nb = blocks_of(c);
+      double *part;
+      if ((rc = sc.get(&part, (size_t)nb * P2)) || (rc = sc.get(&tot2, P2)))
         return rc;
-      const signed char h_ops[6] = {1, 2, 2, 1, 2, 2};
-      OBS_CUDA(cudaMemcpyAsync(ops, h_ops, sizeof(h_ops), cudaMemcpyHostToDevice, c.st));
-      Moments M;
-      for (int i = 0; i < 7; i++) {
-        M.m[i] = cen[i];
-        M.mn[i] = cenn[i];
-      }
-      M.sparse = (flags & TRK_SUMS_SPARSE) ? 1 : 0;
-      sums_pass2<<<nb, OBS_THREADS, 0, c.st>>>(beam_of(c), s, M, pz_mode, part);
-      combine_partials<<<1, 64, 0, c.st>>>(part, nb, P2, 56, 6, ops, out);
-      double h[P2];
-      OBS_CUDA(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, c.st));
-      OBS_CUDA(cudaStreamSynchronize(c.st));
-      if (!(flags & TRK_SUMS_NOMINMAX) && second && np_count > 0) {
-        const int idx[2] = {4, 6};
-        for (int k = 0; k < 2; k++) {
-          const int i = idx[k];
-          if (h[112 + 3 * k + 2] > sums->maxabs[i])
-            sums->maxabs[i] = h[112 + 3 * k + 2];
-          if (h[112 + 3 * k + 1] > sums->max[i])
-            sums->max[i] = h[112 + 3 * k + 1];
-          if (h[112 + 3 * k] < sums->min[i])
-            sums->min[i] = h[112 + 3 * k];
+      const int sparse = (flags & TRK_SUMS_SPARSE) ? 1 : 0;
+      if (id)
+        rc = launch_sums<2, SF_TIME | SF_ID>(c, s, tot1, sparse, pz_mode, ctl + 1, ctl + 3, part);
+      else
+        rc = launch_sums<2, SF_TIME>(c, s, tot1, sparse, pz_mode, ctl + 1, ctl + 3, part);
+      if (!rc && pz_mode)
+        rc = launch_sums<2, SF_TIME | SF_ID | SF_PZ>(c, s, tot1, sparse, 1, ctl + 2, ctl + 3, part);
+      if (rc)
+        return rc;
+      combine_partials<<<1, COMBINE_THREADS, 0, c.st>>>(part, nb, P2, 56, 6, P2_MIN_MASK, P2_MAX_MASK, tot2);
+      OBS_CUDA(cudaGetLastError());
+      OBS_CUDA(cudaMemcpyAsync(h, tot2, sizeof(h), cudaMemcpyDeviceToHost, c.st));
+    }
+    OBS_CUDA(cudaMemcpyAsync(h1, tot1, sizeof(h1), cudaMemcpyDeviceToHost, c.st));
+    OBS_CUDA(cudaMemcpyAsync(&status, ctl + 3, sizeof(int), cudaMemcpyDeviceToHost, c.st));
+    OBS_CUDA(cudaStreamSynchronize(c.st));
+    if ((rc = sums_status(status)))
+      return rc;
+    /* nothing is accumulated without survivors (src/compute_centroids.c:313) */
+    if (h1[34] > 0) {
+      double sum[9], mm[15];
+      for (int k = 0; k < 9; k++)
+        sum[k] = h1[2 * k] + h1[2 * k + 1];
+      np_count = h1[18];
+      for (int k = 0; k < 15; k++)
+        mm[k] = h1[19 + k];
+      if (!(flags & TRK_SUMS_NOMINMAX) && second) {
+        const int cols[5] = {0, 1, 2, 3, 5};
+        for (int k = 0; k < 5; k++) {
+          const int i = cols[k];
+          if (np_count > 0) {
+            if (mm[3 * k + 2] > sums->maxabs[i])
+              sums->maxabs[i] = mm[3 * k + 2];
+            if (mm[3 * k + 1] > sums->max[i])
+              sums->max[i] = mm[3 * k + 1];
+            if (mm[3 * k] < sums->min[i])
+              sums->min[i] = mm[3 * k];
+          }
         }
       }
+      /* centroids of this beam, folded into the running ones
+       * (src/compute_centroids.c:357-385) */
+      if (np_count > 0)
+        for (int i = 0; i < 7; i++)
+          sums->centroid[i] = (sums->centroid[i] * sums->n_part + sum[i]) / (sums->n_part + np_count);
       if (second) {
+        if (!(flags & TRK_SUMS_NOMINMAX) && np_count > 0) {
+          const int idx[2] = {4, 6};
+          for (int k = 0; k < 2; k++) {
+            const int i = idx[k];
+            if (h[112 + 3 * k + 2] > sums->maxabs[i])
+              sums->maxabs[i] = h[112 + 3 * k + 2];
+            if (h[112 + 3 * k + 1] > sums->max[i])
+              sums->max[i] = h[112 + 3 * k + 1];
+            if (h[112 + 3 * k] < sums->min[i])
+              sums->min[i] = h[112 + 3 * k];
+          }
+        }
         /* (src/compute_centroids.c:398-450) */
         int pair = 0;
         for (int i = 0; i < 7; i++)
@@ -621,13 +1004,10 @@ int trk_match_energy(trk_context *ctx, double *p_central, int change_beam) {
   const int nb = (int)((c.n + OBS_CHUNK - 1) / OBS_CHUNK);
   Scratch sc(c.ctx, 4);
   double *part, *out;
-  signed char *ops;
-  if ((rc = sc.get(&part, (size_t)nb * 3)) || (rc = sc.get(&out, 3)) || (rc = sc.get(&ops, 1)))
+  if ((rc = sc.get(&part, (size_t)nb * 3)) || (rc = sc.get(&out, 3)))
     return rc;
-  const signed char op = 0;
-  OBS_CUDA(cudaMemcpyAsync(ops, &op, 1, cudaMemcpyHostToDevice, c.st));
   momentum_sum<<<nb, OBS_THREADS, 0, c.st>>>(beam_of(c), Po, part);
-  combine_partials<<<1, 32, 0, c.st>>>(part, nb, 3, 1, 1, ops, out);
+  combine_partials<<<1, COMBINE_THREADS, 0, c.st>>>(part, nb, 3, 1, 1, 0u, 0u, out);
   double h[3];
   OBS_CUDA(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, c.st));
   OBS_CUDA(cudaStreamSynchronize(c.st));
