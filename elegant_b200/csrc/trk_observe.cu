@@ -87,39 +87,53 @@ struct Select {
   const double *time; /* caller's time coordinates, or null */
 };
 
-/* Beam sums.  The beam is cut into chunks of SUM_CHUNK particles, and every
- * chunk gets its own partial, so the partials do not depend on the grid or on
- * which block sums which chunk.  Within a block a thread keeps, per sum, a
- * running double and the plain sum of the exact errors of its additions
- * (Knuth's TwoSum): a compensated sum whose error is of order u^2 per term.
- * The lanes then combine their pairs as double-double values in a fixed order
- * (a butterfly that leaves value v in lane v), the warps in index order, and
- * the chunks in chunk order, so every total is the double-double of the exact
- * sum of the rounded terms to about 2^-100 relative, rounded once at the end.
- * Particles that are lost or outside the windows add +0.0 and leave the sums
- * unchanged.
+/* Beam sums.  The beam is cut into chunks whose size depends on the number
+ * of particles only (sum_chunk), and every chunk gets its own partial, so the
+ * partials do not depend on the device, the grid or on which block summed
+ * which chunk.  Within a block a thread keeps, per sum, a running double and
+ * the plain sum of the exact errors of its additions (Knuth's TwoSum): a
+ * compensated sum whose error is of order u^2 per term.  The lanes then
+ * combine their pairs as double-double values in a fixed order (a butterfly,
+ * warp_dd_scatter), the warps in index order, and the chunks in chunk order,
+ * so every total is the double-double of the exact sum of the rounded terms to
+ * about 2^-100 relative, rounded once at the end.  Particles that are lost or
+ * outside the windows are skipped.
  *
  * Data movement: persistent blocks take chunks from a counter, and a ring of
  * SUM_STAGES tiles of SUM_TILE particles in shared memory is filled by 1-D
  * bulk copies (cp.async.bulk, from this device's own beam columns) that
- * complete on an mbarrier per stage; the copies of the next tiles stream
- * while the threads sum the current one.  Bulk copies need 16-byte aligned
- * sources and sizes: the beam columns are SUM_TILE-aligned slices of arrays
- * whose stride (the beam capacity) is a multiple of 32 entries, and a tile's
- * copy is rounded up to whole 16-byte units inside that capacity. */
-constexpr int SUM_THREADS = 128;
-constexpr int SUM_WARPS = SUM_THREADS / 32;
+ * complete on an mbarrier per stage; the copies of the next tile stream while
+ * the threads sum the current one.  Bulk copies need 16-byte aligned sources
+ * and sizes: the beam columns are SUM_TILE-aligned slices of arrays whose
+ * stride (the beam capacity) is a multiple of 32 entries, and a tile's copy
+ * is rounded up to whole 16-byte units inside that capacity.
+ *
+ * Pass 1 runs 128 threads a block, one particle a thread.  Pass 2 runs 256:
+ * the even warps take the first 14 of the 28 second moments of a particle and
+ * the odd warps the other 14, which halves the running sums a thread holds,
+ * and so its registers, and doubles the warps an SM keeps in flight. */
 constexpr int SUM_TILE = 512;
 constexpr int SUM_STAGES = 2;
-constexpr long SUM_CHUNK = 8192;
-/* resident blocks per SM: pass 2 keeps 56 running sums per thread */
-template <int PASS> constexpr int sum_blocks_per_sm() { return PASS == 1 ? 3 : 2; }
+constexpr long SUM_CHUNK_MIN = 1024, SUM_CHUNK_MAX = 8192;
 /* a stage: 6 coordinates, ID, caller's time (doubles), loss word (int32) */
 constexpr int STAGE_BYTES = SUM_TILE * (8 * 8 + 4);
 constexpr int SUM_SMEM = SUM_STAGES * STAGE_BYTES;
-constexpr int COMBINE_THREADS = 1024;
+constexpr int COMBINE_THREADS = 256;
 /* a bulk copy that has not completed after this long is reported as an error */
 constexpr unsigned long long SUM_WAIT_NS = 2000000000ull;
+
+template <int PASS> __host__ __device__ constexpr int sum_threads() { return PASS == 1 ? 128 : 256; }
+template <int PASS> __host__ __device__ constexpr int sum_blocks_per_sm() { return PASS == 1 ? 3 : 2; }
+
+/* Particles per chunk: about 4096 chunks (enough for every block of a
+ * persistent grid to take several, so the last ones balance), a multiple of
+ * the tile, at least SUM_CHUNK_MIN so the per-chunk combination stays a small
+ * part of the work.  A function of n alone. */
+__host__ __device__ inline long sum_chunk(long n) {
+  long c = (n + 4095) / 4096;
+  c = (c + SUM_TILE - 1) / SUM_TILE * SUM_TILE;
+  return c < SUM_CHUNK_MIN ? SUM_CHUNK_MIN : (c > SUM_CHUNK_MAX ? SUM_CHUNK_MAX : c);
+}
 
 /* kernel variants: the time coordinate is needed; the ID column is read;
  * the pz-normalized sums (pass 1: x' pz, y' pz; pass 2: sigman) */
@@ -182,6 +196,7 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned b
                : "memory");
 }
 
+/* s + x with the exact error of the addition added into e (Knuth's TwoSum) */
 __device__ __forceinline__ void csum_add(double &s, double &e, double x) {
   const double t = __dadd_rn(s, x);
   const double bb = __dsub_rn(t, s);
@@ -189,45 +204,63 @@ __device__ __forceinline__ void csum_add(double &s, double &e, double x) {
   s = t;
 }
 
+/* double-double addition with the low parts added in plain double (Dekker):
+ * the combinations of already compensated sums, whose low parts are a few
+ * units of 2^-53 of their high parts */
+__device__ __forceinline__ trkcr_dd dd_add(trkcr_dd a, trkcr_dd b) {
+  const trkcr_dd s = trkcr_two_sum(a.hi, b.hi);
+  return trkcr_quick_two_sum(s.hi, __dadd_rn(s.lo, __dadd_rn(a.lo, b.lo)));
+}
+
+/* log2 of a power of two up to 32 */
+template <int NP> __host__ __device__ constexpr int log2_of() { return NP <= 1 ? 0 : 1 + log2_of<NP / 2>(); }
+
 /* Lane butterfly over NP (a power of two <= 32) double-double values: steps
- * with distance >= NP add all values across the lane pair, the others keep
- * half of the values and add the partner's copy of that half.  Afterwards
- * lane L holds value L % NP in h[0], l[0].  Both lanes of a pair add the
- * lower lane's value first, so the result does not depend on the lane. */
+ * at distances 16, 8, ... keep half of the values (the upper half in the lane
+ * whose distance bit is set) and add the partner's copy of that half, until
+ * one value is left; the remaining steps add it across the lane pair.
+ * Afterwards lane L holds value L >> (5 - log2 NP) in h[0], l[0]: NP - 1 + 5 -
+ * log2 NP additions a lane.  Both lanes of a pair add the lower lane's value
+ * first, so the result does not depend on the lane. */
 template <int NP>
 __device__ __forceinline__ void warp_dd_scatter(double (&h)[NP], double (&l)[NP]) {
   const int lane = threadIdx.x & 31;
+  constexpr int K = log2_of<NP>();
 #pragma unroll
-  for (int m = 16; m >= NP; m >>= 1) {
+  for (int j = 0; j < K; j++) {
+    const int m = 16 >> j, half = NP >> (j + 1);
     const bool up = (lane & m) != 0;
 #pragma unroll
-    for (int i = 0; i < NP; i++) {
-      const double rh = __shfl_xor_sync(0xffffffffu, h[i], m), rl = __shfl_xor_sync(0xffffffffu, l[i], m);
-      const trkcr_dd s = trkcr_add(trkcr_make(up ? rh : h[i], up ? rl : l[i]),
-                                   trkcr_make(up ? h[i] : rh, up ? l[i] : rl));
+    for (int i = 0; i < half; i++) {
+      const double sh = up ? h[i] : h[i + half], sl = up ? l[i] : l[i + half];
+      const double kh = up ? h[i + half] : h[i], kl = up ? l[i + half] : l[i];
+      const double rh = __shfl_xor_sync(0xffffffffu, sh, m), rl = __shfl_xor_sync(0xffffffffu, sl, m);
+      const trkcr_dd s = dd_add(trkcr_make(up ? rh : kh, up ? rl : kl), trkcr_make(up ? kh : rh, up ? kl : rl));
       h[i] = s.hi;
       l[i] = s.lo;
     }
   }
 #pragma unroll
-  for (int m = (NP < 32 ? NP / 2 : 16); m >= 1; m >>= 1) {
+  for (int j = K; j < 5; j++) {
+    const int m = 16 >> j;
     const bool up = (lane & m) != 0;
-#pragma unroll
-    for (int i = 0; i < m; i++) {
-      const double sh = up ? h[i] : h[i + m], sl = up ? l[i] : l[i + m];
-      const double kh = up ? h[i + m] : h[i], kl = up ? l[i + m] : l[i];
-      const double rh = __shfl_xor_sync(0xffffffffu, sh, m), rl = __shfl_xor_sync(0xffffffffu, sl, m);
-      const trkcr_dd s = trkcr_add(trkcr_make(up ? rh : kh, up ? rl : kl), trkcr_make(up ? kh : rh, up ? kl : rl));
-      h[i] = s.hi;
-      l[i] = s.lo;
-    }
+    const double rh = __shfl_xor_sync(0xffffffffu, h[0], m), rl = __shfl_xor_sync(0xffffffffu, l[0], m);
+    const trkcr_dd s = dd_add(trkcr_make(up ? rh : h[0], up ? rl : l[0]), trkcr_make(up ? h[0] : rh, up ? l[0] : rl));
+    h[0] = s.hi;
+    l[0] = s.lo;
   }
 }
 
-/* the block's NV double-double totals from the threads' compensated sums
- * (s, e) -> out[2v], out[2v + 1]; `sh` holds 2 NV SUM_WARPS doubles */
-template <int NV, int NP>
-__device__ __forceinline__ void block_dd_totals(double (&s)[NP], double (&e)[NP], double *sh, double *out) {
+/* The block's NG x NV double-double totals from the threads' compensated
+ * sums (s, e).  The warps form NG groups (group of warp w: w % NG), each with
+ * its own NV values; after the butterfly in each warp, thread g NV + u adds
+ * value u over the warps of group g in index order and writes it to
+ * out[2 (g NV + u) os], out[(2 (g NV + u) + 1) os].  `sh` holds 2 NV WARPS
+ * doubles; every thread of the block calls it. */
+template <int NV, int NP, int WARPS, int NG>
+__device__ __forceinline__ void block_dd_totals(double (&s)[NP], double (&e)[NP], double *sh, double *out,
+                                                long os) {
+  constexpr int SHIFT = 5 - log2_of<NP>();
 #pragma unroll
   for (int v = 0; v < NP; v++) {
     const trkcr_dd t = trkcr_two_sum(s[v], e[v]);
@@ -236,26 +269,28 @@ __device__ __forceinline__ void block_dd_totals(double (&s)[NP], double (&e)[NP]
   }
   warp_dd_scatter<NP>(s, e);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane < NV) {
-    sh[2 * (warp * NV + lane)] = s[0];
-    sh[2 * (warp * NV + lane) + 1] = e[0];
+  const int v = lane >> SHIFT;
+  if ((lane & ((1 << SHIFT) - 1)) == 0 && v < NV) {
+    sh[2 * (warp * NV + v)] = s[0];
+    sh[2 * (warp * NV + v) + 1] = e[0];
   }
   __syncthreads();
-  if (threadIdx.x < NV) {
-    const int v = threadIdx.x;
-    trkcr_dd t = trkcr_make(sh[2 * v], sh[2 * v + 1]);
-    for (int w = 1; w < SUM_WARPS; w++)
-      t = trkcr_add(t, trkcr_make(sh[2 * (w * NV + v)], sh[2 * (w * NV + v) + 1]));
-    out[2 * v] = t.hi;
-    out[2 * v + 1] = t.lo;
+  if (threadIdx.x < NG * NV) {
+    const int g = threadIdx.x / NV, u = threadIdx.x % NV;
+    trkcr_dd t = trkcr_make(sh[2 * (g * NV + u)], sh[2 * (g * NV + u) + 1]);
+    for (int w = g + NG; w < WARPS; w += NG)
+      t = dd_add(t, trkcr_make(sh[2 * (w * NV + u)], sh[2 * (w * NV + u) + 1]));
+    out[2 * threadIdx.x * os] = t.hi;
+    out[(2 * threadIdx.x + 1) * os] = t.lo;
   }
   __syncthreads();
 }
 
-/* the block's extremes: value v is a minimum when bit v of `min_mask` is set,
- * else a maximum; `sh` holds NV SUM_WARPS doubles */
-template <int NV>
-__device__ __forceinline__ void block_extremes(double (&x)[NV], unsigned min_mask, double *sh, double *out) {
+/* the block's extremes -> out[v os]: value v is a minimum when bit v of
+ * `min_mask` is set, else a maximum; `sh` holds NV WARPS doubles */
+template <int NV, int WARPS>
+__device__ __forceinline__ void block_extremes(double (&x)[NV], unsigned min_mask, double *sh, double *out,
+                                               long os) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int v = 0; v < NV; v++) {
@@ -272,14 +307,15 @@ __device__ __forceinline__ void block_extremes(double (&x)[NV], unsigned min_mas
     const int v = threadIdx.x;
     const bool is_min = (min_mask >> v) & 1u;
     double t = sh[v];
-    for (int w = 1; w < SUM_WARPS; w++)
+    for (int w = 1; w < WARPS; w++)
       t = is_min ? fmin(t, sh[w * NV + v]) : fmax(t, sh[w * NV + v]);
-    out[v] = t;
+    out[v * os] = t;
   }
   __syncthreads();
 }
 
 /* the block's count of a per-thread integer -> out[0] */
+template <int WARPS>
 __device__ __forceinline__ void block_count(int n, int *sh, double *out) {
   n = __reduce_add_sync(0xffffffffu, n);
   if ((threadIdx.x & 31) == 0)
@@ -287,7 +323,7 @@ __device__ __forceinline__ void block_count(int n, int *sh, double *out) {
   __syncthreads();
   if (threadIdx.x == 0) {
     long t = 0;
-    for (int w = 0; w < SUM_WARPS; w++)
+    for (int w = 0; w < WARPS; w++)
       t += sh[w];
     out[0] = (double)t;
   }
@@ -321,6 +357,30 @@ __device__ __forceinline__ double pz_of(double Po, const Row &r) {
                    __dsqrt_rn(__dadd_rn(__dadd_rn(1.0, __dmul_rn(xp, xp)), __dmul_rn(yp, yp))));
 }
 
+/* P1 / P2: the chunk partial layouts of the two passes (doubles per chunk,
+ * stored value-major: value i of chunk c at part[i nchunks + c]) */
+constexpr int P1 = 39;
+constexpr int P1_COUNT = 18;
+/* plain values (from P1_COUNT): count, 5 x (min, max, maxabs), survivors,
+ * min s, max s, min t, max t */
+constexpr unsigned P1_MIN_MASK = 0x2492u | (1u << 17) | (1u << 19);
+constexpr unsigned P1_MAX_MASK = 0xDB6Cu | (1u << 18) | (1u << 20);
+constexpr int P2 = 118;
+constexpr unsigned P2_MIN_MASK = 0x9u; /* plain values 0 and 3 */
+constexpr unsigned P2_MAX_MASK = 0x36u;
+
+/* (min, max) pairs -> (min, max, max |.|) triples; max |.| = max(|min|,
+ * |max|), which is the largest |value| of the values seen, 0 when none */
+template <int N>
+__device__ __forceinline__ void with_maxabs(const double *mm, double (&x)[3 * N]) {
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+    x[3 * k] = mm[2 * k];
+    x[3 * k + 1] = mm[2 * k + 1];
+    x[3 * k + 2] = mm[2 * k] <= mm[2 * k + 1] ? fmax(fabs(mm[2 * k]), fabs(mm[2 * k + 1])) : 0.0;
+  }
+}
+
 /* the pairs BEAM_SUMS_SPARSE keeps: diagonal blocks and dispersive
  * correlations (src/compute_centroids.c:301-308) */
 #define OBS_SPARSE                                                                                                \
@@ -333,7 +393,7 @@ static const signed char k_sparse_host[7][7] = OBS_SPARSE;
 
 /* centroids of pass 1 (m) and of the normalized coordinates (mn) */
 __device__ __forceinline__ void moments_of(const double *tot1, double m[7], double mn[7]) {
-  const double count = tot1[18];
+  const double count = tot1[P1_COUNT];
 #pragma unroll
   for (int k = 0; k < 7; k++) {
     m[k] = __dadd_rn(tot1[2 * k], tot1[2 * k + 1]);
@@ -353,6 +413,36 @@ __device__ __forceinline__ void moments_of(const double *tot1, double m[7], doub
       mn[k] = m[k];
 }
 
+/* a power of two above x > 0 (2^-1022 for x = 0 or subnormal; infinity
+ * past the range) */
+__device__ __forceinline__ double pow2_above(double x) {
+  const long long e = __double_as_longlong(x) & 0x7ff0000000000000LL;
+  return __longlong_as_double(e + (1LL << 52));
+}
+
+/* Biases of the 28 second-moment sums (pairs in row order).  A thread's sum
+ * of pair (a, c) starts at B = a power of two above 4 K max|d_a| max|d_c|,
+ * K the particles a thread sums per chunk and max|d| the largest centered
+ * value of pass 1's extremes (rounded subtraction and product are monotonic,
+ * so these bound every term).  The running sum then stays within [B/2, 2B]
+ * and above every term, Dekker's condition for Fast2Sum: each addition's
+ * rounding error is x - ((s + x) - s) exactly, 3 operations instead of
+ * TwoSum's 6, and the sum less B is exact at the end.  A bound that
+ * overflows gives B = 0: that pair is then a plain compensated sum. */
+__device__ __forceinline__ void sum_biases(const double *tot1, const double m[7], long K, double bias[28]) {
+  /* extremes of pass 1 by coordinate: x, x', y, y', s, delta, t */
+  const int lo[7] = {19, 22, 25, 28, 35, 31, 37};
+  double D[7];
+  for (int k = 0; k < 7; k++)
+    D[k] = fmax(fabs(__dsub_rn(tot1[lo[k]], m[k])), fabs(__dsub_rn(tot1[lo[k] + 1], m[k])));
+  int pair = 0;
+  for (int a = 0; a < 7; a++)
+    for (int c = a; c < 7; c++, pair++) {
+      const double b = pow2_above(__dmul_rn(4.0 * (double)K, __dmul_rn(D[a], D[c])));
+      bias[pair] = isfinite(b) ? b : 0.0;
+    }
+}
+
 /* the ring of staged tiles: an mbarrier per stage and the tile it holds
  * (chunk -1: no work left) */
 struct Ring {
@@ -363,8 +453,8 @@ struct Ring {
 };
 
 /* tiles of chunk c */
-__device__ __forceinline__ int tiles_of(long c, long n) {
-  const long lo = c * SUM_CHUNK, hi = min(n, lo + SUM_CHUNK);
+__device__ __forceinline__ int tiles_of(long c, long n, long chunk_n) {
+  const long lo = c * chunk_n, hi = min(n, lo + chunk_n);
   return (int)((hi - lo + SUM_TILE - 1) / SUM_TILE);
 }
 
@@ -379,12 +469,12 @@ struct Producer {
  * last chunk the stage gets an end mark and a plain arrival instead. */
 template <int F>
 __device__ void issue_tile(Ring &r, unsigned char *smem, int stage, Producer &p, const Beam &b, const Select &s,
-                           int *next_chunk, long nchunks) {
+                           int *next_chunk, long nchunks, long chunk_n) {
   if (p.tile == p.ntiles) {
     if (p.chunk < nchunks)
       p.chunk = atomicAdd(next_chunk, 1);
     p.tile = 0;
-    p.ntiles = p.chunk < nchunks ? tiles_of(p.chunk, b.n) : 0;
+    p.ntiles = p.chunk < nchunks ? tiles_of(p.chunk, b.n, chunk_n) : 0;
   }
   if (p.chunk >= nchunks) {
     r.chunk[stage] = -1;
@@ -392,7 +482,7 @@ __device__ void issue_tile(Ring &r, unsigned char *smem, int stage, Producer &p,
     return;
   }
   unsigned char *st = smem + (size_t)stage * STAGE_BYTES;
-  const long start = p.chunk * SUM_CHUNK + (long)p.tile * SUM_TILE;
+  const long start = p.chunk * chunk_n + (long)p.tile * SUM_TILE;
   const int cnt = (int)min((long)SUM_TILE, b.n - start);
   /* whole 16-byte units: 2 doubles, 4 loss words (inside the capacity) */
   const unsigned bd = (unsigned)((cnt + 1) & ~1) * 8u, bl = (unsigned)((cnt + 3) & ~3) * 4u;
@@ -411,13 +501,33 @@ __device__ void issue_tile(Ring &r, unsigned char *smem, int stage, Producer &p,
   p.issued++;
 }
 
-/* P1 / P2: the block partial layouts of the two passes (doubles per chunk) */
-constexpr int P1 = 35;
-constexpr unsigned P1_MIN_MASK = 0x2492u; /* plain values 1, 4, 7, 10, 13: the minima */
-constexpr unsigned P1_MAX_MASK = 0xDB6Cu; /* plain values 2, 3, 5, 6, ..., 14, 15 */
-constexpr int P2 = 118;
-constexpr unsigned P2_MIN_MASK = 0x9u; /* plain values 0 and 3 */
-constexpr unsigned P2_MAX_MASK = 0x36u;
+/* The 14 second moments of pair group G (pairs 14 G .. 14 G + 13 in row
+ * order) of one particle: S[k], E[k] += (x_a - c_a) y_c for pair 14 G + k =
+ * (a, c), with c_a = 0 when `center` is null (the factors are then already
+ * centered); pairs BEAM_SUMS_SPARSE drops are left out when `sparse`.
+ * BIASED: the sums run from the biases of sum_biases (Fast2Sum). */
+template <int G, bool BIASED>
+__device__ __forceinline__ void pair_sums(double (&S)[16], double (&E)[16], const double (&x)[7],
+                                          const double (&y)[7], const double *center, int sparse) {
+  int pair = 0;
+#pragma unroll
+  for (int a = 0; a < 7; a++)
+#pragma unroll
+    for (int c = a; c < 7; c++, pair++)
+      if (pair >= 14 * G && pair < 14 * G + 14 && (!sparse || k_sparse[a][c])) {
+        const double xa = center ? __dsub_rn(x[a], center[a]) : x[a];
+        const double t = __dmul_rn(xa, y[c]);
+        if (BIASED) {
+          /* Fast2Sum: the running sum is above every term (sum_biases) */
+          double &sk = S[pair - 14 * G];
+          const double u = __dadd_rn(sk, t);
+          E[pair - 14 * G] = __dadd_rn(E[pair - 14 * G], __dsub_rn(t, __dsub_rn(u, sk)));
+          sk = u;
+        } else {
+          csum_add(S[pair - 14 * G], E[pair - 14 * G], t);
+        }
+      }
+}
 
 /* The beam-sum passes, one partial per chunk.
  *
@@ -442,31 +552,45 @@ constexpr unsigned P2_MAX_MASK = 0x36u;
  * in time; the block then waits (bounded) for its copies in flight and
  * returns. */
 template <int PASS, int F>
-__global__ void __launch_bounds__(SUM_THREADS, sum_blocks_per_sm<PASS>())
+__global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>())
   beam_sums(Beam b, Select s, const double *tot1, int sparse, int pz_pass, int *next_chunk, int *status,
             double *part) {
+  constexpr int THREADS = sum_threads<PASS>(), WARPS = THREADS / 32;
+  constexpr int NV = PASS == 1 ? 9 : 14;  /* sums a thread keeps */
+  constexpr int NP = 16;                  /* butterfly width */
+  constexpr int NM = PASS == 1 ? 14 : 4; /* running (min, max) values */
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ Ring r;
-  __shared__ double red[2 * 28 * SUM_WARPS];
-  __shared__ int redc[SUM_WARPS];
-  constexpr int NP = PASS == 1 ? 16 : 32; /* butterfly width */
-  constexpr int NX = PASS == 1 ? 15 : 6;  /* extremes */
-  __shared__ double sm_m[7], sm_mn[7];
-  const long nchunks = (b.n + SUM_CHUNK - 1) / SUM_CHUNK;
-  if (PASS == 2 && threadIdx.x == 0)
+  __shared__ double red[2 * 14 * 8];
+  __shared__ int redc[WARPS];
+  __shared__ double sm_m[7], sm_mn[7], sm_bias[28];
+  const long n = b.n, chunk_n = sum_chunk(n), nchunks = (n + chunk_n - 1) / chunk_n;
+  constexpr bool BIASED = PASS == 2 && !(F & SF_PZ);
+  if (PASS == 2 && threadIdx.x == 0) {
     moments_of(tot1, sm_m, sm_mn);
-  const double *m = sm_m, *mn = sm_mn;
-  double S[NP], E[NP], X[NX];
+    if (BIASED)
+      sum_biases(tot1, sm_m, (chunk_n + 127) / 128, sm_bias);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  /* pass 2: the pair group of the warp and the particle slot of the thread */
+  const int grp = PASS == 2 ? (warp & 1) : 0;
+  const int slot = PASS == 2 ? (warp >> 1) * 32 + lane : (int)threadIdx.x;
+  double S[NP], E[NP], M[NM];
   int cnt = 0, alive = 0;
   auto reset = [&]() {
 #pragma unroll
     for (int k = 0; k < NP; k++)
       S[k] = E[k] = 0.0;
+    if (BIASED)
 #pragma unroll
-    for (int k = 0; k < NX; k++)
-      X[k] = (k % 3 == 0) ? OBS_BIG : ((k % 3 == 1) ? -OBS_BIG : 0.0);
+      for (int k = 0; k < 14; k++)
+        S[k] = sm_bias[14 * grp + k];
+#pragma unroll
+    for (int k = 0; k < NM; k++)
+      M[k] = (k % 2 == 0) ? OBS_BIG : -OBS_BIG;
     cnt = alive = 0;
   };
+  __syncthreads();
   reset();
   Producer p;
   p.chunk = -1;
@@ -479,9 +603,10 @@ __global__ void __launch_bounds__(SUM_THREADS, sum_blocks_per_sm<PASS>())
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
+  const double *m = sm_m, *mn = sm_mn;
   if (threadIdx.x == 0)
     for (int k = 0; k < SUM_STAGES; k++)
-      issue_tile<F>(r, smem, k, p, b, s, next_chunk, nchunks);
+      issue_tile<F>(r, smem, k, p, b, s, next_chunk, nchunks, chunk_n);
   long it = 0;
   for (;; it++) {
     const int stage = (int)(it % SUM_STAGES);
@@ -497,9 +622,9 @@ __global__ void __launch_bounds__(SUM_THREADS, sum_blocks_per_sm<PASS>())
     if (ok && chunk >= 0) {
       const double *col = (const double *)(smem + (size_t)stage * STAGE_BYTES);
       const int32_t *lost = (const int32_t *)(col + 8 * SUM_TILE);
-      const long start = chunk * SUM_CHUNK + (long)tile * SUM_TILE;
-      const int n_tile = (int)min((long)SUM_TILE, b.n - start);
-      for (int q = threadIdx.x; q < n_tile; q += SUM_THREADS) {
+      const long start = chunk * chunk_n + (long)tile * SUM_TILE;
+      const int n_tile = (int)min((long)SUM_TILE, n - start);
+      for (int q = slot; q < n_tile; q += 128) {
         Row w;
         w.lost = lost[q];
 #pragma unroll
@@ -507,27 +632,31 @@ __global__ void __launch_bounds__(SUM_THREADS, sum_blocks_per_sm<PASS>())
           w.v[k] = col[k * SUM_TILE + q];
         w.id = (F & SF_ID) ? col[6 * SUM_TILE + q] : 0.0;
         w.t = ((F & SF_TIME) && s.time) ? col[7 * SUM_TILE + q] : 0.0;
-        const bool sel = select_row<F>(s, w);
-        if constexpr (PASS == 1) {
+        if (PASS == 1)
           alive += w.lost < 0;
-          cnt += sel;
+        if (!select_row<F>(s, w))
+          continue;
+        if constexpr (PASS == 1) {
+          cnt++;
 #pragma unroll
           for (int k = 0; k < 6; k++)
-            csum_add(S[k], E[k], sel ? w.v[k] : 0.0);
+            csum_add(S[k], E[k], w.v[k]);
           if (F & SF_TIME)
-            csum_add(S[6], E[6], sel ? w.t : 0.0);
+            csum_add(S[6], E[6], w.t);
           if (F & SF_PZ) {
             const double pz = pz_of(s.Po, w);
-            csum_add(S[7], E[7], sel ? __dmul_rn(w.v[1], pz) : 0.0);
-            csum_add(S[8], E[8], sel ? __dmul_rn(w.v[3], pz) : 0.0);
+            csum_add(S[7], E[7], __dmul_rn(w.v[1], pz));
+            csum_add(S[8], E[8], __dmul_rn(w.v[3], pz));
           }
-          const int cols[5] = {0, 1, 2, 3, 5};
+          const int cols[6] = {0, 1, 2, 3, 5, 4};
 #pragma unroll
-          for (int k = 0; k < 5; k++) {
-            const double v = w.v[cols[k]];
-            X[3 * k] = fmin(X[3 * k], sel ? v : OBS_BIG);
-            X[3 * k + 1] = fmax(X[3 * k + 1], sel ? v : -OBS_BIG);
-            X[3 * k + 2] = fmax(X[3 * k + 2], sel ? fabs(v) : 0.0);
+          for (int k = 0; k < 6; k++) {
+            M[2 * k] = fmin(M[2 * k], w.v[cols[k]]);
+            M[2 * k + 1] = fmax(M[2 * k + 1], w.v[cols[k]]);
+          }
+          if (F & SF_TIME) {
+            M[12] = fmin(M[12], w.t);
+            M[13] = fmax(M[13], w.t);
           }
         } else if constexpr (!(F & SF_PZ)) {
           double d[7];
@@ -535,19 +664,15 @@ __global__ void __launch_bounds__(SUM_THREADS, sum_blocks_per_sm<PASS>())
           for (int k = 0; k < 6; k++)
             d[k] = __dsub_rn(w.v[k], m[k]);
           d[6] = __dsub_rn(w.t, m[6]);
-          int pair = 0;
-#pragma unroll
-          for (int a = 0; a < 7; a++)
-#pragma unroll
-            for (int c = a; c < 7; c++, pair++)
-              if (!sparse || k_sparse[a][c])
-                csum_add(S[pair], E[pair], sel ? __dmul_rn(d[a], d[c]) : 0.0);
-          X[0] = fmin(X[0], sel ? d[4] : OBS_BIG);
-          X[1] = fmax(X[1], sel ? d[4] : -OBS_BIG);
-          X[2] = fmax(X[2], sel ? fabs(d[4]) : 0.0);
-          X[3] = fmin(X[3], sel ? d[6] : OBS_BIG);
-          X[4] = fmax(X[4], sel ? d[6] : -OBS_BIG);
-          X[5] = fmax(X[5], sel ? fabs(d[6]) : 0.0);
+          if (grp == 0) {
+            pair_sums<0, BIASED>(S, E, d, d, nullptr, sparse);
+            M[0] = fmin(M[0], d[4]);
+            M[1] = fmax(M[1], d[4]);
+            M[2] = fmin(M[2], d[6]);
+            M[3] = fmax(M[3], d[6]);
+          } else {
+            pair_sums<1, BIASED>(S, E, d, d, nullptr, sparse);
+          }
         } else {
           const double pz = pz_of(s.Po, w);
           double u[7];
@@ -555,13 +680,10 @@ __global__ void __launch_bounds__(SUM_THREADS, sum_blocks_per_sm<PASS>())
           for (int k = 0; k < 6; k++)
             u[k] = (k == 1 || k == 3) ? __dmul_rn(w.v[k], pz) : w.v[k];
           u[6] = w.id;
-          int pair = 0;
-#pragma unroll
-          for (int a = 0; a < 7; a++)
-#pragma unroll
-            for (int c = a; c < 7; c++, pair++)
-              if (!sparse || k_sparse[a][c])
-                csum_add(S[pair], E[pair], sel ? __dmul_rn(__dsub_rn(u[a], mn[a]), u[c]) : 0.0);
+          if (grp == 0)
+            pair_sums<0, false>(S, E, u, u, mn, sparse);
+          else
+            pair_sums<1, false>(S, E, u, u, mn, sparse);
         }
       }
     }
@@ -572,25 +694,32 @@ __global__ void __launch_bounds__(SUM_THREADS, sum_blocks_per_sm<PASS>())
       break;
     if (threadIdx.x == 0) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue_tile<F>(r, smem, stage, p, b, s, next_chunk, nchunks);
+      issue_tile<F>(r, smem, stage, p, b, s, next_chunk, nchunks, chunk_n);
     }
-    if (tile == tiles_of(chunk, b.n) - 1) {
-      /* the chunk is complete: its partial */
+    if (tile == tiles_of(chunk, n, chunk_n) - 1) {
+      /* the chunk is complete: its partial (value i at out[i nchunks]) */
+      double *out = part + chunk;
       if constexpr (PASS == 1) {
-        double *out = part + (size_t)chunk * P1;
-        block_dd_totals<9, NP>(S, E, red, out);
-        block_count(cnt, redc, out + 18);
-        block_extremes<NX>(X, 0x1249u, red, out + 19);
-        block_count(alive, redc, out + 34);
+        double X[15], Y[4] = {M[10], M[11], M[12], M[13]};
+        with_maxabs<5>(M, X);
+        block_dd_totals<NV, NP, WARPS, 1>(S, E, red, out, nchunks);
+        block_count<WARPS>(cnt, redc, out + P1_COUNT * nchunks);
+        block_extremes<15, WARPS>(X, 0x1249u, red, out + 19 * nchunks, nchunks);
+        block_count<WARPS>(alive, redc, out + 34 * nchunks);
+        block_extremes<4, WARPS>(Y, 0x5u, red, out + 35 * nchunks, nchunks);
       } else if constexpr (!(F & SF_PZ)) {
-        double *out = part + (size_t)chunk * P2;
-        block_dd_totals<28, NP>(S, E, red, out);
-        block_extremes<NX>(X, 0x9u, red, out + 112);
+        double X[6];
+        with_maxabs<2>(M, X);
+#pragma unroll
+        for (int k = 0; k < 14; k++)
+          S[k] = __dsub_rn(S[k], sm_bias[14 * grp + k]);
+        block_dd_totals<NV, NP, WARPS, 2>(S, E, red, out, nchunks);
+        block_extremes<6, WARPS>(X, 0x9u, red, out + 112 * nchunks, nchunks);
         if (!pz_pass)
-          for (int k = threadIdx.x; k < 56; k += SUM_THREADS)
-            out[56 + k] = 0.0;
+          for (int k = threadIdx.x; k < 56; k += THREADS)
+            out[(56 + k) * nchunks] = 0.0;
       } else {
-        block_dd_totals<28, NP>(S, E, red, part + (size_t)chunk * P2 + 56);
+        block_dd_totals<NV, NP, WARPS, 2>(S, E, red, out + 56 * nchunks, nchunks);
       }
       reset();
     }
@@ -606,48 +735,65 @@ __global__ void __launch_bounds__(SUM_THREADS, sum_blocks_per_sm<PASS>())
   }
 }
 
-/* Combine the block partials in block order: `n_dd` double-double values at
- * the front, then `n_plain` values, plain value k a minimum when bit k of
- * `min_mask` is set, a maximum when bit k of `max_mask` is set, else a sum.
- * One warp per value: lane l takes blocks l, l + 32, ... in order and the
- * lanes combine in a fixed tree. */
+/* Combine the chunk partials (value-major, `nchunks` per value) in chunk
+ * order: `n_dd` double-double values at the front, then `n_plain` values,
+ * plain value k a minimum when bit k of `min_mask` is set, a maximum when bit
+ * k of `max_mask` is set, else a sum.  One block per value: thread t takes
+ * chunks t, t + COMBINE_THREADS, ... in order, then the lanes combine in a
+ * fixed tree and the warps in index order. */
 __global__ void __launch_bounds__(COMBINE_THREADS)
-  combine_partials(const double *part, int nblocks, int stride, int n_dd, int n_plain, unsigned min_mask,
-                   unsigned max_mask, double *out) {
-  const int lane = threadIdx.x & 31;
-  for (int v = threadIdx.x >> 5; v < n_dd + n_plain; v += COMBINE_THREADS / 32) {
-    if (v < n_dd) {
-      trkcr_dd acc = trkcr_make(0.0, 0.0);
-      for (int b = lane; b < nblocks; b += 32)
-        acc = trkcr_add(acc, trkcr_make(part[(size_t)b * stride + 2 * v], part[(size_t)b * stride + 2 * v + 1]));
-      for (int off = 16; off > 0; off >>= 1) {
-        const double h = __shfl_down_sync(0xffffffffu, acc.hi, off), l = __shfl_down_sync(0xffffffffu, acc.lo, off);
-        acc = trkcr_add(acc, trkcr_make(h, l));
-      }
-      if (lane == 0) {
-        out[2 * v] = acc.hi;
-        out[2 * v + 1] = acc.lo;
-      }
-    } else {
-      const int k = v - n_dd, q = 2 * n_dd + k;
-      const int op = ((min_mask >> k) & 1u) ? 1 : (((max_mask >> k) & 1u) ? 2 : 0);
-      double acc = op == 0 ? 0.0 : (op == 1 ? OBS_BIG : -OBS_BIG);
-      for (int b = lane; b < nblocks; b += 32) {
-        const double x = part[(size_t)b * stride + q];
-        acc = op == 0 ? __dadd_rn(acc, x) : (op == 1 ? fmin(acc, x) : fmax(acc, x));
-      }
-      for (int off = 16; off > 0; off >>= 1) {
-        const double x = __shfl_down_sync(0xffffffffu, acc, off);
-        acc = op == 0 ? __dadd_rn(acc, x) : (op == 1 ? fmin(acc, x) : fmax(acc, x));
-      }
-      if (lane == 0)
-        out[q] = acc;
+  combine_partials(const double *part, int nchunks, int n_dd, int n_plain, unsigned min_mask, unsigned max_mask,
+                   double *out) {
+  __shared__ double sh[2 * (COMBINE_THREADS / 32)];
+  const int v = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (v < n_dd) {
+    const double *ph = part + (size_t)(2 * v) * nchunks, *pl = ph + nchunks;
+    trkcr_dd acc = trkcr_make(0.0, 0.0);
+#pragma unroll 4
+    for (int c = threadIdx.x; c < nchunks; c += COMBINE_THREADS)
+      acc = dd_add(acc, trkcr_make(ph[c], pl[c]));
+    for (int off = 16; off > 0; off >>= 1) {
+      const double h = __shfl_down_sync(0xffffffffu, acc.hi, off), l = __shfl_down_sync(0xffffffffu, acc.lo, off);
+      acc = dd_add(acc, trkcr_make(h, l));
+    }
+    if (lane == 0) {
+      sh[2 * warp] = acc.hi;
+      sh[2 * warp + 1] = acc.lo;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      trkcr_dd t = trkcr_make(sh[0], sh[1]);
+      for (int w = 1; w < COMBINE_THREADS / 32; w++)
+        t = dd_add(t, trkcr_make(sh[2 * w], sh[2 * w + 1]));
+      out[2 * v] = t.hi;
+      out[2 * v + 1] = t.lo;
+    }
+  } else if (v < n_dd + n_plain) {
+    const int k = v - n_dd, q = 2 * n_dd + k;
+    const int op = ((min_mask >> k) & 1u) ? 1 : (((max_mask >> k) & 1u) ? 2 : 0);
+    const double *px = part + (size_t)q * nchunks;
+    double acc = op == 0 ? 0.0 : (op == 1 ? OBS_BIG : -OBS_BIG);
+#pragma unroll 4
+    for (int c = threadIdx.x; c < nchunks; c += COMBINE_THREADS)
+      acc = op == 0 ? __dadd_rn(acc, px[c]) : (op == 1 ? fmin(acc, px[c]) : fmax(acc, px[c]));
+    for (int off = 16; off > 0; off >>= 1) {
+      const double x = __shfl_down_sync(0xffffffffu, acc, off);
+      acc = op == 0 ? __dadd_rn(acc, x) : (op == 1 ? fmin(acc, x) : fmax(acc, x));
+    }
+    if (lane == 0)
+      sh[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = sh[0];
+      for (int w = 1; w < COMBINE_THREADS / 32; w++)
+        t = op == 0 ? __dadd_rn(t, sh[w]) : (op == 1 ? fmin(t, sh[w]) : fmax(t, sh[w]));
+      out[q] = t;
     }
   }
 }
 
 /* Sum over survivors of Po (1 + delta) (src/do_tracking.c:3448-3455); one
- * chunk per block, partial = (hi, lo, count). */
+ * chunk per block, partial = (hi, lo, count), value-major. */
 __global__ void __launch_bounds__(OBS_THREADS) momentum_sum(Beam b, double Po, double *part) {
   __shared__ double sh[2 * (OBS_THREADS / 32)];
   const long lo = (long)blockIdx.x * OBS_CHUNK, hi = min(b.n, lo + OBS_CHUNK);
@@ -661,9 +807,9 @@ __global__ void __launch_bounds__(OBS_THREADS) momentum_sum(Beam b, double Po, d
   const trkcr_dd t = block_dd_sum(acc, sh);
   const trkcr_dd c = block_dd_sum(trkcr_make(cnt, 0.0), sh);
   if (threadIdx.x == 0) {
-    part[3 * blockIdx.x] = t.hi;
-    part[3 * blockIdx.x + 1] = t.lo;
-    part[3 * blockIdx.x + 2] = c.hi;
+    part[blockIdx.x] = t.hi;
+    part[gridDim.x + blockIdx.x] = t.lo;
+    part[2 * gridDim.x + blockIdx.x] = c.hi;
   }
 }
 
@@ -767,17 +913,26 @@ template <int PASS, int F>
 int launch_sums(const Ctx &c, const Select &s, const double *tot1, int sparse, int pz_pass, int *counter,
                 int *status, double *part) {
   auto kernel = beam_sums<PASS, F>;
-  OBS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SUM_SMEM));
+  static int configured[64] = {0}; /* per device: the shared-memory attribute is set */
+  if (c.device < 0 || c.device >= 64 || !configured[c.device]) {
+    OBS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SUM_SMEM));
+    if (c.device >= 0 && c.device < 64)
+      configured[c.device] = 1;
+  }
   int sms = 0;
   OBS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device));
-  const long nchunks = (c.n + SUM_CHUNK - 1) / SUM_CHUNK;
+  const long chunk_n = sum_chunk(c.n), nchunks = (c.n + chunk_n - 1) / chunk_n;
   const int grid = (int)std::max(1L, std::min<long>(nchunks, (long)sms * sum_blocks_per_sm<PASS>()));
-  kernel<<<grid, SUM_THREADS, SUM_SMEM, c.st>>>(beam_of(c), s, tot1, sparse, pz_pass, counter, status, part);
+  kernel<<<grid, sum_threads<PASS>(), SUM_SMEM, c.st>>>(beam_of(c), s, tot1, sparse, pz_pass, counter, status, part);
   OBS_CUDA(cudaGetLastError());
   return TRK_OK;
 }
 
-int blocks_of(const Ctx &c) { return (int)((c.n + SUM_CHUNK - 1) / SUM_CHUNK); }
+/* chunk partials of a beam of c.n particles */
+int blocks_of(const Ctx &c) {
+  const long chunk_n = sum_chunk(c.n);
+  return (int)((c.n + chunk_n - 1) / chunk_n);
+}
 
 /* pass 1 on the device: chunk partials, then their combination into tot1;
  * `ctl` (4 ints: chunk counters of the passes, status) is zeroed here */
@@ -809,7 +964,7 @@ int enqueue_pass1(const Ctx &c, Scratch &sc, const Select &s, int F, double **to
   }
   if (rc)
     return rc;
-  combine_partials<<<1, COMBINE_THREADS, 0, c.st>>>(part, nb, P1, 9, 17, P1_MIN_MASK, P1_MAX_MASK, *tot1);
+  combine_partials<<<9 + 21, COMBINE_THREADS, 0, c.st>>>(part, nb, 9, 21, P1_MIN_MASK, P1_MAX_MASK, *tot1);
   OBS_CUDA(cudaGetLastError());
   return TRK_OK;
 }
@@ -917,7 +1072,7 @@ int trk_accumulate_beam_sums(trk_context *ctx, trk_beam_sums *sums, double p_cen
         rc = launch_sums<2, SF_TIME | SF_ID | SF_PZ>(c, s, tot1, sparse, 1, ctl + 2, ctl + 3, part);
       if (rc)
         return rc;
-      combine_partials<<<1, COMBINE_THREADS, 0, c.st>>>(part, nb, P2, 56, 6, P2_MIN_MASK, P2_MAX_MASK, tot2);
+      combine_partials<<<56 + 6, COMBINE_THREADS, 0, c.st>>>(part, nb, 56, 6, P2_MIN_MASK, P2_MAX_MASK, tot2);
       OBS_CUDA(cudaGetLastError());
       OBS_CUDA(cudaMemcpyAsync(h, tot2, sizeof(h), cudaMemcpyDeviceToHost, c.st));
     }
@@ -1007,7 +1162,7 @@ int trk_match_energy(trk_context *ctx, double *p_central, int change_beam) {
   if ((rc = sc.get(&part, (size_t)nb * 3)) || (rc = sc.get(&out, 3)))
     return rc;
   momentum_sum<<<nb, OBS_THREADS, 0, c.st>>>(beam_of(c), Po, part);
-  combine_partials<<<1, COMBINE_THREADS, 0, c.st>>>(part, nb, 3, 1, 1, 0u, 0u, out);
+  combine_partials<<<2, COMBINE_THREADS, 0, c.st>>>(part, nb, 1, 1, 0u, 0u, out);
   double h[3];
   OBS_CUDA(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, c.st));
   OBS_CUDA(cudaStreamSynchronize(c.st));
