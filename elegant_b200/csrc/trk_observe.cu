@@ -84,7 +84,8 @@ struct Select {
   double Po, tmin, tmax;
   long start_pid, end_pid;
   int pid_window;     /* start_pid or end_pid given */
-  const double *time; /* caller's time coordinates, or null */
+  const double *time; /* time coordinates to read (the caller's, or pass 1's), or null */
+  double *time_out;   /* pass 1 writes the time coordinates it computes here, when set */
 };
 
 /* Beam sums.  The beam is cut into chunks whose size depends on the number
@@ -100,11 +101,11 @@ struct Select {
  * outside the windows are skipped.
  *
  * Data movement: persistent blocks take chunks from a counter, and a ring of
- * SUM_STAGES tiles of SUM_TILE particles in shared memory is filled by 1-D
+ * SUM_STAGES tiles of sum_tile particles in shared memory is filled by 1-D
  * bulk copies (cp.async.bulk, from this device's own beam columns) that
  * complete on an mbarrier per stage; the copies of the next tile stream while
  * the threads sum the current one.  Bulk copies need 16-byte aligned sources
- * and sizes: the beam columns are SUM_TILE-aligned slices of arrays whose
+ * and sizes: the beam columns are tile-aligned slices of arrays whose
  * stride (the beam capacity) is a multiple of 32 entries, and a tile's copy
  * is rounded up to whole 16-byte units inside that capacity.
  *
@@ -112,27 +113,30 @@ struct Select {
  * the even warps take the first 14 of the 28 second moments of a particle and
  * the odd warps the other 14, which halves the running sums a thread holds,
  * and so its registers, and doubles the warps an SM keeps in flight. */
-constexpr int SUM_TILE = 512;
 constexpr int SUM_STAGES = 2;
 constexpr long SUM_CHUNK_MIN = 1024, SUM_CHUNK_MAX = 8192;
-/* a stage: 6 coordinates, ID, caller's time (doubles), loss word (int32) */
-constexpr int STAGE_BYTES = SUM_TILE * (8 * 8 + 4);
-constexpr int SUM_SMEM = SUM_STAGES * STAGE_BYTES;
+/* particles per tile: pass 1 512, pass 2 896 (7 particles a thread between
+ * barriers, and two blocks of two stages fit an SM with the time column) */
+template <int PASS> __host__ __device__ constexpr int sum_tile() { return PASS == 1 ? 512 : 896; }
+/* the most shared memory a pass's stages take (every column staged) */
+template <int PASS> __host__ __device__ constexpr int sum_smem_max() { return SUM_STAGES * sum_tile<PASS>() * (8 * 8 + 4); }
 constexpr int COMBINE_THREADS = 256;
 /* a bulk copy that has not completed after this long is reported as an error */
 constexpr unsigned long long SUM_WAIT_NS = 2000000000ull;
 
 template <int PASS> __host__ __device__ constexpr int sum_threads() { return PASS == 1 ? 128 : 256; }
-template <int PASS> __host__ __device__ constexpr int sum_blocks_per_sm() { return PASS == 1 ? 3 : 2; }
+template <int PASS> __host__ __device__ constexpr int sum_blocks_per_sm() { return PASS == 1 ? 4 : 2; }
 
-/* Particles per chunk: about 4096 chunks (enough for every block of a
- * persistent grid to take several, so the last ones balance), a multiple of
- * the tile, at least SUM_CHUNK_MIN so the per-chunk combination stays a small
- * part of the work.  A function of n alone. */
+/* Particles per chunk of a pass: about 4096 chunks (enough for every block
+ * of a persistent grid to take several, so the last ones balance), between
+ * SUM_CHUNK_MIN and SUM_CHUNK_MAX so the per-chunk combination stays a small
+ * part of the work, a multiple of the pass's tile.  A function of n alone. */
+template <int PASS>
 __host__ __device__ inline long sum_chunk(long n) {
+  constexpr long T = sum_tile<PASS>();
   long c = (n + 4095) / 4096;
-  c = (c + SUM_TILE - 1) / SUM_TILE * SUM_TILE;
-  return c < SUM_CHUNK_MIN ? SUM_CHUNK_MIN : (c > SUM_CHUNK_MAX ? SUM_CHUNK_MAX : c);
+  c = c < SUM_CHUNK_MIN ? SUM_CHUNK_MIN : (c > SUM_CHUNK_MAX ? SUM_CHUNK_MAX : c);
+  return (c + T - 1) / T * T;
 }
 
 /* kernel variants: the time coordinate is needed; the ID column is read;
@@ -453,9 +457,28 @@ struct Ring {
 };
 
 /* tiles of chunk c */
+template <int TILE>
 __device__ __forceinline__ int tiles_of(long c, long n, long chunk_n) {
   const long lo = c * chunk_n, hi = min(n, lo + chunk_n);
-  return (int)((hi - lo + SUM_TILE - 1) / SUM_TILE);
+  return (int)((hi - lo + TILE - 1) / TILE);
+}
+
+/* where a stage keeps its columns: doubles 0..5 the coordinates, then the ID
+ * and the caller's time when the variant reads them (column -1 when not),
+ * the loss words after the last column */
+struct Layout {
+  int id_col, t_col, ncols;
+  unsigned stage_bytes;
+};
+
+template <int F, int TILE>
+__host__ __device__ inline Layout layout_of(const Select &s) {
+  Layout l;
+  l.ncols = 6;
+  l.id_col = (F & SF_ID) ? l.ncols++ : -1;
+  l.t_col = ((F & SF_TIME) && s.time) ? l.ncols++ : -1;
+  l.stage_bytes = (unsigned)TILE * (8u * (unsigned)l.ncols + 4u);
+  return l;
 }
 
 /* the issuing thread's position in its stream of tiles */
@@ -467,36 +490,35 @@ struct Producer {
 /* Issue the next tile of the block's stream into `stage` (thread 0).  A new
  * chunk is taken from the counter when the current one is used up; past the
  * last chunk the stage gets an end mark and a plain arrival instead. */
-template <int F>
-__device__ void issue_tile(Ring &r, unsigned char *smem, int stage, Producer &p, const Beam &b, const Select &s,
-                           int *next_chunk, long nchunks, long chunk_n) {
+template <int F, int TILE>
+__device__ void issue_tile(Ring &r, unsigned char *smem, const Layout &L, int stage, Producer &p, const Beam &b,
+                           const Select &s, int *next_chunk, long nchunks, long chunk_n) {
   if (p.tile == p.ntiles) {
     if (p.chunk < nchunks)
       p.chunk = atomicAdd(next_chunk, 1);
     p.tile = 0;
-    p.ntiles = p.chunk < nchunks ? tiles_of(p.chunk, b.n, chunk_n) : 0;
+    p.ntiles = p.chunk < nchunks ? tiles_of<TILE>(p.chunk, b.n, chunk_n) : 0;
   }
   if (p.chunk >= nchunks) {
     r.chunk[stage] = -1;
     mbar_arrive(&r.bar[stage]);
     return;
   }
-  unsigned char *st = smem + (size_t)stage * STAGE_BYTES;
-  const long start = p.chunk * chunk_n + (long)p.tile * SUM_TILE;
-  const int cnt = (int)min((long)SUM_TILE, b.n - start);
+  unsigned char *st = smem + (size_t)stage * L.stage_bytes;
+  const long start = p.chunk * chunk_n + (long)p.tile * TILE;
+  const int cnt = (int)min((long)TILE, b.n - start);
   /* whole 16-byte units: 2 doubles, 4 loss words (inside the capacity) */
   const unsigned bd = (unsigned)((cnt + 1) & ~1) * 8u, bl = (unsigned)((cnt + 3) & ~3) * 4u;
-  const bool time = (F & SF_TIME) && s.time;
   r.chunk[stage] = p.chunk;
   r.tile[stage] = p.tile;
-  mbar_arrive_expect_tx(&r.bar[stage], bd * (6u + ((F & SF_ID) ? 1u : 0u) + (time ? 1u : 0u)) + bl);
+  mbar_arrive_expect_tx(&r.bar[stage], bd * (unsigned)L.ncols + bl);
   for (int k = 0; k < 6; k++)
-    bulk_load(st + (size_t)k * SUM_TILE * 8, b.c[k] + start, bd, &r.bar[stage]);
-  if (F & SF_ID)
-    bulk_load(st + (size_t)6 * SUM_TILE * 8, b.c[6] + start, bd, &r.bar[stage]);
-  if (time)
-    bulk_load(st + (size_t)7 * SUM_TILE * 8, s.time + start, bd, &r.bar[stage]);
-  bulk_load(st + (size_t)8 * SUM_TILE * 8, b.lost + start, bl, &r.bar[stage]);
+    bulk_load(st + (size_t)k * TILE * 8, b.c[k] + start, bd, &r.bar[stage]);
+  if (L.id_col >= 0)
+    bulk_load(st + (size_t)L.id_col * TILE * 8, b.c[6] + start, bd, &r.bar[stage]);
+  if (L.t_col >= 0)
+    bulk_load(st + (size_t)L.t_col * TILE * 8, s.time + start, bd, &r.bar[stage]);
+  bulk_load(st + (size_t)L.ncols * TILE * 8, b.lost + start, bl, &r.bar[stage]);
   p.tile++;
   p.issued++;
 }
@@ -504,17 +526,17 @@ __device__ void issue_tile(Ring &r, unsigned char *smem, int stage, Producer &p,
 /* The 14 second moments of pair group G (pairs 14 G .. 14 G + 13 in row
  * order) of one particle: S[k], E[k] += (x_a - c_a) y_c for pair 14 G + k =
  * (a, c), with c_a = 0 when `center` is null (the factors are then already
- * centered); pairs BEAM_SUMS_SPARSE drops are left out when `sparse`.
+ * centered); pairs BEAM_SUMS_SPARSE drops are left out when SPARSE.
  * BIASED: the sums run from the biases of sum_biases (Fast2Sum). */
-template <int G, bool BIASED>
+template <int G, bool BIASED, bool SPARSE>
 __device__ __forceinline__ void pair_sums(double (&S)[16], double (&E)[16], const double (&x)[7],
-                                          const double (&y)[7], const double *center, int sparse) {
+                                          const double (&y)[7], const double *center) {
   int pair = 0;
 #pragma unroll
   for (int a = 0; a < 7; a++)
 #pragma unroll
     for (int c = a; c < 7; c++, pair++)
-      if (pair >= 14 * G && pair < 14 * G + 14 && (!sparse || k_sparse[a][c])) {
+      if (pair >= 14 * G && pair < 14 * G + 14 && (!SPARSE || k_sparse[a][c])) {
         const double xa = center ? __dsub_rn(x[a], center[a]) : x[a];
         const double t = __dmul_rn(xa, y[c]);
         if (BIASED) {
@@ -555,7 +577,7 @@ template <int PASS, int F>
 __global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>())
   beam_sums(Beam b, Select s, const double *tot1, int sparse, int pz_pass, int *next_chunk, int *status,
             double *part) {
-  constexpr int THREADS = sum_threads<PASS>(), WARPS = THREADS / 32;
+  constexpr int THREADS = sum_threads<PASS>(), WARPS = THREADS / 32, TILE = sum_tile<PASS>();
   constexpr int NV = PASS == 1 ? 9 : 14;  /* sums a thread keeps */
   constexpr int NP = 16;                  /* butterfly width */
   constexpr int NM = PASS == 1 ? 14 : 4; /* running (min, max) values */
@@ -564,7 +586,8 @@ __global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>()
   __shared__ double red[2 * 14 * 8];
   __shared__ int redc[WARPS];
   __shared__ double sm_m[7], sm_mn[7], sm_bias[28];
-  const long n = b.n, chunk_n = sum_chunk(n), nchunks = (n + chunk_n - 1) / chunk_n;
+  const long n = b.n, chunk_n = sum_chunk<PASS>(n), nchunks = (n + chunk_n - 1) / chunk_n;
+  const Layout L = layout_of<F, TILE>(s);
   constexpr bool BIASED = PASS == 2 && !(F & SF_PZ);
   if (PASS == 2 && threadIdx.x == 0) {
     moments_of(tot1, sm_m, sm_mn);
@@ -606,7 +629,7 @@ __global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>()
   const double *m = sm_m, *mn = sm_mn;
   if (threadIdx.x == 0)
     for (int k = 0; k < SUM_STAGES; k++)
-      issue_tile<F>(r, smem, k, p, b, s, next_chunk, nchunks, chunk_n);
+      issue_tile<F, TILE>(r, smem, L, k, p, b, s, next_chunk, nchunks, chunk_n);
   long it = 0;
   for (;; it++) {
     const int stage = (int)(it % SUM_STAGES);
@@ -620,21 +643,25 @@ __global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>()
       r.fail = 1;
     }
     if (ok && chunk >= 0) {
-      const double *col = (const double *)(smem + (size_t)stage * STAGE_BYTES);
-      const int32_t *lost = (const int32_t *)(col + 8 * SUM_TILE);
-      const long start = chunk * chunk_n + (long)tile * SUM_TILE;
-      const int n_tile = (int)min((long)SUM_TILE, n - start);
+      const double *col = (const double *)(smem + (size_t)stage * L.stage_bytes);
+      const int32_t *lost = (const int32_t *)(col + L.ncols * TILE);
+      const long start = chunk * chunk_n + (long)tile * TILE;
+      const int n_tile = (int)min((long)TILE, n - start);
       for (int q = slot; q < n_tile; q += 128) {
         Row w;
         w.lost = lost[q];
 #pragma unroll
         for (int k = 0; k < 6; k++)
-          w.v[k] = col[k * SUM_TILE + q];
-        w.id = (F & SF_ID) ? col[6 * SUM_TILE + q] : 0.0;
-        w.t = ((F & SF_TIME) && s.time) ? col[7 * SUM_TILE + q] : 0.0;
-        if (PASS == 1)
+          w.v[k] = col[k * TILE + q];
+        w.id = (F & SF_ID) ? col[L.id_col * TILE + q] : 0.0;
+        w.t = ((F & SF_TIME) && s.time) ? col[L.t_col * TILE + q] : 0.0;
+        const bool sel = select_row<F>(s, w);
+        if (PASS == 1) {
           alive += w.lost < 0;
-        if (!select_row<F>(s, w))
+          if ((F & SF_TIME) && s.time_out)
+            s.time_out[start + q] = w.t;
+        }
+        if (!sel)
           continue;
         if constexpr (PASS == 1) {
           cnt++;
@@ -665,13 +692,18 @@ __global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>()
             d[k] = __dsub_rn(w.v[k], m[k]);
           d[6] = __dsub_rn(w.t, m[6]);
           if (grp == 0) {
-            pair_sums<0, BIASED>(S, E, d, d, nullptr, sparse);
+            if (sparse)
+              pair_sums<0, BIASED, true>(S, E, d, d, nullptr);
+            else
+              pair_sums<0, BIASED, false>(S, E, d, d, nullptr);
             M[0] = fmin(M[0], d[4]);
             M[1] = fmax(M[1], d[4]);
             M[2] = fmin(M[2], d[6]);
             M[3] = fmax(M[3], d[6]);
+          } else if (sparse) {
+            pair_sums<1, BIASED, true>(S, E, d, d, nullptr);
           } else {
-            pair_sums<1, BIASED>(S, E, d, d, nullptr, sparse);
+            pair_sums<1, BIASED, false>(S, E, d, d, nullptr);
           }
         } else {
           const double pz = pz_of(s.Po, w);
@@ -681,9 +713,9 @@ __global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>()
             u[k] = (k == 1 || k == 3) ? __dmul_rn(w.v[k], pz) : w.v[k];
           u[6] = w.id;
           if (grp == 0)
-            pair_sums<0, false>(S, E, u, u, mn, sparse);
+            pair_sums<0, false, false>(S, E, u, u, mn);
           else
-            pair_sums<1, false>(S, E, u, u, mn, sparse);
+            pair_sums<1, false, false>(S, E, u, u, mn);
         }
       }
     }
@@ -694,9 +726,9 @@ __global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>()
       break;
     if (threadIdx.x == 0) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue_tile<F>(r, smem, stage, p, b, s, next_chunk, nchunks, chunk_n);
+      issue_tile<F, TILE>(r, smem, L, stage, p, b, s, next_chunk, nchunks, chunk_n);
     }
-    if (tile == tiles_of(chunk, n, chunk_n) - 1) {
+    if (tile == tiles_of<TILE>(chunk, n, chunk_n) - 1) {
       /* the chunk is complete: its partial (value i at out[i nchunks]) */
       double *out = part + chunk;
       if constexpr (PASS == 1) {
@@ -915,29 +947,31 @@ int launch_sums(const Ctx &c, const Select &s, const double *tot1, int sparse, i
   auto kernel = beam_sums<PASS, F>;
   static int configured[64] = {0}; /* per device: the shared-memory attribute is set */
   if (c.device < 0 || c.device >= 64 || !configured[c.device]) {
-    OBS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SUM_SMEM));
+    OBS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sum_smem_max<PASS>()));
     if (c.device >= 0 && c.device < 64)
       configured[c.device] = 1;
   }
   int sms = 0;
   OBS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device));
-  const long chunk_n = sum_chunk(c.n), nchunks = (c.n + chunk_n - 1) / chunk_n;
+  const long chunk_n = sum_chunk<PASS>(c.n), nchunks = (c.n + chunk_n - 1) / chunk_n;
   const int grid = (int)std::max(1L, std::min<long>(nchunks, (long)sms * sum_blocks_per_sm<PASS>()));
-  kernel<<<grid, sum_threads<PASS>(), SUM_SMEM, c.st>>>(beam_of(c), s, tot1, sparse, pz_pass, counter, status, part);
+  const unsigned smem = SUM_STAGES * layout_of<F, sum_tile<PASS>()>(s).stage_bytes;
+  kernel<<<grid, sum_threads<PASS>(), smem, c.st>>>(beam_of(c), s, tot1, sparse, pz_pass, counter, status, part);
   OBS_CUDA(cudaGetLastError());
   return TRK_OK;
 }
 
-/* chunk partials of a beam of c.n particles */
+/* chunk partials of a pass over a beam of c.n particles */
+template <int PASS>
 int blocks_of(const Ctx &c) {
-  const long chunk_n = sum_chunk(c.n);
+  const long chunk_n = sum_chunk<PASS>(c.n);
   return (int)((c.n + chunk_n - 1) / chunk_n);
 }
 
 /* pass 1 on the device: chunk partials, then their combination into tot1;
  * `ctl` (4 ints: chunk counters of the passes, status) is zeroed here */
 int enqueue_pass1(const Ctx &c, Scratch &sc, const Select &s, int F, double **tot1, int **ctl) {
-  const int nb = blocks_of(c);
+  const int nb = blocks_of<1>(c);
   double *part;
   int rc;
   if ((rc = sc.get(&part, (size_t)nb * P1)) || (rc = sc.get(tot1, P1)) || (rc = sc.get(ctl, 4)))
@@ -999,6 +1033,7 @@ int trk_beam_centroids(trk_context *ctx, double *centroid, long *n) {
   s.start_pid = s.end_pid = -1;
   s.pid_window = 0;
   s.time = nullptr;
+  s.time_out = nullptr;
   Scratch sc(c.ctx, 1);
   double *tot, h[P1];
   int *ctl, status = 0;
@@ -1042,6 +1077,7 @@ int trk_accumulate_beam_sums(trk_context *ctx, trk_beam_sums *sums, double p_cen
     s.end_pid = end_pid;
     s.pid_window = start_pid >= 0 || end_pid >= 0;
     s.time = nullptr;
+    s.time_out = nullptr;
     if (time_value) {
       /* the caller's time coordinates, one per loaded particle */
       double *d_time;
@@ -1049,6 +1085,15 @@ int trk_accumulate_beam_sums(trk_context *ctx, trk_beam_sums *sums, double p_cen
         return rc;
       OBS_CUDA(cudaMemcpyAsync(d_time, time_value, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.st));
       s.time = d_time;
+    }
+    /* pass 1 keeps the time coordinates it computes for pass 2 */
+    Select s2 = s;
+    if (second && !s.time) {
+      double *d_t;
+      if ((rc = sc.get(&d_t, (size_t)(c.n + 31) / 32 * 32)))
+        return rc;
+      s.time_out = d_t;
+      s2.time = d_t;
     }
     /* the whole computation is queued on the device: pass 2 forms the
      * centroids from pass 1's totals itself, and the host waits once */
@@ -1059,17 +1104,17 @@ int trk_accumulate_beam_sums(trk_context *ctx, trk_beam_sums *sums, double p_cen
       return rc;
     double h1[P1], h[P2];
     if (second) {
-      const int nb = blocks_of(c);
+      const int nb = blocks_of<2>(c);
       double *part;
       if ((rc = sc.get(&part, (size_t)nb * P2)) || (rc = sc.get(&tot2, P2)))
         return rc;
       const int sparse = (flags & TRK_SUMS_SPARSE) ? 1 : 0;
       if (id)
-        rc = launch_sums<2, SF_TIME | SF_ID>(c, s, tot1, sparse, pz_mode, ctl + 1, ctl + 3, part);
+        rc = launch_sums<2, SF_TIME | SF_ID>(c, s2, tot1, sparse, pz_mode, ctl + 1, ctl + 3, part);
       else
-        rc = launch_sums<2, SF_TIME>(c, s, tot1, sparse, pz_mode, ctl + 1, ctl + 3, part);
+        rc = launch_sums<2, SF_TIME>(c, s2, tot1, sparse, pz_mode, ctl + 1, ctl + 3, part);
       if (!rc && pz_mode)
-        rc = launch_sums<2, SF_TIME | SF_ID | SF_PZ>(c, s, tot1, sparse, 1, ctl + 2, ctl + 3, part);
+        rc = launch_sums<2, SF_TIME | SF_ID | SF_PZ>(c, s2, tot1, sparse, 1, ctl + 2, ctl + 3, part);
       if (rc)
         return rc;
       combine_partials<<<56 + 6, COMBINE_THREADS, 0, c.st>>>(part, nb, 56, 6, P2_MIN_MASK, P2_MAX_MASK, tot2);
