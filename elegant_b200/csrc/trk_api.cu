@@ -134,6 +134,9 @@ struct trk_context {
     size_t bytes;
   };
   std::vector<ScratchSlot> obs_scratch;
+  /* pinned host buffer the observers copy their results into */
+  void *h_obs = nullptr;
+  size_t h_obs_bytes = 0;
 };
 
 /* Passes per launch when compacting: 1, 2, 4, ... up to compact_every,
@@ -173,6 +176,24 @@ int trk_context_scratch(trk_context *ctx, int site, int slot, size_t bytes, void
     return trk_set_error(TRK_ERR_CUDA, "cudaMalloc: %s", cudaGetErrorString(er));
   ctx->obs_scratch.push_back({site, slot, q, bytes});
   *out = q;
+  return TRK_OK;
+}
+
+/* The observers' pinned host buffer of at least `bytes` (one buffer per
+ * context, grown on demand, freed with the context): results copied into
+ * pinned memory need no staging copy and no extra synchronization. */
+int trk_context_host_scratch(trk_context *ctx, size_t bytes, void **out) {
+  if (ctx->h_obs_bytes < bytes) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaFreeHost(ctx->h_obs);
+    ctx->h_obs = nullptr;
+    ctx->h_obs_bytes = 0;
+    cudaError_t er = cudaHostAlloc(&ctx->h_obs, bytes, cudaHostAllocDefault);
+    if (er != cudaSuccess)
+      return trk_set_error(TRK_ERR_CUDA, "cudaHostAlloc: %s", cudaGetErrorString(er));
+    ctx->h_obs_bytes = bytes;
+  }
+  *out = ctx->h_obs;
   return TRK_OK;
 }
 
@@ -820,6 +841,9 @@ void trk_context_destroy(trk_context *ctx) {
   for (trk_context::ScratchSlot &e : ctx->obs_scratch)
     cudaFree(e.p);
   ctx->obs_scratch.clear();
+  cudaFreeHost(ctx->h_obs);
+  ctx->h_obs = nullptr;
+  ctx->h_obs_bytes = 0;
   trk_comm_destroy(ctx->comm);
   cudaFree(ctx->d_effort);
   cudaFree(ctx->d_aos);

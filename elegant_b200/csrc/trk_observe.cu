@@ -38,6 +38,7 @@
 
 /* observer scratch held by the context (defined in trk_api.cu) */
 int trk_context_scratch(trk_context *ctx, int site, int slot, size_t bytes, void **out);
+int trk_context_host_scratch(trk_context *ctx, size_t bytes, void **out);
 
 namespace {
 
@@ -554,10 +555,10 @@ __device__ __forceinline__ void pair_sums(double (&S)[16], double (&E)[16], cons
 /* The beam-sum passes, one partial per chunk.
  *
  * Pass 1 (PASS = 1): sums of x, x', y, y', s, delta, t (SF_TIME) and of
- * x' pz, y' pz (SF_PZ), the count of selected particles, min / max / max |.|
- * of x, x', y, y', delta, and the count of surviving particles.  Partial (P1
- * doubles): [0..17] 9 sums as (hi, lo), [18] count, [19..33] (min, max,
- * maxabs) for coordinates 0, 1, 2, 3, 5, [34] survivors.
+ * x' pz, y' pz (SF_PZ) per chunk: [0..17] 9 sums as (hi, lo).  Per block:
+ * [0] the count of selected particles, [1..15] (min, max, max |.|) of x, x',
+ * y, y', delta, [16] the count of surviving particles, [17..20] min / max of
+ * s and t.
  *
  * Pass 2 (PASS = 2): second moments about the centroids, which each block
  * forms from the combined pass-1 totals `tot1` as the host forms them
@@ -565,18 +566,17 @@ __device__ __forceinline__ void pair_sums(double (&S)[16], double (&E)[16], cons
  * over x, x', y, y', s, delta, t (28 pairs, in row order), and min / max /
  * max |.| of s - m_s and t - m_t; or, with SF_PZ, the sums of the normalized
  * products (src/compute_centroids.c:418-420, as written there: the second
- * factor is not centered and index 6 reads the particle ID column).  Partial
- * (P2 doubles): [0..55] sigma (hi, lo), [56..111] sigman, [112..117] (min,
- * max, maxabs) of s and t.  The pass without SF_PZ writes zeros to the sigman
- * part unless `pz_pass` says the SF_PZ pass follows.
+ * factor is not centered and index 6 reads the particle ID column).  Per
+ * chunk: [0..55] sigma (hi, lo), [56..111] sigman.  Per block (without
+ * SF_PZ): (min, max, max |.|) of s - m_s and t - m_t.
  *
  * `status` gets SUM_STATUS_COPY_TIMEOUT when a staged copy did not complete
  * in time; the block then waits (bounded) for its copies in flight and
  * returns. */
 template <int PASS, int F>
 __global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>())
-  beam_sums(Beam b, Select s, const double *tot1, int sparse, int pz_pass, int *next_chunk, int *status,
-            double *part) {
+  beam_sums(Beam b, Select s, const double *tot1, int sparse, int *next_chunk, int *status, double *part,
+            double *blk) {
   constexpr int THREADS = sum_threads<PASS>(), WARPS = THREADS / 32, TILE = sum_tile<PASS>();
   constexpr int NV = PASS == 1 ? 9 : 14;  /* sums a thread keeps */
   constexpr int NP = 16;                  /* butterfly width */
@@ -600,6 +600,8 @@ __global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>()
   const int slot = PASS == 2 ? (warp >> 1) * 32 + lane : (int)threadIdx.x;
   double S[NP], E[NP], M[NM];
   int cnt = 0, alive = 0;
+  /* the sums restart at every chunk; extremes and counts, which do not
+   * depend on the order they are formed in, run over the block's chunks */
   auto reset = [&]() {
 #pragma unroll
     for (int k = 0; k < NP; k++)
@@ -608,11 +610,10 @@ __global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>()
 #pragma unroll
       for (int k = 0; k < 14; k++)
         S[k] = sm_bias[14 * grp + k];
-#pragma unroll
-    for (int k = 0; k < NM; k++)
-      M[k] = (k % 2 == 0) ? OBS_BIG : -OBS_BIG;
-    cnt = alive = 0;
   };
+#pragma unroll
+  for (int k = 0; k < NM; k++)
+    M[k] = (k % 2 == 0) ? OBS_BIG : -OBS_BIG;
   __syncthreads();
   reset();
   Producer p;
@@ -729,31 +730,36 @@ __global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>()
       issue_tile<F, TILE>(r, smem, L, stage, p, b, s, next_chunk, nchunks, chunk_n);
     }
     if (tile == tiles_of<TILE>(chunk, n, chunk_n) - 1) {
-      /* the chunk is complete: its partial (value i at out[i nchunks]) */
+      /* the chunk is complete: its sums (value i at out[i nchunks]) */
       double *out = part + chunk;
       if constexpr (PASS == 1) {
-        double X[15], Y[4] = {M[10], M[11], M[12], M[13]};
-        with_maxabs<5>(M, X);
         block_dd_totals<NV, NP, WARPS, 1>(S, E, red, out, nchunks);
-        block_count<WARPS>(cnt, redc, out + P1_COUNT * nchunks);
-        block_extremes<15, WARPS>(X, 0x1249u, red, out + 19 * nchunks, nchunks);
-        block_count<WARPS>(alive, redc, out + 34 * nchunks);
-        block_extremes<4, WARPS>(Y, 0x5u, red, out + 35 * nchunks, nchunks);
       } else if constexpr (!(F & SF_PZ)) {
-        double X[6];
-        with_maxabs<2>(M, X);
 #pragma unroll
         for (int k = 0; k < 14; k++)
           S[k] = __dsub_rn(S[k], sm_bias[14 * grp + k]);
         block_dd_totals<NV, NP, WARPS, 2>(S, E, red, out, nchunks);
-        block_extremes<6, WARPS>(X, 0x9u, red, out + 112 * nchunks, nchunks);
-        if (!pz_pass)
-          for (int k = threadIdx.x; k < 56; k += THREADS)
-            out[(56 + k) * nchunks] = 0.0;
       } else {
         block_dd_totals<NV, NP, WARPS, 2>(S, E, red, out + 56 * nchunks, nchunks);
       }
       reset();
+    }
+  }
+  /* the block's extremes and counts (value i at blk[i gridDim.x + block]) */
+  if (!r.fail) {
+    double *bo = blk + blockIdx.x;
+    const long bs = gridDim.x;
+    if constexpr (PASS == 1) {
+      double X[15], Y[4] = {M[10], M[11], M[12], M[13]};
+      with_maxabs<5>(M, X);
+      block_count<WARPS>(cnt, redc, bo);
+      block_extremes<15, WARPS>(X, 0x1249u, red, bo + bs, bs);
+      block_count<WARPS>(alive, redc, bo + 16 * bs);
+      block_extremes<4, WARPS>(Y, 0x5u, red, bo + 17 * bs, bs);
+    } else if constexpr (!(F & SF_PZ)) {
+      double X[6];
+      with_maxabs<2>(M, X);
+      block_extremes<6, WARPS>(X, 0x9u, red, bo, bs);
     }
   }
   if (r.fail && threadIdx.x == 0) {
@@ -767,15 +773,17 @@ __global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>()
   }
 }
 
-/* Combine the chunk partials (value-major, `nchunks` per value) in chunk
- * order: `n_dd` double-double values at the front, then `n_plain` values,
- * plain value k a minimum when bit k of `min_mask` is set, a maximum when bit
- * k of `max_mask` is set, else a sum.  One block per value: thread t takes
- * chunks t, t + COMBINE_THREADS, ... in order, then the lanes combine in a
- * fixed tree and the warps in index order. */
+/* Combine partials: `n_dd` double-double values from the chunk partials
+ * `part` (value-major, `nchunks` per value, combined in chunk order) to
+ * out[2 v], out[2 v + 1]; then `n_plain` values from `plain` (value-major,
+ * `nplain_rows` per value) to out[plain_base + k], value k a minimum when bit
+ * k of `min_mask` is set, a maximum when bit k of `max_mask` is set, else a
+ * sum.  One block per value: thread t takes rows t, t + COMBINE_THREADS, ...
+ * in order, then the lanes combine in a fixed tree and the warps in index
+ * order. */
 __global__ void __launch_bounds__(COMBINE_THREADS)
-  combine_partials(const double *part, int nchunks, int n_dd, int n_plain, unsigned min_mask, unsigned max_mask,
-                   double *out) {
+  combine_partials(const double *part, int nchunks, int n_dd, const double *plain, int nplain_rows, int n_plain,
+                   int plain_base, unsigned min_mask, unsigned max_mask, double *out) {
   __shared__ double sh[2 * (COMBINE_THREADS / 32)];
   const int v = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (v < n_dd) {
@@ -801,12 +809,12 @@ __global__ void __launch_bounds__(COMBINE_THREADS)
       out[2 * v + 1] = t.lo;
     }
   } else if (v < n_dd + n_plain) {
-    const int k = v - n_dd, q = 2 * n_dd + k;
+    const int k = v - n_dd, q = plain_base + k;
     const int op = ((min_mask >> k) & 1u) ? 1 : (((max_mask >> k) & 1u) ? 2 : 0);
-    const double *px = part + (size_t)q * nchunks;
+    const double *px = plain + (size_t)k * nplain_rows;
     double acc = op == 0 ? 0.0 : (op == 1 ? OBS_BIG : -OBS_BIG);
 #pragma unroll 4
-    for (int c = threadIdx.x; c < nchunks; c += COMBINE_THREADS)
+    for (int c = threadIdx.x; c < nplain_rows; c += COMBINE_THREADS)
       acc = op == 0 ? __dadd_rn(acc, px[c]) : (op == 1 ? fmin(acc, px[c]) : fmax(acc, px[c]));
     for (int off = 16; off > 0; off >>= 1) {
       const double x = __shfl_down_sync(0xffffffffu, acc, off);
@@ -939,11 +947,22 @@ struct Scratch {
   }
 };
 
-/* one pass of the beam sums into the chunk partials `part`; `counter` and
- * `status` are device ints the caller has zeroed */
+/* blocks of a pass's persistent grid on the context's device */
+template <int PASS>
+int sums_grid(const Ctx &c, int *grid) {
+  int sms = 0;
+  OBS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device));
+  const long chunk_n = sum_chunk<PASS>(c.n), nchunks = (c.n + chunk_n - 1) / chunk_n;
+  *grid = (int)std::max(1L, std::min<long>(nchunks, (long)sms * sum_blocks_per_sm<PASS>()));
+  return TRK_OK;
+}
+
+/* one pass of the beam sums into the chunk partials `part` and the block
+ * values `blk` over `grid` blocks; `counter` and `status` are device ints
+ * the caller has zeroed */
 template <int PASS, int F>
-int launch_sums(const Ctx &c, const Select &s, const double *tot1, int sparse, int pz_pass, int *counter,
-                int *status, double *part) {
+int launch_sums(const Ctx &c, const Select &s, const double *tot1, int sparse, int grid, int *counter, int *status,
+                double *part, double *blk) {
   auto kernel = beam_sums<PASS, F>;
   static int configured[64] = {0}; /* per device: the shared-memory attribute is set */
   if (c.device < 0 || c.device >= 64 || !configured[c.device]) {
@@ -951,12 +970,8 @@ int launch_sums(const Ctx &c, const Select &s, const double *tot1, int sparse, i
     if (c.device >= 0 && c.device < 64)
       configured[c.device] = 1;
   }
-  int sms = 0;
-  OBS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device));
-  const long chunk_n = sum_chunk<PASS>(c.n), nchunks = (c.n + chunk_n - 1) / chunk_n;
-  const int grid = (int)std::max(1L, std::min<long>(nchunks, (long)sms * sum_blocks_per_sm<PASS>()));
   const unsigned smem = SUM_STAGES * layout_of<F, sum_tile<PASS>()>(s).stage_bytes;
-  kernel<<<grid, sum_threads<PASS>(), smem, c.st>>>(beam_of(c), s, tot1, sparse, pz_pass, counter, status, part);
+  kernel<<<grid, sum_threads<PASS>(), smem, c.st>>>(beam_of(c), s, tot1, sparse, counter, status, part, blk);
   OBS_CUDA(cudaGetLastError());
   return TRK_OK;
 }
@@ -968,37 +983,41 @@ int blocks_of(const Ctx &c) {
   return (int)((c.n + chunk_n - 1) / chunk_n);
 }
 
-/* pass 1 on the device: chunk partials, then their combination into tot1;
- * `ctl` (4 ints: chunk counters of the passes, status) is zeroed here */
-int enqueue_pass1(const Ctx &c, Scratch &sc, const Select &s, int F, double **tot1, int **ctl) {
+/* pass 1 on the device: chunk partials and block values, then their
+ * combination into tot1; `ctl` (4 ints: chunk counters of the passes,
+ * status) is zeroed here */
+int enqueue_pass1(const Ctx &c, Scratch &sc, const Select &s, int F, double *tot1, int *ctl) {
   const int nb = blocks_of<1>(c);
-  double *part;
-  int rc;
-  if ((rc = sc.get(&part, (size_t)nb * P1)) || (rc = sc.get(tot1, P1)) || (rc = sc.get(ctl, 4)))
+  int grid, rc;
+  if ((rc = sums_grid<1>(c, &grid)))
     return rc;
-  OBS_CUDA(cudaMemsetAsync(*ctl, 0, 4 * sizeof(int), c.st));
+  double *part, *blk;
+  if ((rc = sc.get(&part, (size_t)nb * 18)) || (rc = sc.get(&blk, (size_t)grid * 21)))
+    return rc;
+  OBS_CUDA(cudaMemsetAsync(ctl, 0, 4 * sizeof(int), c.st));
   switch (F) {
   case 0:
-    rc = launch_sums<1, 0>(c, s, nullptr, 0, 0, *ctl, *ctl + 3, part);
+    rc = launch_sums<1, 0>(c, s, nullptr, 0, grid, ctl, ctl + 3, part, blk);
     break;
   case SF_TIME:
-    rc = launch_sums<1, SF_TIME>(c, s, nullptr, 0, 0, *ctl, *ctl + 3, part);
+    rc = launch_sums<1, SF_TIME>(c, s, nullptr, 0, grid, ctl, ctl + 3, part, blk);
     break;
   case SF_TIME | SF_ID:
-    rc = launch_sums<1, SF_TIME | SF_ID>(c, s, nullptr, 0, 0, *ctl, *ctl + 3, part);
+    rc = launch_sums<1, SF_TIME | SF_ID>(c, s, nullptr, 0, grid, ctl, ctl + 3, part, blk);
     break;
   case SF_TIME | SF_PZ:
-    rc = launch_sums<1, SF_TIME | SF_PZ>(c, s, nullptr, 0, 0, *ctl, *ctl + 3, part);
+    rc = launch_sums<1, SF_TIME | SF_PZ>(c, s, nullptr, 0, grid, ctl, ctl + 3, part, blk);
     break;
   case SF_TIME | SF_ID | SF_PZ:
-    rc = launch_sums<1, SF_TIME | SF_ID | SF_PZ>(c, s, nullptr, 0, 0, *ctl, *ctl + 3, part);
+    rc = launch_sums<1, SF_TIME | SF_ID | SF_PZ>(c, s, nullptr, 0, grid, ctl, ctl + 3, part, blk);
     break;
   default:
     return trk_set_error(TRK_ERR_ARG, "beam sums: no pass-1 variant %d", F);
   }
   if (rc)
     return rc;
-  combine_partials<<<9 + 21, COMBINE_THREADS, 0, c.st>>>(part, nb, 9, 21, P1_MIN_MASK, P1_MAX_MASK, *tot1);
+  combine_partials<<<9 + 21, COMBINE_THREADS, 0, c.st>>>(part, nb, 9, blk, grid, 21, P1_COUNT, P1_MIN_MASK,
+                                                          P1_MAX_MASK, tot1);
   OBS_CUDA(cudaGetLastError());
   return TRK_OK;
 }
@@ -1034,15 +1053,16 @@ int trk_beam_centroids(trk_context *ctx, double *centroid, long *n) {
   s.pid_window = 0;
   s.time = nullptr;
   s.time_out = nullptr;
+  /* results: pass 1's totals, then the control words, copied back at once */
   Scratch sc(c.ctx, 1);
-  double *tot, h[P1];
-  int *ctl, status = 0;
-  if ((rc = enqueue_pass1(c, sc, s, 0, &tot, &ctl)))
+  double *res, *h;
+  if ((rc = sc.get(&res, P1 + 2)) || (rc = trk_context_host_scratch(c.ctx, sizeof(double) * (P1 + 2), (void **)&h)))
     return rc;
-  OBS_CUDA(cudaMemcpyAsync(h, tot, sizeof(h), cudaMemcpyDeviceToHost, c.st));
-  OBS_CUDA(cudaMemcpyAsync(&status, ctl + 3, sizeof(int), cudaMemcpyDeviceToHost, c.st));
+  if ((rc = enqueue_pass1(c, sc, s, 0, res, (int *)(res + P1))))
+    return rc;
+  OBS_CUDA(cudaMemcpyAsync(h, res, sizeof(double) * (P1 + 2), cudaMemcpyDeviceToHost, c.st));
   OBS_CUDA(cudaStreamSynchronize(c.st));
-  if ((rc = sums_status(status)))
+  if ((rc = sums_status(((const int *)(h + P1))[3])))
     return rc;
   const double count = h[18];
   if (count > 0)
@@ -1098,33 +1118,42 @@ int trk_accumulate_beam_sums(trk_context *ctx, trk_beam_sums *sums, double p_cen
     /* the whole computation is queued on the device: pass 2 forms the
      * centroids from pass 1's totals itself, and the host waits once */
     const int id = s.pid_window ? SF_ID : 0;
-    double *tot1, *tot2 = nullptr;
-    int *ctl, status = 0;
-    if ((rc = enqueue_pass1(c, sc, s, SF_TIME | id | (pz_mode ? SF_PZ : 0), &tot1, &ctl)))
+    /* results: pass 1's totals, pass 2's, the control words; one copy back */
+    double *res, *hres;
+    if ((rc = sc.get(&res, P1 + P2 + 2)) ||
+        (rc = trk_context_host_scratch(c.ctx, sizeof(double) * (P1 + P2 + 2), (void **)&hres)))
       return rc;
-    double h1[P1], h[P2];
+    double *tot1 = res, *tot2 = res + P1;
+    int *ctl = (int *)(res + P1 + P2);
+    if ((rc = enqueue_pass1(c, sc, s, SF_TIME | id | (pz_mode ? SF_PZ : 0), tot1, ctl)))
+      return rc;
+    const double *h1 = hres, *h = hres + P1;
     if (second) {
       const int nb = blocks_of<2>(c);
-      double *part;
-      if ((rc = sc.get(&part, (size_t)nb * P2)) || (rc = sc.get(&tot2, P2)))
+      int grid;
+      if ((rc = sums_grid<2>(c, &grid)))
+        return rc;
+      double *part, *blk;
+      if ((rc = sc.get(&part, (size_t)nb * 112)) || (rc = sc.get(&blk, (size_t)grid * 6)))
         return rc;
       const int sparse = (flags & TRK_SUMS_SPARSE) ? 1 : 0;
       if (id)
-        rc = launch_sums<2, SF_TIME | SF_ID>(c, s2, tot1, sparse, pz_mode, ctl + 1, ctl + 3, part);
+        rc = launch_sums<2, SF_TIME | SF_ID>(c, s2, tot1, sparse, grid, ctl + 1, ctl + 3, part, blk);
       else
-        rc = launch_sums<2, SF_TIME>(c, s2, tot1, sparse, pz_mode, ctl + 1, ctl + 3, part);
+        rc = launch_sums<2, SF_TIME>(c, s2, tot1, sparse, grid, ctl + 1, ctl + 3, part, blk);
       if (!rc && pz_mode)
-        rc = launch_sums<2, SF_TIME | SF_ID | SF_PZ>(c, s2, tot1, sparse, 1, ctl + 2, ctl + 3, part);
+        rc = launch_sums<2, SF_TIME | SF_ID | SF_PZ>(c, s2, tot1, sparse, grid, ctl + 2, ctl + 3, part, blk);
       if (rc)
         return rc;
-      combine_partials<<<56 + 6, COMBINE_THREADS, 0, c.st>>>(part, nb, 56, 6, P2_MIN_MASK, P2_MAX_MASK, tot2);
+      /* sigma, and sigman when asked for; the s and t extremes */
+      const int n_dd = pz_mode ? 56 : 28;
+      combine_partials<<<n_dd + 6, COMBINE_THREADS, 0, c.st>>>(part, nb, n_dd, blk, grid, 6, 112, P2_MIN_MASK,
+                                                                P2_MAX_MASK, tot2);
       OBS_CUDA(cudaGetLastError());
-      OBS_CUDA(cudaMemcpyAsync(h, tot2, sizeof(h), cudaMemcpyDeviceToHost, c.st));
     }
-    OBS_CUDA(cudaMemcpyAsync(h1, tot1, sizeof(h1), cudaMemcpyDeviceToHost, c.st));
-    OBS_CUDA(cudaMemcpyAsync(&status, ctl + 3, sizeof(int), cudaMemcpyDeviceToHost, c.st));
+    OBS_CUDA(cudaMemcpyAsync(hres, res, sizeof(double) * (P1 + P2 + 2), cudaMemcpyDeviceToHost, c.st));
     OBS_CUDA(cudaStreamSynchronize(c.st));
-    if ((rc = sums_status(status)))
+    if ((rc = sums_status(((const int *)(hres + P1 + P2))[3])))
       return rc;
     /* nothing is accumulated without survivors (src/compute_centroids.c:313) */
     if (h1[34] > 0) {
@@ -1207,7 +1236,7 @@ int trk_match_energy(trk_context *ctx, double *p_central, int change_beam) {
   if ((rc = sc.get(&part, (size_t)nb * 3)) || (rc = sc.get(&out, 3)))
     return rc;
   momentum_sum<<<nb, OBS_THREADS, 0, c.st>>>(beam_of(c), Po, part);
-  combine_partials<<<2, COMBINE_THREADS, 0, c.st>>>(part, nb, 1, 1, 0u, 0u, out);
+  combine_partials<<<2, COMBINE_THREADS, 0, c.st>>>(part, nb, 1, part + 2 * nb, nb, 1, 2, 0u, 0u, out);
   double h[3];
   OBS_CUDA(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, c.st));
   OBS_CUDA(cudaStreamSynchronize(c.st));
