@@ -101,11 +101,15 @@ struct Select {
  * about 2^-100 relative, rounded once at the end.  Particles that are lost or
  * outside the windows are skipped.
  *
- * Data movement: persistent blocks take chunks from a counter, and a ring of
- * SUM_STAGES tiles of sum_tile particles in shared memory is filled by 1-D
- * bulk copies (cp.async.bulk, from this device's own beam columns) that
- * complete on an mbarrier per stage; the copies of the next tile stream while
- * the threads sum the current one.  Bulk copies need 16-byte aligned sources
+ * Data movement: persistent block b takes chunks b, b + G, b + 2G, ... (G
+ * blocks; about ten chunks a block), and a ring of SUM_STAGES tiles of
+ * sum_tile particles in shared memory is filled by 1-D bulk copies
+ * (cp.async.bulk, from this device's own beam columns) that complete on a
+ * "full" mbarrier per stage; each warp arrives on the stage's "empty"
+ * mbarrier when it has read the tile, and the issuing thread refills the
+ * stage once every warp has, so the warps synchronize only at chunk ends.
+ * Every warp steps through the same tile sequence itself, so all agree on
+ * the chunk boundaries without reading shared state.  Bulk copies need 16-byte aligned sources
  * and sizes: the beam columns are tile-aligned slices of arrays whose
  * stride (the beam capacity) is a multiple of 32 entries, and a tile's copy
  * is rounded up to whole 16-byte units inside that capacity.
@@ -121,7 +125,7 @@ constexpr long SUM_CHUNK_MIN = 1024, SUM_CHUNK_MAX = 8192;
 template <int PASS> __host__ __device__ constexpr int sum_tile() { return PASS == 1 ? 512 : 896; }
 /* the most shared memory a pass's stages take (every column staged) */
 template <int PASS> __host__ __device__ constexpr int sum_smem_max() { return SUM_STAGES * sum_tile<PASS>() * (8 * 8 + 4); }
-constexpr int COMBINE_THREADS = 256;
+constexpr int COMBINE_THREADS = 512, COMBINE_BATCH = 8;
 /* a bulk copy that has not completed after this long is reported as an error */
 constexpr unsigned long long SUM_WAIT_NS = 2000000000ull;
 
@@ -178,15 +182,16 @@ __device__ __forceinline__ bool mbar_test(uint64_t *bar, unsigned parity) {
   return ok != 0;
 }
 
-/* wait for the phase of `parity` to complete, for SUM_WAIT_NS at most */
-__device__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+/* wait for the phase of `parity` to complete, for SUM_WAIT_NS at most, and
+ * give up at once when `fail` (when given) is set */
+__device__ bool mbar_wait(uint64_t *bar, unsigned parity, const volatile int *fail = nullptr) {
   if (mbar_test(bar, parity))
     return true;
   const unsigned long long t0 = global_ns();
   for (long k = 0; k < (1L << 28); k++) {
     if (mbar_test(bar, parity))
       return true;
-    if (global_ns() - t0 > SUM_WAIT_NS)
+    if ((fail && *fail) || global_ns() - t0 > SUM_WAIT_NS)
       return false;
     __nanosleep(32);
   }
@@ -448,13 +453,11 @@ __device__ __forceinline__ void sum_biases(const double *tot1, const double m[7]
     }
 }
 
-/* the ring of staged tiles: an mbarrier per stage and the tile it holds
- * (chunk -1: no work left) */
+/* the ring of staged tiles: per stage a "full" mbarrier (the tile's copies
+ * landed) and an "empty" one (every warp has read the tile) */
 struct Ring {
-  uint64_t bar[SUM_STAGES];
-  long chunk[SUM_STAGES];
-  int tile[SUM_STAGES];
-  int fail;
+  uint64_t full[SUM_STAGES], empty[SUM_STAGES];
+  volatile int fail;
 };
 
 /* tiles of chunk c */
@@ -482,46 +485,52 @@ __host__ __device__ inline Layout layout_of(const Select &s) {
   return l;
 }
 
-/* the issuing thread's position in its stream of tiles */
-struct Producer {
-  long chunk, issued;
+/* A position in a block's stream of tiles: chunks b, b + G, b + 2G, ... (G
+ * blocks), each cut into tiles.  Every thread can step through it, so all
+ * warps agree on the chunk boundaries without reading shared state. */
+struct TilePos {
+  long chunk;
   int tile, ntiles;
 };
 
-/* Issue the next tile of the block's stream into `stage` (thread 0).  A new
- * chunk is taken from the counter when the current one is used up; past the
- * last chunk the stage gets an end mark and a plain arrival instead. */
-template <int F, int TILE>
-__device__ void issue_tile(Ring &r, unsigned char *smem, const Layout &L, int stage, Producer &p, const Beam &b,
-                           const Select &s, int *next_chunk, long nchunks, long chunk_n) {
-  if (p.tile == p.ntiles) {
-    if (p.chunk < nchunks)
-      p.chunk = atomicAdd(next_chunk, 1);
+struct TileStream {
+  long nchunks, stride, n, chunk_n;
+  template <int TILE>
+  __device__ TilePos first(long c) const {
+    TilePos p;
+    p.chunk = c;
     p.tile = 0;
-    p.ntiles = p.chunk < nchunks ? tiles_of<TILE>(p.chunk, b.n, chunk_n) : 0;
+    p.ntiles = c < nchunks ? tiles_of<TILE>(c, n, chunk_n) : 0;
+    return p;
   }
-  if (p.chunk >= nchunks) {
-    r.chunk[stage] = -1;
-    mbar_arrive(&r.bar[stage]);
-    return;
+  template <int TILE>
+  __device__ void next(TilePos &p) const {
+    if (++p.tile >= p.ntiles) {
+      p.chunk += stride;
+      p.tile = 0;
+      p.ntiles = p.chunk < nchunks ? tiles_of<TILE>(p.chunk, n, chunk_n) : 0;
+    }
   }
+  __device__ bool done(const TilePos &p) const { return p.chunk >= nchunks; }
+};
+
+/* Issue the copies of tile `tile` of chunk `chunk` into `stage` (thread 0). */
+template <int TILE>
+__device__ void issue_tile(Ring &r, unsigned char *smem, const Layout &L, int stage, long chunk, int tile,
+                           const Beam &b, const Select &s, long chunk_n) {
   unsigned char *st = smem + (size_t)stage * L.stage_bytes;
-  const long start = p.chunk * chunk_n + (long)p.tile * TILE;
+  const long start = chunk * chunk_n + (long)tile * TILE;
   const int cnt = (int)min((long)TILE, b.n - start);
   /* whole 16-byte units: 2 doubles, 4 loss words (inside the capacity) */
   const unsigned bd = (unsigned)((cnt + 1) & ~1) * 8u, bl = (unsigned)((cnt + 3) & ~3) * 4u;
-  r.chunk[stage] = p.chunk;
-  r.tile[stage] = p.tile;
-  mbar_arrive_expect_tx(&r.bar[stage], bd * (unsigned)L.ncols + bl);
+  mbar_arrive_expect_tx(&r.full[stage], bd * (unsigned)L.ncols + bl);
   for (int k = 0; k < 6; k++)
-    bulk_load(st + (size_t)k * TILE * 8, b.c[k] + start, bd, &r.bar[stage]);
+    bulk_load(st + (size_t)k * TILE * 8, b.c[k] + start, bd, &r.full[stage]);
   if (L.id_col >= 0)
-    bulk_load(st + (size_t)L.id_col * TILE * 8, b.c[6] + start, bd, &r.bar[stage]);
+    bulk_load(st + (size_t)L.id_col * TILE * 8, b.c[6] + start, bd, &r.full[stage]);
   if (L.t_col >= 0)
-    bulk_load(st + (size_t)L.t_col * TILE * 8, s.time + start, bd, &r.bar[stage]);
-  bulk_load(st + (size_t)L.ncols * TILE * 8, b.lost + start, bl, &r.bar[stage]);
-  p.tile++;
-  p.issued++;
+    bulk_load(st + (size_t)L.t_col * TILE * 8, s.time + start, bd, &r.full[stage]);
+  bulk_load(st + (size_t)L.ncols * TILE * 8, b.lost + start, bl, &r.full[stage]);
 }
 
 /* The 14 second moments of pair group G (pairs 14 G .. 14 G + 13 in row
@@ -575,8 +584,7 @@ __device__ __forceinline__ void pair_sums(double (&S)[16], double (&E)[16], cons
  * returns. */
 template <int PASS, int F>
 __global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>())
-  beam_sums(Beam b, Select s, const double *tot1, int sparse, int *next_chunk, int *status, double *part,
-            double *blk) {
+  beam_sums(Beam b, Select s, const double *tot1, int sparse, int *status, double *part, double *blk) {
   constexpr int THREADS = sum_threads<PASS>(), WARPS = THREADS / 32, TILE = sum_tile<PASS>();
   constexpr int NV = PASS == 1 ? 9 : 14;  /* sums a thread keeps */
   constexpr int NP = 16;                  /* butterfly width */
@@ -616,34 +624,40 @@ __global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>()
     M[k] = (k % 2 == 0) ? OBS_BIG : -OBS_BIG;
   __syncthreads();
   reset();
-  Producer p;
-  p.chunk = -1;
-  p.issued = 0;
-  p.tile = p.ntiles = 0;
   if (threadIdx.x == 0) {
-    for (int k = 0; k < SUM_STAGES; k++)
-      mbar_init(&r.bar[k], 1);
+    for (int k = 0; k < SUM_STAGES; k++) {
+      mbar_init(&r.full[k], 1);
+      mbar_init(&r.empty[k], WARPS);
+    }
     r.fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
   const double *m = sm_m, *mn = sm_mn;
-  if (threadIdx.x == 0)
-    for (int k = 0; k < SUM_STAGES; k++)
-      issue_tile<F, TILE>(r, smem, L, k, p, b, s, next_chunk, nchunks, chunk_n);
+  /* the consumers' position in the block's tiles; the issuing thread keeps
+   * SUM_STAGES tiles ahead */
+  TileStream ts;
+  ts.nchunks = nchunks;
+  ts.stride = gridDim.x;
+  ts.n = n;
+  ts.chunk_n = chunk_n;
+  TilePos cs = ts.first<TILE>(blockIdx.x);
+  long issued = 0;
+  if (threadIdx.x == 0) {
+    TilePos ps = cs;
+    for (int k = 0; k < SUM_STAGES && !ts.done(ps); k++, issued++, ts.next<TILE>(ps))
+      issue_tile<TILE>(r, smem, L, k, ps.chunk, ps.tile, b, s, chunk_n);
+  }
   long it = 0;
-  for (;; it++) {
+  for (; !ts.done(cs); it++, ts.next<TILE>(cs)) {
     const int stage = (int)(it % SUM_STAGES);
-    const bool ok = mbar_wait(&r.bar[stage], (unsigned)((it / SUM_STAGES) & 1));
-    long chunk = -1;
-    int tile = 0;
-    if (ok) {
-      chunk = r.chunk[stage];
-      tile = r.tile[stage];
-    } else {
+    const unsigned parity = (unsigned)((it / SUM_STAGES) & 1);
+    const bool ok = mbar_wait(&r.full[stage], parity, &r.fail);
+    if (!ok)
       r.fail = 1;
-    }
-    if (ok && chunk >= 0) {
+    const long chunk = cs.chunk;
+    const int tile = cs.tile;
+    if (ok) {
       const double *col = (const double *)(smem + (size_t)stage * L.stage_bytes);
       const int32_t *lost = (const int32_t *)(col + L.ncols * TILE);
       const long start = chunk * chunk_n + (long)tile * TILE;
@@ -720,16 +734,27 @@ __global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>()
         }
       }
     }
-    /* the stage is consumed; failures and the end of the work are seen by
-     * every thread after this barrier */
-    __syncthreads();
-    if (r.fail || chunk < 0)
-      break;
-    if (threadIdx.x == 0) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue_tile<F, TILE>(r, smem, L, stage, p, b, s, next_chunk, nchunks, chunk_n);
+    /* this warp is done with the stage; the issuing thread refills it once
+     * every warp is */
+    __syncwarp();
+    if (lane == 0)
+      mbar_arrive(&r.empty[stage]);
+    if (threadIdx.x == 0 && !r.fail) {
+      /* the tile SUM_STAGES ahead of this one goes into this stage */
+      TilePos ps = cs;
+      for (int k = 0; k < SUM_STAGES; k++)
+        ts.next<TILE>(ps);
+      if (!ts.done(ps)) {
+        if (mbar_wait(&r.empty[stage], parity, &r.fail)) {
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          issue_tile<TILE>(r, smem, L, stage, ps.chunk, ps.tile, b, s, chunk_n);
+          issued++;
+        } else {
+          r.fail = 1;
+        }
+      }
     }
-    if (tile == tiles_of<TILE>(chunk, n, chunk_n) - 1) {
+    if (cs.tile == cs.ntiles - 1) {
       /* the chunk is complete: its sums (value i at out[i nchunks]) */
       double *out = part + chunk;
       if constexpr (PASS == 1) {
@@ -745,8 +770,17 @@ __global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>()
       reset();
     }
   }
+  __syncthreads();
+  const bool failed = r.fail != 0;
+  if (failed && threadIdx.x == 0) {
+    /* copies still in flight land before the block's shared memory is
+     * released: wait for the last ones issued, again for a bounded time */
+    for (long t = issued > SUM_STAGES ? issued - SUM_STAGES : 0; t < issued; t++)
+      mbar_wait(&r.full[t % SUM_STAGES], (unsigned)((t / SUM_STAGES) & 1));
+    atomicExch(status, SUM_STATUS_COPY_TIMEOUT);
+  }
   /* the block's extremes and counts (value i at blk[i gridDim.x + block]) */
-  if (!r.fail) {
+  if (!failed) {
     double *bo = blk + blockIdx.x;
     const long bs = gridDim.x;
     if constexpr (PASS == 1) {
@@ -762,15 +796,6 @@ __global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>()
       block_extremes<6, WARPS>(X, 0x9u, red, bo, bs);
     }
   }
-  if (r.fail && threadIdx.x == 0) {
-    /* copies still in flight land before the block's shared memory is
-     * released: wait for them too, again for a bounded time */
-    for (long t = it + 1; t < p.issued; t++)
-      mbar_wait(&r.bar[t % SUM_STAGES], (unsigned)((t / SUM_STAGES) & 1));
-    if (!mbar_test(&r.bar[it % SUM_STAGES], (unsigned)((it / SUM_STAGES) & 1)))
-      mbar_wait(&r.bar[it % SUM_STAGES], (unsigned)((it / SUM_STAGES) & 1));
-    atomicExch(status, SUM_STATUS_COPY_TIMEOUT);
-  }
 }
 
 /* Combine partials: `n_dd` double-double values from the chunk partials
@@ -779,8 +804,8 @@ __global__ void __launch_bounds__(sum_threads<PASS>(), sum_blocks_per_sm<PASS>()
  * `nplain_rows` per value) to out[plain_base + k], value k a minimum when bit
  * k of `min_mask` is set, a maximum when bit k of `max_mask` is set, else a
  * sum.  One block per value: thread t takes rows t, t + COMBINE_THREADS, ...
- * in order, then the lanes combine in a fixed tree and the warps in index
- * order. */
+ * in order (COMBINE_BATCH loads in flight at a time), then the lanes combine
+ * in a fixed tree and the warps in index order. */
 __global__ void __launch_bounds__(COMBINE_THREADS)
   combine_partials(const double *part, int nchunks, int n_dd, const double *plain, int nplain_rows, int n_plain,
                    int plain_base, unsigned min_mask, unsigned max_mask, double *out) {
@@ -789,9 +814,19 @@ __global__ void __launch_bounds__(COMBINE_THREADS)
   if (v < n_dd) {
     const double *ph = part + (size_t)(2 * v) * nchunks, *pl = ph + nchunks;
     trkcr_dd acc = trkcr_make(0.0, 0.0);
-#pragma unroll 4
-    for (int c = threadIdx.x; c < nchunks; c += COMBINE_THREADS)
-      acc = dd_add(acc, trkcr_make(ph[c], pl[c]));
+    for (int c0 = threadIdx.x; c0 < nchunks; c0 += COMBINE_THREADS * COMBINE_BATCH) {
+      /* the batch's loads first, all in flight together, then the sums in order */
+      double h[COMBINE_BATCH], l[COMBINE_BATCH];
+#pragma unroll
+      for (int j = 0; j < COMBINE_BATCH; j++) {
+        const int c = c0 + j * COMBINE_THREADS;
+        h[j] = c < nchunks ? ph[c] : 0.0;
+        l[j] = c < nchunks ? pl[c] : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < COMBINE_BATCH; j++)
+        acc = dd_add(acc, trkcr_make(h[j], l[j]));
+    }
     for (int off = 16; off > 0; off >>= 1) {
       const double h = __shfl_down_sync(0xffffffffu, acc.hi, off), l = __shfl_down_sync(0xffffffffu, acc.lo, off);
       acc = dd_add(acc, trkcr_make(h, l));
@@ -812,10 +847,19 @@ __global__ void __launch_bounds__(COMBINE_THREADS)
     const int k = v - n_dd, q = plain_base + k;
     const int op = ((min_mask >> k) & 1u) ? 1 : (((max_mask >> k) & 1u) ? 2 : 0);
     const double *px = plain + (size_t)k * nplain_rows;
-    double acc = op == 0 ? 0.0 : (op == 1 ? OBS_BIG : -OBS_BIG);
-#pragma unroll 4
-    for (int c = threadIdx.x; c < nplain_rows; c += COMBINE_THREADS)
-      acc = op == 0 ? __dadd_rn(acc, px[c]) : (op == 1 ? fmin(acc, px[c]) : fmax(acc, px[c]));
+    const double init = op == 0 ? 0.0 : (op == 1 ? OBS_BIG : -OBS_BIG);
+    double acc = init;
+    for (int c0 = threadIdx.x; c0 < nplain_rows; c0 += COMBINE_THREADS * COMBINE_BATCH) {
+      double x[COMBINE_BATCH];
+#pragma unroll
+      for (int j = 0; j < COMBINE_BATCH; j++) {
+        const int c = c0 + j * COMBINE_THREADS;
+        x[j] = c < nplain_rows ? px[c] : init;
+      }
+#pragma unroll
+      for (int j = 0; j < COMBINE_BATCH; j++)
+        acc = op == 0 ? __dadd_rn(acc, x[j]) : (op == 1 ? fmin(acc, x[j]) : fmax(acc, x[j]));
+    }
     for (int off = 16; off > 0; off >>= 1) {
       const double x = __shfl_down_sync(0xffffffffu, acc, off);
       acc = op == 0 ? __dadd_rn(acc, x) : (op == 1 ? fmin(acc, x) : fmax(acc, x));
@@ -958,11 +1002,11 @@ int sums_grid(const Ctx &c, int *grid) {
 }
 
 /* one pass of the beam sums into the chunk partials `part` and the block
- * values `blk` over `grid` blocks; `counter` and `status` are device ints
- * the caller has zeroed */
+ * values `blk` over `grid` blocks; `status` is a device int the caller has
+ * zeroed */
 template <int PASS, int F>
-int launch_sums(const Ctx &c, const Select &s, const double *tot1, int sparse, int grid, int *counter, int *status,
-                double *part, double *blk) {
+int launch_sums(const Ctx &c, const Select &s, const double *tot1, int sparse, int grid, int *status, double *part,
+                double *blk) {
   auto kernel = beam_sums<PASS, F>;
   static int configured[64] = {0}; /* per device: the shared-memory attribute is set */
   if (c.device < 0 || c.device >= 64 || !configured[c.device]) {
@@ -971,7 +1015,7 @@ int launch_sums(const Ctx &c, const Select &s, const double *tot1, int sparse, i
       configured[c.device] = 1;
   }
   const unsigned smem = SUM_STAGES * layout_of<F, sum_tile<PASS>()>(s).stage_bytes;
-  kernel<<<grid, sum_threads<PASS>(), smem, c.st>>>(beam_of(c), s, tot1, sparse, counter, status, part, blk);
+  kernel<<<grid, sum_threads<PASS>(), smem, c.st>>>(beam_of(c), s, tot1, sparse, status, part, blk);
   OBS_CUDA(cudaGetLastError());
   return TRK_OK;
 }
@@ -984,8 +1028,8 @@ int blocks_of(const Ctx &c) {
 }
 
 /* pass 1 on the device: chunk partials and block values, then their
- * combination into tot1; `ctl` (4 ints: chunk counters of the passes,
- * status) is zeroed here */
+ * combination into tot1; `ctl` (4 ints, the status word last) is zeroed
+ * here */
 int enqueue_pass1(const Ctx &c, Scratch &sc, const Select &s, int F, double *tot1, int *ctl) {
   const int nb = blocks_of<1>(c);
   int grid, rc;
@@ -997,19 +1041,19 @@ int enqueue_pass1(const Ctx &c, Scratch &sc, const Select &s, int F, double *tot
   OBS_CUDA(cudaMemsetAsync(ctl, 0, 4 * sizeof(int), c.st));
   switch (F) {
   case 0:
-    rc = launch_sums<1, 0>(c, s, nullptr, 0, grid, ctl, ctl + 3, part, blk);
+    rc = launch_sums<1, 0>(c, s, nullptr, 0, grid, ctl + 3, part, blk);
     break;
   case SF_TIME:
-    rc = launch_sums<1, SF_TIME>(c, s, nullptr, 0, grid, ctl, ctl + 3, part, blk);
+    rc = launch_sums<1, SF_TIME>(c, s, nullptr, 0, grid, ctl + 3, part, blk);
     break;
   case SF_TIME | SF_ID:
-    rc = launch_sums<1, SF_TIME | SF_ID>(c, s, nullptr, 0, grid, ctl, ctl + 3, part, blk);
+    rc = launch_sums<1, SF_TIME | SF_ID>(c, s, nullptr, 0, grid, ctl + 3, part, blk);
     break;
   case SF_TIME | SF_PZ:
-    rc = launch_sums<1, SF_TIME | SF_PZ>(c, s, nullptr, 0, grid, ctl, ctl + 3, part, blk);
+    rc = launch_sums<1, SF_TIME | SF_PZ>(c, s, nullptr, 0, grid, ctl + 3, part, blk);
     break;
   case SF_TIME | SF_ID | SF_PZ:
-    rc = launch_sums<1, SF_TIME | SF_ID | SF_PZ>(c, s, nullptr, 0, grid, ctl, ctl + 3, part, blk);
+    rc = launch_sums<1, SF_TIME | SF_ID | SF_PZ>(c, s, nullptr, 0, grid, ctl + 3, part, blk);
     break;
   default:
     return trk_set_error(TRK_ERR_ARG, "beam sums: no pass-1 variant %d", F);
@@ -1138,11 +1182,11 @@ int trk_accumulate_beam_sums(trk_context *ctx, trk_beam_sums *sums, double p_cen
         return rc;
       const int sparse = (flags & TRK_SUMS_SPARSE) ? 1 : 0;
       if (id)
-        rc = launch_sums<2, SF_TIME | SF_ID>(c, s2, tot1, sparse, grid, ctl + 1, ctl + 3, part, blk);
+        rc = launch_sums<2, SF_TIME | SF_ID>(c, s2, tot1, sparse, grid, ctl + 3, part, blk);
       else
-        rc = launch_sums<2, SF_TIME>(c, s2, tot1, sparse, grid, ctl + 1, ctl + 3, part, blk);
+        rc = launch_sums<2, SF_TIME>(c, s2, tot1, sparse, grid, ctl + 3, part, blk);
       if (!rc && pz_mode)
-        rc = launch_sums<2, SF_TIME | SF_ID | SF_PZ>(c, s2, tot1, sparse, grid, ctl + 2, ctl + 3, part, blk);
+        rc = launch_sums<2, SF_TIME | SF_ID | SF_PZ>(c, s2, tot1, sparse, grid, ctl + 3, part, blk);
       if (rc)
         return rc;
       /* sigma, and sigman when asked for; the s and t extremes */
