@@ -54,6 +54,12 @@ void set_up_trwake(TRWAKE *wakeData, RUN *run, long pass, long particles, CHARGE
 static trk_context *g_ctx = NULL;
 static GPUBASE g_base;
 static long g_pass = 0, g_elem = -1, g_np = 0;
+/* the pass the next run starts at (trk_hooks_begin_pass before the run) */
+static long g_pass_start = 0;
+/* the first element of the line and whether it has been seen this run: a
+ * pass begins each time do_tracking reaches it again */
+static const void *g_first_elem = NULL;
+static int g_first_seen = 0;
 static int g_fast = -1;
 static double *g_buf = NULL;
 static long *g_loss_pass = NULL;
@@ -218,8 +224,13 @@ void gpuBaseInit(double **coord, long nOriginal, double **accepted, double **los
   g_base.coord = coord;
   g_base.nOriginal = nOriginal;
   g_base.nLeft = nOriginal;
-  g_pass = 0;
+  /* the beam is on the device from here on: do_tracking's first filter
+   * (src/do_tracking.c:478-484) runs before any element sets the flag */
+  g_base.elementOnGpu = 1;
+  g_pass = g_pass_start;
   g_elem = -1;
+  g_first_elem = NULL;
+  g_first_seen = 0;
 }
 
 double **forceParticlesToCpu(const char *reason) {
@@ -240,7 +251,14 @@ double **forceParticlesToCpu(const char *reason) {
 
 const long *trk_hooks_loss_elements(void) { return g_loss_elem; }
 
+/* do_tracking reads the particles from its coordinate array after this
+ * call (src/do_tracking.c:3172-3178), so the device beam comes back first */
 void gpuBaseDealloc(void) {
+  if (g_ctx && g_base.coord)
+    forceParticlesToCpu("gpuBaseDealloc");
+  g_base.coord = NULL;
+  g_first_elem = NULL;
+  g_first_seen = 0;
   if (g_ctx)
     trk_context_destroy(g_ctx);
   g_ctx = NULL;
@@ -250,12 +268,25 @@ void gpuBaseDealloc(void) {
 }
 
 void trk_hooks_begin_pass(long i_pass) {
-  g_pass = i_pass;
+  g_pass = g_pass_start = i_pass;
   g_elem = -1;
+  g_first_elem = NULL;
+  g_first_seen = 0;
 }
 
+/* do_tracking calls this for every element of every pass
+ * (src/do_tracking.c:1113): the element index counts up within a pass, and
+ * reaching the line's first element again starts the next pass (a caller
+ * that drives its own loop calls trk_hooks_begin_pass instead) */
 void setElementGpuData(void *eptr) {
   const ELEMENT_LIST *e = (const ELEMENT_LIST *)eptr;
+  if (!g_first_seen) {
+    g_first_elem = e;
+    g_first_seen = 1;
+  } else if (e && e == g_first_elem && g_elem >= 0) {
+    g_pass++;
+    g_elem = -1;
+  }
   g_elem++;
   g_base.elementOnGpu = e && library_type(e->type) >= 0;
 }

@@ -197,6 +197,7 @@ def load_ref():
     lib.trk_param_default.argtypes = [I, I]
     lib.trk_param_default.restype = D
     lib.ref_track.argtypes = [P, DP, L, L, L, DP, ctypes.POINTER(_Result)]
+    lib.ref_do_tracking.argtypes = [P, DP, L, L, L, DP, ctypes.POINTER(_Result)]
     lib.ref_set_cr_math.argtypes = [I]
     lib.ref_set_exact_sums.argtypes = [I]
     lib.ref_param_defaults.argtypes = [I, DP, I]
@@ -204,8 +205,12 @@ def load_ref():
     return lib
 
 
-def track_ref(lattice, beam, n_passes, p_central, pass_offset=0, exact_sums=False, cr_math=False):
-    """As track(), through elegant's own element functions."""
+def track_ref(lattice, beam, n_passes, p_central, pass_offset=0, exact_sums=False, cr_math=False, loop="driver"):
+    """As track(), through elegant's own element functions.  loop="driver":
+    the element calls of do_tracking's switch in oracle/ref/ref_driver.c's
+    pass loop; loop="do_tracking": elegant's own do_tracking()
+    (src/do_tracking.c:144), which records no loss element (column 8 is -2
+    for lost rows)."""
     lib = load_ref()
     lib.ref_set_exact_sums(1 if exact_sums else 0)
     lib.ref_set_cr_math(1 if cr_math else 0)
@@ -215,8 +220,9 @@ def track_ref(lattice, beam, n_passes, p_central, pass_offset=0, exact_sums=Fals
     pc = ctypes.c_double(p_central)
     res = _Result()
     try:
-        _check(lib, lib.ref_track(nat.ptr, rows.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), rows.shape[0],
-                                  n_passes, pass_offset, ctypes.byref(pc), ctypes.byref(res)))
+        entry = lib.ref_do_tracking if loop == "do_tracking" else lib.ref_track
+        _check(lib, entry(nat.ptr, rows.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), rows.shape[0], n_passes,
+                          pass_offset, ctypes.byref(pc), ctypes.byref(res)))
     finally:
         nat.close()
         lib.ref_set_exact_sums(0)
@@ -246,9 +252,11 @@ def refgpu_available():
     return os.path.exists(REF_GPU_LIB)
 
 
-def track_refgpu(lattice, beam, n_passes, p_central, pass_offset=0):
+def track_refgpu(lattice, beam, n_passes, p_central, pass_offset=0, loop="driver"):
     """As track_ref(), with every element going through elegant's GPU hooks
-    into the CUDA library (parity build).  Rows come back survivors first."""
+    into the CUDA library (parity build).  Rows come back survivors first.
+    loop="do_tracking": elegant's own do_tracking() drives the hooks
+    (column 8 is -2 for lost rows, as track_ref's do_tracking loop gives)."""
     global _refgpu
     if _refgpu is None:
         lib = ctypes.CDLL(REF_GPU_LIB)
@@ -262,6 +270,7 @@ def track_refgpu(lattice, beam, n_passes, p_central, pass_offset=0):
         lib.trk_lattice_set.argtypes = [P, I, ctypes.c_char_p, D]
         lib.trk_lattice_set_wake.argtypes = [P, I, DP, DP, DP, L]
         lib.refgpu_track.argtypes = [P, DP, L, L, L, DP, ctypes.POINTER(_Result)]
+        lib.refgpu_do_tracking.argtypes = [P, DP, L, L, L, DP, ctypes.POINTER(_Result)]
         _refgpu = lib
     lib = _refgpu
     nat = lattice.native(lib)
@@ -270,8 +279,9 @@ def track_refgpu(lattice, beam, n_passes, p_central, pass_offset=0):
     pc = ctypes.c_double(p_central)
     res = _Result()
     try:
-        _check(lib, lib.refgpu_track(nat.ptr, rows.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), rows.shape[0],
-                                     n_passes, pass_offset, ctypes.byref(pc), ctypes.byref(res)))
+        entry = lib.refgpu_do_tracking if loop == "do_tracking" else lib.refgpu_track
+        _check(lib, entry(nat.ptr, rows.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), rows.shape[0], n_passes,
+                          pass_offset, ctypes.byref(pc), ctypes.byref(res)))
     finally:
         nat.close()
     return rows, res.n_left, res.particle_passes

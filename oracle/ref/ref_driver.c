@@ -33,9 +33,11 @@
 #include "gpu_base.h"
 #include "gpu_compute_centroids.h"
 #define REF_ENTRY refgpu_track
+#define REF_DT_ENTRY refgpu_do_tracking
 #define REF_OBSERVE refgpu_observe
 #else
 #define REF_ENTRY ref_track
+#define REF_DT_ENTRY ref_do_tracking
 #define REF_OBSERVE ref_observe
 #endif
 
@@ -406,6 +408,82 @@ int REF_ENTRY(const trk_lattice *l, double *rows, long np, long n_passes, long p
   free(coord);
   free(lp);
   free(le);
+  free_beamline(&bl);
+  return TRK_OK;
+}
+
+/* The same run through elegant's own do_tracking() (src/do_tracking.c:144),
+ * compiled unmodified: the pass loop, the element switch, the MAXAMP state,
+ * the after-element filters, CHARGE and the loss record are the reference's
+ * own, on the same element structures as ref_track builds.  Flags:
+ * SILENT_RUNNING | INHIBIT_FILE_OUTPUT, no fiducial passes (n_passes_fiducial
+ * = 0).  Rows come back in do_tracking's order, survivors first; a lost row
+ * keeps the loss pass do_tracking records (recordLostParticles,
+ * src/do_tracking.c:4669-4690); do_tracking records no loss element, so
+ * column 8 is -2.  In the hook build the beam goes to the device in
+ * do_tracking's gpuBaseInit and comes back in its gpuBaseDealloc
+ * (src/do_tracking.c:413, :3172-3178); the pass the hooks record losses
+ * with starts at pass_offset. */
+int REF_DT_ENTRY(const trk_lattice *l, double *rows, long np, long n_passes, long pass_offset, double *P_central,
+                 orc_result *result) {
+  if (!l || (!rows && np) || !P_central || l->n < 1)
+    return TRK_ERR_ARG;
+  ref_beamline bl;
+  memset(&bl, 0, sizeof(bl));
+  int rc = build_beamline(l, &bl);
+  if (rc) {
+    free_beamline(&bl);
+    return rc;
+  }
+  /* drifts track through their matrices (do_tracking's MATRIX_TRACKING branch) */
+  for (long i = 0; i < bl.n; i++)
+    bl.el[i].matrix = bl.drift[i];
+  totalPropertiesPerParticle = REF_ROW;
+  sizeOfParticle = REF_ROW * sizeof(double);
+  double *buf = (double *)calloc((size_t)(np > 0 ? np : 1) * REF_ROW, sizeof(double));
+  double **coord = (double **)calloc(np > 0 ? np : 1, sizeof(double *));
+  for (long i = 0; i < np; i++) {
+    coord[i] = buf + (size_t)i * REF_ROW;
+    memcpy(coord[i], rows + (size_t)i * ORC_STRIDE, 7 * sizeof(double));
+    coord[i][lossPassIndex] = -1;
+    coord[i][8] = 0;
+    coord[i][REF_ORIG] = i;
+  }
+  LINE_LIST line;
+  memset(&line, 0, sizeof(line));
+  line.name = "oracle_ref";
+  line.elem = bl.el;
+  line.n_elems = bl.n;
+  line.elast = &bl.el[bl.n - 1];
+  RUN run;
+  memset(&run, 0, sizeof(run));
+  run.default_order = 2;
+  run.wrap_around = 1;
+  run.rootname = "oracle_ref";
+  run.p_central = *P_central;
+  long effort = 0;
+  double final_charge = 0;
+#ifdef REF_GPU_HOOKS
+  trk_hooks_begin_pass(pass_offset);
+#endif
+  const long n_left = do_tracking(NULL, coord, np, &effort, &line, P_central, NULL, NULL, NULL, NULL, &run, 0,
+                                  SILENT_RUNNING | INHIBIT_FILE_OUTPUT, n_passes, pass_offset, NULL, NULL,
+                                  &final_charge, NULL, NULL);
+  for (long i = 0; i < np; i++) {
+    double *r = rows + (size_t)i * ORC_STRIDE;
+    memcpy(r, coord[i], 7 * sizeof(double));
+    r[7] = i < n_left ? -1 : coord[i][lossPassIndex];
+    r[8] = i < n_left ? -1 : -2;
+  }
+  if (result) {
+    result->n_left = n_left;
+    result->particle_passes = effort;
+    result->p_central = *P_central;
+  }
+  for (long i = 0; i < bl.n; i++)
+    bl.el[i].matrix = NULL;
+  free(buf);
+  free(coord);
   free_beamline(&bl);
   return TRK_OK;
 }

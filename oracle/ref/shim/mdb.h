@@ -223,6 +223,12 @@ long SDDS_TransferParameterDefinition();
 long SDDS_CopyPage();
 long SDDS_CopyParameters();
 long match_string();
+/* match_string modes (values of this shim: match_string is not on the tracking path) */
+#define DCL_STYLE_MATCH 0x0001
+#define UNIQUE_MATCH 0x0002
+#define CASE_SENSITIVE 0x0004
+#define MATCH_WHOLE_STRING 0x0008
+#define EXACT_MATCH (CASE_SENSITIVE | MATCH_WHOLE_STRING)
 long str_in();
 long fexists();
 long get_long();

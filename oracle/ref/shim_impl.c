@@ -213,12 +213,6 @@ void push_log() {}
 void pop_log() {}
 
 /* ---------------------------------- elegant functions from other files */
-/* beta from momentum and delta (elegant's do_tracking.c helper) */
-double beta_from_delta(double p, double delta) {
-  p *= 1 + delta;
-  return p / sqrt(p * p + 1);
-}
-
 /* rows are exchanged by content, sizeOfParticle bytes each */
 void swapParticles(double *p1, double *p2) {
   double buffer[MAX_PROPERTIES_PER_PARTICLE];
@@ -250,7 +244,13 @@ void exitElegant(long status) {
   abort();
 }
 
+/* warnings (src/warnings.c, which keeps them in the SDDS toolkit's hash
+ * tables) print nothing here */
 void printWarningForTracking(char *text, char *detail) {
+  (void)text;
+  (void)detail;
+}
+void printWarning(char *text, char *detail) {
   (void)text;
   (void)detail;
 }
@@ -291,4 +291,62 @@ long fill_double_array(double *array, long n, double value) {
   for (long i = 0; i < n; i++)
     array[i] = value;
   return 1;
+}
+
+/* ------------------------- do_tracking's calls outside the tracking path
+ * do_tracking() (src/do_tracking.c) calls these on every run; for the
+ * elements of the tracking path they have nothing to do: there are no
+ * obstructions and no RPN expressions read the stored values. */
+void setObstructionsMode(long state) { (void)state; }
+long rpn_create_mem(char *name, int is_string) {
+  (void)name;
+  (void)is_string;
+  return 0;
+}
+long rpn_store(double value, char *str_value, long memory) {
+  (void)value;
+  (void)str_value;
+  (void)memory;
+  return 0;
+}
+
+/* src/modulate.c and src/ramp.c are built from namelist files this tree
+ * does not generate; their first step returns when no modulation or ramp is
+ * defined (src/modulate.c:26-27), which is the only case here */
+long applyElementModulations(MODULATION_DATA *modData, LINE_LIST *beamline, double pCentral, double **coord, long np,
+                             RUN *run, long iPass) {
+  (void)beamline;
+  (void)pCentral;
+  (void)coord;
+  (void)np;
+  (void)run;
+  (void)iPass;
+  if (modData->nItems > 0)
+    bombElegant("element modulations are outside the tracking path", NULL);
+  return 0;
+}
+long applyElementRamps(RAMP_DATA *rampData, LINE_LIST *beamline, double pCentral, RUN *run, long iPass) {
+  (void)beamline;
+  (void)pCentral;
+  (void)run;
+  (void)iPass;
+  if (rampData->nItems > 0)
+    bombElegant("element ramps are outside the tracking path", NULL);
+  return 0;
+}
+
+/* src/insertSCeffects.cc (C++, built from a namelist file this tree does
+ * not generate): the count of space-charge insertion specifications, none
+ * on the tracking path */
+long getSCMULTSpecCount(void) { return 0; }
+
+/* src/obstructionData.c (built from a namelist file this tree does not
+ * generate): with no obstruction defined no particle is inside one, so the
+ * filter keeps every row */
+long filterParticlesWithObstructions(double **coord, long np, double **accepted, double z, double P_central) {
+  (void)coord;
+  (void)accepted;
+  (void)z;
+  (void)P_central;
+  return np;
 }
