@@ -35,9 +35,11 @@ void startGpuTimer(void);
 void startCpuTimer(void);
 void compareGpuCpu(long n_part, const char *name);
 
-/* Not in the reference: do_tracking's pass loop calls this at the start of
- * every pass so losses are recorded with their pass, and setElementGpuData
- * counts elements from there for the loss element index. */
+/* Not in the reference: the pass the hooks record losses with.  The hooks
+ * count passes themselves (setElementGpuData starts the next pass when the
+ * line's first element comes round again), starting at the pass given here
+ * before a run (0 when never called); a caller that drives its own pass
+ * loop may call it at the start of every pass instead. */
 void trk_hooks_begin_pass(long i_pass);
 /* loss element index (position in the pass, from setElementGpuData) of each
  * row returned by the last forceParticlesToCpu; -1 for survivors */
