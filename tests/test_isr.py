@@ -118,3 +118,25 @@ def test_isr_repeatable_and_independent_of_launch_shape(tracker):
         outs.append(tracker.store()[1])
     assert np.array_equal(outs[0], outs[1])
     assert not np.array_equal(outs[0], outs[2])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("isr1part", [0, 1])
+def test_isr1part_single_particle(tracker, isr1part):
+    """ISR1PART (src/multipole.c:758, src/csbend.c:963): with 0, a beam of
+    one particle gets no quantum excitation (classical radiation stays on);
+    with 1 it does.  The library decides on the beam it was handed (the
+    reference on the particles entering the element, which differ only once
+    all but one have been lost)."""
+    beam = configs.gaussian_beam(1, seed=83)
+    outs = {}
+    for isr in (0, 1):
+        lat = single("CSBEND", L=1.0, ANGLE=2 * math.pi / 80, N_KICKS=16, SYNCH_RAD=1, ISR=isr,
+                     ISR1PART=isr1part)
+        tracker.load(beam)
+        tracker.track(lat, 2, PC, isr_seed=SEED, fast=False)
+        outs[isr] = tracker.store()[1]
+    if isr1part == 0:
+        assert np.array_equal(outs[0], outs[1])
+    else:
+        assert not np.array_equal(outs[0], outs[1])

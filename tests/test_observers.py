@@ -103,6 +103,59 @@ def test_gpu_beam_sums_vs_oracle(tracker, flags):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 7, 1023, 1_000_003, 2_500_001])
+def test_gpu_beam_sums_sizes(tracker, n):
+    """Beams of one particle, ragged tiles and chunks, and sizes with
+    several chunks per block (the chunk size follows the particle count);
+    with an ID window so the ID column is staged too."""
+    beam = _beam(n, seed=66)
+    for kw in ({}, {"start_pid": n // 5, "end_pid": (4 * n) // 5 + 1}):
+        g = _gpu_sums(tracker, beam, SECOND, repeats=1, **kw)
+        with pyoracle.modes(exact_sums=True, cr_math=False):
+            s = pyoracle.zero_beam_sums()
+            pyoracle.accumulate_beam_sums(beam, s, PC, 1e-12, flags=SECOND, **kw)
+        _same_sums(g, s, sigma_rel=1e-13)
+    c, m = tracker.centroids()
+    with pyoracle.modes(exact_sums=True, cr_math=False):
+        assert np.array_equal(c, pyoracle.beam_centroids(beam)) and m == n
+
+
+@pytest.mark.gpu
+def test_gpu_observer_scratch_per_context():
+    """Observer scratch belongs to its context: several contexts created,
+    used side by side on beams of different sizes, and destroyed, give the
+    oracle's sums every time and give their device memory back."""
+    import torch
+    from elegant_b200 import BeamSums, Tracker
+    beams = [_beam(n, seed=67 + n % 5) for n in (30_000, 7_001, 120_000)]
+    with pyoracle.modes(exact_sums=True, cr_math=False):
+        want = []
+        for b in beams:
+            s = pyoracle.zero_beam_sums()
+            pyoracle.accumulate_beam_sums(b, s, PC, 1e-12, flags=SECOND)
+            want.append(s)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(0)[0]
+    for _ in range(3):
+        trks = [Tracker(0) for _ in beams]
+        try:
+            for trk, b in zip(trks, beams):
+                trk.load(b)
+            for _ in range(2):
+                for trk, w in zip(trks, want):
+                    g = BeamSums.zeroed()
+                    trk.accumulate_beam_sums(g, PC, mp_charge=1e-12, flags=SECOND)
+                    _same_sums(g, w, sigma_rel=1e-13)
+                    trk.sort_by_id()
+        finally:
+            for trk in trks:
+                trk.close()
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info(0)[0]
+    assert free0 - free1 < 64 << 20, (free0, free1)
+
+
+@pytest.mark.gpu
 def test_gpu_beam_sums_selection_and_losses(tracker):
     """ID and time windows; lost particles are left out."""
     beam = _beam(20_000, seed=64)
