@@ -508,7 +508,9 @@ int edge_mode(int on, int effects, int edge_order, const char *name) {
     return edge_order <= 1 ? EDGE_HWANG1 : EDGE_HWANG2;
   if (effects == 4)
     return EDGE_HWANGL;
-  trk_set_error(TRK_ERR_UNSUPPORTED, "CSBEND %s: EDGE_EFFECTS=%d is not on this path (0 to 4 are)", name, effects);
+  if (effects == 5)
+    return edge_order <= 1 ? EDGE_CURV1 : EDGE_CURV2;
+  trk_set_error(TRK_ERR_UNSUPPORTED, "CSBEND %s: EDGE_EFFECTS=%d is not on this path (0 to 5 are)", name, effects);
   return -1;
 }
 
@@ -742,6 +744,20 @@ int compile_bend(const trk_lattice *l, int idx, double Po, trk_op *op, std::vect
   d[BD_FF1] = TRK_P(e, CSBEND_FINT1) >= 0 ? TRK_P(e, CSBEND_FINT1) : TRK_P(e, CSBEND_FINT);
   d[BD_FF2] = TRK_P(e, CSBEND_FINT2) >= 0 ? TRK_P(e, CSBEND_FINT2) : TRK_P(e, CSBEND_FINT);
   d[BD_GAP] = 2 * TRK_P(e, CSBEND_HGAP);
+  /* curved-dipole fringe: K1 as track_through_csbend passes it (b[1]/rho0
+   * after the sign change of a negative bend, src/csbend.c:1193, :1370), the
+   * FRINGE1K0..6 / FRINGE2K0..6 integrals and the edge angle's tan and sec,
+   * rounded once as curvedDipoleFringe forms them (src/csbend.c:5720-5721) */
+  d[BD_K1F] = b[1] / rho0;
+  if (m1 == EDGE_CURV1 || m1 == EDGE_CURV2 || m2 == EDGE_CURV1 || m2 == EDGE_CURV2) {
+    for (int k = 0; k < 2; k++) {
+      const double ek = k ? e2 : e1;
+      for (int j = 0; j < 7; j++)
+        field.push_back(e->p[(k ? P_CSBEND_FRINGE2K0 : P_CSBEND_FRINGE1K0) + j]);
+      field.push_back(trkcr_tan(ek));
+      field.push_back(1. / trkcr_cos(ek));
+    }
+  }
   d[BD_N] = n;
   d[BD_RHOINV] = 1.0 / rho0;
   d[BD_INVRHOA] = 1.0 / rho_actual;

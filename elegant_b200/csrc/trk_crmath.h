@@ -38,6 +38,8 @@
 #define TRKCR_ASIN(x) asin(x)
 #define TRKCR_COS(x) cos(x)
 #define TRKCR_EXP(x) exp(x)
+#define TRKCR_SINH(x) sinh(x)
+#define TRKCR_COSH(x) cosh(x)
 #define TRKCR_LDEXP(x, k) ldexp((x), (k))
 #define TRKCR_HIWORD(x) ((unsigned)__double2hiint(x))
 #else
@@ -54,6 +56,8 @@
 #define TRKCR_ASIN(x) asin(x)
 #define TRKCR_COS(x) cos(x)
 #define TRKCR_EXP(x) exp(x)
+#define TRKCR_SINH(x) sinh(x)
+#define TRKCR_COSH(x) cosh(x)
 #define TRKCR_LDEXP(x, k) ldexp((x), (k))
 #include <stdint.h>
 #include <string.h>
@@ -619,6 +623,76 @@ TRKCR_FN double trkcr_exp(double x) {
       return u;
   }
   return trkcr_exp_slow(x);
+}
+
+/* a / b for a double-double a and a double b: the quotient of the high
+ * parts and one correction from the exact remainder */
+TRKCR_FN trkcr_dd trkcr_div_d(trkcr_dd a, double b) {
+  const double q1 = TRKCR_DIV(a.hi, b);
+  const trkcr_dd p = trkcr_two_prod(q1, b);
+  const double r = TRKCR_ADD(TRKCR_SUB(TRKCR_SUB(a.hi, p.hi), p.lo), a.lo);
+  return trkcr_two_sum(q1, TRKCR_DIV(r, b));
+}
+
+/* 1 / b for a double-double b, in the same way */
+TRKCR_FN trkcr_dd trkcr_recip_dd(trkcr_dd b) {
+  const double q1 = TRKCR_DIV(1.0, b.hi);
+  trkcr_dd p = trkcr_two_prod(q1, b.hi);
+  p.lo = TRKCR_FMA(q1, b.lo, p.lo);
+  const trkcr_dd r = trkcr_add(trkcr_make(1.0, 0.0), trkcr_make(-p.hi, -p.lo));
+  return trkcr_two_sum(q1, TRKCR_DIV(r.hi, b.hi));
+}
+
+/* sinh and cosh of |x| in double-double: the Taylor series below 1/8 (its
+ * terms fall by (1/8)^2 / 6 at least, so ten reach 2^-110 of the sum and
+ * nothing cancels), (e^|x| -/+ e^-|x|)/2 above */
+TRKCR_FN trkcr_dd trkcr_sinh_dd(double ax) {
+  if (ax < 0.125) {
+    const trkcr_dd x2 = trkcr_two_prod(ax, ax);
+    trkcr_dd term = trkcr_make(ax, 0.0), sum = term;
+    for (int k = 1; k <= 10; k++) {
+      term = trkcr_div_d(trkcr_mul(term, x2), (double)((2 * k) * (2 * k + 1)));
+      sum = trkcr_add(sum, term);
+    }
+    return sum;
+  }
+  const trkcr_dd E = trkcr_exp_dd(ax), iE = trkcr_recip_dd(E);
+  const trkcr_dd d = trkcr_add(E, trkcr_neg(iE));
+  return trkcr_make(TRKCR_MUL(d.hi, 0.5), TRKCR_MUL(d.lo, 0.5));
+}
+
+TRKCR_FN trkcr_dd trkcr_cosh_dd(double ax) {
+  if (ax < 0.125) {
+    const trkcr_dd x2 = trkcr_two_prod(ax, ax);
+    trkcr_dd term = trkcr_make(1.0, 0.0), sum = term;
+    for (int k = 1; k <= 10; k++) {
+      term = trkcr_div_d(trkcr_mul(term, x2), (double)((2 * k - 1) * (2 * k)));
+      sum = trkcr_add(sum, term);
+    }
+    return sum;
+  }
+  const trkcr_dd E = trkcr_exp_dd(ax), iE = trkcr_recip_dd(E);
+  const trkcr_dd d = trkcr_add(E, iE);
+  return trkcr_make(TRKCR_MUL(d.hi, 0.5), TRKCR_MUL(d.lo, 0.5));
+}
+
+/* sinh, cosh rounded once from the double-double values (bend fringes
+ * only: not inlined); beyond |x| = 700 and for non-finite x, the library's */
+TRKCR_SLOW double trkcr_sinh(double x) {
+  if (x == 0.0 || !(fabs(x) <= 700.0))
+    return TRKCR_SINH(x);
+  const trkcr_dd v = trkcr_sinh_dd(fabs(x));
+  const double r = TRKCR_ADD(v.hi, v.lo);
+  return x < 0 ? -r : r;
+}
+
+TRKCR_SLOW double trkcr_cosh(double x) {
+  if (x == 0.0)
+    return 1.0;
+  if (!(fabs(x) <= 700.0))
+    return TRKCR_COSH(x);
+  const trkcr_dd v = trkcr_cosh_dd(fabs(x));
+  return TRKCR_ADD(v.hi, v.lo);
 }
 
 /*

@@ -44,6 +44,8 @@
 #define M_TAN(x) tan(x)
 #define M_SINCOS(x, s, c) sincos((x), (s), (c))
 #define M_EXP(x) exp(x)
+#define M_SINH(x) sinh(x)
+#define M_COSH(x) cosh(x)
 #else
 #define TRK_NS trk_exact
 #define M_SIN(x) trkcr_sin(x)
@@ -52,6 +54,8 @@
 #define M_TAN(x) trkcr_tan(x)
 #define M_SINCOS(x, s, c) trkcr_sincos((x), (s), (c))
 #define M_EXP(x) trkcr_exp(x)
+#define M_SINH(x) trkcr_sinh(x)
+#define M_COSH(x) trkcr_cosh(x)
 #endif
 
 namespace TRK_NS {
@@ -1161,8 +1165,119 @@ __device__ __noinline__ void fringe_hwang_lindberg(double &x, double &px, double
 #undef FR_P2
 #undef FR_P3
 
+/* R. Lindberg's curved-dipole fringe (curvedDipoleFringe, src/csbend.c:
+ * 5693-5969) in dipole canonical coordinates: the linear map through the
+ * fringe field from the edge integrals K0..K6 (fr[0..6]), the same at both
+ * ends, then for EDGE_ORDER > 1 the edge's second-order terms, which differ
+ * in sign between entrance (inFringe -1) and exit.  fr[7], fr[8]: tan and sec
+ * of the edge angle.  Each expression in the reference's operation order;
+ * returns the path-length change dtau (the reference adds -dtau to s). */
+__device__ __noinline__ double fringe_curved(double &x, double &px, double &y, double &py, double dp, double rho,
+                                             int inFringe, bool second_order, double K1,
+                                             const double *__restrict__ fr) {
+  const double x0 = x, px0 = px, y0 = y, py0 = py, dp0 = dp;
+  const double intK0 = __ldg(&fr[0]), intK1 = __ldg(&fr[1]), intK2 = __ldg(&fr[2]), intK3 = __ldg(&fr[3]),
+               intK4 = __ldg(&fr[4]), intK5 = __ldg(&fr[5]), intK6 = __ldg(&fr[6]);
+  const double tan_edge = __ldg(&fr[7]), sec_edge = __ldg(&fr[8]);
+  double x1, px1, y1, py1, dtau;
+  const double mx = (intK3 + intK4) / (1.0 + dp0);
+  const double my = intK3 / (1.0 + dp0);
+  const double delX = intK0 / (1.0 + dp0);
+  const double focX = intK1 + tan_edge / rho;
+  const double focY = intK2 / (1.0 + dp0);
+  if (fabs(mx) < 1.0e-5) {
+    x1 = x0 * M_EXP(-mx) + dp0 * delX * (1.0 - 0.5 * mx * (1.0 - mx / 3.0 + mx * mx / 12.0));
+    px1 = px0 * M_EXP(mx) + focX * (x0 * (1.0 + mx * mx / 6.0) + dp0 * delX * (0.5 + mx * mx / 24.0));
+    dtau = px0 * (mx * x0 + delX) / (1.0 + dp0) + delX * px0 * 0.5 * mx * (1.0 + mx / 3.0 + mx * mx / 12.0) +
+           focX * x0 * x0 * mx * (0.5 - (mx - 0.5 * mx * mx) / 3.0) / (1.0 + dp0) +
+           dp0 * focX * delX * (delX + mx * x0 / (1.0 + dp0)) * (1.0 + 0.05 * mx * mx) / 6.0 +
+           focX * delX * x0 * 0.5 * (1.0 + mx * mx / 12.0) / (1.0 + dp0) +
+           dp0 * focX * delX * (2.0 * mx * x0 - dp0 * delX) * (1.0 - mx * (0.75 - mx * (0.35 - 0.125 * mx))) /
+             (6.0 * (1.0 + dp0));
+  } else {
+    const double emx = M_EXP(-mx), epx = M_EXP(mx), e2mx = M_EXP(-2.0 * mx);
+    const double shx = M_SINH(mx), chx = M_COSH(mx);
+    x1 = x0 * emx + dp0 * delX * (1.0 - emx) / mx;
+    px1 = px0 * epx + focX * (x0 * shx / mx + dp0 * delX * (chx - 1.0) / (mx * mx));
+    dtau = px0 * (mx * x0 + delX) / (1.0 + dp0) + delX * px0 * (epx - 1.0 - mx) / mx +
+           focX * x0 * x0 * 0.25 * ((e2mx - 1.0) / mx + 2.0) / (1.0 + dp0) +
+           dp0 * focX * delX * (delX + mx * x0 / (1.0 + dp0)) * (shx - mx) / (mx * mx * mx) +
+           focX * delX * x0 * (chx - 1.0) / (mx * mx * (1.0 + dp0)) +
+           dp0 * focX * delX * (2.0 * mx * x0 - dp0 * delX) * 0.25 * (2.0 - (3.0 + e2mx - 4.0 * emx) / mx) /
+             (mx * mx * (1.0 + dp0));
+  }
+  if (fabs(my) < 1.0e-5) {
+    y1 = y0 * M_EXP(my);
+    py1 = py0 * M_EXP(-my) + y0 * (focY - focX) * (1.0 + my * my / 6.0);
+    dtau += (-my * py0 * y0 + 0.5 * (focY + focX * (my + my * my * (2.0 + my) / 3.0) * y0 * y0)) / (1.0 + dp0);
+  } else {
+    y1 = y0 * M_EXP(my);
+    py1 = py0 * M_EXP(-my) + y0 * (focY - focX) * M_SINH(my) / my;
+    dtau += (-my * py0 * y0 + 0.5 * (focY + 0.5 * focX * ((M_EXP(2.0 * my) - 1.0) / my - 2.0)) * y0 * y0) /
+            (1.0 + dp0);
+  }
+  if (second_order) {
+    const double sect2_rho = sec_edge * sec_edge / (rho * (1.0 + dp0));
+    const double tant_rho = tan_edge / (rho * (1.0 + dp0));
+    double x2, y2, px2, py2;
+    if (inFringe == -1) {
+      x2 = x1;
+      y2 = y1 * M_EXP(tan_edge * tant_rho * x1);
+      px2 = px1 - tan_edge * tant_rho * y1 * py1 - (tan_edge * (tan_edge * tant_rho / rho - K1) - 0.5 * intK6) * x1 * x1;
+      py2 = py1 * M_EXP(-tan_edge * tant_rho * x1);
+      dtau += -tan_edge * tant_rho * tant_rho * x1 * x1 * x1 / 3.0 - tant_rho * tant_rho * rho * x1 * y1 * py1;
+      x1 = x2 + 0.5 * sect2_rho * y2 * y2;
+      y1 = y2;
+      px1 = px2 + (0.5 * tant_rho / rho - 0.5 * intK5 - K1 * tan_edge + 0.25 * intK1 * sect2_rho) * y2 * y2;
+      py1 = py2 + (tant_rho / rho - intK5 - 2.0 * K1 * tan_edge + 0.5 * intK1 * sect2_rho) * x2 * y2 -
+            sect2_rho * y2 * px2;
+      dtau += (0.5 * sect2_rho * (0.25 * (2.0 * tan_edge * K1 + intK5) * y2 * y2 - px2) +
+               (0.5 * tant_rho / rho + 0.25 * intK1 * sect2_rho) * x2) *
+              y2 * y2 / (1.0 + dp0);
+      x2 = x1 / (1.0 + 0.5 * tan_edge * tant_rho * x1);
+      y2 = y1;
+      px2 = px1 * (1.0 + 0.5 * tan_edge * tant_rho * x1) * (1.0 + 0.5 * tan_edge * tant_rho * x1);
+      py2 = py1;
+      dtau += 0.5 * tant_rho * tant_rho * rho * x1 * x1 * px1;
+    } else {
+      x2 = x1;
+      y2 = y1 * M_EXP(-tan_edge * tant_rho * x1);
+      px2 = px1 + tan_edge * tant_rho * y1 * py1 +
+            (tan_edge * (0.5 * tan_edge * tant_rho / rho + K1) + 0.5 * intK6) * x1 * x1;
+      py2 = py1 * M_EXP(tan_edge * tant_rho * x1);
+      dtau += tan_edge * tant_rho * tant_rho * x1 * x1 * x1 / 6.0 + tant_rho * tant_rho * rho * x1 * y1 * py1;
+      x1 = x2 - 0.5 * sect2_rho * y2 * y2;
+      y1 = y2;
+      px1 = px2 + (0.5 * tan_edge * tan_edge * tant_rho / rho - 0.5 * intK5 - K1 * tan_edge - 0.25 * intK1 * sect2_rho) *
+                    y2 * y2;
+      py1 = py2 +
+            (tan_edge * tan_edge * tant_rho / rho - intK5 - 2.0 * K1 * tan_edge - 0.5 * intK1 * sect2_rho) * x2 * y2 +
+            sect2_rho * y2 * px2;
+      dtau += (-0.5 * sect2_rho * (0.25 * (2.0 * tan_edge * K1 + intK5) * y2 * y2 - px2) +
+               (0.5 * tan_edge * tan_edge * tant_rho / rho - 0.25 * intK1 * sect2_rho) * x2) *
+              y2 * y2 / (1.0 + dp0);
+      x2 = x1 / (1.0 - 0.5 * tan_edge * tant_rho * x1);
+      y2 = y1;
+      px2 = px1 * (1.0 - 0.5 * tan_edge * tant_rho * x1) * (1.0 + 0.5 * tan_edge * tant_rho * x1);
+      py2 = py1;
+      dtau += -0.5 * tant_rho * tant_rho * rho * x1 * x1 * px1;
+    }
+    x1 = x2;
+    px1 = px2;
+    y1 = y2;
+    py1 = py2;
+  }
+  /* the reference adds the changes to the initial values */
+  x = x0 + (x1 - x0);
+  px = px0 + (px1 - px0);
+  y = y0 + (y1 - y0);
+  py = py0 + (py1 - py0);
+  return dtau;
+}
+
 __device__ __forceinline__ void bend_edge(int mode, const double *__restrict__ d, int base, int which, double rho_a,
-                                          double nidx, double &x, double &xp, double &y, double &yp, double dp) {
+                                          double nidx, const double *__restrict__ fr, double &x, double &xp,
+                                          double &y, double &yp, double &s, double dp) {
   const double e = __ldg(&d[base + 0]), te = __ldg(&d[base + 1]), psi = __ldg(&d[base + 2]);
   const double lim = __ldg(&d[base + 3]), he = __ldg(&d[base + 4]), secb = __ldg(&d[base + 5]);
   if (mode == EDGE_LIN1) {
@@ -1207,6 +1322,16 @@ __device__ __forceinline__ void bend_edge(int mode, const double *__restrict__ d
     f = 1 / sqrt(sqr(1 + dp) - sqr(px) - sqr(py));
     xp = px * f;
     yp = py * f;
+  } else if (mode == EDGE_CURV1 || mode == EDGE_CURV2) {
+    /* src/csbend.c:1183-1203, :1360-1377: the same coordinates, and s takes
+     * the fringe's path-length change */
+    double f = (1 + dp) / sqrt(1 + sqr(xp) + sqr(yp));
+    double px = xp * f, py = yp * f;
+    const double dtau = fringe_curved(x, px, y, py, dp, rho_a, which, mode == EDGE_CURV2, __ldg(&d[BD_K1F]), fr);
+    f = 1 / sqrt(sqr(1 + dp) - sqr(px) - sqr(py));
+    xp = px * f;
+    yp = py * f;
+    s += -dtau;
   }
 }
 
@@ -1222,6 +1347,7 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
   const int eo1 = __ldg(&op->i[3]);
   const double *Fx_xy = field + __ldg(&op->i[4]);
   const double *Fy_xy = Fx_xy + 121;
+  const double *Fr = Fx_xy + (fmode ? 242 : 0); /* curved-fringe records */
   const int edge1 = __ldg(&op->i[5]), edge2 = __ldg(&op->i[6]);
   const int flags = __ldg(&op->i[7]);
   const double rho0 = __ldg(&d[BD_RHO0]), rho_a = __ldg(&d[BD_RHOA]);
@@ -1251,7 +1377,7 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
   dp0 = p.dp;
   const double nidx = __ldg(&d[BD_N]);
   if (edge1)
-    bend_edge(edge1, d, BD_E1, -1, rho_a, nidx, x, xp, y, yp, dp);
+    bend_edge(edge1, d, BD_E1, -1, rho_a, nidx, Fr, x, xp, y, yp, s, dp);
 
   /* convertToDipoleCanonicalCoordinates */
   double X = x, QX, Y = y, QY, S = 0, D = dp;
@@ -1446,7 +1572,7 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
   yp = QY;
   dp = D;
   if (edge2)
-    bend_edge(edge2, d, BD_E2, 1, rho_a, nidx, x, xp, y, yp, dp);
+    bend_edge(edge2, d, BD_E2, 1, rho_a, nidx, Fr + FR_CURV_LEN, x, xp, y, yp, s, dp);
   if (flags & BF_MISALIGN) {
     p.x = x * ct - y * st + __ldg(&d[BD_ET + 0]);
     p.y = x * st + y * ct + __ldg(&d[BD_ET + 2]);

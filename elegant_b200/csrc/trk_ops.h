@@ -173,6 +173,12 @@ typedef struct {
 #define BD_FC2 119
 #define BD_FF2 120
 #define BD_GAP 121
+/* Lindberg's curved-dipole fringe (EDGE_EFFECTS 5): the body gradient
+ * b[1]/rho0 the edge maps take; the edges' records (FR_CURV_LEN values each:
+ * integrals K0..K6, tan and sec of the edge angle, entrance then exit) sit in
+ * the field pool after the bend's field table (at i[4], + 242 where i[2] != 0) */
+#define BD_K1F 122
+#define FR_CURV_LEN 9
 /* i: 0 nSlices, 1 nSub, 2 field mode (0 dipole, 1 normal, 2 skew), 3 expansionOrder1,
  *    4 field pool offset, 5 edge1 mode, 6 edge2 mode, 7 flags */
 #define EDGE_NONE 0
@@ -182,6 +188,8 @@ typedef struct {
 #define EDGE_HWANG1 4 /* EDGE_EFFECTS=2, EDGE_ORDER<=1 (dipoleFringeKHwang, linear terms) */
 #define EDGE_HWANG2 5 /* EDGE_EFFECTS=2, EDGE_ORDER>=2 */
 #define EDGE_HWANGL 6 /* EDGE_EFFECTS=4 (dipoleFringeKHwangRLindberg) */
+#define EDGE_CURV1 7 /* EDGE_EFFECTS=5, EDGE_ORDER<=1 (curvedDipoleFringe, linear map) */
+#define EDGE_CURV2 8 /* EDGE_EFFECTS=5, EDGE_ORDER>=2 (with the edge's second-order terms) */
 
 /* RF */
 #define RD_OMEGA 0

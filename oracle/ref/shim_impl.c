@@ -34,6 +34,8 @@ double ref_cos(double x) { return ref_cr_math ? trkcr_cos(x) : cos(x); }
 double ref_asin(double x) { return ref_cr_math ? trkcr_asin(x) : asin(x); }
 double ref_tan(double x) { return ref_cr_math ? trkcr_tan(x) : tan(x); }
 double ref_exp(double x) { return ref_cr_math ? trkcr_exp(x) : exp(x); }
+double ref_sinh(double x) { return ref_cr_math ? trkcr_sinh(x) : sinh(x); }
+double ref_cosh(double x) { return ref_cr_math ? trkcr_cosh(x) : cosh(x); }
 
 /* ----------------------------------------------------- SDDS mdbmth helpers */
 double ipow(double x, long p) {

@@ -721,6 +721,8 @@ typedef struct {
   double angle, e1, e2, tilt, etilt, rho0, h, n, fse, rho_actual;
   double psi1, psi2, e1_kick_limit, e2_kick_limit, he1, he2;
   double hgap, fint1, fint2; /* fringe: HGAP and FINT1/FINT2 (FINT where negative) */
+  double fringe_int[2][7];   /* EDGE_EFFECTS=5: FRINGE1K0..6, FRINGE2K0..6 */
+  double k1_fringe;          /* b[1]/rho0, the body gradient the edge maps take */
   double cos_ttilt, sin_ttilt, dcoord_etilt[6];
   double dxi, dyi, dzi, dxf, dyf, dzf;
   int edge1, edge2, edge_order, edge1_effects, edge2_effects;
@@ -823,6 +825,11 @@ static int csbend_setup(const trk_lattice *l, int idx, double Po, orc_csbend_set
   double fse_ = TRK_P(e, CSBEND_FSE), fseD = TRK_P(e, CSBEND_FSE_DIPOLE), fseQ = TRK_P(e, CSBEND_FSE_QUADRUPOLE);
   b[1] *= (1 + fse_ + fseQ) / (1 + fse_ + fseD);
   c[1] *= (1 + fse_ + fseQ) / (1 + fse_ + fseD);
+  S->k1_fringe = b[1] / rho0;
+  for (int k = 0; k < 7; k++) {
+    S->fringe_int[0][k] = e->p[P_CSBEND_FRINGE1K0 + k];
+    S->fringe_int[1][k] = e->p[P_CSBEND_FRINGE2K0 + k];
+  }
   b[2] *= (1 + fse_) / (1 + fse_ + fseD);
   c[2] *= (1 + fse_) / (1 + fse_ + fseD);
   b[0] = TRK_P(e, CSBEND_XKICK) / ANGLE;
@@ -935,7 +942,7 @@ static int csbend_setup(const trk_lattice *l, int idx, double Po, orc_csbend_set
   for (int k = 0; k < 2; k++) {
     int eff = k ? S->edge2_effects : S->edge1_effects;
     int on = k ? S->edge2 : S->edge1;
-    if (on && eff != 0 && eff != 1 && eff != 2 && eff != 3 && eff != 4)
+    if (on && (eff < 0 || eff > 5))
       return 1;
     /* EDGE_ORDER > 1 with Hwang's fringe needs HGAP (src/csbend.c:711-712) */
     if (eff == 2 && S->edge_order > 1 && S->hgap == 0)
@@ -1150,8 +1157,120 @@ static void fringe_hwang_lindberg(double *Qf, const double *Qi, double rho, doub
   Qf[5] = dp0;
 }
 
+/* Lindberg's curved-dipole fringe, EDGE_EFFECTS=5 (curvedDipoleFringe,
+ * src/csbend.c:5693-5969): in dipole canonical coordinates, with the edge's
+ * fringe integrals K0..K6 (FRINGE1K0.. / FRINGE2K0..; no element here is
+ * flipped, so no sign changes).  Entrance (inFringe -1) and exit (+1) share
+ * the linear map through the fringe field; EDGE_ORDER > 1 adds the
+ * second-order terms of the edge, which differ in sign between the two.
+ * Written in the reference's operation order, exp/sinh/cosh/cos/tan through
+ * the arithmetic-mode selectors. */
+static void fringe_curved(double *Qf, const double *Qi, double rho, int inFringe, int edgeOrder, double K1,
+                          double edge, const double *K) {
+  const double x0 = Qi[0], px0 = Qi[1], y0 = Qi[2], py0 = Qi[3], dp0 = Qi[5];
+  const double sec_edge = 1. / orc_cos_sel(edge), tan_edge = orc_tan_sel(edge);
+  const double intK0 = K[0], intK1 = K[1], intK2 = K[2], intK3 = K[3], intK4 = K[4], intK5 = K[5], intK6 = K[6];
+  double x1, px1, y1, py1, dtau;
+  /* the linear map through the fringe field (the same at both ends) */
+  const double mx = (intK3 + intK4) / (1.0 + dp0);
+  const double my = intK3 / (1.0 + dp0);
+  const double delX = intK0 / (1.0 + dp0);
+  const double focX = intK1 + tan_edge / rho;
+  const double focY = intK2 / (1.0 + dp0);
+  if (fabs(mx) < 1.0e-5) {
+    x1 = x0 * orc_exp_sel(-mx) + dp0 * delX * (1.0 - 0.5 * mx * (1.0 - mx / 3.0 + mx * mx / 12.0));
+    px1 = px0 * orc_exp_sel(mx) + focX * (x0 * (1.0 + mx * mx / 6.0) + dp0 * delX * (0.5 + mx * mx / 24.0));
+    dtau = px0 * (mx * x0 + delX) / (1.0 + dp0) + delX * px0 * 0.5 * mx * (1.0 + mx / 3.0 + mx * mx / 12.0) +
+           focX * x0 * x0 * mx * (0.5 - (mx - 0.5 * mx * mx) / 3.0) / (1.0 + dp0) +
+           dp0 * focX * delX * (delX + mx * x0 / (1.0 + dp0)) * (1.0 + 0.05 * mx * mx) / 6.0 +
+           focX * delX * x0 * 0.5 * (1.0 + mx * mx / 12.0) / (1.0 + dp0) +
+           dp0 * focX * delX * (2.0 * mx * x0 - dp0 * delX) * (1.0 - mx * (0.75 - mx * (0.35 - 0.125 * mx))) /
+             (6.0 * (1.0 + dp0));
+  } else {
+    x1 = x0 * orc_exp_sel(-mx) + dp0 * delX * (1.0 - orc_exp_sel(-mx)) / mx;
+    px1 = px0 * orc_exp_sel(mx) +
+          focX * (x0 * orc_sinh_sel(mx) / mx + dp0 * delX * (orc_cosh_sel(mx) - 1.0) / (mx * mx));
+    dtau = px0 * (mx * x0 + delX) / (1.0 + dp0) + delX * px0 * (orc_exp_sel(mx) - 1.0 - mx) / mx +
+           focX * x0 * x0 * 0.25 * ((orc_exp_sel(-2.0 * mx) - 1.0) / mx + 2.0) / (1.0 + dp0) +
+           dp0 * focX * delX * (delX + mx * x0 / (1.0 + dp0)) * (orc_sinh_sel(mx) - mx) / (mx * mx * mx) +
+           focX * delX * x0 * (orc_cosh_sel(mx) - 1.0) / (mx * mx * (1.0 + dp0)) +
+           dp0 * focX * delX * (2.0 * mx * x0 - dp0 * delX) * 0.25 *
+             (2.0 - (3.0 + orc_exp_sel(-2.0 * mx) - 4.0 * orc_exp_sel(-mx)) / mx) / (mx * mx * (1.0 + dp0));
+  }
+  if (fabs(my) < 1.0e-5) {
+    y1 = y0 * orc_exp_sel(my);
+    py1 = py0 * orc_exp_sel(-my) + y0 * (focY - focX) * (1.0 + my * my / 6.0);
+    dtau += (-my * py0 * y0 + 0.5 * (focY + focX * (my + my * my * (2.0 + my) / 3.0) * y0 * y0)) / (1.0 + dp0);
+  } else {
+    y1 = y0 * orc_exp_sel(my);
+    py1 = py0 * orc_exp_sel(-my) + y0 * (focY - focX) * orc_sinh_sel(my) / my;
+    dtau += (-my * py0 * y0 + 0.5 * (focY + 0.5 * focX * ((orc_exp_sel(2.0 * my) - 1.0) / my - 2.0)) * y0 * y0) /
+            (1.0 + dp0);
+  }
+  double xo = x1, pxo = px1, yo = y1, pyo = py1;
+  if (edgeOrder > 1) {
+    /* second-order terms of the edge itself */
+    const double sect2_rho = sec_edge * sec_edge / (rho * (1.0 + dp0));
+    const double tant_rho = tan_edge / (rho * (1.0 + dp0));
+    double x2, y2, px2, py2;
+    if (inFringe == -1) {
+      x2 = x1;
+      y2 = y1 * orc_exp_sel(tan_edge * tant_rho * x1);
+      px2 = px1 - tan_edge * tant_rho * y1 * py1 - (tan_edge * (tan_edge * tant_rho / rho - K1) - 0.5 * intK6) * x1 * x1;
+      py2 = py1 * orc_exp_sel(-tan_edge * tant_rho * x1);
+      dtau += -tan_edge * tant_rho * tant_rho * x1 * x1 * x1 / 3.0 - tant_rho * tant_rho * rho * x1 * y1 * py1;
+      x1 = x2 + 0.5 * sect2_rho * y2 * y2;
+      y1 = y2;
+      px1 = px2 + (0.5 * tant_rho / rho - 0.5 * intK5 - K1 * tan_edge + 0.25 * intK1 * sect2_rho) * y2 * y2;
+      py1 = py2 + (tant_rho / rho - intK5 - 2.0 * K1 * tan_edge + 0.5 * intK1 * sect2_rho) * x2 * y2 -
+            sect2_rho * y2 * px2;
+      dtau += (0.5 * sect2_rho * (0.25 * (2.0 * tan_edge * K1 + intK5) * y2 * y2 - px2) +
+               (0.5 * tant_rho / rho + 0.25 * intK1 * sect2_rho) * x2) *
+              y2 * y2 / (1.0 + dp0);
+      x2 = x1 / (1.0 + 0.5 * tan_edge * tant_rho * x1);
+      y2 = y1;
+      px2 = px1 * (1.0 + 0.5 * tan_edge * tant_rho * x1) * (1.0 + 0.5 * tan_edge * tant_rho * x1);
+      py2 = py1;
+      dtau += 0.5 * tant_rho * tant_rho * rho * x1 * x1 * px1;
+    } else {
+      x2 = x1;
+      y2 = y1 * orc_exp_sel(-tan_edge * tant_rho * x1);
+      px2 = px1 + tan_edge * tant_rho * y1 * py1 +
+            (tan_edge * (0.5 * tan_edge * tant_rho / rho + K1) + 0.5 * intK6) * x1 * x1;
+      py2 = py1 * orc_exp_sel(tan_edge * tant_rho * x1);
+      dtau += tan_edge * tant_rho * tant_rho * x1 * x1 * x1 / 6.0 + tant_rho * tant_rho * rho * x1 * y1 * py1;
+      x1 = x2 - 0.5 * sect2_rho * y2 * y2;
+      y1 = y2;
+      px1 = px2 + (0.5 * tan_edge * tan_edge * tant_rho / rho - 0.5 * intK5 - K1 * tan_edge - 0.25 * intK1 * sect2_rho) *
+                    y2 * y2;
+      py1 = py2 +
+            (tan_edge * tan_edge * tant_rho / rho - intK5 - 2.0 * K1 * tan_edge - 0.5 * intK1 * sect2_rho) * x2 * y2 +
+            sect2_rho * y2 * px2;
+      dtau += (-0.5 * sect2_rho * (0.25 * (2.0 * tan_edge * K1 + intK5) * y2 * y2 - px2) +
+               (0.5 * tan_edge * tan_edge * tant_rho / rho - 0.25 * intK1 * sect2_rho) * x2) *
+              y2 * y2 / (1.0 + dp0);
+      x2 = x1 / (1.0 - 0.5 * tan_edge * tant_rho * x1);
+      y2 = y1;
+      px2 = px1 * (1.0 - 0.5 * tan_edge * tant_rho * x1) * (1.0 + 0.5 * tan_edge * tant_rho * x1);
+      py2 = py1;
+      dtau += -0.5 * tant_rho * tant_rho * rho * x1 * x1 * px1;
+    }
+    xo = x2;
+    pxo = px2;
+    yo = y2;
+    pyo = py2;
+  }
+  /* the reference adds the differences to the initial values */
+  Qf[0] = x0 + (xo - x0);
+  Qf[1] = px0 + (pxo - px0);
+  Qf[2] = y0 + (yo - y0);
+  Qf[3] = py0 + (pyo - py0);
+  Qf[4] = -dtau;
+  Qf[5] = Qi[5];
+}
+
 static void csbend_edge(const orc_csbend_setup *S, int which, double *x, double *xp, double *y, double *yp,
-                        double dp) {
+                        double *s, double dp) {
   int eff = which < 0 ? S->edge1_effects : S->edge2_effects;
   double e = which < 0 ? S->e1 : S->e2;
   double psi = which < 0 ? S->psi1 : S->psi2;
@@ -1169,9 +1288,9 @@ static void csbend_edge(const orc_csbend_setup *S, int which, double *x, double 
     apply_edge_effects(x, xp, y, yp, rho, S->n, e, he, psi * (1 + dp), which);
   } else if (eff == 3) {
     simple_dipole_edge_kick(xp, yp, *x, *y, dp, S->rho_actual, e, psi, lim);
-  } else if (eff == 2 || eff == 4) {
-    /* in dipole canonical coordinates (src/csbend.c:1139-1182, :1319-1359) */
-    double Qi[6], Qf[6];
+  } else if (eff == 2 || eff == 4 || eff == 5) {
+    /* in dipole canonical coordinates (src/csbend.c:1139-1200, :1319-1377) */
+    double Qi[6], Qf[6] = {0, 0, 0, 0, 0, 0};
     Qi[0] = *x;
     Qi[1] = *xp;
     Qi[2] = *y;
@@ -1184,8 +1303,10 @@ static void csbend_edge(const orc_csbend_setup *S, int which, double *x, double 
     const double fint = which < 0 ? S->fint1 : S->fint2;
     if (eff == 2)
       fringe_hwang(Qf, Qi, S->rho_actual, (double)which, S->edge_order, e, 2 * S->hgap, fint, he);
-    else
+    else if (eff == 4)
       fringe_hwang_lindberg(Qf, Qi, S->rho_actual, (double)which, e, 2 * S->hgap, fint, he);
+    else
+      fringe_curved(Qf, Qi, S->rho_actual, which, S->edge_order, S->k1_fringe, e, S->fringe_int[which < 0 ? 0 : 1]);
     f = 1 / sqrt(orc_sqr(1 + Qf[5]) - orc_sqr(Qf[1]) - orc_sqr(Qf[3]));
     Qf[1] *= f;
     Qf[3] *= f;
@@ -1193,6 +1314,8 @@ static void csbend_edge(const orc_csbend_setup *S, int which, double *x, double 
     *xp = Qf[1];
     *y = Qf[2];
     *yp = Qf[3];
+    if (eff == 5)
+      *s += Qf[4];
   }
 }
 
@@ -1225,7 +1348,7 @@ static long track_through_csbend(double *coord, long n_part, const trk_lattice *
     s = c[4];
     dp = dp0 = c[5];
     if (S.edge1)
-      csbend_edge(&S, -1, &x, &xp, &y, &yp, dp);
+      csbend_edge(&S, -1, &x, &xp, &y, &yp, &s, dp);
     Qi[0] = x;
     Qi[1] = xp;
     Qi[2] = y;
@@ -1265,7 +1388,7 @@ static long track_through_csbend(double *coord, long n_part, const trk_lattice *
     yp = Qf[3];
     dp = Qf[5];
     if (S.edge2)
-      csbend_edge(&S, 1, &x, &xp, &y, &yp, dp);
+      csbend_edge(&S, 1, &x, &xp, &y, &yp, &s, dp);
     c[0] = x * S.cos_ttilt - y * S.sin_ttilt + S.dcoord_etilt[0];
     c[2] = x * S.sin_ttilt + y * S.cos_ttilt + S.dcoord_etilt[2];
     c[1] = xp * S.cos_ttilt - yp * S.sin_ttilt + S.dcoord_etilt[1];
@@ -1316,6 +1439,8 @@ double orc_cr_cos(double x) { return trkcr_cos(x); }
 double orc_cr_asin(double x) { return trkcr_asin(x); }
 double orc_cr_tan(double x) { return trkcr_tan(x); }
 double orc_cr_exp(double x) { return trkcr_exp(x); }
+double orc_cr_sinh(double x) { return trkcr_sinh(x); }
+double orc_cr_cosh(double x) { return trkcr_cosh(x); }
 /* the double-double evaluations behind the fast paths, and the fast paths'
  * parts (hi, L, error bound e; returns the rounding test's verdict), for the
  * tests of the fast paths' error bounds */

@@ -39,6 +39,8 @@ static inline double orc_cos_sel(double x) { return orc_cr_math ? trkcr_cos(x) :
 static inline double orc_asin_sel(double x) { return orc_cr_math ? trkcr_asin(x) : asin(x); }
 static inline double orc_tan_sel(double x) { return orc_cr_math ? trkcr_tan(x) : tan(x); }
 static inline double orc_exp_sel(double x) { return orc_cr_math ? trkcr_exp(x) : exp(x); }
+static inline double orc_sinh_sel(double x) { return orc_cr_math ? trkcr_sinh(x) : sinh(x); }
+static inline double orc_cosh_sel(double x) { return orc_cr_math ? trkcr_cosh(x) : cosh(x); }
 
 #ifndef ORC_R
 #define ORC_R double

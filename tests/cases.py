@@ -15,6 +15,44 @@ QUAD_FRINGE_INTEGRALS = dict(I0P=0.01, I1P=2e-5, I2P=1e-7, I3P=5e-10, LAMBDA2P=3
                              I2M=8e-8, I3M=-4e-10, LAMBDA2M=2e-7)
 
 
+# Lindberg's edge integrals K0..K6 for both ends of a bend (EDGE_EFFECTS=5)
+CURVED_FRINGE = dict(FRINGE1K0=2e-3, FRINGE1K1=0.01, FRINGE1K2=0.02, FRINGE1K3=3e-3, FRINGE1K4=-1e-3,
+                     FRINGE1K5=0.05, FRINGE1K6=0.1, FRINGE2K0=1.5e-3, FRINGE2K1=-0.02, FRINGE2K2=0.015,
+                     FRINGE2K3=2e-3, FRINGE2K4=5e-4, FRINGE2K5=-0.04, FRINGE2K6=0.3)
+
+def fringe_ring(cells=2):
+    """A small FODO ring whose bends mix every dipole-edge model (curved-dipole
+    fringe of both orders with and without a field table, Hwang-Lindberg,
+    symplectic kick, plain linear edge) among fringed quadrupoles and weak
+    sextupoles, so that several fringe records share the field pool."""
+    lat = Lattice()
+    a = 2 * math.pi / 80
+    for c in range(cells):
+        lat.add("KQUAD", f"QF{c}", L=0.3, K1=1.2, N_KICKS=8, EDGE1_EFFECTS=2, EDGE2_EFFECTS=2,
+                **QUAD_FRINGE_INTEGRALS)
+        lat.add("DRIF", f"D1{c}", L=1.0)
+        lat.add("CSBEND", f"BA{c}", L=1.0, ANGLE=a, E1=a / 2, E2=a / 2, K1=-0.05, EDGE1_EFFECTS=5,
+                EDGE2_EFFECTS=5, EDGE_ORDER=2, N_SLICES=8, **CURVED_FRINGE)
+        lat.add("DRIF", f"D2{c}", L=1.0)
+        lat.add("KQUAD", f"QD{c}", L=0.3, K1=-1.2, N_KICKS=8)
+        lat.add("KSEXT", f"SD{c}", L=0.2, K2=-4.0, N_KICKS=4)
+        lat.add("DRIF", f"D3{c}", L=1.0)
+        lat.add("CSBEND", f"BB{c}", L=1.0, ANGLE=a, E1=a / 2, E2=0.0, EDGE1_EFFECTS=5, EDGE2_EFFECTS=3,
+                N_SLICES=8, **CURVED_FRINGE)
+        lat.add("DRIF", f"D4{c}", L=1.0)
+        lat.add("KQUAD", f"QF2{c}", L=0.3, K1=1.2, N_KICKS=8)
+        lat.add("KSEXT", f"SF{c}", L=0.2, K2=4.0, N_KICKS=4)
+        lat.add("DRIF", f"D5{c}", L=1.0)
+        lat.add("CSBEND", f"BC{c}", L=1.0, ANGLE=a, E1=0.03, E2=0.05, HGAP=0.02, FINT=0.5, K2=3.0,
+                EDGE1_EFFECTS=4, EDGE2_EFFECTS=5, N_SLICES=8, **CURVED_FRINGE)
+        lat.add("DRIF", f"D6{c}", L=1.0)
+        lat.add("KQUAD", f"QD2{c}", L=0.3, K1=-1.2, N_KICKS=8)
+        lat.add("DRIF", f"D7{c}", L=1.0)
+        lat.add("CSBEND", f"BD{c}", L=1.0, ANGLE=a, E1=0.02, E2=0.02, N_SLICES=8)
+        lat.add("DRIF", f"D8{c}", L=1.0)
+    return lat
+
+
 def _lossy_fringe_quad():
     lat = Lattice()
     lat.add("MAXAMP", "AP", X_MAX=0.0012, Y_MAX=0.001, ELLIPTICAL=1)
@@ -62,6 +100,17 @@ ELEMENT_CASES = {
                                     H2=-0.2, EDGE1_EFFECTS=4, EDGE2_EFFECTS=4, N_SLICES=8),
     "csbend_hwang_negative": single("CSBEND", L=1.0, ANGLE=-0.06, E1=0.02, E2=0.05, HGAP=0.02, FINT=0.6,
                                     EDGE1_EFFECTS=4, EDGE2_EFFECTS=2, N_SLICES=8),
+    "csbend_curved": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=0.03, K1=0.2, EDGE1_EFFECTS=5,
+                            EDGE2_EFFECTS=5, N_SLICES=8, **CURVED_FRINGE),
+    "csbend_curved_order2": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=-0.03, K1=-0.3, EDGE1_EFFECTS=5,
+                                   EDGE2_EFFECTS=5, EDGE_ORDER=2, N_SLICES=8, **CURVED_FRINGE),
+    "csbend_curved_small_m": single("CSBEND", L=1.0, ANGLE=-0.06, E1=0.02, E2=0.05, K1=0.1, EDGE1_EFFECTS=5,
+                                    EDGE2_EFFECTS=5, EDGE_ORDER=2, N_SLICES=8, FRINGE1K0=1.5e-3, FRINGE1K1=0.02,
+                                    FRINGE1K2=0.03, FRINGE1K3=4e-6, FRINGE1K4=2e-6, FRINGE1K5=0.04, FRINGE1K6=-0.1,
+                                    FRINGE2K0=-1e-3, FRINGE2K1=0.01, FRINGE2K2=0.02, FRINGE2K3=-3e-6,
+                                    FRINGE2K4=1e-6, FRINGE2K5=0.06, FRINGE2K6=0.2),
+    "csbend_curved_mixed": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=0.03, HGAP=0.02, FINT=0.5,
+                                  EDGE1_EFFECTS=5, EDGE2_EFFECTS=2, N_SLICES=8, **CURVED_FRINGE),
     "csbend_xreference": single("CSBEND", L=1.0, ANGLE=0.06, XREFERENCE=0.02, F1=1e-3, F2=-2e-3, F3=5e-4, G1=4e-4,
                                 G2=-1e-4, N_SLICES=8, EPITCH=1e-3, EYAW=-2e-3, XSTEERING=1, SQRT_ORDER=2,
                                 FRINGE1K0=0.1, TRACKING_MATRIX=2),

@@ -1,5 +1,6 @@
 """Ring cases of the golden fixtures (shared by make_golden.py and the test)."""
 from elegant_b200 import Lattice, configs
+from tests.cases import fringe_ring
 
 
 def ring_cases():
@@ -16,4 +17,5 @@ def ring_cases():
         "ring_rf_wake": (configs.c2_lattice(cells=2, n_bins=300), configs.gaussian_beam(200, seed=63), 2),
         "ring_lossy": (lossy, configs.gaussian_beam(100, seed=64, sigma_x=2e-3, sigma_xp=2e-4), 3),
         "ring_trwake": (trw, configs.gaussian_beam(100, seed=65), 2),
+        "ring_fringes": (fringe_ring(), configs.gaussian_beam(100, seed=66), 3),
     }

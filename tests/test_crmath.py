@@ -125,6 +125,24 @@ def test_exp_correctly_rounded():
     assert not bad, bad[:3]
 
 
+@pytest.mark.parametrize("kind", ["sinh", "cosh"])
+def test_sinh_cosh_correctly_rounded(kind):
+    """trkcr_sinh / trkcr_cosh (the curved-dipole fringe's, EDGE_EFFECTS=5)
+    against 120-digit values, on the Taylor path (|x| < 1/8), across the
+    switch and on the exponential path up to |x| = 30."""
+    lib = pyoracle.load()
+    f = getattr(lib, "orc_cr_" + kind)
+    f.argtypes = [ctypes_double()]
+    f.restype = ctypes_double()
+    rng = np.random.Generator(np.random.Philox(9))
+    xs = np.concatenate([rng.uniform(-0.125, 0.125, 200), rng.uniform(0.1, 0.2, 60),
+                         np.ldexp(rng.uniform(1, 2, 40), rng.integers(-40, -3, 40)), rng.uniform(-30, 30, 100)])
+    sign = 1 if kind == "cosh" else -1
+    bad = [x for x in xs if f(float(x)) != float((dexp(float(x)) + sign * dexp(-float(x))) / 2)]
+    assert not bad, bad[:3]
+    assert f(0.0) == (1.0 if kind == "cosh" else 0.0)
+
+
 def ctypes_double():
     import ctypes
     return ctypes.c_double

@@ -14,7 +14,7 @@ import pytest
 
 from elegant_b200 import Lattice, configs
 from oracle import pyoracle
-from tests.cases import ELEMENT_CASES
+from tests.cases import ELEMENT_CASES, fringe_ring
 
 PC = configs.P_CENTRAL
 
@@ -48,6 +48,7 @@ def test_rings_loop_is_do_tracking(mode):
     assert_same_loop(configs.c2_lattice(cells=2, n_bins=300), configs.gaussian_beam(1500, seed=23), 3, mode)
     assert_same_loop(configs.c2_lattice(cells=2, n_bins=300), configs.gaussian_beam(500, seed=27), 2, mode,
                      pass_offset=5)
+    assert_same_loop(fringe_ring(), configs.gaussian_beam(400, seed=28), 3, mode)
 
 
 @pytest.mark.parametrize("mode", sorted(MODES))

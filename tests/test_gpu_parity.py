@@ -16,11 +16,12 @@ import pytest
 
 from elegant_b200 import Lattice, configs
 from oracle import pyoracle
-from tests.cases import ELEMENT_CASES, single  # noqa: F401
+from tests.cases import ELEMENT_CASES, fringe_ring, single  # noqa: F401
 from tests.helpers import compare, gpu_run, oracle_run
 
 pytestmark = pytest.mark.gpu
 PC = configs.P_CENTRAL
+GLIBC_SINH_CASES = {"csbend_curved", "csbend_curved_order2", "csbend_curved_mixed"}
 
 
 @pytest.mark.parametrize("name", sorted(ELEMENT_CASES))
@@ -49,8 +50,11 @@ def test_element_parity_glibc(tracker, name):
     r = compare(g, rows, nl, nlo)
     assert r["same_survivors"]
     # glibc misrounds sin/cos/asin on a few calls per million; the CSBEND
-    # drift amplifies a one-ulp cos difference by ~rho0/x
-    assert r["n_diff"] <= max(2, 0.05 * r["n_alive"]), r
+    # drift amplifies a one-ulp cos difference by ~rho0/x.  glibc's sinh and
+    # cosh (per particle in the curved-dipole fringe) are off by an ulp on a
+    # large share of arguments, so those cases differ on more rows.
+    share = 0.25 if name in GLIBC_SINH_CASES else 0.05
+    assert r["n_diff"] <= max(2, share * r["n_alive"]), r
     assert r["max_err"] < 1e-10, r
 
 
@@ -75,6 +79,29 @@ def test_fodo_ring_exact(tracker):
     r = compare(g, rows, nl, nlo)
     assert r["same_survivors"] and r["bit_exact"], r
     assert st["particle_passes"] == eff
+
+
+def test_fringe_ring_exact(tracker):
+    """Bends with every edge model in one ring: the curved-dipole fringe's
+    records found in the field pool after each bend's field table."""
+    lat = fringe_ring(cells=3)
+    beam = configs.gaussian_beam(3000, seed=14)
+    nl, g, lp, le, st = gpu_run(tracker, lat, beam, 4, PC, fast=False)
+    with pyoracle.modes(exact_sums=True, cr_math=True):
+        rows, nlo, eff = oracle_run(lat, beam, 4, PC)
+    r = compare(g, rows, nl, nlo)
+    assert r["same_survivors"] and r["bit_exact"], r
+    assert st["particle_passes"] == eff
+
+
+def test_fringe_ring_fast(tracker):
+    lat = fringe_ring(cells=3)
+    beam = configs.gaussian_beam(3000, seed=14)
+    nl, g, lp, le, _ = gpu_run(tracker, lat, beam, 2, PC, fast=True)
+    with pyoracle.modes(exact_sums=True, cr_math=True):
+        rows, nlo, _ = oracle_run(lat, beam, 2, PC)
+    r = compare(g, rows, nl, nlo)
+    assert r["same_survivors"] and r["max_err"] < 2e-8, r
 
 
 def test_fodo_ring_fast_one_turn(tracker):

@@ -15,7 +15,7 @@ import pytest
 
 from elegant_b200 import TYPE_CODE, Lattice, configs
 from oracle import pyoracle
-from tests.cases import ELEMENT_CASES
+from tests.cases import ELEMENT_CASES, fringe_ring
 
 PC = configs.P_CENTRAL
 
@@ -53,6 +53,12 @@ def test_element_matches_reference(name, mode):
 def test_fodo_ring_matches_reference(mode):
     beam = configs.gaussian_beam(300, seed=22)
     assert_same(*both(configs.c1_lattice(cells=4), beam, 3, mode))
+
+
+@pytest.mark.parametrize("mode", sorted(MODES))
+def test_fringe_ring_matches_reference(mode):
+    beam = configs.gaussian_beam(600, seed=29)
+    assert_same(*both(fringe_ring(cells=3), beam, 4, mode))
 
 
 @pytest.mark.parametrize("mode", sorted(MODES))
