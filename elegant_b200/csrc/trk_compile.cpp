@@ -518,9 +518,9 @@ int edge_mode(int on, int effects, int edge_order, const char *name) {
 int compile_bend(const trk_lattice *l, int idx, double Po, trk_op *op, std::vector<double> &field) {
   const trk_elem *e = &l->e[idx];
   if (TRK_P(e, CSBEND_REFERENCE_CORRECTION) || TRK_P(e, CSBEND_FSE_CORRECTION) || TRK_P(e, CSBEND_MALIGN_METHOD) ||
-      TRK_P(e, CSBEND_EXPAND_HAMILTONIAN) || TRK_P(e, CSBEND_USE_RAD_DIST))
+      TRK_P(e, CSBEND_USE_RAD_DIST))
     return trk_set_error(TRK_ERR_UNSUPPORTED,
-                         "CSBEND %s: REFERENCE_CORRECTION, FSE_CORRECTION, MALIGN_METHOD!=0, EXPAND_HAMILTONIAN and "
+                         "CSBEND %s: REFERENCE_CORRECTION, FSE_CORRECTION, MALIGN_METHOD!=0 and "
                          "USE_RAD_DIST (photon-based radiation) are not on this path",
                          e->name);
   const double L = TRK_P(e, CSBEND_L), ANGLE = TRK_P(e, CSBEND_ANGLE);
@@ -694,6 +694,8 @@ int compile_bend(const trk_lattice *l, int idx, double Po, trk_op *op, std::vect
     flags |= BF_ISR_ROUNDTRIP; /* isrConstant < 0 but nonzero (src/csbend.c:931-934) */
   if (dx || dy || dz || ttilt || etilt)
     flags |= BF_MISALIGN;
+  if (TRK_P(e, CSBEND_EXPAND_HAMILTONIAN))
+    flags |= BF_EXPAND; /* integrate_csbend_ordn_expanded (src/csbend.c:1227-1229) */
   /* classical radiation (src/csbend.c:953-959) */
   if (TRK_P(e, CSBEND_SYNCH_RAD)) {
     const double rad_coef = (TRK_E_MKS * TRK_E_MKS) * (Po * Po * Po) * ((1 + fse) * (1 + fse)) /
@@ -701,6 +703,11 @@ int compile_bend(const trk_lattice *l, int idx, double Po, trk_op *op, std::vect
     if (rad_coef) {
       flags |= BF_RAD;
       d[BD_RAD] = rad_coef;
+      /* delta adjusted at edges with nonzero angles (src/csbend.c:1215-1222, :1270-1281) */
+      if (ed1 && e1 != 0)
+        flags |= BF_RADE1;
+      if (ed2 && e2 != 0)
+        flags |= BF_RADE2;
     }
   }
   /* incoherent radiation: isrConstant (src/csbend.c:961-964) */
@@ -723,17 +730,17 @@ int compile_bend(const trk_lattice *l, int idx, double Po, trk_op *op, std::vect
   }
   op->i[7] = flags;
   d[BD_E1] = e1;
-  d[BD_TE1] = std::tan(e1);
+  d[BD_TE1] = trkcr_tan(e1); /* tan and sec of the edge angles rounded once */
   d[BD_PSI1] = psi1;
   d[BD_LIM1] = lim1;
   d[BD_HE1] = he1;
-  d[BD_SE1] = 1. / std::cos(e1);
+  d[BD_SE1] = 1. / trkcr_cos(e1);
   d[BD_E2] = e2;
-  d[BD_TE2] = std::tan(e2);
+  d[BD_TE2] = trkcr_tan(e2);
   d[BD_PSI2] = psi2;
   d[BD_LIM2] = lim2;
   d[BD_HE2] = he2;
-  d[BD_SE2] = 1. / std::cos(e2);
+  d[BD_SE2] = 1. / trkcr_cos(e2);
   /* Hwang fringes: the values dipoleFringeKHwang / ...RLindberg form per call
    * (src/csbend.c:4360-4363, :4443-4446); FINT1/FINT2 where >= 0, else FINT
    * (src/csbend.c:1150, :1329) */
@@ -1014,7 +1021,8 @@ int trk_compile(const trk_lattice *l, double Po, CompiledLattice &out) {
                            (op.i[5] == EDGE_LIN1 && op.d[BD_TE1] == 0 && op.d[BD_PSI1] == 0 && op.d[BD_LIM1] <= 0);
       const bool e2_noop = op.i[6] == EDGE_NONE ||
                            (op.i[6] == EDGE_LIN1 && op.d[BD_TE2] == 0 && op.d[BD_PSI2] == 0 && op.d[BD_LIM2] <= 0);
-      const bool plain = op.i[1] == 4 && !(op.i[7] & (BF_MISALIGN | BF_APTILT | BF_RAD)) && e1_noop && e2_noop;
+      const bool plain =
+        op.i[1] == 4 && !(op.i[7] & (BF_MISALIGN | BF_APTILT | BF_RAD | BF_EXPAND)) && e1_noop && e2_noop;
       if (plain && op.i[2] == 0)
         op.kind = OPK_DIPOLE;
       else if (plain && op.i[2] == 1 && op.i[3] == 5) {

@@ -1276,8 +1276,8 @@ __device__ __noinline__ double fringe_curved(double &x, double &px, double &y, d
 }
 
 __device__ __forceinline__ void bend_edge(int mode, const double *__restrict__ d, int base, int which, double rho_a,
-                                          double nidx, const double *__restrict__ fr, double &x, double &xp,
-                                          double &y, double &yp, double &s, double dp) {
+                                          double nidx, const double *__restrict__ fr, bool expanded, double &x,
+                                          double &xp, double &y, double &yp, double &s, double dp) {
   const double e = __ldg(&d[base + 0]), te = __ldg(&d[base + 1]), psi = __ldg(&d[base + 2]);
   const double lim = __ldg(&d[base + 3]), he = __ldg(&d[base + 4]), secb = __ldg(&d[base + 5]);
   if (mode == EDGE_LIN1) {
@@ -1294,7 +1294,7 @@ __device__ __forceinline__ void bend_edge(int mode, const double *__restrict__ d
   } else if (mode == EDGE_SYMP) {
     /* applySimpleDipoleEdgeKick (src/csbend.c:5664-5690) */
     double Q1 = xp, Q3 = yp;
-    double f = (1 + dp) / sqrt(1 + sqr(Q1) + sqr(Q3));
+    double f = expanded ? (1 + dp) : (1 + dp) / sqrt(1 + sqr(Q1) + sqr(Q3));
     Q1 *= f;
     Q3 *= f;
     double dqx = te / rho_a * x;
@@ -1304,13 +1304,13 @@ __device__ __forceinline__ void bend_edge(int mode, const double *__restrict__ d
     double dqy = -t2 / rho_a * y;
     Q1 += dqx;
     Q3 += dqy;
-    f = 1 / sqrt(sqr(1 + dp) - sqr(Q1) - sqr(Q3));
+    f = expanded ? 1 / (1 + dp) : 1 / sqrt(sqr(1 + dp) - sqr(Q1) - sqr(Q3));
     xp = Q1 * f;
     yp = Q3 * f;
   } else if (mode == EDGE_HWANG1 || mode == EDGE_HWANG2 || mode == EDGE_HWANGL) {
     /* in dipole canonical coordinates (src/csbend.c:1139-1182, :1319-1359;
      * convert{To,From}DipoleCanonicalCoordinates, :1436-1457) */
-    double f = (1 + dp) / sqrt(1 + sqr(xp) + sqr(yp));
+    double f = expanded ? (1 + dp) : (1 + dp) / sqrt(1 + sqr(xp) + sqr(yp));
     double px = xp * f, py = yp * f;
     const int k = which < 0 ? 0 : 1;
     const double sn = __ldg(&d[BD_FS1 + 3 * k]), cs = __ldg(&d[BD_FC1 + 3 * k]), fint = __ldg(&d[BD_FF1 + 3 * k]);
@@ -1319,16 +1319,16 @@ __device__ __forceinline__ void bend_edge(int mode, const double *__restrict__ d
       fringe_hwang_lindberg(x, px, y, py, dp, rho_a, (double)which, secb, te, sn, cs, gap, fint, he);
     else
       fringe_hwang(x, px, y, py, dp, rho_a, (double)which, mode == EDGE_HWANG2, secb, te, sn, cs, gap, fint, he);
-    f = 1 / sqrt(sqr(1 + dp) - sqr(px) - sqr(py));
+    f = expanded ? 1 / (1 + dp) : 1 / sqrt(sqr(1 + dp) - sqr(px) - sqr(py));
     xp = px * f;
     yp = py * f;
   } else if (mode == EDGE_CURV1 || mode == EDGE_CURV2) {
     /* src/csbend.c:1183-1203, :1360-1377: the same coordinates, and s takes
      * the fringe's path-length change */
-    double f = (1 + dp) / sqrt(1 + sqr(xp) + sqr(yp));
+    double f = expanded ? (1 + dp) : (1 + dp) / sqrt(1 + sqr(xp) + sqr(yp));
     double px = xp * f, py = yp * f;
     const double dtau = fringe_curved(x, px, y, py, dp, rho_a, which, mode == EDGE_CURV2, __ldg(&d[BD_K1F]), fr);
-    f = 1 / sqrt(sqr(1 + dp) - sqr(px) - sqr(py));
+    f = expanded ? 1 / (1 + dp) : 1 / sqrt(sqr(1 + dp) - sqr(px) - sqr(py));
     xp = px * f;
     yp = py * f;
     s += -dtau;
@@ -1350,6 +1350,7 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
   const double *Fr = Fx_xy + (fmode ? 242 : 0); /* curved-fringe records */
   const int edge1 = __ldg(&op->i[5]), edge2 = __ldg(&op->i[6]);
   const int flags = __ldg(&op->i[7]);
+  const bool expanded = (flags & BF_EXPAND) != 0;
   const double rho0 = __ldg(&d[BD_RHO0]), rho_a = __ldg(&d[BD_RHOA]);
   const double ct = __ldg(&d[BD_CT]), st = __ldg(&d[BD_ST]);
   const bool aptilt = (flags & BF_APTILT) != 0;
@@ -1377,12 +1378,24 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
   dp0 = p.dp;
   const double nidx = __ldg(&d[BD_N]);
   if (edge1)
-    bend_edge(edge1, d, BD_E1, -1, rho_a, nidx, Fr, x, xp, y, yp, s, dp);
+    bend_edge(edge1, d, BD_E1, -1, rho_a, nidx, Fr, expanded, x, xp, y, yp, s, dp);
 
-  /* convertToDipoleCanonicalCoordinates */
   double X = x, QX, Y = y, QY, S = 0, D = dp;
+  if (flags & BF_RADE1) {
+    /* radiation: delta pre-adjusted for the sector integration (src/csbend.c:1215-1222) */
+    double Fx, Fy;
+    if (fmode == 0) {
+      Fx = 0;
+      Fy = 1;
+    } else
+      bend_fields(fmode, eo1, Fx_xy, Fy_xy, x, y, Fx, Fy);
+    const double dp_prime =
+      -__ldg(&d[BD_RAD]) * (sqr(Fx) + sqr(Fy)) * sqr(1 + dp) * sqrt(sqr(1 + x / rho0) + sqr(xp) + sqr(yp));
+    D -= dp_prime * x * __ldg(&d[BD_TE1]);
+  }
+  /* convertToDipoleCanonicalCoordinates */
   {
-    double f = (1 + D) / sqrt(1 + sqr(xp) + sqr(yp));
+    double f = expanded ? (1 + D) : (1 + D) / sqrt(1 + sqr(xp) + sqr(yp));
     QX = xp * f;
     QY = yp * f;
   }
@@ -1390,7 +1403,67 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
   bool ok = true;
   double dist = 0, dz_lost = 0;
   const double sl = __ldg(&d[BD_SLICE]);
-  if (fmode == 0 && !(flags & BF_RAD)) { /* the radiating dipole takes the general body */
+  if (expanded) {
+    /* integrate_csbend_ordn_expanded (src/csbend.c:1722-1900): leading-order
+     * drift, aperture after every drift substep as well as per slice */
+    for (int i = 0; i < nSlices && ok; i++) {
+      if (!check_aperture(X, Y, ap, aptilt, apc, aps)) {
+        ok = false;
+        break;
+      }
+      for (int j = 0; j < nSub; j++) {
+        const double dsh = __ldg(&d[BD_DSH + j]);
+        QX += dsh * (1 + D) / (2 * rho0);
+        dist += dsh * (1 + (sqr(QX) + sqr(QY)) / 2);
+        dz_lost += dsh;
+        X += QX * dsh / (1 + D);
+        Y += QY * dsh / (1 + D);
+        QX += dsh * (1 + D) / (2 * rho0);
+        if (!check_aperture(X, Y, ap, aptilt, apc, aps)) {
+          ok = false;
+          break;
+        }
+        if (j == nSub - 1)
+          break;
+        const double ds = __ldg(&d[BD_DS + j]);
+        double Fx, Fy;
+        if (fmode == 0) {
+          Fx = 0;
+          Fy = 1;
+        } else
+          bend_fields(fmode, eo1, Fx_xy, Fy_xy, X, Y, Fx, Fy);
+        QX += -ds * (1 + X / rho0) * Fy / rho_a;
+        QY += ds * (1 + X / rho0) * Fx / rho_a;
+        if (flags & BF_RAD) {
+          /* src/csbend.c:1833-1863 (dsISR = s/3 in this integrator) */
+          const double hX = 1 + X * __ldg(&d[BD_RHOINV]);
+          const double f = hX / sqrt(sqr(1 + D) - sqr(QX) - sqr(QY));
+          const double xpr = QX * f, ypr = QY * f;
+          const double dsFactor = sqrt(sqr(hX) + sqr(xpr) + sqr(ypr));
+          const double F2 = sqr(Fx) + sqr(Fy);
+          const double deltaFactor = sqr(1 + D);
+          const double dsISR = sl / 3;
+          QX /= (1 + D);
+          QY /= (1 + D);
+          const double rad_coef = __ldg(&d[BD_RAD]);
+          if (rad_coef != 0)
+            D -= rad_coef * deltaFactor * F2 * ds * dsFactor;
+          if ((flags & BF_ISR) && isr && !(isr->single && (flags & BF_ISR1OFF))) {
+            const double g =
+              trk_isr_gauss(isr->seed, isr->id, isr->pass, isr->elem, (unsigned)(i * 8 + j), isr->limit);
+            D -= __ldg(&d[BD_ISR]) * deltaFactor * pow(F2, 0.75) * sqrt(dsISR * dsFactor) * g;
+          }
+          QX *= (1 + D);
+          QY *= (1 + D);
+        } else if (flags & BF_ISR_ROUNDTRIP) {
+          QX /= (1 + D);
+          QY /= (1 + D);
+          QX *= (1 + D);
+          QY *= (1 + D);
+        }
+      }
+    }
+  } else if (fmode == 0 && !(flags & BF_RAD)) { /* the radiating dipole takes the general body */
     int done = 0;
 #if TRK_FAST
     if (nSub == 4)
@@ -1536,7 +1609,7 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
   }
   /* convertFromDipoleCanonicalCoordinates */
   {
-    double f = 1 / sqrt(sqr(1 + D) - sqr(QX) - sqr(QY));
+    double f = expanded ? 1 / (1 + D) : 1 / sqrt(sqr(1 + D) - sqr(QX) - sqr(QY));
     QX *= f;
     QY *= f;
   }
@@ -1549,6 +1622,18 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
     p.s = z_start + dz_lost;
     p.dp = Po * (1 + D);
     return false;
+  }
+  if (flags & BF_RADE2) {
+    /* radiation: delta post-adjusted (src/csbend.c:1270-1281) */
+    double Fx, Fy;
+    if (fmode == 0) {
+      Fx = 0;
+      Fy = 1;
+    } else
+      bend_fields(fmode, eo1, Fx_xy, Fy_xy, X, Y, Fx, Fy);
+    const double dp_prime =
+      -__ldg(&d[BD_RAD]) * (sqr(Fx) + sqr(Fy)) * sqr(1 + D) * sqrt(sqr(1 + X / rho0) + sqr(QX) + sqr(QY));
+    D -= dp_prime * X * __ldg(&d[BD_TE2]);
   }
 #if TRK_FAST
   if (flags & BF_RAD) {
@@ -1572,7 +1657,7 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
   yp = QY;
   dp = D;
   if (edge2)
-    bend_edge(edge2, d, BD_E2, 1, rho_a, nidx, Fr + FR_CURV_LEN, x, xp, y, yp, s, dp);
+    bend_edge(edge2, d, BD_E2, 1, rho_a, nidx, Fr + FR_CURV_LEN, expanded, x, xp, y, yp, s, dp);
   if (flags & BF_MISALIGN) {
     p.x = x * ct - y * st + __ldg(&d[BD_ET + 0]);
     p.y = x * st + y * ct + __ldg(&d[BD_ET + 2]);

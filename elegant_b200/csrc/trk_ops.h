@@ -58,6 +58,9 @@ enum trk_op_kind {
 #define BF_RAD 8       /* radiation block after each kick (SYNCH_RAD and/or ISR) */
 #define BF_ISR 16      /* incoherent synchrotron radiation (ISR) */
 #define BF_ISR1OFF 32  /* ISR1PART=0: no ISR when a single particle is tracked */
+#define BF_EXPAND 64   /* EXPAND_HAMILTONIAN: leading-order drift, (1+delta) coordinate factors */
+#define BF_RADE1 128   /* SYNCH_RAD with an entrance edge angle: delta pre-adjusted at the entrance */
+#define BF_RADE2 256   /* ... and post-adjusted at the exit */
 
 /* RF flags (i[3]) */
 #define RF_SAME_DGAMMA 1

@@ -791,7 +791,7 @@ static int csbend_setup(const trk_lattice *l, int idx, double Po, orc_csbend_set
   double b[9], c[9];
   memset(S, 0, sizeof(*S));
   if (TRK_P(e, CSBEND_REFERENCE_CORRECTION) || TRK_P(e, CSBEND_FSE_CORRECTION) || TRK_P(e, CSBEND_MALIGN_METHOD) ||
-      TRK_P(e, CSBEND_EXPAND_HAMILTONIAN) || TRK_P(e, CSBEND_USE_RAD_DIST))
+      TRK_P(e, CSBEND_USE_RAD_DIST))
     return 1;
   if (TRK_P(e, CSBEND_ANGLE) == 0) {
     S->is_drift = 1;
@@ -895,6 +895,7 @@ static int csbend_setup(const trk_lattice *l, int idx, double Po, orc_csbend_set
   if (S->bd.nSlices < 1)
     return 1;
   S->bd.integ_order = io;
+  S->bd.expanded = TRK_P(e, CSBEND_EXPAND_HAMILTONIAN) != 0;
   /* isrConstant is nonzero (negative) whenever Po>0 even with ISR=0
    * (src/csbend.c:931-934), which enables the (1+DPoP) round trip */
   S->bd.isr_or_rad = Po > 0;
@@ -987,19 +988,19 @@ static void apply_edge_effects(double *x, double *xp, double *y, double *yp, dou
   *yp = yp0 + R43 * y0 + T441 * yp0 * x0 + T431 * x0 * y0 + T432 * xp0 * y0;
 }
 
-/* applySimpleDipoleEdgeKick (src/csbend.c:5664-5690), non-expanded */
+/* applySimpleDipoleEdgeKick (src/csbend.c:5664-5690) */
 static void simple_dipole_edge_kick(double *xp, double *yp, double x, double y, double delta, double rho,
-                                    double ea, double psi, double kickLimit) {
+                                    double ea, double psi, double kickLimit, int expanded) {
   double Qi[6] = {x, *xp, y, *yp, 0, delta};
   double dqx, dqy;
-  orc_to_dipole_canonical(Qi);
+  orc_to_dipole_canonical_x(Qi, expanded);
   dqx = tan(ea) / rho * x;
   if (kickLimit > 0 && fabs(dqx) > kickLimit)
     dqx = SIGN(dqx) * kickLimit;
   dqy = -orc_tan_sel(ea - psi / (1 + delta)) / rho * y;
   Qi[1] += dqx;
   Qi[3] += dqy;
-  orc_from_dipole_canonical(Qi);
+  orc_from_dipole_canonical_x(Qi, expanded);
   *xp = Qi[1];
   *yp = Qi[3];
 }
@@ -1287,7 +1288,7 @@ static void csbend_edge(const orc_csbend_setup *S, int which, double *x, double 
     double rho = (1 + dp) * S->rho_actual;
     apply_edge_effects(x, xp, y, yp, rho, S->n, e, he, psi * (1 + dp), which);
   } else if (eff == 3) {
-    simple_dipole_edge_kick(xp, yp, *x, *y, dp, S->rho_actual, e, psi, lim);
+    simple_dipole_edge_kick(xp, yp, *x, *y, dp, S->rho_actual, e, psi, lim, S->bd.expanded);
   } else if (eff == 2 || eff == 4 || eff == 5) {
     /* in dipole canonical coordinates (src/csbend.c:1139-1200, :1319-1377) */
     double Qi[6], Qf[6] = {0, 0, 0, 0, 0, 0};
@@ -1297,9 +1298,7 @@ static void csbend_edge(const orc_csbend_setup *S, int which, double *x, double 
     Qi[3] = *yp;
     Qi[4] = 0;
     Qi[5] = dp;
-    double f = (1 + Qi[5]) / sqrt(1 + orc_sqr(Qi[1]) + orc_sqr(Qi[3]));
-    Qi[1] *= f;
-    Qi[3] *= f;
+    orc_to_dipole_canonical_x(Qi, S->bd.expanded);
     const double fint = which < 0 ? S->fint1 : S->fint2;
     if (eff == 2)
       fringe_hwang(Qf, Qi, S->rho_actual, (double)which, S->edge_order, e, 2 * S->hgap, fint, he);
@@ -1307,9 +1306,7 @@ static void csbend_edge(const orc_csbend_setup *S, int which, double *x, double 
       fringe_hwang_lindberg(Qf, Qi, S->rho_actual, (double)which, e, 2 * S->hgap, fint, he);
     else
       fringe_curved(Qf, Qi, S->rho_actual, which, S->edge_order, S->k1_fringe, e, S->fringe_int[which < 0 ? 0 : 1]);
-    f = 1 / sqrt(orc_sqr(1 + Qf[5]) - orc_sqr(Qf[1]) - orc_sqr(Qf[3]));
-    Qf[1] *= f;
-    Qf[3] *= f;
+    orc_from_dipole_canonical_x(Qf, S->bd.expanded);
     *x = Qf[0];
     *xp = Qf[1];
     *y = Qf[2];
@@ -1355,10 +1352,19 @@ static long track_through_csbend(double *coord, long n_part, const trk_lattice *
     Qi[3] = yp;
     Qi[4] = 0;
     Qi[5] = dp;
-    orc_to_dipole_canonical(Qi);
+    if (S.edge1 && S.e1 != 0 && S.bd.rad_coef) {
+      /* radiation: pre-adjust delta for the sector integration (src/csbend.c:1215-1222) */
+      double Fx, Fy;
+      orc_csbend_fields(&S.bd, &Fx, &Fy, x, y);
+      double dp_prime =
+        -S.bd.rad_coef * (orc_sqr(Fx) + orc_sqr(Fy)) * orc_sqr(1 + dp) * sqrt(orc_sqr(1 + x / S.rho0) + orc_sqr(xp) + orc_sqr(yp));
+      Qi[5] -= dp_prime * x * orc_tan_sel(S.e1);
+    }
+    orc_to_dipole_canonical_x(Qi, S.bd.expanded);
     orc_isr.id = (uint32_t)(long long)c[6];
-    int lost = !orc_integrate_csbend(Qf, Qi, &S.bd, &ap, &dz_lost);
-    orc_from_dipole_canonical(Qf);
+    int lost = S.bd.expanded ? !orc_integrate_csbend_expanded(Qf, Qi, &S.bd, &ap, &dz_lost)
+                             : !orc_integrate_csbend(Qf, Qi, &S.bd, &ap, &dz_lost);
+    orc_from_dipole_canonical_x(Qf, S.bd.expanded);
     if (lost) {
       memcpy(c, Qf, sizeof(double) * 6);
       /* convertFromCSBendCoords (src/csbend.c:4527-4548) */
@@ -1373,6 +1379,14 @@ static long track_through_csbend(double *coord, long n_part, const trk_lattice *
       i_top--;
       i_part--;
       continue;
+    }
+    if (S.edge2 && S.e2 != 0 && S.bd.rad_coef) {
+      /* radiation: post-adjust delta (src/csbend.c:1270-1281) */
+      double Fx, Fy;
+      orc_csbend_fields(&S.bd, &Fx, &Fy, Qf[0], Qf[2]);
+      double dp_prime = -S.bd.rad_coef * (orc_sqr(Fx) + orc_sqr(Fy)) * orc_sqr(1 + Qf[5]) *
+                        sqrt(orc_sqr(1 + Qf[0] / S.rho0) + orc_sqr(Qf[1]) + orc_sqr(Qf[3]));
+      Qf[5] -= dp_prime * Qf[0] * orc_tan_sel(S.e2);
     }
     if (S.bd.isr_or_rad) {
       double p0 = Po * (1 + dp0);

@@ -401,6 +401,7 @@ typedef struct {
   double rad_coef; /* classical radiation (SYNCH_RAD), 0 without */
   double isr_constant; /* incoherent radiation (ISR), 0 without */
   int isr1off;         /* ISR1PART=0 */
+  int expanded;        /* EXPAND_HAMILTONIAN */
 } orc_bend;
 
 /* computeCSBENDFields (src/csbend.c:99-172) */
@@ -524,17 +525,102 @@ static int orc_integrate_csbend(orc_r *Qf, const orc_r *Qi, const orc_bend *b, c
   return 1;
 }
 
-/* convertToDipoleCanonicalCoordinates / convertFrom... (src/csbend.c:1436-1454) */
-static inline void orc_to_dipole_canonical(orc_r *Q) {
-  orc_r f = (1 + Q[5]) / ORC_SQRT(1 + orc_sqr(Q[1]) + orc_sqr(Q[3]));
+/* convertToDipoleCanonicalCoordinates / convertFrom... (src/csbend.c:1436-1454);
+ * with the expanded Hamiltonian the factors are (1+delta) and 1/(1+delta) */
+static inline void orc_to_dipole_canonical_x(orc_r *Q, int expanded) {
+  orc_r f;
+  if (expanded)
+    f = (1 + Q[5]);
+  else
+    f = (1 + Q[5]) / ORC_SQRT(1 + orc_sqr(Q[1]) + orc_sqr(Q[3]));
   Q[1] *= f;
   Q[3] *= f;
 }
 
-static inline void orc_from_dipole_canonical(orc_r *Q) {
-  orc_r f = 1 / ORC_SQRT(orc_sqr(1 + Q[5]) - orc_sqr(Q[1]) - orc_sqr(Q[3]));
+static inline void orc_from_dipole_canonical_x(orc_r *Q, int expanded) {
+  orc_r f;
+  if (expanded)
+    f = 1 / (1 + Q[5]);
+  else
+    f = 1 / ORC_SQRT(orc_sqr(1 + Q[5]) - orc_sqr(Q[1]) - orc_sqr(Q[3]));
   Q[1] *= f;
   Q[3] *= f;
+}
+
+static inline void orc_to_dipole_canonical(orc_r *Q) { orc_to_dipole_canonical_x(Q, 0); }
+static inline void orc_from_dipole_canonical(orc_r *Q) { orc_from_dipole_canonical_x(Q, 0); }
+
+/* integrate_csbend_ordn_expanded (src/csbend.c:1722-1900): the Hamiltonian
+ * expanded to leading order, drift Hd1 + Hd2 + Hd1 with
+ * Hd1 = -(1+x/rho0)(1+delta)/2 and Hd2 = (qx^2+qy^2)/(2(1+delta)); the
+ * aperture is checked at each slice start, after every drift substep and at
+ * the end; no reference-trajectory correction, iSlice=-1. */
+static int orc_integrate_csbend_expanded(orc_r *Qf, const orc_r *Qi, const orc_bend *b, const orc_aperture *ap,
+                                         orc_r *dz_lost) {
+  const double *driftFrac, *kickFrac;
+  int nSubsteps = orc_substeps(b->integ_order, &driftFrac, &kickFrac);
+  double rho0 = b->rho0;
+  long n = b->nSlices, i;
+  orc_r dist, Fx, Fy;
+  double s = b->length;
+  for (int k = 0; k < 6; k++)
+    Qf[k] = Qi[k];
+  dist = 0;
+  s /= n;
+  *dz_lost = 0;
+  for (i = 0; i < n; i++) {
+    if (ap && !orc_check_mult_aperture(Qf[0], Qf[2], ap))
+      return 0;
+    for (int j = 0; j < nSubsteps; j++) {
+      double dsh = s * driftFrac[j];
+      Qf[1] += dsh * (1 + Qf[5]) / (2 * rho0);
+      dist += dsh * (1 + (orc_sqr(Qf[1]) + orc_sqr(Qf[3])) / 2);
+      *dz_lost += dsh;
+      Qf[0] += Qf[1] * dsh / (1 + Qf[5]);
+      Qf[2] += Qf[3] * dsh / (1 + Qf[5]);
+      Qf[1] += dsh * (1 + Qf[5]) / (2 * rho0);
+      if (ap && !orc_check_mult_aperture(Qf[0], Qf[2], ap))
+        return 0;
+      if (kickFrac[j] == 0)
+        break;
+      double ds = s * kickFrac[j];
+      orc_csbend_fields(b, &Fx, &Fy, Qf[0], Qf[2]);
+      Qf[1] += -ds * (1 + Qf[0] / rho0) * Fy / b->rho_actual;
+      Qf[3] += ds * (1 + Qf[0] / rho0) * Fx / b->rho_actual;
+      if (b->isr_or_rad && (b->rad_coef || b->isr_constant > 0)) {
+        /* src/csbend.c:1833-1863 */
+        orc_r f = (1 + Qf[0] * (1. / rho0)) / ORC_SQRT(orc_sqr(1 + Qf[5]) - orc_sqr(Qf[1]) - orc_sqr(Qf[3]));
+        orc_r xp = Qf[1] * f;
+        orc_r yp = Qf[3] * f;
+        orc_r dsFactor = ORC_SQRT(orc_sqr(1 + Qf[0] * (1. / rho0)) + orc_sqr(xp) + orc_sqr(yp));
+        orc_r F2 = orc_sqr(Fx) + orc_sqr(Fy);
+        orc_r deltaFactor = orc_sqr(1 + Qf[5]);
+        double dsISR = s / 3;
+        Qf[1] /= (1 + Qf[5]);
+        Qf[3] /= (1 + Qf[5]);
+        if (b->rad_coef)
+          Qf[5] -= b->rad_coef * deltaFactor * F2 * ds * dsFactor;
+        if (b->isr_constant > 0 && !(orc_isr.single && b->isr1off)) {
+          const double g =
+            trk_isr_gauss(orc_isr.seed, orc_isr.id, orc_isr.pass, orc_isr.elem, (uint32_t)(i * 8 + j), 3.0);
+          Qf[5] -= b->isr_constant * deltaFactor * pow(ORC_VAL(F2), 0.75) * ORC_SQRT(dsISR * dsFactor) * g;
+        }
+        Qf[1] *= (1 + Qf[5]);
+        Qf[3] *= (1 + Qf[5]);
+      } else if (b->isr_or_rad) {
+        Qf[1] /= (1 + Qf[5]);
+        Qf[3] /= (1 + Qf[5]);
+        Qf[1] *= (1 + Qf[5]);
+        Qf[3] *= (1 + Qf[5]);
+      }
+    }
+  }
+  if (ap && !orc_check_mult_aperture(Qf[0], Qf[2], ap)) {
+    *dz_lost = n * s;
+    return 0;
+  }
+  Qf[4] += dist;
+  return 1;
 }
 
 /* ------------------------------------------------------------ RF energy */

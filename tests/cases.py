@@ -111,6 +111,15 @@ ELEMENT_CASES = {
                                     FRINGE2K4=1e-6, FRINGE2K5=0.06, FRINGE2K6=0.2),
     "csbend_curved_mixed": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=0.03, HGAP=0.02, FINT=0.5,
                                   EDGE1_EFFECTS=5, EDGE2_EFFECTS=2, N_SLICES=8, **CURVED_FRINGE),
+    "csbend_rad_edges": single("CSBEND", L=1.0, ANGLE=-0.08, E1=0.04, E2=0.03, K1=0.1, SYNCH_RAD=1, N_SLICES=8),
+    "csbend_expanded": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=0.03, K1=0.2, K2=3.0, EXPAND_HAMILTONIAN=1,
+                              N_SLICES=8),
+    "csbend_expanded_fringes": single("CSBEND", L=1.0, ANGLE=-0.07, E1=0.03, E2=0.05, HGAP=0.02, FINT=0.5,
+                                      EDGE1_EFFECTS=5, EDGE2_EFFECTS=3, EXPAND_HAMILTONIAN=1, N_SLICES=8,
+                                      INTEGRATION_ORDER=6, **CURVED_FRINGE),
+    "csbend_expanded_hwang_rad": single("CSBEND", L=1.0, ANGLE=0.08, E1=0.04, E2=0.03, HGAP=0.02, FINT=0.5,
+                                        EDGE1_EFFECTS=2, EDGE2_EFFECTS=4, K1=0.1, SYNCH_RAD=1, EXPAND_HAMILTONIAN=1,
+                                        N_SLICES=8, INTEGRATION_ORDER=2),
     "csbend_xreference": single("CSBEND", L=1.0, ANGLE=0.06, XREFERENCE=0.02, F1=1e-3, F2=-2e-3, F3=5e-4, G1=4e-4,
                                 G2=-1e-4, N_SLICES=8, EPITCH=1e-3, EYAW=-2e-3, XSTEERING=1, SQRT_ORDER=2,
                                 FRINGE1K0=0.1, TRACKING_MATRIX=2),

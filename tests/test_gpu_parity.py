@@ -21,7 +21,7 @@ from tests.helpers import compare, gpu_run, oracle_run
 
 pytestmark = pytest.mark.gpu
 PC = configs.P_CENTRAL
-GLIBC_SINH_CASES = {"csbend_curved", "csbend_curved_order2", "csbend_curved_mixed"}
+GLIBC_SINH_CASES = {"csbend_curved", "csbend_curved_order2", "csbend_curved_mixed", "csbend_expanded_fringes"}
 
 
 @pytest.mark.parametrize("name", sorted(ELEMENT_CASES))
