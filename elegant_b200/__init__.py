@@ -71,6 +71,13 @@ class _ApertureSearch(ctypes.Structure):
                 ("split_fraction", ctypes.c_double), ("orbit", ctypes.c_double * 6)]
 
 
+class _ApertureGrid(ctypes.Structure):
+    _fields_ = [("delta_mode", ctypes.c_int32), ("reserved", ctypes.c_int32), ("nx", ctypes.c_long),
+                ("ny", ctypes.c_long), ("ndelta", ctypes.c_long), ("xmin", ctypes.c_double), ("xmax", ctypes.c_double),
+                ("ymin", ctypes.c_double), ("ymax", ctypes.c_double), ("deltamin", ctypes.c_double),
+                ("deltamax", ctypes.c_double), ("orbit", ctypes.c_double * 6)]
+
+
 class _Stats(ctypes.Structure):
     _fields_ = [("n_total", ctypes.c_long), ("n_left", ctypes.c_long), ("particle_passes", ctypes.c_long),
                 ("device_ms", ctypes.c_double), ("kernel_launches", ctypes.c_long), ("p_central", ctypes.c_double),
@@ -141,6 +148,8 @@ def _declare(lib):
         "trk_sort_by_id": (I, [P]),
         "trk_aperture_search_lines": (I, [P, ctypes.POINTER(P), I, ctypes.POINTER(_ApertureSearch),
                                           ctypes.POINTER(_Run), DP, DP, DP, DP, DP, DP, DP, DP]),
+        "trk_aperture_search_grid": (I, [P, ctypes.POINTER(P), I, ctypes.POINTER(_ApertureGrid),
+                                         ctypes.POINTER(_Run), DP, DP, DP, DP, DP, DP, DP]),
         "trk_adjoint_ensemble": (I, [P, ctypes.POINTER(P), I, ctypes.POINTER(L), ctypes.POINTER(_Run), D, DP, DP, I]),
         "trk_adjoint_param_count": (I, [P]),
         "trk_objective": (I, [P, D, DP]),
@@ -441,6 +450,40 @@ class Tracker:
             _dptr(out["x_clipped"]), _dptr(out["y_clipped"]), _dptr(out["x_lost"]), _dptr(out["y_lost"]),
             _dptr(out["s_lost"]), _dptr(area)))
         res = {k: v.reshape(V, lines) for k, v in out.items()}
+        res["area"] = area
+        return res
+
+    def aperture_search_grid(self, lattices, p_central, n_passes, nx=0, ny=0, xmin=0.0, xmax=0.0, ymin=0.0, ymax=0.0,
+                             delta_mode=0, ndelta=0, deltamin=0.0, deltamax=0.0, orbit=None, fast=True, variant=-1):
+        """elegant's grid-mode aperture search for one lattice or a list of
+        error-seed lattices.  Returns a dict of (variants, 2, nu) arrays
+        u_limit, v_limit, x_lost, y_lost, s_lost, delta_lost (side 1 only
+        when the v range reaches below zero) and area (variants,).  The
+        loaded beam is replaced."""
+        lats = lattices if isinstance(lattices, (list, tuple)) else [lattices]
+        nats = [self.native(lat) for lat in lats]
+        arr = (ctypes.c_void_p * len(nats))(*[n.ptr.value for n in nats])
+        G = _ApertureGrid()
+        G.delta_mode, G.nx, G.ny, G.ndelta = delta_mode, nx, ny, ndelta
+        G.xmin, G.xmax, G.ymin, G.ymax, G.deltamin, G.deltamax = xmin, xmax, ymin, ymax, deltamin, deltamax
+        for k, v in enumerate(np.zeros(6) if orbit is None else orbit):
+            G.orbit[k] = float(v)
+        run = _Run()
+        self.lib.trk_run_defaults(ctypes.byref(run))
+        run.p_central = p_central
+        run.n_passes = n_passes
+        run.fast_math = 1 if fast else 0
+        run.variant = variant
+        V = len(nats)
+        nu = ndelta if delta_mode else nx
+        out = {k: np.zeros(V * 2 * max(nu, 1)) for k in ("u_limit", "v_limit", "x_lost", "y_lost", "s_lost",
+                                                          "delta_lost")}
+        area = np.zeros(V)
+        _check(self.lib, self.lib.trk_aperture_search_grid(
+            self.ctx, arr, V, ctypes.byref(G), ctypes.byref(run), _dptr(out["u_limit"]), _dptr(out["v_limit"]),
+            _dptr(out["x_lost"]), _dptr(out["y_lost"]), _dptr(out["s_lost"]), _dptr(out["delta_lost"]),
+            _dptr(area)))
+        res = {k: v.reshape(V, 2, -1) for k, v in out.items()}
         res["area"] = area
         return res
 

@@ -305,3 +305,150 @@ extern "C" int trk_aperture_search_lines(trk_context *ctx, const trk_lattice *co
   }
   return TRK_OK;
 }
+
+/* do_aperture_search_grid (src/aperture_search.c:1236-1521) over n_variants
+ * lattices: each side's grid for every variant in one launch, then the
+ * reference's column reduction (survivors raise v_limit, a loss nearer the
+ * origin lowers it again) and area. */
+extern "C" int trk_aperture_search_grid(trk_context *ctx, const trk_lattice *const *lattices, int n_variants,
+                                        const trk_aperture_grid *grid, const trk_run *run, double *u_limit,
+                                        double *v_limit, double *x_lost, double *y_lost, double *s_lost,
+                                        double *delta_lost, double *area) {
+  if (!ctx || !lattices || !grid || !run || n_variants < 1 || !v_limit)
+    return trk_set_error(TRK_ERR_ARG, "null argument");
+  for (int v = 0; v < n_variants; v++)
+    if (!lattices[v])
+      return trk_set_error(TRK_ERR_ARG, "null lattice %d", v);
+  const trk_aperture_grid &G = *grid;
+  int icu, icv;
+  long nu, nv;
+  double umin, umax, vmin, vmax;
+  if (G.delta_mode == 1) { /* DELTA_X_MODE */
+    icu = 5, icv = 0, nu = G.ndelta, umin = G.deltamin, umax = G.deltamax, nv = G.nx, vmin = G.xmin, vmax = G.xmax;
+  } else if (G.delta_mode == 2) { /* DELTA_Y_MODE */
+    icu = 5, icv = 2, nu = G.ndelta, umin = G.deltamin, umax = G.deltamax, nv = G.ny, vmin = G.ymin, vmax = G.ymax;
+  } else if (G.delta_mode == 0) {
+    icu = 0, icv = 2, nu = G.nx, umin = G.xmin, umax = G.xmax, nv = G.ny, vmin = G.ymin, vmax = G.ymax;
+  } else
+    return trk_set_error(TRK_ERR_ARG, "delta_mode must be 0, 1 or 2");
+  if (nu < 2 || nv < 2)
+    return trk_set_error(TRK_ERR_ARG, "grid needs at least 2 points per axis");
+  const double DMAX = 1.7976931348623157e308;
+  const double du = (umax - umin) / (nu - 1);
+  const int sides = vmin < 0 ? 2 : 1;
+  const size_t per = (size_t)nu * nv;
+  const long n = (long)(per * n_variants);
+  for (int v = 0; v < n_variants; v++) {
+    if (area)
+      area[v] = 0;
+    for (int side = 0; side < 2; side++)
+      for (long iu = 0; iu < nu; iu++) {
+        const size_t o = ((size_t)v * 2 + side) * nu + iu;
+        v_limit[o] = 0;
+        if (u_limit)
+          u_limit[o] = 0;
+        if (x_lost)
+          x_lost[o] = DMAX;
+        if (y_lost)
+          y_lost[o] = DMAX;
+        if (s_lost)
+          s_lost[o] = DMAX;
+        if (delta_lost)
+          delta_lost[o] = DMAX;
+      }
+  }
+  std::vector<double> rows((size_t)n * 7), out((size_t)n * 7);
+  std::vector<long> lost_pass(n), offsets(n_variants + 1), at(n);
+  std::vector<double> vl(nu), vl1(nu), xl(nu), yl(nu), sl(nu), dl(nu);
+  for (int v = 0; v <= n_variants; v++)
+    offsets[v] = (long)(per * v);
+  int rc;
+  for (int side = 0; side < sides; side++) {
+    const double dv = side == 0 ? vmax / (nv - 1) : vmin / (nv - 1);
+    long r = 0;
+    for (int v = 0; v < n_variants; v++)
+      for (long iu = 0; iu < nu; iu++)
+        for (long iv = 0; iv < nv; iv++, r++) {
+          double *row = &rows[(size_t)r * 7];
+          for (int c = 0; c < 6; c++)
+            row[c] = 0;
+          row[icu] = iu * du + umin;
+          row[icv] = iv * dv;
+          for (int c = 0; c < 6; c++)
+            row[c] += G.orbit[c];
+          row[6] = (double)(r + 1);
+        }
+    if ((rc = trk_beam_load(ctx, rows.data(), n, 7)))
+      return rc;
+    trk_stats stats;
+    rc = n_variants == 1 ? trk_track(ctx, lattices[0], run, &stats)
+                         : trk_track_ensemble(ctx, lattices, n_variants, offsets.data(), run, &stats);
+    if (rc)
+      return rc;
+    long n_left = 0;
+    if ((rc = trk_beam_store(ctx, out.data(), 7, &n_left, lost_pass.data(), nullptr)))
+      return rc;
+    for (long i = 0; i < n; i++)
+      at[i] = -1;
+    for (long i = 0; i < n; i++) {
+      const long id = (long)out[(size_t)i * 7 + 6] - 1;
+      if (id >= 0 && id < n)
+        at[id] = i;
+    }
+    for (int v = 0; v < n_variants; v++) {
+      const long base = offsets[v];
+      long survivors = 0;
+      for (long iu = 0; iu < nu; iu++) {
+        vl[iu] = 0;
+        vl1[iu] = side == 0 ? vmax + dv : vmin + dv;
+        xl[iu] = yl[iu] = sl[iu] = dl[iu] = DMAX;
+      }
+      /* survivors first, then the lost particles (src/aperture_search.c:1422-1449) */
+      for (int pass = 0; pass < 2; pass++)
+        for (long k = 0; k < (long)per; k++) {
+          const long i = at[base + k];
+          const bool lost = i < 0 || lost_pass[i] >= 0;
+          if (lost != (pass == 1))
+            continue;
+          const long iu = k / nv, iv = k % nv;
+          const double vv = iv * dv;
+          if (!lost) {
+            survivors++;
+            if ((side == 0 && vv > vl[iu]) || (side == 1 && vv < vl[iu]))
+              vl[iu] = vv;
+            continue;
+          }
+          if ((side == 0 && vv < vl[iu]) || (side == 1 && vv > vl[iu]))
+            vl[iu] = vv;
+          if (i >= 0 && ((side == 0 && vv < vl1[iu]) || (side == 1 && vv > vl1[iu]))) {
+            vl1[iu] = vv;
+            xl[iu] = out[(size_t)i * 7 + 0];
+            yl[iu] = out[(size_t)i * 7 + 2];
+            sl[iu] = out[(size_t)i * 7 + 4];
+            dl[iu] = out[(size_t)i * 7 + 5];
+          }
+        }
+      double a = 0;
+      if (survivors)
+        for (long iu = 0; iu < nu; iu++)
+          a += std::fabs(vl[iu] * du);
+      if (area)
+        area[v] += a;
+      for (long iu = 0; iu < nu; iu++) {
+        const size_t o = ((size_t)v * 2 + side) * nu + iu;
+        v_limit[o] = vl[iu];
+        if (u_limit)
+          u_limit[o] = iu * du + umin;
+        if (x_lost)
+          x_lost[o] = xl[iu];
+        if (y_lost)
+          y_lost[o] = yl[iu];
+        if (s_lost)
+          s_lost[o] = sl[iu];
+        if (delta_lost)
+          delta_lost[o] = dl[iu];
+      }
+    }
+  }
+  return TRK_OK;
+}

@@ -353,6 +353,32 @@ int trk_aperture_search_lines(trk_context *ctx, const trk_lattice *const *lattic
                               double *y_limit, double *x_clipped, double *y_clipped, double *x_lost, double *y_lost,
                               double *s_lost, double *area);
 
+/* The grid mode of elegant's aperture search (do_aperture_search_grid,
+ * src/aperture_search.c:1236-1521): a grid of u (x or delta) by v (y or x)
+ * tracked for run->n_passes passes, once for v >= 0 and, when vmin < 0, once
+ * more for v <= 0. */
+typedef struct {
+  int32_t delta_mode; /* 0: u = x, v = y; 1: u = delta, v = x; 2: u = delta, v = y */
+  int32_t reserved;
+  long nx, ny, ndelta; /* points per axis (the two the mode uses, each >= 2) */
+  double xmin, xmax, ymin, ymax, deltamin, deltamax;
+  double orbit[6]; /* added to every particle (offset_by_orbit; zeros otherwise) */
+} trk_aperture_grid;
+/* For each of n_variants lattices, every grid point of a side tracked in one
+ * launch.  Per variant v, side (0: v >= 0; 1: v <= 0, only if vmin < 0) and
+ * u column iu, at [(v * 2 + side) * nu + iu]: u_limit (the column's u),
+ * v_limit (the largest |v| below the first loss of the column, as the
+ * reference reduces it), and the coordinates of that first lost particle at
+ * its loss, x_lost, y_lost, s_lost, delta_lost (its momentum p, as the
+ * reference's lost rows hold it; DBL_MAX where nothing was lost); rows of a
+ * side not searched are zero with lost coordinates DBL_MAX.  area[v] = sum
+ * over sides that kept a survivor of |v_limit du|.  Any output but v_limit
+ * may be NULL.  Particle IDs count up over the whole launch.  The loaded
+ * beam is replaced. */
+int trk_aperture_search_grid(trk_context *ctx, const trk_lattice *const *lattices, int n_variants,
+                             const trk_aperture_grid *grid, const trk_run *run, double *u_limit, double *v_limit,
+                             double *x_lost, double *y_lost, double *s_lost, double *delta_lost, double *area);
+
 /* ------------------------------------------------------ batched ensembles */
 /* Track `n_variants` lattices that differ only in element parameter values
  * (error seeds, grids) in one launch.  `lattices` holds n_variants lattices of

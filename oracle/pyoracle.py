@@ -396,6 +396,67 @@ def observe_refgpu(beam, p_central, mp_charge=0.0, flags=0x8, start_pid=-1, end_
 
 
 # ------------------------------------------------------------ aperture search
+def aperture_search_grid(lattice, p_central, n_passes, nx=0, ny=0, xmin=0.0, xmax=0.0, ymin=0.0, ymax=0.0,
+                         delta_mode=0, ndelta=0, deltamin=0.0, deltamax=0.0, orbit=None):
+    """do_aperture_search_grid (src/aperture_search.c:1236-1521) restated:
+    each side's grid tracked by the oracle as one beam (IDs 1.. in grid
+    order), then the reference's reduction over the survivor rows and the
+    lost rows in their order.  Returns dict of (2, nu) arrays u_limit,
+    v_limit, x_lost, y_lost, s_lost, delta_lost and the area."""
+    orbit = np.zeros(6) if orbit is None else np.asarray(orbit, dtype=np.float64)
+    if delta_mode == 1:
+        icu, icv, nu, umin, umax, nv, vmin, vmax = 5, 0, ndelta, deltamin, deltamax, nx, xmin, xmax
+    elif delta_mode == 2:
+        icu, icv, nu, umin, umax, nv, vmin, vmax = 5, 2, ndelta, deltamin, deltamax, ny, ymin, ymax
+    else:
+        icu, icv, nu, umin, umax, nv, vmin, vmax = 0, 2, nx, xmin, xmax, ny, ymin, ymax
+    big = 1.7976931348623157e308
+    du = (umax - umin) / (nu - 1)
+    out = {k: np.zeros((2, nu)) for k in ("u_limit", "v_limit")}
+    out.update({k: np.full((2, nu), big) for k in ("x_lost", "y_lost", "s_lost", "delta_lost")})
+    area = 0.0
+    for side in range(2 if vmin < 0 else 1):
+        dv = vmax / (nv - 1) if side == 0 else vmin / (nv - 1)
+        b = np.zeros((nu * nv, 7))
+        ip = 0
+        for iu in range(nu):
+            for iv in range(nv):
+                b[ip, icu] = iu * du + umin
+                b[ip, icv] = iv * dv
+                b[ip, 6] = ip + 1
+                ip += 1
+        b[:, :6] += orbit
+        rows, n_left, _ = track(lattice, b, n_passes, p_central)
+        vl = [0.0] * nu
+        vl1 = [(vmax if side == 0 else vmin) + dv] * nu
+        for ip in range(n_left):
+            pid = int(rows[ip, 6])
+            iu, iv = (pid - 1) // nv, (pid - 1) % nv
+            v = iv * dv
+            if (side == 0 and v > vl[iu]) or (side == 1 and v < vl[iu]):
+                vl[iu] = v
+        for ip in range(n_left, nu * nv):
+            pid = int(rows[ip, 6])
+            iu, iv = (pid - 1) // nv, (pid - 1) % nv
+            v = iv * dv
+            if (side == 0 and v < vl[iu]) or (side == 1 and v > vl[iu]):
+                vl[iu] = v
+            if (side == 0 and v < vl1[iu]) or (side == 1 and v > vl1[iu]):
+                vl1[iu] = v
+                out["x_lost"][side, iu] = rows[ip, 0]
+                out["y_lost"][side, iu] = rows[ip, 2]
+                out["s_lost"][side, iu] = rows[ip, 4]
+                out["delta_lost"][side, iu] = rows[ip, 5]
+        if n_left:
+            for iu in range(nu):
+                area += abs(vl[iu] * du)
+        for iu in range(nu):
+            out["u_limit"][side, iu] = iu * du + umin
+            out["v_limit"][side, iu] = vl[iu]
+    out["area"] = area
+    return out
+
+
 def aperture_search_lines(lattice, p_central, n_passes, lines, nx, xmax, ymax, n_splits=0, split_fraction=0.5,
                           full_plane=0, slope_mode=0, xpmax=0.0, ypmax=0.0, orbit=None, area_fn=None):
     """do_aperture_search_line (src/aperture_search.c:985-1234) restated

@@ -1,8 +1,10 @@
-"""Line-mode dynamic-aperture search (trk_aperture_search_lines) against
+"""Dynamic-aperture searches.  Line modes (trk_aperture_search_lines) against
 elegant's do_aperture_search_line restated serially over the oracle
 (oracle/pyoracle.py: one particle at a time, each sweep stopping at the first
 loss), and its island clipping and area against elegant's own
-trimApertureSearchResult (compiled from the reference sources)."""
+trimApertureSearchResult (compiled from the reference sources).  Grid mode
+(trk_aperture_search_grid) against do_aperture_search_grid restated over the
+oracle, in (x, y), (delta, x) and (delta, y), one- and two-sided."""
 import numpy as np
 import pytest
 
@@ -87,3 +89,54 @@ def test_error_seed_batch_equals_separate_searches(tracker, fast):
             assert np.array_equal(g[k][v], one[k][0]), (v, k)
         assert g["area"][v] == one["area"][0]
     assert len(set(np.round(g["area"], 12))) > 1  # the seeds differ
+
+
+def test_grid_restatement_on_a_known_aperture():
+    """On the elliptical box, each column's limit is the last grid point
+    inside the ellipse, and both sides agree by symmetry."""
+    r = pyoracle.aperture_search_grid(_box_lattice(), PC, 1, nx=11, ny=9, xmin=-0.012, xmax=0.012, ymin=-0.006,
+                                      ymax=0.006)
+    u, v = r["u_limit"][0], r["v_limit"][0]
+    dv = 0.006 / 8
+    for k in range(11):
+        inside = [j * dv for j in range(9) if (u[k] / 0.01) ** 2 + (j * dv / 0.005) ** 2 <= 1]
+        assert v[k] == (max(inside) if inside else 0.0)
+    assert np.array_equal(r["v_limit"][1], -r["v_limit"][0])
+    assert r["area"] > 0
+
+
+GRID_CASES = [dict(nx=9, ny=7, xmin=-0.03, xmax=0.03, ymin=0.0, ymax=0.015),
+              dict(nx=8, ny=6, xmin=-0.03, xmax=0.025, ymin=-0.012, ymax=0.015),
+              dict(delta_mode=1, ndelta=7, nx=8, deltamin=-0.02, deltamax=0.02, xmin=-0.03, xmax=0.03),
+              dict(delta_mode=2, ndelta=6, ny=7, deltamin=-0.015, deltamax=0.02, ymin=0.0, ymax=0.015)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("opts", GRID_CASES)
+def test_grid_search_equals_reference_restatement(tracker, opts):
+    lat, passes = _ring(), 30
+    g = tracker.aperture_search_grid(lat, PC, passes, fast=False, **opts)
+    with pyoracle.modes(exact_sums=True, cr_math=True):
+        r = pyoracle.aperture_search_grid(lat, PC, passes, **opts)
+    for k in ("u_limit", "v_limit", "x_lost", "y_lost", "s_lost", "delta_lost"):
+        assert np.array_equal(g[k][0], r[k]), (k, g[k][0], r[k])
+    assert g["area"][0] == r["area"]
+    assert np.any(r["x_lost"] < 1e300) and np.any(r["v_limit"] != 0)
+
+
+@pytest.mark.gpu
+def test_grid_error_seed_batch_equals_separate_searches(tracker):
+    lats = [_ring(seed=s) for s in range(3)]
+    kw = GRID_CASES[1]
+    g = tracker.aperture_search_grid(lats, PC, 30, fast=True, **kw)
+    for v, lat in enumerate(lats):
+        one = tracker.aperture_search_grid(lat, PC, 30, fast=True, **kw)
+        for k in ("u_limit", "v_limit", "x_lost", "y_lost", "s_lost", "delta_lost"):
+            assert np.array_equal(g[k][v], one[k][0]), (v, k)
+        assert g["area"][v] == one["area"][0]
+
+
+@pytest.mark.gpu
+def test_grid_rejects_a_one_point_axis(tracker):
+    with pytest.raises(Exception):
+        tracker.aperture_search_grid(_box_lattice(), PC, 1, nx=1, ny=5, xmax=0.01, ymax=0.01)
