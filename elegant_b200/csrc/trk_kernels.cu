@@ -1275,19 +1275,27 @@ __device__ __noinline__ double fringe_curved(double &x, double &px, double &y, d
   return dtau;
 }
 
+/* linear edge kick, EDGE_EFFECTS=1 with EDGE_ORDER <= 1 (src/csbend.c:1127-1134) */
+__device__ __forceinline__ void edge_lin1(const double *__restrict__ d, int base, double rho_a, double x, double &xp,
+                                          double y, double &yp, double dp) {
+  const double e = __ldg(&d[base + 0]), te = __ldg(&d[base + 1]), psi = __ldg(&d[base + 2]);
+  const double lim = __ldg(&d[base + 3]);
+  double rho = (1 + dp) * rho_a;
+  double delta_xp = te / rho * x;
+  if (lim > 0 && fabs(delta_xp) > lim)
+    delta_xp = (delta_xp < 0 ? -1 : 1) * lim;
+  xp += delta_xp;
+  double t2 = psi == 0 ? te : M_TAN(e - psi / (1 + dp));
+  yp -= t2 / rho * y;
+}
+
 __device__ __forceinline__ void bend_edge(int mode, const double *__restrict__ d, int base, int which, double rho_a,
                                           double nidx, const double *__restrict__ fr, bool expanded, double &x,
                                           double &xp, double &y, double &yp, double &s, double dp) {
   const double e = __ldg(&d[base + 0]), te = __ldg(&d[base + 1]), psi = __ldg(&d[base + 2]);
   const double lim = __ldg(&d[base + 3]), he = __ldg(&d[base + 4]), secb = __ldg(&d[base + 5]);
   if (mode == EDGE_LIN1) {
-    double rho = (1 + dp) * rho_a;
-    double delta_xp = te / rho * x;
-    if (lim > 0 && fabs(delta_xp) > lim)
-      delta_xp = (delta_xp < 0 ? -1 : 1) * lim;
-    xp += delta_xp;
-    double t2 = psi == 0 ? te : M_TAN(e - psi / (1 + dp));
-    yp -= t2 / rho * y;
+    edge_lin1(d, base, rho_a, x, xp, y, yp, dp);
   } else if (mode == EDGE_LIN2) {
     double rho = (1 + dp) * rho_a;
     edge_order2(x, xp, y, yp, rho, nidx, e, te, secb, he, psi * (1 + dp), which);
@@ -1679,6 +1687,85 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
   }
   return true;
 }
+
+#if !TRK_FAST
+/* op_bend restricted to what a plain pure dipole reaches (OPK_DIPOLE: no
+ * misalignment, tilt, radiation, field expansion or expanded Hamiltonian;
+ * edges at most the linear kick), with the same operations in the same
+ * order, the signed-zero-preserving tilt products of a loss included.  The
+ * lean parity kernels take it so that the general body's other branches do
+ * not weigh on their register allocation. */
+__device__ __forceinline__ bool op_dipole_exact(const trk_op *__restrict__ op, Part &p, double Po, double z_start,
+                                                const trk_aperture *ap) {
+  const double *d = op->d;
+  const int nSlices = __ldg(&op->i[0]);
+  const int nSub = __ldg(&op->i[1]);
+  const int edge1 = __ldg(&op->i[5]), edge2 = __ldg(&op->i[6]);
+  const int flags = __ldg(&op->i[7]);
+  const double rho0 = __ldg(&d[BD_RHO0]), rho_a = __ldg(&d[BD_RHOA]);
+  double x = p.x, y = p.y, xp = p.xp, yp = p.yp, s = p.s, dp = p.dp;
+  const double dp0 = p.dp;
+  if (edge1 == EDGE_LIN1)
+    edge_lin1(d, BD_E1, rho_a, x, xp, y, yp, dp);
+  double X = x, QX, Y = y, QY, S = 0, D = dp;
+  {
+    double f = (1 + D) / sqrt(1 + sqr(xp) + sqr(yp));
+    QX = xp * f;
+    QY = yp * f;
+  }
+  double dist = 0, dz_lost = 0;
+  int done = 0;
+  bool ok = bend_dipole_exact(d, nSlices, nSub, rho0, (flags & BF_ISR_ROUNDTRIP) != 0, ap, false, 1.0, 0.0, X, QX,
+                              Y, QY, D, dist, done);
+  if (!ok)
+    for (int k = 0; k < done; k++)
+      dz_lost += __ldg(&d[BD_DSH + k % nSub]);
+  if (ok) {
+    dz_lost = nSlices * __ldg(&d[BD_SLICE]);
+    if (!check_aperture(X, Y, ap, false, 1.0, 0.0))
+      ok = false;
+    else
+      S += dist;
+  }
+  {
+    double f = 1 / sqrt(sqr(1 + D) - sqr(QX) - sqr(QY));
+    QX *= f;
+    QY *= f;
+  }
+  if (!ok) {
+    const double ct = __ldg(&d[BD_CT]), st = __ldg(&d[BD_ST]);
+    p.x = X * ct - Y * st;
+    p.y = X * st + Y * ct;
+    p.xp = QX * ct - QY * st;
+    p.yp = QX * st + QY * ct;
+    p.s = z_start + dz_lost;
+    p.dp = Po * (1 + D);
+    return false;
+  }
+  if (flags & BF_ISR_ROUNDTRIP) {
+    double p0 = Po * (1 + dp0);
+    double beta0 = p0 / sqrt(sqr(p0) + 1);
+    double p1 = Po * (1 + D);
+    double beta1 = p1 / sqrt(sqr(p1) + 1);
+    s = beta1 * s / beta0 + S;
+  } else
+    s += S;
+  x = X;
+  xp = QX;
+  y = Y;
+  yp = QY;
+  dp = D;
+  if (edge2 == EDGE_LIN1)
+    edge_lin1(d, BD_E2, rho_a, x, xp, y, yp, dp);
+  p.x = x;
+  p.xp = xp;
+  p.y = y;
+  p.yp = yp;
+  p.s = s;
+  p.dp = dp;
+  return true;
+}
+#endif
 
 /* ----------------------------------------------------------------- RFCA */
 /* add_to_particle_energy (src/simple_rfca.c:987-1006) */
@@ -2305,7 +2392,7 @@ __device__ __forceinline__ bool track_particle(const TrackArgs &a, const trk_op 
 #if TRK_FAST
         ok = op_dipole_fast(op, p, a.Po, h.z_start, ap_in);
 #else
-        ok = op_bend(op, p, a.Po, h.z_start, ap_in, a.field);
+        ok = op_dipole_exact(op, p, a.Po, h.z_start, ap_in);
 #endif
         break;
       case OPK_CFBEND:
@@ -2313,7 +2400,8 @@ __device__ __forceinline__ bool track_particle(const TrackArgs &a, const trk_op 
         if (LEAN != 1)
           ok = op_cfbend_fast(op, p, a.Po, h.z_start, ap_in, a.field);
 #else
-        ok = op_bend(op, p, a.Po, h.z_start, ap_in, a.field);
+        if (LEAN != 1) /* flavour 1 lattices hold no combined-function bend */
+          ok = op_bend(op, p, a.Po, h.z_start, ap_in, a.field);
 #endif
         break;
       case OPK_RF:
@@ -3502,7 +3590,9 @@ void launch_track(const TrackArgs &a, int variant, int lean, long n, int max_blo
     launch_track_t<2>(a, variant, (int)g, block, st);
   else if (lean)
 #else
-  if (lean)
+  /* the parity build's combined-function bends take the general body, which
+   * flavour 1 leaves out: such lattices run the full flavour */
+  if (lean == 1)
 #endif
     launch_track_t<1>(a, variant, (int)g, block, st);
   else
