@@ -5,6 +5,8 @@
  * A run is scheduled as a list of steps per pass:
  *   SEG(ob, oe)   one launch of the fused tracking kernel over ops [ob, oe)
  *   FID(op)       RFCA "tmean" fiducial before the first pass through op
+ *   TAVE(op)      mean arrival time at a LOCK_PHASE / LINEARIZE RFCA, every
+ *                 later pass (the first pass takes it from the fiducial's sum)
  *   WAKE(op)      time statistics, binning, convolution and kick of a wake
  * Passes whose step list is one SEG over the whole lattice are merged into a
  * single multi-pass launch, so a lattice without collective elements runs
@@ -65,7 +67,8 @@ struct trk_context {
   size_t aps_cap = 0;
   double *d_field = nullptr;
   size_t field_cap = 0;
-  double *d_rf_phase = nullptr;
+  double *d_rf_phase = nullptr; /* fiducial phase per RF slot, then (at + rf_cap) the pass's mean time */
+  double *d_rf_tave = nullptr;
   int rf_cap = 0;
   std::vector<int> rf_fid_done;
   int *d_status = nullptr;
@@ -415,6 +418,7 @@ TrackArgs track_args(trk_context *ctx) {
   a.aps = ctx->d_aps;
   a.field = ctx->d_field;
   a.rf_phase = ctx->d_rf_phase;
+  a.rf_tave = ctx->d_rf_tave;
   a.n = ctx->np;
   a.id = c + 6 * cap;
   a.isr_limit = 3.0; /* srGaussianLimit's default (src/track_data.c:65) */
@@ -454,9 +458,11 @@ int upload_compiled(trk_context *ctx) {
   if (c.n_rf_slots > ctx->rf_cap) {
     cudaFree(ctx->d_rf_phase);
     ctx->d_rf_phase = nullptr;
-    CUDA_TRY(cudaMalloc(&ctx->d_rf_phase, sizeof(double) * c.n_rf_slots));
-    CUDA_TRY(cudaMemsetAsync(ctx->d_rf_phase, 0, sizeof(double) * c.n_rf_slots, ctx->stream));
+    ctx->d_rf_tave = nullptr;
+    CUDA_TRY(cudaMalloc(&ctx->d_rf_phase, sizeof(double) * 2 * c.n_rf_slots));
+    CUDA_TRY(cudaMemsetAsync(ctx->d_rf_phase, 0, sizeof(double) * 2 * c.n_rf_slots, ctx->stream));
     ctx->rf_cap = c.n_rf_slots;
+    ctx->d_rf_tave = ctx->d_rf_phase + c.n_rf_slots;
   }
   if ((int)ctx->rf_fid_done.size() < c.n_rf_slots)
     ctx->rf_fid_done.resize(c.n_rf_slots, 0);
@@ -702,9 +708,11 @@ int run_wake(trk_context *ctx, bool fast, int opi, long pass, long fresh_pass, d
 }
 
 struct Step {
-  int kind; /* 0 SEG, 1 FID, 2 WAKE */
+  int kind; /* 0 SEG, 1 FID (and TAVE where the cavity needs it), 2 WAKE, 3 TAVE */
   int ob, oe;
 };
+
+bool rf_needs_tave(const trk_op &op) { return op.kind == OPK_RF && (op.i[3] & (RF_LOCK | RF_LINEAR)); }
 
 void pass_steps(const CompiledLattice &c, std::vector<int> &fid_done, std::vector<Step> &steps) {
   steps.clear();
@@ -712,10 +720,10 @@ void pass_steps(const CompiledLattice &c, std::vector<int> &fid_done, std::vecto
   const int n = (int)c.ops.size();
   for (int k = 0; k < n; k++) {
     const trk_op &op = c.ops[k];
-    if (op.kind == OPK_RF && !fid_done[op.i[1]]) {
+    if (op.kind == OPK_RF && (!fid_done[op.i[1]] || rf_needs_tave(op))) {
       if (k > seg)
         steps.push_back({0, seg, k});
-      steps.push_back({1, k, k + 1});
+      steps.push_back({fid_done[op.i[1]] ? 3 : 1, k, k + 1});
       fid_done[op.i[1]] = 1;
       seg = k;
     } else if (op.kind == OPK_WAKE || op.kind == OPK_TRWAKE) {
@@ -1188,6 +1196,16 @@ int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, 
                                           ctx->d_status, ctx->stream);
           ctx->last_launches++;
           ctx->rf_fid_done[slot] = 1;
+          if (rf_needs_tave(op)) {
+            trk_exact::launch_rf_tave(ctx->d_stats, ctx->d_rf_tave, slot, ctx->stream);
+            ctx->last_launches++;
+          }
+        } else if (st.kind == 3) {
+          const trk_op &op = c.ops[st.ob];
+          if ((rc = time_stats(ctx, fast, 1, op.d[RD_SOFF], Po)))
+            return rc;
+          trk_exact::launch_rf_tave(ctx->d_stats, ctx->d_rf_tave, op.i[1], ctx->stream);
+          ctx->last_launches++;
         } else {
           if ((rc = run_wake(ctx, fast, st.ob, pass, fresh, Po)))
             return rc;
@@ -1334,6 +1352,14 @@ int trk_track_element(trk_context *ctx, const trk_lattice *lattice, int element,
                                    cudaMemcpyDeviceToHost, ctx->stream));
           CUDA_TRY(cudaStreamSynchronize(ctx->stream));
           state->rf_fiducial_seen = 1;
+        }
+        if (rf_needs_tave(op)) {
+          /* the mean arrival time of this call's beam (src/simple_rfca.c:503-556) */
+          if ((rc = time_stats(ctx, fast, 1, op.d[RD_SOFF], Po))) {
+            ctx->comp_src = nullptr;
+            return rc;
+          }
+          trk_exact::launch_rf_tave(ctx->d_stats, ctx->d_rf_tave, slot, ctx->stream);
         }
       }
       TrackArgs ta = track_args(ctx);

@@ -777,10 +777,8 @@ int compile_bend(const trk_lattice *l, int idx, double Po, trk_op *op, std::vect
 }
 
 int compile_rf(const trk_elem *e, trk_op *op, int slot) {
-  if (TRK_P(e, RFCA_CHANGE_T) || TRK_P(e, RFCA_LINEARIZE) || TRK_P(e, RFCA_LOCK_PHASE) || TRK_P(e, RFCA_CHANGE_P0) ||
-      TRK_P(e, RFCA_STANDING_WAVE))
-    return trk_set_error(TRK_ERR_UNSUPPORTED,
-                         "RFCA %s: CHANGE_T, LINEARIZE, LOCK_PHASE, CHANGE_P0 and STANDING_WAVE are not on this path",
+  if (TRK_P(e, RFCA_CHANGE_T) || TRK_P(e, RFCA_CHANGE_P0) || TRK_P(e, RFCA_STANDING_WAVE))
+    return trk_set_error(TRK_ERR_UNSUPPORTED, "RFCA %s: CHANGE_T, CHANGE_P0 and STANDING_WAVE are not on this path",
                          e->name);
   double length = TRK_P(e, RFCA_L);
   if (TRK_P(e, RFCA_VOLT) == 0) {
@@ -792,6 +790,9 @@ int compile_rf(const trk_elem *e, trk_op *op, int slot) {
   if (nKicks <= 0)
     return trk_set_error(TRK_ERR_UNSUPPORTED, "RFCA %s: L>0 with N_KICKS=0 (matrix method) is not on this path",
                          e->name);
+  const bool lock = TRK_P(e, RFCA_LOCK_PHASE) != 0, linearize = TRK_P(e, RFCA_LINEARIZE) != 0;
+  if ((lock || linearize) && nKicks != 1)
+    return trk_set_error(TRK_ERR_PHYSICS, "Must use n_kicks=1 for linearized rf cavity"); /* src/simple_rfca.c:505 */
   double omega = TRK_PIx2 * TRK_P(e, RFCA_FREQ);
   double volt = TRK_P(e, RFCA_VOLT) / (1e6 * TRK_ME_MEV * TRK_PARTICLE_REL_SIGN);
   double tau = omega ? TRK_P(e, RFCA_Q) / omega : 0;
@@ -809,6 +810,10 @@ int compile_rf(const trk_elem *e, trk_op *op, int slot) {
     flags |= RF_END2;
   if (TRK_P(e, RFCA_DX) || TRK_P(e, RFCA_DY))
     flags |= RF_OFFSET;
+  if (lock)
+    flags |= RF_LOCK;
+  if (linearize)
+    flags |= RF_LINEAR;
   op->i[3] = flags;
   op->d[RD_OMEGA] = omega;
   op->d[RD_VOLT] = volt;
@@ -820,6 +825,7 @@ int compile_rf(const trk_elem *e, trk_op *op, int slot) {
   op->d[RD_DY] = TRK_P(e, RFCA_DY);
   op->d[RD_SOFF] = length / 2;
   op->d[RD_TREF] = TRK_P(e, RFCA_T_REFERENCE);
+  op->d[RD_PHASE_LOCK] = TRK_PI / 180 * TRK_P(e, RFCA_PHASE);
   return TRK_OK;
 }
 

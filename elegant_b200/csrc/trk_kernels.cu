@@ -1788,7 +1788,7 @@ __device__ __forceinline__ void add_energy(Part &p, double t, double Po, double 
 /* trackRfCavityWithWakes (src/simple_rfca.c:295-985), kick method,
  * traveling wave, per particle; ends with removeInvalidParticles. */
 __device__ __forceinline__ bool op_rf(const trk_op *__restrict__ op, Part &p, double Po, double z_end,
-                                      const double *__restrict__ rf_phase) {
+                                      const double *__restrict__ rf_phase, const double *__restrict__ rf_tave) {
   const double *d = op->d;
   const int nKicks = __ldg(&op->i[0]);
   const int slot = __ldg(&op->i[1]);
@@ -1801,6 +1801,16 @@ __device__ __forceinline__ bool op_rf(const trk_op *__restrict__ op, Part &p, do
   double dgamma = 0;
   if (flags & RF_SAME_DGAMMA)
     dgamma = volt * M_SIN(phase);
+  /* LOCK_PHASE / LINEARIZE: the pass's mean arrival time (src/simple_rfca.c:500-556) */
+  double tAve = 0, dgammaAve = 0;
+  if (flags & (RF_LOCK | RF_LINEAR)) {
+    tAve = rf_tave[slot];
+    if (flags & RF_LOCK) {
+      phase = __ldg(&d[RD_PHASE_LOCK]);
+      dgammaAve = volt * M_SIN(phase);
+    } else
+      dgammaAve = volt * M_SIN(omega * (tAve - 0.0) + phase);
+  }
   if (flags & RF_OFFSET) {
     p.x -= __ldg(&d[RD_DX]);
     p.y -= __ldg(&d[RD_DY]);
@@ -1817,9 +1827,12 @@ __device__ __forceinline__ bool op_rf(const trk_op *__restrict__ op, Part &p, do
       if (dt < 0)
         dt = 0;
       if (!(flags & RF_SAME_DGAMMA)) {
-        double phi = omega * (t - 0 - ik * dtLight) + phase;
-        double dfactor = tau ? sqrt(1 - exp(-dt / tau)) : 1;
-        dgamma = volt * M_SIN(phi) * dfactor;
+        if (!(flags & RF_LINEAR)) {
+          double phi = omega * (t - ((flags & RF_LOCK) ? tAve : 0) - ik * dtLight) + phase;
+          double dfactor = tau ? sqrt(1 - exp(-dt / tau)) : 1;
+          dgamma = volt * M_SIN(phi) * dfactor;
+        } else
+          dgamma = dgammaAve + volt * omega * (t - tAve) * M_COS(omega * (tAve - 0.0) + phase);
       }
       if (length) {
         if ((flags & RF_END1) && ik == 0) {
@@ -2405,7 +2418,7 @@ __device__ __forceinline__ bool track_particle(const TrackArgs &a, const trk_op 
 #endif
         break;
       case OPK_RF:
-        ok = op_rf(op, p, a.Po, h.z_end, a.rf_phase);
+        ok = op_rf(op, p, a.Po, h.z_end, a.rf_phase, a.rf_tave);
         break;
       case OPK_MULT:
       case OPK_BEND:
@@ -2486,7 +2499,7 @@ __device__ __forceinline__ bool lean_op(const TrackArgs &a, const trk_op *__rest
   case OPK_CFBEND:
     return op_cfbend_fast(op, p, a.Po, z_start, ap_in, a.field);
   case OPK_RF:
-    return op_rf(op, p, a.Po, h.z_end, a.rf_phase);
+    return op_rf(op, p, a.Po, h.z_end, a.rf_phase, a.rf_tave);
   default:
     return true;
   }
@@ -2704,6 +2717,14 @@ __global__ void rf_fiducial_kernel(const double *stats, double omega, double t_r
       t0 = stats[0] / stats[1];
   }
   rf_phase[slot] = -omega * t0;
+}
+
+/* the mean arrival time of the pass for LOCK_PHASE / LINEARIZE: the same
+ * sum as the "tmean" fiducial's, divided by the particle count */
+__global__ void rf_tave_kernel(const double *stats, double *rf_tave, int slot) {
+  if (threadIdx.x != 0 || blockIdx.x != 0)
+    return;
+  rf_tave[slot] = stats[0] / stats[1];
 }
 
 /* ------------------------------------------------------------ wakes */
@@ -3607,6 +3628,10 @@ void launch_time_stats(const TimeStatsArgs &a, int grid, cudaStream_t st) {
 void launch_rf_fiducial(const double *stats, double omega, double t_reference, double *rf_phase, int slot,
                         int *status, cudaStream_t st) {
   rf_fiducial_kernel<<<1, 1, 0, st>>>(stats, omega, t_reference, rf_phase, slot, status);
+}
+
+void launch_rf_tave(const double *stats, double *rf_tave, int slot, cudaStream_t st) {
+  rf_tave_kernel<<<1, 1, 0, st>>>(stats, rf_tave, slot);
 }
 
 void launch_wake(const WakeArgs &a, int grid, cudaStream_t st) {

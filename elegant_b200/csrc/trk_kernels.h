@@ -32,6 +32,7 @@ struct TrackArgs {
   const trk_aperture *aps;
   const double *field;
   const double *rf_phase;
+  const double *rf_tave; /* mean arrival time per RF slot, this pass (LOCK_PHASE / LINEARIZE) */
   long n;
   int op_begin, op_end;
   long pass_begin, pass_end;
@@ -132,6 +133,7 @@ struct AdjArgs {
   void launch_time_stats(const TimeStatsArgs &a, int grid, cudaStream_t st);                                 \
   void launch_rf_fiducial(const double *stats, double omega, double t_reference, double *rf_phase, int slot, \
                           int *status, cudaStream_t st);                                                     \
+  void launch_rf_tave(const double *stats, double *rf_tave, int slot, cudaStream_t st);                      \
   void launch_wake(const WakeArgs &a, int grid, cudaStream_t st);                                            \
   void launch_wake_bin(const WakeArgs &a, int grid, cudaStream_t st);                                        \
   void launch_wake_apply(const WakeArgs &a, int grid, cudaStream_t st);                                      \

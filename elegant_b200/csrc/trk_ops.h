@@ -67,6 +67,8 @@ enum trk_op_kind {
 #define RF_END1 2
 #define RF_END2 4
 #define RF_OFFSET 8
+#define RF_LOCK 16   /* LOCK_PHASE: phase PHASE only, kick at t - <t> of the pass */
+#define RF_LINEAR 32 /* LINEARIZE: kick linear in t - <t> about the mean */
 
 typedef struct {
   int32_t kind;
@@ -206,6 +208,7 @@ typedef struct {
 #define RD_HALF 8   /* length/2 */
 #define RD_SOFF 9   /* fiducial sOffset = length/2 */
 #define RD_TREF 10  /* T_REFERENCE or -1 */
+#define RD_PHASE_LOCK 11 /* PI/180*PHASE, LOCK_PHASE's phase (src/simple_rfca.c:551) */
 /* i: 0 nKicks, 1 rf state slot, 2 unused, 3 flags */
 
 /* DRIFT */

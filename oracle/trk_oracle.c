@@ -1683,8 +1683,9 @@ static double beta_from_delta(double p, double delta) {
 }
 
 /* simple_rf_cavity -> trackRfCavityWithWakes (src/simple_rfca.c:264-985):
- * traveling-wave kick method (no matrix method, no backtracking, no
- * linearization, fiducial mode "tmean" with Kahan summation). */
+ * traveling-wave kick method (no matrix method, no backtracking), fiducial
+ * mode "tmean" with Kahan summation; LOCK_PHASE and LINEARIZE with the beam's
+ * mean arrival time of each pass (:500-556). */
 static long rf_cavity(double *coord, long np, const trk_elem *e, orc_rf_state *rs, double *P_central, double zEnd,
                       int *err) {
   double length = TRK_P(e, RFCA_L);
@@ -1693,8 +1694,8 @@ static long rf_cavity(double *coord, long np, const trk_elem *e, orc_rf_state *r
   (void)To;
   if (np <= 0 && orc_world <= 1)
     return np;
-  if (TRK_P(e, RFCA_CHANGE_T) || TRK_P(e, RFCA_LINEARIZE) || TRK_P(e, RFCA_LOCK_PHASE) || TRK_P(e, RFCA_CHANGE_P0) ||
-      TRK_P(e, RFCA_STANDING_WAVE)) {
+  const int lock = TRK_P(e, RFCA_LOCK_PHASE) != 0, linearize = TRK_P(e, RFCA_LINEARIZE) != 0;
+  if (TRK_P(e, RFCA_CHANGE_T) || TRK_P(e, RFCA_CHANGE_P0) || TRK_P(e, RFCA_STANDING_WAVE)) {
     *err = 1;
     return np;
   }
@@ -1715,6 +1716,10 @@ static long rf_cavity(double *coord, long np, const trk_elem *e, orc_rf_state *r
   nKicks = length ? (long)TRK_P(e, RFCA_N_KICKS) : 1;
   if (nKicks <= 0) {
     *err = 1; /* matrix method: not on this path */
+    return np;
+  }
+  if ((lock || linearize) && nKicks != 1) {
+    *err = 1; /* "Must use n_kicks=1 for linearized rf cavity" (src/simple_rfca.c:505-506) */
     return np;
   }
   length /= nKicks;
@@ -1768,6 +1773,39 @@ static long rf_cavity(double *coord, long np, const trk_elem *e, orc_rf_state *r
     same_dgamma = 1;
   }
   double timeOffset = 0;
+  double tAve = 0, dgammaAve = 0;
+  if (linearize || lock) {
+    /* the mean arrival time (src/simple_rfca.c:503-556) */
+    double error = 0, hi = 0, lo = 0;
+    for (long ip = 0; ip < np; ip++) {
+      double *c = ROW(ip);
+      double P = *P_central * (1 + c[5]), gamma;
+      double beta_i = P / (gamma = sqrt(orc_sqr(P) + 1));
+      double t = (c[4] + length / 2) / (TRK_C_MKS * beta_i) - timeOffset;
+      if (orc_exact_sums)
+        dd_acc(&hi, &lo, t);
+      else
+        tAve = kahan_plus(tAve, t, &error);
+    }
+    if (orc_exact_sums)
+      tAve = hi + lo;
+    double nt = (double)np;
+    if (orc_world > 1) {
+      double mn = DBL_MAX, mx = -DBL_MAX;
+      if (!orc_exact_sums) {
+        hi = tAve;
+        lo = 0;
+      }
+      shard_stats(&hi, &lo, &nt, &mn, &mx);
+      tAve = hi + lo;
+    }
+    tAve /= nt;
+    if (lock) {
+      phase = TRK_PI / 180 * TRK_P(e, RFCA_PHASE);
+      dgammaAve = volt * orc_sin_sel(phase);
+    } else
+      dgammaAve = volt * orc_sin_sel(omega * (tAve - timeOffset) + phase);
+  }
   for (long ip = 0; ip < np; ip++) {
     ROW(ip)[0] -= TRK_P(e, RFCA_DX);
     ROW(ip)[2] -= TRK_P(e, RFCA_DY);
@@ -1789,9 +1827,12 @@ static long rf_cavity(double *coord, long np, const trk_elem *e, orc_rf_state *r
       if ((dt = t - t0) < 0)
         dt = 0;
       if (!same_dgamma) {
-        double phi = omega * (t - 0 - ik * dtLight) + phase;
-        double dfactor = tau ? sqrt(1 - exp(-dt / tau)) : 1;
-        dgamma = volt * orc_sin_sel(phi) * dfactor;
+        if (!linearize) {
+          double phi = omega * (t - (lock ? tAve : 0) - ik * dtLight) + phase;
+          double dfactor = tau ? sqrt(1 - exp(-dt / tau)) : 1;
+          dgamma = volt * orc_sin_sel(phi) * dfactor;
+        } else
+          dgamma = dgammaAve + volt * omega * (t - tAve) * orc_cos_sel(omega * (tAve - timeOffset) + phase);
       }
       if (length) {
         if (TRK_P(e, RFCA_END1_FOCUS) && ik == 0) {

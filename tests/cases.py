@@ -137,4 +137,9 @@ ELEMENT_CASES = {
     "rfca_long": single("RFCA", L=0.5, VOLT=2e6, FREQ=500e6, PHASE=160.0, N_KICKS=5, END1_FOCUS=1, END2_FOCUS=1),
     "rfca_tref": single("RFCA", L=0.0, VOLT=1e6, FREQ=352e6, PHASE=90.0, T_REFERENCE=1e-12),
     "rfca_zero_volt": single("RFCA", L=0.3, VOLT=0.0),
+    "rfca_lock_phase": single("RFCA", L=0.0, VOLT=2e6, FREQ=352e6, PHASE=160.0, LOCK_PHASE=1),
+    "rfca_linearize": single("RFCA", L=0.3, VOLT=2e6, FREQ=352e6, PHASE=170.0, N_KICKS=1, LINEARIZE=1, END1_FOCUS=1,
+                             END2_FOCUS=1),
+    "rfca_lock_linearize": single("RFCA", L=0.2, VOLT=1e6, FREQ=500e6, PHASE=150.0, N_KICKS=1, LOCK_PHASE=1,
+                                  LINEARIZE=1),
 }

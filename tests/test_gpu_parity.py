@@ -94,6 +94,23 @@ def test_fringe_ring_exact(tracker):
     assert st["particle_passes"] == eff
 
 
+def test_locked_rf_ring_exact(tracker):
+    """LOCK_PHASE and LINEARIZE cavities in a ring with a wake: the mean
+    arrival time is taken anew on every pass (a statistics step before the
+    cavity each pass), bit-exact against the oracle."""
+    lat = configs.c2_lattice(cells=2, n_bins=300)
+    for el in lat.elements:
+        if el[0] == "RFCA":
+            el[2]["LOCK_PHASE"] = 1
+    lat.add("RFCA", "RF2", L=0.0, VOLT=5e5, FREQ=500e6, PHASE=175.0, LINEARIZE=1)
+    beam = configs.gaussian_beam(3000, seed=31)
+    nl, g, lp, le, st = gpu_run(tracker, lat, beam, 5, PC, fast=False)
+    with pyoracle.modes(exact_sums=True, cr_math=True):
+        rows, nlo, eff = oracle_run(lat, beam, 5, PC)
+    r = compare(g, rows, nl, nlo)
+    assert r["same_survivors"] and r["bit_exact"], r
+
+
 def test_fringe_ring_fast(tracker):
     lat = fringe_ring(cells=3)
     beam = configs.gaussian_beam(3000, seed=14)

@@ -62,6 +62,19 @@ def test_fringe_ring_matches_reference(mode):
 
 
 @pytest.mark.parametrize("mode", sorted(MODES))
+def test_locked_rf_ring_matches_reference(mode):
+    """LOCK_PHASE and LINEARIZE cavities take the beam's mean arrival time
+    anew on every pass."""
+    beam = configs.gaussian_beam(800, seed=30)
+    lat = configs.c2_lattice(cells=2, n_bins=300)
+    for el in lat.elements:
+        if el[0] == "RFCA":
+            el[2]["LOCK_PHASE"] = 1
+    lat.add("RFCA", "RF2", L=0.0, VOLT=5e5, FREQ=500e6, PHASE=175.0, LINEARIZE=1)
+    assert_same(*both(lat, beam, 4, mode))
+
+
+@pytest.mark.parametrize("mode", sorted(MODES))
 def test_rf_wake_ring_matches_reference(mode):
     beam = configs.gaussian_beam(1500, seed=23)
     lat = configs.c2_lattice(cells=2, n_bins=300)
