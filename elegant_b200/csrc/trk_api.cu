@@ -708,7 +708,7 @@ int run_wake(trk_context *ctx, bool fast, int opi, long pass, long fresh_pass, d
 }
 
 struct Step {
-  int kind; /* 0 SEG, 1 FID (and TAVE where the cavity needs it), 2 WAKE, 3 TAVE */
+  int kind; /* 0 SEG, 1 FID (and TAVE where the cavity needs it), 2 WAKE, 3 TAVE, 4 MATCH (CHANGE_P0) */
   int ob, oe;
 };
 
@@ -730,6 +730,14 @@ void pass_steps(const CompiledLattice &c, std::vector<int> &fid_done, std::vecto
       if (k > seg)
         steps.push_back({0, seg, k});
       steps.push_back({2, k, k + 1});
+      seg = k + 1;
+      if (c.wakes[op.i[0]].change_p0)
+        steps.push_back({4, k, k + 1});
+    }
+    if (op.kind == OPK_RF && (op.i[3] & RF_CHANGE_P0)) {
+      /* the cavity ends its segment; the central momentum follows the beam's */
+      steps.push_back({0, seg, k + 1});
+      steps.push_back({4, k, k + 1});
       seg = k + 1;
     }
   }
@@ -1097,7 +1105,7 @@ int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, 
   if (run->n_passes < 0)
     return trk_set_error(TRK_ERR_ARG, "negative pass count");
   CUDA_TRY(cudaSetDevice(ctx->device));
-  const double Po = run->p_central;
+  double Po = run->p_central; /* follows the beam at CHANGE_P0 elements */
   if (!(Po > 0))
     return trk_set_error(TRK_ERR_ARG, "p_central must be positive");
   int rc = upload_lattice(ctx, lattice, Po);
@@ -1200,6 +1208,16 @@ int trk_track(trk_context *ctx, const trk_lattice *lattice, const trk_run *run, 
             trk_exact::launch_rf_tave(ctx->d_stats, ctx->d_rf_tave, slot, ctx->stream);
             ctx->last_launches++;
           }
+        } else if (st.kind == 4) {
+          /* do_match_energy(part, np, P_central, 0) (src/simple_rfca.c:977, src/wake.c:289) */
+          if (ctx->comm)
+            return trk_set_error(TRK_ERR_UNSUPPORTED, "CHANGE_P0 in a sharded run is not on this path");
+          double pc = Po;
+          if ((rc = trk_match_energy(ctx, &pc, 0)))
+            return rc;
+          Po = pc;
+          ta.Po = Po;
+          ctx->last_launches += 3;
         } else if (st.kind == 3) {
           const trk_op &op = c.ops[st.ob];
           if ((rc = time_stats(ctx, fast, 1, op.d[RD_SOFF], Po)))

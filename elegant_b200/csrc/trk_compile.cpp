@@ -777,9 +777,8 @@ int compile_bend(const trk_lattice *l, int idx, double Po, trk_op *op, std::vect
 }
 
 int compile_rf(const trk_elem *e, trk_op *op, int slot) {
-  if (TRK_P(e, RFCA_CHANGE_T) || TRK_P(e, RFCA_CHANGE_P0) || TRK_P(e, RFCA_STANDING_WAVE))
-    return trk_set_error(TRK_ERR_UNSUPPORTED, "RFCA %s: CHANGE_T, CHANGE_P0 and STANDING_WAVE are not on this path",
-                         e->name);
+  if (TRK_P(e, RFCA_CHANGE_T) || TRK_P(e, RFCA_STANDING_WAVE))
+    return trk_set_error(TRK_ERR_UNSUPPORTED, "RFCA %s: CHANGE_T and STANDING_WAVE are not on this path", e->name);
   double length = TRK_P(e, RFCA_L);
   if (TRK_P(e, RFCA_VOLT) == 0) {
     op->kind = OPK_RFDRIFT; /* src/simple_rfca.c:389-401 */
@@ -814,6 +813,8 @@ int compile_rf(const trk_elem *e, trk_op *op, int slot) {
     flags |= RF_LOCK;
   if (linearize)
     flags |= RF_LINEAR;
+  if (TRK_P(e, RFCA_CHANGE_P0))
+    flags |= RF_CHANGE_P0; /* do_match_energy after the cavity (src/simple_rfca.c:977-978) */
   op->i[3] = flags;
   op->d[RD_OMEGA] = omega;
   op->d[RD_VOLT] = volt;
@@ -835,8 +836,6 @@ int compile_wake(const trk_elem *e, trk_op *op, CompiledWake &w) {
     return trk_set_error(TRK_ERR_ARG, "%s %s: no wake table (trk_lattice_set_wake)", tr ? "TRWAKE" : "WAKE", e->name);
   if (tr ? TRK_P(e, TRWAKE_SMOOTHING) : TRK_P(e, WAKE_SMOOTHING))
     return trk_set_error(TRK_ERR_UNSUPPORTED, "%s: SMOOTHING is not on this path", e->name);
-  if (!tr && TRK_P(e, WAKE_CHANGE_P0))
-    return trk_set_error(TRK_ERR_UNSUPPORTED, "WAKE %s: CHANGE_P0 is not on this path", e->name);
   if ((tr ? TRK_P(e, TRWAKE_START_BUNCH) : TRK_P(e, WAKE_START_BUNCH)) >= 0 ||
       (tr ? TRK_P(e, TRWAKE_END_BUNCH) : TRK_P(e, WAKE_END_BUNCH)) >= 0)
     return trk_set_error(TRK_ERR_UNSUPPORTED, "%s: START_BUNCH/END_BUNCH (bunched-beam mode) are not on this path",
@@ -877,6 +876,7 @@ int compile_wake(const trk_elem *e, trk_op *op, CompiledWake &w) {
   w.W = e->wake_w0;
   w.Wy = e->wake_w1;
   w.transverse = tr;
+  w.change_p0 = !tr && TRK_P(e, WAKE_CHANGE_P0) != 0; /* src/wake.c:289-290 */
   w.factor = tr ? TRK_P(e, TRWAKE_FACTOR) : TRK_P(e, WAKE_FACTOR);
   w.xfactor = tr ? TRK_P(e, TRWAKE_XFACTOR) : 1;
   w.yfactor = tr ? TRK_P(e, TRWAKE_YFACTOR) : 1;
@@ -1063,6 +1063,18 @@ int trk_compile(const trk_lattice *l, double Po, CompiledLattice &out) {
   }
   out.total_length = z;
   out.n_rf_slots = (int)rf_ref_ids.size();
+  /* CHANGE_P0 moves the central momentum inside the run; the radiation
+   * constants are formed from it once, at compile time */
+  bool change_p0 = false;
+  for (const trk_op &op : out.ops)
+    change_p0 = change_p0 || (op.kind == OPK_RF && (op.i[3] & RF_CHANGE_P0));
+  for (const CompiledWake &w : out.wakes)
+    change_p0 = change_p0 || w.change_p0;
+  if (change_p0)
+    for (const trk_op &op : out.ops)
+      if ((op.kind == OPK_BEND && (op.i[7] & BF_RAD)) || (op.kind == OPK_MULT && (op.i[6] & MF_RAD)))
+        return trk_set_error(TRK_ERR_UNSUPPORTED,
+                             "CHANGE_P0 with radiating elements (SYNCH_RAD, ISR) is not on this path");
   return TRK_OK;
 }
 

@@ -21,6 +21,7 @@ struct CompiledWake {
   long ramp_passes = 0;
   int x_power = 1, y_power = 1, x_probe = 0, y_probe = 0;
   double tdx = 0, tdy = 0, tilt = 0;
+  int change_p0 = 0; /* WAKE CHANGE_P0: match the central momentum to the beam's after the kick */
 };
 
 struct CompiledLattice {

@@ -69,6 +69,7 @@ enum trk_op_kind {
 #define RF_OFFSET 8
 #define RF_LOCK 16   /* LOCK_PHASE: phase PHASE only, kick at t - <t> of the pass */
 #define RF_LINEAR 32 /* LINEARIZE: kick linear in t - <t> about the mean */
+#define RF_CHANGE_P0 64 /* CHANGE_P0: the central momentum follows the beam's after the cavity */
 
 typedef struct {
   int32_t kind;

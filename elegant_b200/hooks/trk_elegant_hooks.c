@@ -377,7 +377,10 @@ long gpu_trackRfCavityWithWakes(long np, RFCA *rfca, double **accepted, double *
   if (wake || trwake || LSCKick)
     bombElegant("RFCA with attached wakes is outside the GPU path", NULL);
   trk_lattice *L = element_lattice(T_RFCA, (const char *)rfca, "RF");
-  return element_on_device(L, g_pass, zEnd - rfca->length, NULL, state_of(rfca), *P_central);
+  const long n = element_on_device(L, g_pass, zEnd - rfca->length, NULL, state_of(rfca), *P_central);
+  if (rfca->change_p0) /* src/simple_rfca.c:977-978 */
+    check(trk_match_energy(g_ctx, P_central, 0), "trk_match_energy");
+  return n;
 }
 
 void gpu_track_through_wake(long np0, WAKE *wakeData, double *PoInput, RUN *run, long i_pass, CHARGE *charge) {
@@ -389,6 +392,8 @@ void gpu_track_through_wake(long np0, WAKE *wakeData, double *PoInput, RUN *run,
   trk_element_state *st = state_of(wakeData);
   st->macro_charge = wakeData->macroParticleCharge;
   element_on_device(L, i_pass, 0.0, NULL, st, *PoInput);
+  if (wakeData->change_p0) /* src/wake.c:289-290 */
+    check(trk_match_energy(g_ctx, PoInput, 0), "trk_match_energy");
 }
 
 void gpu_track_through_trwake(long np0, TRWAKE *wakeData, double Po, RUN *run, long i_pass, CHARGE *charge) {

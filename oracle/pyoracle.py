@@ -137,6 +137,20 @@ def track(lattice, beam, n_passes, p_central, pass_offset=0):
     return rows, res.n_left, res.particle_passes
 
 
+def final_p_central(lattice, beam, n_passes, p_central, pass_offset=0):
+    """The central momentum after tracking (CHANGE_P0 elements move it)."""
+    lib = load()
+    nat = lattice.native(lib)
+    rows = np.zeros((beam.shape[0], STRIDE), dtype=np.float64)
+    rows[:, :7] = beam[:, :7]
+    pc = ctypes.c_double(p_central)
+    res = _Result()
+    _check(lib, lib.orc_track(nat.ptr, rows.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), rows.shape[0],
+                              n_passes, pass_offset, ctypes.byref(pc), ctypes.byref(res)))
+    nat.close()
+    return pc.value
+
+
 def track_element(lattice, element, beam, pass_index, p_central):
     lib = load()
     nat = lattice.native(lib)

@@ -1682,6 +1682,8 @@ static double beta_from_delta(double p, double delta) {
   return p / sqrt(p * p + 1);
 }
 
+void orc_match_energy(double *coord, long np, double *P_central, int change_beam);
+
 /* simple_rf_cavity -> trackRfCavityWithWakes (src/simple_rfca.c:264-985):
  * traveling-wave kick method (no matrix method, no backtracking), fiducial
  * mode "tmean" with Kahan summation; LOCK_PHASE and LINEARIZE with the beam's
@@ -1695,7 +1697,7 @@ static long rf_cavity(double *coord, long np, const trk_elem *e, orc_rf_state *r
   if (np <= 0 && orc_world <= 1)
     return np;
   const int lock = TRK_P(e, RFCA_LOCK_PHASE) != 0, linearize = TRK_P(e, RFCA_LINEARIZE) != 0;
-  if (TRK_P(e, RFCA_CHANGE_T) || TRK_P(e, RFCA_CHANGE_P0) || TRK_P(e, RFCA_STANDING_WAVE)) {
+  if (TRK_P(e, RFCA_CHANGE_T) || TRK_P(e, RFCA_STANDING_WAVE) || (TRK_P(e, RFCA_CHANGE_P0) && orc_world > 1)) {
     *err = 1;
     return np;
   }
@@ -1868,7 +1870,10 @@ static long rf_cavity(double *coord, long np, const trk_elem *e, orc_rf_state *r
     ROW(ip)[0] += TRK_P(e, RFCA_DX);
     ROW(ip)[2] += TRK_P(e, RFCA_DY);
   }
-  return remove_invalid(coord, np, zEnd, *P_central);
+  np = remove_invalid(coord, np, zEnd, *P_central);
+  if (TRK_P(e, RFCA_CHANGE_P0)) /* src/simple_rfca.c:977-978 */
+    orc_match_energy(coord, np, P_central, 0);
+  return np;
 }
 
 /* ----------------------------------------------------------------- wakes */
@@ -1925,11 +1930,12 @@ static int wake_table_setup(const trk_elem *e, double *dt, long *i0, int acausal
 }
 
 /* track_through_wake (src/wake.c:23-304), one bunch, no smoothing */
-static int track_through_wake(double *coord, long np, const trk_elem *e, double Po, long i_pass,
+static int track_through_wake(double *coord, long np, const trk_elem *e, double *P_central, long i_pass,
                               orc_wake_state *ws, const double *chargeMacro) {
   double dt, tmean, tmin, tmax, factor, rampFactor;
   long i0, nb;
-  if (TRK_P(e, WAKE_SMOOTHING) || TRK_P(e, WAKE_CHANGE_P0))
+  const double Po = *P_central;
+  if (TRK_P(e, WAKE_SMOOTHING) || (TRK_P(e, WAKE_CHANGE_P0) && orc_world > 1))
     return 1;
   if (wake_table_setup(e, &dt, &i0, (int)TRK_P(e, WAKE_ACAUSAL_ALLOWED)))
     return 1;
@@ -2040,6 +2046,8 @@ static int track_through_wake(double *coord, long np, const trk_elem *e, double 
   free(Vtime);
   free(time);
   free(pbin);
+  if (TRK_P(e, WAKE_CHANGE_P0)) /* src/wake.c:289-290 */
+    orc_match_energy(coord, np, P_central, 0);
   return 0;
 }
 
@@ -2232,7 +2240,7 @@ static int track_one_element(const trk_lattice *l, int idx, double *coord, long 
     nLeft = rf_cavity(coord, nToTrack, e, &rs->rf[idx], P_central, z, &err);
     break;
   case TRK_WAKE:
-    err = track_through_wake(coord, nToTrack, e, *P_central, i_pass, &rs->wake[idx],
+    err = track_through_wake(coord, nToTrack, e, P_central, i_pass, &rs->wake[idx],
                              rs->have_charge ? &rs->chargeMacro : NULL);
     break;
   case TRK_TRWAKE:

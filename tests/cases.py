@@ -140,6 +140,7 @@ ELEMENT_CASES = {
     "rfca_lock_phase": single("RFCA", L=0.0, VOLT=2e6, FREQ=352e6, PHASE=160.0, LOCK_PHASE=1),
     "rfca_linearize": single("RFCA", L=0.3, VOLT=2e6, FREQ=352e6, PHASE=170.0, N_KICKS=1, LINEARIZE=1, END1_FOCUS=1,
                              END2_FOCUS=1),
+    "rfca_change_p0": single("RFCA", L=0.2, VOLT=3e6, FREQ=352e6, PHASE=60.0, N_KICKS=2, CHANGE_P0=1),
     "rfca_lock_linearize": single("RFCA", L=0.2, VOLT=1e6, FREQ=500e6, PHASE=150.0, N_KICKS=1, LOCK_PHASE=1,
                                   LINEARIZE=1),
 }

@@ -111,6 +111,24 @@ def test_locked_rf_ring_exact(tracker):
     assert r["same_survivors"] and r["bit_exact"], r
 
 
+def test_change_p0_ring_exact(tracker):
+    """RFCA and WAKE with CHANGE_P0: a match step after each moves the
+    central momentum to the beam's; every coordinate bit-exact against the
+    oracle and the final central momentum equal to the oracle's."""
+    lat = configs.c2_lattice(cells=2, n_bins=300)
+    for el in lat.elements:
+        if el[0] in ("RFCA", "WAKE"):
+            el[2]["CHANGE_P0"] = 1
+    beam = configs.gaussian_beam(3000, seed=33)
+    nl, g, lp, le, st = gpu_run(tracker, lat, beam, 4, PC, fast=False)
+    with pyoracle.modes(exact_sums=True, cr_math=True):
+        rows, nlo, eff = oracle_run(lat, beam, 4, PC)
+        pc = pyoracle.final_p_central(lat, beam, 4, PC)
+    r = compare(g, rows, nl, nlo)
+    assert r["same_survivors"] and r["bit_exact"], r
+    assert st["p_central"] == pc != PC
+
+
 def test_fringe_ring_fast(tracker):
     lat = fringe_ring(cells=3)
     beam = configs.gaussian_beam(3000, seed=14)

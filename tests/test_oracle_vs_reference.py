@@ -75,6 +75,19 @@ def test_locked_rf_ring_matches_reference(mode):
 
 
 @pytest.mark.parametrize("mode", sorted(MODES))
+def test_change_p0_ring_matches_reference(mode):
+    """RFCA and WAKE with CHANGE_P0: the central momentum follows the beam's
+    mean after each (do_match_energy), and every later element sees it."""
+    beam = configs.gaussian_beam(800, seed=32)
+    lat = configs.c2_lattice(cells=2, n_bins=300)
+    for el in lat.elements:
+        if el[0] in ("RFCA", "WAKE"):
+            el[2]["CHANGE_P0"] = 1
+    r, o = both(lat, beam, 4, mode)
+    assert_same(r, o)
+
+
+@pytest.mark.parametrize("mode", sorted(MODES))
 def test_rf_wake_ring_matches_reference(mode):
     beam = configs.gaussian_beam(1500, seed=23)
     lat = configs.c2_lattice(cells=2, n_bins=300)
