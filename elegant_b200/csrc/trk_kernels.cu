@@ -1343,6 +1343,95 @@ __device__ __forceinline__ void bend_edge(int mode, const double *__restrict__ d
   }
 }
 
+/* the radiation correction of delta at a bend edge of nonzero angle,
+ * dp' x tan(e) with dp' = -rad_coef F^2 (1+delta)^2 sqrt((1+x/rho0)^2 + x'^2
+ * + y'^2) (src/csbend.c:1215-1222, :1270-1281) */
+__device__ __noinline__ double rad_edge_dp(const double *__restrict__ d, int te_index, int fmode, int eo1,
+                                           const double *__restrict__ Fx_xy, const double *__restrict__ Fy_xy,
+                                           double rho0, double x, double xp, double y, double yp, double dp) {
+  double Fx, Fy;
+  if (fmode == 0) {
+    Fx = 0;
+    Fy = 1;
+  } else
+    bend_fields(fmode, eo1, Fx_xy, Fy_xy, x, y, Fx, Fy);
+  const double dp_prime =
+    -__ldg(&d[BD_RAD]) * (sqr(Fx) + sqr(Fy)) * sqr(1 + dp) * sqrt(sqr(1 + x / rho0) + sqr(xp) + sqr(yp));
+  return dp_prime * x * __ldg(&d[te_index]);
+}
+
+/* integrate_csbend_ordn_expanded (src/csbend.c:1722-1900): leading-order
+ * drift, aperture after every drift substep as well as per slice; out of
+ * line so that the exact body's register allocation does not carry it */
+__device__ __noinline__ bool bend_body_expanded(const trk_op *__restrict__ op, const double *__restrict__ Fx_xy,
+                                                const double *__restrict__ Fy_xy, int fmode, int eo1, int nSlices,
+                                                int nSub, int flags, double rho0, double rho_a, const trk_aperture *ap,
+                                                bool aptilt, double apc, double aps, const IsrKey *isr, double &X,
+                                                double &QX, double &Y, double &QY, double &D, double &dist,
+                                                double &dz_lost) {
+  const double *d = op->d;
+  const double sl = __ldg(&d[BD_SLICE]);
+  bool ok = true;
+  for (int i = 0; i < nSlices && ok; i++) {
+    if (!check_aperture(X, Y, ap, aptilt, apc, aps)) {
+      ok = false;
+      break;
+    }
+    for (int j = 0; j < nSub; j++) {
+      const double dsh = __ldg(&d[BD_DSH + j]);
+      QX += dsh * (1 + D) / (2 * rho0);
+      dist += dsh * (1 + (sqr(QX) + sqr(QY)) / 2);
+      dz_lost += dsh;
+      X += QX * dsh / (1 + D);
+      Y += QY * dsh / (1 + D);
+      QX += dsh * (1 + D) / (2 * rho0);
+      if (!check_aperture(X, Y, ap, aptilt, apc, aps)) {
+        ok = false;
+        break;
+      }
+      if (j == nSub - 1)
+        break;
+      const double ds = __ldg(&d[BD_DS + j]);
+      double Fx, Fy;
+      if (fmode == 0) {
+        Fx = 0;
+        Fy = 1;
+      } else
+        bend_fields(fmode, eo1, Fx_xy, Fy_xy, X, Y, Fx, Fy);
+      QX += -ds * (1 + X / rho0) * Fy / rho_a;
+      QY += ds * (1 + X / rho0) * Fx / rho_a;
+      if (flags & BF_RAD) {
+        /* src/csbend.c:1833-1863 (dsISR = s/3 in this integrator) */
+        const double hX = 1 + X * __ldg(&d[BD_RHOINV]);
+        const double f = hX / sqrt(sqr(1 + D) - sqr(QX) - sqr(QY));
+        const double xpr = QX * f, ypr = QY * f;
+        const double dsFactor = sqrt(sqr(hX) + sqr(xpr) + sqr(ypr));
+        const double F2 = sqr(Fx) + sqr(Fy);
+        const double deltaFactor = sqr(1 + D);
+        const double dsISR = sl / 3;
+        QX /= (1 + D);
+        QY /= (1 + D);
+        const double rad_coef = __ldg(&d[BD_RAD]);
+        if (rad_coef != 0)
+          D -= rad_coef * deltaFactor * F2 * ds * dsFactor;
+        if ((flags & BF_ISR) && isr && !(isr->single && (flags & BF_ISR1OFF))) {
+          const double g =
+            trk_isr_gauss(isr->seed, isr->id, isr->pass, isr->elem, (unsigned)(i * 8 + j), isr->limit);
+          D -= __ldg(&d[BD_ISR]) * deltaFactor * pow(F2, 0.75) * sqrt(dsISR * dsFactor) * g;
+        }
+        QX *= (1 + D);
+        QY *= (1 + D);
+      } else if (flags & BF_ISR_ROUNDTRIP) {
+        QX /= (1 + D);
+        QY /= (1 + D);
+        QX *= (1 + D);
+        QY *= (1 + D);
+      }
+    }
+  }
+  return ok;
+}
+
 /* track_through_csbend (src/csbend.c:654-1434) with integrate_csbend_ordn
  * (src/csbend.c:1459-1720); no radiation, MALIGN_METHOD=0. */
 __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, double Po, double z_start,
@@ -1389,18 +1478,8 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
     bend_edge(edge1, d, BD_E1, -1, rho_a, nidx, Fr, expanded, x, xp, y, yp, s, dp);
 
   double X = x, QX, Y = y, QY, S = 0, D = dp;
-  if (flags & BF_RADE1) {
-    /* radiation: delta pre-adjusted for the sector integration (src/csbend.c:1215-1222) */
-    double Fx, Fy;
-    if (fmode == 0) {
-      Fx = 0;
-      Fy = 1;
-    } else
-      bend_fields(fmode, eo1, Fx_xy, Fy_xy, x, y, Fx, Fy);
-    const double dp_prime =
-      -__ldg(&d[BD_RAD]) * (sqr(Fx) + sqr(Fy)) * sqr(1 + dp) * sqrt(sqr(1 + x / rho0) + sqr(xp) + sqr(yp));
-    D -= dp_prime * x * __ldg(&d[BD_TE1]);
-  }
+  if (flags & BF_RADE1) /* radiation: delta pre-adjusted for the sector integration (src/csbend.c:1215-1222) */
+    D -= rad_edge_dp(d, BD_TE1, fmode, eo1, Fx_xy, Fy_xy, rho0, x, xp, y, yp, dp);
   /* convertToDipoleCanonicalCoordinates */
   {
     double f = expanded ? (1 + D) : (1 + D) / sqrt(1 + sqr(xp) + sqr(yp));
@@ -1412,65 +1491,8 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
   double dist = 0, dz_lost = 0;
   const double sl = __ldg(&d[BD_SLICE]);
   if (expanded) {
-    /* integrate_csbend_ordn_expanded (src/csbend.c:1722-1900): leading-order
-     * drift, aperture after every drift substep as well as per slice */
-    for (int i = 0; i < nSlices && ok; i++) {
-      if (!check_aperture(X, Y, ap, aptilt, apc, aps)) {
-        ok = false;
-        break;
-      }
-      for (int j = 0; j < nSub; j++) {
-        const double dsh = __ldg(&d[BD_DSH + j]);
-        QX += dsh * (1 + D) / (2 * rho0);
-        dist += dsh * (1 + (sqr(QX) + sqr(QY)) / 2);
-        dz_lost += dsh;
-        X += QX * dsh / (1 + D);
-        Y += QY * dsh / (1 + D);
-        QX += dsh * (1 + D) / (2 * rho0);
-        if (!check_aperture(X, Y, ap, aptilt, apc, aps)) {
-          ok = false;
-          break;
-        }
-        if (j == nSub - 1)
-          break;
-        const double ds = __ldg(&d[BD_DS + j]);
-        double Fx, Fy;
-        if (fmode == 0) {
-          Fx = 0;
-          Fy = 1;
-        } else
-          bend_fields(fmode, eo1, Fx_xy, Fy_xy, X, Y, Fx, Fy);
-        QX += -ds * (1 + X / rho0) * Fy / rho_a;
-        QY += ds * (1 + X / rho0) * Fx / rho_a;
-        if (flags & BF_RAD) {
-          /* src/csbend.c:1833-1863 (dsISR = s/3 in this integrator) */
-          const double hX = 1 + X * __ldg(&d[BD_RHOINV]);
-          const double f = hX / sqrt(sqr(1 + D) - sqr(QX) - sqr(QY));
-          const double xpr = QX * f, ypr = QY * f;
-          const double dsFactor = sqrt(sqr(hX) + sqr(xpr) + sqr(ypr));
-          const double F2 = sqr(Fx) + sqr(Fy);
-          const double deltaFactor = sqr(1 + D);
-          const double dsISR = sl / 3;
-          QX /= (1 + D);
-          QY /= (1 + D);
-          const double rad_coef = __ldg(&d[BD_RAD]);
-          if (rad_coef != 0)
-            D -= rad_coef * deltaFactor * F2 * ds * dsFactor;
-          if ((flags & BF_ISR) && isr && !(isr->single && (flags & BF_ISR1OFF))) {
-            const double g =
-              trk_isr_gauss(isr->seed, isr->id, isr->pass, isr->elem, (unsigned)(i * 8 + j), isr->limit);
-            D -= __ldg(&d[BD_ISR]) * deltaFactor * pow(F2, 0.75) * sqrt(dsISR * dsFactor) * g;
-          }
-          QX *= (1 + D);
-          QY *= (1 + D);
-        } else if (flags & BF_ISR_ROUNDTRIP) {
-          QX /= (1 + D);
-          QY /= (1 + D);
-          QX *= (1 + D);
-          QY *= (1 + D);
-        }
-      }
-    }
+    ok = bend_body_expanded(op, Fx_xy, Fy_xy, fmode, eo1, nSlices, nSub, flags, rho0, rho_a, ap, aptilt, apc, aps, isr,
+                            X, QX, Y, QY, D, dist, dz_lost);
   } else if (fmode == 0 && !(flags & BF_RAD)) { /* the radiating dipole takes the general body */
     int done = 0;
 #if TRK_FAST
@@ -1631,18 +1653,8 @@ __device__ __forceinline__ bool op_bend(const trk_op *__restrict__ op, Part &p, 
     p.dp = Po * (1 + D);
     return false;
   }
-  if (flags & BF_RADE2) {
-    /* radiation: delta post-adjusted (src/csbend.c:1270-1281) */
-    double Fx, Fy;
-    if (fmode == 0) {
-      Fx = 0;
-      Fy = 1;
-    } else
-      bend_fields(fmode, eo1, Fx_xy, Fy_xy, X, Y, Fx, Fy);
-    const double dp_prime =
-      -__ldg(&d[BD_RAD]) * (sqr(Fx) + sqr(Fy)) * sqr(1 + D) * sqrt(sqr(1 + X / rho0) + sqr(QX) + sqr(QY));
-    D -= dp_prime * X * __ldg(&d[BD_TE2]);
-  }
+  if (flags & BF_RADE2) /* radiation: delta post-adjusted (src/csbend.c:1270-1281) */
+    D -= rad_edge_dp(d, BD_TE2, fmode, eo1, Fx_xy, Fy_xy, rho0, X, QX, Y, QY, D);
 #if TRK_FAST
   if (flags & BF_RAD) {
     const double p0 = Po * (1 + dp0), p1 = Po * (1 + D);
@@ -1787,6 +1799,24 @@ __device__ __forceinline__ void add_energy(Part &p, double t, double Po, double 
 
 /* trackRfCavityWithWakes (src/simple_rfca.c:295-985), kick method,
  * traveling wave, per particle; ends with removeInvalidParticles. */
+/* LOCK_PHASE / LINEARIZE set-up (src/simple_rfca.c:550-556): the locked
+ * phase replaces the fiducial one; returns dgammaAve.  Out of line, as is
+ * the linearized kick, so the common cavity carries neither. */
+__device__ __noinline__ double rf_locked_phase(const double *__restrict__ d, int flags, double volt, double omega,
+                                               double tAve, double &phase) {
+  if (flags & RF_LOCK) {
+    phase = __ldg(&d[RD_PHASE_LOCK]);
+    return volt * M_SIN(phase);
+  }
+  return volt * M_SIN(omega * (tAve - 0.0) + phase);
+}
+
+/* the linearized kick (src/simple_rfca.c:603-604) */
+__device__ __noinline__ double rf_linear_dgamma(double dgammaAve, double volt, double omega, double t, double tAve,
+                                                double phase) {
+  return dgammaAve + volt * omega * (t - tAve) * M_COS(omega * (tAve - 0.0) + phase);
+}
+
 __device__ __forceinline__ bool op_rf(const trk_op *__restrict__ op, Part &p, double Po, double z_end,
                                       const double *__restrict__ rf_phase, const double *__restrict__ rf_tave) {
   const double *d = op->d;
@@ -1805,11 +1835,7 @@ __device__ __forceinline__ bool op_rf(const trk_op *__restrict__ op, Part &p, do
   double tAve = 0, dgammaAve = 0;
   if (flags & (RF_LOCK | RF_LINEAR)) {
     tAve = rf_tave[slot];
-    if (flags & RF_LOCK) {
-      phase = __ldg(&d[RD_PHASE_LOCK]);
-      dgammaAve = volt * M_SIN(phase);
-    } else
-      dgammaAve = volt * M_SIN(omega * (tAve - 0.0) + phase);
+    dgammaAve = rf_locked_phase(d, flags, volt, omega, tAve, phase);
   }
   if (flags & RF_OFFSET) {
     p.x -= __ldg(&d[RD_DX]);
@@ -1832,7 +1858,7 @@ __device__ __forceinline__ bool op_rf(const trk_op *__restrict__ op, Part &p, do
           double dfactor = tau ? sqrt(1 - exp(-dt / tau)) : 1;
           dgamma = volt * M_SIN(phi) * dfactor;
         } else
-          dgamma = dgammaAve + volt * omega * (t - tAve) * M_COS(omega * (tAve - 0.0) + phase);
+          dgamma = rf_linear_dgamma(dgammaAve, volt, omega, t, tAve, phase);
       }
       if (length) {
         if ((flags & RF_END1) && ik == 0) {
