@@ -111,6 +111,20 @@ def test_locked_rf_ring_exact(tracker):
     assert r["same_survivors"] and r["bit_exact"], r
 
 
+def test_fringe_and_locked_rf_ring_100_turns_exact(tracker):
+    """Every edge model, a locked cavity and CHANGE_P0 in one ring for 100
+    turns: the parity build bit-exact against the oracle throughout."""
+    lat = fringe_ring(cells=2)
+    lat.add("RFCA", "RF", L=0.0, VOLT=3e6, FREQ=352e6, PHASE=175.0, LOCK_PHASE=1, CHANGE_P0=1)
+    beam = configs.gaussian_beam(1000, seed=34)
+    nl, g, lp, le, st = gpu_run(tracker, lat, beam, 100, PC, fast=False)
+    with pyoracle.modes(exact_sums=True, cr_math=True):
+        rows, nlo, eff = oracle_run(lat, beam, 100, PC)
+    r = compare(g, rows, nl, nlo)
+    assert r["same_survivors"] and r["bit_exact"], r
+    assert st["particle_passes"] == eff
+
+
 def test_change_p0_ring_exact(tracker):
     """RFCA and WAKE with CHANGE_P0: a match step after each moves the
     central momentum to the beam's; every coordinate bit-exact against the
